@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 fractal-flame render path.
+
+One step = one whole frame of the full forward workload: a synthetic flame of
+8 transforms + 1 final (each 3-5 of the twelve variations), 1920x1080 with 2x
+supersampling (3840x2160 internal), 1e9 plotted samples from 65,536 walkers,
+density estimation radius 9 -> 0, log tone map fused with the firefly
+downsample.  `value` is samples/s on the device (config already parsed into
+a device table, output left in HBM); `e2e` is the same frame through the
+reference's own boundary (`fae_call` render request -> RGBA8 in host memory).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank renders its own shard of walkers (weak scaling, no
+data-path collective); rank 0 prints one JSON line.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (ROOT, os.path.join(ROOT, "fflame-rust_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+FULL_SEED = 6
+
+
+def workload(name):
+    from ffb200 import synthetic
+    if name == "full_1080p_ss2":
+        return dict(cfg=synthetic.full_flame(FULL_SEED), width=1920, height=1080, supersample=2,
+                    iterations=1_000_000_000, walkers=65536,
+                    desc="8 xforms + final, 12 variations, 1920x1080 ss2 (3840x2160 internal), 1e9 samples, "
+                         "65536 walkers, DE radius 9->0, u32 count + FP32 RGB histogram")
+    if name == "plain_256":
+        return dict(cfg=synthetic.plain_flame(1), width=256, height=256, supersample=1, iterations=10_000_000,
+                    walkers=16384, desc="3 xforms {linear,sinusoidal,spherical}, 256x256 ss1, 1e7 samples, no DE")
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        load = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch of the chaos kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"ffb_chaos_{name}.txt")
+    try:
+        for line in open(path, encoding="utf-8"):
+            if line.startswith("dram_bytes_per_launch_full:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------ CPU baseline --
+def cpu_baseline(wl, budget_s=12.0, threads=None):
+    """The oracle port on the host cores, on a bounded sample of the same
+    workload (same flame, same internal resolution, same RNG); samples/s."""
+    from oracle import oracle as O
+    O.build()
+    threads = threads or min(os.cpu_count() or 1, 64)
+    W, H = wl["width"] * wl["supersample"], wl["height"] * wl["supersample"]
+    fl = O.Flame(wl["cfg"], W, H)
+    walkers = threads * 64
+    iters = 64
+    t0 = time.perf_counter()
+    fl.render(walkers, iters + 20, threads=threads)
+    dt = time.perf_counter() - t0
+    rate = walkers * iters / max(dt, 1e-6)
+    per = max(64, int(rate * budget_s / walkers))
+    t0 = time.perf_counter()
+    plotted, _, _, _ = fl.render(walkers, per + 20, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": plotted / dt, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"{plotted:.3g} samples of the same flame at {W}x{H} ({walkers} walkers x {per} after burn-in 20), "
+                      f"{dt:.1f} s, f32, private histograms per thread"}
+
+
+# ------------------------------------------------------------------ ours --
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from ffb200 import Engine, _native
+
+    torch.cuda.set_device(local_rank)
+    wl = workload(args.workload)
+    cfg = json.dumps(wl["cfg"])
+    W, H, ss = wl["width"], wl["height"], wl["supersample"]
+    r = _native.Renderer(local_rank)
+    job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, walker0=rank * wl["walkers"],
+               seed=0x5EED + 0)
+    d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    out = r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=True, **job)   # compile + first frame
+    samples_per_step = out.total_iterations
+    launches_per_step = out.kernel_launches
+    for _ in range(args.warmup):
+        r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=False, **job)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    clocks = ClockSampler(local_rank) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_start.record()
+    for _ in range(args.steps):
+        r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=False, **job)
+    t_end.record()
+    t_end.synchronize()
+    torch.cuda.synchronize()
+    ms = t_start.elapsed_time(t_end) / args.steps
+    clk = clocks.stop() if clocks else None
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if rank != 0:
+        return None
+
+    # Dominant kernel: the chaos game alone (events around its launch).
+    chaos_ms, inframe = [], []
+    for _ in range(3):
+        _, _, o = r.histogram(cfg, W, H, **job)
+        chaos_ms.append(o.render_time_ms)
+        inframe.append(o.inframe_samples)
+    c_ms = statistics.median(chaos_ms)
+    bytes_per_launch = 16.0 * statistics.median(inframe)          # 4 x 4-byte RMW per splatted sample
+    peaks, peak_kind = measured_peaks()
+    achieved = bytes_per_launch / (c_ms * 1e-3) / 1e9
+    traffic = profile_traffic(args.workload)
+    # The splat's own ceiling: random-address 4-atomic splats into a histogram
+    # of the same size (microbenchmark in the same run).
+    npx = W * ss * H * ss
+    bench_ms = r.atomic_bench(npx, 400_000_000, 0)
+    splat_peak = 400_000_000 / (bench_ms * 1e-3)
+    splat_rate = statistics.median(inframe) / (c_ms * 1e-3)
+
+    # End to end: the reference's boundary, host buffers, copies inside.
+    eng = Engine()
+    req_iters = wl["iterations"]
+    e2e_times = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        image = eng.render(cfg, W, H, iterations=req_iters, supersample=ss)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_times.append(dt)
+        info = image.info
+    e2e_s = statistics.mean(e2e_times)
+    o_e2e = _native.Output()
+    # bytes the library copies for one render request (h2d: tables; d2h: RGBA8)
+    rr = r.render(cfg, W, H, **job)[1]
+    line = {
+        "metric": "samples/s", "value": samples_per_step * world / (ms * 1e-3), "unit": "samples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded flame generator; no dataset)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
+                   "samples_per_step": samples_per_step, "walkers": wl["walkers"], "rng": "philox",
+                   "l2": "histogram 132.7 MB > 126 MB L2, cleared every step", "parallelism": f"walker shards x{world}"},
+        "ms_per_frame": ms,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "kernel": "ffb_chaos", "kernel_ms": c_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "peak_kind": peak_kind},
+        "l2_atomic": {"achieved_splats_per_s": splat_rate, "peak_splats_per_s": splat_peak,
+                      "frac": splat_rate / splat_peak, "peak_from": "ffb_atomic_bench kind 0, same histogram size"},
+        "e2e": {"value": samples_per_step / e2e_s, "unit": "samples/s", "ms_per_frame": e2e_s * 1e3,
+                "h2d_bytes_per_step": rr.h2d_bytes, "d2h_bytes_per_step": W * H * 4,
+                "path": "fae_call render request (JSON config in, RGBA8 host bytes out)",
+                "info_ms": info.get("ms") if info else None},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    return line
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU path: there is none (variations exist only as
+    WGSL; benches/flame_bench.rs:1-10), so the oracle port of it runs on all
+    host threads, each step a bounded sample of the same workload."""
+    if rank != 0:
+        return None
+    wl = workload(args.workload)
+    from oracle import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    W, H = wl["width"] * wl["supersample"], wl["height"] * wl["supersample"]
+    fl = O.Flame(wl["cfg"], W, H)
+    walkers = threads * 32
+    per = 128
+    rates = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        plotted, _, _, _ = fl.render(walkers, per + 20, threads=threads, walker0=i * walkers)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            rates.append(plotted / dt)
+    v = statistics.mean(rates)
+    ms_frame = wl["iterations"] / v * 1e3
+    sample = f"{walkers * per} samples a step ({walkers} walkers x {per}) of the same flame at {W}x{H}"
+    return {
+        "impl": "reference", "metric": "samples/s", "value": v, "unit": "samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_frame, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flame generator)",
+        "config": {"workload": args.workload, "desc": wl["desc"]},
+        "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference has no CPU render path; this is the oracle's restatement of it (oracle/)",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        line = run_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

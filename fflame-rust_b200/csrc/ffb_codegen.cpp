@@ -1,0 +1,172 @@
+// ffb_codegen.cpp -- see ffb_codegen.hpp.
+
+#include "ffb_codegen.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <sstream>
+
+#include "ffb_device_src.inc"
+
+namespace ffb {
+
+namespace {
+
+// Normal-phase variations: those a normal transform uses at a weight other
+// than 0, in local order.  The reference emits every active variation and
+// gates each on `xform.variations[idx] != 0.0` (shader_builder_v2.rs
+// 2755-2763); one no transform uses never fires, so leaving it out changes
+// nothing.
+std::vector<const VarDef*> normal_vars(const Flame& f) {
+    std::vector<const VarDef*> out;
+    for (const VarDef* v : f.local) {
+        bool used = false;
+        for (auto& x : f.xf) used |= x.var_weight(v) != 0.0f;
+        if (used) out.push_back(v);
+    }
+    return out;
+}
+
+std::vector<const VarDef*> final_vars(const Flame& f, const XForm& x) {
+    std::vector<const VarDef*> out;
+    for (const VarDef* v : f.local) if (x.var_weight(v) != 0.0f) out.push_back(v);
+    return out;
+}
+
+std::string call(const VarDef* v, const std::string& prm0, const std::string& prm1, int slot) {
+    std::ostringstream o;
+    o << v->fn << "(x, y";
+    if (v->needs_rng) o << ", rng.draw(" << slot << ")";
+    if (v->nparams >= 1) o << ", " << prm0;
+    if (v->nparams >= 2) o << ", " << prm1;
+    o << ", ox, oy)";
+    return o.str();
+}
+
+}  // namespace
+
+Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads) {
+    Plan p;
+    p.rng_mode = rng_mode;
+    p.math_mode = math_mode;
+    p.threads = threads;
+    p.maxx = std::max<int>(maxx, (int)f.xf.size());
+    p.normal = normal_vars(f);
+    int slot = 2;                                   // 0: transform pick, 1: opacity
+    for (const VarDef* v : p.normal) p.normal_slot.push_back(v->needs_rng ? slot++ : -1);
+    for (int c : f.fin_chain) {
+        Plan::Fin fi;
+        fi.vars = final_vars(f, f.fin[c]);
+        for (const VarDef* v : fi.vars) fi.slot.push_back(v->needs_rng ? slot++ : -1);
+        p.fin.push_back(fi);
+    }
+    p.n_slots = slot;
+    for (auto& x : f.xf) p.has_post |= x.post;
+    const int M = p.maxx, NVN = (int)p.normal.size();
+    p.t_cum = 1;
+    p.t_xf = p.t_cum + M;
+    p.t_vw = p.t_xf + 16 * M;
+    p.t_vp = p.t_vw + NVN * M;
+    p.t_fin = p.t_vp + 2 * NVN * M;
+    int off = p.t_fin;
+    for (auto& fi : p.fin) { fi.off = off; off += 13 + 3 * (int)fi.vars.size(); }
+    p.table_size = off;
+
+    std::ostringstream s;
+    s << "// generated by ffb_codegen for one flame structure\n";
+    s << "#define FFB_MAXX " << M << "\n#define FFB_NVN " << NVN << "\n#define FFB_NFIN " << p.fin.size() << "\n";
+    s << "#define FFB_HAS_POST " << (p.has_post ? 1 : 0) << "\n#define FFB_NSLOTS " << p.n_slots << "\n";
+    s << "#define FFB_RNG_MODE " << rng_mode << "\n#define FFB_THREADS " << threads << "\n";
+    if (math_mode == MATH_SFU) s << "#define FFB_SFU 1\n";
+    s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
+    s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw
+      << "\n#define T_VP " << p.t_vp << "\n";
+    s << kDeviceSrc << "\n";
+    // The normal phase (shader_builder_v2.rs:2714-2795): `result += w * V(p)`
+    // from zero, in local order, each gated on its weight.
+    s << "template <class R> __device__ __forceinline__ void ffb_normal(const float* __restrict__ sm, int k, float& x, float& y, R& rng) {\n";
+    s << "    float rx = 0.0f, ry = 0.0f, ox, oy;\n";
+    for (int j = 0; j < NVN; ++j) {
+        const VarDef* v = p.normal[j];
+        std::ostringstream w, a0, a1;
+        w << "sm[T_VW + " << j << " * FFB_MAXX + k]";
+        a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + k]";
+        a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + k]";
+        s << "    { const float w = " << w.str() << "; if (w != 0.0f) { " << call(v, a0.str(), a1.str(), p.normal_slot[j])
+          << "; rx = rx + w * ox; ry = ry + w * oy; } }   // " << v->name << "\n";
+    }
+    s << "    x = rx; y = ry;\n}\n";
+    // One final of the chain (main_template.wgsl:679-704): affine,
+    // variations, post-affine; `aff` false evaluates the variations alone.
+    s << "template <class R> __device__ __forceinline__ void ffb_final_one(const float* __restrict__ sm, int c, float& x, float& y, R& rng, bool aff) {\n";
+    s << "    float rx = 0.0f, ry = 0.0f, ox, oy;\n    switch (c) {\n";
+    for (size_t c = 0; c < p.fin.size(); ++c) {
+        const Plan::Fin& fi = p.fin[c];
+        s << "    case " << c << ": {\n        const float* q = sm + " << fi.off << ";\n";
+        s << "        if (aff) { float ax = q[0] * x + q[1] * y + q[4]; float ay = q[2] * x + q[3] * y + q[5]; x = ax; y = ay; }\n";
+        const int nv = (int)fi.vars.size();
+        for (int j = 0; j < nv; ++j) {
+            std::ostringstream w, a0, a1;
+            w << "q[" << 13 + j << "]";
+            a0 << "q[" << 13 + nv + 2 * j << "]";
+            a1 << "q[" << 13 + nv + 2 * j + 1 << "]";
+            s << "        { const float w = " << w.str() << "; if (w != 0.0f) { " << call(fi.vars[j], a0.str(), a1.str(), fi.slot[j])
+              << "; rx = rx + w * ox; ry = ry + w * oy; } }   // " << fi.vars[j]->name << "\n";
+        }
+        s << "        if (aff && q[12] > 0.5f) { float px = q[6] * rx + q[7] * ry + q[10]; float py = q[8] * rx + q[9] * ry + q[11]; rx = px; ry = py; }\n";
+        s << "        x = rx; y = ry;\n        break; }\n";
+    }
+    s << "    default: break;\n    }\n}\n";
+    s << "template <class R> __device__ __forceinline__ void ffb_finals(const float* __restrict__ sm, float& x, float& y, R& rng) {\n";
+    for (size_t c = 0; c < p.fin.size(); ++c) s << "    ffb_final_one(sm, " << c << ", x, y, rng, true);\n";
+    s << "}\n";
+    s << kKernelsSrc << "\n";
+    p.source = s.str();
+    return p;
+}
+
+bool plan_fits(const Plan& p, const Flame& f) {
+    if ((int)f.xf.size() > p.maxx) return false;
+    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads);
+    return q.source == p.source;
+}
+
+std::vector<float> make_table(const Plan& p, const Flame& f) {
+    std::vector<float> t((size_t)p.table_size, 0.0f);
+    const int M = p.maxx;
+    // utilities.wgsl:35-54: total and running sums in f32, left to right.
+    float total = 0.0f;
+    for (auto& x : f.xf) total += x.weight;
+    t[0] = total;
+    float cum = 0.0f;
+    for (size_t k = 0; k < f.xf.size(); ++k) { cum += f.xf[k].weight; t[p.t_cum + k] = cum; }
+    for (size_t k = f.xf.size(); k < (size_t)M; ++k) t[p.t_cum + k] = INFINITY;
+    for (size_t k = 0; k < f.xf.size(); ++k) {
+        const XForm& x = f.xf[k];
+        const float rec[16] = {x.a, x.b, x.c, x.d, x.e, x.f, x.pa, x.pb, x.pc, x.pd, x.pe, x.pf,
+                               x.post ? 1.0f : 0.0f,
+                               (1.0f + x.speed) / 2.0f,                 // main_template.wgsl:499-500
+                               x.color * (1.0f - x.speed) / 2.0f,
+                               x.opacity};
+        for (int fld = 0; fld < 16; ++fld) t[p.t_xf + fld * M + k] = rec[fld];
+        for (size_t j = 0; j < p.normal.size(); ++j) {
+            const VarDef* v = p.normal[j];
+            t[p.t_vw + j * M + k] = x.var_weight(v);
+            for (int q = 0; q < v->nparams; ++q) t[p.t_vp + (2 * j + q) * M + k] = x.param(v, q);
+        }
+    }
+    for (size_t c = 0; c < p.fin.size(); ++c) {
+        const Plan::Fin& fi = p.fin[c];
+        const XForm& x = f.fin[f.fin_chain[c]];
+        const float rec[13] = {x.a, x.b, x.c, x.d, x.e, x.f, x.pa, x.pb, x.pc, x.pd, x.pe, x.pf, x.post ? 1.0f : 0.0f};
+        for (int q = 0; q < 13; ++q) t[fi.off + q] = rec[q];
+        const int nv = (int)fi.vars.size();
+        for (int j = 0; j < nv; ++j) {
+            t[fi.off + 13 + j] = x.var_weight(fi.vars[j]);
+            for (int q = 0; q < fi.vars[j]->nparams; ++q) t[fi.off + 13 + nv + 2 * j + q] = x.param(fi.vars[j], q);
+        }
+    }
+    return t;
+}
+
+}  // namespace ffb

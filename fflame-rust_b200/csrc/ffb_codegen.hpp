@@ -1,0 +1,52 @@
+// ffb_codegen.hpp -- per-flame-structure CUDA source for NVRTC, and the
+// float table the compiled kernel reads.
+//
+// The B200 counterpart of the reference's shader builder
+// (src/shader_builder_v2.rs: build_definitions 1832-2030,
+// build_apply_variations_2d 2525-2807, variation_call 653-681): it emits
+// only the variations the flame uses, in the reference's dispatch order,
+// with the NeedsRng draw of each placed at a static slot of the iteration's
+// counter-based stream.  Unlike the reference's inlined-constants mode it
+// bakes STRUCTURE only (which variations, in which order, how many finals);
+// coefficients, weights and colours stay in a table, so flames and
+// animation frames that share a structure share one compiled module.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "ffb_flame.hpp"
+
+namespace ffb {
+
+enum RngMode { RNG_PCG = 0, RNG_PHILOX = 1 };
+enum MathMode { MATH_PRECISE = 0, MATH_SFU = 1 };
+
+struct Plan {
+    int maxx = 0;                          // normal transforms (table capacity)
+    std::vector<const VarDef*> normal;     // normal-phase variations, local order
+    std::vector<int> normal_slot;          // draw slot per normal variation (-1: none)
+    struct Fin { std::vector<const VarDef*> vars; std::vector<int> slot; int off = 0; };
+    std::vector<Fin> fin;                  // one per final in the chain
+    bool has_post = false;
+    int n_slots = 2;
+    int table_size = 0;
+    int t_cum = 0, t_xf = 0, t_vw = 0, t_vp = 0, t_fin = 0;
+    int rng_mode = RNG_PHILOX;
+    int math_mode = MATH_PRECISE;
+    int threads = 128;
+    std::string source;                    // full NVRTC source (structure key)
+};
+
+// Structure of `f` (rng/math modes as given; maxx >= f.xf.size()).
+Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx = 0, int threads = 128);
+// The table of `f` for a plan made from a flame of the same structure.
+std::vector<float> make_table(const Plan& p, const Flame& f);
+// Whether `f` fits plan `p` (same structure, n_xf <= maxx).
+bool plan_fits(const Plan& p, const Flame& f);
+
+// Embedded device sources (generated into ffb_device_src.inc at build time).
+extern const char* const kDeviceSrc;
+extern const char* const kKernelsSrc;
+
+}  // namespace ffb

@@ -1,0 +1,392 @@
+// ffb_flame.cpp -- parsing the `.fae` flame description and deriving the
+// tables the kernels read.  See ffb_flame.hpp for the reference files.
+
+#include "ffb_flame.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+
+namespace ffb {
+
+// The variations this build carries, in the reference's registry order
+// (ALL_VARIATIONS, src/variations/defs/mod.rs:446).  Bodies live in
+// ffb_device.cuh; parameters and their defaults from the defs
+// (src/variations/defs/basic.rs, advanced.rs).
+static const VarDef kRegistry[] = {
+    {"linear", 0, false, 0, {nullptr, nullptr}, {0, 0}, "v_linear"},
+    {"sinusoidal", 1, false, 0, {nullptr, nullptr}, {0, 0}, "v_sinusoidal"},
+    {"spherical", 2, false, 0, {nullptr, nullptr}, {0, 0}, "v_spherical"},
+    {"swirl", 3, false, 0, {nullptr, nullptr}, {0, 0}, "v_swirl"},
+    {"horseshoe", 4, false, 0, {nullptr, nullptr}, {0, 0}, "v_horseshoe"},
+    {"polar", 5, false, 0, {nullptr, nullptr}, {0, 0}, "v_polar"},
+    {"disc", 8, false, 0, {nullptr, nullptr}, {0, 0}, "v_disc"},
+    {"ex", 12, false, 0, {nullptr, nullptr}, {0, 0}, "v_ex"},
+    {"julia", 13, true, 0, {nullptr, nullptr}, {0, 0}, "v_julia"},
+    {"bubble", 27, false, 0, {nullptr, nullptr}, {0, 0}, "v_bubble"},
+    {"cylinder", 28, false, 0, {nullptr, nullptr}, {0, 0}, "v_cylinder"},
+    {"curl", 47, false, 2, {"c1", "c2"}, {1.0f, 0.0f}, "v_curl"},   // advanced.rs:1666-1678
+};
+
+const VarDef* registry_find(const std::string& name) {
+    for (const auto& v : kRegistry) if (name == v.name) return &v;
+    return nullptr;
+}
+
+const std::vector<const VarDef*>& registry_all() {
+    static std::vector<const VarDef*> all = [] {
+        std::vector<const VarDef*> a;
+        for (const auto& v : kRegistry) a.push_back(&v);
+        return a;
+    }();
+    return all;
+}
+
+float XForm::param(const VarDef* v, int j) const {
+    std::string key = std::string(v->name) + "." + v->pname[j];
+    for (auto& p : params) if (p.first == key) return p.second;
+    return v->pdef[j];
+}
+
+float XForm::var_weight(const VarDef* v) const {
+    for (auto& p : vars) if (p.first == v) return p.second;
+    return 0.0f;
+}
+
+namespace {
+
+[[noreturn]] void fail(const std::string& s) { throw std::runtime_error(s); }
+
+float num_field(const Json& o, const char* k, bool required, float dflt) {
+    const Json* v = o.get(k);
+    if (!v || v->kind == Json::Null) {
+        if (required) fail(std::string("missing field `") + k + "`");
+        return dflt;
+    }
+    if (v->kind != Json::Number) fail(std::string("`") + k + "` is not a number");
+    return (float)v->num;
+}
+
+XForm parse_transform(const Json& t) {
+    if (t.kind != Json::Object) fail("a transform is not an object");
+    XForm x;
+    x.a = num_field(t, "a", true, 0); x.b = num_field(t, "b", true, 0); x.c = num_field(t, "c", true, 0);
+    x.d = num_field(t, "d", true, 0); x.e = num_field(t, "e", true, 0); x.f = num_field(t, "f", true, 0);
+    x.weight = num_field(t, "weight", true, 0);
+    // color: a palette position, or the old [r,g,b] form averaged (transforms.rs:1440-1458).
+    const Json* c = t.get("color");
+    if (!c) fail("missing field `color`");
+    if (c->kind == Json::Number) x.color = (float)c->num;
+    else if (c->kind == Json::Array && c->arr.size() >= 3) {
+        float r = (float)c->arr[0]->num, g = (float)c->arr[1]->num, b = (float)c->arr[2]->num;
+        x.color = (r + g + b) / 3.0f;
+    } else x.color = 0.5f;
+    x.speed = num_field(t, "color_speed", false, 0.0f);       // transforms.rs:1538
+    x.opacity = num_field(t, "opacity", false, 1.0f);
+    x.post = t.bool_or("post_affine_enabled", false);        // transforms.rs:1542
+    x.pa = num_field(t, "post_a", false, 1); x.pb = num_field(t, "post_b", false, 0);
+    x.pc = num_field(t, "post_c", false, 0); x.pd = num_field(t, "post_d", false, 1);
+    x.pe = num_field(t, "post_e", false, 0); x.pf = num_field(t, "post_f", false, 0);
+    const Json* vs = t.get("variations");
+    if (!vs || vs->kind != Json::Object) fail("missing field `variations`");
+    std::vector<std::pair<const VarDef*, float>> found;
+    for (auto& kv : vs->obj) {
+        const VarDef* d = registry_find(kv.first);
+        if (!d) fail("variation `" + kv.first + "` is not supported by this build");
+        if (kv.second->kind != Json::Number) fail("variation weight of `" + kv.first + "` is not a number");
+        found.emplace_back(d, (float)kv.second->num);
+    }
+    // Dispatch order (transforms.rs:668-682): `variation_order` first, then
+    // the registry's order.
+    std::vector<const VarDef*> order;
+    if (const Json* vo = t.get("variation_order"); vo && vo->kind == Json::Array) {
+        for (auto& e : vo->arr) {
+            if (e->kind != Json::String) continue;
+            const VarDef* d = registry_find(e->str);
+            if (!d) continue;
+            bool present = false;
+            for (auto& p : found) present |= p.first == d;
+            if (present && std::find(order.begin(), order.end(), d) == order.end()) order.push_back(d);
+        }
+    }
+    for (const VarDef* d : registry_all())
+        for (auto& p : found)
+            if (p.first == d && std::find(order.begin(), order.end(), d) == order.end()) order.push_back(d);
+    for (const VarDef* d : order)
+        for (auto& p : found) if (p.first == d) x.vars.emplace_back(d, p.second);
+    if (const Json* vp = t.get("variation_params"); vp && vp->kind == Json::Object)
+        for (auto& kv : vp->obj) if (kv.second->kind == Json::Number) x.params.emplace_back(kv.first, (float)kv.second->num);
+    if (const Json* fa = t.get("final_attachments"); fa && fa->kind == Json::Array)
+        for (auto& e : fa->arr) if (e->kind == Json::Number) x.final_att.push_back((int)e->num);
+    if (const Json* la = t.get("linked_attachments"); la && la->kind == Json::Array && !la->arr.empty())
+        fail("linked transforms are not supported by this build");
+    return x;
+}
+
+int mode_code(const std::string& s, const char* const* names, int n, const char* what) {
+    for (int i = 0; i < n; ++i) {
+        const char* a = names[2 * i];
+        const char* b = names[2 * i + 1];
+        if (s == a || s == b) return i;
+    }
+    fail(std::string("unknown ") + what + " `" + s + "`");
+}
+
+}  // namespace
+
+Flame parse_config(const Json& cfg) {
+    if (cfg.kind != Json::Object) fail("the config is not a JSON object");
+    const Json* fl = cfg.get("flame");
+    if (!fl || fl->kind != Json::Object) fail("missing field `flame`");
+    Flame F;
+    std::string rm = cfg.string_or("render_mode", fl->string_or("render_mode", "TwoD"));
+    if (rm != "TwoD" && rm != "2d" && rm != "two_d") fail("render mode `" + rm + "` is not supported by this build (2-D flames only)");
+    const Json* ts = fl->get("transforms");
+    if (!ts || ts->kind != Json::Array) fail("missing field `transforms`");
+    for (auto& t : ts->arr) F.xf.push_back(parse_transform(*t));
+    if (const Json* lt = fl->get("linked_transforms"); lt && lt->kind == Json::Array && !lt->arr.empty())
+        fail("linked transforms are not supported by this build");
+    if (const Json* ft = fl->get("final_transforms"); ft && ft->kind == Json::Array)
+        for (auto& t : ft->arr) F.fin.push_back(parse_transform(*t));
+    // A legacy singular final joins the pool attached to every normal
+    // (transforms.rs:2253-2266).
+    if (const Json* lf = fl->get("final_transform"); lf && lf->kind == Json::Object) {
+        int idx = (int)F.fin.size();
+        F.fin.push_back(parse_transform(*lf));
+        for (auto& x : F.xf)
+            if (std::find(x.final_att.begin(), x.final_att.end(), idx) == x.final_att.end()) x.final_att.push_back(idx);
+    }
+    if (F.xf.empty()) fail("the flame has no transforms");
+    if (F.xf.size() > 128)
+        fail("TooLarge: the flame has " + std::to_string(F.xf.size()) + " transforms; the renderer holds 128");
+    for (auto& x : F.xf)
+        for (int a : x.final_att)
+            if (a < 0 || a >= (int)F.fin.size()) fail("a final attachment points past the final pool");
+    F.fin_chain = F.xf[0].final_att;
+    for (auto& x : F.xf)
+        if (x.final_att != F.fin_chain)
+            fail("transforms with different final attachments are not supported by this build");
+    if (F.fin_chain.size() > 8) fail("more than 8 chained final transforms are not supported");
+    // Local variation order (transforms.rs:2297-2319): normals then finals.
+    auto absorb = [&](const XForm& x) {
+        for (auto& p : x.vars)
+            if (std::find(F.local.begin(), F.local.end(), p.first) == F.local.end()) F.local.push_back(p.first);
+    };
+    for (auto& x : F.xf) absorb(x);
+    for (auto& x : F.fin) absorb(x);
+    // View.
+    F.zoom = num_field(cfg, "zoom", false, 1.0f);
+    if (const Json* v = cfg.get("pan_x"); v && v->kind == Json::Number) F.pan_x = v->num;
+    if (const Json* v = cfg.get("pan_y"); v && v->kind == Json::Number) F.pan_y = v->num;
+    F.rotation = num_field(cfg, "rotation", false, 0.0f);
+    // Palette (palette.rs:453-482, 890-910; default Palette::fire, palette.rs:148-174).
+    if (const Json* p = cfg.get("palette"); p && p->kind == Json::Object) {
+        if (const Json* hx = p->get("indexed_colors"); hx && hx->kind == Json::String) {
+            const std::string& s = hx->str;
+            size_t i = 0; int k = 0;
+            while (i <= s.size()) {
+                size_t j = s.find(',', i);
+                if (j == std::string::npos) j = s.size();
+                std::string h = s.substr(i, j - i);
+                if (h.size() != 6) fail("Invalid hex color '" + h + "' at index " + std::to_string(k));
+                float rgb[3];
+                for (int q = 0; q < 3; ++q) {
+                    char* end = nullptr;
+                    std::string part = h.substr(q * 2, 2);
+                    long v = std::strtol(part.c_str(), &end, 16);
+                    if (!end || *end) fail("Invalid hex color '" + h + "'");
+                    rgb[q] = (float)v / 255.0f;
+                }
+                F.stop_pos.push_back((float)k / 255.0f);
+                F.stop_col.insert(F.stop_col.end(), rgb, rgb + 3);
+                ++k;
+                i = j + 1;
+            }
+        } else if (const Json* st = p->get("stops"); st && st->kind == Json::Array) {
+            for (auto& s : st->arr) {
+                F.stop_pos.push_back((float)s->number_or("position", 0.0));
+                const Json* col = s->get("color");
+                for (int q = 0; q < 3; ++q)
+                    F.stop_col.push_back(col && col->kind == Json::Array && (int)col->arr.size() > q ? (float)col->arr[q]->num : 1.0f);
+            }
+        } else fail("a palette with either 'indexed_colors' or 'stops'");
+    } else {
+        const float pos[5] = {0.0f, 0.25f, 0.5f, 0.75f, 1.0f};
+        const float col[15] = {0, 0, 0, 0.5f, 0, 0, 1.0f, 0.3f, 0, 1.0f, 0.8f, 0, 1.0f, 1.0f, 0.8f};
+        F.stop_pos.assign(pos, pos + 5);
+        F.stop_col.assign(col, col + 15);
+    }
+    F.palette_size = (int)num_field(cfg, "palette_size", false, 256.0f);
+    if (F.palette_size < 2 || F.palette_size > 4096) fail("palette_size must be 2..4096");
+    F.palette_rotation = num_field(cfg, "palette_rotation", false, 0.0f);
+    F.palette_reverse = cfg.bool_or("palette_reverse", false);
+    if (num_field(cfg, "palette_squeeze", false, 1.0f) != 1.0f || num_field(cfg, "palette_log_strength", false, 0.0f) != 0.0f)
+        fail("palette squeeze / log redistribution are not supported by this build");
+    if (const Json* cm = cfg.get("color_mode"); cm && cm->kind == Json::String && cm->str != "Palette" && cm->str != "palette")
+        fail("colour mode `" + cm->str + "` is not supported by this build (palette only)");
+    if (num_field(cfg, "filter_radius", false, 0.0f) != 0.0f)
+        fail("the histogram filter (filter_radius) is not supported by this build");
+    // Tone map (defaults.rs:18-52; fractal_config.rs field defaults).
+    ToneMap& tm = F.tm;
+    static const char* const kModes[] = {"linear", "Linear", "logarithmic", "Logarithmic", "density", "DensityVisualization"};
+    static const char* const kHigh[] = {"clip", "Clip", "max_norm", "MaxNorm", "reinhard", "Reinhard", "filmic", "Filmic", "agx", "AgX", "agx_punchy", "AgXPunchy"};
+    if (const Json* m = cfg.get("tonemap_mode"); m && m->kind == Json::String) tm.mode = mode_code(m->str, kModes, 3, "tone map mode");
+    if (const Json* m = cfg.get("highlight_mode"); m && m->kind == Json::String) tm.highlight = mode_code(m->str, kHigh, 6, "highlight mode");
+    if (tm.highlight >= 4) fail("the AgX highlight modes are not supported by this build");
+    tm.exposure = num_field(cfg, "exposure", false, 1.0f);
+    tm.gamma = num_field(cfg, "gamma", false, 4.0f);
+    tm.gamma_threshold = num_field(cfg, "gamma_threshold", false, 5.0f);
+    tm.brightness = num_field(cfg, "brightness", false, 4.0f);
+    tm.vibrancy = num_field(cfg, "vibrancy", false, 1.0f);
+    tm.white_level = num_field(cfg, "white_level", false, 200.0f);
+    tm.saturation = num_field(cfg, "saturation", false, 1.0f);
+    tm.hue_shift = num_field(cfg, "hue_shift", false, 0.0f);
+    tm.alpha_blend_low = num_field(cfg, "alpha_blend_low", false, 0.3f);
+    tm.alpha_blend_high = num_field(cfg, "alpha_blend_high", false, 0.8f);
+    tm.density_scale = num_field(cfg, "density_scale", false, 1.0f);
+    tm.levels_enabled = cfg.bool_or("levels_enabled", true);
+    tm.levels_low = num_field(cfg, "levels_low", false, 0.0f);
+    tm.levels_high = num_field(cfg, "levels_high", false, 10.0f);
+    tm.levels_gamma = num_field(cfg, "levels_gamma", false, 0.5f);
+    if (const Json* bg = cfg.get("background_color"); bg && bg->kind == Json::Array)
+        for (int q = 0; q < 3 && q < (int)bg->arr.size(); ++q) tm.background[q] = (float)bg->arr[q]->num;
+    tm.use_curve = cfg.bool_or("use_curve", true);
+    if (const Json* tc = cfg.get("tonemap_curve"); tc && tc->kind == Json::Object) {
+        if (const Json* pts = tc->get("points"); pts && pts->kind == Json::Array && pts->arr.size() >= 2) {
+            tm.curve.clear();
+            for (auto& p : pts->arr) tm.curve.push_back({(float)p->number_or("x", 0), (float)p->number_or("y", 0)});
+        }
+    }
+    // Density estimation: this build's extension (flam3's estimator
+    // radius / minimum / curve; the reference writes them unused,
+    // src/flame_xml.rs:1488-1490).
+    if (const Json* de = cfg.get("density_estimation"); de && de->kind == Json::Object) {
+        F.de.max_radius = (float)de->number_or("radius", 0.0);
+        F.de.min_radius = (float)de->number_or("minimum", 0.0);
+        F.de.curve = (float)de->number_or("curve", 0.4);
+        if (F.de.max_radius < 0 || F.de.max_radius > 32) fail("density_estimation.radius must be 0..32");
+    }
+    if (const Json* mi = cfg.get("max_iterations"); mi && mi->kind == Json::Number) F.max_iterations = (uint64_t)mi->num;
+    F.deterministic_rng = cfg.bool_or("deterministic_rng", false);
+    if (F.deterministic_rng) F.seed = 12345;
+    else {
+        std::random_device rd;
+        F.seed = ((uint64_t)rd() << 32) | rd();
+    }
+    return F;
+}
+
+Flame parse_config_text(const std::string& text) {
+    JsonPtr j;
+    try { j = json_parse(text); }
+    catch (const std::exception& e) { fail(std::string("config is not JSON: ") + e.what()); }
+    return parse_config(*j);
+}
+
+// Round-to-nearest-even half precision (the palette and curve texels,
+// gpu/buffers.rs:3215-3221, tonemap.rs:289-304).
+float f16_round(float v) {
+    uint32_t x; std::memcpy(&x, &v, 4);
+    uint32_t sign = x & 0x80000000u; x ^= sign;
+    float a; std::memcpy(&a, &x, 4);
+    float r;
+    if (x >= 0x477ff000u) r = 65504.0f;
+    else if (x < 0x38800000u) r = std::nearbyint(a * 16777216.0f) / 16777216.0f;
+    else {
+        uint32_t lsb = (x >> 13) & 1u;
+        x += 0xfffu + lsb;
+        x &= ~0x1fffu;
+        std::memcpy(&r, &x, 4);
+    }
+    uint32_t rb; std::memcpy(&rb, &r, 4); rb |= sign; std::memcpy(&r, &rb, 4);
+    return r;
+}
+
+std::vector<float> palette_table(const Flame& f) {
+    const int size = f.palette_size;
+    const int ns = (int)f.stop_pos.size();
+    const float* pos = f.stop_pos.data();
+    const float* col = f.stop_col.data();
+    std::vector<float> base((size_t)size * 3);
+    for (int i = 0; i < size; ++i) {                       // palette.rs:265-278
+        float t = (float)i / (float)(size - 1);
+        float c[3] = {1.f, 1.f, 1.f};
+        if (ns > 0) {                                      // palette.rs:310-360
+            t = std::min(std::max(t, 0.f), 1.f);
+            if (t < pos[0]) { for (int k = 0; k < 3; ++k) c[k] = col[k]; }
+            else {
+                int idx = 0;
+                for (int s = 0; s < ns; ++s) { if (pos[s] > t) break; idx = s; }
+                if (idx == ns - 1) { for (int k = 0; k < 3; ++k) c[k] = col[idx * 3 + k]; }
+                else {
+                    float range = pos[idx + 1] - pos[idx];
+                    if (range < 1e-6f) { for (int k = 0; k < 3; ++k) c[k] = col[idx * 3 + k]; }
+                    else {
+                        float lt = (t - pos[idx]) / range;
+                        for (int k = 0; k < 3; ++k) c[k] = col[idx * 3 + k] + (col[(idx + 1) * 3 + k] - col[idx * 3 + k]) * lt;
+                    }
+                }
+            }
+        }
+        for (int k = 0; k < 3; ++k) base[(size_t)i * 3 + k] = c[k];
+    }
+    std::vector<float> rot = base;
+    if (f.palette_rotation != 0.f) {                      // palette.rs:768-783
+        int amt = (int)std::round(f.palette_rotation * (float)size);
+        for (int i = 0; i < size; ++i) {
+            int src = ((i + amt) % size + size) % size;
+            for (int k = 0; k < 3; ++k) rot[(size_t)i * 3 + k] = base[(size_t)src * 3 + k];
+        }
+    }
+    std::vector<float> out((size_t)size * 4);
+    for (int i = 0; i < size; ++i) {
+        int src = f.palette_reverse ? size - 1 - i : i;    // palette.rs:786-797
+        for (int k = 0; k < 3; ++k) {
+            float v = f16_round(std::min(std::max(rot[(size_t)src * 3 + k], 0.f), 1.f));
+            out[(size_t)i * 4 + k] = (float)std::pow((double)std::max(v, 0.f), 2.2);   // utilities.wgsl:143-145
+        }
+        out[(size_t)i * 4 + 3] = 1.0f;
+    }
+    return out;
+}
+
+// ToneCurve::evaluate (src/scene/tonemap.rs:209-284): monotone cubic Hermite.
+static float curve_eval(const std::vector<CurvePt>& pts, float x) {
+    x = std::min(std::max(x, 0.0f), 1.0f);
+    for (size_t i = 0; i + 1 < pts.size(); ++i) {
+        const CurvePt& p0 = pts[i];
+        const CurvePt& p1 = pts[i + 1];
+        if (x >= p0.x && x <= p1.x) {
+            float delta = (p1.y - p0.y) / (p1.x - p0.x);
+            float m0 = i == 0 ? delta : ((p0.y - pts[i - 1].y) / (p0.x - pts[i - 1].x) + delta) * 0.5f;
+            float m1 = i == pts.size() - 2 ? delta : (delta + (pts[i + 2].y - p1.y) / (pts[i + 2].x - p1.x)) * 0.5f;
+            float m0f, m1f;
+            if (std::fabs(delta) < 1e-6f) { m0f = 0; m1f = 0; }
+            else {
+                float al = m0 / delta, be = m1 / delta;
+                if (al < 0 || be < 0) { m0f = delta; m1f = delta; }
+                else {
+                    float ss = al * al + be * be;
+                    if (ss > 9.0f) { float tau = 3.0f / std::sqrt(ss); m0f = tau * al * delta; m1f = tau * be * delta; }
+                    else { m0f = m0; m1f = m1; }
+                }
+            }
+            float t = (x - p0.x) / (p1.x - p0.x);
+            float t2 = t * t, t3 = t2 * t;
+            float h00 = 2.0f * t3 - 3.0f * t2 + 1.0f, h10 = t3 - 2.0f * t2 + t;
+            float h01 = -2.0f * t3 + 3.0f * t2, h11 = t3 - t2;
+            float dx = p1.x - p0.x;
+            return h00 * p0.y + h10 * dx * m0f + h01 * p1.y + h11 * dx * m1f;
+        }
+    }
+    return x;
+}
+
+std::vector<float> curve_lut(const ToneMap& tm) {
+    std::vector<float> lut(256);
+    for (int i = 0; i < 256; ++i) lut[i] = f16_round(curve_eval(tm.curve, (float)i / 255.0f));
+    return lut;
+}
+
+}  // namespace ffb

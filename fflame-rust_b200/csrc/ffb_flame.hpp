@@ -1,0 +1,102 @@
+// ffb_flame.hpp -- the flame description the render path consumes.
+//
+// The `.fae` / `.fflame` JSON subset of the 2-D flame path
+// (src/config/fractal_config.rs:178-520, src/scene/transforms.rs:337-420,
+// 1348-1558, 2016-2091), the variation registry subset this build carries
+// (src/variations/defs/mod.rs:446, positions kept as registry ids), the
+// per-flame local variation order (src/scene/transforms.rs:40-70, 668-682,
+// 2297-2319), the palette table (src/scene/palette.rs:265-360, 453-482,
+// 684-800) and the tone-map parameters (src/config/defaults.rs:18-52,
+// src/renderer/compute_kernel.rs:1796-1866).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ffb_json.hpp"
+
+namespace ffb {
+
+struct VarDef {
+    const char* name;
+    int id;            // position in the reference's ALL_VARIATIONS
+    bool needs_rng;    // Feature::NeedsRng
+    int nparams;
+    const char* pname[2];
+    float pdef[2];
+    const char* fn;    // device function name
+};
+
+const VarDef* registry_find(const std::string& name);
+const std::vector<const VarDef*>& registry_all();
+
+struct XForm {
+    float a = 1, b = 0, c = 0, d = 1, e = 0, f = 0;
+    float pa = 1, pb = 0, pc = 0, pd = 1, pe = 0, pf = 0;
+    bool post = false;
+    float weight = 1, color = 0.5f, speed = 0, opacity = 1;
+    // (variation, weight) in the transform's dispatch order.
+    std::vector<std::pair<const VarDef*, float>> vars;
+    // "name.param" -> value
+    std::vector<std::pair<std::string, float>> params;
+    std::vector<int> final_att;   // indices into the finals pool
+    float param(const VarDef* v, int j) const;
+    float var_weight(const VarDef* v) const;
+};
+
+struct CurvePt { float x, y; };
+
+struct ToneMap {
+    int mode = 1;              // 0 linear, 1 logarithmic, 2 density
+    int highlight = 0;         // 0 clip, 1 max_norm, 2 reinhard, 3 filmic, 4 agx, 5 agx_punchy
+    float exposure = 1.0f, gamma = 4.0f, gamma_threshold = 5.0f, brightness = 4.0f, vibrancy = 1.0f;
+    float white_level = 200.0f, saturation = 1.0f, hue_shift = 0.0f;
+    float alpha_blend_low = 0.3f, alpha_blend_high = 0.8f, density_scale = 1.0f;
+    bool levels_enabled = true;
+    float levels_low = 0.0f, levels_high = 10.0f, levels_gamma = 0.5f;
+    float background[3] = {0, 0, 0};
+    bool use_curve = true;
+    std::vector<CurvePt> curve{{0.f, 0.f}, {1.f, 1.f}};
+};
+
+struct DensityEstimation {
+    float max_radius = 0.0f;   // final-image pixels; 0 = off
+    float min_radius = 0.0f;
+    float curve = 0.4f;
+};
+
+struct Flame {
+    std::vector<XForm> xf;              // normal transforms
+    std::vector<XForm> fin;             // final transforms pool
+    std::vector<int> fin_chain;         // the final chain every normal runs
+    std::vector<const VarDef*> local;   // local variation order
+    float zoom = 1.0f;
+    double pan_x = 0.0, pan_y = 0.0;
+    float rotation = 0.0f;
+    // palette
+    std::vector<float> stop_pos, stop_col;
+    int palette_size = 256;
+    float palette_rotation = 0.0f;
+    bool palette_reverse = false;
+    ToneMap tm;
+    DensityEstimation de;
+    uint64_t max_iterations = 1000000000ull;
+    bool deterministic_rng = false;
+    uint64_t seed = 12345;               // first dispatch seed, compute_kernel.rs:3541-3553
+};
+
+// Parse a `.fae` configuration.  Throws std::runtime_error with the reason.
+Flame parse_config(const Json& cfg);
+Flame parse_config_text(const std::string& text);
+
+// The palette table the chaos game samples: `size` entries of linear RGB
+// (f16 texels of the stop gradient, decoded with pow 2.2), RGBA f32.
+std::vector<float> palette_table(const Flame& f);
+
+// The tone curve LUT (tonemap.rs:289-304): 256 f16-rounded values.
+std::vector<float> curve_lut(const ToneMap& tm);
+float f16_round(float v);
+
+}  // namespace ffb

@@ -1,0 +1,785 @@
+// ffb_runtime.cpp -- the render driver and the C ABI (include/ffb200.h).
+//
+// FlameRenderer's job (src/renderer/compute_kernel.rs:374-3600,
+// src/renderer/render.rs:371-804) done the B200 way: the flame is parsed
+// on the host, its structure compiled once by NVRTC for sm_100a (kept in a
+// module cache, the counterpart of src/shader_cache.rs), its numbers
+// uploaded as a small table; one persistent-walker launch runs the whole
+// sample budget (the reference's host loop of ~120 dispatches with an
+// accumulate pass every 4 becomes a handful of launches into one exact-count
+// histogram), and one fused kernel tone-maps (and 2x-downsamples) it.
+// No CPU fallback: without a CUDA device every call fails.
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <list>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include "../../include/ffb200.h"
+#include "ffb_codegen.hpp"
+#include "ffb_flame.hpp"
+#include "ffb_json.hpp"
+#include "ffb_tail.cuh"
+
+#define FFB_API extern "C" __attribute__((visibility("default")))
+
+namespace ffb {
+namespace {
+
+thread_local std::string g_err;
+
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string& m) { throw Fail{code, m}; }
+
+void ck(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    int code = (e == cudaErrorMemoryAllocation) ? FFB_ERR_OUT_OF_MEMORY
+               : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? FFB_ERR_NO_DEVICE : FFB_ERR_CUDA;
+    fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        g_err.clear();
+        return FFB_OK;
+    } catch (const Fail& e) {
+        g_err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_err = "out of host memory";
+        return FFB_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return FFB_ERR_CONFIG;
+    }
+}
+
+// Host mirror of the device-side launch record (ffb_kernels.cuh, ffb_launch).
+struct Launch {
+    const void* table;
+    const void* palette;
+    void* hist;
+    void* walkers;
+    void* counters;
+    uint32_t n_walkers, walker0, block0, n_xf;
+    uint32_t seed_lo, seed_hi, burn_in, ipt;
+    uint64_t it0;
+    uint32_t n_iters, pal_n;
+    int32_t width, height;
+    float zoom, pan_x, pan_y, cos_r, sin_r;
+};
+static_assert(sizeof(Launch) == 120, "launch record layout");
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    void* ensure(size_t bytes) {
+        if (bytes <= n && p) return p;
+        if (p) cudaFree(p);
+        p = nullptr; n = 0;
+        ck(cudaMalloc(&p, std::max<size_t>(bytes, 256)), "cudaMalloc");
+        n = std::max<size_t>(bytes, 256);
+        return p;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+};
+
+struct Module {
+    std::string key;
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t chaos = nullptr, probe = nullptr, apply = nullptr;
+    int smem_attr = 0;
+};
+
+std::string nvrtc_options_key() { return "sm_100a|c++17|ftz|prec-div|prec-sqrt|nofmad"; }
+
+}  // namespace
+}  // namespace ffb
+
+using namespace ffb;
+
+struct ffb_renderer {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;
+    std::list<Module> cache;     // most recent first
+    DevBuf hist, walkers, table, palette, counters, jobs, rgba, de_out, de_tab, lut, f_out, tmp_in;
+    uint64_t h2d = 0, d2h = 0;      // bytes copied by the current call
+    uint32_t launches = 0;          // kernels launched by the current call
+
+    void reset_counts() { h2d = d2h = 0; launches = 0; }
+    void fill_counts(ffb_output* o) const { if (o) { o->h2d_bytes = h2d; o->d2h_bytes = d2h; o->kernel_launches = launches; } }
+
+    ~ffb_renderer() {
+        cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& m : cache) if (m.lib) cudaLibraryUnload(m.lib);
+        for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in}) b->release();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    Module& module_for(const std::string& src) {
+        for (auto it = cache.begin(); it != cache.end(); ++it)
+            if (it->key == src) { cache.splice(cache.begin(), cache, it); return cache.front(); }
+        Module m;
+        m.key = src;
+        compile(src, m);
+        cache.push_front(std::move(m));
+        while (cache.size() > 32) {                         // src/shader_cache.rs keeps an LRU too
+            if (cache.back().lib) cudaLibraryUnload(cache.back().lib);
+            cache.pop_back();
+        }
+        return cache.front();
+    }
+
+    static void compile(const std::string& src, Module& m) {
+        std::vector<char> cubin = nvrtc_cubin(src);
+        ck(cudaLibraryLoadData(&m.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0), "cudaLibraryLoadData");
+        ck(cudaLibraryGetKernel(&m.chaos, m.lib, "ffb_chaos"), "cudaLibraryGetKernel(ffb_chaos)");
+        ck(cudaLibraryGetKernel(&m.probe, m.lib, "ffb_probe"), "cudaLibraryGetKernel(ffb_probe)");
+        ck(cudaLibraryGetKernel(&m.apply, m.lib, "ffb_apply_points"), "cudaLibraryGetKernel(ffb_apply_points)");
+    }
+
+    static std::vector<char> nvrtc_cubin(const std::string& src) {
+        nvrtcProgram prog;
+        if (nvrtcCreateProgram(&prog, src.c_str(), "ffb_flame.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+            fail(FFB_ERR_COMPILE, "nvrtcCreateProgram failed");
+        const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--ftz=true", "--prec-div=true",
+                              "--prec-sqrt=true", "--fmad=false", "-lineinfo"};
+        nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+        if (r != NVRTC_SUCCESS) {
+            size_t n = 0;
+            nvrtcGetProgramLogSize(prog, &n);
+            std::string log(n, '\0');
+            nvrtcGetProgramLog(prog, &log[0]);
+            nvrtcDestroyProgram(&prog);
+            fail(FFB_ERR_COMPILE, std::string("NVRTC: ") + nvrtcGetErrorString(r) + "\n" + log);
+        }
+        size_t n = 0;
+        nvrtcGetCUBINSize(prog, &n);
+        std::vector<char> cubin(n);
+        nvrtcGetCUBIN(prog, cubin.data());
+        nvrtcDestroyProgram(&prog);
+        return cubin;
+    }
+
+    void begin() { ck(cudaSetDevice(device), "cudaSetDevice"); }
+};
+
+namespace ffb {
+namespace {
+
+constexpr uint32_t kMaxDim = 32768;                           // config/defaults.rs MAX_IMAGE_DIM
+
+struct Prepared {
+    Flame flame;
+    Plan plan;
+    std::vector<float> table, palette;
+    uint32_t ss = 1, wi = 0, hi = 0, walkers = 0, burn_in = 20, ipt = 1024, threads = 128;
+    uint64_t target = 0, per_walker = 0, seed = 0;
+    int rng = RNG_PHILOX, math = MATH_PRECISE;
+};
+
+Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_size = true) {
+    if (!config) fail(FFB_ERR_INVALID, "config is NULL");
+    if (!job) fail(FFB_ERR_INVALID, "job is NULL");
+    Prepared P;
+    try { P.flame = parse_config_text(std::string(config, len)); }
+    catch (const std::exception& e) {
+        std::string m = e.what();
+        fail(m.rfind("TooLarge", 0) == 0 ? FFB_ERR_TOO_LARGE : FFB_ERR_CONFIG, "config did not parse: " + m);
+    }
+    P.ss = job->supersample ? job->supersample : 1;
+    if (P.ss != 1 && P.ss != 2) fail(FFB_ERR_INVALID, "supersample must be 1 or 2");
+    if (need_size) {
+        if (job->width == 0 || job->height == 0) fail(FFB_ERR_INVALID, "width and height must be nonzero");   // render.rs:259-264
+        if (job->width > kMaxDim || job->height > kMaxDim) fail(FFB_ERR_TOO_LARGE, "width and height must be at most 32768");
+    }
+    P.wi = job->width * P.ss;
+    P.hi = job->height * P.ss;
+    P.rng = job->rng < 0 ? RNG_PHILOX : job->rng;
+    if (P.rng != RNG_PCG && P.rng != RNG_PHILOX) fail(FFB_ERR_INVALID, "rng must be 0 (pcg) or 1 (philox)");
+    P.math = job->math;
+    if (P.math != MATH_PRECISE && P.math != MATH_SFU) fail(FFB_ERR_INVALID, "math must be 0 (precise) or 1 (sfu)");
+    P.threads = job->threads ? job->threads : 128;
+    if (P.threads % 32 || P.threads > 1024) fail(FFB_ERR_INVALID, "threads must be a multiple of 32, at most 1024");
+    P.burn_in = job->burn_in ? job->burn_in : 20;
+    P.ipt = job->iterations_per_thread ? job->iterations_per_thread : 1024;
+    P.target = job->iterations ? job->iterations : P.flame.max_iterations * (uint64_t)P.ss * P.ss;
+    uint64_t w = job->walkers;
+    if (!w) w = std::min<uint64_t>(148ull * 2048, std::max<uint64_t>(4096, P.target / 1024));
+    w = (w + 31) / 32 * 32;
+    if (w > 0xFFFFFFFFull) fail(FFB_ERR_INVALID, "too many walkers");
+    P.walkers = (uint32_t)w;
+    P.per_walker = (P.target + w - 1) / w;
+    if (P.rng == RNG_PCG) {
+        // Launch chunks stay on dispatch boundaries of the PCG stream.
+        if (P.per_walker + P.burn_in > (uint64_t)P.ipt * 0xFFFFFFFFull) fail(FFB_ERR_INVALID, "budget too large for the pcg stream");
+    }
+    P.seed = job->seed ? job->seed : P.flame.seed;
+    P.plan = make_plan(P.flame, P.rng, P.math, 0, (int)P.threads);
+    P.table = make_table(P.plan, P.flame);
+    P.palette = palette_table(P.flame);
+    return P;
+}
+
+// The tone map's constants (tonemap.wgsl:94-112, 224-590;
+// compute_kernel.rs:1796-1866, 3813-3866), in double, for a render at
+// wi x hi with `samples` plotted samples.
+TonemapArgs tonemap_args(const Flame& f, uint32_t wi, uint32_t hi, double sample_density, int transparent, bool count_is_float) {
+    const ToneMap& t = f.tm;
+    TonemapArgs a{};
+    a.mode = t.mode;
+    a.highlight = t.highlight;
+    a.use_curve = t.use_curve ? 1 : 0;
+    a.transparent = transparent;
+    a.levels_enabled = t.levels_enabled ? 1 : 0;
+    a.count_is_float = count_is_float ? 1 : 0;
+    a.exposure = t.exposure;
+    const double g = t.gamma == 0.0f ? (double)t.gamma : 1.0 / (double)t.gamma;
+    a.inv_gamma = (float)g;
+    a.density_scale = t.density_scale;
+    const double ppu = (double)std::min(wi, hi) * 0.25 * (double)f.zoom;
+    const double area = (double)wi * (double)hi / (ppu * ppu);
+    const double pw = 67108864.0, bright_adjust = 2.3;
+    const double k1 = bright_adjust * (double)t.brightness * 268.0 * pw / 256.0;
+    const double k2 = 1.0 / (area * (double)t.white_level * sample_density);
+    a.ls_a = (float)(k1 / (pw * std::log(10.0)));
+    a.ls_b = (float)((double)t.white_level * k2);
+    a.white_level = t.white_level;
+    a.gamma_threshold = t.gamma_threshold;
+    a.funcval = t.gamma_threshold != 0.0f ? (float)std::pow((double)t.gamma_threshold, g - 1.0) : 0.0f;
+    const double vib = std::nearbyint((double)t.vibrancy * 256.0);
+    a.vib = (float)vib;
+    a.notvib = (float)(256.0 - vib);
+    a.saturation = t.saturation;
+    a.hue_shift = t.hue_shift;
+    a.alpha_blend_low = t.alpha_blend_low;
+    a.alpha_blend_high = t.alpha_blend_high;
+    a.levels_low = t.levels_low;
+    a.levels_high = t.levels_high;
+    a.levels_gamma = t.levels_gamma;
+    a.levels_density = (float)sample_density;
+    for (int k = 0; k < 3; ++k) a.bg_lin[k] = (float)std::pow(std::max((double)t.background[k], 0.0), 2.2);
+    return a;
+}
+
+// Density-estimation table (see ffb_tail.cu): entry c for counts 0..n-2,
+// entry n-1 for every larger count.
+std::vector<float> de_table(double r_max, double r_min, double curve, int& n_out, int& radius) {
+    radius = (int)std::floor(r_max);
+    auto h_of = [&](double c) { return std::max(r_min, r_max / std::pow(c, curve)); };
+    std::vector<float> t;
+    int c = 0;
+    for (;; ++c) {
+        double h = c == 0 ? 0.0 : h_of((double)c);
+        double h2 = h * h;
+        double dmax2 = c == 0 ? -1.0 : std::floor(h2);
+        double norm = 0.0;
+        int rr = (int)std::floor(std::sqrt(std::max(dmax2, 0.0)));
+        for (int dy = -rr; dy <= rr; ++dy)
+            for (int dx = -rr; dx <= rr; ++dx) {
+                double d2 = dx * dx + dy * dy;
+                if (d2 <= h2) norm += std::exp(-4.5 * d2 / h2);
+            }
+        if (c == 0) norm = 1.0;
+        t.push_back((float)dmax2);
+        t.push_back(h2 > 0 ? (float)(1.0 / h2) : 0.0f);
+        t.push_back((float)(1.0 / norm));
+        t.push_back(0.0f);
+        // Past this count every larger one has the same disc and weights.
+        if (c >= 1 && (h < 1.0 || h <= r_min)) break;
+        if (c > 10000000) fail(FFB_ERR_INVALID, "density estimation table too large");
+    }
+    n_out = (int)(t.size() / 4);
+    return t;
+}
+
+void check_de(const Flame& f, uint32_t ss) {
+    if (f.de.max_radius * ss > 40.0f) fail(FFB_ERR_INVALID, "density estimation radius too large");
+}
+
+// Chaos game of a prepared flame into r->hist (wi*hi float4, cleared here).
+void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walker0, uint64_t* inframe_out) {
+    Module& m = r->module_for(P.plan.source);
+    const size_t npx = (size_t)P.wi * P.hi;
+    float4* hist = (float4*)r->hist.ensure(npx * sizeof(float4));
+    ck(cudaMemsetAsync(hist, 0, npx * sizeof(float4), s), "clear histogram");
+    void* d_table = r->table.ensure(P.table.size() * 4);
+    ck(cudaMemcpyAsync(d_table, P.table.data(), P.table.size() * 4, cudaMemcpyHostToDevice, s), "upload table");
+    r->h2d += P.table.size() * 4;
+    void* d_pal = r->palette.ensure(P.palette.size() * 4);
+    ck(cudaMemcpyAsync(d_pal, P.palette.data(), P.palette.size() * 4, cudaMemcpyHostToDevice, s), "upload palette");
+    r->h2d += P.palette.size() * 4;
+    void* d_walk = r->walkers.ensure((size_t)P.walkers * 16);
+    uint64_t* d_cnt = (uint64_t*)r->counters.ensure(64);
+    ck(cudaMemsetAsync(d_cnt, 0, 64, s), "clear counters");
+    const uint32_t pal_n = (uint32_t)(P.palette.size() / 4);
+    const int smem = ((P.plan.table_size + 3) / 4) * 16 + (int)pal_n * 16;
+    if (smem > 48 * 1024 && m.smem_attr < smem) {
+        ck(cudaFuncSetAttribute((const void*)m.chaos, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
+        m.smem_attr = smem;
+    }
+    const uint64_t total_iters = P.per_walker + P.burn_in;
+    uint64_t chunk = 1ull << 16;
+    if (P.rng == RNG_PCG) chunk = std::max<uint64_t>(1, chunk / P.ipt) * P.ipt;
+    const uint32_t blocks = (P.walkers + P.threads - 1) / P.threads;
+    const double rot = P.flame.rotation;
+    Launch L{};
+    L.table = d_table; L.palette = d_pal; L.hist = hist; L.walkers = d_walk; L.counters = d_cnt;
+    L.n_walkers = P.walkers; L.walker0 = walker0; L.block0 = 0; L.n_xf = (uint32_t)P.flame.xf.size();
+    L.seed_lo = (uint32_t)P.seed; L.seed_hi = (uint32_t)(P.seed >> 32); L.burn_in = P.burn_in; L.ipt = P.ipt;
+    L.pal_n = pal_n; L.width = (int32_t)P.wi; L.height = (int32_t)P.hi;
+    L.zoom = P.flame.zoom; L.pan_x = (float)P.flame.pan_x; L.pan_y = (float)P.flame.pan_y;
+    L.cos_r = (float)std::cos(rot); L.sin_r = (float)std::sin(rot);
+    const size_t n_chunks = (size_t)((total_iters + chunk - 1) / chunk);
+    Launch* d_jobs = (Launch*)r->jobs.ensure(sizeof(Launch) * std::max<size_t>(1, n_chunks));
+    std::vector<Launch> ls;
+    for (uint64_t it0 = 0; it0 < total_iters; it0 += chunk) {
+        L.it0 = it0;
+        L.n_iters = (uint32_t)std::min<uint64_t>(chunk, total_iters - it0);
+        ls.push_back(L);
+    }
+    ck(cudaMemcpyAsync(d_jobs, ls.data(), ls.size() * sizeof(Launch), cudaMemcpyHostToDevice, s), "upload launches");
+    r->h2d += ls.size() * sizeof(Launch);
+    for (size_t i = 0; i < ls.size(); ++i) {
+        Launch* jp = d_jobs + i;
+        int nj = 1;
+        void* args[] = {&jp, &nj};
+        ck(cudaLaunchKernel((const void*)m.chaos, dim3(blocks), dim3(P.threads), args, (size_t)smem, s), "launch ffb_chaos");
+        r->launches += 1;
+    }
+    if (inframe_out) {
+        ck(cudaMemcpyAsync(inframe_out, d_cnt, 8, cudaMemcpyDeviceToHost, s), "read counters");
+        r->d2h += 8;
+    }
+}
+
+// Density estimation of r->hist into r->de_out (count as float).
+float4* run_de(ffb_renderer* r, const float4* hist, uint32_t w, uint32_t h, double r_max, double r_min, double curve, cudaStream_t s) {
+    int n = 0, radius = 0;
+    std::vector<float> tab = de_table(r_max, r_min, curve, n, radius);
+    float4* d_tab = (float4*)r->de_tab.ensure(tab.size() * 4);
+    ck(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, s), "upload DE table");
+    r->h2d += tab.size() * 4;
+    float4* out = (float4*)r->de_out.ensure((size_t)w * h * sizeof(float4));
+    ck(launch_density_estimate(hist, (int)w, (int)h, d_tab, n, radius, out, s), "density estimation");
+    r->launches += 1;
+    return out;
+}
+
+const float* upload_lut(ffb_renderer* r, const Flame& f, cudaStream_t s) {
+    std::vector<float> lut = curve_lut(f.tm);
+    float* d = (float*)r->lut.ensure(256 * 4);
+    ck(cudaMemcpyAsync(d, lut.data(), 256 * 4, cudaMemcpyHostToDevice, s), "upload curve");
+    r->h2d += 256 * 4;
+    return d;
+}
+
+// One whole render into device RGBA8 `d_rgba`.
+void render_device(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, void* d_rgba, cudaStream_t s,
+                   bool sync, ffb_output* out) {
+    Prepared P = prepare(config, len, job);
+    check_de(P.flame, P.ss);
+    ck(cudaEventRecord(r->ev0, s), "event");
+    uint64_t* h_inframe = nullptr;
+    static thread_local uint64_t inframe_slot;
+    if (sync) h_inframe = &inframe_slot;
+    run_chaos(r, P, s, job->walker0, h_inframe);
+    const float4* hist = (const float4*)r->hist.p;
+    bool count_f = false;
+    if (P.flame.de.max_radius > 0.0f) {
+        hist = run_de(r, hist, P.wi, P.hi, (double)P.flame.de.max_radius * P.ss, (double)P.flame.de.min_radius * P.ss,
+                      (double)P.flame.de.curve, s);
+        count_f = true;
+    }
+    const uint64_t plotted = (uint64_t)P.walkers * P.per_walker;
+    const double sd = std::max((double)plotted / ((double)P.wi * (double)P.hi), 1e-6);   // compute_kernel.rs:1796-1840
+    TonemapArgs a = tonemap_args(P.flame, P.wi, P.hi, sd, job->transparent, count_f);
+    const float* lut = upload_lut(r, P.flame, s);
+    ck(launch_tonemap(hist, (int)P.wi, (int)P.hi, (int)P.ss, a, lut, (uint8_t*)d_rgba, nullptr, s), "tone map");
+    r->launches += 1;
+    ck(cudaEventRecord(r->ev1, s), "event");
+    if (out) {
+        out->width = job->width; out->height = job->height;
+        out->total_iterations = plotted;
+        out->inframe_samples = 0;
+        out->render_time_ms = 0.0;
+    }
+    if (sync) {
+        ck(cudaStreamSynchronize(s), "render");
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, r->ev0, r->ev1), "event time");
+        if (out) { out->render_time_ms = ms; out->inframe_samples = *h_inframe; }
+    }
+    r->fill_counts(out);
+}
+
+// ------------------------------------------------------------ fae_call ---
+thread_local std::vector<uint8_t> g_output, g_info;
+std::mutex g_fae_mu;
+std::unique_ptr<ffb_renderer> g_fae_renderer;
+
+ffb_renderer* fae_renderer() {
+    if (!g_fae_renderer) {
+        ffb_renderer* r = nullptr;
+        int st = ffb_renderer_create(0, &r);
+        if (st != FFB_OK) fail(st, g_err.empty() ? "no CUDA device" : g_err);
+        g_fae_renderer.reset(r);
+    }
+    return g_fae_renderer.get();
+}
+
+std::string variations_json() {
+    std::string s = "[";
+    bool first = true;
+    for (const VarDef* v : registry_all()) {
+        if (!first) s += ",";
+        first = false;
+        s += "{\"name\":" + JsonWriter::quote(v->name) + ",\"params\":[";
+        for (int j = 0; j < v->nparams; ++j) s += (j ? "," : "") + JsonWriter::quote(v->pname[j]);
+        s += "]}";
+    }
+    return s + "]";
+}
+
+uint32_t u32_arg(const Json& r, const char* k) {
+    const Json* v = r.get(k);
+    if (!v || v->kind != Json::Number || v->num < 0) fail(FFB_ERR_INVALID, std::string("`") + k + "` (a number) is missing");
+    return (uint32_t)v->num;
+}
+
+void fae_dispatch(const Json& r, std::vector<uint8_t>& out, std::string& info) {
+    const Json* fn = r.get("fn");
+    if (!fn || fn->kind != Json::String) fail(FFB_ERR_INVALID, "`fn` is missing");
+    const std::string& f = fn->str;
+    if (f == "info") {
+        info = std::string("{\"result\":{\"version\":") + JsonWriter::quote(ffb_version()) +
+               ",\"engines\":[\"flame\"],\"device\":\"cuda sm_100a\"}}";
+    } else if (f == "variations") {
+        info = "{\"result\":" + variations_json() + "}";
+    } else if (f == "render") {
+        const Json* c = r.get("config");
+        if (!c || c->kind != Json::String) fail(FFB_ERR_INVALID, "`config` (a string) is missing");
+        ffb_job job{};
+        job.width = u32_arg(r, "width");
+        job.height = u32_arg(r, "height");
+        if (const Json* it = r.get("iterations"); it && it->kind == Json::Number && it->num > 0) job.iterations = (uint64_t)it->num;
+        if (const Json* it = r.get("iterations_per_thread"); it && it->kind == Json::Number) job.iterations_per_thread = (uint32_t)it->num;
+        job.iterations_per_thread = job.iterations_per_thread ? job.iterations_per_thread : 1024;   // DEFAULT_EXPORT_ITERATIONS_PER_THREAD
+        const bool tr = r.bool_or("transparent", false), pm = r.bool_or("premultiplied", false);
+        job.transparent = tr ? (pm ? 2 : 1) : 0;
+        job.supersample = (uint32_t)r.number_or("supersample", 1.0);
+        job.rng = (int32_t)r.number_or("rng", -1.0);
+        job.walkers = (uint32_t)r.number_or("walkers", 0.0);
+        ffb_renderer* R = fae_renderer();
+        std::lock_guard<std::mutex> lk(R->mu);
+        R->begin();
+        out.resize((size_t)job.width * job.height * 4);
+        void* d = R->rgba.ensure(out.size());
+        ffb_output o{};
+        R->reset_counts();
+        render_device(R, c->str.data(), c->str.size(), &job, d, R->stream, true, &o);
+        ck(cudaMemcpyAsync(out.data(), d, out.size(), cudaMemcpyDeviceToHost, R->stream), "readback");
+        R->d2h += out.size();
+        ck(cudaStreamSynchronize(R->stream), "readback");
+        JsonWriter w;
+        w.begin().num("width", job.width).num("height", job.height).num("iterations", (double)o.total_iterations)
+            .num("ms", o.render_time_ms).num("iterations_per_thread", job.iterations_per_thread).end();
+        info = w.s();
+    } else {
+        fail(FFB_ERR_INVALID, "`" + f + "` is not supported by this build (render, info, variations)");
+    }
+}
+
+}  // namespace
+}  // namespace ffb
+
+// ================================================================ ABI ====
+FFB_API const char* ffb_last_error(void) { return g_err.c_str(); }
+FFB_API const char* ffb_version(void) { return "ffb200 0.1.0 (sm_100a)"; }
+
+FFB_API int ffb_renderer_create(int device, ffb_renderer** out) {
+    return guard([&] {
+        if (!out) fail(FFB_ERR_INVALID, "out is NULL");
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess || n == 0) fail(FFB_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+        if (device < 0 || device >= n) fail(FFB_ERR_INVALID, "no such device");
+        auto r = std::make_unique<ffb_renderer>();
+        r->device = device;
+        r->begin();
+        ck(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaEventCreate(&r->ev0), "cudaEventCreate");
+        ck(cudaEventCreate(&r->ev1), "cudaEventCreate");
+        *out = r.release();
+    });
+}
+
+FFB_API void ffb_renderer_destroy(ffb_renderer* r) { delete r; }
+
+FFB_API int ffb_render(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, uint8_t* rgba, ffb_output* out) {
+    return guard([&] {
+        if (!r || !rgba || !job) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        const size_t bytes = (size_t)job->width * job->height * 4;
+        void* d = r->rgba.ensure(bytes);
+        ffb_output o{};
+        r->reset_counts();
+        render_device(r, config, len, job, d, r->stream, true, &o);
+        ck(cudaMemcpyAsync(rgba, d, bytes, cudaMemcpyDeviceToHost, r->stream), "readback");
+        r->d2h += bytes;
+        ck(cudaStreamSynchronize(r->stream), "readback");
+        r->fill_counts(&o);
+        if (out) *out = o;
+    });
+}
+
+FFB_API int ffb_render_device(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, void* d_rgba, void* stream,
+                              int sync, ffb_output* out) {
+    return guard([&] {
+        if (!r || !d_rgba || !job) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        r->reset_counts();
+        render_device(r, config, len, job, d_rgba, stream ? (cudaStream_t)stream : r->stream, sync != 0, out);
+    });
+}
+
+FFB_API int ffb_histogram(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, uint32_t* counts, float* rgb,
+                          ffb_output* out) {
+    return guard([&] {
+        if (!r || !job) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Prepared P = prepare(config, len, job);
+        r->reset_counts();
+        uint64_t inframe = 0;
+        ck(cudaEventRecord(r->ev0, r->stream), "event");
+        run_chaos(r, P, r->stream, job->walker0, &inframe);
+        ck(cudaEventRecord(r->ev1, r->stream), "event");
+        const size_t npx = (size_t)P.wi * P.hi;
+        std::vector<float> h(npx * 4);
+        ck(cudaMemcpyAsync(h.data(), r->hist.p, npx * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "histogram");
+        for (size_t i = 0; i < npx; ++i) {
+            if (counts) { uint32_t c; std::memcpy(&c, &h[i * 4 + 3], 4); counts[i] = c; }
+            if (rgb) { rgb[i * 3] = h[i * 4]; rgb[i * 3 + 1] = h[i * 4 + 1]; rgb[i * 3 + 2] = h[i * 4 + 2]; }
+        }
+        if (out) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+            out->width = P.wi; out->height = P.hi;
+            out->total_iterations = (uint64_t)P.walkers * P.per_walker;
+            out->inframe_samples = inframe;
+            out->render_time_ms = ms;
+            r->fill_counts(out);
+            out->d2h_bytes += npx * 16;
+        }
+    });
+}
+
+FFB_API int ffb_tonemap(ffb_renderer* r, const char* config, size_t len, const float* counts, const float* rgb, uint32_t w,
+                        uint32_t h, uint32_t ss, double sample_density, int32_t transparent, uint8_t* rgba, float* rgba_f) {
+    return guard([&] {
+        if (!r || !counts || !rgb || !rgba) fail(FFB_ERR_INVALID, "NULL argument");
+        if (ss != 1 && ss != 2) fail(FFB_ERR_INVALID, "ss must be 1 or 2");
+        if (w == 0 || h == 0 || (ss == 2 && (w % 2 || h % 2))) fail(FFB_ERR_INVALID, "bad size");
+        if (rgba_f && ss != 1) fail(FFB_ERR_INVALID, "float output at ss 1 only");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Flame f;
+        try { f = parse_config_text(std::string(config, len)); }
+        catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
+        const size_t npx = (size_t)w * h;
+        std::vector<float> hv(npx * 4);
+        for (size_t i = 0; i < npx; ++i) { hv[i * 4] = rgb[i * 3]; hv[i * 4 + 1] = rgb[i * 3 + 1]; hv[i * 4 + 2] = rgb[i * 3 + 2]; hv[i * 4 + 3] = counts[i]; }
+        float4* d_in = (float4*)r->tmp_in.ensure(npx * 16);
+        ck(cudaMemcpyAsync(d_in, hv.data(), npx * 16, cudaMemcpyHostToDevice, r->stream), "upload");
+        TonemapArgs a = tonemap_args(f, w, h, sample_density, transparent, true);
+        const float* lut = upload_lut(r, f, r->stream);
+        const size_t out_px = ss == 1 ? npx : npx / 4;
+        void* d_out = r->rgba.ensure(out_px * 4);
+        float4* d_f = rgba_f ? (float4*)r->f_out.ensure(npx * 16) : nullptr;
+        ck(launch_tonemap(d_in, (int)w, (int)h, (int)ss, a, lut, (uint8_t*)d_out, d_f, r->stream), "tone map");
+        ck(cudaMemcpyAsync(rgba, d_out, out_px * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+        if (rgba_f) ck(cudaMemcpyAsync(rgba_f, d_f, npx * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "tone map");
+    });
+}
+
+FFB_API int ffb_density_estimate(ffb_renderer* r, const uint32_t* counts, const float* rgb, uint32_t w, uint32_t h,
+                                 float max_radius, float min_radius, float curve, float* out_counts, float* out_rgb) {
+    return guard([&] {
+        if (!r || !counts || !rgb || !out_counts || !out_rgb) fail(FFB_ERR_INVALID, "NULL argument");
+        if (max_radius <= 0.f || max_radius > 40.f || min_radius < 0.f || curve < 0.f) fail(FFB_ERR_INVALID, "bad DE parameters");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        const size_t npx = (size_t)w * h;
+        std::vector<float> hv(npx * 4);
+        for (size_t i = 0; i < npx; ++i) {
+            hv[i * 4] = rgb[i * 3]; hv[i * 4 + 1] = rgb[i * 3 + 1]; hv[i * 4 + 2] = rgb[i * 3 + 2];
+            std::memcpy(&hv[i * 4 + 3], &counts[i], 4);
+        }
+        float4* d_in = (float4*)r->tmp_in.ensure(npx * 16);
+        ck(cudaMemcpyAsync(d_in, hv.data(), npx * 16, cudaMemcpyHostToDevice, r->stream), "upload");
+        float4* o = run_de(r, d_in, w, h, max_radius, min_radius, curve, r->stream);
+        std::vector<float> ov(npx * 4);
+        ck(cudaMemcpyAsync(ov.data(), o, npx * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "density estimation");
+        for (size_t i = 0; i < npx; ++i) {
+            out_rgb[i * 3] = ov[i * 4]; out_rgb[i * 3 + 1] = ov[i * 4 + 1]; out_rgb[i * 3 + 2] = ov[i * 4 + 2];
+            out_counts[i] = ov[i * 4 + 3];
+        }
+    });
+}
+
+FFB_API int ffb_probe(ffb_renderer* r, const char* config, size_t len, const float* pts, uint32_t npts, int32_t math, float* out,
+                      uint32_t out_pairs) {
+    return guard([&] {
+        if (!r || !pts || !out) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Flame f;
+        try { f = parse_config_text(std::string(config, len)); }
+        catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
+        Plan p = make_plan(f, RNG_PCG, math, 0, 128);
+        std::vector<float> tab = make_table(p, f);
+        const int n_all = (int)(f.xf.size() + f.fin_chain.size());
+        if (out_pairs < (uint32_t)n_all * npts) fail(FFB_ERR_INVALID, "output too small");
+        Module& m = r->module_for(p.source);
+        void* d_tab = r->table.ensure(tab.size() * 4);
+        ck(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, r->stream), "upload");
+        float* d_pts = (float*)r->tmp_in.ensure((size_t)npts * 8);
+        ck(cudaMemcpyAsync(d_pts, pts, (size_t)npts * 8, cudaMemcpyHostToDevice, r->stream), "upload");
+        float* d_out = (float*)r->f_out.ensure((size_t)n_all * npts * 8);
+        int nx = (int)f.xf.size(), np = (int)npts;
+        const float* tp = (const float*)d_tab;
+        void* args[] = {&tp, &nx, (void*)&n_all, &d_pts, &np, &d_out};
+        const int total = n_all * np;
+        ck(cudaLaunchKernel((const void*)m.probe, dim3((total + 127) / 128), dim3(128), args, 0, r->stream), "launch ffb_probe");
+        ck(cudaMemcpyAsync(out, d_out, (size_t)total * 8, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "probe");
+    });
+}
+
+FFB_API int ffb_apply_points(ffb_renderer* r, const char* config, size_t len, int32_t xform, uint32_t n, const float* xs,
+                             const float* ys, const float* words, int32_t with_affine, int32_t math, float* xo, float* yo) {
+    return guard([&] {
+        if (!r || !xs || !ys || !words || !xo || !yo) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Flame f;
+        try { f = parse_config_text(std::string(config, len)); }
+        catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
+        const int n_all = (int)(f.xf.size() + f.fin_chain.size());
+        if (xform < 0 || xform >= n_all) fail(FFB_ERR_INVALID, "no such transform");
+        Plan p = make_plan(f, RNG_PHILOX, math, 0, 128);
+        std::vector<float> tab = make_table(p, f);
+        Module& m = r->module_for(p.source);
+        void* d_tab = r->table.ensure(tab.size() * 4);
+        ck(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, r->stream), "upload");
+        const size_t nn = n;
+        float* d_in = (float*)r->tmp_in.ensure(nn * 4 * 2 + nn * 16 * 4);
+        float* d_x = d_in, *d_y = d_in + nn, *d_w = d_in + 2 * nn;
+        ck(cudaMemcpyAsync(d_x, xs, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
+        ck(cudaMemcpyAsync(d_y, ys, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
+        ck(cudaMemcpyAsync(d_w, words, nn * 64, cudaMemcpyHostToDevice, r->stream), "upload");
+        float* d_out = (float*)r->f_out.ensure(nn * 8);
+        float* d_xo = d_out, *d_yo = d_out + nn;
+        int nx = (int)f.xf.size(), xi = xform, ni = (int)n, wa = with_affine;
+        const float* tp = (const float*)d_tab;
+        void* args[] = {&tp, &nx, &xi, &ni, &d_x, &d_y, &d_w, &wa, &d_xo, &d_yo};
+        ck(cudaLaunchKernel((const void*)m.apply, dim3((n + 127) / 128), dim3(128), args, 0, r->stream), "launch ffb_apply_points");
+        ck(cudaMemcpyAsync(xo, d_xo, nn * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaMemcpyAsync(yo, d_yo, nn * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "apply points");
+    });
+}
+
+FFB_API int ffb_specialize(const char* config, size_t len, int32_t rng, int32_t math, size_t* cubin_bytes, char* source,
+                           size_t source_len) {
+    return guard([&] {
+        if (!config) fail(FFB_ERR_INVALID, "config is NULL");
+        Flame f;
+        try { f = parse_config_text(std::string(config, len)); }
+        catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
+        Plan p = make_plan(f, rng, math, 0, 128);
+        std::vector<char> cubin = ffb_renderer::nvrtc_cubin(p.source);
+        if (cubin_bytes) *cubin_bytes = cubin.size();
+        if (source && source_len) {
+            size_t n = std::min(source_len - 1, p.source.size());
+            std::memcpy(source, p.source.data(), n);
+            source[n] = 0;
+        }
+    });
+}
+
+FFB_API int ffb_atomic_bench(ffb_renderer* r, uint32_t pixels, uint64_t samples, int32_t kind, double* ms) {
+    return guard([&] {
+        if (!r || !ms || pixels == 0) fail(FFB_ERR_INVALID, "bad argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        uint32_t* buf = (uint32_t*)r->hist.ensure((size_t)pixels * 16);
+        ck(cudaMemsetAsync(buf, 0, (size_t)pixels * 16, r->stream), "clear");
+        int dev_sms = 148;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, r->device);
+        ck(launch_atomic_bench(buf, pixels, samples / 16, kind, dev_sms * 8, r->stream), "warm-up");
+        ck(cudaEventRecord(r->ev0, r->stream), "event");
+        ck(launch_atomic_bench(buf, pixels, samples, kind, dev_sms * 8, r->stream), "atomic bench");
+        ck(cudaEventRecord(r->ev1, r->stream), "event");
+        ck(cudaStreamSynchronize(r->stream), "atomic bench");
+        float t = 0.f;
+        ck(cudaEventElapsedTime(&t, r->ev0, r->ev1), "event time");
+        *ms = t;
+    });
+}
+
+// ------------------------------------------------------------ drop-in ----
+FFB_API uint8_t* fae_alloc(size_t len) { return (uint8_t*)std::malloc(std::max<size_t>(len, 1)); }
+FFB_API void fae_free(uint8_t* ptr, size_t) { std::free(ptr); }
+FFB_API const uint8_t* fae_output_ptr(void) { return g_output.data(); }
+FFB_API size_t fae_output_len(void) { return g_output.size(); }
+FFB_API const uint8_t* fae_info_ptr(void) { return g_info.data(); }
+FFB_API size_t fae_info_len(void) { return g_info.size(); }
+
+FFB_API int32_t fae_call(const uint8_t* req, size_t req_len, const uint8_t* data, size_t data_len) {
+    (void)data; (void)data_len;
+    std::vector<uint8_t> out;
+    std::string info;
+    int st = guard([&] {
+        std::string text(req ? (const char*)req : "", req ? req_len : 0);
+        JsonPtr j;
+        try { j = json_parse(text); }
+        catch (const std::exception& e) { fail(FFB_ERR_INVALID, std::string("request is not JSON: ") + e.what()); }
+        std::lock_guard<std::mutex> lk(g_fae_mu);
+        fae_dispatch(*j, out, info);
+    });
+    if (st == FFB_OK) {
+        g_output = std::move(out);
+        g_info.assign(info.begin(), info.end());
+        return 0;
+    }
+    g_output.assign(g_err.begin(), g_err.end());
+    g_info.clear();
+    return 1;
+}

@@ -1,0 +1,49 @@
+// ffb_tail.cuh -- host interface of the ahead-of-time kernels (ffb_tail.cu):
+// density estimation, the tone map with the fused 2x firefly downsample,
+// and the splat-throughput microbenchmark.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ffb {
+
+// Per-pixel tone-map constants, derived on the host (in double) from the
+// flame's ToneMap and the render's sample density (tonemap.wgsl:94-590).
+struct TonemapArgs {
+    int mode;              // 0 linear, 1 log, 2 density
+    int highlight;         // 0 clip, 1 max_norm, 2 reinhard, 3 filmic
+    int use_curve;
+    int transparent;       // 0 opaque, 1 straight, 2 premultiplied
+    int levels_enabled;
+    int count_is_float;    // histogram .w holds a float count (after DE) instead of u32 bits
+    float exposure, inv_gamma, density_scale;
+    float ls_a;            // k1 / (prefilter_white * ln 10)
+    float ls_b;            // white_level * k2
+    float white_level;
+    float gamma_threshold, funcval;
+    float vib, notvib;
+    float saturation, hue_shift;
+    float alpha_blend_low, alpha_blend_high;
+    float levels_low, levels_high, levels_gamma, levels_density;
+    float bg_lin[3];
+};
+
+// hist: wi*hi float4 (r, g, b sums, count).  ss = 1: out is wi*hi RGBA8 (and
+// out_f, if not null, the float RGBA before quantisation); ss = 2: out is
+// (wi/2)*(hi/2) RGBA8 after the firefly downsample.
+cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const TonemapArgs& a, const float* curve_lut,
+                           uint8_t* out, float4* out_f, cudaStream_t s);
+
+// Density estimation table: entry c (counts 0..n-1, the last entry serving
+// every larger count): (max accepted d^2, 1/h^2, 1/normaliser, unused).
+struct DeTable { int n; int radius; };
+cudaError_t launch_density_estimate(const float4* hist, int w, int h, const float4* table, int table_n, int radius,
+                                    float4* out, cudaStream_t s);
+
+// Splat-throughput microbenchmark: `n_ops` random-address atomic splats of
+// the given kind into `buf` (n_words u32 words): kind 0 = 4 scalar atomics a
+// sample (the splat), 1 = one u32 atomic, 2 = one vector f32x4 reduction.
+cudaError_t launch_atomic_bench(uint32_t* buf, uint32_t n_pixels, uint64_t n_samples, int kind, int blocks, cudaStream_t s);
+
+}  // namespace ffb

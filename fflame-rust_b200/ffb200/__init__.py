@@ -1,0 +1,89 @@
+"""ffb200 -- the B200-native fractal-flame render path of calibas/fflame-rust.
+
+The Python face mirrors the reference's client (python/pyfae/__init__.py):
+`Engine().render(config, width, height, iterations=..., ...)` -> Image.  It
+drives the CUDA library through the reference's own boundary (`fae_call`,
+a JSON request), so code written against pyfae runs unchanged apart from
+the import.  `Renderer` is the typed API underneath (include/ffb200.h).
+"""
+
+import json
+
+from ._module import Module, find_module
+from ._native import EngineError, Output, Renderer, make_job, specialize  # noqa: F401
+
+__all__ = ["Engine", "Image", "Module", "EngineError", "Renderer", "specialize"]
+
+
+def _text(config):
+    if isinstance(config, str):
+        if config.lstrip().startswith("{"):
+            return config
+        with open(config, encoding="utf-8") as f:
+            return f.read()
+    if hasattr(config, "data"):
+        config = config.data
+    return json.dumps(config)
+
+
+class Image:
+    """A render: RGBA8 bytes and the engine's note (pyfae's Image)."""
+
+    def __init__(self, engine, rgba, info, config_text):
+        self.engine = engine
+        self.rgba = rgba
+        self.info = info or {}
+        self.config = config_text
+
+    @property
+    def width(self):
+        return self.info.get("width")
+
+    @property
+    def height(self):
+        return self.info.get("height")
+
+    def array(self):
+        import numpy as np
+        return np.frombuffer(self.rgba, np.uint8).reshape(self.height, self.width, 4)
+
+
+class Engine:
+    """The engine (pyfae.Engine, python/pyfae/__init__.py:159-221)."""
+
+    def __init__(self, module=None):
+        self._module = Module(module)
+
+    def _call(self, request, data=b""):
+        return self._module.call(request, data)
+
+    def _data(self, request, data=b""):
+        return self._call(request, data)[1]["result"]
+
+    def info(self):
+        return self._data({"fn": "info"})
+
+    def variations(self):
+        """{name: [parameter names]} in registration order."""
+        return {v["name"]: v["params"] for v in self._data({"fn": "variations"})}
+
+    def render(self, config, width, height, *, iterations=None, iterations_per_thread=None,
+               transparent=False, premultiplied=False, sticky=False, sequence=False, supersample=None):
+        """A config (dict, JSON, or a path) at `width` x `height` (python/pyfae/__init__.py:201-221).
+
+        `iterations`: the flame's budget (default: the config's own).
+        `iterations_per_thread`: default the CLI's, 1024.  `supersample` 2
+        renders at twice the size and boxes it down with the firefly clamp.
+        """
+        text = _text(config)
+        request = {"fn": "render", "config": text, "width": width, "height": height,
+                   "transparent": transparent, "premultiplied": premultiplied,
+                   "sticky": sticky, "sequence": sequence}
+        if iterations:
+            request["iterations"] = int(iterations)
+        if iterations_per_thread:
+            request["iterations_per_thread"] = int(iterations_per_thread)
+        if supersample:
+            request["supersample"] = int(supersample)
+        out, info = self._call(request)
+        return Image(self, out, info, text)

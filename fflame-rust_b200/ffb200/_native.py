@@ -1,0 +1,233 @@
+"""ctypes binding of libffb200.so (include/ffb200.h).
+
+The library is built in-tree by fflame-rust_b200/build.py.  Nothing here
+computes anything on the CPU: every render call goes to the CUDA kernels,
+and fails loudly (EngineError) when the library or a device is missing.
+"""
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libffb200.so")
+
+OK, ERR_INVALID, ERR_CONFIG, ERR_TOO_LARGE, ERR_OUT_OF_MEMORY, ERR_CUDA, ERR_COMPILE, ERR_CANCELLED, ERR_NO_DEVICE = range(9)
+STATUS_NAMES = ["OK", "Invalid", "Config", "TooLarge", "OutOfMemory", "Cuda", "Compile", "Cancelled", "NoDevice"]
+RNG = {"pcg": 0, "philox": 1}
+MATH = {"precise": 0, "sfu": 1}
+
+# Every symbol include/ffb200.h declares.
+EXPORTS = [
+    "fae_alloc", "fae_free", "fae_output_ptr", "fae_output_len", "fae_info_ptr", "fae_info_len", "fae_call",
+    "ffb_last_error", "ffb_version", "ffb_renderer_create", "ffb_renderer_destroy", "ffb_render",
+    "ffb_render_device", "ffb_histogram", "ffb_tonemap", "ffb_density_estimate", "ffb_probe",
+    "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench",
+]
+
+
+class EngineError(ValueError):
+    """A call the engine refused or failed, with its reason (pyfae's EngineError)."""
+
+    def __init__(self, msg, status=ERR_INVALID):
+        super().__init__(msg)
+        self.status = status
+
+
+class Job(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("iterations", ctypes.c_uint64),
+        ("iterations_per_thread", ctypes.c_uint32), ("burn_in", ctypes.c_uint32), ("walkers", ctypes.c_uint32),
+        ("supersample", ctypes.c_uint32), ("rng", ctypes.c_int32), ("math", ctypes.c_int32),
+        ("transparent", ctypes.c_int32), ("threads", ctypes.c_int32), ("seed", ctypes.c_uint64),
+        ("walker0", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+    ]
+
+
+class Output(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("total_iterations", ctypes.c_uint64),
+        ("inframe_samples", ctypes.c_uint64), ("render_time_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built: run `python fflame-rust_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.ffb_last_error.restype = ctypes.c_char_p
+        L.ffb_version.restype = ctypes.c_char_p
+        L.fae_alloc.restype = ctypes.c_void_p
+        L.fae_alloc.argtypes = [ctypes.c_size_t]
+        L.fae_free.argtypes = [ctypes.c_void_p, ctypes.c_size_t]
+        L.fae_output_ptr.restype = ctypes.c_void_p
+        L.fae_info_ptr.restype = ctypes.c_void_p
+        L.fae_output_len.restype = ctypes.c_size_t
+        L.fae_info_len.restype = ctypes.c_size_t
+        L.fae_call.restype = ctypes.c_int32
+        L.fae_call.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]
+        L.ffb_renderer_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.ffb_renderer_destroy.argtypes = [ctypes.c_void_p]
+        L.ffb_renderer_destroy.restype = None
+        _lib = L
+    return _lib
+
+
+def _check(st):
+    if st != OK:
+        msg = lib().ffb_last_error().decode(errors="replace")
+        raise EngineError(f"{STATUS_NAMES[st] if st < len(STATUS_NAMES) else st}: {msg}", st)
+
+
+def _text(config):
+    if isinstance(config, (bytes, bytearray)):
+        return bytes(config)
+    if isinstance(config, str):
+        if config.lstrip().startswith("{"):
+            return config.encode()
+        with open(config, "rb") as f:
+            return f.read()
+    if hasattr(config, "data"):
+        config = config.data
+    return json.dumps(config).encode()
+
+
+def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0, walkers=0, supersample=1,
+             rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0):
+    j = Job()
+    j.width, j.height, j.iterations = width, height, int(iterations or 0)
+    j.iterations_per_thread, j.burn_in, j.walkers = iterations_per_thread, burn_in, walkers
+    j.supersample = supersample
+    j.rng = RNG[rng] if isinstance(rng, str) else rng
+    j.math = MATH[math] if isinstance(math, str) else math
+    j.transparent, j.threads, j.seed, j.walker0 = int(transparent), threads, int(seed), walker0
+    return j
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+class Renderer:
+    """FlameRenderer: one CUDA device, its stream and the compiled-flame cache."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        _check(lib().ffb_renderer_create(device, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ffb_renderer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, config, width, height, **job):
+        """config -> (RGBA8 [height, width, 4], Output)."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        out = np.zeros((height, width, 4), np.uint8)
+        o = Output()
+        _check(lib().ffb_render(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), _p(out, ctypes.c_uint8), ctypes.byref(o)))
+        return out, o
+
+    def render_device(self, config, width, height, d_rgba, stream=None, sync=True, **job):
+        """The render into device memory at `d_rgba` (an int pointer)."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        o = Output()
+        _check(lib().ffb_render_device(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), ctypes.c_void_p(d_rgba),
+                                       ctypes.c_void_p(stream or 0), ctypes.c_int(1 if sync else 0), ctypes.byref(o)))
+        return o
+
+    def histogram(self, config, width, height, **job):
+        """The chaos game alone: (counts u32 [H, W], rgb f32 [H, W, 3], Output) at the internal size."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        ss = j.supersample or 1
+        H, W = height * ss, width * ss
+        cnt = np.zeros((H, W), np.uint32)
+        rgb = np.zeros((H, W, 3), np.float32)
+        o = Output()
+        _check(lib().ffb_histogram(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), _p(cnt, ctypes.c_uint32),
+                                   _p(rgb, ctypes.c_float), ctypes.byref(o)))
+        return cnt, rgb, o
+
+    def tonemap(self, config, counts, rgb, sample_density, ss=1, transparent=0, want_float=False):
+        cfg = _text(config)
+        counts = np.ascontiguousarray(counts, np.float32)
+        rgb = np.ascontiguousarray(rgb, np.float32)
+        h, w = counts.shape
+        oh, ow = (h, w) if ss == 1 else (h // 2, w // 2)
+        out = np.zeros((oh, ow, 4), np.uint8)
+        f = np.zeros((h, w, 4), np.float32) if want_float else None
+        _check(lib().ffb_tonemap(self._h, cfg, ctypes.c_size_t(len(cfg)), _p(counts, ctypes.c_float), _p(rgb, ctypes.c_float),
+                                 ctypes.c_uint32(w), ctypes.c_uint32(h), ctypes.c_uint32(ss), ctypes.c_double(sample_density),
+                                 ctypes.c_int32(transparent), _p(out, ctypes.c_uint8), _p(f, ctypes.c_float) if want_float else None))
+        return (out, f) if want_float else out
+
+    def density_estimate(self, counts, rgb, max_radius, min_radius=0.0, curve=0.4):
+        counts = np.ascontiguousarray(counts, np.uint32)
+        rgb = np.ascontiguousarray(rgb, np.float32)
+        h, w = counts.shape
+        oc = np.zeros((h, w), np.float32)
+        orgb = np.zeros((h, w, 3), np.float32)
+        _check(lib().ffb_density_estimate(self._h, _p(counts, ctypes.c_uint32), _p(rgb, ctypes.c_float), ctypes.c_uint32(w),
+                                          ctypes.c_uint32(h), ctypes.c_float(max_radius), ctypes.c_float(min_radius),
+                                          ctypes.c_float(curve), _p(oc, ctypes.c_float), _p(orgb, ctypes.c_float)))
+        return oc, orgb
+
+    def probe(self, config, pts, n_transforms, math="precise"):
+        cfg = _text(config)
+        pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 2)
+        out = np.zeros((n_transforms * len(pts), 2), np.float32)
+        _check(lib().ffb_probe(self._h, cfg, ctypes.c_size_t(len(cfg)), _p(pts, ctypes.c_float), ctypes.c_uint32(len(pts)),
+                               ctypes.c_int32(MATH[math] if isinstance(math, str) else math), _p(out, ctypes.c_float),
+                               ctypes.c_uint32(len(out))))
+        return out.reshape(n_transforms, len(pts), 2)
+
+    def apply_points(self, config, xform, xs, ys, words, with_affine=True, math="precise"):
+        cfg = _text(config)
+        xs = np.ascontiguousarray(xs, np.float32)
+        ys = np.ascontiguousarray(ys, np.float32)
+        words = np.ascontiguousarray(words, np.float32)
+        n = len(xs)
+        assert words.size == n * 16
+        xo, yo = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        _check(lib().ffb_apply_points(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.c_int32(xform), ctypes.c_uint32(n),
+                                      _p(xs, ctypes.c_float), _p(ys, ctypes.c_float), _p(words, ctypes.c_float),
+                                      ctypes.c_int32(1 if with_affine else 0), ctypes.c_int32(MATH[math] if isinstance(math, str) else math),
+                                      _p(xo, ctypes.c_float), _p(yo, ctypes.c_float)))
+        return xo, yo
+
+    def atomic_bench(self, pixels, samples, kind=0):
+        ms = ctypes.c_double()
+        _check(lib().ffb_atomic_bench(self._h, ctypes.c_uint32(pixels), ctypes.c_uint64(samples), ctypes.c_int32(kind), ctypes.byref(ms)))
+        return ms.value
+
+
+def specialize(config, rng="philox", math="precise"):
+    """NVRTC-compile a config's chaos kernel for sm_100a (no device needed): (cubin bytes, source)."""
+    cfg = _text(config)
+    n = ctypes.c_size_t()
+    buf = ctypes.create_string_buffer(1 << 20)
+    _check(lib().ffb_specialize(cfg, ctypes.c_size_t(len(cfg)), ctypes.c_int32(RNG[rng]), ctypes.c_int32(MATH[math]),
+                                ctypes.byref(n), buf, ctypes.c_size_t(len(buf))))
+    return n.value, buf.value.decode()

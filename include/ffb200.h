@@ -1,0 +1,173 @@
+/*
+ * ffb200.h -- C ABI of the B200 fractal-flame render path.
+ *
+ * Two layers, both plain C (pointers and sizes, no CUDA or torch types):
+ *
+ *  1. The drop-in: the exports of the reference's engine module
+ *     (calibas/fflame-rust wasm/python/src/lib.rs), with the same JSON
+ *     protocol -- `fae_call({"fn": "render", "config": <.fae JSON>, "width",
+ *     "height", "iterations"?, "iterations_per_thread"?, "transparent"?,
+ *     "premultiplied"?})` answers RGBA8 bytes as the output and
+ *     {width, height, iterations, ms, iterations_per_thread} as the info
+ *     (wasm/python/src/render.rs:45-91).  A status of 1 carries the error's
+ *     text as the output.  OUTPUT and INFO are owned by the library, per
+ *     calling thread, valid until that thread's next fae_call.
+ *
+ *  2. The typed render API, the C mirror of the reference's Rust surface
+ *     `render(device, queue, RenderJob) -> Result<RenderOutput, RenderError>`
+ *     (src/renderer/render.rs:48-466), plus the stages the render is made of
+ *     (histogram, density estimation, tone map, variation probe), which the
+ *     parity tests and the benchmark call directly.
+ *
+ * Every function returns an ffb_status; ffb_last_error() holds the message
+ * of the calling thread's last failure.  Nothing here falls back to the CPU:
+ * without a CUDA device the calls fail with FFB_ERR_NO_DEVICE.
+ */
+#ifndef FFB200_H
+#define FFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ drop-in --- */
+
+/* wasm/python/src/lib.rs:49-55: a request buffer in the library's memory. */
+uint8_t* fae_alloc(size_t len);
+/* wasm/python/src/lib.rs:57-62: frees a fae_alloc'd buffer. */
+void fae_free(uint8_t* ptr, size_t len);
+/* wasm/python/src/lib.rs:64-72: the last call's output bytes. */
+const uint8_t* fae_output_ptr(void);
+size_t fae_output_len(void);
+/* wasm/python/src/lib.rs:74-82: the last call's info JSON. */
+const uint8_t* fae_info_ptr(void);
+size_t fae_info_len(void);
+/* wasm/python/src/lib.rs:84-101: one call; 0, or 1 with the error's text
+ * as the output.  Calls: "info", "variations", "render". */
+int32_t fae_call(const uint8_t* req, size_t req_len, const uint8_t* data, size_t data_len);
+
+/* ---------------------------------------------------------- typed API --- */
+
+/* RenderError (src/renderer/render.rs:312-330) and the failures this build adds. */
+typedef enum {
+    FFB_OK = 0,
+    FFB_ERR_INVALID = 1,        /* a bad argument */
+    FFB_ERR_CONFIG = 2,         /* the config did not parse or asks for what this build lacks */
+    FFB_ERR_TOO_LARGE = 3,      /* RenderError::TooLarge */
+    FFB_ERR_OUT_OF_MEMORY = 4,  /* RenderError::OutOfMemory */
+    FFB_ERR_CUDA = 5,           /* a CUDA call failed */
+    FFB_ERR_COMPILE = 6,        /* NVRTC rejected the specialised kernel */
+    FFB_ERR_CANCELLED = 7,      /* RenderError::Cancelled */
+    FFB_ERR_NO_DEVICE = 8       /* no CUDA device */
+} ffb_status;
+
+enum { FFB_RNG_PCG = 0, FFB_RNG_PHILOX = 1 };       /* ffb_job.rng */
+enum { FFB_MATH_PRECISE = 0, FFB_MATH_SFU = 1 };    /* ffb_job.math */
+
+/* RenderJob (src/renderer/render.rs:48-137).  Zero means "default". */
+typedef struct {
+    uint32_t width, height;            /* output size */
+    uint64_t iterations;               /* plotted samples of the internal render; 0: config max_iterations x ss^2 */
+    uint32_t iterations_per_thread;    /* dispatch length of the PCG stream (0: 1024, the CLI's) */
+    uint32_t burn_in;                  /* 0: 20 (render.rs:126) */
+    uint32_t walkers;                  /* 0: sized to the budget */
+    uint32_t supersample;              /* 1 or 2 (src/export/supersample.rs); 0: 1 */
+    int32_t rng;                       /* FFB_RNG_* (default FFB_RNG_PHILOX) ; -1 = default */
+    int32_t math;                      /* FFB_MATH_* */
+    int32_t transparent;               /* 0 opaque, 1 straight alpha, 2 premultiplied */
+    int32_t threads;                   /* threads a block (0: 128) */
+    uint64_t seed;                     /* 0: the config's (12345 under deterministic_rng) */
+    uint32_t walker0;                  /* first walker id of this shard (multi-GPU sharding) */
+    uint32_t reserved;
+} ffb_job;
+
+/* RenderOutput (src/renderer/render.rs:207-218). */
+typedef struct {
+    uint32_t width, height;
+    uint64_t total_iterations;         /* plotted samples (post burn-in) */
+    uint64_t inframe_samples;          /* samples splatted into the frame */
+    double render_time_ms;             /* device time of the whole render */
+    uint64_t h2d_bytes;                /* host->device bytes this call copied */
+    uint64_t d2h_bytes;                /* device->host bytes this call copied */
+    uint32_t kernel_launches;          /* this library's kernels launched by this call */
+    uint32_t reserved;
+} ffb_output;
+
+typedef struct ffb_renderer ffb_renderer;   /* FlameRenderer: a device, a stream, the module cache */
+
+/* The calling thread's last error message ("" when none). */
+const char* ffb_last_error(void);
+/* Build version and the device it would use. */
+const char* ffb_version(void);
+
+int ffb_renderer_create(int device, ffb_renderer** out);
+void ffb_renderer_destroy(ffb_renderer* r);
+
+/* A full render: config (.fae JSON) -> RGBA8 into the host buffer `rgba`
+ * (width*height*4 bytes).  The timed region of the reference's
+ * render_with (render.rs:483-804) plus the readback. */
+int ffb_render(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
+               uint8_t* rgba, ffb_output* out);
+
+/* The same render with the RGBA8 result left in device memory (`d_rgba`,
+ * width*height*4 bytes); `stream` is a cudaStream_t or NULL for the
+ * renderer's own.  Returns once the work is enqueued when `sync` is 0. */
+int ffb_render_device(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
+                      void* d_rgba, void* stream, int sync, ffb_output* out);
+
+/* The chaos game alone into a histogram read back to the host: `counts`
+ * (w*h u32 hits) and `rgb` (w*h*3 f32 colour sums) at the internal size
+ * (width*ss x height*ss).  The high-resolution export's readback path
+ * (src/export/high_res.rs:2139-2175). */
+int ffb_histogram(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
+                  uint32_t* counts, float* rgb, ffb_output* out);
+
+/* The tone map of a host histogram (counts as f32, colour sums), with the
+ * config's tone-map settings and the given sample density:
+ * tonemap.wgsl:224-590.  ss 1: rgba is w*h*4 bytes and `rgba_f` (if not
+ * NULL) w*h*4 floats before quantisation; ss 2: rgba is (w/2)*(h/2)*4 after
+ * the firefly downsample. */
+int ffb_tonemap(ffb_renderer* r, const char* config, size_t config_len, const float* counts, const float* rgb,
+                uint32_t w, uint32_t h, uint32_t ss, double sample_density, int32_t transparent,
+                uint8_t* rgba, float* rgba_f);
+
+/* Density estimation of a host histogram (counts, colour sums): radii in
+ * histogram pixels.  Output counts and sums as f32. */
+int ffb_density_estimate(ffb_renderer* r, const uint32_t* counts, const float* rgb, uint32_t w, uint32_t h,
+                         float max_radius, float min_radius, float curve, float* out_counts, float* out_rgb);
+
+/* The variation probe (shaders/core/main_template.wgsl:1467-1567): every
+ * transform of the config (normals, then the final chain) at `npts`
+ * points (x, y pairs), RNG slot = transform*npts + point.  `out` holds
+ * n_transforms*npts (x, y) pairs.  `math` as ffb_job.math. */
+int ffb_probe(ffb_renderer* r, const char* config, size_t config_len, const float* pts, uint32_t npts, int32_t math,
+              float* out, uint32_t out_pairs);
+
+/* One transform step at n points with explicit draw words (16 a point):
+ * affine, variations, post (with_affine) or the variations alone.  The
+ * single-step parity entry; `xform` >= normals selects a final. */
+int ffb_apply_points(ffb_renderer* r, const char* config, size_t config_len, int32_t xform, uint32_t n,
+                     const float* xs, const float* ys, const float* words, int32_t with_affine, int32_t math,
+                     float* xo, float* yo);
+
+/* Compile the chaos-game kernel of a config's structure for sm_100a with
+ * NVRTC, without a device (the shader builder's build step,
+ * src/shader_builder_v2.rs:2337; src/shader_cache.rs).  Writes the CUBIN
+ * size to *cubin_bytes and, if `source` is not NULL, up to source_len
+ * bytes of the generated source.  Needs no GPU. */
+int ffb_specialize(const char* config, size_t config_len, int32_t rng, int32_t math, size_t* cubin_bytes,
+                   char* source, size_t source_len);
+
+/* The splat-throughput microbenchmark: `samples` random splats of `kind`
+ * (0: the 4-atomic splat, 1: one u32 atomic, 2: one f32x4 reduction) into
+ * a histogram of `pixels`; returns the device milliseconds. */
+int ffb_atomic_bench(ffb_renderer* r, uint32_t pixels, uint64_t samples, int32_t kind, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFB200_H */

@@ -1,0 +1,342 @@
+"""ctypes front of the CPU oracle (oracle/flame_oracle.cpp) -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module, and only as the checker.  The product never does.
+
+The oracle restates the reference's render path (see the C++ header for the
+file:line of every function).  This module turns a flame description (the
+`.fae` JSON subset, as a Python dict) into the oracle's flat arrays: the
+local variation order of the reference (src/scene/transforms.rs:40-70,
+668-682, 2297-2319), the f32 transform records, the palette table.
+"""
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+# Registry ids: positions in ALL_VARIATIONS (src/variations/defs/mod.rs:446).
+REGISTRY = {
+    "linear": 0, "sinusoidal": 1, "spherical": 2, "swirl": 3, "horseshoe": 4,
+    "polar": 5, "disc": 8, "ex": 12, "julia": 13, "bubble": 27, "cylinder": 28,
+    "curl": 47,
+}
+PARAMS = {"curl": [("c1", 1.0), ("c2", 0.0)]}   # advanced.rs:1666-1678 defaults
+
+XF_STRIDE = 17
+
+
+def build():
+    """Compile the oracle (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.of_probe.restype = ctypes.c_uint64
+        L.of_probe_digest.restype = ctypes.c_uint64
+        L.of_render.restype = ctypes.c_uint64
+        L.of_pcg_hash.restype = ctypes.c_uint32
+        L.of_rng_next.restype = ctypes.c_uint32
+        L.of_f16_round.restype = ctypes.c_float
+        L.of_f16_round.argtypes = [ctypes.c_float]
+        L.of_select.argtypes = [ctypes.c_void_p, ctypes.c_float]
+        L.of_world_to_pixel.argtypes = [ctypes.c_void_p, ctypes.c_float, ctypes.c_float,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        _lib = L
+    return _lib
+
+
+class OFlame(ctypes.Structure):
+    _fields_ = [
+        ("n_xf", ctypes.c_int), ("n_fin", ctypes.c_int), ("n_var", ctypes.c_int),
+        ("var_id", ctypes.POINTER(ctypes.c_int)),
+        ("xf", ctypes.POINTER(ctypes.c_float)),
+        ("var_w", ctypes.POINTER(ctypes.c_float)),
+        ("var_p", ctypes.POINTER(ctypes.c_float)),
+        ("zoom", ctypes.c_float), ("pan_x", ctypes.c_float), ("pan_y", ctypes.c_float),
+        ("cos_r", ctypes.c_float), ("sin_r", ctypes.c_float),
+        ("width", ctypes.c_int), ("height", ctypes.c_int),
+        ("palette", ctypes.POINTER(ctypes.c_float)), ("pal_n", ctypes.c_int),
+    ]
+
+
+class TonemapParams(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int), ("exposure", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("density_scale", ctypes.c_double), ("bg", ctypes.c_double * 3),
+        ("use_curve", ctypes.c_int), ("curve", ctypes.POINTER(ctypes.c_float)),
+        ("vibrancy", ctypes.c_double), ("brightness", ctypes.c_double), ("white_level", ctypes.c_double),
+        ("prefilter_white", ctypes.c_double), ("bright_adjust", ctypes.c_double),
+        ("area", ctypes.c_double), ("sample_density", ctypes.c_double),
+        ("saturation", ctypes.c_double), ("hue_shift", ctypes.c_double), ("gamma_threshold", ctypes.c_double),
+        ("alpha_blend_low", ctypes.c_double), ("alpha_blend_high", ctypes.c_double),
+        ("transparent_mode", ctypes.c_int), ("highlight_mode", ctypes.c_int), ("levels_enabled", ctypes.c_int),
+        ("levels_low", ctypes.c_double), ("levels_high", ctypes.c_double), ("levels_gamma", ctypes.c_double),
+        ("levels_density", ctypes.c_double),
+    ]
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def f32(x):
+    return float(np.float32(x))
+
+
+# ------------------------------------------------------------------ flames --
+
+def ordered_variation_names(t):
+    """transforms.rs:668-682: `variation_order` entries first, then registry order."""
+    out = []
+    for n in t.get("variation_order", []):
+        if n in t["variations"] and n not in out:
+            out.append(n)
+    for n in sorted(REGISTRY, key=REGISTRY.get):
+        if n in t["variations"] and n not in out:
+            out.append(n)
+    for n in t["variations"]:
+        if n not in REGISTRY:
+            raise ValueError(f"variation `{n}` is not in this oracle's registry")
+    return out
+
+
+def finals_of(flame):
+    fins = list(flame.get("final_transforms", []))
+    if flame.get("final_transform"):
+        fins.append(flame["final_transform"])
+    return fins
+
+
+def local_order(flame):
+    """transforms.rs:2297-2319: normals then finals, first appearance wins."""
+    out = []
+    for t in list(flame["transforms"]) + finals_of(flame):
+        for n in ordered_variation_names(t):
+            if n not in out:
+                out.append(n)
+    return out
+
+
+def hex_stops(hexs):
+    """palette.rs:453-482: `indexed_colors` -> stops at i/255."""
+    pos, col = [], []
+    for i, h in enumerate(hexs.split(",")):
+        pos.append(f32(f32(i) / f32(255.0)))
+        col += [f32(int(h[k:k + 2], 16)) / f32(255.0) for k in (0, 2, 4)]
+    return np.array(pos, np.float32), np.array(col, np.float32)
+
+
+def palette_table(cfg):
+    pal = cfg.get("palette")
+    size = int(cfg.get("palette_size", 256))
+    if pal is None:
+        pos, col = np.zeros(0, np.float32), np.zeros(0, np.float32)
+    elif "indexed_colors" in pal:
+        pos, col = hex_stops(pal["indexed_colors"])
+    else:
+        pos = np.array([s["position"] for s in pal["stops"]], np.float32)
+        col = np.array([c for s in pal["stops"] for c in s["color"]], np.float32)
+    out = np.zeros(size * 3, np.float32)
+    lib().of_palette_table(ctypes.c_int(len(pos)), _fp(pos), _fp(col), ctypes.c_int(size),
+                           ctypes.c_float(cfg.get("palette_rotation", 0.0)),
+                           ctypes.c_int(1 if cfg.get("palette_reverse") else 0), _fp(out))
+    return out
+
+
+class Flame:
+    """A config (dict) flattened for the oracle; keeps its arrays alive."""
+
+    def __init__(self, cfg, width, height):
+        flame = cfg["flame"]
+        self.names = local_order(flame)
+        normals = flame["transforms"]
+        fins = finals_of(flame)
+        allx = list(normals) + fins
+        nv = len(self.names)
+        self.var_id = np.array([REGISTRY[n] for n in self.names], np.int32)
+        self.xf = np.zeros(len(allx) * XF_STRIDE, np.float32)
+        self.var_w = np.zeros(len(allx) * max(nv, 1), np.float32)
+        self.var_p = np.zeros(len(allx) * max(nv, 1) * 2, np.float32)
+        for i, t in enumerate(allx):
+            post = bool(t.get("post_affine_enabled", False))      # transforms.rs:1542; buffers.rs:467
+            rec = [t["a"], t["b"], t["c"], t["d"], t["e"], t["f"],
+                   t.get("post_a", 1.0), t.get("post_b", 0.0), t.get("post_c", 0.0),
+                   t.get("post_d", 1.0), t.get("post_e", 0.0), t.get("post_f", 0.0),
+                   1.0 if post else 0.0, t.get("weight", 1.0), t.get("color", 0.5),
+                   t.get("color_speed", 0.0), t.get("opacity", 1.0)]
+            self.xf[i * XF_STRIDE:(i + 1) * XF_STRIDE] = rec
+            for v, n in enumerate(self.names):
+                self.var_w[i * nv + v] = t["variations"].get(n, 0.0)
+                for j, (pn, dflt) in enumerate(PARAMS.get(n, [])):
+                    self.var_p[(i * nv + v) * 2 + j] = t.get("variation_params", {}).get(f"{n}.{pn}", dflt)
+        self.palette = palette_table(cfg)
+        rot = float(cfg.get("rotation", 0.0))
+        s = OFlame()
+        s.n_xf, s.n_fin, s.n_var = len(normals), len(fins), nv
+        s.var_id = self.var_id.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        s.xf, s.var_w, s.var_p = _fp(self.xf), _fp(self.var_w), _fp(self.var_p)
+        s.zoom = cfg.get("zoom", 1.0)
+        s.pan_x, s.pan_y = cfg.get("pan_x", 0.0), cfg.get("pan_y", 0.0)
+        s.cos_r, s.sin_r = math.cos(rot), math.sin(rot)
+        s.width, s.height = width, height
+        s.palette, s.pal_n = _fp(self.palette), len(self.palette) // 3
+        self.s = s
+        self.width, self.height = width, height
+
+    @property
+    def ptr(self):
+        return ctypes.byref(self.s)
+
+    def render(self, walkers, iters, *, seed=12345, seed_hi=0, rng="philox", burn_in=20, ipt=1024,
+               threads=1, walker0=0, hist=True, f64=False):
+        """The chaos game: (plotted, inframe, counts[h,w] u32, rgb sums[h,w,3] f64)."""
+        n = self.width * self.height
+        cnt = np.zeros(n, np.uint32) if hist else None
+        rgb = np.zeros(n * 3, np.float64) if hist else None
+        inframe = ctypes.c_int64(0)
+        plotted = lib().of_render(
+            self.ptr, ctypes.c_int(0 if rng == "pcg" else 1), ctypes.c_uint32(seed & 0xFFFFFFFF),
+            ctypes.c_uint32(seed_hi & 0xFFFFFFFF), ctypes.c_uint32(burn_in), ctypes.c_uint32(ipt),
+            ctypes.c_uint32(walker0), ctypes.c_uint32(walkers), ctypes.c_uint64(iters), ctypes.c_int(threads),
+            cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)) if hist else None,
+            rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if hist else None,
+            ctypes.byref(inframe), ctypes.c_int(1 if f64 else 0))
+        if not hist:
+            return plotted, inframe.value, None, None
+        return plotted, inframe.value, cnt.reshape(self.height, self.width), rgb.reshape(self.height, self.width, 3)
+
+    def apply_xform(self, xi, xs, ys, draws=None, with_affine=True):
+        xs = np.ascontiguousarray(xs, np.float32)
+        ys = np.ascontiguousarray(ys, np.float32)
+        n = len(xs)
+        d = np.zeros(n * 16, np.float32) if draws is None else np.ascontiguousarray(draws, np.float32)
+        xo, yo = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        lib().of_apply_xform(self.ptr, ctypes.c_int(xi), ctypes.c_int(n), _fp(xs), _fp(ys), _fp(d), _fp(xo), _fp(yo),
+                             ctypes.c_int(1 if with_affine else 0))
+        return xo, yo
+
+    def select(self, u):
+        return lib().of_select(self.ptr, ctypes.c_float(u))
+
+    def draw_slots(self):
+        return lib().of_draw_slots(self.ptr)
+
+    def world_to_pixel(self, x, y):
+        px, py = ctypes.c_int(), ctypes.c_int()
+        lib().of_world_to_pixel(self.ptr, ctypes.c_float(x), ctypes.c_float(y), ctypes.byref(px), ctypes.byref(py))
+        return px.value, py.value
+
+
+# ------------------------------------------------------------ variations --
+
+def variation(name, xs, ys, draws=None, params=None, f64=False, ftz=True):
+    xs = np.ascontiguousarray(xs, np.float32)
+    ys = np.ascontiguousarray(ys, np.float32)
+    n = len(xs)
+    prm = np.array(params if params is not None else [d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
+    d = None if draws is None else np.ascontiguousarray(draws, np.float32)
+    xo, yo = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    lib().of_variation(ctypes.c_int(REGISTRY[name]), _fp(prm), ctypes.c_int(n), _fp(xs), _fp(ys),
+                       _fp(d) if d is not None else None, _fp(xo), _fp(yo), ctypes.c_int(1 if f64 else 0),
+                       ctypes.c_int(1 if ftz else 0))
+    return xo, yo
+
+
+def probe(name, xform_slot=None, fold_first=None):
+    """(classes, digest, raw outputs) as src/probe/ reports them."""
+    vid = REGISTRY[name]
+    slot = vid if xform_slot is None else xform_slot
+    fold = (slot == 0) if fold_first is None else fold_first
+    prm = np.array([d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
+    cls = ctypes.create_string_buffer(64)
+    out = np.zeros(54, np.float32)
+    dig = lib().of_probe(ctypes.c_int(vid), _fp(prm), ctypes.c_int(slot), ctypes.c_int(1 if fold else 0), cls, _fp(out))
+    return cls.value.decode(), dig, out
+
+
+def probe_digest(vals):
+    v = np.ascontiguousarray(vals, np.float32)
+    cls = ctypes.create_string_buffer(64)
+    dig = lib().of_probe_digest(_fp(v), cls)
+    return cls.value.decode(), dig
+
+
+# ------------------------------------------------------------------- RNG --
+
+def pcg_hash(x):
+    return lib().of_pcg_hash(ctypes.c_uint32(x))
+
+
+def rng_init(tid, seed):
+    st = (ctypes.c_uint32 * 2)()
+    lib().of_rng_init(ctypes.c_uint32(tid), ctypes.c_uint32(seed), st)
+    return st
+
+
+def rng_next(st):
+    return lib().of_rng_next(st)
+
+
+def philox(k0, k1, ctr):
+    c = (ctypes.c_uint32 * 4)(*ctr)
+    o = (ctypes.c_uint32 * 4)()
+    lib().of_philox(ctypes.c_uint32(k0), ctypes.c_uint32(k1), c, o)
+    return list(o)
+
+
+def f16_round(v):
+    return lib().of_f16_round(ctypes.c_float(v))
+
+
+# ------------------------------------------------------------ tone map ----
+
+def curve_lut_identity():
+    """tonemap.rs:289-304 for the linear (identity) curve: f16(i/255)."""
+    return np.array([f16_round(f32(i) / f32(255.0)) for i in range(256)], np.float32)
+
+
+def tonemap(params, cnt, rgb):
+    """Double-precision tone map: (float RGBA [n,4], RGBA8 [n,4])."""
+    cnt = np.ascontiguousarray(cnt, np.float64).ravel()
+    rgb = np.ascontiguousarray(rgb, np.float64).ravel()
+    n = len(cnt)
+    of = np.zeros(n * 4, np.float64)
+    ou = np.zeros(n * 4, np.uint8)
+    lib().of_tonemap(ctypes.byref(params), cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.c_int(n),
+                     of.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ou.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    return of.reshape(n, 4), ou.reshape(n, 4)
+
+
+def downsample_firefly(rgba, ow, oh):
+    src = np.ascontiguousarray(rgba, np.uint8).ravel()
+    out = np.zeros(ow * oh * 4, np.uint8)
+    lib().of_downsample_firefly(src.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), ctypes.c_int(ow), ctypes.c_int(oh),
+                                out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    return out.reshape(oh, ow, 4)
+
+
+def density_estimate(cnt, rgb, w, h, r_max, r_min=0.0, curve=0.4):
+    cnt = np.ascontiguousarray(cnt, np.float64).ravel()
+    rgb = np.ascontiguousarray(rgb, np.float64).ravel()
+    oc = np.zeros(w * h, np.float64)
+    orgb = np.zeros(w * h * 3, np.float64)
+    P = ctypes.POINTER(ctypes.c_double)
+    lib().of_density_estimate(cnt.ctypes.data_as(P), rgb.ctypes.data_as(P), ctypes.c_int(w), ctypes.c_int(h),
+                              ctypes.c_double(r_max), ctypes.c_double(r_min), ctypes.c_double(curve),
+                              oc.ctypes.data_as(P), orgb.ctypes.data_as(P))
+    return oc.reshape(h, w), orgb.reshape(h, w, 3)

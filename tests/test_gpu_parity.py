@@ -1,0 +1,348 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances:
+* per-step iterate, per variation: <= 4 ulp FP32 (cancellations: 4 ulp of
+  the terms' magnitude);
+* histograms: bit-exact counts for a linear-only flame (no transcendental
+  arithmetic, identical orbits); otherwise normalised log-density within
+  the Monte-Carlo noise measured between two oracle renders;
+* tone map and density estimation: 1e-5 relative of the FP64 oracle.
+"""
+
+import json
+import math
+
+import numpy as np
+import pytest
+
+from ffb200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+TWELVE = synthetic.TWELVE
+PROBE_PTS = None
+
+
+def ulp_dist(a, b):
+    a = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
+    b = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
+    a = np.where(a < 0, -(a & 0x7FFFFFFF), a)
+    b = np.where(b < 0, -(b & 0x7FFFFFFF), b)
+    return np.abs(a - b)
+
+
+def close_f32(gpu, ref, scale, ulps=4):
+    """Per component: <= `ulps` ulp, or <= `ulps` ulp of `scale` (the size of
+    the terms a cancellation subtracted)."""
+    gpu, ref = np.asarray(gpu, np.float32), np.asarray(ref, np.float32)
+    same_class = (np.isnan(gpu) == np.isnan(ref)) & (np.isinf(gpu) == np.isinf(ref))
+    finite = np.isfinite(gpu) & np.isfinite(ref)
+    ok = np.where(finite, ulp_dist(gpu, ref) <= ulps, same_class & ((gpu == ref) | np.isnan(gpu)))
+    tol = ulps * np.spacing(np.maximum(np.abs(scale), 1e-30).astype(np.float32))
+    ok |= finite & (np.abs(gpu.astype(np.float64) - ref) <= tol)
+    return ok
+
+
+def one_xform(name, a=(1, 0, 0, 1, 0, 0), params=None):
+    t = {"a": a[0], "b": a[1], "c": a[2], "d": a[3], "e": a[4], "f": a[5], "weight": 1.0, "color": 0.5,
+         "variations": {name: 1.0}}
+    if params:
+        t["variation_params"] = params
+    return {"flame": {"transforms": [t]}, "deterministic_rng": True}
+
+
+@pytest.fixture(scope="module")
+def pts(oracle):
+    _, _, _ = oracle.probe("linear")
+    # The 27 probe inputs (src/probe/inputs.rs:49-77), as the oracle holds them.
+    vals = []
+    for x, y in [(0.0, 0.0), (0.0, -0.0), (-0.0, 0.0), (-0.0, -0.0), (1, 0), (-1, 0), (0, 1), (0, -1), (1, 1), (-1, 1),
+                 (-1, -1), (1, -1), (0.5, 0.3), (0.12345679, -0.9876543), (2.5, -1.5), (math.pi, math.e), (1, 0),
+                 (0.70710677, 0.70710677), (1e-20, -1e-20), (1.1754944e-38, 1.1754944e-38), (1e-40, -1e-40),
+                 (1e20, -1e20), (9e31, -9e31), (1e33, -1e33), (1e30, 1e-30), (1.0, -0.0), (-0.0, 1.0)]:
+        vals += [x, y]
+    return np.array(vals, np.float32).reshape(-1, 2)
+
+
+@pytest.mark.parametrize("name", TWELVE)
+def test_probe_matches_oracle(renderer, oracle, pts, name):
+    """The variation probe at the 27 inputs: CUDA (precise math) vs the oracle,
+    both at probe slot 0 (RNG rng_init(point, 0x9E3779B9))."""
+    out = renderer.probe(one_xform(name), pts, 1)[0]
+    _, _, ref = oracle.probe(name, xform_slot=0, fold_first=False)
+    ref = ref.reshape(27, 2)
+    scale = np.maximum(np.abs(pts).max(axis=1, keepdims=True), np.abs(ref).max(axis=1, keepdims=True))
+    scale = np.broadcast_to(scale, ref.shape)
+    ok = close_f32(out, ref, scale)
+    bad = [(i, pts[i].tolist(), out[i].tolist(), ref[i].tolist()) for i in range(27) if not ok[i].all()]
+    assert not bad, f"{name}: {bad}"
+
+
+def test_probe_sfu_math_reproduces_reference_classes(renderer, oracle, pts):
+    """With the hardware's approximate sin/cos (math = sfu) the CUDA probe
+    reproduces the reference GPU's class glyphs at every input, including
+    those where IEEE sin differs (tests/golden/variation_probe_2d.txt)."""
+    import os
+    GOLDEN = {}
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "variation_probe_2d.txt")) as f:
+        for line in f:
+            if not line.startswith("#") and line.strip():
+                n, c, d = line.split()
+                GOLDEN[n] = (c, int(d, 16))
+    mism = {}
+    for name in TWELVE:
+        slot = oracle.REGISTRY[name]
+        # Place the variation at its probe-batch transform so julia's draw matches.
+        cfg = {"flame": {"transforms": [one_xform(name)["flame"]["transforms"][0]] * (slot + 1)}}
+        out = renderer.probe(cfg, pts, slot + 1, math="sfu")[slot].reshape(-1)
+        classes, _ = oracle.probe_digest(out)
+        gold = GOLDEN[name][0]
+        if name == "linear":
+            # signed zeros: the reference compiler folded 0 + x into x for the batch's first variation
+            gold = gold.replace("o", "0")
+            classes = classes.replace("o", "0")
+        diff = [i for i in range(54) if classes[i] != gold[i]]
+        if diff:
+            mism[name] = (classes, gold, diff)
+    assert len(mism) <= 2, mism
+
+
+def test_apply_points_matches_oracle(renderer, oracle):
+    """Single step of every transform of a flame using all twelve variations
+    (affine, weighted variation sum, post-affine; finals too) at 4096 random
+    points with random draws: <= 4 ulp."""
+    rng = np.random.default_rng(5)
+    t1 = {"a": 0.7, "b": -0.3, "c": 0.4, "d": 0.9, "e": 0.1, "f": -0.2, "weight": 1.0, "color": 0.1,
+          "variations": {n: float(rng.uniform(0.1, 1.0)) for n in TWELVE[:6]},
+          "variation_params": {"curl.c1": 0.7, "curl.c2": 0.2}}
+    t2 = {"a": -0.5, "b": 0.6, "c": 0.3, "d": 0.2, "e": -0.4, "f": 0.3, "weight": 2.0, "color": 0.9,
+          "post_affine_enabled": True, "post_a": 0.9, "post_b": 0.1, "post_c": -0.2, "post_d": 1.1, "post_e": 0.05,
+          "post_f": 0.0, "variations": {n: float(rng.uniform(0.1, 1.0)) for n in TWELVE[6:]},
+          "variation_params": {"curl.c1": 0.4, "curl.c2": -0.3}}
+    fin = {"a": 1.0, "b": 0.1, "c": -0.1, "d": 1.0, "e": 0.0, "f": 0.0, "weight": 1.0, "color": 0.0,
+           "variations": {"julia": 0.5, "swirl": 0.3, "disc": 0.2}}
+    cfg = {"flame": {"transforms": [t1, t2], "final_transform": fin}}
+    fl = oracle.Flame(cfg, 64, 64)
+    n = 4096
+    xs = rng.uniform(-2.5, 2.5, n).astype(np.float32)
+    ys = rng.uniform(-2.5, 2.5, n).astype(np.float32)
+    words = (rng.integers(0, 1 << 24, (n, 16)) / float(1 << 24)).astype(np.float32)
+    worst = {}
+    for xi in range(3):
+        for aff in (True, False):
+            gx, gy = renderer.apply_points(cfg, xi, xs, ys, words, with_affine=aff)
+            rx, ry = fl.apply_xform(xi, xs, ys, words, with_affine=aff)
+            scale = np.maximum.reduce([np.abs(xs), np.abs(ys), np.abs(rx), np.abs(ry), np.ones(n, np.float32)])
+            okx = close_f32(gx, rx, scale * 4)
+            oky = close_f32(gy, ry, scale * 4)
+            worst[(xi, aff)] = int(max(ulp_dist(gx, rx)[np.isfinite(rx)].max(), ulp_dist(gy, ry)[np.isfinite(ry)].max()))
+            bad = np.where(~(okx & oky))[0]
+            assert len(bad) == 0, (xi, aff, [(xs[i], ys[i], gx[i], rx[i], gy[i], ry[i]) for i in bad[:5]])
+    print("worst ulp per (transform, affine):", worst)
+
+
+@pytest.mark.parametrize("rng_mode", ["pcg", "philox"])
+def test_histogram_bit_exact_for_a_linear_flame(renderer, oracle, rng_mode):
+    """No transcendentals: the GPU walks the oracle's orbits exactly, so the
+    count plane is identical, pixel for pixel, and sums to the in-frame count."""
+    cfg = synthetic.sierpinski()
+    W, H = 96, 64
+    job = dict(iterations=2048 * 700, walkers=2048, rng=rng_mode, iterations_per_thread=256)
+    cnt, rgb, out = renderer.histogram(cfg, W, H, **job)
+    fl = oracle.Flame(cfg, W, H)
+    plotted, inframe, rc, rr = fl.render(2048, 700 + 20, rng=rng_mode, ipt=256, threads=8)
+    assert out.total_iterations == plotted == 2048 * 700
+    assert int(cnt.sum()) == out.inframe_samples == inframe
+    assert np.array_equal(cnt, rc)
+    np.testing.assert_allclose(rgb, rr, rtol=1e-5, atol=1e-3)
+
+
+def log_density_l1(a, b):
+    la, lb = np.log1p(a.astype(np.float64)), np.log1p(b.astype(np.float64))
+    lit = (a > 0) | (b > 0)
+    d = np.abs(la - lb)[lit]
+    return d.mean(), np.percentile(d, 99)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_histogram_density_within_monte_carlo_noise(renderer, oracle, seed):
+    """A plain 3-transform flame (linear/sinusoidal/spherical): the GPU's
+    normalised log-density differs from the oracle's by no more than two
+    independent oracle renders differ (L1 and 99th percentile)."""
+    cfg = synthetic.plain_flame(seed)
+    W = H = 128
+    walkers, per = 8192, 400
+    cnt, _, out = renderer.histogram(cfg, W, H, iterations=walkers * per, walkers=walkers, seed=1001)
+    fl = oracle.Flame(cfg, W, H)
+    _, _, o1, _ = fl.render(walkers, per + 20, seed=1001, threads=8)
+    _, _, o2, _ = fl.render(walkers, per + 20, seed=2002, threads=8)
+    if o1.sum() < 1000:
+        pytest.skip("flame lights too little of the frame")
+    l1_go, p99_go = log_density_l1(cnt, o1)
+    l1_oo, p99_oo = log_density_l1(o2, o1)
+    assert l1_go <= 1.25 * l1_oo + 0.01, (l1_go, l1_oo)
+    assert p99_go <= 1.25 * p99_oo + 0.05, (p99_go, p99_oo)
+    # 16x16-block densities: |z| > 5 blocks no more than between the oracle's replicates.
+    def blocks(c):
+        return c.reshape(H // 16, 16, W // 16, 16).sum(axis=(1, 3)).astype(np.float64)
+    bg, b1, b2 = blocks(cnt), blocks(o1), blocks(o2)
+    se = np.sqrt(np.maximum(b1 + b2, 1.0))
+    assert (np.abs(bg - b1) / se > 5).sum() <= max(2, (np.abs(b2 - b1) / se > 5).sum() + 2)
+
+
+def tonemap_params(oracle, cfg, w, h, sd, transparent=0):
+    tm = oracle.TonemapParams()
+    modes = {"linear": 0, "Linear": 0, "logarithmic": 1, "Logarithmic": 1, "density": 2, "DensityVisualization": 2}
+    highs = {"clip": 0, "max_norm": 1, "reinhard": 2, "filmic": 3}
+    tm.mode = modes[cfg.get("tonemap_mode", "logarithmic")]
+    tm.highlight_mode = highs[cfg.get("highlight_mode", "clip")]
+    tm.exposure = cfg.get("exposure", 1.0)
+    tm.gamma = cfg.get("gamma", 4.0)
+    tm.density_scale = cfg.get("density_scale", 1.0)
+    bg = cfg.get("background_color", [0, 0, 0])
+    for k in range(3):
+        tm.bg[k] = bg[k]
+    tm.use_curve = 1 if cfg.get("use_curve", True) else 0
+    lut = oracle.curve_lut_identity()
+    tm._lut = lut
+    tm.curve = lut.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_float))
+    tm.vibrancy = cfg.get("vibrancy", 1.0)
+    tm.brightness = cfg.get("brightness", 4.0)
+    tm.white_level = cfg.get("white_level", 200.0)
+    tm.prefilter_white = 67108864.0
+    tm.bright_adjust = 2.3
+    ppu = min(w, h) * 0.25 * float(np.float32(cfg.get("zoom", 1.0)))
+    tm.area = w * h / (ppu * ppu)
+    tm.sample_density = sd
+    tm.saturation = cfg.get("saturation", 1.0)
+    tm.hue_shift = cfg.get("hue_shift", 0.0)
+    tm.gamma_threshold = cfg.get("gamma_threshold", 5.0)
+    tm.alpha_blend_low = cfg.get("alpha_blend_low", 0.3)
+    tm.alpha_blend_high = cfg.get("alpha_blend_high", 0.8)
+    tm.transparent_mode = transparent
+    tm.levels_enabled = 1 if cfg.get("levels_enabled", True) else 0
+    tm.levels_low = cfg.get("levels_low", 0.0)
+    tm.levels_high = cfg.get("levels_high", 10.0)
+    tm.levels_gamma = cfg.get("levels_gamma", 0.5)
+    tm.levels_density = sd
+    return tm
+
+
+TONEMAP_VARIANTS = [
+    {},
+    {"vibrancy": 0.5, "gamma": 2.2, "gamma_threshold": 0.01},
+    {"saturation": 1.5, "hue_shift": 40.0, "highlight_mode": "max_norm"},
+    {"highlight_mode": "reinhard", "exposure": 3.0, "levels_enabled": False},
+    {"highlight_mode": "filmic", "background_color": [0.2, 0.1, 0.05]},
+    {"tonemap_mode": "linear", "gamma": 2.0},
+    {"tonemap_mode": "density", "exposure": 0.5},
+]
+
+
+@pytest.fixture(scope="module")
+def c1_hist(renderer):
+    cfg = synthetic.plain_flame(3)
+    cnt, rgb, out = renderer.histogram(cfg, 128, 128, iterations=2_000_000, seed=77)
+    return cfg, cnt, rgb, out
+
+
+@pytest.mark.parametrize("variant", range(len(TONEMAP_VARIANTS)))
+@pytest.mark.parametrize("transparent", [0, 1, 2])
+def test_tonemap_matches_f64_oracle(renderer, oracle, c1_hist, variant, transparent):
+    base, cnt, rgb, out = c1_hist
+    cfg = dict(base, **TONEMAP_VARIANTS[variant])
+    h, w = cnt.shape
+    sd = out.total_iterations / (w * h)
+    u8, f = renderer.tonemap(cfg, cnt.astype(np.float32), rgb, sd, ss=1, transparent=transparent, want_float=True)
+    P = tonemap_params(oracle, cfg, w, h, sd, transparent)
+    rf, ru = oracle.tonemap(P, cnt.astype(np.float64), rgb.astype(np.float64))
+    f = f.reshape(-1, 4).astype(np.float64)
+    err = np.abs(f - rf) / np.maximum(np.abs(rf), 1e-3)
+    assert err.max() <= 1e-5, (variant, transparent, float(err.max()), np.unravel_index(err.argmax(), err.shape))
+    # 8-bit output: equal except where the value sits on a rounding boundary.
+    d = np.abs(u8.reshape(-1, 4).astype(int) - ru.astype(int))
+    frac = np.abs(rf * 255 - np.round(rf * 255))
+    assert d.max() <= 1 and (d > 0).sum() <= max(3, int(0.001 * d.size))
+    assert np.all((d == 0) | (np.abs(frac - 0.5) < 1e-3))
+
+
+def test_supersample_downsample_matches_oracle(renderer, oracle, c1_hist):
+    """ss 2: the fused tone map + firefly box vs the oracle's tone map, 8-bit
+    quantisation and supersample.rs:132-167."""
+    cfg, cnt, rgb, out = c1_hist
+    h, w = cnt.shape
+    sd = out.total_iterations / (w * h)
+    u8 = renderer.tonemap(cfg, cnt.astype(np.float32), rgb, sd, ss=2)
+    P = tonemap_params(oracle, cfg, w, h, sd)
+    _, ru = oracle.tonemap(P, cnt.astype(np.float64), rgb.astype(np.float64))
+    ref = oracle.downsample_firefly(ru.reshape(h, w, 4), w // 2, h // 2)
+    d = np.abs(u8.astype(int) - ref.astype(int))
+    assert d.max() <= 1 and (d > 0).mean() < 0.002
+
+
+@pytest.mark.parametrize("radius", [3.0, 9.0, 18.0])
+def test_density_estimation_matches_f64_oracle(renderer, oracle, radius):
+    cfg = synthetic.plain_flame(3)
+    cnt, rgb, _ = renderer.histogram(cfg, 96, 80, iterations=150_000, seed=5)
+    gc, grgb = renderer.density_estimate(cnt, rgb, radius, 0.0, 0.4)
+    oc, orgb = oracle.density_estimate(cnt, rgb, 96, 80, radius, 0.0, 0.4)
+    # Conservation: DE moves density, it does not make or lose it (away from the edges).
+    assert abs(gc.sum() - cnt.sum()) / cnt.sum() < 0.05
+    scale = max(oc.max(), 1.0)
+    assert np.max(np.abs(gc - oc) / np.maximum(np.abs(oc), 1e-3 * scale)) <= 1e-5
+    assert np.max(np.abs(grgb - orgb) / np.maximum(np.abs(orgb), 1e-3 * max(orgb.max(), 1.0))) <= 1e-5
+
+
+def test_point_render_known_answer(renderer):
+    """compute_kernel.rs:6502-6511 through the CUDA path: at 64x64 a point at
+    x = -1.96875 lights column 0 of the middle row alone; -2.03125 lights nothing."""
+    for x, lit in ((-1.96875, 1), (-2.03125, 0)):
+        cfg = {"flame": {"transforms": [{"a": 0, "b": 0, "c": 0, "d": 0, "e": x, "f": 0, "weight": 1, "color": 0,
+                                         "variations": {"linear": 1.0}}]}, "deterministic_rng": True}
+        cnt, _, out = renderer.histogram(cfg, 64, 64, iterations=200_000)
+        assert int((cnt > 0).sum()) == lit
+        if lit:
+            assert cnt[32, 0] == out.inframe_samples == out.total_iterations
+        img, o = renderer.render(cfg, 64, 64, iterations=200_000)
+        assert int((img[..., :3].max(axis=2) > 0).sum()) == lit
+
+
+def test_render_counts_what_it_plotted(renderer):
+    """render.rs:598-708: the render stops on plotted samples and reports them."""
+    cfg = synthetic.plain_flame(2)
+    _, o = renderer.render(cfg, 32, 32, iterations=4_000_000, iterations_per_thread=16, burn_in=30)
+    assert o.total_iterations >= 4_000_000
+
+
+def test_errors_are_reported_not_raised_on_the_device(renderer, native):
+    t = synthetic.plain_flame(1)["flame"]["transforms"][0]
+    with pytest.raises(native.EngineError) as e:
+        renderer.render({"flame": {"transforms": [t] * 129}}, 16, 16, iterations=1000)
+    assert e.value.status == native.ERR_TOO_LARGE and "129" in str(e.value)
+    with pytest.raises(native.EngineError) as e:
+        renderer.render(synthetic.plain_flame(1), 0, 16)
+    assert e.value.status == native.ERR_INVALID
+    with pytest.raises(native.EngineError) as e:
+        renderer.render('{"flame": ', 16, 16)
+    assert e.value.status == native.ERR_CONFIG
+    # The renderer still works after refusing.
+    img, _ = renderer.render(synthetic.plain_flame(1), 16, 16, iterations=10_000)
+    assert img.shape == (16, 16, 4)
+
+
+def test_engine_renders_like_pyfae():
+    """python/tests/test_render.py:34-41, 52-57 against the drop-in Engine."""
+    import ffb200
+    eng = ffb200.Engine()
+    cfg = synthetic.plain_flame(3)
+    image = eng.render(cfg, 160, 120, iterations=5_000_000)
+    assert (image.width, image.height) == (160, 120)
+    assert len(image.rgba) == 160 * 120 * 4
+    assert image.info["iterations"] >= 5_000_000
+    assert image.info["iterations_per_thread"] == 1024
+    lit = int((image.array()[..., :3].max(axis=2) > 0).sum())
+    assert lit > 1000
+    again = ffb200.Engine().render(cfg, 160, 120, iterations=5_000_000)
+    a, b = image.array().astype(int), again.array().astype(int)
+    # Counts are exact; FP32 colour sums may round in another order.
+    assert np.abs(a - b).max() <= 1 and (a != b).mean() < 0.01
