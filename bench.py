@@ -154,9 +154,12 @@ def run_ours(args, rank, world, local_rank):
     W, H, ss = wl["width"], wl["height"], wl["supersample"]
     r = _native.Renderer(local_rank)
     job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, walker0=rank * wl["walkers"],
-               seed=0x5EED + 0)
+               seed=0x5EED + 0, schedule=args.schedule)
     d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
-    stream = torch.cuda.current_stream().cuda_stream
+    # The library's kernels and the timing events share one (non-default) stream.
+    side = torch.cuda.Stream()
+    torch.cuda.set_stream(side)
+    stream = side.cuda_stream
     out = r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=True, **job)   # compile + first frame
     samples_per_step = out.total_iterations
     launches_per_step = out.kernel_launches
@@ -230,6 +233,7 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded flame generator; no dataset)",
         "config": {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
                    "samples_per_step": samples_per_step, "walkers": wl["walkers"], "rng": "philox",
+                   "schedule": args.schedule,
                    "l2": "histogram 132.7 MB > 126 MB L2, cleared every step", "parallelism": f"walker shards x{world}"},
         "ms_per_frame": ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -293,11 +297,26 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted"],
+                    help="walker scheduling of the chaos kernel (same orbits either way)")
+    ap.add_argument("--profile", type=float, default=0.0,
+                    help="profiling run for ncu: only the chaos kernel of the workload, at this many samples")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.profile:
+        from ffb200 import _native
+        wl = workload(args.workload)
+        r = _native.Renderer(local_rank)
+        job = dict(iterations=int(args.profile), walkers=wl["walkers"], supersample=wl["supersample"], seed=0x5EED,
+                   schedule=args.schedule)
+        for _ in range(args.warmup + args.steps):
+            _, _, o = r.histogram(json.dumps(wl["cfg"]), wl["width"], wl["height"], **job)
+        print(json.dumps({"profile": args.workload, "samples": o.total_iterations, "inframe": o.inframe_samples,
+                          "ms": o.render_time_ms}))
+        return
     if args.impl == "reference":
         line = run_reference(args, rank, world)
     else:

@@ -48,11 +48,9 @@ __device__ __forceinline__ void ffb_splat(float4* __restrict__ hist, u32 idx, fl
     atomicAdd(reinterpret_cast<u32*>(p + 3), 1u);
 }
 
-extern "C" __global__ void __launch_bounds__(FFB_THREADS)
-ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
-    extern __shared__ float4 ffb_smem4[];
-    float* sm = reinterpret_cast<float*>(ffb_smem4);
-    // The job owning this block (block-uniform binary search).
+// The job owning this block (block-uniform binary search) and its tables
+// staged in shared memory.
+__device__ __forceinline__ const ffb_launch& ffb_stage(const ffb_launch* __restrict__ jobs, int n_jobs, float* sm, float4*& pal) {
     int lo = 0, hi = n_jobs - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
@@ -60,18 +58,15 @@ ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
     }
     const ffb_launch& J = jobs[lo];
     for (int i = threadIdx.x; i < FFB_TABLE_SIZE; i += blockDim.x) sm[i] = J.table[i];
-    float4* pal = ffb_smem4 + FFB_TABLE_VEC4;
+    pal = reinterpret_cast<float4*>(sm) + FFB_TABLE_VEC4;
     for (u32 i = threadIdx.x; i < J.pal_n; i += blockDim.x) pal[i] = J.palette[i];
     __syncthreads();
+    return J;
+}
 
-    const u32 w = (blockIdx.x - J.block0) * blockDim.x + threadIdx.x;
-    if (w >= J.n_walkers) return;
-    const u32 gw = J.walker0 + w;
-    const int n_xf = (int)J.n_xf;
-    float x, y, ci;
-    u32 fuse;
-    const u64 it0 = J.it0, it1 = J.it0 + J.n_iters;
-    if (it0 == 0) {
+// A walker's start (main_template.wgsl:25-55) or its stored state.
+__device__ __forceinline__ void ffb_start(const ffb_launch& J, u32 w, u32 gw, float& x, float& y, float& ci, u32& fuse) {
+    if (J.it0 == 0) {
         ci = 0.0f;
         fuse = J.burn_in;
 #if FFB_RNG_MODE == 1
@@ -79,12 +74,98 @@ ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
         x = u24(o.x) * 2.0f - 1.0f;
         y = u24(o.y) * 2.0f - 1.0f;
 #else
-        x = 0.0f; y = 0.0f;   // drawn at it == 0 below
+        x = 0.0f; y = 0.0f;   // drawn at it == 0 by ffb_pcg_dispatch
 #endif
     } else {
         float4 s = J.walkers[w];
         x = s.x; y = s.y; ci = s.z; fuse = __float_as_uint(s.w);
     }
+}
+
+#if FFB_RNG_MODE == 0
+// A dispatch boundary of the reference's stream: re-seeded per dispatch, the
+// two start draws consumed before the orbit resumes (main_template.wgsl:25-55,
+// 125-181; compute_kernel.rs:3541-3553).
+__device__ __forceinline__ void ffb_pcg_dispatch(const ffb_launch& J, PcgRng& rng, u32 gw, u64 it, float& x, float& y) {
+    if (it == J.it0 || (J.ipt != 0 && it % J.ipt == 0)) {
+        u32 d = J.ipt ? (u32)(it / J.ipt) : 0u;
+        rng.init(gw, J.seed_lo + d * 2654435761u);
+        float s0 = rng.draw(0), s1 = rng.draw(0);
+        if (it == 0) { x = s0 * 2.0f - 1.0f; y = s1 * 2.0f - 1.0f; }
+    }
+}
+#endif
+
+// The rest of an iteration once transform k is picked and the opacity draw
+// made: affine, variations, post, bad-value respawn, colour, fuse, finals,
+// palette, world_to_pixel and the splat (main_template.wgsl:366-1320).
+template <class R>
+__device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
+                                         int k, bool plot, R& rng, u32 gw, u64 it, float& x, float& y, float& ci, u32& fuse,
+                                         float cx, float cy, float scale, u32& inframe) {
+    const float* q = sm + T_XF + k;
+    float ax = q[F_A * FFB_MAXX] * x + q[F_B * FFB_MAXX] * y + q[F_E * FFB_MAXX];
+    float ay = q[F_C * FFB_MAXX] * x + q[F_D * FFB_MAXX] * y + q[F_F * FFB_MAXX];
+    ffb_normal(sm, k, ax, ay, rng);                                         // main_template.wgsl:366-376
+#if FFB_HAS_POST
+    if (q[F_POST * FFB_MAXX] > 0.5f) {                                      // main_template.wgsl:380-384
+        float px = q[F_PA * FFB_MAXX] * ax + q[F_PB * FFB_MAXX] * ay + q[F_PE * FFB_MAXX];
+        float py = q[F_PC * FFB_MAXX] * ax + q[F_PD * FFB_MAXX] * ay + q[F_PF * FFB_MAXX];
+        ax = px; ay = py;
+    }
+#endif
+    if (!(fabsf(ax) <= 1e32f) || !(fabsf(ay) <= 1e32f)) {                  // main_template.wgsl:449-479
+#if FFB_RNG_MODE == 1
+        uint4 o = philox4(J.seed_lo, J.seed_hi, gw, (u32)it, 0xFFFFFFFFu, (u32)(it >> 32));
+        x = u24(o.x) * 2.0f - 1.0f;
+        y = u24(o.y) * 2.0f - 1.0f;
+#else
+        x = rng.draw(0) * 2.0f - 1.0f;
+        y = rng.draw(0) * 2.0f - 1.0f;
+#endif
+        fuse = J.burn_in;
+        return;
+    }
+    x = ax; y = ay;
+    ci = ci * q[F_C1 * FFB_MAXX] + q[F_C2 * FFB_MAXX];                       // main_template.wgsl:496-508
+    if (fuse > 0u) { fuse -= 1u; return; }                                 // main_template.wgsl:510-514
+    float fx = x, fy = y;
+    ffb_finals(sm, fx, fy, rng);                                            // main_template.wgsl:663-717
+    const float4 c = pal[ffb_palette_index(ci, J.pal_n)];                   // main_template.wgsl:766-772
+    // world_to_pixel (utilities.wgsl:417-450).
+    float tx = fx - J.pan_x, ty = fy - J.pan_y;
+    float rx = tx * J.cos_r - ty * J.sin_r;
+    float ry = tx * J.sin_r + ty * J.cos_r;
+    rx = rx * J.zoom; ry = ry * J.zoom;
+    const float pxf = floorf(cx + rx * scale), pyf = floorf(cy + ry * scale);
+    if (plot && pxf >= 0.0f && pyf >= 0.0f && pxf < (float)J.width && pyf < (float)J.height) {
+        const u32 idx = (u32)pyf * (u32)J.width + (u32)pxf;
+        ffb_splat(J.hist, idx, c);
+        ++inframe;
+    }
+}
+
+__device__ __forceinline__ void ffb_count_inframe(const ffb_launch& J, u32 inframe) {
+    // In-frame splat count (count conservation: the sum of the count plane).
+    const unsigned live = __activemask();
+    const u32 tot = __reduce_add_sync(live, inframe);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(live) - 1) && tot) atomicAdd(J.counters, (u64)tot);
+}
+
+// One walker a thread, for the whole launch.
+extern "C" __global__ void __launch_bounds__(FFB_THREADS)
+ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
+    extern __shared__ float4 ffb_smem4[];
+    float* sm = reinterpret_cast<float*>(ffb_smem4);
+    float4* pal;
+    const ffb_launch& J = ffb_stage(jobs, n_jobs, sm, pal);
+    const u32 w = (blockIdx.x - J.block0) * blockDim.x + threadIdx.x;
+    if (w >= J.n_walkers) return;
+    const u32 gw = J.walker0 + w;
+    const int n_xf = (int)J.n_xf;
+    float x, y, ci;
+    u32 fuse;
+    ffb_start(J, w, gw, x, y, ci, fuse);
     const float scale = (float)min(J.width, J.height) * 0.25f;
     const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
     u32 inframe = 0;
@@ -92,70 +173,123 @@ ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
     PcgRng rng;
     rng.state = 0; rng.inc = 1;
 #endif
-    for (u64 it = it0; it < it1; ++it) {
+    const u64 it1 = J.it0 + J.n_iters;
+    for (u64 it = J.it0; it < it1; ++it) {
 #if FFB_RNG_MODE == 0
-        // A dispatch boundary: the stream is re-seeded per dispatch and the
-        // two start draws are consumed before the orbit resumes
-        // (main_template.wgsl:25-55, 125-181; compute_kernel.rs:3541-3553).
-        if (it == it0 || (J.ipt != 0 && it % J.ipt == 0)) {
-            u32 d = J.ipt ? (u32)(it / J.ipt) : 0u;
-            rng.init(gw, J.seed_lo + d * 2654435761u);
-            float s0 = rng.draw(0), s1 = rng.draw(0);
-            if (it == 0) { x = s0 * 2.0f - 1.0f; y = s1 * 2.0f - 1.0f; }
-        }
+        ffb_pcg_dispatch(J, rng, gw, it, x, y);
 #else
         PhiloxRng rng;
         rng.fill(J.seed_lo, J.seed_hi, gw, it);
 #endif
         const int k = ffb_select(sm, n_xf, rng.draw(0));                     // main_template.wgsl:198-223
         const bool plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];       // main_template.wgsl:249
-        const float* q = sm + T_XF + k;
-        float ax = q[F_A * FFB_MAXX] * x + q[F_B * FFB_MAXX] * y + q[F_E * FFB_MAXX];
-        float ay = q[F_C * FFB_MAXX] * x + q[F_D * FFB_MAXX] * y + q[F_F * FFB_MAXX];
-        ffb_normal(sm, k, ax, ay, rng);                                         // main_template.wgsl:366-376
-#if FFB_HAS_POST
-        if (q[F_POST * FFB_MAXX] > 0.5f) {                                      // main_template.wgsl:380-384
-            float px = q[F_PA * FFB_MAXX] * ax + q[F_PB * FFB_MAXX] * ay + q[F_PE * FFB_MAXX];
-            float py = q[F_PC * FFB_MAXX] * ax + q[F_PD * FFB_MAXX] * ay + q[F_PF * FFB_MAXX];
-            ax = px; ay = py;
-        }
-#endif
-        if (!(fabsf(ax) <= 1e32f) || !(fabsf(ay) <= 1e32f)) {                  // main_template.wgsl:449-479
-#if FFB_RNG_MODE == 1
-            uint4 o = philox4(J.seed_lo, J.seed_hi, gw, (u32)it, 0xFFFFFFFFu, (u32)(it >> 32));
-            x = u24(o.x) * 2.0f - 1.0f;
-            y = u24(o.y) * 2.0f - 1.0f;
-#else
-            x = rng.draw(0) * 2.0f - 1.0f;
-            y = rng.draw(0) * 2.0f - 1.0f;
-#endif
-            fuse = J.burn_in;
-            continue;
-        }
-        x = ax; y = ay;
-        ci = ci * q[F_C1 * FFB_MAXX] + q[F_C2 * FFB_MAXX];                       // main_template.wgsl:496-508
-        if (fuse > 0u) { fuse -= 1u; continue; }                               // main_template.wgsl:510-514
-        float fx = x, fy = y;
-        ffb_finals(sm, fx, fy, rng);                                            // main_template.wgsl:663-717
-        const float4 c = pal[ffb_palette_index(ci, J.pal_n)];                   // main_template.wgsl:766-772
-        // world_to_pixel (utilities.wgsl:417-450).
-        float tx = fx - J.pan_x, ty = fy - J.pan_y;
-        float rx = tx * J.cos_r - ty * J.sin_r;
-        float ry = tx * J.sin_r + ty * J.cos_r;
-        rx = rx * J.zoom; ry = ry * J.zoom;
-        const float pxf = floorf(cx + rx * scale), pyf = floorf(cy + ry * scale);
-        if (plot && pxf >= 0.0f && pyf >= 0.0f && pxf < (float)J.width && pyf < (float)J.height) {
-            const u32 idx = (u32)pyf * (u32)J.width + (u32)pxf;
-            ffb_splat(J.hist, idx, c);
-            ++inframe;
-        }
+        ffb_step(sm, pal, J, k, plot, rng, gw, it, x, y, ci, fuse, cx, cy, scale, inframe);
     }
     J.walkers[w] = make_float4(x, y, ci, __uint_as_float(fuse));
-    // In-frame splat count (count conservation: sum of the count plane).
-    // Lanes past n_walkers have returned, so reduce over the live ones.
-    const unsigned live = __activemask();
-    const u32 tot = __reduce_add_sync(live, inframe);
-    if ((threadIdx.x & 31) == (unsigned)(__ffs(live) - 1) && tot) atomicAdd(J.counters, (u64)tot);
+    ffb_count_inframe(J, inframe);
+}
+
+// Transform-coherent scheduling.  A thread holds a walker only for one
+// iteration: after each walker picks its transform, the block regroups the
+// walkers by transform (a counting sort through shared memory, the state
+// travelling with the walker's id), so a warp runs mostly one transform and
+// the variation branches of ffb_normal are warp-uniform.  Every walker still
+// draws from its own counter-based stream, keyed by its id, so the orbits
+// are bit-identical to ffb_chaos's; only which thread carries them changes.
+extern "C" __global__ void __launch_bounds__(1024, 1)
+ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
+    extern __shared__ float4 ffb_smem4[];
+    float* sm = reinterpret_cast<float*>(ffb_smem4);
+    float4* pal;
+    const ffb_launch& J = ffb_stage(jobs, n_jobs, sm, pal);
+    const int P = blockDim.x, tid = threadIdx.x, lane = tid & 31;
+    float* s_x = reinterpret_cast<float*>(pal + J.pal_n);
+    float* s_y = s_x + P;
+    float* s_ci = s_y + P;
+    u32* s_fuse = reinterpret_cast<u32*>(s_ci + P);
+    u32* s_kp = s_fuse + P;                     // k | plot << 31
+    u32* s_wid = s_kp + P;
+    u32* s_r0 = s_wid + P;                      // philox words 2, 3 / pcg state, inc
+    u32* s_r1 = s_r0 + P;
+    u32* s_cnt = s_r1 + P;                      // [2][FFB_MAXX + 1], ping-pong by iteration
+    const int NC = FFB_MAXX + 1;
+    for (int i = tid; i < 2 * NC; i += P) s_cnt[i] = 0u;
+    const u32 w0 = (blockIdx.x - J.block0) * P + tid;
+    bool active = w0 < J.n_walkers;
+    u32 wid = J.walker0 + w0;
+    float x = 0.f, y = 0.f, ci = 0.f;
+    u32 fuse = 0;
+    if (active) ffb_start(J, w0, wid, x, y, ci, fuse);
+    const int n_xf = (int)J.n_xf;
+    const float scale = (float)min(J.width, J.height) * 0.25f;
+    const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
+    u32 inframe = 0;
+#if FFB_RNG_MODE == 0
+    PcgRng rng;
+    rng.state = 0; rng.inc = 1;
+#endif
+    __syncthreads();
+    const u64 it1 = J.it0 + J.n_iters;
+    int par = 0;
+    for (u64 it = J.it0; it < it1; ++it, par ^= 1) {
+        u32* cnt = s_cnt + par * NC;
+        int k = FFB_MAXX;                        // inactive threads sort last
+        bool plot = false;
+        u32 r0 = 0, r1 = 0;
+        if (active) {
+#if FFB_RNG_MODE == 0
+            ffb_pcg_dispatch(J, rng, wid, it, x, y);
+            k = ffb_select(sm, n_xf, rng.draw(0));
+            plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];
+            r0 = rng.state; r1 = rng.inc;
+#else
+            PhiloxRng rng;
+            rng.fill(J.seed_lo, J.seed_hi, wid, it);
+            k = ffb_select(sm, n_xf, rng.draw(0));
+            plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];
+            r0 = __float_as_uint(rng.w[2]); r1 = __float_as_uint(rng.w[3]);
+#endif
+        }
+        // Counting sort by transform: warp-aggregated counts, then each
+        // walker's slot = (walkers of lower transforms) + its rank.
+        const unsigned grp = __match_any_sync(0xffffffffu, k);
+        const int leader = __ffs(grp) - 1;
+        const u32 rank = __popc(grp & ((1u << lane) - 1u));
+        u32 base = 0;
+        if (lane == leader) base = atomicAdd(&cnt[k], (u32)__popc(grp));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        u32* nxt = s_cnt + (par ^ 1) * NC;
+        __syncthreads();                                                        // counts complete
+        for (int i = tid; i < NC; i += P) nxt[i] = 0u;                          // next iteration's counters
+        u32 off = 0;
+#pragma unroll 4
+        for (int j = 0; j < k; ++j) off += cnt[j];
+        const u32 slot = off + base + rank;
+        s_x[slot] = x; s_y[slot] = y; s_ci[slot] = ci; s_fuse[slot] = fuse;
+        s_kp[slot] = (u32)k | (plot ? 0x80000000u : 0u);
+        s_wid[slot] = wid; s_r0[slot] = r0; s_r1[slot] = r1;
+        __syncthreads();                                                        // states regrouped
+        x = s_x[tid]; y = s_y[tid]; ci = s_ci[tid]; fuse = s_fuse[tid];
+        const u32 kp = s_kp[tid];
+        k = (int)(kp & 0x7FFFFFFFu);
+        plot = (kp >> 31) != 0u;
+        wid = s_wid[tid];
+        active = k < FFB_MAXX;
+        if (active) {
+#if FFB_RNG_MODE == 0
+            rng.state = s_r0[tid]; rng.inc = s_r1[tid];
+            ffb_step(sm, pal, J, k, plot, rng, wid, it, x, y, ci, fuse, cx, cy, scale, inframe);
+#else
+            PhiloxRng rng;
+            rng.w[2] = __uint_as_float(s_r0[tid]);
+            rng.w[3] = __uint_as_float(s_r1[tid]);
+            rng.fill_from(1, J.seed_lo, J.seed_hi, wid, it);
+            ffb_step(sm, pal, J, k, plot, rng, wid, it, x, y, ci, fuse, cx, cy, scale, inframe);
+#endif
+        }
+    }
+    if (active) J.walkers[wid - J.walker0] = make_float4(x, y, ci, __uint_as_float(fuse));
+    ffb_count_inframe(J, inframe);
 }
 
 // The variation probe (main_template.wgsl:1467-1567): transform xi's

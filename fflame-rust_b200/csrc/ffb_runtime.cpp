@@ -102,8 +102,8 @@ struct DevBuf {
 struct Module {
     std::string key;
     cudaLibrary_t lib = nullptr;
-    cudaKernel_t chaos = nullptr, probe = nullptr, apply = nullptr;
-    int smem_attr = 0;
+    cudaKernel_t chaos = nullptr, chaos_sorted = nullptr, probe = nullptr, apply = nullptr;
+    int smem_attr = 0, smem_attr_sorted = 0;
 };
 
 std::string nvrtc_options_key() { return "sm_100a|c++17|ftz|prec-div|prec-sqrt|nofmad"; }
@@ -115,6 +115,7 @@ using namespace ffb;
 
 struct ffb_renderer {
     int device = 0;
+    int n_sm = 148;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
@@ -154,6 +155,7 @@ struct ffb_renderer {
         std::vector<char> cubin = nvrtc_cubin(src);
         ck(cudaLibraryLoadData(&m.lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0), "cudaLibraryLoadData");
         ck(cudaLibraryGetKernel(&m.chaos, m.lib, "ffb_chaos"), "cudaLibraryGetKernel(ffb_chaos)");
+        ck(cudaLibraryGetKernel(&m.chaos_sorted, m.lib, "ffb_chaos_sorted"), "cudaLibraryGetKernel(ffb_chaos_sorted)");
         ck(cudaLibraryGetKernel(&m.probe, m.lib, "ffb_probe"), "cudaLibraryGetKernel(ffb_probe)");
         ck(cudaLibraryGetKernel(&m.apply, m.lib, "ffb_apply_points"), "cudaLibraryGetKernel(ffb_apply_points)");
     }
@@ -196,6 +198,7 @@ struct Prepared {
     uint32_t ss = 1, wi = 0, hi = 0, walkers = 0, burn_in = 20, ipt = 1024, threads = 128;
     uint64_t target = 0, per_walker = 0, seed = 0;
     int rng = RNG_PHILOX, math = MATH_PRECISE;
+    uint32_t schedule = 0;
 };
 
 Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_size = true) {
@@ -235,6 +238,8 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
         if (P.per_walker + P.burn_in > (uint64_t)P.ipt * 0xFFFFFFFFull) fail(FFB_ERR_INVALID, "budget too large for the pcg stream");
     }
     P.seed = job->seed ? job->seed : P.flame.seed;
+    P.schedule = job->schedule;
+    if (P.schedule > 2) fail(FFB_ERR_INVALID, "schedule must be 0 (auto), 1 (plain) or 2 (sorted)");
     P.plan = make_plan(P.flame, P.rng, P.math, 0, (int)P.threads);
     P.table = make_table(P.plan, P.flame);
     P.palette = palette_table(P.flame);
@@ -304,7 +309,7 @@ std::vector<float> de_table(double r_max, double r_min, double curve, int& n_out
         t.push_back((float)dmax2);
         t.push_back(h2 > 0 ? (float)(1.0 / h2) : 0.0f);
         t.push_back((float)(1.0 / norm));
-        t.push_back(0.0f);
+        t.push_back((float)rr);                        // the disc's reach in whole pixels
         // Past this count every larger one has the same disc and weights.
         if (c >= 1 && (h < 1.0 || h <= r_min)) break;
         if (c > 10000000) fail(FFB_ERR_INVALID, "density estimation table too large");
@@ -314,7 +319,7 @@ std::vector<float> de_table(double r_max, double r_min, double curve, int& n_out
 }
 
 void check_de(const Flame& f, uint32_t ss) {
-    if (f.de.max_radius * ss > 40.0f) fail(FFB_ERR_INVALID, "density estimation radius too large");
+    if (f.de.max_radius * ss > 36.0f) fail(FFB_ERR_INVALID, "density estimation radius too large (at most 36 histogram pixels)");
 }
 
 // Chaos game of a prepared flame into r->hist (wi*hi float4, cleared here).
@@ -333,15 +338,26 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     uint64_t* d_cnt = (uint64_t*)r->counters.ensure(64);
     ck(cudaMemsetAsync(d_cnt, 0, 64, s), "clear counters");
     const uint32_t pal_n = (uint32_t)(P.palette.size() / 4);
-    const int smem = ((P.plan.table_size + 3) / 4) * 16 + (int)pal_n * 16;
-    if (smem > 48 * 1024 && m.smem_attr < smem) {
-        ck(cudaFuncSetAttribute((const void*)m.chaos, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
-        m.smem_attr = smem;
+    const bool sorted = P.schedule != 1;
+    // Sorted schedule: about one block a multiprocessor holding its share
+    // of the walkers (the regrouping works within a block).
+    uint32_t threads = P.threads;
+    if (sorted) {
+        uint32_t per_sm = (P.walkers + (uint32_t)r->n_sm - 1) / (uint32_t)r->n_sm;
+        threads = std::min<uint32_t>(1024, std::max<uint32_t>(64, (per_sm + 31) / 32 * 32));
+    }
+    int smem = ((P.plan.table_size + 3) / 4) * 16 + (int)pal_n * 16;
+    if (sorted) smem += (int)threads * 8 * 4 + 2 * (P.plan.maxx + 1) * 4;
+    const void* kfn = sorted ? (const void*)m.chaos_sorted : (const void*)m.chaos;
+    int& attr = sorted ? m.smem_attr_sorted : m.smem_attr;
+    if (smem > 48 * 1024 && attr < smem) {
+        ck(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
+        attr = smem;
     }
     const uint64_t total_iters = P.per_walker + P.burn_in;
     uint64_t chunk = 1ull << 16;
     if (P.rng == RNG_PCG) chunk = std::max<uint64_t>(1, chunk / P.ipt) * P.ipt;
-    const uint32_t blocks = (P.walkers + P.threads - 1) / P.threads;
+    const uint32_t blocks = (P.walkers + threads - 1) / threads;
     const double rot = P.flame.rotation;
     Launch L{};
     L.table = d_table; L.palette = d_pal; L.hist = hist; L.walkers = d_walk; L.counters = d_cnt;
@@ -364,7 +380,7 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         Launch* jp = d_jobs + i;
         int nj = 1;
         void* args[] = {&jp, &nj};
-        ck(cudaLaunchKernel((const void*)m.chaos, dim3(blocks), dim3(P.threads), args, (size_t)smem, s), "launch ffb_chaos");
+        ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch ffb_chaos");
         r->launches += 1;
     }
     if (inframe_out) {
@@ -527,6 +543,7 @@ FFB_API int ffb_renderer_create(int device, ffb_renderer** out) {
         auto r = std::make_unique<ffb_renderer>();
         r->device = device;
         r->begin();
+        ck(cudaDeviceGetAttribute(&r->n_sm, cudaDevAttrMultiProcessorCount, device), "device attribute");
         ck(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaEventCreate(&r->ev0), "cudaEventCreate");
         ck(cudaEventCreate(&r->ev1), "cudaEventCreate");
@@ -631,7 +648,7 @@ FFB_API int ffb_density_estimate(ffb_renderer* r, const uint32_t* counts, const 
                                  float max_radius, float min_radius, float curve, float* out_counts, float* out_rgb) {
     return guard([&] {
         if (!r || !counts || !rgb || !out_counts || !out_rgb) fail(FFB_ERR_INVALID, "NULL argument");
-        if (max_radius <= 0.f || max_radius > 40.f || min_radius < 0.f || curve < 0.f) fail(FFB_ERR_INVALID, "bad DE parameters");
+        if (max_radius <= 0.f || max_radius > 36.f || min_radius < 0.f || curve < 0.f) fail(FFB_ERR_INVALID, "bad DE parameters");
         std::lock_guard<std::mutex> lk(r->mu);
         r->begin();
         const size_t npx = (size_t)w * h;

@@ -20,134 +20,144 @@ namespace {
 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
-__device__ __forceinline__ float3 rgb_to_hsv(float3 c) {                 // tonemap.wgsl:152-184
-    float mx = fmaxf(fmaxf(c.x, c.y), c.z), mn = fminf(fminf(c.x, c.y), c.z), d = mx - mn;
-    float h = 0.f, s = 0.f;
-    if (d > 0.00001f) {
+struct D3 { double x, y, z; };
+__device__ __forceinline__ double clampd(double v, double lo, double hi) { return fmin(fmax(v, lo), hi); }
+
+__device__ __forceinline__ D3 rgb_to_hsv(D3 c) {                         // tonemap.wgsl:152-184
+    double mx = fmax(fmax(c.x, c.y), c.z), mn = fmin(fmin(c.x, c.y), c.z), d = mx - mn;
+    double h = 0.0, s = 0.0;
+    if (d > 0.00001) {
         s = d / mx;
-        if (c.x >= mx) h = (c.y - c.z) / d; else if (c.y >= mx) h = 2.0f + (c.z - c.x) / d; else h = 4.0f + (c.x - c.y) / d;
-        h *= 60.0f; if (h < 0.f) h += 360.0f;
+        if (c.x >= mx) h = (c.y - c.z) / d; else if (c.y >= mx) h = 2.0 + (c.z - c.x) / d; else h = 4.0 + (c.x - c.y) / d;
+        h *= 60.0; if (h < 0.0) h += 360.0;
     }
-    return make_float3(h, s, mx);
+    return {h, s, mx};
 }
-__device__ __forceinline__ float3 hsv_to_rgb(float3 c) {                 // tonemap.wgsl:187-220
-    float h = c.x, s = c.y, v = c.z;
-    if (s <= 0.f) return make_float3(v, v, v);
-    float hh = h >= 360.0f ? 0.0f : h;
-    hh /= 60.0f;
+__device__ __forceinline__ D3 hsv_to_rgb(D3 c) {                         // tonemap.wgsl:187-220
+    double h = c.x, s = c.y, v = c.z;
+    if (s <= 0.0) return {v, v, v};
+    double hh = h >= 360.0 ? 0.0 : h;
+    hh /= 60.0;
     unsigned i = (unsigned)hh;
-    float ff = hh - (float)i;
-    float p = v * (1.f - s), q = v * (1.f - s * ff), t = v * (1.f - s * (1.f - ff));
-    switch (i) { case 0: return make_float3(v, t, p); case 1: return make_float3(q, v, p); case 2: return make_float3(p, v, t);
-                 case 3: return make_float3(p, q, v); case 4: return make_float3(t, p, v); default: return make_float3(v, p, q); }
+    double ff = hh - (double)i;
+    double p = v * (1.0 - s), q = v * (1.0 - s * ff), t = v * (1.0 - s * (1.0 - ff));
+    switch (i) { case 0: return {v, t, p}; case 1: return {q, v, p}; case 2: return {p, v, t};
+                 case 3: return {p, q, v}; case 4: return {t, p, v}; default: return {v, p, q}; }
 }
-__device__ __forceinline__ float curve_sample(const float* lut, float x) {
+__device__ __forceinline__ double curve_sample(const float* lut, double x) {
     // Linear filter, clamp-to-edge, read at u = (255x + 0.5)/256 (tonemap.wgsl:478-485).
-    float t = clampf(x * 255.0f, 0.0f, 255.0f);
-    int i0 = (int)floorf(t);
+    double t = clampd(x * 255.0, 0.0, 255.0);
+    int i0 = (int)floor(t);
     int i1 = min(i0 + 1, 255);
-    float fr = t - (float)i0;
-    return lut[i0] * (1.0f - fr) + lut[i1] * fr;
+    double fr = t - (double)i0;
+    return (double)lut[i0] * (1.0 - fr) + (double)lut[i1] * fr;
 }
-__device__ __forceinline__ float smooth(float e0, float e1, float x) {
-    float t = clampf((x - e0) / (e1 - e0), 0.f, 1.f);
-    return t * t * (3.f - 2.f * t);
+__device__ __forceinline__ double smooth(double e0, double e1, double x) {
+    double t = clampd((x - e0) / (e1 - e0), 0.0, 1.0);
+    return t * t * (3.0 - 2.0 * t);
 }
 
 // One pixel of the tone map: cnt = hits, sum = colour sums.  Returns the
-// RGBA before quantisation.
-__device__ float4 tonemap_px(const TonemapArgs& A, const float* lut, float cnt, float3 sum) {
-    float3 mean = make_float3(0.f, 0.f, 0.f);
-    if (cnt > 0.f) {                                                     // accumulate.wgsl:205-210
-        mean = make_float3(clampf(sum.x / cnt, 0.f, 1.f), clampf(sum.y / cnt, 0.f, 1.f), clampf(sum.z / cnt, 0.f, 1.f));
-    }
-    const float bucket = cnt * 100.0f;                                   // tonemap.wgsl:252
-    float3 color;
-    float alpha = 0.f;
-    const float g = A.inv_gamma;
+// RGBA before quantisation.  Computed in FP64: the pass is bound by HBM
+// (16 bytes in, 4 out a pixel), so the double arithmetic is free, and the
+// ill-conditioned corners (HSV near grey, the gamma threshold blend) keep
+// the result within 1e-5 of an exact evaluation.
+__device__ D3 tonemap_rgb(const TonemapArgs& A, const float* lut, double cnt, D3 sum, double& fa_out) {
+    D3 mean{0.0, 0.0, 0.0};
+    if (cnt > 0.0) mean = {clampd(sum.x / cnt, 0.0, 1.0), clampd(sum.y / cnt, 0.0, 1.0), clampd(sum.z / cnt, 0.0, 1.0)};   // accumulate.wgsl:205-210
+    const double bucket = cnt * 100.0;                                   // tonemap.wgsl:252
+    D3 color;
+    double alpha = 0.0;
+    const double g = A.inv_gamma;
     if (A.mode == 0) {
-        color = make_float3(powf(mean.x * A.exposure, g), powf(mean.y * A.exposure, g), powf(mean.z * A.exposure, g));
-        alpha = clampf(bucket * 0.01f * A.density_scale, 0.f, 1.f);
+        color = {pow(mean.x * A.exposure, g), pow(mean.y * A.exposure, g), pow(mean.z * A.exposure, g)};
+        alpha = clampd(bucket * 0.01 * A.density_scale, 0.0, 1.0);
     } else if (A.mode == 2) {
-        float nd = clampf(bucket * 0.01f * A.exposure, 0.f, 1.f);
-        float gd = powf(nd, g);
-        color = make_float3(gd, gd, gd);
+        double nd = clampd(bucket * 0.01 * A.exposure, 0.0, 1.0);
+        double gd = pow(nd, g);
+        color = {gd, gd, gd};
         alpha = nd;
     } else {
         // brightness_scale (tonemap.wgsl:94-112), log10(1+x) through log1p.
-        float ls = 0.f;
-        if (!(bucket < 0.001f)) ls = A.ls_a * log1pf(A.ls_b * bucket) / (A.white_level * bucket);
-        const float fp0 = ls * (mean.x * bucket), fp1 = ls * (mean.y * bucket), fp2 = ls * (mean.z * bucket);
-        const float fp3 = ls * bucket * A.white_level;
-        if (fp3 > 0.f) {
+        double ls = 0.0;
+        if (!(bucket < 0.001)) ls = A.ls_a * log1p(A.ls_b * bucket) / (A.white_level * bucket);
+        const double fp0 = ls * (mean.x * bucket), fp1 = ls * (mean.y * bucket), fp2 = ls * (mean.z * bucket);
+        const double fp3 = ls * bucket * A.white_level;
+        if (fp3 > 0.0) {
             if (fp3 <= A.gamma_threshold) {
-                float fr = fp3 / A.gamma_threshold;
-                alpha = (1.f - fr) * fp3 * A.funcval + fr * powf(fp3, g);
-            } else alpha = powf(fp3, g);
+                double fr = fp3 / A.gamma_threshold;
+                alpha = (1.0 - fr) * fp3 * A.funcval + fr * pow(fp3, g);
+            } else alpha = pow(fp3, g);
         }
-        const float l2 = fp3 > 0.f ? A.vib * alpha / fp3 : 0.f;
-        if (A.notvib > 0.f)
-            color = make_float3(l2 * fp0 + A.notvib * powf(fp0, g), l2 * fp1 + A.notvib * powf(fp1, g), l2 * fp2 + A.notvib * powf(fp2, g));
+        const double l2 = fp3 > 0.0 ? A.vib * alpha / fp3 : 0.0;
+        if (A.notvib > 0.0)
+            color = {l2 * fp0 + A.notvib * pow(fp0, g), l2 * fp1 + A.notvib * pow(fp1, g), l2 * fp2 + A.notvib * pow(fp2, g)};
         else
-            color = make_float3(l2 * fp0, l2 * fp1, l2 * fp2);
+            color = {l2 * fp0, l2 * fp1, l2 * fp2};
     }
-    if (A.saturation != 1.0f || A.hue_shift != 0.0f) {                   // tonemap.wgsl:371-401
-        float3 h = rgb_to_hsv(color);
-        if (A.hue_shift != 0.0f) { h.x += A.hue_shift; if (h.x < 0.f) h.x += 360.f; else if (h.x >= 360.f) h.x -= 360.f; }
-        if (A.saturation != 1.0f) h.y = clampf(h.y * A.saturation, 0.f, 1.f);
+    if (A.saturation != 1.0 || A.hue_shift != 0.0) {                     // tonemap.wgsl:371-401
+        D3 h = rgb_to_hsv(color);
+        if (A.hue_shift != 0.0) { h.x += A.hue_shift; if (h.x < 0.0) h.x += 360.0; else if (h.x >= 360.0) h.x -= 360.0; }
+        if (A.saturation != 1.0) h.y = clampd(h.y * A.saturation, 0.0, 1.0);
         color = hsv_to_rgb(h);
     }
     if (A.mode == 1) { color.x *= A.exposure; color.y *= A.exposure; color.z *= A.exposure; }
-    color = make_float3(fmaxf(color.x, 0.f), fmaxf(color.y, 0.f), fmaxf(color.z, 0.f));
+    color = {fmax(color.x, 0.0), fmax(color.y, 0.0), fmax(color.z, 0.0)};
     if (A.highlight == 1) {                                              // tonemap.wgsl:414-477
-        float m = fmaxf(color.x, fmaxf(color.y, color.z));
-        if (m > 1.f) color = make_float3(color.x / m, color.y / m, color.z / m);
+        double m = fmax(color.x, fmax(color.y, color.z));
+        if (m > 1.0) color = {color.x / m, color.y / m, color.z / m};
     } else if (A.highlight == 2) {
-        float lum = 0.2126f * color.x + 0.7152f * color.y + 0.0722f * color.z;
-        if (lum > 1e-6f) { float s = (lum / (1.f + lum)) / lum; color = make_float3(color.x * s, color.y * s, color.z * s); }
-        color = make_float3(fminf(color.x, 1.f), fminf(color.y, 1.f), fminf(color.z, 1.f));
+        double lum = 0.2126 * color.x + 0.7152 * color.y + 0.0722 * color.z;
+        if (lum > 1e-6) { double s = (lum / (1.0 + lum)) / lum; color = {color.x * s, color.y * s, color.z * s}; }
+        color = {fmin(color.x, 1.0), fmin(color.y, 1.0), fmin(color.z, 1.0)};
     } else if (A.highlight == 3) {
-        auto aces = [](float x) { return clampf((x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f), 0.f, 1.f); };
-        color = make_float3(aces(color.x), aces(color.y), aces(color.z));
+        auto aces = [](double x) { return clampd((x * (2.51 * x + 0.03)) / (x * (2.43 * x + 0.59) + 0.14), 0.0, 1.0); };
+        color = {aces(color.x), aces(color.y), aces(color.z)};
     } else {
-        color = make_float3(fminf(color.x, 1.f), fminf(color.y, 1.f), fminf(color.z, 1.f));
+        color = {fmin(color.x, 1.0), fmin(color.y, 1.0), fmin(color.z, 1.0)};
     }
-    float3 fc = color;
-    if (A.use_curve && bucket > 0.001f)                                  // tonemap.wgsl:486-493
-        fc = make_float3(curve_sample(lut, color.x), curve_sample(lut, color.y), curve_sample(lut, color.z));
-    float lev = 1.f;                                                     // apply_levels, tonemap.wgsl:124-149
-    if (A.levels_density > 0.f) {
-        float nd = cnt / A.levels_density;
-        if (A.levels_high <= A.levels_low) lev = nd > A.levels_low ? 1.f : 0.f;
+    D3 fc = color;
+    if (A.use_curve && bucket > 0.001)                                   // tonemap.wgsl:486-493
+        fc = {curve_sample(lut, color.x), curve_sample(lut, color.y), curve_sample(lut, color.z)};
+    double lev = 1.0;                                                    // apply_levels, tonemap.wgsl:124-149
+    if (A.levels_density > 0.0) {
+        double nd = cnt / (double)A.levels_density;
+        if (A.levels_high <= A.levels_low) lev = nd > A.levels_low ? 1.0 : 0.0;
         else {
-            float cl = clampf((nd - A.levels_low) / (A.levels_high - A.levels_low), 0.f, 1.f);
-            lev = (A.levels_gamma != 1.0f && A.levels_gamma > 0.f) ? powf(cl, A.levels_gamma) : cl;
+            double cl = clampd((nd - A.levels_low) / ((double)A.levels_high - A.levels_low), 0.0, 1.0);
+            lev = (A.levels_gamma != 1.0f && A.levels_gamma > 0.0f) ? pow(cl, (double)A.levels_gamma) : cl;
         }
     }
-    const float lin_a = clampf(bucket * 0.01f * A.density_scale, 0.f, 1.f);   // tonemap.wgsl:514-529
-    const float gam_a = clampf(alpha, 0.f, 1.f);
-    const float bt = smooth(A.alpha_blend_low, A.alpha_blend_high, gam_a);
-    const float base_a = gam_a + (lin_a - gam_a) * bt;
-    const float fa = A.levels_enabled ? fminf(base_a, lev) : base_a;
-    const float inv22 = 1.0f / 2.2f;
+    const double lin_a = clampd(bucket * 0.01 * A.density_scale, 0.0, 1.0);   // tonemap.wgsl:514-529
+    const double gam_a = clampd(alpha, 0.0, 1.0);
+    const double bt = smooth(A.alpha_blend_low, A.alpha_blend_high, gam_a);
+    const double base_a = gam_a + (lin_a - gam_a) * bt;
+    fa_out = A.levels_enabled ? fmin(base_a, lev) : base_a;
+    return fc;
+}
+
+__device__ double4 tonemap_px(const TonemapArgs& A, const float* lut, double cnt, D3 sum) {
+    double fa;
+    const D3 fc = tonemap_rgb(A, lut, cnt, sum, fa);
+    const double inv22 = 1.0 / 2.2;
     if (A.transparent != 0) {                                            // tonemap.wgsl:531-577
-        float3 os = make_float3(powf(fmaxf(fc.x * fa, 0.f), inv22), powf(fmaxf(fc.y * fa, 0.f), inv22), powf(fmaxf(fc.z * fa, 0.f), inv22));
-        if (A.transparent == 2) return make_float4(os.x, os.y, os.z, fa);
-        float cov = fmaxf(os.x, fmaxf(os.y, os.z));
-        if (cov > 0.f) return make_float4(os.x / cov, os.y / cov, os.z / cov, cov);
-        return make_float4(0.f, 0.f, 0.f, cov);
+        D3 os = {pow(fmax(fc.x * fa, 0.0), inv22), pow(fmax(fc.y * fa, 0.0), inv22), pow(fmax(fc.z * fa, 0.0), inv22)};
+        if (A.transparent == 2) return make_double4(os.x, os.y, os.z, fa);
+        double cov = fmax(os.x, fmax(os.y, os.z));
+        if (cov > 0.0) return make_double4(os.x / cov, os.y / cov, os.z / cov, cov);
+        return make_double4(0.0, 0.0, 0.0, cov);
     }
-    float3 f = make_float3(A.bg_lin[0] * (1.f - fa) + fc.x * fa, A.bg_lin[1] * (1.f - fa) + fc.y * fa, A.bg_lin[2] * (1.f - fa) + fc.z * fa);
-    return make_float4(powf(f.x, inv22), powf(f.y, inv22), powf(f.z, inv22), 1.0f);   // tonemap.wgsl:582-589
+    D3 f = {A.bg_lin[0] * (1.0 - fa) + fc.x * fa, A.bg_lin[1] * (1.0 - fa) + fc.y * fa, A.bg_lin[2] * (1.0 - fa) + fc.z * fa};
+    return make_double4(pow(f.x, inv22), pow(f.y, inv22), pow(f.z, inv22), 1.0);   // tonemap.wgsl:582-589
 }
 
-__device__ __forceinline__ float hist_count(const float4& v, int count_is_float) {
-    return count_is_float ? v.w : (float)__float_as_uint(v.w);
+__device__ __forceinline__ double hist_count(const float4& v, int count_is_float) {
+    return count_is_float ? (double)v.w : (double)__float_as_uint(v.w);
 }
 
-__device__ __forceinline__ uchar4 quantise(float4 o) {
-    return make_uchar4((unsigned char)rintf(clampf(o.x, 0.f, 1.f) * 255.f), (unsigned char)rintf(clampf(o.y, 0.f, 1.f) * 255.f),
-                       (unsigned char)rintf(clampf(o.z, 0.f, 1.f) * 255.f), (unsigned char)rintf(clampf(o.w, 0.f, 1.f) * 255.f));
+__device__ __forceinline__ uchar4 quantise(double4 o) {
+    return make_uchar4((unsigned char)rint(clampd(o.x, 0.0, 1.0) * 255.0), (unsigned char)rint(clampd(o.y, 0.0, 1.0) * 255.0),
+                       (unsigned char)rint(clampd(o.z, 0.0, 1.0) * 255.0), (unsigned char)rint(clampd(o.w, 0.0, 1.0) * 255.0));
 }
 
 __global__ void __launch_bounds__(256) k_tonemap1(const float4* __restrict__ hist, int n, TonemapArgs A, const float* __restrict__ lut_g,
@@ -158,9 +168,9 @@ __global__ void __launch_bounds__(256) k_tonemap1(const float4* __restrict__ his
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 v = hist[i];
-    const float4 o = tonemap_px(A, lut, hist_count(v, A.count_is_float), make_float3(v.x, v.y, v.z));
+    const double4 o = tonemap_px(A, lut, hist_count(v, A.count_is_float), D3{v.x, v.y, v.z});
     out[i] = quantise(o);
-    if (out_f) out_f[i] = o;
+    if (out_f) out_f[i] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)o.w);
 }
 
 // 2x: tone map the four internal pixels of an output pixel, quantise each
@@ -178,7 +188,7 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float4 v = hist[(size_t)(oy * 2 + dy[k]) * wi + (ox * 2 + dx[k])];
-        const uchar4 q = quantise(tonemap_px(A, lut, hist_count(v, A.count_is_float), make_float3(v.x, v.y, v.z)));
+        const uchar4 q = quantise(tonemap_px(A, lut, hist_count(v, A.count_is_float), D3{v.x, v.y, v.z}));
         s[k][0] = q.x; s[k][1] = q.y; s[k][2] = q.z; s[k][3] = q.w;
         lum[k] = s[k][0] + 2.0f * s[k][1] + s[k][2];
     }
@@ -204,38 +214,58 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
 }
 
 // Density estimation, gather form: output pixel p sums, over sources q in
-// the (2R+1)^2 window, w(|p-q|, count_q) * (rgb_q, count_q).  The source
-// window is staged in shared memory per 32x8 tile.
-constexpr int DE_TX = 32, DE_TY = 8;
+// the (2R+1)^2 window, w(|p-q|, count_q) * (rgb_q, count_q).  Each block
+// stages its 32x16 tile's source window in shared memory once, with every
+// source's table entry resolved (its accepted d^2, 4.5/h^2, and its values
+// premultiplied by the normaliser), so a neighbour outside its disc costs
+// one 8-byte shared load and a compare; and the window shrinks to the
+// largest radius any staged source actually has (dense regions, where
+// every count is high, gather over a few pixels only).
+constexpr int DE_TX = 32, DE_TY = 16;
 __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, int w, int h, const float4* __restrict__ tab,
                                                            int tab_n, int R, float4* __restrict__ out) {
-    extern __shared__ float4 tile[];                                     // (TX+2R) x (TY+2R) sources
-    const int tw = DE_TX + 2 * R, th = DE_TY + 2 * R;
+    extern __shared__ float4 de_smem[];
+    const int tw = DE_TX + 2 * R, th = DE_TY + 2 * R, n = tw * th;
+    float4* val = de_smem;                                                // (rgb, count) / normaliser
+    float2* par = reinterpret_cast<float2*>(de_smem + n);                 // (accepted d^2, 4.5 / h^2)
+    __shared__ int reach;
+    if (threadIdx.x == 0) reach = 0;
+    __syncthreads();
     const int x0 = blockIdx.x * DE_TX - R, y0 = blockIdx.y * DE_TY - R;
-    for (int i = threadIdx.x; i < tw * th; i += blockDim.x) {
+    int my_reach = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int sx = x0 + i % tw, sy = y0 + i / tw;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 pr = make_float2(-1.0f, 0.0f);                              // empty: never accepted
         if (sx >= 0 && sy >= 0 && sx < w && sy < h) {
             const float4 hv = hist[(size_t)sy * w + sx];
-            v = make_float4(hv.x, hv.y, hv.z, (float)__float_as_uint(hv.w));
+            const unsigned c = __float_as_uint(hv.w);
+            if (c > 0u) {
+                const float4 e = tab[c < (unsigned)(tab_n - 1) ? c : (unsigned)(tab_n - 1)];
+                const float cf = (float)c;
+                v = make_float4(hv.x * e.z, hv.y * e.z, hv.z * e.z, cf * e.z);
+                pr = make_float2(e.x, 4.5f * e.y);
+                my_reach = max(my_reach, (int)e.w);
+            }
         }
-        tile[i] = v;
+        val[i] = v;
+        par[i] = pr;
     }
+    atomicMax(&reach, my_reach);
     __syncthreads();
+    const int rb = min(R, reach);
     const int lx = threadIdx.x % DE_TX, ly = threadIdx.x / DE_TX;
     const int px = blockIdx.x * DE_TX + lx, py = blockIdx.y * DE_TY + ly;
     if (px >= w || py >= h) return;
     float ar = 0.f, ag = 0.f, ab = 0.f, ac = 0.f;
-    for (int dy = -R; dy <= R; ++dy) {
-        const float4* row = tile + (ly + R + dy) * tw + (lx + R);
-        for (int dx = -R; dx <= R; ++dx) {
-            const float4 v = row[dx];
-            if (v.w <= 0.f) continue;
-            const int ci = v.w < (float)(tab_n - 1) ? (int)v.w : tab_n - 1;
-            const float4 e = tab[ci];
+    for (int dy = -rb; dy <= rb; ++dy) {
+        const int row = (ly + R + dy) * tw + (lx + R);
+        for (int dx = -rb; dx <= rb; ++dx) {
+            const float2 pp = par[row + dx];
             const float d2 = (float)(dx * dx + dy * dy);
-            if (d2 > e.x) continue;
-            const float wt = __expf(-4.5f * d2 * e.y) * e.z;
+            if (d2 > pp.x) continue;
+            const float wt = __expf(-pp.y * d2);
+            const float4 v = val[row + dx];
             ar += wt * v.x; ag += wt * v.y; ab += wt * v.z; ac += wt * v.w;
         }
     }
@@ -280,7 +310,7 @@ cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const Ton
 
 cudaError_t launch_density_estimate(const float4* hist, int w, int h, const float4* table, int table_n, int radius,
                                     float4* out, cudaStream_t s) {
-    const size_t smem = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius) * sizeof(float4);
+    const size_t smem = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius) * (sizeof(float4) + sizeof(float2));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

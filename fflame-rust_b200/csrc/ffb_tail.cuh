@@ -36,8 +36,7 @@ cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const Ton
                            uint8_t* out, float4* out_f, cudaStream_t s);
 
 // Density estimation table: entry c (counts 0..n-1, the last entry serving
-// every larger count): (max accepted d^2, 1/h^2, 1/normaliser, unused).
-struct DeTable { int n; int radius; };
+// every larger count): (max accepted d^2, 1/h^2, 1/normaliser, reach).
 cudaError_t launch_density_estimate(const float4* hist, int w, int h, const float4* table, int table_n, int radius,
                                     float4* out, cudaStream_t s);
 

@@ -42,7 +42,7 @@ class Job(ctypes.Structure):
         ("iterations_per_thread", ctypes.c_uint32), ("burn_in", ctypes.c_uint32), ("walkers", ctypes.c_uint32),
         ("supersample", ctypes.c_uint32), ("rng", ctypes.c_int32), ("math", ctypes.c_int32),
         ("transparent", ctypes.c_int32), ("threads", ctypes.c_int32), ("seed", ctypes.c_uint64),
-        ("walker0", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+        ("walker0", ctypes.c_uint32), ("schedule", ctypes.c_uint32),
     ]
 
 
@@ -104,8 +104,11 @@ def _text(config):
     return json.dumps(config).encode()
 
 
+SCHEDULE = {"auto": 0, "plain": 1, "sorted": 2}
+
+
 def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0, walkers=0, supersample=1,
-             rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0):
+             rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0, schedule="auto"):
     j = Job()
     j.width, j.height, j.iterations = width, height, int(iterations or 0)
     j.iterations_per_thread, j.burn_in, j.walkers = iterations_per_thread, burn_in, walkers
@@ -113,6 +116,7 @@ def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0
     j.rng = RNG[rng] if isinstance(rng, str) else rng
     j.math = MATH[math] if isinstance(math, str) else math
     j.transparent, j.threads, j.seed, j.walker0 = int(transparent), threads, int(seed), walker0
+    j.schedule = SCHEDULE[schedule] if isinstance(schedule, str) else schedule
     return j
 
 

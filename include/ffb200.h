@@ -81,7 +81,7 @@ typedef struct {
     int32_t threads;                   /* threads a block (0: 128) */
     uint64_t seed;                     /* 0: the config's (12345 under deterministic_rng) */
     uint32_t walker0;                  /* first walker id of this shard (multi-GPU sharding) */
-    uint32_t reserved;
+    uint32_t schedule;                 /* 0 auto, 1 one walker a thread, 2 transform-sorted (same orbits) */
 } ffb_job;
 
 /* RenderOutput (src/renderer/render.rs:207-218). */

@@ -144,7 +144,9 @@ def palette_table(cfg):
     pal = cfg.get("palette")
     size = int(cfg.get("palette_size", 256))
     if pal is None:
-        pos, col = np.zeros(0, np.float32), np.zeros(0, np.float32)
+        # Palette::fire, the config default (palette.rs:148-174; fractal_config.rs default_palette).
+        pos = np.array([0.0, 0.25, 0.5, 0.75, 1.0], np.float32)
+        col = np.array([0, 0, 0, 0.5, 0, 0, 1.0, 0.3, 0, 1.0, 0.8, 0, 1.0, 1.0, 0.8], np.float32)
     elif "indexed_colors" in pal:
         pos, col = hex_stops(pal["indexed_colors"])
     else:
@@ -219,15 +221,20 @@ class Flame:
             return plotted, inframe.value, None, None
         return plotted, inframe.value, cnt.reshape(self.height, self.width), rgb.reshape(self.height, self.width, 3)
 
-    def apply_xform(self, xi, xs, ys, draws=None, with_affine=True):
+    def apply_xform(self, xi, xs, ys, draws=None, with_affine=True, scales=False):
+        """One step of transform xi; with `scales`, also the magnitude of the
+        terms each output component sums (f64), for cancellation-aware tolerances."""
         xs = np.ascontiguousarray(xs, np.float32)
         ys = np.ascontiguousarray(ys, np.float32)
         n = len(xs)
         d = np.zeros(n * 16, np.float32) if draws is None else np.ascontiguousarray(draws, np.float32)
         xo, yo = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        sx, sy = np.zeros(n, np.float64), np.zeros(n, np.float64)
+        P = ctypes.POINTER(ctypes.c_double)
         lib().of_apply_xform(self.ptr, ctypes.c_int(xi), ctypes.c_int(n), _fp(xs), _fp(ys), _fp(d), _fp(xo), _fp(yo),
-                             ctypes.c_int(1 if with_affine else 0))
-        return xo, yo
+                             ctypes.c_int(1 if with_affine else 0),
+                             sx.ctypes.data_as(P) if scales else None, sy.ctypes.data_as(P) if scales else None)
+        return (xo, yo, sx, sy) if scales else (xo, yo)
 
     def select(self, u):
         return lib().of_select(self.ptr, ctypes.c_float(u))
@@ -256,6 +263,20 @@ def variation(name, xs, ys, draws=None, params=None, f64=False, ftz=True):
     return xo, yo
 
 
+def variation_scale(name, xs, ys, draws=None, params=None):
+    """Per-component magnitude of the terms of one variation (f64)."""
+    xs = np.ascontiguousarray(xs, np.float32)
+    ys = np.ascontiguousarray(ys, np.float32)
+    n = len(xs)
+    prm = np.array(params if params is not None else [d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
+    d = None if draws is None else np.ascontiguousarray(draws, np.float32)
+    sx, sy = np.zeros(n, np.float64), np.zeros(n, np.float64)
+    P = ctypes.POINTER(ctypes.c_double)
+    lib().of_variation_scale(ctypes.c_int(REGISTRY[name]), _fp(prm), ctypes.c_int(n), _fp(xs), _fp(ys),
+                             _fp(d) if d is not None else None, sx.ctypes.data_as(P), sy.ctypes.data_as(P))
+    return sx, sy
+
+
 def probe(name, xform_slot=None, fold_first=None):
     """(classes, digest, raw outputs) as src/probe/ reports them."""
     vid = REGISTRY[name]
@@ -266,6 +287,12 @@ def probe(name, xform_slot=None, fold_first=None):
     out = np.zeros(54, np.float32)
     dig = lib().of_probe(ctypes.c_int(vid), _fp(prm), ctypes.c_int(slot), ctypes.c_int(1 if fold else 0), cls, _fp(out))
     return cls.value.decode(), dig, out
+
+
+def probe_draw(slot, seed=0x9E3779B9):
+    """The first draw of rng_init(slot, seed) as rng_nextf returns it."""
+    st = rng_init(slot, seed)
+    return (rng_next(st) >> 8) * (1.0 / 16777216.0)
 
 
 def probe_digest(vals):

@@ -31,16 +31,29 @@ def ulp_dist(a, b):
     return np.abs(a - b)
 
 
-def close_f32(gpu, ref, scale, ulps=4):
-    """Per component: <= `ulps` ulp, or <= `ulps` ulp of `scale` (the size of
-    the terms a cancellation subtracted)."""
-    gpu, ref = np.asarray(gpu, np.float32), np.asarray(ref, np.float32)
-    same_class = (np.isnan(gpu) == np.isnan(ref)) & (np.isinf(gpu) == np.isinf(ref))
+EXACT = {"linear", "spherical", "horseshoe", "bubble", "curl"}   # no transcendental arithmetic
+ULPS = 4
+EPS = 2.0 ** -23
+
+
+def within(gpu, ref, scale):
+    """<= 4 ulp of the result, or <= 4 ulp of the magnitude of the terms the
+    result was summed from (`scale`, from the oracle): a cancellation's
+    error is a few ulp of its terms.  NaN and infinities must agree."""
+    gpu = np.asarray(gpu, np.float32)
+    ref = np.asarray(ref, np.float32)
     finite = np.isfinite(gpu) & np.isfinite(ref)
-    ok = np.where(finite, ulp_dist(gpu, ref) <= ulps, same_class & ((gpu == ref) | np.isnan(gpu)))
-    tol = ulps * np.spacing(np.maximum(np.abs(scale), 1e-30).astype(np.float32))
-    ok |= finite & (np.abs(gpu.astype(np.float64) - ref) <= tol)
-    return ok
+    same_special = (np.isnan(gpu) & np.isnan(ref)) | (~np.isnan(gpu) & ~np.isnan(ref) & ~finite & (gpu == ref))
+    ok_ulp = ulp_dist(np.where(finite, gpu, 0), np.where(finite, ref, 0)) <= ULPS
+    diff = np.abs(np.where(finite, gpu, 0).astype(np.float64) - np.where(finite, ref, 0))
+    ok_scale = diff <= ULPS * EPS * np.asarray(scale, np.float64)
+    return np.where(finite, ok_ulp | ok_scale, same_special)
+
+
+def bit_equal(gpu, ref):
+    g = np.asarray(gpu, np.float32)
+    r = np.asarray(ref, np.float32)
+    return (g.view(np.uint32) == r.view(np.uint32)) | (np.isnan(g) & np.isnan(r))
 
 
 def one_xform(name, a=(1, 0, 0, 1, 0, 0), params=None):
@@ -67,13 +80,19 @@ def pts(oracle):
 @pytest.mark.parametrize("name", TWELVE)
 def test_probe_matches_oracle(renderer, oracle, pts, name):
     """The variation probe at the 27 inputs: CUDA (precise math) vs the oracle,
-    both at probe slot 0 (RNG rng_init(point, 0x9E3779B9))."""
+    both at probe slot 0 (RNG rng_init(point, 0x9E3779B9)).  Variations with
+    no transcendental arithmetic are bit-identical; the others within 4 ulp
+    (of the terms, where the result cancels)."""
     out = renderer.probe(one_xform(name), pts, 1)[0]
     _, _, ref = oracle.probe(name, xform_slot=0, fold_first=False)
     ref = ref.reshape(27, 2)
-    scale = np.maximum(np.abs(pts).max(axis=1, keepdims=True), np.abs(ref).max(axis=1, keepdims=True))
-    scale = np.broadcast_to(scale, ref.shape)
-    ok = close_f32(out, ref, scale)
+    if name in EXACT:
+        ok = bit_equal(out, ref)
+    else:
+        flushed = np.where(np.abs(pts) < 1.17549435e-38, np.copysign(0.0, pts), pts).astype(np.float32)
+        draws = np.array([oracle.probe_draw(i) for i in range(27)], np.float32)
+        sx, sy = oracle.variation_scale(name, flushed[:, 0], flushed[:, 1], draws if name == "julia" else None)
+        ok = within(out, ref, np.stack([sx, sy], axis=1))
     bad = [(i, pts[i].tolist(), out[i].tolist(), ref[i].tolist()) for i in range(27) if not ok[i].all()]
     assert not bad, f"{name}: {bad}"
 
@@ -110,7 +129,8 @@ def test_probe_sfu_math_reproduces_reference_classes(renderer, oracle, pts):
 def test_apply_points_matches_oracle(renderer, oracle):
     """Single step of every transform of a flame using all twelve variations
     (affine, weighted variation sum, post-affine; finals too) at 4096 random
-    points with random draws: <= 4 ulp."""
+    points with random draws: within 4 ulp (of the terms, where they cancel);
+    a transform of non-transcendental variations only is bit-identical."""
     rng = np.random.default_rng(5)
     t1 = {"a": 0.7, "b": -0.3, "c": 0.4, "d": 0.9, "e": 0.1, "f": -0.2, "weight": 1.0, "color": 0.1,
           "variations": {n: float(rng.uniform(0.1, 1.0)) for n in TWELVE[:6]},
@@ -119,26 +139,27 @@ def test_apply_points_matches_oracle(renderer, oracle):
           "post_affine_enabled": True, "post_a": 0.9, "post_b": 0.1, "post_c": -0.2, "post_d": 1.1, "post_e": 0.05,
           "post_f": 0.0, "variations": {n: float(rng.uniform(0.1, 1.0)) for n in TWELVE[6:]},
           "variation_params": {"curl.c1": 0.4, "curl.c2": -0.3}}
+    t3 = {"a": 0.3, "b": 0.2, "c": -0.6, "d": 0.4, "e": 0.2, "f": 0.1, "weight": 1.0, "color": 0.5,
+          "variations": {n: float(rng.uniform(0.1, 1.0)) for n in sorted(EXACT)},
+          "variation_params": {"curl.c1": 0.3, "curl.c2": 0.1}}
     fin = {"a": 1.0, "b": 0.1, "c": -0.1, "d": 1.0, "e": 0.0, "f": 0.0, "weight": 1.0, "color": 0.0,
            "variations": {"julia": 0.5, "swirl": 0.3, "disc": 0.2}}
-    cfg = {"flame": {"transforms": [t1, t2], "final_transform": fin}}
+    cfg = {"flame": {"transforms": [t1, t2, t3], "final_transform": fin}}
     fl = oracle.Flame(cfg, 64, 64)
     n = 4096
     xs = rng.uniform(-2.5, 2.5, n).astype(np.float32)
     ys = rng.uniform(-2.5, 2.5, n).astype(np.float32)
     words = (rng.integers(0, 1 << 24, (n, 16)) / float(1 << 24)).astype(np.float32)
-    worst = {}
-    for xi in range(3):
+    for xi in range(4):
         for aff in (True, False):
             gx, gy = renderer.apply_points(cfg, xi, xs, ys, words, with_affine=aff)
-            rx, ry = fl.apply_xform(xi, xs, ys, words, with_affine=aff)
-            scale = np.maximum.reduce([np.abs(xs), np.abs(ys), np.abs(rx), np.abs(ry), np.ones(n, np.float32)])
-            okx = close_f32(gx, rx, scale * 4)
-            oky = close_f32(gy, ry, scale * 4)
-            worst[(xi, aff)] = int(max(ulp_dist(gx, rx)[np.isfinite(rx)].max(), ulp_dist(gy, ry)[np.isfinite(ry)].max()))
-            bad = np.where(~(okx & oky))[0]
-            assert len(bad) == 0, (xi, aff, [(xs[i], ys[i], gx[i], rx[i], gy[i], ry[i]) for i in bad[:5]])
-    print("worst ulp per (transform, affine):", worst)
+            rx, ry, sx, sy = fl.apply_xform(xi, xs, ys, words, with_affine=aff, scales=True)
+            if xi == 2:
+                ok = bit_equal(gx, rx) & bit_equal(gy, ry)
+            else:
+                ok = within(gx, rx, sx) & within(gy, ry, sy)
+            bad = np.where(~ok)[0]
+            assert len(bad) == 0, (xi, aff, [(xs[i], ys[i], gx[i], rx[i], gy[i], ry[i], sx[i], sy[i]) for i in bad[:5]])
 
 
 @pytest.mark.parametrize("rng_mode", ["pcg", "philox"])
@@ -154,7 +175,28 @@ def test_histogram_bit_exact_for_a_linear_flame(renderer, oracle, rng_mode):
     assert out.total_iterations == plotted == 2048 * 700
     assert int(cnt.sum()) == out.inframe_samples == inframe
     assert np.array_equal(cnt, rc)
-    np.testing.assert_allclose(rgb, rr, rtol=1e-5, atol=1e-3)
+    # Colour sums: FP32 atomics in any order vs an f64 sum of the same
+    # values: within n * 2^-24 of the sum's magnitude.
+    tol = cnt[..., None].astype(np.float64) * 2.0 ** -24 * np.maximum(rr, 1.0) + 1e-6
+    assert np.all(np.abs(rgb - rr) <= tol)
+
+
+def test_sorted_schedule_walks_the_same_orbits(renderer):
+    """The transform-sorted schedule moves walkers between threads but keeps
+    each walker's stream: the count plane is identical to one walker a
+    thread, for a flame with every variation, a final and 2x supersampling."""
+    from ffb200 import synthetic as S
+    cfg = S.full_flame(6, de_radius=0)
+    job = dict(iterations=3_000_000, walkers=6000, supersample=2)
+    a, ra, oa = renderer.histogram(cfg, 160, 90, schedule="plain", **job)
+    b, rb, ob = renderer.histogram(cfg, 160, 90, schedule="sorted", **job)
+    assert np.array_equal(a, b)
+    assert oa.inframe_samples == ob.inframe_samples == int(a.sum())
+    np.testing.assert_allclose(ra, rb, rtol=1e-4, atol=1e-3)
+    for rng in ("pcg", "philox"):
+        a, _, _ = renderer.histogram(cfg, 160, 90, schedule="plain", rng=rng, iterations_per_thread=64, **job)
+        b, _, _ = renderer.histogram(cfg, 160, 90, schedule="sorted", rng=rng, iterations_per_thread=64, **job)
+        assert np.array_equal(a, b), rng
 
 
 def log_density_l1(a, b):
@@ -191,40 +233,45 @@ def test_histogram_density_within_monte_carlo_noise(renderer, oracle, seed):
 
 
 def tonemap_params(oracle, cfg, w, h, sd, transparent=0):
+    """The oracle's tone-map parameters from a config.  The reference's config
+    fields are f32 (src/config/fractal_config.rs), so each is rounded to f32
+    first, as the product's parser does; everything after is f64."""
+    import ctypes
+    f = lambda key, d: float(np.float32(cfg.get(key, d)))
     tm = oracle.TonemapParams()
     modes = {"linear": 0, "Linear": 0, "logarithmic": 1, "Logarithmic": 1, "density": 2, "DensityVisualization": 2}
     highs = {"clip": 0, "max_norm": 1, "reinhard": 2, "filmic": 3}
     tm.mode = modes[cfg.get("tonemap_mode", "logarithmic")]
     tm.highlight_mode = highs[cfg.get("highlight_mode", "clip")]
-    tm.exposure = cfg.get("exposure", 1.0)
-    tm.gamma = cfg.get("gamma", 4.0)
-    tm.density_scale = cfg.get("density_scale", 1.0)
+    tm.exposure = f("exposure", 1.0)
+    tm.gamma = f("gamma", 4.0)
+    tm.density_scale = f("density_scale", 1.0)
     bg = cfg.get("background_color", [0, 0, 0])
     for k in range(3):
-        tm.bg[k] = bg[k]
+        tm.bg[k] = float(np.float32(bg[k]))
     tm.use_curve = 1 if cfg.get("use_curve", True) else 0
     lut = oracle.curve_lut_identity()
     tm._lut = lut
-    tm.curve = lut.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_float))
-    tm.vibrancy = cfg.get("vibrancy", 1.0)
-    tm.brightness = cfg.get("brightness", 4.0)
-    tm.white_level = cfg.get("white_level", 200.0)
+    tm.curve = lut.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    tm.vibrancy = f("vibrancy", 1.0)
+    tm.brightness = f("brightness", 4.0)
+    tm.white_level = f("white_level", 200.0)
     tm.prefilter_white = 67108864.0
     tm.bright_adjust = 2.3
-    ppu = min(w, h) * 0.25 * float(np.float32(cfg.get("zoom", 1.0)))
+    ppu = min(w, h) * 0.25 * f("zoom", 1.0)
     tm.area = w * h / (ppu * ppu)
     tm.sample_density = sd
-    tm.saturation = cfg.get("saturation", 1.0)
-    tm.hue_shift = cfg.get("hue_shift", 0.0)
-    tm.gamma_threshold = cfg.get("gamma_threshold", 5.0)
-    tm.alpha_blend_low = cfg.get("alpha_blend_low", 0.3)
-    tm.alpha_blend_high = cfg.get("alpha_blend_high", 0.8)
+    tm.saturation = f("saturation", 1.0)
+    tm.hue_shift = f("hue_shift", 0.0)
+    tm.gamma_threshold = f("gamma_threshold", 5.0)
+    tm.alpha_blend_low = f("alpha_blend_low", 0.3)
+    tm.alpha_blend_high = f("alpha_blend_high", 0.8)
     tm.transparent_mode = transparent
     tm.levels_enabled = 1 if cfg.get("levels_enabled", True) else 0
-    tm.levels_low = cfg.get("levels_low", 0.0)
-    tm.levels_high = cfg.get("levels_high", 10.0)
-    tm.levels_gamma = cfg.get("levels_gamma", 0.5)
-    tm.levels_density = sd
+    tm.levels_low = f("levels_low", 0.0)
+    tm.levels_high = f("levels_high", 10.0)
+    tm.levels_gamma = f("levels_gamma", 0.5)
+    tm.levels_density = float(np.float32(sd))
     return tm
 
 
@@ -259,11 +306,11 @@ def test_tonemap_matches_f64_oracle(renderer, oracle, c1_hist, variant, transpar
     f = f.reshape(-1, 4).astype(np.float64)
     err = np.abs(f - rf) / np.maximum(np.abs(rf), 1e-3)
     assert err.max() <= 1e-5, (variant, transparent, float(err.max()), np.unravel_index(err.argmax(), err.shape))
-    # 8-bit output: equal except where the value sits on a rounding boundary.
+    # 8-bit output: equal except where the value sits on a rounding tie.
     d = np.abs(u8.reshape(-1, 4).astype(int) - ru.astype(int))
-    frac = np.abs(rf * 255 - np.round(rf * 255))
-    assert d.max() <= 1 and (d > 0).sum() <= max(3, int(0.001 * d.size))
-    assert np.all((d == 0) | (np.abs(frac - 0.5) < 1e-3))
+    frac = np.abs(rf * 255 - np.floor(rf * 255))
+    assert d.max() <= 1
+    assert np.all((d == 0) | (np.abs(frac - 0.5) < 1e-4))
 
 
 def test_supersample_downsample_matches_oracle(renderer, oracle, c1_hist):
@@ -297,8 +344,8 @@ def test_point_render_known_answer(renderer):
     """compute_kernel.rs:6502-6511 through the CUDA path: at 64x64 a point at
     x = -1.96875 lights column 0 of the middle row alone; -2.03125 lights nothing."""
     for x, lit in ((-1.96875, 1), (-2.03125, 0)):
-        cfg = {"flame": {"transforms": [{"a": 0, "b": 0, "c": 0, "d": 0, "e": x, "f": 0, "weight": 1, "color": 0,
-                                         "variations": {"linear": 1.0}}]}, "deterministic_rng": True}
+        cfg = {"flame": {"transforms": [{"a": 0, "b": 0, "c": 0, "d": 0, "e": x, "f": 0, "weight": 1, "color": 0.5,
+                                         "color_speed": 0.5, "variations": {"linear": 1.0}}]}, "deterministic_rng": True}
         cnt, _, out = renderer.histogram(cfg, 64, 64, iterations=200_000)
         assert int((cnt > 0).sum()) == lit
         if lit:
