@@ -45,10 +45,11 @@ std::string call(const VarDef* v, const std::string& prm0, const std::string& pr
 
 }  // namespace
 
-Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads) {
+Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads, bool per_xform) {
     Plan p;
     p.rng_mode = rng_mode;
     p.math_mode = math_mode;
+    p.per_xform = per_xform;
     p.threads = threads;
     p.maxx = std::max<int>(maxx, (int)f.xf.size());
     p.normal = normal_vars(f);
@@ -96,6 +97,31 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
           << "; rx = rx + w * ox; ry = ry + w * oy; } }   // " << v->name << "\n";
     }
     s << "    x = rx; y = ry;\n}\n";
+    // Per-transform form for the sorted schedule, where k is (mostly)
+    // warp-uniform: each case evaluates only its transform's variations, in
+    // the same local order, straight-line (their chains overlap).
+    s << "template <class R> __device__ __forceinline__ void ffb_normal_k(const float* __restrict__ sm, int k, float& x, float& y, R& rng) {\n";
+    if (per_xform) {
+        s << "    float rx = 0.0f, ry = 0.0f, ox, oy;\n    switch (k) {\n";
+        for (size_t k = 0; k < f.xf.size(); ++k) {
+            s << "    case " << k << ": {\n";
+            for (int j = 0; j < NVN; ++j) {
+                const VarDef* v = p.normal[j];
+                if (f.xf[k].var_weight(v) == 0.0f) continue;
+                std::ostringstream w, a0, a1;
+                w << "sm[T_VW + " << j << " * FFB_MAXX + " << k << "]";
+                a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + " << k << "]";
+                a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + " << k << "]";
+                s << "        { const float w = " << w.str() << "; " << call(v, a0.str(), a1.str(), p.normal_slot[j])
+                  << "; rx = rx + w * ox; ry = ry + w * oy; }   // " << v->name << "\n";
+            }
+            s << "        break; }\n";
+        }
+        s << "    default: ffb_normal(sm, k, x, y, rng); return;\n    }\n    x = rx; y = ry;\n";
+    } else {
+        s << "    ffb_normal(sm, k, x, y, rng);\n";
+    }
+    s << "}\n";
     // One final of the chain (main_template.wgsl:679-704): affine,
     // variations, post-affine; `aff` false evaluates the variations alone.
     s << "template <class R> __device__ __forceinline__ void ffb_final_one(const float* __restrict__ sm, int c, float& x, float& y, R& rng, bool aff) {\n";
@@ -127,7 +153,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
 
 bool plan_fits(const Plan& p, const Flame& f) {
     if ((int)f.xf.size() > p.maxx) return false;
-    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads);
+    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform);
     return q.source == p.source;
 }
 

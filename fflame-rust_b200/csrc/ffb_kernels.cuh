@@ -99,14 +99,15 @@ __device__ __forceinline__ void ffb_pcg_dispatch(const ffb_launch& J, PcgRng& rn
 // The rest of an iteration once transform k is picked and the opacity draw
 // made: affine, variations, post, bad-value respawn, colour, fuse, finals,
 // palette, world_to_pixel and the splat (main_template.wgsl:366-1320).
-template <class R>
+template <bool PER_XFORM, class R>
 __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
                                          int k, bool plot, R& rng, u32 gw, u64 it, float& x, float& y, float& ci, u32& fuse,
                                          float cx, float cy, float scale, u32& inframe) {
     const float* q = sm + T_XF + k;
     float ax = q[F_A * FFB_MAXX] * x + q[F_B * FFB_MAXX] * y + q[F_E * FFB_MAXX];
     float ay = q[F_C * FFB_MAXX] * x + q[F_D * FFB_MAXX] * y + q[F_F * FFB_MAXX];
-    ffb_normal(sm, k, ax, ay, rng);                                         // main_template.wgsl:366-376
+    if (PER_XFORM) ffb_normal_k(sm, k, ax, ay, rng);                        // main_template.wgsl:366-376
+    else ffb_normal(sm, k, ax, ay, rng);
 #if FFB_HAS_POST
     if (q[F_POST * FFB_MAXX] > 0.5f) {                                      // main_template.wgsl:380-384
         float px = q[F_PA * FFB_MAXX] * ax + q[F_PB * FFB_MAXX] * ay + q[F_PE * FFB_MAXX];
@@ -183,7 +184,7 @@ ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
 #endif
         const int k = ffb_select(sm, n_xf, rng.draw(0));                     // main_template.wgsl:198-223
         const bool plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];       // main_template.wgsl:249
-        ffb_step(sm, pal, J, k, plot, rng, gw, it, x, y, ci, fuse, cx, cy, scale, inframe);
+        ffb_step<false>(sm, pal, J, k, plot, rng, gw, it, x, y, ci, fuse, cx, cy, scale, inframe);
     }
     J.walkers[w] = make_float4(x, y, ci, __uint_as_float(fuse));
     ffb_count_inframe(J, inframe);
@@ -278,13 +279,13 @@ ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
         if (active) {
 #if FFB_RNG_MODE == 0
             rng.state = s_r0[tid]; rng.inc = s_r1[tid];
-            ffb_step(sm, pal, J, k, plot, rng, wid, it, x, y, ci, fuse, cx, cy, scale, inframe);
+            ffb_step<true>(sm, pal, J, k, plot, rng, wid, it, x, y, ci, fuse, cx, cy, scale, inframe);
 #else
             PhiloxRng rng;
             rng.w[2] = __uint_as_float(s_r0[tid]);
             rng.w[3] = __uint_as_float(s_r1[tid]);
             rng.fill_from(1, J.seed_lo, J.seed_hi, wid, it);
-            ffb_step(sm, pal, J, k, plot, rng, wid, it, x, y, ci, fuse, cx, cy, scale, inframe);
+            ffb_step<true>(sm, pal, J, k, plot, rng, wid, it, x, y, ci, fuse, cx, cy, scale, inframe);
 #endif
         }
     }
