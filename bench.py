@@ -154,7 +154,7 @@ def run_ours(args, rank, world, local_rank):
     W, H, ss = wl["width"], wl["height"], wl["supersample"]
     r = _native.Renderer(local_rank)
     job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, walker0=rank * wl["walkers"],
-               seed=0x5EED + 0, schedule=args.schedule)
+               seed=0x5EED + 0, schedule=args.schedule, math=args.math)
     d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
     # The library's kernels and the timing events share one (non-default) stream.
     side = torch.cuda.Stream()
@@ -233,7 +233,7 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded flame generator; no dataset)",
         "config": {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
                    "samples_per_step": samples_per_step, "walkers": wl["walkers"], "rng": "philox",
-                   "schedule": args.schedule,
+                   "schedule": args.schedule, "math": args.math,
                    "l2": "histogram 132.7 MB > 126 MB L2, cleared every step", "parallelism": f"walker shards x{world}"},
         "ms_per_frame": ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -297,6 +297,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--math", default="precise", choices=["precise", "sfu"],
+                    help="precise: IEEE-accurate sin/cos (the parity-tested path); sfu: the hardware's, as the reference GPU")
     ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted"],
                     help="walker scheduling of the chaos kernel (same orbits either way)")
     ap.add_argument("--profile", type=float, default=0.0,

@@ -35,12 +35,16 @@ struct Plan {
     int rng_mode = RNG_PHILOX;
     int math_mode = MATH_PRECISE;
     int threads = 128;
-    bool per_xform = true;                 // emit ffb_normal_k per transform
+    // Emit ffb_normal_k as one straight-line case per transform.  Measured
+    // slower on B200 (the inlined cases overflow the instruction cache:
+    // no-instruction stalls 0.4 -> 1.7 a cycle), so off by default; the
+    // union form is warp-uniform after the sorted schedule's regrouping.
+    bool per_xform = false;
     std::string source;                    // full NVRTC source (structure key)
 };
 
 // Structure of `f` (rng/math modes as given; maxx >= f.xf.size()).
-Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx = 0, int threads = 128, bool per_xform = true);
+Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx = 0, int threads = 128, bool per_xform = false);
 // The table of `f` for a plan made from a flame of the same structure.
 std::vector<float> make_table(const Plan& p, const Flame& f);
 // Whether `f` fits plan `p` (same structure, n_xf <= maxx).
