@@ -11,8 +11,10 @@ reference's own boundary (`fae_call` render request -> RGBA8 in host memory).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank renders its own shard of walkers (weak scaling, no
-data-path collective); rank 0 prints one JSON line.
+Under torchrun each rank renders its own 65,536 walkers (weak scaling); the
+ranks' histograms are summed with an NCCL all-reduce (the path's one exchange
+step), each rank tone-maps a band of rows and the bands are gathered; the
+step time is the max over ranks, and rank 0 prints one JSON line.
 """
 
 import argparse
@@ -160,11 +162,25 @@ def run_ours(args, rank, world, local_rank):
     side = torch.cuda.Stream()
     torch.cuda.set_stream(side)
     stream = side.cuda_stream
+    if world > 1:
+        # Weak scaling: every rank renders its own 65,536 walkers x 1e9
+        # samples; the frame sums all ranks' histograms (NCCL all-reduce),
+        # each rank tone-maps a band of rows, the bands are gathered.
+        from ffb200 import distributed as D
+        backend = D.CudaBackend(r, torch.device("cuda", local_rank), side)
+        djob = {k: v for k, v in job.items() if k not in ("iterations", "walkers", "supersample", "walker0")}
+
+        def step():
+            return D.render(backend, cfg, W, H, iterations=wl["iterations"] * world, walkers=wl["walkers"] * world,
+                            supersample=ss, **djob)
+    else:
+        def step():
+            return r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=False, **job)
     out = r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=True, **job)   # compile + first frame
     samples_per_step = out.total_iterations
-    launches_per_step = out.kernel_launches
+    launches_per_step = out.kernel_launches + (2 if world > 1 else 0)
     for _ in range(args.warmup):
-        r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=False, **job)
+        step()
     torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
@@ -178,7 +194,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t_start.record()
     for _ in range(args.steps):
-        r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=stream, sync=False, **job)
+        step()
     t_end.record()
     t_end.synchronize()
     torch.cuda.synchronize()
@@ -234,7 +250,8 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
                    "samples_per_step": samples_per_step, "walkers": wl["walkers"], "rng": "philox",
                    "schedule": args.schedule, "math": args.math,
-                   "l2": "histogram 132.7 MB > 126 MB L2, cleared every step", "parallelism": f"walker shards x{world}"},
+                   "l2": "histogram 132.7 MB > 126 MB L2, cleared every step",
+                   "parallelism": f"walker shards x{world}" + (" + NCCL histogram all-reduce + row bands" if world > 1 else "")},
         "ms_per_frame": ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,

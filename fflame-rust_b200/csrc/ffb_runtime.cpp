@@ -323,10 +323,11 @@ void check_de(const Flame& f, uint32_t ss) {
 }
 
 // Chaos game of a prepared flame into r->hist (wi*hi float4, cleared here).
-void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walker0, uint64_t* inframe_out) {
+void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walker0, uint64_t* inframe_out,
+               float4* ext_hist = nullptr) {
     Module& m = r->module_for(P.plan.source);
     const size_t npx = (size_t)P.wi * P.hi;
-    float4* hist = (float4*)r->hist.ensure(npx * sizeof(float4));
+    float4* hist = ext_hist ? ext_hist : (float4*)r->hist.ensure(npx * sizeof(float4));
     ck(cudaMemsetAsync(hist, 0, npx * sizeof(float4), s), "clear histogram");
     void* d_table = r->table.ensure(P.table.size() * 4);
     ck(cudaMemcpyAsync(d_table, P.table.data(), P.table.size() * 4, cudaMemcpyHostToDevice, s), "upload table");
@@ -389,15 +390,18 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     }
 }
 
-// Density estimation of r->hist into r->de_out (count as float).
-float4* run_de(ffb_renderer* r, const float4* hist, uint32_t w, uint32_t h, double r_max, double r_min, double curve, cudaStream_t s) {
+// Density estimation of output rows [y_lo, y_lo + h_out) of a w x h
+// histogram into r->de_out (count as float; row y_lo first).
+float4* run_de(ffb_renderer* r, const float4* hist, uint32_t w, uint32_t h, double r_max, double r_min, double curve, cudaStream_t s,
+               uint32_t y_lo = 0, uint32_t h_out = 0) {
+    if (h_out == 0) h_out = h - y_lo;
     int n = 0, radius = 0;
     std::vector<float> tab = de_table(r_max, r_min, curve, n, radius);
     float4* d_tab = (float4*)r->de_tab.ensure(tab.size() * 4);
     ck(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, s), "upload DE table");
     r->h2d += tab.size() * 4;
-    float4* out = (float4*)r->de_out.ensure((size_t)w * h * sizeof(float4));
-    ck(launch_density_estimate(hist, (int)w, (int)h, d_tab, n, radius, out, s), "density estimation");
+    float4* out = (float4*)r->de_out.ensure((size_t)w * h_out * sizeof(float4));
+    ck(launch_density_estimate(hist, (int)w, (int)h, d_tab, n, radius, (int)y_lo, (int)h_out, out, s), "density estimation");
     r->launches += 1;
     return out;
 }
@@ -410,6 +414,27 @@ const float* upload_lut(ffb_renderer* r, const Flame& f, cudaStream_t s) {
     return d;
 }
 
+// The tail of a render: density estimation (if configured) and the tone map
+// of output rows [row0, row0 + rows) of a summed histogram holding
+// `samples` plotted samples, into `d_rgba` (that band, row0 first).
+void finish_device(ffb_renderer* r, const Prepared& P, const float4* hist, uint64_t samples, uint32_t row0, uint32_t rows,
+                   int transparent, void* d_rgba, cudaStream_t s) {
+    const uint32_t ss = P.ss;
+    const uint32_t y_lo = row0 * ss, h_band = rows * ss;
+    const float4* src = hist + (size_t)y_lo * P.wi;
+    bool count_f = false;
+    if (P.flame.de.max_radius > 0.0f) {
+        src = run_de(r, hist, P.wi, P.hi, (double)P.flame.de.max_radius * ss, (double)P.flame.de.min_radius * ss,
+                     (double)P.flame.de.curve, s, y_lo, h_band);
+        count_f = true;
+    }
+    const double sd = std::max((double)samples / ((double)P.wi * (double)P.hi), 1e-6);   // compute_kernel.rs:1796-1840
+    TonemapArgs a = tonemap_args(P.flame, P.wi, P.hi, sd, transparent, count_f);
+    const float* lut = upload_lut(r, P.flame, s);
+    ck(launch_tonemap(src, (int)P.wi, (int)h_band, (int)ss, a, lut, (uint8_t*)d_rgba, nullptr, s), "tone map");
+    r->launches += 1;
+}
+
 // One whole render into device RGBA8 `d_rgba`.
 void render_device(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, void* d_rgba, cudaStream_t s,
                    bool sync, ffb_output* out) {
@@ -420,19 +445,8 @@ void render_device(ffb_renderer* r, const char* config, size_t len, const ffb_jo
     static thread_local uint64_t inframe_slot;
     if (sync) h_inframe = &inframe_slot;
     run_chaos(r, P, s, job->walker0, h_inframe);
-    const float4* hist = (const float4*)r->hist.p;
-    bool count_f = false;
-    if (P.flame.de.max_radius > 0.0f) {
-        hist = run_de(r, hist, P.wi, P.hi, (double)P.flame.de.max_radius * P.ss, (double)P.flame.de.min_radius * P.ss,
-                      (double)P.flame.de.curve, s);
-        count_f = true;
-    }
     const uint64_t plotted = (uint64_t)P.walkers * P.per_walker;
-    const double sd = std::max((double)plotted / ((double)P.wi * (double)P.hi), 1e-6);   // compute_kernel.rs:1796-1840
-    TonemapArgs a = tonemap_args(P.flame, P.wi, P.hi, sd, job->transparent, count_f);
-    const float* lut = upload_lut(r, P.flame, s);
-    ck(launch_tonemap(hist, (int)P.wi, (int)P.hi, (int)P.ss, a, lut, (uint8_t*)d_rgba, nullptr, s), "tone map");
-    r->launches += 1;
+    finish_device(r, P, (const float4*)r->hist.p, plotted, 0, job->height, job->transparent, d_rgba, s);
     ck(cudaEventRecord(r->ev1, s), "event");
     if (out) {
         out->width = job->width; out->height = job->height;
@@ -730,6 +744,57 @@ FFB_API int ffb_apply_points(ffb_renderer* r, const char* config, size_t len, in
         ck(cudaMemcpyAsync(xo, d_xo, nn * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
         ck(cudaMemcpyAsync(yo, d_yo, nn * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
         ck(cudaStreamSynchronize(r->stream), "apply points");
+    });
+}
+
+FFB_API int ffb_chaos_device(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, void* d_hist, void* stream,
+                             ffb_output* out) {
+    return guard([&] {
+        if (!r || !job || !d_hist) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        r->reset_counts();
+        Prepared P = prepare(config, len, job);
+        cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
+        run_chaos(r, P, s, job->walker0, nullptr, (float4*)d_hist);
+        if (out) {
+            *out = ffb_output{};
+            out->width = P.wi; out->height = P.hi;
+            out->total_iterations = (uint64_t)P.walkers * P.per_walker;
+            r->fill_counts(out);
+        }
+    });
+}
+
+FFB_API int ffb_hist_pack(ffb_renderer* r, const void* d_hist, uint64_t pixels, void* d_counts, void* d_rgb, void* stream) {
+    return guard([&] {
+        if (!r || !d_hist || !d_counts || !d_rgb) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        ck(launch_pack((const float4*)d_hist, pixels, (unsigned*)d_counts, (float*)d_rgb, stream ? (cudaStream_t)stream : r->stream), "pack");
+    });
+}
+
+FFB_API int ffb_hist_unpack(ffb_renderer* r, const void* d_counts, const void* d_rgb, uint64_t pixels, void* d_hist, void* stream) {
+    return guard([&] {
+        if (!r || !d_hist || !d_counts || !d_rgb) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        ck(launch_unpack((const unsigned*)d_counts, (const float*)d_rgb, pixels, (float4*)d_hist, stream ? (cudaStream_t)stream : r->stream), "unpack");
+    });
+}
+
+FFB_API int ffb_finish_device(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, const void* d_hist,
+                              uint64_t total_samples, uint32_t row0, uint32_t rows, void* d_rgba, void* stream) {
+    return guard([&] {
+        if (!r || !job || !d_hist || !d_rgba) fail(FFB_ERR_INVALID, "NULL argument");
+        if (rows == 0 || row0 + rows > job->height) fail(FFB_ERR_INVALID, "row band outside the image");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Prepared P = prepare(config, len, job);
+        check_de(P.flame, P.ss);
+        finish_device(r, P, (const float4*)d_hist, total_samples, row0, rows, job->transparent, d_rgba,
+                      stream ? (cudaStream_t)stream : r->stream);
     });
 }
 

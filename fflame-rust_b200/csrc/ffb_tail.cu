@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
 // every count is high, gather over a few pixels only).
 constexpr int DE_TX = 32, DE_TY = 16;
 __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, int w, int h, const float4* __restrict__ tab,
-                                                           int tab_n, int R, float4* __restrict__ out) {
+                                                           int tab_n, int R, int y_lo, int h_out, float4* __restrict__ out) {
     extern __shared__ float4 de_smem[];
     const int tw = DE_TX + 2 * R, th = DE_TY + 2 * R, n = tw * th;
     float4* val = de_smem;                                                // (rgb, count) / normaliser
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
     __shared__ int reach;
     if (threadIdx.x == 0) reach = 0;
     __syncthreads();
-    const int x0 = blockIdx.x * DE_TX - R, y0 = blockIdx.y * DE_TY - R;
+    const int x0 = blockIdx.x * DE_TX - R, y0 = y_lo + blockIdx.y * DE_TY - R;
     int my_reach = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int sx = x0 + i % tw, sy = y0 + i / tw;
@@ -255,8 +255,8 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
     __syncthreads();
     const int rb = min(R, reach);
     const int lx = threadIdx.x % DE_TX, ly = threadIdx.x / DE_TX;
-    const int px = blockIdx.x * DE_TX + lx, py = blockIdx.y * DE_TY + ly;
-    if (px >= w || py >= h) return;
+    const int px = blockIdx.x * DE_TX + lx, py = y_lo + blockIdx.y * DE_TY + ly;
+    if (px >= w || py >= h || py >= y_lo + h_out) return;
     float ar = 0.f, ag = 0.f, ab = 0.f, ac = 0.f;
     for (int dy = -rb; dy <= rb; ++dy) {
         const int row = (ly + R + dy) * tw + (lx + R);
@@ -269,7 +269,21 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
             ar += wt * v.x; ag += wt * v.y; ab += wt * v.z; ac += wt * v.w;
         }
     }
-    out[(size_t)py * w + px] = make_float4(ar, ag, ab, ac);
+    out[(size_t)(py - y_lo) * w + px] = make_float4(ar, ag, ab, ac);
+}
+
+// Histogram planes for a collective: AoS (r, g, b, count bits) <-> a u32
+// count plane and an f32 (r, g, b) plane, each summable by NCCL in its own type.
+__global__ void k_pack(const float4* __restrict__ hist, size_t n, unsigned* __restrict__ cnt, float* __restrict__ rgb) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float4 v = hist[i];
+        cnt[i] = __float_as_uint(v.w);
+        rgb[3 * i] = v.x; rgb[3 * i + 1] = v.y; rgb[3 * i + 2] = v.z;
+    }
+}
+__global__ void k_unpack(const unsigned* __restrict__ cnt, const float* __restrict__ rgb, size_t n, float4* __restrict__ hist) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        hist[i] = make_float4(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], __uint_as_float(cnt[i]));
 }
 
 // Random-address splat microbenchmark (the L2 atomic peak this kernel
@@ -309,14 +323,24 @@ cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const Ton
 }
 
 cudaError_t launch_density_estimate(const float4* hist, int w, int h, const float4* table, int table_n, int radius,
-                                    float4* out, cudaStream_t s) {
+                                    int y_lo, int h_out, float4* out, cudaStream_t s) {
     const size_t smem = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius) * (sizeof(float4) + sizeof(float2));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    dim3 grid((w + DE_TX - 1) / DE_TX, (h + DE_TY - 1) / DE_TY);
-    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, w, h, table, table_n, radius, out);
+    dim3 grid((w + DE_TX - 1) / DE_TX, (h_out + DE_TY - 1) / DE_TY);
+    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, w, h, table, table_n, radius, y_lo, h_out, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const float4* hist, size_t n, unsigned* cnt, float* rgb, cudaStream_t s) {
+    k_pack<<<148 * 8, 256, 0, s>>>(hist, n, cnt, rgb);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const unsigned* cnt, const float* rgb, size_t n, float4* hist, cudaStream_t s) {
+    k_unpack<<<148 * 8, 256, 0, s>>>(cnt, rgb, n, hist);
     return cudaGetLastError();
 }
 

@@ -37,8 +37,14 @@ cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const Ton
 
 // Density estimation table: entry c (counts 0..n-1, the last entry serving
 // every larger count): (max accepted d^2, 1/h^2, 1/normaliser, reach).
+// Computes output rows [y_lo, y_lo + h_out) into `out` (row y_lo first),
+// reading sources from the whole w x h histogram.
 cudaError_t launch_density_estimate(const float4* hist, int w, int h, const float4* table, int table_n, int radius,
-                                    float4* out, cudaStream_t s);
+                                    int y_lo, int h_out, float4* out, cudaStream_t s);
+
+// Histogram <-> (u32 count plane, f32 rgb plane), for collectives.
+cudaError_t launch_pack(const float4* hist, size_t n, unsigned* cnt, float* rgb, cudaStream_t s);
+cudaError_t launch_unpack(const unsigned* cnt, const float* rgb, size_t n, float4* hist, cudaStream_t s);
 
 // Splat-throughput microbenchmark: `n_ops` random-address atomic splats of
 // the given kind into `buf` (n_words u32 words): kind 0 = 4 scalar atomics a

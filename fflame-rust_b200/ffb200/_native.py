@@ -24,7 +24,8 @@ EXPORTS = [
     "fae_alloc", "fae_free", "fae_output_ptr", "fae_output_len", "fae_info_ptr", "fae_info_len", "fae_call",
     "ffb_last_error", "ffb_version", "ffb_renderer_create", "ffb_renderer_destroy", "ffb_render",
     "ffb_render_device", "ffb_histogram", "ffb_tonemap", "ffb_density_estimate", "ffb_probe",
-    "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench",
+    "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench", "ffb_chaos_device", "ffb_hist_pack",
+    "ffb_hist_unpack", "ffb_finish_device",
 ]
 
 
@@ -220,6 +221,30 @@ class Renderer:
                                       ctypes.c_int32(1 if with_affine else 0), ctypes.c_int32(MATH[math] if isinstance(math, str) else math),
                                       _p(xo, ctypes.c_float), _p(yo, ctypes.c_float)))
         return xo, yo
+
+    def chaos_device(self, config, width, height, d_hist, stream=None, **job):
+        """The chaos game of the job's walker shard into a device histogram (int pointer)."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        o = Output()
+        _check(lib().ffb_chaos_device(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), ctypes.c_void_p(d_hist),
+                                      ctypes.c_void_p(stream or 0), ctypes.byref(o)))
+        return o
+
+    def hist_pack(self, d_hist, pixels, d_counts, d_rgb, stream=None):
+        _check(lib().ffb_hist_pack(self._h, ctypes.c_void_p(d_hist), ctypes.c_uint64(pixels), ctypes.c_void_p(d_counts),
+                                   ctypes.c_void_p(d_rgb), ctypes.c_void_p(stream or 0)))
+
+    def hist_unpack(self, d_counts, d_rgb, pixels, d_hist, stream=None):
+        _check(lib().ffb_hist_unpack(self._h, ctypes.c_void_p(d_counts), ctypes.c_void_p(d_rgb), ctypes.c_uint64(pixels),
+                                     ctypes.c_void_p(d_hist), ctypes.c_void_p(stream or 0)))
+
+    def finish_device(self, config, width, height, d_hist, total_samples, row0, rows, d_rgba, stream=None, **job):
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        _check(lib().ffb_finish_device(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), ctypes.c_void_p(d_hist),
+                                       ctypes.c_uint64(total_samples), ctypes.c_uint32(row0), ctypes.c_uint32(rows),
+                                       ctypes.c_void_p(d_rgba), ctypes.c_void_p(stream or 0)))
 
     def atomic_bench(self, pixels, samples, kind=0):
         ms = ctypes.c_double()

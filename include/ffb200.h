@@ -153,6 +153,22 @@ int ffb_apply_points(ffb_renderer* r, const char* config, size_t config_len, int
                      const float* xs, const float* ys, const float* words, int32_t with_affine, int32_t math,
                      float* xo, float* yo);
 
+/* ---- multi-GPU building blocks (one renderer a rank; the caller owns the
+ * collectives).  The render of a walker shard into a caller-owned device
+ * histogram (width*ss x height*ss float4: r, g, b sums and the u32 count's
+ * bits), cleared here. */
+int ffb_chaos_device(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, void* d_hist,
+                     void* stream, ffb_output* out);
+/* Split a device histogram into a u32 count plane and an f32 rgb plane
+ * (pixels*3), each summable by a collective in its own type, and back. */
+int ffb_hist_pack(ffb_renderer* r, const void* d_hist, uint64_t pixels, void* d_counts, void* d_rgb, void* stream);
+int ffb_hist_unpack(ffb_renderer* r, const void* d_counts, const void* d_rgb, uint64_t pixels, void* d_hist, void* stream);
+/* Density estimation and tone map of output rows [row0, row0+rows) of a
+ * summed histogram holding `total_samples` plotted samples, into `d_rgba`
+ * (rows*width*4 bytes).  The DE halo is read from the whole histogram. */
+int ffb_finish_device(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, const void* d_hist,
+                      uint64_t total_samples, uint32_t row0, uint32_t rows, void* d_rgba, void* stream);
+
 /* Compile the chaos-game kernel of a config's structure for sm_100a with
  * NVRTC, without a device (the shader builder's build step,
  * src/shader_builder_v2.rs:2337; src/shader_cache.rs).  Writes the CUBIN

@@ -336,6 +336,49 @@ def curve_lut_identity():
     return np.array([f16_round(f32(i) / f32(255.0)) for i in range(256)], np.float32)
 
 
+def tonemap_params_for(cfg, w, h, sd, transparent=0):
+    """The oracle's tone-map parameters from a config.  The reference's config
+    fields are f32 (src/config/fractal_config.rs), so each is rounded to f32
+    first, as the product's parser does; everything after is f64."""
+    import ctypes
+    f = lambda key, d: float(np.float32(cfg.get(key, d)))
+    tm = TonemapParams()
+    modes = {"linear": 0, "Linear": 0, "logarithmic": 1, "Logarithmic": 1, "density": 2, "DensityVisualization": 2}
+    highs = {"clip": 0, "max_norm": 1, "reinhard": 2, "filmic": 3}
+    tm.mode = modes[cfg.get("tonemap_mode", "logarithmic")]
+    tm.highlight_mode = highs[cfg.get("highlight_mode", "clip")]
+    tm.exposure = f("exposure", 1.0)
+    tm.gamma = f("gamma", 4.0)
+    tm.density_scale = f("density_scale", 1.0)
+    bg = cfg.get("background_color", [0, 0, 0])
+    for k in range(3):
+        tm.bg[k] = float(np.float32(bg[k]))
+    tm.use_curve = 1 if cfg.get("use_curve", True) else 0
+    lut = curve_lut_identity()
+    tm._lut = lut
+    tm.curve = lut.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    tm.vibrancy = f("vibrancy", 1.0)
+    tm.brightness = f("brightness", 4.0)
+    tm.white_level = f("white_level", 200.0)
+    tm.prefilter_white = 67108864.0
+    tm.bright_adjust = 2.3
+    ppu = min(w, h) * 0.25 * f("zoom", 1.0)
+    tm.area = w * h / (ppu * ppu)
+    tm.sample_density = sd
+    tm.saturation = f("saturation", 1.0)
+    tm.hue_shift = f("hue_shift", 0.0)
+    tm.gamma_threshold = f("gamma_threshold", 5.0)
+    tm.alpha_blend_low = f("alpha_blend_low", 0.3)
+    tm.alpha_blend_high = f("alpha_blend_high", 0.8)
+    tm.transparent_mode = transparent
+    tm.levels_enabled = 1 if cfg.get("levels_enabled", True) else 0
+    tm.levels_low = f("levels_low", 0.0)
+    tm.levels_high = f("levels_high", 10.0)
+    tm.levels_gamma = f("levels_gamma", 0.5)
+    tm.levels_density = float(np.float32(sd))
+    return tm
+
+
 def tonemap(params, cnt, rgb):
     """Double-precision tone map: (float RGBA [n,4], RGBA8 [n,4])."""
     cnt = np.ascontiguousarray(cnt, np.float64).ravel()
