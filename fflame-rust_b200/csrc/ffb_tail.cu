@@ -151,8 +151,14 @@ __device__ double4 tonemap_px(const TonemapArgs& A, const float* lut, double cnt
     return make_double4(pow(f.x, inv22), pow(f.y, inv22), pow(f.z, inv22), 1.0);   // tonemap.wgsl:582-589
 }
 
-__device__ __forceinline__ double hist_count(const float4& v, int count_is_float) {
-    return count_is_float ? (double)v.w : (double)__float_as_uint(v.w);
+__device__ __forceinline__ double hist_count(const TonemapArgs& A, const float4& v, size_t i) {
+    if (A.count_is_float) return (double)v.w;
+    if (A.count64) return (double)A.count64[i];
+    return (double)__float_as_uint(v.w);
+}
+__device__ __forceinline__ D3 hist_rgb(const TonemapArgs& A, const float4& v, size_t i) {
+    if (A.rgb64 && !A.count_is_float) return D3{A.rgb64[3 * i], A.rgb64[3 * i + 1], A.rgb64[3 * i + 2]};
+    return D3{v.x, v.y, v.z};
 }
 
 __device__ __forceinline__ uchar4 quantise(double4 o) {
@@ -168,7 +174,7 @@ __global__ void __launch_bounds__(256) k_tonemap1(const float4* __restrict__ his
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 v = hist[i];
-    const double4 o = tonemap_px(A, lut, hist_count(v, A.count_is_float), D3{v.x, v.y, v.z});
+    const double4 o = tonemap_px(A, lut, hist_count(A, v, (size_t)i), hist_rgb(A, v, (size_t)i));
     out[i] = quantise(o);
     if (out_f) out_f[i] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)o.w);
 }
@@ -187,8 +193,9 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
     const int dx[4] = {0, 1, 0, 1}, dy[4] = {0, 0, 1, 1};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const float4 v = hist[(size_t)(oy * 2 + dy[k]) * wi + (ox * 2 + dx[k])];
-        const uchar4 q = quantise(tonemap_px(A, lut, hist_count(v, A.count_is_float), D3{v.x, v.y, v.z}));
+        const size_t idx = (size_t)(oy * 2 + dy[k]) * wi + (ox * 2 + dx[k]);
+        const float4 v = hist[idx];
+        const uchar4 q = quantise(tonemap_px(A, lut, hist_count(A, v, idx), hist_rgb(A, v, idx)));
         s[k][0] = q.x; s[k][1] = q.y; s[k][2] = q.z; s[k][3] = q.w;
         lum[k] = s[k][0] + 2.0f * s[k][1] + s[k][2];
     }
@@ -222,7 +229,8 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
 // largest radius any staged source actually has (dense regions, where
 // every count is high, gather over a few pixels only).
 constexpr int DE_TX = 32, DE_TY = 16;
-__global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, int w, int h, const float4* __restrict__ tab,
+__global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, const unsigned long long* __restrict__ count64,
+                                                           const double* __restrict__ rgb64, int w, int h, const float4* __restrict__ tab,
                                                            int tab_n, int R, int y_lo, int h_out, float4* __restrict__ out) {
     extern __shared__ float4 de_smem[];
     const int tw = DE_TX + 2 * R, th = DE_TY + 2 * R, n = tw * th;
@@ -238,12 +246,14 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         float2 pr = make_float2(-1.0f, 0.0f);                              // empty: never accepted
         if (sx >= 0 && sy >= 0 && sx < w && sy < h) {
-            const float4 hv = hist[(size_t)sy * w + sx];
-            const unsigned c = __float_as_uint(hv.w);
-            if (c > 0u) {
-                const float4 e = tab[c < (unsigned)(tab_n - 1) ? c : (unsigned)(tab_n - 1)];
+            const size_t si = (size_t)sy * w + sx;
+            const float4 hv = hist[si];
+            const unsigned long long c = count64 ? count64[si] : (unsigned long long)__float_as_uint(hv.w);
+            if (c > 0ull) {
+                const float4 e = tab[c < (unsigned long long)(tab_n - 1) ? c : (unsigned long long)(tab_n - 1)];
                 const float cf = (float)c;
-                v = make_float4(hv.x * e.z, hv.y * e.z, hv.z * e.z, cf * e.z);
+                if (rgb64) v = make_float4((float)(rgb64[3 * si] * e.z), (float)(rgb64[3 * si + 1] * e.z), (float)(rgb64[3 * si + 2] * e.z), cf * e.z);
+                else v = make_float4(hv.x * e.z, hv.y * e.z, hv.z * e.z, cf * e.z);
                 pr = make_float2(e.x, 4.5f * e.y);
                 my_reach = max(my_reach, (int)e.w);
             }
@@ -270,6 +280,18 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
         }
     }
     out[(size_t)(py - y_lo) * w + px] = make_float4(ar, ag, ab, ac);
+}
+
+__global__ void k_fold(float4* __restrict__ hist, unsigned long long* __restrict__ count64, double* __restrict__ rgb64, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float4 v = hist[i];
+        const unsigned c = __float_as_uint(v.w);
+        if (c) {
+            count64[i] += c;
+            rgb64[3 * i] += (double)v.x; rgb64[3 * i + 1] += (double)v.y; rgb64[3 * i + 2] += (double)v.z;
+            hist[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
 }
 
 // Histogram planes for a collective: AoS (r, g, b, count bits) <-> a u32
@@ -322,15 +344,20 @@ cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const Ton
     return cudaGetLastError();
 }
 
-cudaError_t launch_density_estimate(const float4* hist, int w, int h, const float4* table, int table_n, int radius,
-                                    int y_lo, int h_out, float4* out, cudaStream_t s) {
+cudaError_t launch_density_estimate(const float4* hist, const unsigned long long* count64, const double* rgb64, int w, int h,
+                                    const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s) {
     const size_t smem = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius) * (sizeof(float4) + sizeof(float2));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     dim3 grid((w + DE_TX - 1) / DE_TX, (h_out + DE_TY - 1) / DE_TY);
-    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, w, h, table, table_n, radius, y_lo, h_out, out);
+    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, count64, rgb64, w, h, table, table_n, radius, y_lo, h_out, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_counts(float4* hist, unsigned long long* count64, double* rgb64, size_t n, cudaStream_t s) {
+    k_fold<<<148 * 8, 256, 0, s>>>(hist, count64, rgb64, n);
     return cudaGetLastError();
 }
 

@@ -25,7 +25,7 @@ EXPORTS = [
     "ffb_last_error", "ffb_version", "ffb_renderer_create", "ffb_renderer_destroy", "ffb_render",
     "ffb_render_device", "ffb_histogram", "ffb_tonemap", "ffb_density_estimate", "ffb_probe",
     "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench", "ffb_chaos_device", "ffb_hist_pack",
-    "ffb_hist_unpack", "ffb_finish_device",
+    "ffb_hist_unpack", "ffb_finish_device", "ffb_histogram_u64",
 ]
 
 
@@ -43,7 +43,8 @@ class Job(ctypes.Structure):
         ("iterations_per_thread", ctypes.c_uint32), ("burn_in", ctypes.c_uint32), ("walkers", ctypes.c_uint32),
         ("supersample", ctypes.c_uint32), ("rng", ctypes.c_int32), ("math", ctypes.c_int32),
         ("transparent", ctypes.c_int32), ("threads", ctypes.c_int32), ("seed", ctypes.c_uint64),
-        ("walker0", ctypes.c_uint32), ("schedule", ctypes.c_uint32),
+        ("walker0", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("count_bits", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 
@@ -109,7 +110,7 @@ SCHEDULE = {"auto": 0, "plain": 1, "sorted": 2}
 
 
 def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0, walkers=0, supersample=1,
-             rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0, schedule="auto"):
+             rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0, schedule="auto", count_bits=32):
     j = Job()
     j.width, j.height, j.iterations = width, height, int(iterations or 0)
     j.iterations_per_thread, j.burn_in, j.walkers = iterations_per_thread, burn_in, walkers
@@ -118,6 +119,7 @@ def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0
     j.math = MATH[math] if isinstance(math, str) else math
     j.transparent, j.threads, j.seed, j.walker0 = int(transparent), threads, int(seed), walker0
     j.schedule = SCHEDULE[schedule] if isinstance(schedule, str) else schedule
+    j.count_bits = count_bits
     return j
 
 
@@ -173,6 +175,19 @@ class Renderer:
         o = Output()
         _check(lib().ffb_histogram(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), _p(cnt, ctypes.c_uint32),
                                    _p(rgb, ctypes.c_float), ctypes.byref(o)))
+        return cnt, rgb, o
+
+    def histogram_u64(self, config, width, height, **job):
+        """The chaos game with exact u64 counts: (counts u64 [H, W], rgb f32 [H, W, 3], Output)."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        ss = j.supersample or 1
+        H, W = height * ss, width * ss
+        cnt = np.zeros((H, W), np.uint64)
+        rgb = np.zeros((H, W, 3), np.float32)
+        o = Output()
+        _check(lib().ffb_histogram_u64(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), _p(cnt, ctypes.c_uint64),
+                                       _p(rgb, ctypes.c_float), ctypes.byref(o)))
         return cnt, rgb, o
 
     def tonemap(self, config, counts, rgb, sample_density, ss=1, transparent=0, want_float=False):

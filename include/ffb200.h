@@ -82,6 +82,10 @@ typedef struct {
     uint64_t seed;                     /* 0: the config's (12345 under deterministic_rng) */
     uint32_t walker0;                  /* first walker id of this shard (multi-GPU sharding) */
     uint32_t schedule;                 /* 0 auto, 1 one walker a thread, 2 transform-sorted (same orbits) */
+    uint32_t count_bits;               /* 32 (0) or 64: exact accumulation -- u32 counts and FP32 colour
+                                          sums folded every <= 2^28 samples into u64 counts and FP64
+                                          sums (accumulate.wgsl:185-199) */
+    uint32_t reserved;
 } ffb_job;
 
 /* RenderOutput (src/renderer/render.rs:207-218). */
@@ -124,6 +128,11 @@ int ffb_render_device(ffb_renderer* r, const char* config, size_t config_len, co
  * (src/export/high_res.rs:2139-2175). */
 int ffb_histogram(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
                   uint32_t* counts, float* rgb, ffb_output* out);
+
+/* The same with exact u64 counts (job->count_bits taken as 64): counts is
+ * w*h u64 hits. */
+int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
+                      uint64_t* counts, float* rgb, ffb_output* out);
 
 /* The tone map of a host histogram (counts as f32, colour sums), with the
  * config's tone-map settings and the given sample density:

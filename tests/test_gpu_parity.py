@@ -354,3 +354,26 @@ def test_engine_renders_like_pyfae():
     a, b = image.array().astype(int), again.array().astype(int)
     # Counts are exact; FP32 colour sums may round in another order.
     assert np.abs(a - b).max() <= 1 and (a != b).mean() < 0.01
+
+
+def test_exact_u64_counts_carry_past_2_32(renderer):
+    """compute_kernel.rs:6996-7072 (exact u64 count, carry into the high
+    word) through the render: every sample of a point flame lands in one
+    pixel, 65,536 x 65,537 = 2^32 + 65,536 of them.  With count_bits 64 the
+    count is exact and the mean colour stays the palette entry's."""
+    cfg = {"flame": {"transforms": [{"a": 0, "b": 0, "c": 0, "d": 0, "e": 0.25, "f": -0.25, "weight": 1, "color": 0.7,
+                                     "color_speed": 0.0, "variations": {"linear": 1.0}}]}, "deterministic_rng": True}
+    n = 65536 * 65537
+    cnt, rgb, out = renderer.histogram_u64(cfg, 16, 16, iterations=n, walkers=65536)
+    assert out.total_iterations == n
+    lit = np.argwhere(cnt > 0)
+    assert len(lit) == 1
+    y, x = lit[0]
+    assert int(cnt[y, x]) == n == out.inframe_samples
+    assert n > 2 ** 32
+    # All samples share one palette entry: its colour, to f32 precision.
+    mean = rgb[y, x].astype(np.float64) / n
+    img, _ = renderer.render(cfg, 16, 16, iterations=2_000_000, walkers=4096)
+    cnt2, rgb2, _ = renderer.histogram(cfg, 16, 16, iterations=2_000_000, walkers=4096)
+    ref = rgb2[y, x].astype(np.float64) / cnt2[y, x]
+    np.testing.assert_allclose(mean, ref, rtol=1e-6)

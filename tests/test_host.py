@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def header_functions():
     text = open(os.path.join(ROOT, "include", "ffb200.h"), encoding="utf-8").read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b((?:fae|ffb)_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b((?:fae|ffb)_[a-z_0-9]+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol(native):
