@@ -233,7 +233,7 @@ def run_ours(args, rank, world, local_rank):
     info = None
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        image = eng.render(cfg, W, H, iterations=req_iters, supersample=ss)
+        image = eng.render(cfg, W, H, iterations=req_iters, supersample=ss, walkers=wl["walkers"])
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)

@@ -39,13 +39,38 @@ __device__ __forceinline__ int ffb_palette_index(float ci, u32 n) {
     return (int)t;
 }
 
-// Splat one sample: exact u32 count, FP32 colour sums.
-__device__ __forceinline__ void ffb_splat(float4* __restrict__ hist, u32 idx, float4 c) {
+// Splat one sample: exact u32 count, FP32 colour sums.  Warp-aggregated:
+// the lanes of a warp splatting the same pixel with the same palette entry
+// find each other (__match_any_sync on a 64-bit key) and their lowest lane
+// adds n * colour and n once, so a hot pixel (an attractor's fixed point)
+// costs one atomic per warp instead of one per lane.  A lone lane adds
+// exactly what it would have alone.
+__device__ __forceinline__ void ffb_splat(float4* __restrict__ hist, u32 idx, float4 c, int pal_idx) {
     float* p = reinterpret_cast<float*>(hist + idx);
+#ifdef FFB_NO_AGGREGATION
     atomicAdd(p + 0, c.x);
     atomicAdd(p + 1, c.y);
     atomicAdd(p + 2, c.z);
     atomicAdd(reinterpret_cast<u32*>(p + 3), 1u);
+#else
+    const unsigned live = __activemask();
+    const unsigned long long key = ((unsigned long long)idx << 16) | (unsigned)pal_idx;
+    const unsigned peers = __match_any_sync(live, key);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) {
+        const u32 n = __popc(peers);
+        if (n == 1u) {
+            atomicAdd(p + 0, c.x);
+            atomicAdd(p + 1, c.y);
+            atomicAdd(p + 2, c.z);
+        } else {
+            const float fn = (float)n;
+            atomicAdd(p + 0, fn * c.x);
+            atomicAdd(p + 1, fn * c.y);
+            atomicAdd(p + 2, fn * c.z);
+        }
+        atomicAdd(reinterpret_cast<u32*>(p + 3), n);
+    }
+#endif
 }
 
 // The job owning this block (block-uniform binary search) and its tables
@@ -132,7 +157,8 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
     if (fuse > 0u) { fuse -= 1u; return; }                                 // main_template.wgsl:510-514
     float fx = x, fy = y;
     ffb_finals(sm, fx, fy, rng);                                            // main_template.wgsl:663-717
-    const float4 c = pal[ffb_palette_index(ci, J.pal_n)];                   // main_template.wgsl:766-772
+    const int pal_idx = ffb_palette_index(ci, J.pal_n);
+    const float4 c = pal[pal_idx];                                          // main_template.wgsl:766-772
     // world_to_pixel (utilities.wgsl:417-450).
     float tx = fx - J.pan_x, ty = fy - J.pan_y;
     float rx = tx * J.cos_r - ty * J.sin_r;
@@ -141,7 +167,7 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
     const float pxf = floorf(cx + rx * scale), pyf = floorf(cy + ry * scale);
     if (plot && pxf >= 0.0f && pyf >= 0.0f && pxf < (float)J.width && pyf < (float)J.height) {
         const u32 idx = (u32)pyf * (u32)J.width + (u32)pxf;
-        ffb_splat(J.hist, idx, c);
+        ffb_splat(J.hist, idx, c, pal_idx);
         ++inframe;
     }
 }

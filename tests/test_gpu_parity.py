@@ -371,9 +371,11 @@ def test_exact_u64_counts_carry_past_2_32(renderer):
     y, x = lit[0]
     assert int(cnt[y, x]) == n == out.inframe_samples
     assert n > 2 ** 32
-    # All samples share one palette entry: its colour, to f32 precision.
+    # Every plotted sample carries one palette entry (the colour index has
+    # converged to 0.7 after the burn-in): the exact sums give its colour.
+    import sys, os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from oracle import oracle as O
+    entry = O.palette_table(cfg).reshape(-1, 3)[int(np.floor(np.float32(0.7) * 256))]
     mean = rgb[y, x].astype(np.float64) / n
-    img, _ = renderer.render(cfg, 16, 16, iterations=2_000_000, walkers=4096)
-    cnt2, rgb2, _ = renderer.histogram(cfg, 16, 16, iterations=2_000_000, walkers=4096)
-    ref = rgb2[y, x].astype(np.float64) / cnt2[y, x]
-    np.testing.assert_allclose(mean, ref, rtol=1e-6)
+    np.testing.assert_allclose(mean, entry, rtol=2e-6)
