@@ -271,6 +271,61 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def run_batched(args, local_rank):
+    """256 synthetic flames (transform counts 2-12, 128^2-1024^2, 50-2000
+    samples a pixel): one batched, graph-captured render against the same
+    flames rendered one after another.  flames/s, device-timed."""
+    import torch
+    from ffb200 import Batch, _native, synthetic
+    torch.cuda.set_device(local_rank)
+    r = _native.Renderer(local_rank)
+    items = synthetic.batch_flames(n=256, seed=3)
+    t0 = time.perf_counter()
+    b = Batch(r, items, tune=True)
+    setup_s = time.perf_counter() - t0
+    info = b.info()
+    for _ in range(args.warmup):
+        b.run()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms_b = [b.run() for _ in range(args.steps)]
+    clk = clocks.stop()
+    batched_ms = statistics.median(ms_b)
+    # Serial: each flame its own render (same budgets), back to back on one stream.
+    side = torch.cuda.Stream()
+    outs = [torch.empty(w * h * 4, dtype=torch.uint8, device="cuda") for _, w, h, _, _ in items]
+    def serial():
+        for (cfg, w, h, samples, seed), o in zip(items, outs):
+            r.render_device(json.dumps(cfg), w, h, o.data_ptr(), stream=side.cuda_stream, sync=False,
+                            iterations=samples, seed=seed)
+    serial()
+    side.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms_s = []
+    for _ in range(max(1, args.steps // 2)):
+        ev0.record(side)
+        serial()
+        ev1.record(side)
+        ev1.synchronize()
+        ms_s.append(ev0.elapsed_time(ev1))
+    serial_ms = statistics.median(ms_s)
+    b.close()
+    n = len(items)
+    return {
+        "metric": "flames/s (batched 256)", "value": n / (batched_ms * 1e-3), "unit": "flames/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flame generator)",
+        "config": {"workload": "batched_256", "flames": n, "samples": info["samples"],
+                   "desc": "256 flames, 2-12 transforms {linear,sinusoidal,spherical}, 128^2-1024^2, 50-2000 spp",
+                   "tuned": {"threads": info["threads"], "iterations_per_walker": info["iterations_per_walker"]},
+                   "groups": info["groups"], "setup_s": setup_s},
+        "samples_per_s": info["samples"] / (batched_ms * 1e-3),
+        "serial": {"value": n / (serial_ms * 1e-3), "unit": "flames/s", "ms": serial_ms},
+        "batched_over_serial": serial_ms / batched_ms,
+        "clocks": clk,
+    }
+
+
 def run_reference(args, rank, world):
     """The reference's CPU path: there is none (variations exist only as
     WGSL; benches/flame_bench.rs:1-10), so the oracle port of it runs on all
@@ -312,7 +367,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256"])
+    ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256", "batched_256"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--math", default="precise", choices=["precise", "sfu"],
                     help="precise: IEEE-accurate sin/cos (the parity-tested path); sfu: the hardware's, as the reference GPU")
@@ -335,6 +390,11 @@ def main():
             _, _, o = r.histogram(json.dumps(wl["cfg"]), wl["width"], wl["height"], **job)
         print(json.dumps({"profile": args.workload, "samples": o.total_iterations, "inframe": o.inframe_samples,
                           "ms": o.render_time_ms}))
+        return
+    if args.workload == "batched_256" and args.impl == "ours":
+        line = run_batched(args, local_rank) if rank == 0 else None
+        if line is not None:
+            print(json.dumps(line), flush=True)
         return
     if args.impl == "reference":
         line = run_reference(args, rank, world)

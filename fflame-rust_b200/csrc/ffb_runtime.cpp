@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <list>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -104,6 +105,7 @@ struct Module {
     cudaLibrary_t lib = nullptr;
     cudaKernel_t chaos = nullptr, chaos_sorted = nullptr, probe = nullptr, apply = nullptr;
     int smem_attr = 0, smem_attr_sorted = 0;
+    int pins = 0;                  // batches holding this module (not evicted while > 0)
 };
 
 std::string nvrtc_options_key() { return "sm_100a|c++17|ftz|prec-div|prec-sqrt|nofmad"; }
@@ -145,8 +147,14 @@ struct ffb_renderer {
         compile(src, m);
         cache.push_front(std::move(m));
         while (cache.size() > 32) {                         // src/shader_cache.rs keeps an LRU too
-            if (cache.back().lib) cudaLibraryUnload(cache.back().lib);
-            cache.pop_back();
+            auto victim = cache.end();
+            for (auto it = std::prev(cache.end()); ; --it) {
+                if (it->pins == 0 && it != cache.begin()) { victim = it; break; }
+                if (it == cache.begin()) break;
+            }
+            if (victim == cache.end()) break;              // everything pinned: keep growing
+            if (victim->lib) cudaLibraryUnload(victim->lib);
+            cache.erase(victim);
         }
         return cache.front();
     }
@@ -891,6 +899,312 @@ FFB_API int ffb_atomic_bench(ffb_renderer* r, uint32_t pixels, uint64_t samples,
         ck(cudaEventElapsedTime(&t, r->ev0, r->ev1), "event time");
         *ms = t;
     });
+}
+
+
+// =============================================================== batches ===
+// Many flames in one persistent launch a structure group (the batched
+// addition beside the reference's one-flame-a-call render, render.rs:483-804):
+// walkers a flame sized to its budget, every block owning walkers of one
+// flame (ffb_chaos_sorted finds its flame by binary search over block0),
+// one batched tone-map launch, the device work captured once as a CUDA graph
+// and replayed.  Threads a block and iterations a walker are picked by
+// timing candidates on a scaled-down copy of the batch.
+
+namespace ffb {
+namespace {
+
+struct BatchFlame {
+    Prepared P;
+    uint64_t budget = 0;
+    uint32_t group = 0;
+    uint32_t walkers = 0, per_walker = 0;
+    size_t hist_off = 0, walk_off = 0, rgba_off = 0, tab_off = 0, pal_off = 0;
+};
+
+struct BatchGroup {
+    Module* mod = nullptr;
+    std::string src;
+    int table_size = 0, maxx = 0, max_pal = 0;
+    std::vector<uint32_t> members;
+};
+
+}  // namespace
+}  // namespace ffb
+
+struct ffb_batch {
+    ffb_renderer* r = nullptr;
+    std::vector<BatchFlame> flames;
+    std::vector<BatchGroup> groups;
+    DevBuf hist, walk, rgba, tables, palettes, counters, launches, tjobs, luts;
+    uint32_t threads = 256, iters = 1024;
+    uint64_t total_samples = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int rng = RNG_PHILOX, transparent = 0;
+    ~ffb_batch() {
+        for (auto& G : groups) if (G.mod) G.mod->pins -= 1;
+        groups.clear();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (DevBuf* b : {&hist, &walk, &rgba, &tables, &palettes, &counters, &launches, &tjobs, &luts}) b->release();
+    }
+};
+
+namespace ffb {
+namespace {
+
+// Walkers and launch records of every group for (threads, iters), scaling
+// each budget by 1/`scale` (the tuner's trial runs); enqueues the clears,
+// the chaos launches and the tone map on `s`.
+void batch_enqueue(ffb_batch* B, uint32_t threads, uint32_t iters, uint64_t scale, cudaStream_t s, bool tonemap,
+                   bool upload = true) {
+    ffb_renderer* r = B->r;
+    size_t walk_total = 0;
+    for (auto& F : B->flames) {
+        const uint64_t budget = std::max<uint64_t>(1, F.budget / scale);
+        uint64_t w = (budget + iters - 1) / iters;
+        w = std::max<uint64_t>(w, threads);
+        w = (w + threads - 1) / threads * threads;
+        F.walkers = (uint32_t)w;
+        F.per_walker = (uint32_t)((budget + w - 1) / w);
+        F.walk_off = walk_total;
+        walk_total += w;
+    }
+    void* d_walk = B->walk.ensure(walk_total * 16);
+    size_t hist_bytes = 0;
+    for (auto& F : B->flames) hist_bytes = std::max(hist_bytes, (F.hist_off + (size_t)F.P.wi * F.P.hi) * 16);
+    ck(cudaMemsetAsync(B->hist.p, 0, hist_bytes, s), "clear histograms");
+    ck(cudaMemsetAsync(B->counters.p, 0, B->flames.size() * 8, s), "clear counters");
+    std::vector<Launch> all;
+    std::vector<size_t> first;
+    for (auto& G : B->groups) {
+        first.push_back(all.size());
+        uint32_t block0 = 0;
+        for (uint32_t j : G.members) {
+            BatchFlame& F = B->flames[j];
+            const Prepared& P = F.P;
+            Launch L{};
+            L.table = (const float*)B->tables.p + F.tab_off;
+            L.palette = (const float*)B->palettes.p + F.pal_off;
+            L.hist = (float4*)B->hist.p + F.hist_off;
+            L.walkers = (float4*)d_walk + F.walk_off;
+            L.counters = (uint64_t*)B->counters.p + j;
+            L.n_walkers = F.walkers; L.walker0 = 0; L.block0 = block0; L.n_xf = (uint32_t)P.flame.xf.size();
+            L.seed_lo = (uint32_t)P.seed; L.seed_hi = (uint32_t)(P.seed >> 32); L.burn_in = P.burn_in; L.ipt = P.ipt;
+            L.it0 = 0; L.n_iters = F.per_walker + P.burn_in;
+            L.pal_n = (uint32_t)(P.palette.size() / 4);
+            L.width = (int32_t)P.wi; L.height = (int32_t)P.hi;
+            L.zoom = P.flame.zoom; L.pan_x = (float)P.flame.pan_x; L.pan_y = (float)P.flame.pan_y;
+            L.cos_r = (float)std::cos((double)P.flame.rotation); L.sin_r = (float)std::sin((double)P.flame.rotation);
+            block0 += F.walkers / threads;
+            all.push_back(L);
+        }
+    }
+    // Under graph capture (upload false) the records uploaded by the
+    // identical uncaptured call before are reused: a capture may not copy
+    // from pageable host memory, nor allocate.
+    Launch* d_l = (Launch*)B->launches.ensure(all.size() * sizeof(Launch));
+    if (upload) ck(cudaMemcpyAsync(d_l, all.data(), all.size() * sizeof(Launch), cudaMemcpyHostToDevice, s), "upload launches");
+    for (size_t g = 0; g < B->groups.size(); ++g) {
+        BatchGroup& G = B->groups[g];
+        uint32_t blocks = 0;
+        for (uint32_t j : G.members) blocks += B->flames[j].walkers / threads;
+        const int smem = ((G.table_size + 3) / 4) * 16 + G.max_pal * 16 + (int)threads * 8 * 4 + 2 * (G.maxx + 1) * 4;
+        if (smem > 48 * 1024 && G.mod->smem_attr_sorted < smem) {
+            ck(cudaFuncSetAttribute((const void*)G.mod->chaos_sorted, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
+            G.mod->smem_attr_sorted = smem;
+        }
+        Launch* jp = d_l + first[g];
+        int nj = (int)G.members.size();
+        void* args[] = {&jp, &nj};
+        ck(cudaLaunchKernel((const void*)G.mod->chaos_sorted, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch batch");
+        r->launches += 1;
+    }
+    if (!tonemap) return;
+    std::vector<TonemapJob> tj;
+    long long px = 0;
+    for (size_t j = 0; j < B->flames.size(); ++j) {
+        BatchFlame& F = B->flames[j];
+        TonemapJob J{};
+        J.hist = (const float4*)B->hist.p + F.hist_off;
+        J.out = (uint8_t*)B->rgba.p + F.rgba_off;
+        J.lut = (const float*)B->luts.p + 256 * j;
+        J.px0 = px;
+        J.w = (int)F.P.wi; J.h = (int)F.P.hi;
+        const uint64_t plotted = (uint64_t)F.walkers * F.per_walker;
+        const double sd = std::max((double)plotted / ((double)F.P.wi * (double)F.P.hi), 1e-6);
+        J.a = tonemap_args(F.P.flame, F.P.wi, F.P.hi, sd, B->transparent, false);
+        tj.push_back(J);
+        px += (long long)F.P.wi * F.P.hi;
+    }
+    TonemapJob* d_tj = (TonemapJob*)B->tjobs.ensure(tj.size() * sizeof(TonemapJob));
+    if (upload) ck(cudaMemcpyAsync(d_tj, tj.data(), tj.size() * sizeof(TonemapJob), cudaMemcpyHostToDevice, s), "upload tone-map jobs");
+    ck(launch_tonemap_batch(d_tj, (int)tj.size(), px, s), "batched tone map");
+    r->launches += 1;
+}
+
+}  // namespace
+}  // namespace ffb
+
+FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint32_t n, const ffb_job* common, int32_t tune,
+                             ffb_batch** out) {
+    return guard([&] {
+        if (!r || !items || !common || !out || n == 0) fail(FFB_ERR_INVALID, "bad argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        auto B = std::make_unique<ffb_batch>();
+        B->r = r;
+        B->rng = common->rng < 0 ? RNG_PHILOX : common->rng;
+        B->transparent = common->transparent;
+        // Parse every flame; one transform capacity for the whole batch so
+        // flames that differ only in their transform count share a module.
+        int maxx = 1;
+        B->flames.resize(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            ffb_job j = *common;
+            j.width = items[i].width; j.height = items[i].height; j.iterations = items[i].iterations;
+            j.seed = items[i].seed; j.supersample = 1;
+            if (j.iterations == 0) fail(FFB_ERR_INVALID, "every batch item needs its sample budget");
+            B->flames[i].P = prepare(items[i].config, items[i].config_len, &j);
+            if (B->flames[i].P.flame.de.max_radius > 0.0f) fail(FFB_ERR_INVALID, "density estimation is not available in batches");
+            B->flames[i].budget = j.iterations;
+            maxx = std::max<int>(maxx, (int)B->flames[i].P.flame.xf.size());
+        }
+        std::map<std::string, uint32_t> by_src;
+        size_t hist_px = 0, rgba_bytes = 0, tab_floats = 0, pal_floats = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            BatchFlame& F = B->flames[i];
+            F.P.plan = make_plan(F.P.flame, B->rng, F.P.math, maxx, 128);
+            F.P.table = make_table(F.P.plan, F.P.flame);
+            auto it = by_src.find(F.P.plan.source);
+            if (it == by_src.end()) {
+                it = by_src.emplace(F.P.plan.source, (uint32_t)B->groups.size()).first;
+                BatchGroup G;
+                G.src = F.P.plan.source;
+                G.table_size = F.P.plan.table_size;
+                G.maxx = F.P.plan.maxx;
+                B->groups.push_back(G);
+            }
+            F.group = it->second;
+            BatchGroup& G = B->groups[F.group];
+            G.members.push_back(i);
+            G.max_pal = std::max<int>(G.max_pal, (int)(F.P.palette.size() / 4));
+            F.hist_off = hist_px; hist_px += (size_t)F.P.wi * F.P.hi;
+            F.rgba_off = rgba_bytes; rgba_bytes += (size_t)F.P.wi * F.P.hi * 4;
+            F.tab_off = tab_floats; tab_floats += (F.P.table.size() + 3) / 4 * 4;
+            F.pal_off = pal_floats; pal_floats += F.P.palette.size();
+            B->total_samples += F.budget;
+        }
+        for (auto& G : B->groups) { G.mod = &r->module_for(G.src); G.mod->pins += 1; }
+        B->hist.ensure(hist_px * 16);
+        B->rgba.ensure(rgba_bytes);
+        B->counters.ensure(n * 8);
+        std::vector<float> tabs(tab_floats), pals(pal_floats), luts((size_t)n * 256);
+        for (uint32_t i = 0; i < n; ++i) {
+            BatchFlame& F = B->flames[i];
+            std::copy(F.P.table.begin(), F.P.table.end(), tabs.begin() + F.tab_off);
+            std::copy(F.P.palette.begin(), F.P.palette.end(), pals.begin() + F.pal_off);
+            std::vector<float> lut = curve_lut(F.P.flame.tm);
+            std::copy(lut.begin(), lut.end(), luts.begin() + (size_t)i * 256);
+        }
+        cudaStream_t s = r->stream;
+        ck(cudaMemcpyAsync(B->tables.ensure(tabs.size() * 4), tabs.data(), tabs.size() * 4, cudaMemcpyHostToDevice, s), "upload tables");
+        ck(cudaMemcpyAsync(B->palettes.ensure(pals.size() * 4), pals.data(), pals.size() * 4, cudaMemcpyHostToDevice, s), "upload palettes");
+        ck(cudaMemcpyAsync(B->luts.ensure(luts.size() * 4), luts.data(), luts.size() * 4, cudaMemcpyHostToDevice, s), "upload curves");
+        // Autotune: time each (threads, iterations a walker) on 1/64 of
+        // every budget; keep the fastest per sample.
+        B->threads = common->threads ? (uint32_t)common->threads : 256;
+        B->iters = common->iterations_per_thread ? common->iterations_per_thread : 1024;
+        if (tune) {
+            double best = 1e30;
+            const uint32_t cand_t[] = {128, 256, 512};
+            const uint32_t cand_i[] = {256, 1024, 4096};
+            for (uint32_t t : cand_t)
+                for (uint32_t it : cand_i) {
+                    batch_enqueue(B.get(), t, it, 64, s, false);             // warm (allocations)
+                    ck(cudaEventRecord(r->ev0, s), "event");
+                    batch_enqueue(B.get(), t, it, 64, s, false);
+                    ck(cudaEventRecord(r->ev1, s), "event");
+                    ck(cudaStreamSynchronize(s), "tune");
+                    float ms = 0.f;
+                    ck(cudaEventElapsedTime(&ms, r->ev0, r->ev1), "event time");
+                    uint64_t samples = 0;
+                    for (auto& F : B->flames) samples += (uint64_t)F.walkers * F.per_walker;
+                    const double per = ms / (double)samples;
+                    if (per < best) { best = per; B->threads = t; B->iters = it; }
+                }
+        }
+        // Size the buffers for the real run, then capture it as a graph.
+        batch_enqueue(B.get(), B->threads, B->iters, 1, s, true);
+        ck(cudaStreamSynchronize(s), "batch warm-up");
+        ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        try {
+            batch_enqueue(B.get(), B->threads, B->iters, 1, s, true, false);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        ck(cudaStreamEndCapture(s, &B->graph), "end capture");
+        ck(cudaGraphInstantiate(&B->exec, B->graph, 0), "graph instantiate");
+        *out = B.release();
+    });
+}
+
+FFB_API int ffb_batch_run(ffb_batch* b, void* stream, int32_t sync, double* ms) {
+    return guard([&] {
+        if (!b) fail(FFB_ERR_INVALID, "NULL batch");
+        ffb_renderer* r = b->r;
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
+        ck(cudaEventRecord(r->ev0, s), "event");
+        ck(cudaGraphLaunch(b->exec, s), "graph launch");
+        ck(cudaEventRecord(r->ev1, s), "event");
+        if (sync || ms) {
+            ck(cudaStreamSynchronize(s), "batch");
+            float t = 0.f;
+            ck(cudaEventElapsedTime(&t, r->ev0, r->ev1), "event time");
+            if (ms) *ms = t;
+        }
+    });
+}
+
+FFB_API int ffb_batch_output(ffb_batch* b, uint32_t index, uint8_t* rgba, uint64_t* plotted) {
+    return guard([&] {
+        if (!b || index >= b->flames.size()) fail(FFB_ERR_INVALID, "no such batch item");
+        ffb_renderer* r = b->r;
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        const BatchFlame& F = b->flames[index];
+        if (rgba) {
+            ck(cudaMemcpyAsync(rgba, (uint8_t*)b->rgba.p + F.rgba_off, (size_t)F.P.wi * F.P.hi * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+            ck(cudaStreamSynchronize(r->stream), "readback");
+        }
+        if (plotted) *plotted = (uint64_t)F.walkers * F.per_walker;
+    });
+}
+
+FFB_API int ffb_batch_info(ffb_batch* b, uint64_t* total_samples, uint32_t* threads, uint32_t* iters_per_walker, uint32_t* groups) {
+    return guard([&] {
+        if (!b) fail(FFB_ERR_INVALID, "NULL batch");
+        uint64_t t = 0;
+        for (auto& F : b->flames) t += (uint64_t)F.walkers * F.per_walker;
+        if (total_samples) *total_samples = t;
+        if (threads) *threads = b->threads;
+        if (iters_per_walker) *iters_per_walker = b->iters;
+        if (groups) *groups = (uint32_t)b->groups.size();
+    });
+}
+
+FFB_API void ffb_batch_destroy(ffb_batch* b) {
+    if (!b) return;
+    std::lock_guard<std::mutex> lk(b->r->mu);
+    b->r->begin();
+    cudaStreamSynchronize(b->r->stream);
+    delete b;
 }
 
 // ------------------------------------------------------------ drop-in ----

@@ -179,6 +179,23 @@ __global__ void __launch_bounds__(256) k_tonemap1(const float4* __restrict__ his
     if (out_f) out_f[i] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)o.w);
 }
 
+// Many flames in one launch: a grid-stride over the concatenated pixels of
+// every flame, each pixel finding its flame by binary search over px0.
+__global__ void __launch_bounds__(256) k_tonemap_batch(const TonemapJob* __restrict__ jobs, int n_jobs, long long total) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_jobs - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].px0 <= g) lo = mid; else hi = mid - 1;
+        }
+        const TonemapJob& J = jobs[lo];
+        const size_t i = (size_t)(g - J.px0);
+        const float4 v = J.hist[i];
+        const double4 o = tonemap_px(J.a, J.lut, hist_count(J.a, v, i), hist_rgb(J.a, v, i));
+        reinterpret_cast<uchar4*>(J.out)[i] = quantise(o);
+    }
+}
+
 // 2x: tone map the four internal pixels of an output pixel, quantise each
 // to 8 bits, then the firefly clamp and box (supersample.rs:132-167).
 __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ hist, int wi, int ow, int oh, TonemapArgs A,
@@ -341,6 +358,11 @@ cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const Ton
     } else {
         return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long total_px, cudaStream_t s) {
+    k_tonemap_batch<<<148 * 16, 256, 0, s>>>(jobs, n_jobs, total_px);
     return cudaGetLastError();
 }
 

@@ -37,6 +37,18 @@ struct TonemapArgs {
 cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const TonemapArgs& a, const float* curve_lut,
                            uint8_t* out, float4* out_f, cudaStream_t s);
 
+// One flame of a batched tone map (ss 1): its histogram, output, size, the
+// first pixel's index in the batch's pixel sequence, its constants.
+struct TonemapJob {
+    const float4* hist;
+    uint8_t* out;
+    const float* lut;
+    long long px0;
+    int w, h;
+    TonemapArgs a;
+};
+cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long total_px, cudaStream_t s);
+
 // Density estimation table: entry c (counts 0..n-1, the last entry serving
 // every larger count): (max accepted d^2, 1/h^2, 1/normaliser, reach).
 // Computes output rows [y_lo, y_lo + h_out) into `out` (row y_lo first),

@@ -10,9 +10,9 @@ the import.  `Renderer` is the typed API underneath (include/ffb200.h).
 import json
 
 from ._module import Module, find_module
-from ._native import EngineError, Output, Renderer, make_job, specialize  # noqa: F401
+from ._native import Batch, EngineError, Output, Renderer, make_job, specialize  # noqa: F401
 
-__all__ = ["Engine", "Image", "Module", "EngineError", "Renderer", "specialize"]
+__all__ = ["Engine", "Image", "Module", "EngineError", "Renderer", "Batch", "specialize"]
 
 
 def _text(config):

@@ -25,7 +25,8 @@ EXPORTS = [
     "ffb_last_error", "ffb_version", "ffb_renderer_create", "ffb_renderer_destroy", "ffb_render",
     "ffb_render_device", "ffb_histogram", "ffb_tonemap", "ffb_density_estimate", "ffb_probe",
     "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench", "ffb_chaos_device", "ffb_hist_pack",
-    "ffb_hist_unpack", "ffb_finish_device", "ffb_histogram_u64",
+    "ffb_hist_unpack", "ffb_finish_device", "ffb_histogram_u64", "ffb_batch_create", "ffb_batch_run",
+    "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy",
 ]
 
 
@@ -265,6 +266,74 @@ class Renderer:
         ms = ctypes.c_double()
         _check(lib().ffb_atomic_bench(self._h, ctypes.c_uint32(pixels), ctypes.c_uint64(samples), ctypes.c_int32(kind), ctypes.byref(ms)))
         return ms.value
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [("config", ctypes.c_char_p), ("config_len", ctypes.c_size_t), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("iterations", ctypes.c_uint64), ("seed", ctypes.c_uint64)]
+
+
+class Batch:
+    """Many flames rendered by one persistent launch a structure group and
+    one batched tone map, captured as a CUDA graph (ffb_batch_*).
+
+    items: (config, width, height, samples[, seed]) tuples."""
+
+    def __init__(self, renderer, items, tune=True, **common):
+        self._r = renderer
+        self._texts = [_text(it[0]) for it in items]
+        arr = (BatchItem * len(items))()
+        for k, (it, t) in enumerate(zip(items, self._texts)):
+            arr[k].config, arr[k].config_len = t, len(t)
+            arr[k].width, arr[k].height, arr[k].iterations = it[1], it[2], int(it[3])
+            arr[k].seed = int(it[4]) if len(it) > 4 else 0
+        self._items = arr
+        self.sizes = [(it[1], it[2]) for it in items]
+        j = make_job(**common)
+        h = ctypes.c_void_p()
+        L = lib()
+        L.ffb_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.ffb_batch_destroy.restype = None
+        _check(L.ffb_batch_create(renderer._h, arr, ctypes.c_uint32(len(items)), ctypes.byref(j), ctypes.c_int32(1 if tune else 0),
+                                  ctypes.byref(h)))
+        self._h = h
+
+    def run(self, stream=None, sync=True):
+        """Replay the batch; the device milliseconds when `sync`."""
+        ms = ctypes.c_double()
+        _check(lib().ffb_batch_run(self._h, ctypes.c_void_p(stream or 0), ctypes.c_int32(1 if sync else 0),
+                                   ctypes.byref(ms) if sync else None))
+        return ms.value if sync else None
+
+    def output(self, index):
+        w, h = self.sizes[index]
+        out = np.zeros((h, w, 4), np.uint8)
+        plotted = ctypes.c_uint64()
+        _check(lib().ffb_batch_output(self._h, ctypes.c_uint32(index), _p(out, ctypes.c_uint8), ctypes.byref(plotted)))
+        return out, plotted.value
+
+    def info(self):
+        t, th, it, g = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().ffb_batch_info(self._h, ctypes.byref(t), ctypes.byref(th), ctypes.byref(it), ctypes.byref(g)))
+        return {"samples": t.value, "threads": th.value, "iterations_per_walker": it.value, "groups": g.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ffb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def walkers_for(samples, threads, iters):
+        """The walkers and per-walker iterations a batch gives a flame of `samples`."""
+        w = max(-(-samples // iters), threads)
+        w = -(-w // threads) * threads
+        return w, -(-samples // w)
 
 
 def specialize(config, rng="philox", math="precise"):

@@ -10,6 +10,9 @@ Shapes follow the benchmark's configuration list:
 * `full_flame`   -- 8 transforms + 1 final, each with 3-5 of the twelve
   variations at weights ~U[0,1], affines ~U[-1.5,1.5]; density estimation
   radius 9 -> 0.
+* `batch_flames` -- 256 flames for the batched renderer: transform counts
+  ~U{2..12}, variations as the plain flame, sizes ~{128,256,512,1024}^2,
+  budgets ~U[50,2000] samples a pixel, a seed each.
 """
 
 import numpy as np
@@ -77,3 +80,16 @@ def sierpinski():
                   "color_speed": 0.3, "variations": {"linear": 1.0}})
     return {"name": "sierpinski", "flame": {"transforms": t}, "render_mode": "TwoD", "deterministic_rng": True,
             "zoom": 1.0}
+
+
+def batch_flames(n=256, seed=3, spp=(50, 2000), sizes=(128, 256, 512, 1024)):
+    """(config, width, height, samples, seed) tuples."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        k = int(rng.integers(2, 13))
+        cfg = plain_flame(int(rng.integers(1, 2 ** 31)), n_xforms=k)
+        side = int(rng.choice(sizes))
+        samples = int(rng.uniform(*spp) * side * side)
+        out.append((cfg, side, side, samples, 1000 + i))
+    return out

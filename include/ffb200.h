@@ -178,6 +178,30 @@ int ffb_hist_unpack(ffb_renderer* r, const void* d_counts, const void* d_rgb, ui
 int ffb_finish_device(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, const void* d_hist,
                       uint64_t total_samples, uint32_t row0, uint32_t rows, void* d_rgba, void* stream);
 
+/* ---- batches: many flames in one persistent launch a structure group,
+ * tone-mapped in one launch, the device work captured as a CUDA graph.
+ * The batched addition beside the reference's one-flame render. */
+typedef struct {
+    const char* config;      /* .fae JSON */
+    size_t config_len;
+    uint32_t width, height;  /* output size (no supersampling in batches) */
+    uint64_t iterations;     /* this flame's plotted-sample budget */
+    uint64_t seed;           /* this flame's stream key (0: the config's) */
+} ffb_batch_item;
+typedef struct ffb_batch ffb_batch;
+/* Parse, specialise and upload every flame; with `tune`, time candidate
+ * (threads a block, iterations a walker) pairs on 1/64 of every budget and
+ * keep the fastest; capture the batch as a graph.  common: rng, math,
+ * burn_in, transparent, threads / iterations_per_thread (used when not tuning). */
+int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint32_t n, const ffb_job* common, int32_t tune,
+                     ffb_batch** out);
+/* Replay the batch (stream NULL: the renderer's).  `ms`: device time. */
+int ffb_batch_run(ffb_batch* b, void* stream, int32_t sync, double* ms);
+/* Item `index`'s RGBA8 (width*height*4 host bytes) and its plotted samples. */
+int ffb_batch_output(ffb_batch* b, uint32_t index, uint8_t* rgba, uint64_t* plotted);
+int ffb_batch_info(ffb_batch* b, uint64_t* total_samples, uint32_t* threads, uint32_t* iters_per_walker, uint32_t* groups);
+void ffb_batch_destroy(ffb_batch* b);
+
 /* Compile the chaos-game kernel of a config's structure for sm_100a with
  * NVRTC, without a device (the shader builder's build step,
  * src/shader_builder_v2.rs:2337; src/shader_cache.rs).  Writes the CUBIN

@@ -379,3 +379,39 @@ def test_exact_u64_counts_carry_past_2_32(renderer):
     entry = O.palette_table(cfg).reshape(-1, 3)[int(np.floor(np.float32(0.7) * 256))]
     mean = rgb[y, x].astype(np.float64) / n
     np.testing.assert_allclose(mean, entry, rtol=2e-6)
+
+
+def test_batch_matches_single_renders(renderer):
+    """A batch of flames of different transform counts and sizes, one
+    launch, graph-replayed: each flame's picture is the single render of the
+    same walkers and budget (the streams are keyed by walker and seed)."""
+    from ffb200 import Batch
+    items = synthetic.batch_flames(n=12, seed=5, spp=(20, 60), sizes=(64, 96, 128))
+    b = Batch(renderer, items, tune=False, threads=128, iterations_per_thread=256)
+    info = b.info()
+    assert info["groups"] == 1 and info["threads"] == 128
+    ms = b.run()
+    assert ms > 0
+    b.run()                                   # replays give the same pictures
+    for k, (cfg, w, h, samples, seed) in enumerate(items):
+        img, plotted = b.output(k)
+        walkers, per = Batch.walkers_for(samples, 128, 256)
+        assert plotted == walkers * per >= samples
+        ref, o = renderer.render(cfg, w, h, iterations=walkers * per, walkers=walkers, seed=seed, schedule="sorted",
+                                 threads=128)
+        assert o.total_iterations == plotted
+        d = np.abs(img.astype(int) - ref.astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 0.01, (k, d.max(), (d > 0).mean())
+    b.close()
+
+
+def test_batch_autotune_picks_a_candidate(renderer):
+    from ffb200 import Batch
+    items = synthetic.batch_flames(n=6, seed=9, spp=(20, 40), sizes=(64, 128))
+    b = Batch(renderer, items, tune=True)
+    info = b.info()
+    assert info["threads"] in (128, 256, 512) and info["iterations_per_walker"] in (256, 1024, 4096)
+    b.run()
+    img, _ = b.output(0)
+    assert (img[..., :3].max(axis=2) > 0).sum() > 0
+    b.close()
