@@ -45,8 +45,9 @@ std::string call(const VarDef* v, const std::string& prm0, const std::string& pr
 
 }  // namespace
 
-Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads, bool per_xform) {
+Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads, bool per_xform, bool exact) {
     Plan p;
+    p.exact = exact;
     p.rng_mode = rng_mode;
     p.math_mode = math_mode;
     p.per_xform = per_xform;
@@ -79,6 +80,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     s << "#define FFB_HAS_POST " << (p.has_post ? 1 : 0) << "\n#define FFB_NSLOTS " << p.n_slots << "\n";
     s << "#define FFB_RNG_MODE " << rng_mode << "\n#define FFB_THREADS " << threads << "\n";
     if (math_mode == MATH_SFU) s << "#define FFB_SFU 1\n";
+    if (exact) s << "#define FFB_EXACT 1\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
     s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw
       << "\n#define T_VP " << p.t_vp << "\n";
@@ -153,7 +155,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
 
 bool plan_fits(const Plan& p, const Flame& f) {
     if ((int)f.xf.size() > p.maxx) return false;
-    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform);
+    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform, p.exact);
     return q.source == p.source;
 }
 

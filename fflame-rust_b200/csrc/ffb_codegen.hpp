@@ -40,11 +40,13 @@ struct Plan {
     // no-instruction stalls 0.4 -> 1.7 a cycle), so off by default; the
     // union form is warp-uniform after the sorted schedule's regrouping.
     bool per_xform = false;
+    bool exact = false;                    // u64 fixed-point histogram (ulonglong4 a pixel)
     std::string source;                    // full NVRTC source (structure key)
 };
 
 // Structure of `f` (rng/math modes as given; maxx >= f.xf.size()).
-Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx = 0, int threads = 128, bool per_xform = false);
+Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx = 0, int threads = 128, bool per_xform = false,
+               bool exact = false);
 // The table of `f` for a plan made from a flame of the same structure.
 std::vector<float> make_table(const Plan& p, const Flame& f);
 // Whether `f` fits plan `p` (same structure, n_xf <= maxx).

@@ -6,7 +6,7 @@
 struct ffb_launch {
     const float* table;        // FFB_TABLE_SIZE floats
     const float4* palette;     // pal_n entries: linear rgb, 1
-    float4* hist;              // width*height: (r sum, g sum, b sum, count bits)
+    void* hist;                // width*height: float4 (r, g, b sums, count bits); exact mode: ulonglong4 (r, g, b, count)
     float4* walkers;           // n_walkers: (x, y, colour index, fuse bits)
     u64* counters;             // [0] in-frame splats
     u32 n_walkers, walker0, block0, n_xf;
@@ -45,31 +45,42 @@ __device__ __forceinline__ int ffb_palette_index(float ci, u32 n) {
 // adds n * colour and n once, so a hot pixel (an attractor's fixed point)
 // costs one atomic per warp instead of one per lane.  A lone lane adds
 // exactly what it would have alone.
-__device__ __forceinline__ void ffb_splat(float4* __restrict__ hist, u32 idx, float4 c, int pal_idx) {
-    float* p = reinterpret_cast<float*>(hist + idx);
+//
+// Exact mode (FFB_EXACT): the pixel is four u64 (r, g, b, count), colour in
+// 24-bit fixed point (round(c * 2^24) a sample): integer sums, exact to
+// 2^40 hits a pixel and independent of the order of the atomics.
+__device__ __forceinline__ void ffb_splat(void* __restrict__ hist_v, u32 idx, float4 c, int pal_idx) {
 #ifdef FFB_NO_AGGREGATION
-    atomicAdd(p + 0, c.x);
-    atomicAdd(p + 1, c.y);
-    atomicAdd(p + 2, c.z);
-    atomicAdd(reinterpret_cast<u32*>(p + 3), 1u);
+    const u32 n = 1u;
+    const bool lead = true;
 #else
     const unsigned live = __activemask();
     const unsigned long long key = ((unsigned long long)idx << 16) | (unsigned)pal_idx;
     const unsigned peers = __match_any_sync(live, key);
-    if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) {
-        const u32 n = __popc(peers);
-        if (n == 1u) {
-            atomicAdd(p + 0, c.x);
-            atomicAdd(p + 1, c.y);
-            atomicAdd(p + 2, c.z);
-        } else {
-            const float fn = (float)n;
-            atomicAdd(p + 0, fn * c.x);
-            atomicAdd(p + 1, fn * c.y);
-            atomicAdd(p + 2, fn * c.z);
-        }
-        atomicAdd(reinterpret_cast<u32*>(p + 3), n);
+    const bool lead = (threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1);
+    const u32 n = __popc(peers);
+#endif
+    if (!lead) return;
+#ifdef FFB_EXACT
+    unsigned long long* p = reinterpret_cast<unsigned long long*>(reinterpret_cast<ulonglong4*>(hist_v) + idx);
+    const unsigned long long nn = n;
+    atomicAdd(p + 0, nn * (unsigned long long)__float2uint_rn(c.x * 16777216.0f));
+    atomicAdd(p + 1, nn * (unsigned long long)__float2uint_rn(c.y * 16777216.0f));
+    atomicAdd(p + 2, nn * (unsigned long long)__float2uint_rn(c.z * 16777216.0f));
+    atomicAdd(p + 3, nn);
+#else
+    float* p = reinterpret_cast<float*>(reinterpret_cast<float4*>(hist_v) + idx);
+    if (n == 1u) {
+        atomicAdd(p + 0, c.x);
+        atomicAdd(p + 1, c.y);
+        atomicAdd(p + 2, c.z);
+    } else {
+        const float fn = (float)n;
+        atomicAdd(p + 0, fn * c.x);
+        atomicAdd(p + 1, fn * c.y);
+        atomicAdd(p + 2, fn * c.z);
     }
+    atomicAdd(reinterpret_cast<u32*>(p + 3), n);
 #endif
 }
 

@@ -122,7 +122,7 @@ struct ffb_renderer {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::mutex mu;
     std::list<Module> cache;     // most recent first
-    DevBuf hist, walkers, table, palette, counters, jobs, rgba, de_out, de_tab, lut, f_out, tmp_in, count64, rgb64;
+    DevBuf hist, walkers, table, palette, counters, jobs, rgba, de_out, de_tab, lut, f_out, tmp_in;
     uint64_t h2d = 0, d2h = 0;      // bytes copied by the current call
     uint32_t launches = 0;          // kernels launched by the current call
 
@@ -133,7 +133,7 @@ struct ffb_renderer {
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
         for (auto& m : cache) if (m.lib) cudaLibraryUnload(m.lib);
-        for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in, &count64, &rgb64}) b->release();
+        for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in}) b->release();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -251,7 +251,7 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     if (P.schedule > 2) fail(FFB_ERR_INVALID, "schedule must be 0 (auto), 1 (plain) or 2 (sorted)");
     P.count_bits = job->count_bits ? job->count_bits : 32;
     if (P.count_bits != 32 && P.count_bits != 64) fail(FFB_ERR_INVALID, "count_bits must be 32 or 64");
-    P.plan = make_plan(P.flame, P.rng, P.math, 0, (int)P.threads);
+    P.plan = make_plan(P.flame, P.rng, P.math, 0, 128, false, P.count_bits == 64);
     P.table = make_table(P.plan, P.flame);
     P.palette = palette_table(P.flame);
     return P;
@@ -338,8 +338,10 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
                float4* ext_hist = nullptr) {
     Module& m = r->module_for(P.plan.source);
     const size_t npx = (size_t)P.wi * P.hi;
-    float4* hist = ext_hist ? ext_hist : (float4*)r->hist.ensure(npx * sizeof(float4));
-    ck(cudaMemsetAsync(hist, 0, npx * sizeof(float4), s), "clear histogram");
+    // Exact mode: four u64 a pixel (ulonglong4); otherwise float4.
+    const size_t px_bytes = P.plan.exact ? 32 : 16;
+    float4* hist = ext_hist ? ext_hist : (float4*)r->hist.ensure(npx * px_bytes);
+    ck(cudaMemsetAsync(hist, 0, npx * px_bytes, s), "clear histogram");
     void* d_table = r->table.ensure(P.table.size() * 4);
     ck(cudaMemcpyAsync(d_table, P.table.data(), P.table.size() * 4, cudaMemcpyHostToDevice, s), "upload table");
     r->h2d += P.table.size() * 4;
@@ -368,20 +370,6 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     }
     const uint64_t total_iters = P.per_walker + P.burn_in;
     uint64_t chunk = 1ull << 16;
-    unsigned long long* c64 = nullptr;
-    double* rgb64 = nullptr;
-    if (P.count_bits == 64) {
-        // Exact accumulation past 2^32 hits: a launch splats at most 2^28
-        // samples into the u32 counts and FP32 sums, which are then folded
-        // into a u64 count plane and FP64 colour planes and cleared, so no
-        // FP32 partial sum grows long enough to lose its small terms.
-        chunk = std::min<uint64_t>(chunk, (1ull << 28) / P.walkers);
-        if (chunk == 0) fail(FFB_ERR_INVALID, "too many walkers for exact accumulation (at most 2^28)");
-        c64 = (unsigned long long*)r->count64.ensure(npx * 8);
-        rgb64 = (double*)r->rgb64.ensure(npx * 24);
-        ck(cudaMemsetAsync(c64, 0, npx * 8, s), "clear u64 counts");
-        ck(cudaMemsetAsync(rgb64, 0, npx * 24, s), "clear f64 sums");
-    }
     if (P.rng == RNG_PCG) {
         if (chunk < P.ipt) fail(FFB_ERR_INVALID, "the pcg stream's dispatch does not fit a launch");
         chunk = chunk / P.ipt * P.ipt;
@@ -411,10 +399,7 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         void* args[] = {&jp, &nj};
         ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch ffb_chaos");
         r->launches += 1;
-        if (c64) {
-            ck(launch_fold_counts(hist, c64, rgb64, npx, s), "fold counts");
-            r->launches += 1;
-        }
+
     }
     if (inframe_out) {
         ck(cudaMemcpyAsync(inframe_out, d_cnt, 8, cudaMemcpyDeviceToHost, s), "read counters");
@@ -425,7 +410,7 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
 // Density estimation of output rows [y_lo, y_lo + h_out) of a w x h
 // histogram into r->de_out (count as float; row y_lo first).
 float4* run_de(ffb_renderer* r, const float4* hist, uint32_t w, uint32_t h, double r_max, double r_min, double curve, cudaStream_t s,
-               uint32_t y_lo = 0, uint32_t h_out = 0, const unsigned long long* count64 = nullptr, const double* rgb64 = nullptr) {
+               uint32_t y_lo = 0, uint32_t h_out = 0, const ulonglong4* exact = nullptr) {
     if (h_out == 0) h_out = h - y_lo;
     int n = 0, radius = 0;
     std::vector<float> tab = de_table(r_max, r_min, curve, n, radius);
@@ -433,7 +418,7 @@ float4* run_de(ffb_renderer* r, const float4* hist, uint32_t w, uint32_t h, doub
     ck(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, s), "upload DE table");
     r->h2d += tab.size() * 4;
     float4* out = (float4*)r->de_out.ensure((size_t)w * h_out * sizeof(float4));
-    ck(launch_density_estimate(hist, count64, rgb64, (int)w, (int)h, d_tab, n, radius, (int)y_lo, (int)h_out, out, s), "density estimation");
+    ck(launch_density_estimate(hist, exact, (int)w, (int)h, d_tab, n, radius, (int)y_lo, (int)h_out, out, s), "density estimation");
     r->launches += 1;
     return out;
 }
@@ -453,18 +438,18 @@ void finish_device(ffb_renderer* r, const Prepared& P, const float4* hist, uint6
                    int transparent, void* d_rgba, cudaStream_t s) {
     const uint32_t ss = P.ss;
     const uint32_t y_lo = row0 * ss, h_band = rows * ss;
-    const float4* src = hist + (size_t)y_lo * P.wi;
+    const float4* src = P.plan.exact ? nullptr : hist + (size_t)y_lo * P.wi;
     bool count_f = false;
-    const unsigned long long* c64 = P.count_bits == 64 ? (const unsigned long long*)r->count64.p : nullptr;
-    const double* rgb64 = P.count_bits == 64 ? (const double*)r->rgb64.p : nullptr;
+    const ulonglong4* ex = P.plan.exact ? (const ulonglong4*)hist : nullptr;
+    if (ex) src = nullptr;
     if (P.flame.de.max_radius > 0.0f) {
-        src = run_de(r, hist, P.wi, P.hi, (double)P.flame.de.max_radius * ss, (double)P.flame.de.min_radius * ss,
-                     (double)P.flame.de.curve, s, y_lo, h_band, c64, rgb64);
+        src = run_de(r, ex ? nullptr : hist, P.wi, P.hi, (double)P.flame.de.max_radius * ss, (double)P.flame.de.min_radius * ss,
+                     (double)P.flame.de.curve, s, y_lo, h_band, ex);
         count_f = true;
     }
     const double sd = std::max((double)samples / ((double)P.wi * (double)P.hi), 1e-6);   // compute_kernel.rs:1796-1840
     TonemapArgs a = tonemap_args(P.flame, P.wi, P.hi, sd, transparent, count_f);
-    if (!count_f && c64) { a.count64 = c64 + (size_t)y_lo * P.wi; a.rgb64 = rgb64 + (size_t)y_lo * P.wi * 3; }
+    if (!count_f && ex) a.exact = ex + (size_t)y_lo * P.wi;
     const float* lut = upload_lut(r, P.flame, s);
     ck(launch_tonemap(src, (int)P.wi, (int)h_band, (int)ss, a, lut, (uint8_t*)d_rgba, nullptr, s), "tone map");
     r->launches += 1;
@@ -677,12 +662,13 @@ FFB_API int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t len, c
         uint64_t inframe = 0;
         run_chaos(r, P, r->stream, j.walker0, &inframe);
         const size_t npx = (size_t)P.wi * P.hi;
-        ck(cudaMemcpyAsync(counts, r->count64.p, npx * 8, cudaMemcpyDeviceToHost, r->stream), "readback");
-        std::vector<double> h(npx * 3);
-        if (rgb) ck(cudaMemcpyAsync(h.data(), r->rgb64.p, npx * 24, cudaMemcpyDeviceToHost, r->stream), "readback");
+        std::vector<unsigned long long> h(npx * 4);
+        ck(cudaMemcpyAsync(h.data(), r->hist.p, npx * 32, cudaMemcpyDeviceToHost, r->stream), "readback");
         ck(cudaStreamSynchronize(r->stream), "histogram");
-        if (rgb)
-            for (size_t i = 0; i < npx * 3; ++i) rgb[i] = (float)h[i];
+        for (size_t i = 0; i < npx; ++i) {
+            counts[i] = h[i * 4 + 3];
+            if (rgb) for (int q = 0; q < 3; ++q) rgb[i * 3 + q] = (float)((double)h[i * 4 + q] / 16777216.0);
+        }
         if (out) {
             *out = ffb_output{};
             out->width = P.wi; out->height = P.hi;

@@ -153,11 +153,15 @@ __device__ double4 tonemap_px(const TonemapArgs& A, const float* lut, double cnt
 
 __device__ __forceinline__ double hist_count(const TonemapArgs& A, const float4& v, size_t i) {
     if (A.count_is_float) return (double)v.w;
-    if (A.count64) return (double)A.count64[i];
+    if (A.exact) return (double)A.exact[i].w;
     return (double)__float_as_uint(v.w);
 }
 __device__ __forceinline__ D3 hist_rgb(const TonemapArgs& A, const float4& v, size_t i) {
-    if (A.rgb64 && !A.count_is_float) return D3{A.rgb64[3 * i], A.rgb64[3 * i + 1], A.rgb64[3 * i + 2]};
+    if (A.exact && !A.count_is_float) {
+        const ulonglong4 e = A.exact[i];
+        const double q = 1.0 / 16777216.0;
+        return D3{(double)e.x * q, (double)e.y * q, (double)e.z * q};
+    }
     return D3{v.x, v.y, v.z};
 }
 
@@ -173,7 +177,7 @@ __global__ void __launch_bounds__(256) k_tonemap1(const float4* __restrict__ his
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 v = hist[i];
+    const float4 v = A.exact && !A.count_is_float ? make_float4(0.f, 0.f, 0.f, 0.f) : hist[i];
     const double4 o = tonemap_px(A, lut, hist_count(A, v, (size_t)i), hist_rgb(A, v, (size_t)i));
     out[i] = quantise(o);
     if (out_f) out_f[i] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)o.w);
@@ -190,7 +194,7 @@ __global__ void __launch_bounds__(256) k_tonemap_batch(const TonemapJob* __restr
         }
         const TonemapJob& J = jobs[lo];
         const size_t i = (size_t)(g - J.px0);
-        const float4 v = J.hist[i];
+        const float4 v = J.a.exact && !J.a.count_is_float ? make_float4(0.f, 0.f, 0.f, 0.f) : J.hist[i];
         const double4 o = tonemap_px(J.a, J.lut, hist_count(J.a, v, i), hist_rgb(J.a, v, i));
         reinterpret_cast<uchar4*>(J.out)[i] = quantise(o);
     }
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const size_t idx = (size_t)(oy * 2 + dy[k]) * wi + (ox * 2 + dx[k]);
-        const float4 v = hist[idx];
+        const float4 v = A.exact && !A.count_is_float ? make_float4(0.f, 0.f, 0.f, 0.f) : hist[idx];
         const uchar4 q = quantise(tonemap_px(A, lut, hist_count(A, v, idx), hist_rgb(A, v, idx)));
         s[k][0] = q.x; s[k][1] = q.y; s[k][2] = q.z; s[k][3] = q.w;
         lum[k] = s[k][0] + 2.0f * s[k][1] + s[k][2];
@@ -246,8 +250,8 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
 // largest radius any staged source actually has (dense regions, where
 // every count is high, gather over a few pixels only).
 constexpr int DE_TX = 32, DE_TY = 16;
-__global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, const unsigned long long* __restrict__ count64,
-                                                           const double* __restrict__ rgb64, int w, int h, const float4* __restrict__ tab,
+__global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, const ulonglong4* __restrict__ exact,
+                                                           int w, int h, const float4* __restrict__ tab,
                                                            int tab_n, int R, int y_lo, int h_out, float4* __restrict__ out) {
     extern __shared__ float4 de_smem[];
     const int tw = DE_TX + 2 * R, th = DE_TY + 2 * R, n = tw * th;
@@ -264,13 +268,21 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
         float2 pr = make_float2(-1.0f, 0.0f);                              // empty: never accepted
         if (sx >= 0 && sy >= 0 && sx < w && sy < h) {
             const size_t si = (size_t)sy * w + sx;
-            const float4 hv = hist[si];
-            const unsigned long long c = count64 ? count64[si] : (unsigned long long)__float_as_uint(hv.w);
+            float4 hv;
+            unsigned long long c;
+            if (exact) {
+                const ulonglong4 q = exact[si];
+                c = q.w;
+                const double f = 1.0 / 16777216.0;
+                hv = make_float4((float)((double)q.x * f), (float)((double)q.y * f), (float)((double)q.z * f), 0.f);
+            } else {
+                hv = hist[si];
+                c = (unsigned long long)__float_as_uint(hv.w);
+            }
             if (c > 0ull) {
                 const float4 e = tab[c < (unsigned long long)(tab_n - 1) ? c : (unsigned long long)(tab_n - 1)];
                 const float cf = (float)c;
-                if (rgb64) v = make_float4((float)(rgb64[3 * si] * e.z), (float)(rgb64[3 * si + 1] * e.z), (float)(rgb64[3 * si + 2] * e.z), cf * e.z);
-                else v = make_float4(hv.x * e.z, hv.y * e.z, hv.z * e.z, cf * e.z);
+                v = make_float4(hv.x * e.z, hv.y * e.z, hv.z * e.z, cf * e.z);
                 pr = make_float2(e.x, 4.5f * e.y);
                 my_reach = max(my_reach, (int)e.w);
             }
@@ -297,18 +309,6 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
         }
     }
     out[(size_t)(py - y_lo) * w + px] = make_float4(ar, ag, ab, ac);
-}
-
-__global__ void k_fold(float4* __restrict__ hist, unsigned long long* __restrict__ count64, double* __restrict__ rgb64, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float4 v = hist[i];
-        const unsigned c = __float_as_uint(v.w);
-        if (c) {
-            count64[i] += c;
-            rgb64[3 * i] += (double)v.x; rgb64[3 * i + 1] += (double)v.y; rgb64[3 * i + 2] += (double)v.z;
-            hist[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    }
 }
 
 // Histogram planes for a collective: AoS (r, g, b, count bits) <-> a u32
@@ -366,7 +366,7 @@ cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long t
     return cudaGetLastError();
 }
 
-cudaError_t launch_density_estimate(const float4* hist, const unsigned long long* count64, const double* rgb64, int w, int h,
+cudaError_t launch_density_estimate(const float4* hist, const ulonglong4* exact, int w, int h,
                                     const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s) {
     const size_t smem = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius) * (sizeof(float4) + sizeof(float2));
     if (smem > 48 * 1024) {
@@ -374,12 +374,7 @@ cudaError_t launch_density_estimate(const float4* hist, const unsigned long long
         if (e != cudaSuccess) return e;
     }
     dim3 grid((w + DE_TX - 1) / DE_TX, (h_out + DE_TY - 1) / DE_TY);
-    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, count64, rgb64, w, h, table, table_n, radius, y_lo, h_out, out);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_fold_counts(float4* hist, unsigned long long* count64, double* rgb64, size_t n, cudaStream_t s) {
-    k_fold<<<148 * 8, 256, 0, s>>>(hist, count64, rgb64, n);
+    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, exact, w, h, table, table_n, radius, y_lo, h_out, out);
     return cudaGetLastError();
 }
 

@@ -17,8 +17,7 @@ struct TonemapArgs {
     int transparent;       // 0 opaque, 1 straight, 2 premultiplied
     int levels_enabled;
     int count_is_float;    // histogram .w holds a float count (after DE) instead of u32 bits
-    const unsigned long long* count64;   // if not null: the exact u64 counts (row-major, same pixels)
-    const double* rgb64;                 // if not null: the f64 colour sums (3 a pixel)
+    const ulonglong4* exact;             // if not null: the exact histogram (r, g, b in 2^-24, count), read instead
     float exposure, inv_gamma, density_scale;
     float ls_a;            // k1 / (prefilter_white * ln 10)
     float ls_b;            // white_level * k2
@@ -52,14 +51,10 @@ cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long t
 // Density estimation table: entry c (counts 0..n-1, the last entry serving
 // every larger count): (max accepted d^2, 1/h^2, 1/normaliser, reach).
 // Computes output rows [y_lo, y_lo + h_out) into `out` (row y_lo first),
-// reading sources from the whole w x h histogram (counts from `count64`
-// when given, else the u32 bits in .w).
-cudaError_t launch_density_estimate(const float4* hist, const unsigned long long* count64, const double* rgb64, int w, int h,
+// reading sources from the whole w x h histogram (`exact`, when given,
+// instead of `hist`).
+cudaError_t launch_density_estimate(const float4* hist, const ulonglong4* exact, int w, int h,
                                     const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s);
-
-// The exact accumulator (accumulate.wgsl:185-199): count64 += the u32
-// counts in hist's .w and rgb64 += its f32 colour sums; hist is cleared.
-cudaError_t launch_fold_counts(float4* hist, unsigned long long* count64, double* rgb64, size_t n, cudaStream_t s);
 
 // Histogram <-> (u32 count plane, f32 rgb plane), for collectives.
 cudaError_t launch_pack(const float4* hist, size_t n, unsigned* cnt, float* rgb, cudaStream_t s);

@@ -82,9 +82,10 @@ typedef struct {
     uint64_t seed;                     /* 0: the config's (12345 under deterministic_rng) */
     uint32_t walker0;                  /* first walker id of this shard (multi-GPU sharding) */
     uint32_t schedule;                 /* 0 auto, 1 one walker a thread, 2 transform-sorted (same orbits) */
-    uint32_t count_bits;               /* 32 (0) or 64: exact accumulation -- u32 counts and FP32 colour
-                                          sums folded every <= 2^28 samples into u64 counts and FP64
-                                          sums (accumulate.wgsl:185-199) */
+    uint32_t count_bits;               /* 32 (0): u32 count + FP32 colour sums (16 B a pixel); 64: exact
+                                          integer accumulation -- u64 count and u64 colour sums in 24-bit
+                                          fixed point (32 B a pixel), independent of the atomics' order
+                                          (the exact count of accumulate.wgsl:185-199) */
     uint32_t reserved;
 } ffb_job;
 
@@ -129,8 +130,8 @@ int ffb_render_device(ffb_renderer* r, const char* config, size_t config_len, co
 int ffb_histogram(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
                   uint32_t* counts, float* rgb, ffb_output* out);
 
-/* The same with exact u64 counts (job->count_bits taken as 64): counts is
- * w*h u64 hits. */
+/* The same in exact mode (job->count_bits taken as 64): counts is w*h u64
+ * hits, rgb the colour sums (f32 of the exact fixed-point sums). */
 int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
                       uint64_t* counts, float* rgb, ffb_output* out);
 
