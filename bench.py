@@ -41,6 +41,11 @@ def workload(name):
                     iterations=1_000_000_000, walkers=65536,
                     desc="8 xforms + final, 12 variations, 1920x1080 ss2 (3840x2160 internal), 1e9 samples, "
                          "65536 walkers, DE radius 9->0, u32 count + FP32 RGB histogram")
+    if name == "stress_4k":
+        return dict(cfg=synthetic.stress_flame(21), width=3840, height=2160, supersample=2,
+                    iterations=10_000_000_000, walkers=0, count_bits=64,
+                    desc="16 xforms (6 rotations by k*60 deg), 3840x2160 ss2 (7680x4320 internal), 1e10 samples, "
+                         "exact u64 count + u64 fixed-point RGB, DE radius 12->0")
     if name == "plain_256":
         return dict(cfg=synthetic.plain_flame(1), width=256, height=256, supersample=1, iterations=10_000_000,
                     walkers=16384, desc="3 xforms {linear,sinusoidal,spherical}, 256x256 ss1, 1e7 samples, no DE")
@@ -156,7 +161,7 @@ def run_ours(args, rank, world, local_rank):
     W, H, ss = wl["width"], wl["height"], wl["supersample"]
     r = _native.Renderer(local_rank)
     job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, walker0=rank * wl["walkers"],
-               seed=0x5EED + 0, schedule=args.schedule, math=args.math)
+               seed=0x5EED + 0, schedule=args.schedule, math=args.math, count_bits=wl.get("count_bits", 32))
     d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
     # The library's kernels and the timing events share one (non-default) stream.
     side = torch.cuda.Stream()
@@ -210,12 +215,20 @@ def run_ours(args, rank, world, local_rank):
 
     # Dominant kernel: the chaos game alone (events around its launch).
     chaos_ms, inframe = [], []
+    exact = wl.get("count_bits", 32) == 64
     for _ in range(3):
-        _, _, o = r.histogram(cfg, W, H, **job)
-        chaos_ms.append(o.render_time_ms)
+        if exact:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            _, _, o = r.histogram_u64(cfg, W, H, **job)
+            chaos_ms.append(o.render_time_ms or 0.0)
+        else:
+            _, _, o = r.histogram(cfg, W, H, **job)
+            chaos_ms.append(o.render_time_ms)
         inframe.append(o.inframe_samples)
-    c_ms = statistics.median(chaos_ms)
-    bytes_per_launch = 16.0 * statistics.median(inframe)          # 4 x 4-byte RMW per splatted sample
+    c_ms = statistics.median(chaos_ms) or ms
+    # 4 read-modify-writes per splatted sample: 4 B each (u32 count + FP32
+    # colour), or 8 B each in exact mode (u64 count + u64 fixed-point colour).
+    bytes_per_launch = (32.0 if exact else 16.0) * statistics.median(inframe)
     peaks, peak_kind = measured_peaks()
     achieved = bytes_per_launch / (c_ms * 1e-3) / 1e9
     traffic = profile_traffic(args.workload)
@@ -233,7 +246,7 @@ def run_ours(args, rank, world, local_rank):
     info = None
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        image = eng.render(cfg, W, H, iterations=req_iters, supersample=ss, walkers=wl["walkers"])
+        image = eng.render(cfg, W, H, iterations=req_iters, supersample=ss, walkers=wl["walkers"], exact=exact)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)
@@ -367,7 +380,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256", "batched_256"])
+    ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256", "batched_256", "stress_4k"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--math", default="precise", choices=["precise", "sfu"],
                     help="precise: IEEE-accurate sin/cos (the parity-tested path); sfu: the hardware's, as the reference GPU")

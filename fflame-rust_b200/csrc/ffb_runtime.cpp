@@ -540,6 +540,7 @@ void fae_dispatch(const Json& r, std::vector<uint8_t>& out, std::string& info) {
         job.supersample = (uint32_t)r.number_or("supersample", 1.0);
         job.rng = (int32_t)r.number_or("rng", -1.0);
         job.walkers = (uint32_t)r.number_or("walkers", 0.0);
+        job.count_bits = r.bool_or("exact", false) ? 64 : 32;
         ffb_renderer* R = fae_renderer();
         std::lock_guard<std::mutex> lk(R->mu);
         R->begin();
@@ -660,7 +661,9 @@ FFB_API int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t len, c
         Prepared P = prepare(config, len, &j);
         r->reset_counts();
         uint64_t inframe = 0;
+        ck(cudaEventRecord(r->ev0, r->stream), "event");
         run_chaos(r, P, r->stream, j.walker0, &inframe);
+        ck(cudaEventRecord(r->ev1, r->stream), "event");
         const size_t npx = (size_t)P.wi * P.hi;
         std::vector<unsigned long long> h(npx * 4);
         ck(cudaMemcpyAsync(h.data(), r->hist.p, npx * 32, cudaMemcpyDeviceToHost, r->stream), "readback");
@@ -671,9 +674,12 @@ FFB_API int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t len, c
         }
         if (out) {
             *out = ffb_output{};
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, r->ev0, r->ev1);
             out->width = P.wi; out->height = P.hi;
             out->total_iterations = (uint64_t)P.walkers * P.per_walker;
             out->inframe_samples = inframe;
+            out->render_time_ms = ms;
             r->fill_counts(out);
         }
     });
@@ -908,6 +914,12 @@ struct BatchFlame {
     size_t hist_off = 0, walk_off = 0, rgba_off = 0, tab_off = 0, pal_off = 0;
 };
 
+struct BatchDe {
+    size_t flame = 0, off = 0;
+    int n = 0, radius = 0;
+    std::vector<float> table;
+};
+
 struct BatchGroup {
     Module* mod = nullptr;
     std::string src;
@@ -922,9 +934,10 @@ struct ffb_batch {
     ffb_renderer* r = nullptr;
     std::vector<BatchFlame> flames;
     std::vector<BatchGroup> groups;
-    DevBuf hist, walk, rgba, tables, palettes, counters, launches, tjobs, luts;
+    DevBuf hist, walk, rgba, tables, palettes, counters, launches, tjobs, luts, de, detab;
     uint32_t threads = 256, iters = 1024;
     uint64_t total_samples = 0;
+    std::vector<BatchDe> de_tabs;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int rng = RNG_PHILOX, transparent = 0;
@@ -933,7 +946,7 @@ struct ffb_batch {
         groups.clear();
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        for (DevBuf* b : {&hist, &walk, &rgba, &tables, &palettes, &counters, &launches, &tjobs, &luts}) b->release();
+        for (DevBuf* b : {&hist, &walk, &rgba, &tables, &palettes, &counters, &launches, &tjobs, &luts, &de, &detab}) b->release();
     }
 };
 
@@ -1008,21 +1021,52 @@ void batch_enqueue(ffb_batch* B, uint32_t threads, uint32_t iters, uint64_t scal
         r->launches += 1;
     }
     if (!tonemap) return;
+    // Density estimation, flame by flame, into the DE arena (same layout as
+    // the histograms); the tone map then reads the float counts there.
+    if (upload) {
+        B->de_tabs.clear();
+        for (size_t j = 0; j < B->flames.size(); ++j) {
+            const Flame& fl = B->flames[j].P.flame;
+            if (fl.de.max_radius <= 0.0f) continue;
+            BatchDe d;
+            d.flame = j;
+            const uint32_t ss = B->flames[j].P.ss;
+            d.table = de_table((double)fl.de.max_radius * ss, (double)fl.de.min_radius * ss, (double)fl.de.curve, d.n, d.radius);
+            B->de_tabs.push_back(std::move(d));
+        }
+        size_t tab_floats = 0;
+        for (auto& d : B->de_tabs) { d.off = tab_floats; tab_floats += d.table.size(); }
+        std::vector<float> all_tabs(tab_floats);
+        for (auto& d : B->de_tabs) std::copy(d.table.begin(), d.table.end(), all_tabs.begin() + d.off);
+        if (tab_floats) {
+            ck(cudaMemcpyAsync(B->detab.ensure(tab_floats * 4), all_tabs.data(), tab_floats * 4, cudaMemcpyHostToDevice, s), "upload DE tables");
+            B->de.ensure(hist_bytes);
+        }
+    }
+    for (auto& d : B->de_tabs) {
+        BatchFlame& F = B->flames[d.flame];
+        ck(launch_density_estimate((const float4*)B->hist.p + F.hist_off, nullptr, (int)F.P.wi, (int)F.P.hi,
+                                   (const float4*)((const float*)B->detab.p + d.off), d.n, d.radius, 0, (int)F.P.hi,
+                                   (float4*)B->de.p + F.hist_off, s), "batch density estimation");
+        r->launches += 1;
+    }
     std::vector<TonemapJob> tj;
     long long px = 0;
     for (size_t j = 0; j < B->flames.size(); ++j) {
         BatchFlame& F = B->flames[j];
+        const bool has_de = F.P.flame.de.max_radius > 0.0f;
         TonemapJob J{};
-        J.hist = (const float4*)B->hist.p + F.hist_off;
+        J.hist = (const float4*)(has_de ? B->de.p : B->hist.p) + F.hist_off;
         J.out = (uint8_t*)B->rgba.p + F.rgba_off;
         J.lut = (const float*)B->luts.p + 256 * j;
         J.px0 = px;
         J.w = (int)F.P.wi; J.h = (int)F.P.hi;
+        J.ss = (int)F.P.ss;
         const uint64_t plotted = (uint64_t)F.walkers * F.per_walker;
         const double sd = std::max((double)plotted / ((double)F.P.wi * (double)F.P.hi), 1e-6);
-        J.a = tonemap_args(F.P.flame, F.P.wi, F.P.hi, sd, B->transparent, false);
+        J.a = tonemap_args(F.P.flame, F.P.wi, F.P.hi, sd, B->transparent, has_de);
         tj.push_back(J);
-        px += (long long)F.P.wi * F.P.hi;
+        px += (long long)(F.P.wi / F.P.ss) * (F.P.hi / F.P.ss);
     }
     TonemapJob* d_tj = (TonemapJob*)B->tjobs.ensure(tj.size() * sizeof(TonemapJob));
     if (upload) ck(cudaMemcpyAsync(d_tj, tj.data(), tj.size() * sizeof(TonemapJob), cudaMemcpyHostToDevice, s), "upload tone-map jobs");
@@ -1050,10 +1094,10 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
         for (uint32_t i = 0; i < n; ++i) {
             ffb_job j = *common;
             j.width = items[i].width; j.height = items[i].height; j.iterations = items[i].iterations;
-            j.seed = items[i].seed; j.supersample = 1;
+            j.seed = items[i].seed;
             if (j.iterations == 0) fail(FFB_ERR_INVALID, "every batch item needs its sample budget");
             B->flames[i].P = prepare(items[i].config, items[i].config_len, &j);
-            if (B->flames[i].P.flame.de.max_radius > 0.0f) fail(FFB_ERR_INVALID, "density estimation is not available in batches");
+            check_de(B->flames[i].P.flame, B->flames[i].P.ss);
             B->flames[i].budget = j.iterations;
             maxx = std::max<int>(maxx, (int)B->flames[i].P.flame.xf.size());
         }
@@ -1077,7 +1121,7 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
             G.members.push_back(i);
             G.max_pal = std::max<int>(G.max_pal, (int)(F.P.palette.size() / 4));
             F.hist_off = hist_px; hist_px += (size_t)F.P.wi * F.P.hi;
-            F.rgba_off = rgba_bytes; rgba_bytes += (size_t)F.P.wi * F.P.hi * 4;
+            F.rgba_off = rgba_bytes; rgba_bytes += (size_t)(F.P.wi / F.P.ss) * (F.P.hi / F.P.ss) * 4;
             F.tab_off = tab_floats; tab_floats += (F.P.table.size() + 3) / 4 * 4;
             F.pal_off = pal_floats; pal_floats += F.P.palette.size();
             B->total_samples += F.budget;
@@ -1166,7 +1210,8 @@ FFB_API int ffb_batch_output(ffb_batch* b, uint32_t index, uint8_t* rgba, uint64
         r->begin();
         const BatchFlame& F = b->flames[index];
         if (rgba) {
-            ck(cudaMemcpyAsync(rgba, (uint8_t*)b->rgba.p + F.rgba_off, (size_t)F.P.wi * F.P.hi * 4, cudaMemcpyDeviceToHost, r->stream), "readback");
+            const size_t bytes = (size_t)(F.P.wi / F.P.ss) * (F.P.hi / F.P.ss) * 4;
+            ck(cudaMemcpyAsync(rgba, (uint8_t*)b->rgba.p + F.rgba_off, bytes, cudaMemcpyDeviceToHost, r->stream), "readback");
             ck(cudaStreamSynchronize(r->stream), "readback");
         }
         if (plotted) *plotted = (uint64_t)F.walkers * F.per_walker;

@@ -183,33 +183,9 @@ __global__ void __launch_bounds__(256) k_tonemap1(const float4* __restrict__ his
     if (out_f) out_f[i] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)o.w);
 }
 
-// Many flames in one launch: a grid-stride over the concatenated pixels of
-// every flame, each pixel finding its flame by binary search over px0.
-__global__ void __launch_bounds__(256) k_tonemap_batch(const TonemapJob* __restrict__ jobs, int n_jobs, long long total) {
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
-        int lo = 0, hi = n_jobs - 1;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (jobs[mid].px0 <= g) lo = mid; else hi = mid - 1;
-        }
-        const TonemapJob& J = jobs[lo];
-        const size_t i = (size_t)(g - J.px0);
-        const float4 v = J.a.exact && !J.a.count_is_float ? make_float4(0.f, 0.f, 0.f, 0.f) : J.hist[i];
-        const double4 o = tonemap_px(J.a, J.lut, hist_count(J.a, v, i), hist_rgb(J.a, v, i));
-        reinterpret_cast<uchar4*>(J.out)[i] = quantise(o);
-    }
-}
-
 // 2x: tone map the four internal pixels of an output pixel, quantise each
 // to 8 bits, then the firefly clamp and box (supersample.rs:132-167).
-__global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ hist, int wi, int ow, int oh, TonemapArgs A,
-                                                  const float* __restrict__ lut_g, uchar4* __restrict__ out) {
-    __shared__ float lut[256];
-    lut[threadIdx.x] = lut_g[threadIdx.x];
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ow * oh) return;
-    const int ox = i % ow, oy = i / ow;
+__device__ __forceinline__ uchar4 tonemap2_px(const TonemapArgs& A, const float* lut, const float4* __restrict__ hist, int wi, int ox, int oy) {
     float s[4][4], lum[4];
     const int dx[4] = {0, 1, 0, 1}, dy[4] = {0, 0, 1, 1};
 #pragma unroll
@@ -238,7 +214,39 @@ __global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ his
     unsigned char r[4];
 #pragma unroll
     for (int c2 = 0; c2 < 4; ++c2) r[c2] = (unsigned char)clampf(roundf(acc[c2] * 0.25f), 0.f, 255.f);
-    out[i] = make_uchar4(r[0], r[1], r[2], r[3]);
+    return make_uchar4(r[0], r[1], r[2], r[3]);
+}
+
+__global__ void __launch_bounds__(256) k_tonemap2(const float4* __restrict__ hist, int wi, int ow, int oh, TonemapArgs A,
+                                                  const float* __restrict__ lut_g, uchar4* __restrict__ out) {
+    __shared__ float lut[256];
+    lut[threadIdx.x] = lut_g[threadIdx.x];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ow * oh) return;
+    out[i] = tonemap2_px(A, lut, hist, wi, i % ow, i / ow);
+}
+
+// Many flames in one launch: a grid-stride over the concatenated OUTPUT
+// pixels of every flame, each finding its flame by binary search over px0.
+__global__ void __launch_bounds__(256) k_tonemap_batch(const TonemapJob* __restrict__ jobs, int n_jobs, long long total) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total; g += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_jobs - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (jobs[mid].px0 <= g) lo = mid; else hi = mid - 1;
+        }
+        const TonemapJob& J = jobs[lo];
+        const size_t i = (size_t)(g - J.px0);
+        if (J.ss == 2) {
+            const int ow = J.w / 2;
+            reinterpret_cast<uchar4*>(J.out)[i] = tonemap2_px(J.a, J.lut, J.hist, J.w, (int)(i % ow), (int)(i / ow));
+        } else {
+            const float4 v = J.a.exact && !J.a.count_is_float ? make_float4(0.f, 0.f, 0.f, 0.f) : J.hist[i];
+            const double4 o = tonemap_px(J.a, J.lut, hist_count(J.a, v, i), hist_rgb(J.a, v, i));
+            reinterpret_cast<uchar4*>(J.out)[i] = quantise(o);
+        }
+    }
 }
 
 // Density estimation, gather form: output pixel p sums, over sources q in

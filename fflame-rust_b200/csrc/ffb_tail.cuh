@@ -36,14 +36,15 @@ struct TonemapArgs {
 cudaError_t launch_tonemap(const float4* hist, int wi, int hi, int ss, const TonemapArgs& a, const float* curve_lut,
                            uint8_t* out, float4* out_f, cudaStream_t s);
 
-// One flame of a batched tone map (ss 1): its histogram, output, size, the
-// first pixel's index in the batch's pixel sequence, its constants.
+// One flame of a batched tone map: its histogram, output, size, the first
+// output pixel's index in the batch's pixel sequence, its constants.
 struct TonemapJob {
-    const float4* hist;
-    uint8_t* out;
+    const float4* hist;        // internal-resolution histogram (or DE output)
+    uint8_t* out;              // output RGBA8
     const float* lut;
-    long long px0;
-    int w, h;
+    long long px0;             // first OUTPUT pixel's index in the batch
+    int w, h;                  // internal size
+    int ss;                    // 1, or 2 (fused firefly downsample)
     TonemapArgs a;
 };
 cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long total_px, cudaStream_t s);

@@ -68,14 +68,16 @@ class Engine:
         return {v["name"]: v["params"] for v in self._data({"fn": "variations"})}
 
     def render(self, config, width, height, *, iterations=None, iterations_per_thread=None,
-               transparent=False, premultiplied=False, sticky=False, sequence=False, supersample=None, walkers=None):
+               transparent=False, premultiplied=False, sticky=False, sequence=False, supersample=None, walkers=None,
+               exact=False):
         """A config (dict, JSON, or a path) at `width` x `height` (python/pyfae/__init__.py:201-221).
 
         `iterations`: the flame's budget (default: the config's own).
         `iterations_per_thread`: default the CLI's, 1024.  `supersample` 2
         renders at twice the size and boxes it down with the firefly clamp;
         `walkers` fixes the number of concurrent orbits (default: sized to
-        the budget).
+        the budget); `exact` accumulates u64 counts and fixed-point colour
+        sums (long renders, order-independent results).
         """
         text = _text(config)
         request = {"fn": "render", "config": text, "width": width, "height": height,
@@ -89,5 +91,7 @@ class Engine:
             request["supersample"] = int(supersample)
         if walkers:
             request["walkers"] = int(walkers)
+        if exact:
+            request["exact"] = True
         out, info = self._call(request)
         return Image(self, out, info, text)

@@ -10,6 +10,9 @@ Shapes follow the benchmark's configuration list:
 * `full_flame`   -- 8 transforms + 1 final, each with 3-5 of the twelve
   variations at weights ~U[0,1], affines ~U[-1.5,1.5]; density estimation
   radius 9 -> 0.
+* `stress_flame` -- 16 transforms: 10 as the full flame's plus 6 rotations
+  by k*60 degrees (6-fold rotational symmetry as ordinary transforms);
+  density estimation radius 12 -> 0.
 * `batch_flames` -- 256 flames for the batched renderer: transform counts
   ~U{2..12}, variations as the plain flame, sizes ~{128,256,512,1024}^2,
   budgets ~U[50,2000] samples a pixel, a seed each.
@@ -93,3 +96,17 @@ def batch_flames(n=256, seed=3, spp=(50, 2000), sizes=(128, 256, 512, 1024)):
         samples = int(rng.uniform(*spp) * side * side)
         out.append((cfg, side, side, samples, 1000 + i))
     return out
+
+
+def stress_flame(seed=21, de_radius=12.0):
+    """The 4K stress flame: 10 random transforms + 6 rotation transforms."""
+    import math
+    base = full_flame(seed, n_xforms=10, de_radius=de_radius)
+    rng = np.random.default_rng(seed + 1)
+    for k in range(6):
+        th = k * math.pi / 3.0
+        base["flame"]["transforms"].append({
+            "a": math.cos(th), "b": -math.sin(th), "c": math.sin(th), "d": math.cos(th), "e": 0.0, "f": 0.0,
+            "weight": 0.5, "color": float(rng.uniform(0, 1)), "color_speed": 0.5, "variations": {"linear": 1.0}})
+    base["name"] = f"stress-{seed}"
+    return base
