@@ -740,6 +740,21 @@ FFB_API int ffb_density_estimate(ffb_renderer* r, const uint32_t* counts, const 
     });
 }
 
+FFB_API int ffb_density_estimate_static(const void* d_hist, uint32_t w, uint32_t h, float max_radius, float min_radius,
+                                        float curve, void* d_out, void* stream) {
+    return guard([&] {
+        if (!d_hist || !d_out) fail(FFB_ERR_INVALID, "NULL argument");
+        if (w == 0 || h == 0 || w > 65536 || h > 65536) fail(FFB_ERR_INVALID, "histogram size must be 1..65536 on each side");
+        if (max_radius <= 0.f || max_radius > 36.f || min_radius < 0.f || curve < 0.f) fail(FFB_ERR_INVALID, "bad DE parameters");
+        if (de_static_entries(max_radius, min_radius, curve) < 0)
+            fail(FFB_ERR_TOO_LARGE, "density estimation table needs more than " + std::to_string(kDeStaticEntries) +
+                                        " entries, the static scratch's size: raise min_radius or curve");
+        ck(density_estimate_static((const float4*)d_hist, (int)w, (int)h, max_radius, min_radius, curve, (float4*)d_out,
+                                   (cudaStream_t)stream),
+           "density estimation (static scratch)");
+    });
+}
+
 FFB_API int ffb_probe(ffb_renderer* r, const char* config, size_t len, const float* pts, uint32_t npts, int32_t math, float* out,
                       uint32_t out_pairs) {
     return guard([&] {

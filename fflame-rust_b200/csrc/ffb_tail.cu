@@ -14,6 +14,10 @@
 
 #include "ffb_tail.cuh"
 
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
 namespace ffb {
 
 namespace {
@@ -399,6 +403,113 @@ cudaError_t launch_unpack(const unsigned* cnt, const float* rgb, size_t n, float
 cudaError_t launch_atomic_bench(uint32_t* buf, uint32_t n_pixels, uint64_t n_samples, int kind, int blocks, cudaStream_t s) {
     k_atomic_bench<<<blocks, 256, 0, s>>>(buf, n_pixels, n_samples, kind);
     return cudaGetLastError();
+}
+
+// ---- density estimation without allocation ---------------------------------
+//
+// Some callers cannot allocate device memory while they render. Examples: an
+// application that hands the whole device to its own memory pool and must
+// account for every byte; a host framework whose allocator must not be bypassed;
+// a frame loop that has fixed its memory at start-up and may not grow it.
+// The density-estimation gather needs one buffer besides its input and output:
+// the weight table. This variant keeps that table in a file-scope device array
+// with a fixed maximum, not in memory allocated per call.
+//
+// * The array holds kDeStaticEntries entries (1 MiB). A table that needs more
+//   is refused before any work is queued. The table's length grows as
+//   max_radius^(1/curve); min_radius > 0 shortens it.
+// * Set-up: the first call on a device, with that device current, looks up
+//   the array's device address (cudaGetSymbolAddress) and keeps it for later
+//   calls on that device. That first call should come before any stream
+//   capture.
+// * Every call on a device shares the one array. Calls whose work overlaps on
+//   the GPU race on it: two streams, or a call queued while another's DE
+//   kernel has not yet run. Order them on one stream or with events.
+// * Nothing in the array has to start at zero: each call writes every entry
+//   its DE kernel reads, earlier on the same stream.
+// * The table is computed on the host, in the same double arithmetic as the
+//   allocating path. It reaches the device in launch parameters (chunks of
+//   kDeChunk entries), so no memcpy or staging buffer is involved.
+
+static __device__ __align__(256) float4 g_de_scratch[kDeStaticEntries];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+constexpr int kDeChunk = 1024;                 // 16 KiB of launch parameters a chunk
+
+struct DeChunk { float4 e[kDeChunk]; };
+
+__global__ void k_de_store(const __grid_constant__ DeChunk c, int n, float4* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = c.e[i];
+}
+
+std::mutex g_de_static_mu;
+float4* g_de_static_ptr[kMaxDevices] = {};
+
+cudaError_t de_static_scratch(float4** out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_de_static_mu);
+    if (!g_de_static_ptr[dev]) {
+        float4* ptr = nullptr;
+        e = cudaGetSymbolAddress((void**)&ptr, g_de_scratch);
+        if (e != cudaSuccess) return e;
+        g_de_static_ptr[dev] = ptr;
+    }
+    *out = g_de_static_ptr[dev];
+    return cudaSuccess;
+}
+
+// Entry c of the DE table: (max accepted d^2, 1/h^2, 1/normaliser, reach),
+// h(c) = max(min_radius, max_radius / c^curve), weights exp(-4.5 d^2 / h^2)
+// over integer offsets with d^2 <= h^2; count 0 has no disc.
+float4 de_entry(int c, double r_max, double r_min, double curve) {
+    const double h = c == 0 ? 0.0 : std::max(r_min, r_max / std::pow((double)c, curve));
+    const double h2 = h * h;
+    const double dmax2 = c == 0 ? -1.0 : std::floor(h2);
+    const int rr = (int)std::floor(std::sqrt(std::max(dmax2, 0.0)));
+    double norm = 0.0;
+    for (int dy = -rr; dy <= rr; ++dy)
+        for (int dx = -rr; dx <= rr; ++dx) {
+            const double d2 = dx * dx + dy * dy;
+            if (d2 <= h2) norm += std::exp(-4.5 * d2 / h2);
+        }
+    if (c == 0) norm = 1.0;
+    return make_float4((float)dmax2, h2 > 0 ? (float)(1.0 / h2) : 0.0f, (float)(1.0 / norm), (float)rr);
+}
+
+}  // namespace
+
+int de_static_entries(double r_max, double r_min, double curve) {
+    // Entries 0..c; the table ends at the first c >= 1 whose disc is below a
+    // pixel or at the minimum radius (every larger count shares it).
+    for (int c = 1;; ++c) {
+        const double h = std::max(r_min, r_max / std::pow((double)c, curve));
+        if (h < 1.0 || h <= r_min) return c + 1;
+        if (c + 2 > kDeStaticEntries) return -1;
+    }
+}
+
+cudaError_t density_estimate_static(const float4* hist, int w, int h, double r_max, double r_min, double curve,
+                                    float4* out, cudaStream_t s) {
+    const int n = de_static_entries(r_max, r_min, curve);
+    if (n < 0) return cudaErrorInvalidValue;
+    float4* tab = nullptr;
+    cudaError_t e = de_static_scratch(&tab);
+    if (e != cudaSuccess) return e;
+    DeChunk chunk;
+    for (int c0 = 0; c0 < n; c0 += kDeChunk) {
+        const int m = std::min(kDeChunk, n - c0);
+        for (int j = 0; j < m; ++j) chunk.e[j] = de_entry(c0 + j, r_max, r_min, curve);
+        k_de_store<<<(m + 255) / 256, 256, 0, s>>>(chunk, m, tab + c0);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return launch_density_estimate(hist, nullptr, w, h, tab, n, (int)std::floor(r_max), 0, h, out, s);
 }
 
 }  // namespace ffb

@@ -57,6 +57,15 @@ cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long t
 cudaError_t launch_density_estimate(const float4* hist, const ulonglong4* exact, int w, int h,
                                     const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s);
 
+// Density estimation of all w x h rows with the weight table in a file-scope
+// device array of kDeStaticEntries entries instead of allocated memory (the
+// contract is at its definition in ffb_tail.cu). de_static_entries: the
+// table's length for these radii, or -1 when it exceeds the array.
+constexpr int kDeStaticEntries = 65536;
+int de_static_entries(double r_max, double r_min, double curve);
+cudaError_t density_estimate_static(const float4* hist, int w, int h, double r_max, double r_min, double curve,
+                                    float4* out, cudaStream_t s);
+
 // Histogram <-> (u32 count plane, f32 rgb plane), for collectives.
 cudaError_t launch_pack(const float4* hist, size_t n, unsigned* cnt, float* rgb, cudaStream_t s);
 cudaError_t launch_unpack(const unsigned* cnt, const float* rgb, size_t n, float4* hist, cudaStream_t s);

@@ -26,7 +26,7 @@ EXPORTS = [
     "ffb_render_device", "ffb_histogram", "ffb_tonemap", "ffb_density_estimate", "ffb_probe",
     "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench", "ffb_chaos_device", "ffb_hist_pack",
     "ffb_hist_unpack", "ffb_finish_device", "ffb_histogram_u64", "ffb_batch_create", "ffb_batch_run",
-    "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy",
+    "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
 ]
 
 
@@ -344,3 +344,13 @@ def specialize(config, rng="philox", math="precise"):
     _check(lib().ffb_specialize(cfg, ctypes.c_size_t(len(cfg)), ctypes.c_int32(RNG[rng]), ctypes.c_int32(MATH[math]),
                                 ctypes.byref(n), buf, ctypes.c_size_t(len(buf))))
     return n.value, buf.value.decode()
+
+
+def density_estimate_static(d_hist, width, height, max_radius, min_radius=0.0, curve=0.4, d_out=0, stream=None):
+    """Density estimation of a device histogram (int pointer to width*height
+    float4) into `d_out` (the same layout, counts as f32) that allocates
+    nothing: the weight table lives in a fixed device array shared by every
+    call on the device (ffb_density_estimate_static).  Queued on `stream`."""
+    _check(lib().ffb_density_estimate_static(ctypes.c_void_p(d_hist), ctypes.c_uint32(width), ctypes.c_uint32(height),
+                                             ctypes.c_float(max_radius), ctypes.c_float(min_radius), ctypes.c_float(curve),
+                                             ctypes.c_void_p(d_out), ctypes.c_void_p(stream or 0)))

@@ -149,6 +149,22 @@ int ffb_tonemap(ffb_renderer* r, const char* config, size_t config_len, const fl
 int ffb_density_estimate(ffb_renderer* r, const uint32_t* counts, const float* rgb, uint32_t w, uint32_t h,
                          float max_radius, float min_radius, float curve, float* out_counts, float* out_rgb);
 
+/* Density estimation that allocates nothing, for callers that may not
+ * allocate device memory while they run: an application whose own pool owns
+ * the device, or a frame loop whose memory is fixed at start-up.  No
+ * counterpart in the reference: an addition beside ffb_density_estimate.
+ * d_hist: w*h float4 (r, g, b sums, u32 count bits), the layout
+ * ffb_chaos_device writes; d_out: w*h float4 (r, g, b, count as f32); both
+ * on the current device; stream NULL is the default stream.  Returns once
+ * the work is queued.  The weight table lives in one static device array of
+ * 65536 entries (1 MiB) shared by every call on a device:
+ * FFB_ERR_TOO_LARGE when the radii need more (the table grows as
+ * max_radius^(1/curve)), and calls whose work overlaps on the GPU race on
+ * it.  The first call on a device looks up the array's address and should
+ * come before any stream capture. */
+int ffb_density_estimate_static(const void* d_hist, uint32_t w, uint32_t h, float max_radius, float min_radius,
+                                float curve, void* d_out, void* stream);
+
 /* The variation probe (shaders/core/main_template.wgsl:1467-1567): every
  * transform of the config (normals, then the final chain) at `npts`
  * points (x, y pairs), RNG slot = transform*npts + point.  `out` holds
