@@ -16,19 +16,21 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "ffb200", "libffb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["ffb_tail.cu", "ffb_runtime.cpp", "ffb_flame.cpp", "ffb_codegen.cpp"]
-HEADERS = ["ffb_json.hpp", "ffb_flame.hpp", "ffb_codegen.hpp", "ffb_tail.cuh", "ffb_device.cuh", "ffb_kernels.cuh"]
+SOURCES = ["ffb_tail.cu", "ffb_diff_tail.cu", "ffb_runtime.cpp", "ffb_flame.cpp", "ffb_codegen.cpp"]
+HEADERS = ["ffb_json.hpp", "ffb_flame.hpp", "ffb_codegen.hpp", "ffb_tail.cuh", "ffb_device.cuh", "ffb_kernels.cuh",
+           "ffb_diff_jac.cuh", "ffb_diff.cuh"]
 
 
 def embed():
     """Device sources as raw string literals for NVRTC."""
     parts = []
-    for name, var in (("ffb_device.cuh", "kDeviceSrc"), ("ffb_kernels.cuh", "kKernelsSrc")):
+    for name, var in (("ffb_device.cuh", "kDeviceSrc"), ("ffb_kernels.cuh", "kKernelsSrc"),
+                      ("ffb_diff_jac.cuh", "kDiffJacSrc"), ("ffb_diff.cuh", "kDiffSrc")):
         with open(os.path.join(CSRC, name), encoding="utf-8") as f:
             text = f.read()
         assert ")FFBSRC\"" not in text
         parts.append(f'extern const char* const {var} = R"FFBSRC(\n{text})FFBSRC";\n')
-    body = ("// generated by build.py from ffb_device.cuh and ffb_kernels.cuh\nnamespace ffb {\n"
+    body = ("// generated by build.py from the device sources (ffb_device.cuh, ffb_kernels.cuh, ffb_diff*.cuh)\nnamespace ffb {\n"
             + "".join(parts) + "}  // namespace ffb\n")
     path = os.path.join(CSRC, "ffb_device_src.inc")
     old = open(path, encoding="utf-8").read() if os.path.exists(path) else None

@@ -43,11 +43,63 @@ std::string call(const VarDef* v, const std::string& prm0, const std::string& pr
     return o.str();
 }
 
+// The Jacobian of a variation body (ffb_diff.cuh): "v_name" -> "dj_name".
+std::string jcall(const VarDef* v, const std::string& prm0, const std::string& prm1, int slot) {
+    std::ostringstream o;
+    o << "dj_" << (v->fn + 2) << "(x, y";
+    if (v->needs_rng) o << ", rng.draw(" << slot << ")";
+    if (v->nparams >= 1) o << ", " << prm0;
+    if (v->nparams >= 2) o << ", " << prm1;
+    o << ")";
+    return o.str();
+}
+
+// The differentiable render's generated functions and kernels.
+void emit_diff(std::ostringstream& s, const Plan& p) {
+    const int NVN = (int)p.normal.size();
+    s << kDiffJacSrc << "\n";
+    s << "#define FFB_WINDOW " << p.diff_window << "\n#define FFB_CKPT " << p.diff_ckpt << "\n";
+    s << "#define FFB_NPARAM " << p.maxx * (7 + NVN) << "\n";
+    // Normal phase of transform k for the adjoint: the weight gradient of
+    // each variation (a . V_j(x, y)) into gw[j * P], and J = sum_j w_j J_j.
+    s << "template <class R> __device__ __forceinline__ void ffb_dnormal(const float* __restrict__ sm, int k, float x, float y, R& rng, "
+         "float ax, float ay, float* __restrict__ gw, int P, float4& J) {\n";
+    s << "    J = make_float4(0.f, 0.f, 0.f, 0.f);\n    float ox, oy;\n";
+    for (int j = 0; j < NVN; ++j) {
+        const VarDef* v = p.normal[j];
+        std::ostringstream w, a0, a1;
+        w << "sm[T_VW + " << j << " * FFB_MAXX + k]";
+        a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + k]";
+        a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + k]";
+        s << "    { " << call(v, a0.str(), a1.str(), p.normal_slot[j]) << "; const float g = ax * ox + ay * oy; if (isfinite(g)) gw["
+          << j << " * P] += g;\n      const float w = " << w.str() << "; if (w != 0.0f) { const float4 jj = "
+          << jcall(v, a0.str(), a1.str(), p.normal_slot[j])
+          << "; J.x += w * jj.x; J.y += w * jj.y; J.z += w * jj.z; J.w += w * jj.w; } }   // " << v->name << "\n";
+    }
+    s << "    if (!(isfinite(J.x) && isfinite(J.y) && isfinite(J.z) && isfinite(J.w))) J = make_float4(0.f, 0.f, 0.f, 0.f);\n}\n";
+    // One normal variation's value and Jacobian (the probe).
+    s << "template <class R> __device__ __forceinline__ void ffb_dvar_one(const float* __restrict__ sm, int j, int k, float x, float y, R& rng, "
+         "float& ox, float& oy, float4& J) {\n    switch (j) {\n";
+    for (int j = 0; j < NVN; ++j) {
+        const VarDef* v = p.normal[j];
+        std::ostringstream a0, a1;
+        a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + k]";
+        a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + k]";
+        s << "    case " << j << ": " << call(v, a0.str(), a1.str(), p.normal_slot[j]) << "; J = "
+          << jcall(v, a0.str(), a1.str(), p.normal_slot[j]) << "; break;\n";
+    }
+    s << "    default: ox = 0.f; oy = 0.f; J = make_float4(0.f, 0.f, 0.f, 0.f); break;\n    }\n}\n";
+    s << kDiffSrc << "\n";
+}
+
 }  // namespace
 
-Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads, bool per_xform, bool exact) {
+Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads, bool per_xform, bool exact,
+               int diff_window, int diff_ckpt) {
     Plan p;
     p.exact = exact;
+    p.diff_window = diff_window;
+    p.diff_ckpt = diff_ckpt;
     p.rng_mode = rng_mode;
     p.math_mode = math_mode;
     p.per_xform = per_xform;
@@ -149,13 +201,14 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     for (size_t c = 0; c < p.fin.size(); ++c) s << "    ffb_final_one(sm, " << c << ", x, y, rng, true);\n";
     s << "}\n";
     s << kKernelsSrc << "\n";
+    if (diff_window > 0) emit_diff(s, p);
     p.source = s.str();
     return p;
 }
 
 bool plan_fits(const Plan& p, const Flame& f) {
     if ((int)f.xf.size() > p.maxx) return false;
-    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform, p.exact);
+    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform, p.exact, p.diff_window, p.diff_ckpt);
     return q.source == p.source;
 }
 

@@ -41,12 +41,15 @@ struct Plan {
     // union form is warp-uniform after the sorted schedule's regrouping.
     bool per_xform = false;
     bool exact = false;                    // u64 fixed-point histogram (ulonglong4 a pixel)
+    // Differentiable render (ffb_diff.cuh): window = iterations each sample
+    // is differentiated through, ckpt = checkpoint interval; 0 = off.
+    int diff_window = 0, diff_ckpt = 0;
     std::string source;                    // full NVRTC source (structure key)
 };
 
 // Structure of `f` (rng/math modes as given; maxx >= f.xf.size()).
 Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx = 0, int threads = 128, bool per_xform = false,
-               bool exact = false);
+               bool exact = false, int diff_window = 0, int diff_ckpt = 0);
 // The table of `f` for a plan made from a flame of the same structure.
 std::vector<float> make_table(const Plan& p, const Flame& f);
 // Whether `f` fits plan `p` (same structure, n_xf <= maxx).
@@ -55,5 +58,7 @@ bool plan_fits(const Plan& p, const Flame& f);
 // Embedded device sources (generated into ffb_device_src.inc at build time).
 extern const char* const kDeviceSrc;
 extern const char* const kKernelsSrc;
+extern const char* const kDiffJacSrc;
+extern const char* const kDiffSrc;
 
 }  // namespace ffb

@@ -19,6 +19,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -104,7 +105,9 @@ struct Module {
     std::string key;
     cudaLibrary_t lib = nullptr;
     cudaKernel_t chaos = nullptr, chaos_sorted = nullptr, probe = nullptr, apply = nullptr;
-    int smem_attr = 0, smem_attr_sorted = 0;
+    // Differentiable-render modules (ffb_diff.cuh) only.
+    cudaKernel_t dforward = nullptr, dadjoint = nullptr, dtheta = nullptr, dprobe = nullptr;
+    int smem_attr = 0, smem_attr_sorted = 0, smem_attr_dadj = 0;
     int pins = 0;                  // batches holding this module (not evicted while > 0)
 };
 
@@ -114,6 +117,12 @@ std::string nvrtc_options_key() { return "sm_100a|c++17|ftz|prec-div|prec-sqrt|n
 }  // namespace ffb
 
 using namespace ffb;
+
+// Objects that borrow a renderer's modules: when the renderer goes first it
+// orphans them (their modules are unloaded with it), so destroying them
+// later frees only their own device memory and touches nothing else.
+static void batch_orphan(ffb_batch* b);
+static void diff_orphan(ffb_diff* d);
 
 struct ffb_renderer {
     int device = 0;
@@ -125,12 +134,19 @@ struct ffb_renderer {
     DevBuf hist, walkers, table, palette, counters, jobs, rgba, de_out, de_tab, lut, f_out, tmp_in;
     uint64_t h2d = 0, d2h = 0;      // bytes copied by the current call
     uint32_t launches = 0;          // kernels launched by the current call
+    std::set<ffb_batch*> batches;   // live objects borrowing this renderer's modules
+    std::set<ffb_diff*> diffs;
 
     void reset_counts() { h2d = d2h = 0; launches = 0; }
     void fill_counts(ffb_output* o) const { if (o) { o->h2d_bytes = h2d; o->d2h_bytes = d2h; o->kernel_launches = launches; } }
 
     ~ffb_renderer() {
         cudaSetDevice(device);
+        cudaDeviceSynchronize();
+        for (ffb_batch* b : batches) batch_orphan(b);
+        for (ffb_diff* d : diffs) diff_orphan(d);
+        batches.clear();
+        diffs.clear();
         if (stream) cudaStreamSynchronize(stream);
         for (auto& m : cache) if (m.lib) cudaLibraryUnload(m.lib);
         for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in}) b->release();
@@ -166,6 +182,12 @@ struct ffb_renderer {
         ck(cudaLibraryGetKernel(&m.chaos_sorted, m.lib, "ffb_chaos_sorted"), "cudaLibraryGetKernel(ffb_chaos_sorted)");
         ck(cudaLibraryGetKernel(&m.probe, m.lib, "ffb_probe"), "cudaLibraryGetKernel(ffb_probe)");
         ck(cudaLibraryGetKernel(&m.apply, m.lib, "ffb_apply_points"), "cudaLibraryGetKernel(ffb_apply_points)");
+        if (src.find("ffb_diff_forward") != std::string::npos) {
+            ck(cudaLibraryGetKernel(&m.dforward, m.lib, "ffb_diff_forward"), "cudaLibraryGetKernel(ffb_diff_forward)");
+            ck(cudaLibraryGetKernel(&m.dadjoint, m.lib, "ffb_diff_adjoint"), "cudaLibraryGetKernel(ffb_diff_adjoint)");
+            ck(cudaLibraryGetKernel(&m.dtheta, m.lib, "ffb_diff_theta"), "cudaLibraryGetKernel(ffb_diff_theta)");
+            ck(cudaLibraryGetKernel(&m.dprobe, m.lib, "ffb_dprobe"), "cudaLibraryGetKernel(ffb_dprobe)");
+        }
     }
 
     static std::vector<char> nvrtc_cubin(const std::string& src) {
@@ -947,6 +969,7 @@ struct BatchGroup {
 
 struct ffb_batch {
     ffb_renderer* r = nullptr;
+    int device = 0;
     std::vector<BatchFlame> flames;
     std::vector<BatchGroup> groups;
     DevBuf hist, walk, rgba, tables, palettes, counters, launches, tjobs, luts, de, detab;
@@ -1194,6 +1217,8 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
         }
         ck(cudaStreamEndCapture(s, &B->graph), "end capture");
         ck(cudaGraphInstantiate(&B->exec, B->graph, 0), "graph instantiate");
+        B->device = r->device;
+        r->batches.insert(B.get());
         *out = B.release();
     });
 }
@@ -1201,6 +1226,7 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
 FFB_API int ffb_batch_run(ffb_batch* b, void* stream, int32_t sync, double* ms) {
     return guard([&] {
         if (!b) fail(FFB_ERR_INVALID, "NULL batch");
+        if (!b->r) fail(FFB_ERR_INVALID, "the batch's renderer was destroyed");
         ffb_renderer* r = b->r;
         std::lock_guard<std::mutex> lk(r->mu);
         r->begin();
@@ -1220,6 +1246,7 @@ FFB_API int ffb_batch_run(ffb_batch* b, void* stream, int32_t sync, double* ms) 
 FFB_API int ffb_batch_output(ffb_batch* b, uint32_t index, uint8_t* rgba, uint64_t* plotted) {
     return guard([&] {
         if (!b || index >= b->flames.size()) fail(FFB_ERR_INVALID, "no such batch item");
+        if (!b->r) fail(FFB_ERR_INVALID, "the batch's renderer was destroyed");
         ffb_renderer* r = b->r;
         std::lock_guard<std::mutex> lk(r->mu);
         r->begin();
@@ -1245,12 +1272,322 @@ FFB_API int ffb_batch_info(ffb_batch* b, uint64_t* total_samples, uint32_t* thre
     });
 }
 
+static void batch_orphan(ffb_batch* b) {
+    for (auto& G : b->groups) G.mod = nullptr;
+    b->r = nullptr;
+}
+
 FFB_API void ffb_batch_destroy(ffb_batch* b) {
     if (!b) return;
-    std::lock_guard<std::mutex> lk(b->r->mu);
-    b->r->begin();
-    cudaStreamSynchronize(b->r->stream);
+    if (b->r) {
+        std::lock_guard<std::mutex> lk(b->r->mu);
+        cudaSetDevice(b->r->device);
+        cudaStreamSynchronize(b->r->stream);
+        b->r->batches.erase(b);
+        delete b;
+        return;
+    }
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
     delete b;
+}
+
+// ------------------------------------------------------- differentiable ----
+// The differentiable render (ffb_diff.cuh, ffb_diff_tail.cu): no reference
+// counterpart.  One object holds a specialised module, the base coefficient
+// table, the histogram of the last forward pass and the walkers'
+// checkpoints; theta lives in the caller's device memory.
+
+namespace ffb {
+namespace {
+
+// Host mirror of ffb_diff_args (ffb_diff.cuh).
+struct DiffArgs {
+    const void* table;
+    const void* palette;
+    void* hist;
+    void* ckpt;
+    const void* dh;
+    void* grad;
+    void* counters;
+    void* fixed;
+    uint32_t n_walkers, walker0, n_xf, pal_n;
+    uint32_t seed_lo, seed_hi, burn_in, n_iters;
+    int32_t width, height;
+    float zoom, pan_x, pan_y, cos_r, sin_r;
+};
+static_assert(sizeof(DiffArgs) == 128, "diff launch record layout");
+
+}  // namespace
+}  // namespace ffb
+
+struct ffb_diff {
+    ffb_renderer* r = nullptr;
+    int device = 0;
+    Prepared P;
+    Module* mod = nullptr;
+    uint32_t n_xf = 0, nvn = 0, n_params = 0, n_iters = 0, n_ckpt = 0, window = 0, ckpt = 0;
+    uint32_t smem_fwd = 0, smem_adj = 0;
+    TonemapArgs ta{};
+    double area = 0, white = 0, npx = 0;
+    DevBuf table, base, oms, palette, lut, hist, ckpts, counters, dh, fixed;
+    bool exact = false;                 // deterministic accumulation (job count_bits 64)
+
+    ~ffb_diff() {
+        for (DevBuf* b : {&table, &base, &oms, &palette, &lut, &hist, &ckpts, &counters, &dh, &fixed}) b->release();
+        if (mod) mod->pins -= 1;
+    }
+
+    DiffArgs args(cudaStream_t) const {
+        DiffArgs a{};
+        a.table = table.p; a.palette = palette.p; a.hist = hist.p; a.ckpt = ckpts.p; a.dh = dh.p; a.grad = nullptr;
+        a.counters = counters.p;
+        a.fixed = exact ? fixed.p : nullptr;
+        a.n_walkers = P.walkers; a.walker0 = 0; a.n_xf = n_xf; a.pal_n = (uint32_t)(P.palette.size() / 4);
+        a.seed_lo = (uint32_t)P.seed; a.seed_hi = (uint32_t)(P.seed >> 32); a.burn_in = P.burn_in; a.n_iters = n_iters;
+        a.width = (int32_t)P.wi; a.height = (int32_t)P.hi;
+        const double rot = (double)P.flame.rotation;
+        a.zoom = P.flame.zoom; a.pan_x = (float)P.flame.pan_x; a.pan_y = (float)P.flame.pan_y;
+        a.cos_r = (float)std::cos(rot); a.sin_r = (float)std::sin(rot);
+        return a;
+    }
+};
+
+FFB_API int ffb_diff_create(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, uint32_t window,
+                            uint32_t checkpoint, ffb_diff** out) {
+    return guard([&] {
+        if (!r || !out) fail(FFB_ERR_INVALID, "NULL argument");
+        *out = nullptr;
+        if (window == 0) window = 16;
+        if (checkpoint == 0) checkpoint = 64;
+        if (window > 32) fail(FFB_ERR_INVALID, "window must be at most 32 iterations");
+        if (checkpoint > 256) fail(FFB_ERR_INVALID, "checkpoint interval must be at most 256 iterations");
+        if (!job) fail(FFB_ERR_INVALID, "job is NULL");
+        ffb_job j = *job;
+        j.rng = RNG_PHILOX;
+        const bool exact = job->count_bits == 64;
+        if (job->count_bits != 0 && job->count_bits != 32 && !exact) fail(FFB_ERR_INVALID, "count_bits must be 32 or 64");
+        j.count_bits = 32;
+        std::unique_ptr<ffb_diff> d(new ffb_diff);
+        d->exact = exact;
+        d->P = prepare(config, len, &j);
+        const Flame& f = d->P.flame;
+        if (d->P.ss != 1) fail(FFB_ERR_INVALID, "the differentiable render has no supersampling");
+        if (!f.fin_chain.empty()) fail(FFB_ERR_CONFIG, "the differentiable render takes no final transforms");
+        if (f.de.max_radius > 0.0f) fail(FFB_ERR_CONFIG, "the differentiable render takes no density estimation");
+        if (job->transparent) fail(FFB_ERR_INVALID, "the differentiable render is opaque");
+        if (f.tm.mode != 1 || f.tm.highlight != 0 || f.tm.saturation != 1.0f || f.tm.hue_shift != 0.0f)
+            fail(FFB_ERR_CONFIG, "the differentiable tone map is the log mode with clip highlights and no HSV adjustment");
+        const uint64_t iters = d->P.per_walker + d->P.burn_in;
+        if (iters > 0xFFFFFFFFull) fail(FFB_ERR_INVALID, "too many iterations a walker");
+        d->n_iters = (uint32_t)iters;
+        d->window = window;
+        d->ckpt = checkpoint;
+        d->n_ckpt = (d->n_iters + checkpoint - 1) / checkpoint;
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        d->r = r;
+        d->P.plan = make_plan(f, RNG_PHILOX, d->P.math, 0, (int)d->P.threads, false, false, (int)window, (int)checkpoint);
+        d->P.table = make_table(d->P.plan, f);
+        d->n_xf = (uint32_t)f.xf.size();
+        d->nvn = (uint32_t)d->P.plan.normal.size();
+        d->n_params = d->n_xf * (7 + d->nvn);
+        Module& m = r->module_for(d->P.plan.source);
+        m.pins += 1;
+        d->mod = &m;
+        std::vector<float> oms(d->n_xf);
+        for (uint32_t k = 0; k < d->n_xf; ++k) oms[k] = 1.0f - f.xf[k].speed;
+        std::vector<float> lut = curve_lut(f.tm);
+        auto up = [&](DevBuf& b, const void* src, size_t bytes) {
+            ck(cudaMemcpyAsync(b.ensure(bytes), src, bytes, cudaMemcpyHostToDevice, r->stream), "upload");
+        };
+        up(d->base, d->P.table.data(), d->P.table.size() * 4);
+        d->table.ensure(d->P.table.size() * 4);
+        up(d->oms, oms.data(), oms.size() * 4);
+        up(d->palette, d->P.palette.data(), d->P.palette.size() * 4);
+        up(d->lut, lut.data(), lut.size() * 4);
+        d->npx = (double)d->P.wi * (double)d->P.hi;
+        d->hist.ensure((size_t)d->P.wi * d->P.hi * 16);
+        d->dh.ensure((size_t)d->P.wi * d->P.hi * 16);
+        d->ckpts.ensure((size_t)d->n_ckpt * d->P.walkers * 16);
+        d->counters.ensure(16);
+        if (exact) d->fixed.ensure((size_t)d->P.wi * d->P.hi * 32);
+        ck(cudaStreamSynchronize(r->stream), "upload");
+        d->ta = tonemap_args(f, d->P.wi, d->P.hi, 1.0, 0, true);
+        const double ppu = (double)std::min(d->P.wi, d->P.hi) * 0.25 * (double)f.zoom;
+        d->area = d->npx / (ppu * ppu);
+        d->white = f.tm.white_level;
+        const uint32_t table_bytes = (uint32_t)((d->P.plan.table_size + 3) / 4) * 16;
+        d->smem_fwd = table_bytes + (uint32_t)(d->P.palette.size() / 4) * 16;
+        d->smem_adj = d->smem_fwd + (uint32_t)d->P.plan.maxx * (7 + d->nvn) * d->P.threads * 4;
+        if (d->smem_adj > 227 * 1024) fail(FFB_ERR_TOO_LARGE, "too many parameters for the adjoint's shared memory: use fewer threads");
+        if (d->smem_adj > 48 * 1024) {
+            ck(cudaFuncSetAttribute((const void*)m.dadjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem_adj), "smem attribute");
+        }
+        if (d->smem_fwd > 48 * 1024) {
+            ck(cudaFuncSetAttribute((const void*)m.dforward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->smem_fwd), "smem attribute");
+        }
+        d->device = r->device;
+        r->diffs.insert(d.get());
+        *out = d.release();
+    });
+}
+
+FFB_API int ffb_diff_specialize(const char* config, size_t len, uint32_t window, uint32_t checkpoint, size_t* cubin_bytes,
+                                char* source, size_t source_len) {
+    return guard([&] {
+        if (!config) fail(FFB_ERR_INVALID, "config is NULL");
+        Flame f;
+        try { f = parse_config_text(std::string(config, len)); }
+        catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
+        Plan p = make_plan(f, RNG_PHILOX, MATH_PRECISE, 0, 128, false, false, window ? (int)window : 16, checkpoint ? (int)checkpoint : 64);
+        std::vector<char> cubin = ffb_renderer::nvrtc_cubin(p.source);
+        if (cubin_bytes) *cubin_bytes = cubin.size();
+        if (source && source_len) {
+            size_t n = std::min(source_len - 1, p.source.size());
+            std::memcpy(source, p.source.data(), n);
+            source[n] = 0;
+        }
+    });
+}
+
+FFB_API int ffb_diff_layout(ffb_diff* d, uint32_t* n_xforms, uint32_t* n_variations, uint32_t* walkers, uint32_t* iterations,
+                            char* names, size_t names_cap) {
+    return guard([&] {
+        if (!d) fail(FFB_ERR_INVALID, "NULL object");
+        if (n_xforms) *n_xforms = d->n_xf;
+        if (n_variations) *n_variations = d->nvn;
+        if (walkers) *walkers = d->P.walkers;
+        if (iterations) *iterations = d->n_iters;
+        if (names) {
+            std::string s;
+            for (size_t j = 0; j < d->P.plan.normal.size(); ++j) s += (j ? "," : "") + std::string(d->P.plan.normal[j]->name);
+            if (s.size() + 1 > names_cap) fail(FFB_ERR_INVALID, "names buffer too small");
+            std::memcpy(names, s.c_str(), s.size() + 1);
+        }
+    });
+}
+
+FFB_API int ffb_diff_theta(ffb_diff* d, float* theta) {
+    return guard([&] {
+        if (!d || !theta) fail(FFB_ERR_INVALID, "NULL argument");
+        const Flame& f = d->P.flame;
+        for (uint32_t k = 0; k < d->n_xf; ++k) {
+            const XForm& x = f.xf[k];
+            const float a[6] = {x.a, x.b, x.c, x.d, x.e, x.f};
+            for (int i = 0; i < 6; ++i) theta[k * 6 + i] = a[i];
+            for (uint32_t j = 0; j < d->nvn; ++j) theta[d->n_xf * 6 + k * d->nvn + j] = x.var_weight(d->P.plan.normal[j]);
+            theta[d->n_xf * (6 + d->nvn) + k] = x.color;
+        }
+    });
+}
+
+FFB_API int ffb_diff_forward(ffb_diff* d, const float* d_theta, float* d_image, float* d_hist, void* stream) {
+    return guard([&] {
+        if (!d || !d_theta || !d_image) fail(FFB_ERR_INVALID, "NULL argument");
+        if (!d->r) fail(FFB_ERR_INVALID, "the differentiable render's renderer was destroyed");
+        ck(cudaSetDevice(d->r->device), "cudaSetDevice");
+        cudaStream_t s = (cudaStream_t)stream;
+        Module& m = *d->mod;
+        {
+            const float* th = d_theta;
+            const void* bp = d->base.p;
+            const void* op = d->oms.p;
+            void* tp = d->table.p;
+            int nx = (int)d->n_xf;
+            void* a[] = {&th, &bp, &op, &tp, &nx};
+            ck(cudaLaunchKernel((const void*)m.dtheta, dim3(1), dim3(256), a, 0, s), "launch ffb_diff_theta");
+        }
+        const size_t hb = (size_t)d->P.wi * d->P.hi * 16;
+        if (d->exact) ck(cudaMemsetAsync(d->fixed.p, 0, hb * 2, s), "clear histogram");
+        else ck(cudaMemsetAsync(d->hist.p, 0, hb, s), "clear histogram");
+        ck(cudaMemsetAsync(d->counters.p, 0, 16, s), "clear counters");
+        DiffArgs A = d->args(s);
+        void* a[] = {&A};
+        const uint32_t blocks = (d->P.walkers + d->P.threads - 1) / d->P.threads;
+        ck(cudaLaunchKernel((const void*)m.dforward, dim3(blocks), dim3(d->P.threads), a, d->smem_fwd, s), "launch ffb_diff_forward");
+        if (d->exact) ck(launch_fixed_to_float((const ulonglong4*)d->fixed.p, (size_t)d->npx, (float4*)d->hist.p, s), "fixed to float");
+        ck(launch_diff_tonemap((const float4*)d->hist.p, (size_t)d->npx, d->ta, (const float*)d->lut.p, (const uint64_t*)d->counters.p,
+                               d->npx, d->area, d->white, (float4*)d_image, s), "differentiable tone map");
+        if (d_hist) ck(cudaMemcpyAsync(d_hist, d->hist.p, hb, cudaMemcpyDeviceToDevice, s), "histogram copy");
+    });
+}
+
+FFB_API int ffb_diff_backward(ffb_diff* d, const float* d_grad_image, double* d_grad_theta, float* d_grad_hist, void* stream) {
+    return guard([&] {
+        if (!d || !d_grad_image || !d_grad_theta) fail(FFB_ERR_INVALID, "NULL argument");
+        if (!d->r) fail(FFB_ERR_INVALID, "the differentiable render's renderer was destroyed");
+        ck(cudaSetDevice(d->r->device), "cudaSetDevice");
+        cudaStream_t s = (cudaStream_t)stream;
+        ck(launch_diff_tonemap_vjp((const float4*)d->hist.p, (const float4*)d_grad_image, (size_t)d->npx, d->ta, (const float*)d->lut.p,
+                                   (const uint64_t*)d->counters.p, d->npx, d->area, d->white, (float4*)d->dh.p, s),
+           "tone map gradient");
+        ck(cudaMemsetAsync(d_grad_theta, 0, (size_t)d->n_params * 8, s), "clear gradient");
+        DiffArgs A = d->args(s);
+        A.grad = d_grad_theta;
+        void* a[] = {&A};
+        const uint32_t blocks = (d->P.walkers + d->P.threads - 1) / d->P.threads;
+        ck(cudaLaunchKernel((const void*)d->mod->dadjoint, dim3(blocks), dim3(d->P.threads), a, d->smem_adj, s), "launch ffb_diff_adjoint");
+        if (d_grad_hist)
+            ck(cudaMemcpyAsync(d_grad_hist, d->dh.p, (size_t)d->P.wi * d->P.hi * 16, cudaMemcpyDeviceToDevice, s), "gradient copy");
+    });
+}
+
+FFB_API int ffb_diff_samples(ffb_diff* d, uint64_t* plotted, uint64_t* inframe, void* stream) {
+    return guard([&] {
+        if (!d) fail(FFB_ERR_INVALID, "NULL object");
+        ck(cudaSetDevice(d->device), "cudaSetDevice");
+        uint64_t c[2] = {0, 0};
+        ck(cudaMemcpyAsync(c, d->counters.p, 16, cudaMemcpyDeviceToHost, (cudaStream_t)stream), "readback");
+        ck(cudaStreamSynchronize((cudaStream_t)stream), "readback");
+        if (plotted) *plotted = c[0];
+        if (inframe) *inframe = c[1];
+    });
+}
+
+FFB_API int ffb_diff_jacobians(ffb_diff* d, int32_t xform, uint32_t n, const float* xs, const float* ys, const float* words, float* out) {
+    return guard([&] {
+        if (!d || !xs || !ys || !words || !out) fail(FFB_ERR_INVALID, "NULL argument");
+        if (!d->r) fail(FFB_ERR_INVALID, "the differentiable render's renderer was destroyed");
+        if (xform < 0 || (uint32_t)xform >= d->n_xf) fail(FFB_ERR_INVALID, "no such transform");
+        std::lock_guard<std::mutex> lk(d->r->mu);
+        d->r->begin();
+        ffb_renderer* r = d->r;
+        const size_t nn = n;
+        float* d_in = (float*)r->tmp_in.ensure(nn * 4 * 2 + nn * 64);
+        float* d_x = d_in, *d_y = d_in + nn, *d_w = d_in + 2 * nn;
+        ck(cudaMemcpyAsync(d_x, xs, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
+        ck(cudaMemcpyAsync(d_y, ys, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
+        ck(cudaMemcpyAsync(d_w, words, nn * 64, cudaMemcpyHostToDevice, r->stream), "upload");
+        const size_t ob = nn * d->nvn * 6 * 4;
+        float* d_out = (float*)r->f_out.ensure(std::max<size_t>(ob, 4));
+        const void* tp = d->base.p;
+        int k = xform, ni = (int)n;
+        void* a[] = {&tp, &k, &ni, &d_x, &d_y, &d_w, &d_out};
+        ck(cudaLaunchKernel((const void*)d->mod->dprobe, dim3((n + 127) / 128), dim3(128), a, 0, r->stream), "launch ffb_dprobe");
+        ck(cudaMemcpyAsync(out, d_out, ob, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "jacobians");
+    });
+}
+
+static void diff_orphan(ffb_diff* d) {
+    d->mod = nullptr;
+    d->r = nullptr;
+}
+
+FFB_API void ffb_diff_destroy(ffb_diff* d) {
+    if (!d) return;
+    if (d->r) {
+        std::lock_guard<std::mutex> lk(d->r->mu);
+        cudaSetDevice(d->r->device);
+        cudaDeviceSynchronize();
+        d->r->diffs.erase(d);
+        delete d;
+        return;
+    }
+    cudaSetDevice(d->device);
+    cudaDeviceSynchronize();
+    delete d;
 }
 
 // ------------------------------------------------------------ drop-in ----

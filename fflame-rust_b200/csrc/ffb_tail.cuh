@@ -66,6 +66,19 @@ int de_static_entries(double r_max, double r_min, double curve);
 cudaError_t density_estimate_static(const float4* hist, int w, int h, double r_max, double r_min, double curve,
                                     float4* out, cudaStream_t s);
 
+// The differentiable render's tone map (ffb_diff_tail.cu): n pixels of a
+// bilinear histogram (r, g, b sums, weight) to linear-light RGBA (alpha 1),
+// and its vector-Jacobian product dh = J^T dimg per pixel.  `samples` is the
+// forward pass's device counter of plotted samples; npx, area and white give
+// the sample density's constants as tonemap_args derives them.
+cudaError_t launch_diff_tonemap(const float4* hist, size_t n, const TonemapArgs& a, const float* lut, const uint64_t* samples,
+                                double npx, double area, double white, float4* out, cudaStream_t s);
+cudaError_t launch_diff_tonemap_vjp(const float4* hist, const float4* dimg, size_t n, const TonemapArgs& a, const float* lut,
+                                    const uint64_t* samples, double npx, double area, double white, float4* dh, cudaStream_t s);
+
+// The deterministic accumulation's u64 sums (2^-32 units) as float4.
+cudaError_t launch_fixed_to_float(const ulonglong4* fx, size_t n, float4* out, cudaStream_t s);
+
 // Histogram <-> (u32 count plane, f32 rgb plane), for collectives.
 cudaError_t launch_pack(const float4* hist, size_t n, unsigned* cnt, float* rgb, cudaStream_t s);
 cudaError_t launch_unpack(const unsigned* cnt, const float* rgb, size_t n, float4* hist, cudaStream_t s);

@@ -27,6 +27,8 @@ EXPORTS = [
     "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench", "ffb_chaos_device", "ffb_hist_pack",
     "ffb_hist_unpack", "ffb_finish_device", "ffb_histogram_u64", "ffb_batch_create", "ffb_batch_run",
     "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
+    "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
+    "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize",
 ]
 
 

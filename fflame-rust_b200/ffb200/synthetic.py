@@ -13,6 +13,10 @@ Shapes follow the benchmark's configuration list:
 * `stress_flame` -- 16 transforms: 10 as the full flame's plus 6 rotations
   by k*60 degrees (6-fold rotational symmetry as ordinary transforms);
   density estimation radius 12 -> 0.
+* `diff_flame`   -- 4 transforms for the differentiable render: the plain
+  flame's distributions with each affine's linear part scaled by 0.6, so
+  every transform contracts on average and a sample's sensitivity to
+  iterations more than 16 back is below 1e-4 of its gradient;
 * `batch_flames` -- 256 flames for the batched renderer: transform counts
   ~U{2..12}, variations as the plain flame, sizes ~{128,256,512,1024}^2,
   budgets ~U[50,2000] samples a pixel, a seed each.
@@ -110,3 +114,13 @@ def stress_flame(seed=21, de_radius=12.0):
             "weight": 0.5, "color": float(rng.uniform(0, 1)), "color_speed": 0.5, "variations": {"linear": 1.0}})
     base["name"] = f"stress-{seed}"
     return base
+
+
+def diff_flame(seed=4, n_xforms=4):
+    """The differentiable render's flame (4 transforms, contractive)."""
+    cfg = plain_flame(seed, n_xforms=n_xforms)
+    for t in cfg["flame"]["transforms"]:
+        for k in "abcd":
+            t[k] = float(np.float32(t[k] * 0.6))
+    cfg["name"] = f"diff-{seed}"
+    return cfg

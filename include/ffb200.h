@@ -195,6 +195,47 @@ int ffb_hist_unpack(ffb_renderer* r, const void* d_counts, const void* d_rgb, ui
 int ffb_finish_device(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, const void* d_hist,
                       uint64_t total_samples, uint32_t row0, uint32_t rows, void* d_rgba, void* stream);
 
+/* ---- the differentiable render: an addition beside the reference's render
+ * (which has no gradients).  The chaos game with a bilinear splat and a
+ * linearly interpolated palette, the log tone map in linear light (alpha 1),
+ * and the gradient of a loss with respect to
+ * theta = [n_xf*6 affine a..f | n_xf*n_var variation weights, transform-major
+ * | n_xf colours], each plotted sample differentiated through the last
+ * `window` iterations of its walker (default 16) from walker states
+ * checkpointed every `checkpoint` iterations (default 64).  Philox stream,
+ * no final transforms, supersampling or density estimation; log tone map,
+ * clip highlights.  job->count_bits 64 accumulates the histogram in u64
+ * fixed point (2^-32 units): the same bits whatever the order of the
+ * atomics, so renders at nearby theta differ only by theta (finite
+ * differences at small steps).  Device pointers; `stream` is a cudaStream_t passed
+ * through as given (NULL: the legacy default stream); calls only enqueue. */
+typedef struct ffb_diff ffb_diff;
+int ffb_diff_create(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, uint32_t window,
+                    uint32_t checkpoint, ffb_diff** out);
+/* ffb_specialize for the differentiable render's module (no device needed). */
+int ffb_diff_specialize(const char* config, size_t config_len, uint32_t window, uint32_t checkpoint, size_t* cubin_bytes,
+                        char* source, size_t source_len);
+/* theta's shape: transforms, variations (and their names, comma-separated,
+ * in theta's order), walkers and iterations a walker (burn-in included). */
+int ffb_diff_layout(ffb_diff* d, uint32_t* n_xforms, uint32_t* n_variations, uint32_t* walkers, uint32_t* iterations,
+                    char* names, size_t names_cap);
+/* The config's own theta (host, n_xf*(7+n_var) floats). */
+int ffb_diff_theta(ffb_diff* d, float* theta);
+/* Forward at d_theta: the image (width*height float4, linear rgb, 1) and, if
+ * d_hist is not NULL, a copy of the histogram (r, g, b sums, weight). */
+int ffb_diff_forward(ffb_diff* d, const float* d_theta, float* d_image, float* d_hist, void* stream);
+/* dL/dtheta (n_xf*(7+n_var) doubles) of the most recent forward, given
+ * dL/dimage (width*height float4; alpha ignored), and, if d_grad_hist is
+ * not NULL, dL/dhistogram (width*height float4). */
+int ffb_diff_backward(ffb_diff* d, const float* d_grad_image, double* d_grad_theta, float* d_grad_hist, void* stream);
+/* The most recent forward's plotted and in-frame samples (synchronises `stream`). */
+int ffb_diff_samples(ffb_diff* d, uint64_t* plotted, uint64_t* inframe, void* stream);
+/* Each variation's value and Jacobian at n points for transform `xform`
+ * (host buffers; words as ffb_apply_points): out is n*n_var*6 floats
+ * (vx, vy, dvx/dx, dvx/dy, dvy/dx, dvy/dy). */
+int ffb_diff_jacobians(ffb_diff* d, int32_t xform, uint32_t n, const float* xs, const float* ys, const float* words, float* out);
+void ffb_diff_destroy(ffb_diff* d);
+
 /* ---- batches: many flames in one persistent launch a structure group,
  * tone-mapped in one launch, the device work captured as a CUDA graph.
  * The batched addition beside the reference's one-flame render. */

@@ -410,3 +410,102 @@ def density_estimate(cnt, rgb, w, h, r_max, r_min=0.0, curve=0.4):
                               ctypes.c_double(r_max), ctypes.c_double(r_min), ctypes.c_double(curve),
                               oc.ctypes.data_as(P), orgb.ctypes.data_as(P))
     return oc.reshape(h, w), orgb.reshape(h, w, 3)
+
+
+# ------------------------------------------------------------ gradients --
+
+class DiffCfg(ctypes.Structure):
+    _fields_ = [
+        ("seed_lo", ctypes.c_uint32), ("seed_hi", ctypes.c_uint32), ("burn_in", ctypes.c_uint32),
+        ("walker0", ctypes.c_uint32), ("walkers", ctypes.c_uint32), ("iters", ctypes.c_uint64),
+        ("window", ctypes.c_int), ("use_f64", ctypes.c_int), ("threads", ctypes.c_int),
+    ]
+
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def theta_layout(cfg):
+    """(n_xf, variation names) of the differentiable render's theta:
+    [n_xf*6 affine | n_xf*n_var weights, transform-major | n_xf colours]."""
+    return len(cfg["flame"]["transforms"]), local_order(cfg["flame"])
+
+
+def theta_of(cfg):
+    n, names = theta_layout(cfg)
+    t = cfg["flame"]["transforms"]
+    aff = [f32(x[k]) for x in t for k in "abcdef"]
+    w = [f32(x["variations"].get(v, 0.0)) for x in t for v in names]
+    col = [f32(x.get("color", 0.5)) for x in t]
+    return np.array(aff + w + col, np.float32)
+
+
+def with_theta(cfg, theta):
+    """A copy of the config with theta's values in place (f32-exact)."""
+    import copy
+    n, names = theta_layout(cfg)
+    out = copy.deepcopy(cfg)
+    theta = np.asarray(theta, np.float64)
+    for k, x in enumerate(out["flame"]["transforms"]):
+        for i, key in enumerate("abcdef"):
+            x[key] = float(theta[k * 6 + i])
+        x["variations"] = {v: float(theta[n * 6 + k * len(names) + j]) for j, v in enumerate(names)}
+        x["color"] = float(theta[n * (6 + len(names)) + k])
+    return out
+
+
+class DiffFlame(Flame):
+    """The differentiable render's oracle for one config at one theta."""
+
+    def _cfg(self, walkers, iters, seed, burn_in, window, f64, threads, walker0=0):
+        c = DiffCfg()
+        c.seed_lo, c.seed_hi, c.burn_in = seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF, burn_in
+        c.walker0, c.walkers, c.iters = walker0, walkers, iters
+        c.window, c.use_f64, c.threads = window, 1 if f64 else 0, threads
+        return c
+
+    def render(self, walkers, iters, *, seed=12345, burn_in=20, f64=False, threads=8):
+        """(bilinear histogram [h, w, 4] f64, plotted samples)."""
+        hist = np.zeros(self.width * self.height * 4, np.float64)
+        c = self._cfg(walkers, iters, seed, burn_in, 0, f64, threads)
+        lib().of_diff_render.restype = ctypes.c_uint64
+        n = lib().of_diff_render(self.ptr, ctypes.byref(c), hist.ctypes.data_as(_DP))
+        return hist.reshape(self.height, self.width, 4), n
+
+    def grad(self, dh, walkers, iters, *, seed=12345, burn_in=20, window=16, f64=False, threads=8):
+        """dL/dtheta given dL/dhistogram [h, w, 4]."""
+        dh = np.ascontiguousarray(dh, np.float64).ravel()
+        n_xf = self.s.n_xf
+        g = np.zeros(n_xf * (7 + self.s.n_var), np.float64)
+        c = self._cfg(walkers, iters, seed, burn_in, window, f64, threads)
+        lib().of_diff_grad(self.ptr, ctypes.byref(c), dh.ctypes.data_as(_DP), g.ctypes.data_as(_DP))
+        return g
+
+
+def diff_tonemap(params, hist):
+    """Linear-light tone map of a bilinear histogram [..., 4] -> [..., 4]."""
+    h = np.ascontiguousarray(hist, np.float64)
+    out = np.zeros_like(h)
+    lib().of_diff_tonemap(ctypes.byref(params), h.ctypes.data_as(_DP), ctypes.c_int(h.size // 4), out.ctypes.data_as(_DP))
+    return out
+
+
+def diff_tonemap_vjp(params, hist, dimg):
+    h = np.ascontiguousarray(hist, np.float64)
+    d = np.ascontiguousarray(dimg, np.float64)
+    out = np.zeros_like(h)
+    lib().of_diff_tonemap_vjp(ctypes.byref(params), h.ctypes.data_as(_DP), d.ctypes.data_as(_DP), ctypes.c_int(h.size // 4),
+                              out.ctypes.data_as(_DP))
+    return out
+
+
+def variation_jacobian(name, xs, ys, draws=None, params=None):
+    """(vx, vy, J00, J01, J10, J11) [n, 6] by central differences in double."""
+    xs = np.ascontiguousarray(xs, np.float32)
+    ys = np.ascontiguousarray(ys, np.float32)
+    prm = np.array(params if params is not None else [d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
+    d = None if draws is None else np.ascontiguousarray(draws, np.float32)
+    out = np.zeros(len(xs) * 6, np.float64)
+    lib().of_variation_jacobian(ctypes.c_int(REGISTRY[name]), _fp(prm), ctypes.c_int(len(xs)), _fp(xs), _fp(ys),
+                                _fp(d) if d is not None else None, out.ctypes.data_as(_DP))
+    return out.reshape(-1, 6)
