@@ -263,7 +263,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
                    "samples_per_step": samples_per_step, "walkers": wl["walkers"], "rng": "philox",
                    "schedule": args.schedule, "math": args.math,
-                   "l2": "histogram 132.7 MB > 126 MB L2, cleared every step",
+                   "l2": f"histogram {W * ss * H * ss * (32 if exact else 16) / 1e6:.1f} MB > 126 MB L2, cleared every step",
                    "parallelism": f"walker shards x{world}" + (" + NCCL histogram all-reduce + row bands" if world > 1 else "")},
         "ms_per_frame": ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -339,12 +339,169 @@ def run_batched(args, local_rank):
     }
 
 
+def run_diff(args, local_rank):
+    """The differentiable configuration: 4 transforms at 512^2, bilinear
+    splat, 2e8 samples, loss = L2 between the image and the image at
+    theta + N(0, 0.05).  One step = forward (theta -> image), the loss's
+    gradient with respect to the image, and the adjoint (-> dL/dtheta).
+    `value` is the step's time over the forward's (fwd+bwd / fwd)."""
+    import numpy as np
+    import torch
+    from ffb200 import _native, diff, synthetic
+    torch.cuda.set_device(local_rank)
+    side = torch.cuda.Stream()
+    torch.cuda.set_stream(side)
+    cfg = synthetic.diff_flame(4)
+    W, samples, walkers = 512, 200_000_000, 65536
+    r = _native.Renderer(local_rank)
+    dr = diff.DiffRenderer(cfg, W, W, samples, walkers=walkers, seed=2024, renderer=r)
+    th = dr.theta0()
+    noisy = th + torch.from_numpy(np.random.default_rng(2).normal(0, 0.05, th.numel()).astype(np.float32)).cuda()
+    target = dr.forward_raw(noisy).clone()
+
+    def fwd():
+        return dr.forward_raw(th)
+
+    def step():
+        img = dr.forward_raw(th)
+        d = 2.0 * (img - target)
+        d[..., 3] = 0.0
+        return dr.backward_raw(d)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    for _ in range(args.steps):
+        fwd()
+    ev[1].record()
+    for _ in range(args.steps):
+        step()
+    ev[2].record()
+    ev[2].synchronize()
+    clk = clocks.stop()
+    fwd_ms = ev[0].elapsed_time(ev[1]) / args.steps
+    step_ms = ev[1].elapsed_time(ev[2]) / args.steps
+    plotted, inframe = dr.samples()
+    # The adjoint kernel alone, and the forward kernel's splat against the
+    # vector-reduction ceiling at the same histogram size.
+    img = dr.forward_raw(th)
+    d = 2.0 * (img - target)
+    ev[0].record()
+    dr.backward_raw(d)
+    ev[1].record()
+    ev[1].synchronize()
+    bwd_ms = ev[0].elapsed_time(ev[1])
+    bench_ms = r.atomic_bench(W * W, 400_000_000, 2)
+    v4_peak = 400_000_000 / (bench_ms * 1e-3)
+    peaks, peak_kind = measured_peaks()
+    bytes_per_launch = 64.0 * inframe            # 4 corners x one 16-byte vector reduction
+    achieved = bytes_per_launch / (fwd_ms * 1e-3) / 1e9
+    # End to end through the autograd Function: theta from pinned host memory,
+    # the scalar loss and dL/dtheta back to the host, every step.
+    host_th = th.cpu().pin_memory()
+    host_g = torch.empty(th.numel(), dtype=torch.float32).pin_memory()
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t = host_th.to("cuda", non_blocking=True).requires_grad_()
+        loss = ((dr.render(t)[..., :3] - target[..., :3]) ** 2).sum()
+        loss.backward()
+        host_g.copy_(t.grad, non_blocking=True)
+        lv = loss.item()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    e2e_ms = statistics.mean(e2e) * 1e3
+    e2e_fwd = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t = host_th.to("cuda", non_blocking=True)
+        lv = ((dr.forward_raw(t)[..., :3] - target[..., :3]) ** 2).sum().item()
+        if i >= args.warmup:
+            e2e_fwd.append(time.perf_counter() - t0)
+    e2e_fwd_ms = statistics.mean(e2e_fwd) * 1e3
+    cpu = None
+    if not args.no_cpu:
+        cpu = cpu_baseline_diff(cfg, W)
+    dr.close()
+    return {
+        "metric": "fwd+bwd time / fwd time", "value": step_ms / fwd_ms, "unit": "x", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flame generator)",
+        "config": {"workload": "diff_512", "desc": "4 xforms {linear,sinusoidal,spherical} (contractive), 512x512 ss1, "
+                   "2e8 samples, 65536 walkers, bilinear splat, L2 loss vs image at theta+N(0,0.05); "
+                   f"grads for {dr.n_params} parameters through the last 16 iterations, checkpoints every 64",
+                   "l2": "histogram 4 MB (L2-resident), cleared every forward"},
+        "fwd_ms": fwd_ms, "fwd_bwd_ms": step_ms, "bwd_kernel_ms": bwd_ms,
+        "samples_per_s_fwd": plotted / (fwd_ms * 1e-3), "samples_per_s_fwd_bwd": plotted / (step_ms * 1e-3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": "ffb_diff_forward",
+                     "kernel_ms": fwd_ms, "algorithmic_bytes_per_launch": bytes_per_launch, "peak_kind": peak_kind},
+        "l2_atomic": {"achieved_v4_reductions_per_s": 4 * inframe / (fwd_ms * 1e-3), "peak_v4_reductions_per_s": v4_peak,
+                      "frac": 4 * inframe / (fwd_ms * 1e-3) / v4_peak, "peak_from": "ffb_atomic_bench kind 2, 512^2 pixels"},
+        "e2e": {"value": e2e_ms / e2e_fwd_ms, "unit": "x", "ms_fwd_bwd": e2e_ms, "ms_fwd": e2e_fwd_ms,
+                "h2d_bytes_per_step": th.numel() * 4, "d2h_bytes_per_step": th.numel() * 4 + 8,
+                "path": "ffb200.diff.DiffRenderer.render (torch.autograd.Function): theta from pinned host memory, "
+                        "loss and dL/dtheta back to the host"},
+        "gpu_launches": 5 * args.steps + 3 * args.steps,
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+
+
+def cpu_baseline_diff(cfg, W, budget_s=10.0):
+    """The FP64 oracle's forward and gradient on the host cores, on a bounded
+    sample of the same flame at 512^2: samples/s of fwd and of fwd+bwd."""
+    import numpy as np
+    from oracle import oracle as O
+    O.build()
+    threads = min(os.cpu_count() or 1, 64)
+    fl = O.DiffFlame(cfg, W, W)
+    walkers, iters = threads * 16, 20 + 64
+    t0 = time.perf_counter()
+    hist, n = fl.render(walkers, iters, threads=threads)
+    t_f = time.perf_counter() - t0
+    scale = max(1, int(budget_s / 2 / max(t_f, 1e-3)))
+    walkers *= min(scale, 64)
+    t0 = time.perf_counter()
+    hist, n = fl.render(walkers, iters, threads=threads)
+    t_f = time.perf_counter() - t0
+    dh = np.random.default_rng(0).normal(0, 1e-3, hist.shape)
+    t0 = time.perf_counter()
+    fl.grad(dh, walkers, iters, threads=threads)
+    t_b = time.perf_counter() - t0
+    return {"value": n / (t_f + t_b), "unit": "samples/s (fwd+bwd)", "fwd_samples_per_s": n / t_f, "cores": threads,
+            "kind": "port", "sample": f"{n} samples ({walkers} walkers x 64 after burn-in 20) of the same flame at {W}x{W}; "
+                                      "gradient per sample walking its 16-iteration window, FD Jacobians, f64"}
+
+
 def run_reference(args, rank, world):
     """The reference's CPU path: there is none (variations exist only as
     WGSL; benches/flame_bench.rs:1-10), so the oracle port of it runs on all
     host threads, each step a bounded sample of the same workload."""
     if rank != 0:
         return None
+    if args.workload == "diff_512":
+        from ffb200 import synthetic
+        rates = [cpu_baseline_diff(synthetic.diff_flame(4), 512, budget_s=4.0) for _ in range(args.steps)]
+        v = statistics.mean(r["value"] for r in rates)
+        fwd = statistics.mean(r["fwd_samples_per_s"] for r in rates)
+        return {
+            "impl": "reference", "metric": "fwd+bwd time / fwd time", "value": fwd / v, "unit": "x", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 2e8 / v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded flame generator)",
+            "config": {"workload": "diff_512"},
+            "cpu_baseline": dict(rates[-1], value=fwd / v, unit="x"),
+            "e2e": {"value": fwd / v, "unit": "x", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference has no gradients; this is the oracle's FP64 restatement of this build's definition",
+        }
     wl = workload(args.workload)
     from oracle import oracle as O
     O.build()
@@ -380,7 +537,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="full_1080p_ss2", choices=["full_1080p_ss2", "plain_256", "batched_256", "stress_4k"])
+    ap.add_argument("--workload", default="full_1080p_ss2",
+                    choices=["full_1080p_ss2", "plain_256", "batched_256", "stress_4k", "diff_512"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--math", default="precise", choices=["precise", "sfu"],
                     help="precise: IEEE-accurate sin/cos (the parity-tested path); sfu: the hardware's, as the reference GPU")
@@ -393,6 +551,18 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.profile and args.workload == "diff_512":
+        import torch
+        from ffb200 import diff, synthetic
+        dr = diff.DiffRenderer(synthetic.diff_flame(4), 512, 512, int(args.profile), walkers=65536, seed=2024)
+        th = dr.theta0()
+        for _ in range(args.warmup + args.steps):
+            img = dr.forward_raw(th)
+            g = dr.backward_raw(img * 0.01)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "diff_512", "samples": dr.samples()[0], "grad_norm": float(g.norm())}))
+        dr.close()
+        return
     if args.profile:
         from ffb200 import _native
         wl = workload(args.workload)
@@ -404,8 +574,9 @@ def main():
         print(json.dumps({"profile": args.workload, "samples": o.total_iterations, "inframe": o.inframe_samples,
                           "ms": o.render_time_ms}))
         return
-    if args.workload == "batched_256" and args.impl == "ours":
-        line = run_batched(args, local_rank) if rank == 0 else None
+    if args.workload in ("batched_256", "diff_512") and args.impl == "ours":
+        runner = run_batched if args.workload == "batched_256" else run_diff
+        line = runner(args, local_rank) if rank == 0 else None
         if line is not None:
             print(json.dumps(line), flush=True)
         return
