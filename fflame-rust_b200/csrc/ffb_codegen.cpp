@@ -12,6 +12,8 @@ namespace ffb {
 
 namespace {
 
+constexpr int kSymBlock = 6 + 64;            // post-symmetry table block (floats)
+
 // Normal-phase variations: those a normal transform uses at a weight other
 // than 0, in local order.  The reference emits every active variation and
 // gates each on `xform.variations[idx] != 0.0` (shader_builder_v2.rs
@@ -124,6 +126,9 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     p.t_fin = p.t_vp + 2 * NVN * M;
     int off = p.t_fin;
     for (auto& fi : p.fin) { fi.off = off; off += 13 + 3 * (int)fi.vars.size(); }
+    p.sym_kind = f.sym.kind;
+    p.t_sym = off;
+    if (p.sym_kind != 0) off += kSymBlock;
     p.table_size = off;
 
     std::ostringstream s;
@@ -133,6 +138,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     s << "#define FFB_RNG_MODE " << rng_mode << "\n#define FFB_THREADS " << threads << "\n";
     if (math_mode == MATH_SFU) s << "#define FFB_SFU 1\n";
     if (exact) s << "#define FFB_EXACT 1\n";
+    s << "#define FFB_SYM_KIND " << p.sym_kind << "\n#define T_SYM " << p.t_sym << "\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
     s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw
       << "\n#define T_VP " << p.t_vp << "\n";
@@ -234,6 +240,23 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
             const VarDef* v = p.normal[j];
             t[p.t_vw + j * M + k] = x.var_weight(v);
             for (int q = 0; q < v->nparams; ++q) t[p.t_vp + (2 * j + q) * M + k] = x.param(v, q);
+        }
+    }
+    if (p.sym_kind != 0) {
+        // Post-symmetry block: copies, centre, half the pair's separation,
+        // cos/sin of the axis modes' pre-rotation (-rotation), then cos/sin
+        // of each point-mode copy's angle k * 2pi / order
+        // (utilities.wgsl:470-568), computed here in f32.
+        const PostSym& y = f.sym;
+        float* q = t.data() + p.t_sym;
+        q[0] = (float)y.copies();
+        q[1] = y.cx; q[2] = y.cy;
+        q[3] = y.distance * 0.5f;
+        q[4] = std::cos(-y.rotation); q[5] = std::sin(-y.rotation);
+        for (int k = 0; k < 32; ++k) {
+            const float th = ((float)k * 6.28318530717958647692f) / (float)std::max(y.order, 1);
+            q[6 + 2 * k] = std::cos(th);
+            q[7 + 2 * k] = std::sin(th);
         }
     }
     for (size_t c = 0; c < p.fin.size(); ++c) {

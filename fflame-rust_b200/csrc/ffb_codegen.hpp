@@ -32,6 +32,7 @@ struct Plan {
     int n_slots = 2;
     int table_size = 0;
     int t_cum = 0, t_xf = 0, t_vw = 0, t_vp = 0, t_fin = 0;
+    int sym_kind = 0, t_sym = 0;           // post-symmetry (compile-time kind; its table block at t_sym)
     int rng_mode = RNG_PHILOX;
     int math_mode = MATH_PRECISE;
     int threads = 128;

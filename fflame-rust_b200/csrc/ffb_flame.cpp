@@ -168,6 +168,22 @@ Flame parse_config(const Json& cfg) {
         if (x.final_att != F.fin_chain)
             fail("transforms with different final attachments are not supported by this build");
     if (F.fin_chain.size() > 8) fail("more than 8 chained final transforms are not supported");
+    // Post-symmetry (transforms.rs:2149-2167; serde: `ty` lowercase, the
+    // other fields required when the object is present).
+    if (const Json* ps = fl->get("post_symmetry"); ps && ps->kind == Json::Object) {
+        const std::string ty = ps->string_or("ty", "none");
+        F.sym.kind = ty == "none" ? 0 : ty == "xaxis" ? 1 : ty == "yaxis" ? 2 : ty == "point" ? 3 : -1;
+        if (F.sym.kind < 0) fail("unknown variant `" + ty + "`, expected one of `none`, `xaxis`, `yaxis`, `point`");
+        const float order = num_field(*ps, "order", true, 3.0f);
+        if (!(order >= 0.0f) || order != std::floor(order)) fail("`order` is not a u32");
+        F.sym.order = (int)std::min(std::max(order, 1.0f), 32.0f);           // clamp(1, 32): buffers.rs:958
+        F.sym.cx = num_field(*ps, "center_x", true, 0.0f);
+        F.sym.cy = num_field(*ps, "center_y", true, 0.0f);
+        F.sym.distance = num_field(*ps, "distance", true, 1.25f);
+        const float deg = num_field(*ps, "rotation_deg", true, 6.0f);
+        const float rads_per_deg = 3.14159265358979323846f / 180.0f;      // f32::to_radians
+        F.sym.rotation = deg * rads_per_deg;
+    }
     // Local variation order (transforms.rs:2297-2319): normals then finals.
     auto absorb = [&](const XForm& x) {
         for (auto& p : x.vars)

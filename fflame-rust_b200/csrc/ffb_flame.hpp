@@ -67,6 +67,17 @@ struct DensityEstimation {
     float curve = 0.4f;
 };
 
+// Plot-time symmetry (scene/transforms.rs:2093-2190, GpuPostSymmetry in
+// gpu/buffers.rs:936-966): every kept sample is plotted once per copy.
+struct PostSym {
+    int kind = 0;              // 0 none, 1 x axis (reflects y), 2 y axis (reflects x), 3 point
+    int order = 3;             // point mode: copies, clamped to 1..32
+    float cx = 0.0f, cy = 0.0f;
+    float distance = 1.25f;    // axis modes: total separation of the pair
+    float rotation = 0.0f;     // axis modes: pre-rotation, radians (rotation_deg.to_radians())
+    int copies() const { return kind == 0 ? 1 : kind == 3 ? order : 2; }
+};
+
 struct Flame {
     std::vector<XForm> xf;              // normal transforms
     std::vector<XForm> fin;             // final transforms pool
@@ -75,6 +86,7 @@ struct Flame {
     float zoom = 1.0f;
     double pan_x = 0.0, pan_y = 0.0;
     float rotation = 0.0f;
+    PostSym sym;
     // palette
     std::vector<float> stop_pos, stop_col;
     int palette_size = 256;

@@ -132,6 +132,40 @@ __device__ __forceinline__ void ffb_pcg_dispatch(const ffb_launch& J, PcgRng& rn
 }
 #endif
 
+#if FFB_SYM_KIND != 0
+// Copy k of a plotted point under the flame's post-symmetry
+// (utilities.wgsl:470-568): point mode rotates copy k by k*2pi/order about
+// the centre; the axis modes pan by half the separation, pre-rotate by
+// -rotation about the centre, and reflect copy 1.
+__device__ __forceinline__ void ffb_sym_copy(const float* __restrict__ sm, int k, float& x, float& y) {
+    const float cx = sm[T_SYM + 1], cy = sm[T_SYM + 2];
+#if FFB_SYM_KIND == 3
+    if (k == 0) return;
+    const float cs = sm[T_SYM + 6 + 2 * k], sn = sm[T_SYM + 7 + 2 * k];
+    const float dx = x - cx, dy = y - cy;
+    x = dx * cs - dy * sn + cx;
+    y = dx * sn + dy * cs + cy;
+#else
+#if FFB_SYM_KIND == 1
+    y = y + sm[T_SYM + 3];
+#else
+    x = x + sm[T_SYM + 3];
+#endif
+    const float cs = sm[T_SYM + 4], sn = sm[T_SYM + 5];
+    const float dx = x - cx, dy = y - cy;
+    x = dx * cs - dy * sn + cx;
+    y = dx * sn + dy * cs + cy;
+    if (k == 1) {
+#if FFB_SYM_KIND == 1
+        y = 2.0f * cy - y;
+#else
+        x = 2.0f * cx - x;
+#endif
+    }
+#endif
+}
+#endif
+
 // The rest of an iteration once transform k is picked and the opacity draw
 // made: affine, variations, post, bad-value respawn, colour, fuse, finals,
 // palette, world_to_pixel and the splat (main_template.wgsl:366-1320).
@@ -170,16 +204,26 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
     ffb_finals(sm, fx, fy, rng);                                            // main_template.wgsl:663-717
     const int pal_idx = ffb_palette_index(ci, J.pal_n);
     const float4 c = pal[pal_idx];                                          // main_template.wgsl:766-772
-    // world_to_pixel (utilities.wgsl:417-450).
-    float tx = fx - J.pan_x, ty = fy - J.pan_y;
-    float rx = tx * J.cos_r - ty * J.sin_r;
-    float ry = tx * J.sin_r + ty * J.cos_r;
-    rx = rx * J.zoom; ry = ry * J.zoom;
-    const float pxf = floorf(cx + rx * scale), pyf = floorf(cy + ry * scale);
-    if (plot && pxf >= 0.0f && pyf >= 0.0f && pxf < (float)J.width && pyf < (float)J.height) {
-        const u32 idx = (u32)pyf * (u32)J.width + (u32)pxf;
-        ffb_splat(J.hist, idx, c, pal_idx);
-        ++inframe;
+#if FFB_SYM_KIND != 0
+    const int ncopy = (int)sm[T_SYM];                                       // main_template.wgsl:747-755, 858-870
+    for (int sk = 0; sk < ncopy; ++sk) {
+        float sx = fx, sy = fy;
+        ffb_sym_copy(sm, sk, sx, sy);
+#else
+    {
+        const float sx = fx, sy = fy;
+#endif
+        // world_to_pixel (utilities.wgsl:417-450).
+        float tx = sx - J.pan_x, ty = sy - J.pan_y;
+        float rx = tx * J.cos_r - ty * J.sin_r;
+        float ry = tx * J.sin_r + ty * J.cos_r;
+        rx = rx * J.zoom; ry = ry * J.zoom;
+        const float pxf = floorf(cx + rx * scale), pyf = floorf(cy + ry * scale);
+        if (plot && pxf >= 0.0f && pyf >= 0.0f && pxf < (float)J.width && pyf < (float)J.height) {
+            const u32 idx = (u32)pyf * (u32)J.width + (u32)pxf;
+            ffb_splat(J.hist, idx, c, pal_idx);
+            ++inframe;
+        }
     }
 }
 

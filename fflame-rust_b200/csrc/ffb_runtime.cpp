@@ -1375,6 +1375,7 @@ FFB_API int ffb_diff_create(ffb_renderer* r, const char* config, size_t len, con
         if (d->P.ss != 1) fail(FFB_ERR_INVALID, "the differentiable render has no supersampling");
         if (!f.fin_chain.empty()) fail(FFB_ERR_CONFIG, "the differentiable render takes no final transforms");
         if (f.de.max_radius > 0.0f) fail(FFB_ERR_CONFIG, "the differentiable render takes no density estimation");
+        if (f.sym.kind != 0) fail(FFB_ERR_CONFIG, "the differentiable render takes no post-symmetry");
         if (job->transparent) fail(FFB_ERR_INVALID, "the differentiable render is opaque");
         if (f.tm.mode != 1 || f.tm.highlight != 0 || f.tm.saturation != 1.0f || f.tm.hue_shift != 0.0f)
             fail(FFB_ERR_CONFIG, "the differentiable tone map is the log mode with clip highlights and no HSV adjustment");

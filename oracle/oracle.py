@@ -70,6 +70,9 @@ class OFlame(ctypes.Structure):
         ("cos_r", ctypes.c_float), ("sin_r", ctypes.c_float),
         ("width", ctypes.c_int), ("height", ctypes.c_int),
         ("palette", ctypes.POINTER(ctypes.c_float)), ("pal_n", ctypes.c_int),
+        ("sym_kind", ctypes.c_int), ("sym_order", ctypes.c_int),
+        ("sym_cx", ctypes.c_float), ("sym_cy", ctypes.c_float), ("sym_distance", ctypes.c_float),
+        ("sym_rotation", ctypes.c_float),
     ]
 
 
@@ -196,6 +199,13 @@ class Flame:
         s.cos_r, s.sin_r = math.cos(rot), math.sin(rot)
         s.width, s.height = width, height
         s.palette, s.pal_n = _fp(self.palette), len(self.palette) // 3
+        ps = flame.get("post_symmetry")
+        if ps:
+            s.sym_kind = {"none": 0, "xaxis": 1, "yaxis": 2, "point": 3}[ps.get("ty", "none")]
+            s.sym_order = int(ps["order"])
+            s.sym_cx, s.sym_cy, s.sym_distance = ps["center_x"], ps["center_y"], ps["distance"]
+            # f32::to_radians: deg * f32(f32(pi) / 180)
+            s.sym_rotation = f32(f32(ps["rotation_deg"]) * f32(f32(math.pi) / f32(180.0)))
         self.s = s
         self.width, self.height = width, height
 
