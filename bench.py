@@ -161,7 +161,8 @@ def run_ours(args, rank, world, local_rank):
     W, H, ss = wl["width"], wl["height"], wl["supersample"]
     r = _native.Renderer(local_rank)
     job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, walker0=rank * wl["walkers"],
-               seed=0x5EED + 0, schedule=args.schedule, math=args.math, count_bits=wl.get("count_bits", 32))
+               seed=0x5EED + 0, schedule=args.schedule, math=args.math, count_bits=wl.get("count_bits", 32),
+               accumulate=args.accumulate)
     d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
     # The library's kernels and the timing events share one (non-default) stream.
     side = torch.cuda.Stream()
@@ -246,7 +247,8 @@ def run_ours(args, rank, world, local_rank):
     info = None
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        image = eng.render(cfg, W, H, iterations=req_iters, supersample=ss, walkers=wl["walkers"], exact=exact)
+        image = eng.render(cfg, W, H, iterations=req_iters, supersample=ss, walkers=wl["walkers"], exact=exact,
+                           accumulate=args.accumulate)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)
@@ -262,7 +264,7 @@ def run_ours(args, rank, world, local_rank):
         "data": "synthetic (seeded flame generator; no dataset)",
         "config": {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
                    "samples_per_step": samples_per_step, "walkers": wl["walkers"], "rng": "philox",
-                   "schedule": args.schedule, "math": args.math,
+                   "schedule": args.schedule, "math": args.math, "accumulate": args.accumulate,
                    "l2": f"histogram {W * ss * H * ss * (32 if exact else 16) / 1e6:.1f} MB > 126 MB L2, cleared every step",
                    "parallelism": f"walker shards x{world}" + (" + NCCL histogram all-reduce + row bands" if world > 1 else "")},
         "ms_per_frame": ms,
@@ -544,6 +546,8 @@ def main():
                     help="precise: IEEE-accurate sin/cos (the parity-tested path); sfu: the hardware's, as the reference GPU")
     ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted"],
                     help="walker scheduling of the chaos kernel (same orbits either way)")
+    ap.add_argument("--accumulate", default="auto", choices=["auto", "direct", "tiled"],
+                    help="exact mode: direct atomics on the histogram or tile-sorted accumulation")
     ap.add_argument("--profile", type=float, default=0.0,
                     help="profiling run for ncu: only the chaos kernel of the workload, at this many samples")
     args = ap.parse_args()
@@ -568,9 +572,10 @@ def main():
         wl = workload(args.workload)
         r = _native.Renderer(local_rank)
         job = dict(iterations=int(args.profile), walkers=wl["walkers"], supersample=wl["supersample"], seed=0x5EED,
-                   schedule=args.schedule)
+                   schedule=args.schedule, count_bits=wl.get("count_bits", 32), accumulate=args.accumulate)
+        hist = r.histogram_u64 if wl.get("count_bits", 32) == 64 else r.histogram
         for _ in range(args.warmup + args.steps):
-            _, _, o = r.histogram(json.dumps(wl["cfg"]), wl["width"], wl["height"], **job)
+            _, _, o = hist(json.dumps(wl["cfg"]), wl["width"], wl["height"], **job)
         print(json.dumps({"profile": args.workload, "samples": o.total_iterations, "inframe": o.inframe_samples,
                           "ms": o.render_time_ms}))
         return

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "ffb200", "libffb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["ffb_tail.cu", "ffb_diff_tail.cu", "ffb_runtime.cpp", "ffb_flame.cpp", "ffb_codegen.cpp"]
+SOURCES = ["ffb_tail.cu", "ffb_diff_tail.cu", "ffb_tiles.cu", "ffb_runtime.cpp", "ffb_flame.cpp", "ffb_codegen.cpp"]
 HEADERS = ["ffb_json.hpp", "ffb_flame.hpp", "ffb_codegen.hpp", "ffb_tail.cuh", "ffb_device.cuh", "ffb_kernels.cuh",
            "ffb_diff_jac.cuh", "ffb_diff.cuh"]
 

@@ -97,9 +97,10 @@ void emit_diff(std::ostringstream& s, const Plan& p) {
 }  // namespace
 
 Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads, bool per_xform, bool exact,
-               int diff_window, int diff_ckpt) {
+               int diff_window, int diff_ckpt, bool emit) {
     Plan p;
     p.exact = exact;
+    p.emit = emit;
     p.diff_window = diff_window;
     p.diff_ckpt = diff_ckpt;
     p.rng_mode = rng_mode;
@@ -138,6 +139,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     s << "#define FFB_RNG_MODE " << rng_mode << "\n#define FFB_THREADS " << threads << "\n";
     if (math_mode == MATH_SFU) s << "#define FFB_SFU 1\n";
     if (exact) s << "#define FFB_EXACT 1\n";
+    if (emit) s << "#define FFB_EMIT 1\n";
     s << "#define FFB_SYM_KIND " << p.sym_kind << "\n#define T_SYM " << p.t_sym << "\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
     s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw
@@ -214,7 +216,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
 
 bool plan_fits(const Plan& p, const Flame& f) {
     if ((int)f.xf.size() > p.maxx) return false;
-    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform, p.exact, p.diff_window, p.diff_ckpt);
+    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform, p.exact, p.diff_window, p.diff_ckpt, p.emit);
     return q.source == p.source;
 }
 

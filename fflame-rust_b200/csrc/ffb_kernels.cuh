@@ -84,6 +84,56 @@ __device__ __forceinline__ void ffb_splat(void* __restrict__ hist_v, u32 idx, fl
 #endif
 }
 
+#ifdef FFB_EMIT
+// Tile-sorted accumulation, first stage: instead of the splat, each sample
+// becomes a record (pixel index | palette index << 32).  Block b owns
+// segment b of the launch's record buffer (`hist`): threads x iterations x
+// symmetry copies records, as many as its walkers can produce, behind a
+// cursor in shared memory that each warp advances once for all its lanes;
+// the block's count follows the segments (ffb_emit_finish).  A record past
+// the segment (impossible by its size) sets counters[3].
+__shared__ u32 ffb_s_emit;
+
+__device__ __forceinline__ u64 ffb_seg_cap(const ffb_launch& J, u32 copies) {
+    return (u64)blockDim.x * J.n_iters * copies;
+}
+
+__device__ __forceinline__ void ffb_emit(const ffb_launch& J, bool valid, u32 idx, int pal_idx, u32 copies) {
+    const unsigned live = __activemask();
+    const unsigned m = __ballot_sync(live, valid);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(live) - 1;
+    u32 base = 0;
+    if (lane == leader) base = atomicAdd(&ffb_s_emit, (u32)__popc(m));
+    base = __shfl_sync(live, base, leader);
+    if (valid) {
+        const u64 cap = ffb_seg_cap(J, copies);
+        const u64 slot = (u64)base + (u64)__popc(m & ((1u << lane) - 1u));
+        if (slot < cap) reinterpret_cast<u64*>(J.hist)[(u64)blockIdx.x * cap + slot] = (u64)idx | ((u64)pal_idx << 32);
+        else atomicOr(reinterpret_cast<unsigned int*>(J.counters + 3), 1u);
+    }
+}
+
+// Every thread of the block: the block's record count after the segments.
+__device__ __forceinline__ void ffb_emit_finish(const ffb_launch& J, u32 copies) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const u64 cap = ffb_seg_cap(J, copies);
+        u32* counts = reinterpret_cast<u32*>(reinterpret_cast<u64*>(J.hist) + (u64)gridDim.x * cap);
+        counts[blockIdx.x] = (u32)min((u64)ffb_s_emit, cap);
+    }
+}
+#endif
+
+__device__ __forceinline__ u32 ffb_copies(const float* __restrict__ sm) {
+#if FFB_SYM_KIND != 0
+    return (u32)sm[T_SYM];
+#else
+    return 1u;
+#endif
+}
+
 // The job owning this block (block-uniform binary search) and its tables
 // staged in shared memory.
 __device__ __forceinline__ const ffb_launch& ffb_stage(const ffb_launch* __restrict__ jobs, int n_jobs, float* sm, float4*& pal) {
@@ -96,6 +146,9 @@ __device__ __forceinline__ const ffb_launch& ffb_stage(const ffb_launch* __restr
     for (int i = threadIdx.x; i < FFB_TABLE_SIZE; i += blockDim.x) sm[i] = J.table[i];
     pal = reinterpret_cast<float4*>(sm) + FFB_TABLE_VEC4;
     for (u32 i = threadIdx.x; i < J.pal_n; i += blockDim.x) pal[i] = J.palette[i];
+#ifdef FFB_EMIT
+    if (threadIdx.x == 0) ffb_s_emit = 0u;
+#endif
     __syncthreads();
     return J;
 }
@@ -219,11 +272,17 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
         float ry = tx * J.sin_r + ty * J.cos_r;
         rx = rx * J.zoom; ry = ry * J.zoom;
         const float pxf = floorf(cx + rx * scale), pyf = floorf(cy + ry * scale);
-        if (plot && pxf >= 0.0f && pyf >= 0.0f && pxf < (float)J.width && pyf < (float)J.height) {
+        const bool hit = plot && pxf >= 0.0f && pyf >= 0.0f && pxf < (float)J.width && pyf < (float)J.height;
+#ifdef FFB_EMIT
+        ffb_emit(J, hit, hit ? (u32)pyf * (u32)J.width + (u32)pxf : 0u, pal_idx, ffb_copies(sm));
+        inframe += hit ? 1u : 0u;
+#else
+        if (hit) {
             const u32 idx = (u32)pyf * (u32)J.width + (u32)pxf;
             ffb_splat(J.hist, idx, c, pal_idx);
             ++inframe;
         }
+#endif
     }
 }
 
@@ -234,15 +293,9 @@ __device__ __forceinline__ void ffb_count_inframe(const ffb_launch& J, u32 infra
     if ((threadIdx.x & 31) == (unsigned)(__ffs(live) - 1) && tot) atomicAdd(J.counters, (u64)tot);
 }
 
-// One walker a thread, for the whole launch.
-extern "C" __global__ void __launch_bounds__(FFB_THREADS)
-ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
-    extern __shared__ float4 ffb_smem4[];
-    float* sm = reinterpret_cast<float*>(ffb_smem4);
-    float4* pal;
-    const ffb_launch& J = ffb_stage(jobs, n_jobs, sm, pal);
-    const u32 w = (blockIdx.x - J.block0) * blockDim.x + threadIdx.x;
-    if (w >= J.n_walkers) return;
+// One walker's whole launch (the body of ffb_chaos).
+__device__ __forceinline__ void ffb_chaos_walker(const float* __restrict__ sm, const float4* __restrict__ pal,
+                                                 const ffb_launch& J, u32 w) {
     const u32 gw = J.walker0 + w;
     const int n_xf = (int)J.n_xf;
     float x, y, ci;
@@ -269,6 +322,20 @@ ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
     }
     J.walkers[w] = make_float4(x, y, ci, __uint_as_float(fuse));
     ffb_count_inframe(J, inframe);
+}
+
+// One walker a thread, for the whole launch.
+extern "C" __global__ void __launch_bounds__(FFB_THREADS)
+ffb_chaos(const ffb_launch* __restrict__ jobs, int n_jobs) {
+    extern __shared__ float4 ffb_smem4[];
+    float* sm = reinterpret_cast<float*>(ffb_smem4);
+    float4* pal;
+    const ffb_launch& J = ffb_stage(jobs, n_jobs, sm, pal);
+    const u32 w = (blockIdx.x - J.block0) * blockDim.x + threadIdx.x;
+    if (w < J.n_walkers) ffb_chaos_walker(sm, pal, J, w);
+#ifdef FFB_EMIT
+    ffb_emit_finish(J, ffb_copies(sm));                  // every thread reaches its barrier
+#endif
 }
 
 // Transform-coherent scheduling.  A thread holds a walker only for one
@@ -372,6 +439,9 @@ ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
     }
     if (active) J.walkers[wid - J.walker0] = make_float4(x, y, ci, __uint_as_float(fuse));
     ffb_count_inframe(J, inframe);
+#ifdef FFB_EMIT
+    ffb_emit_finish(J, ffb_copies(sm));
+#endif
 }
 
 // The variation probe (main_template.wgsl:1467-1567): transform xi's

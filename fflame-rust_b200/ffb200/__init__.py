@@ -69,7 +69,7 @@ class Engine:
 
     def render(self, config, width, height, *, iterations=None, iterations_per_thread=None,
                transparent=False, premultiplied=False, sticky=False, sequence=False, supersample=None, walkers=None,
-               exact=False):
+               exact=False, accumulate=None):
         """A config (dict, JSON, or a path) at `width` x `height` (python/pyfae/__init__.py:201-221).
 
         `iterations`: the flame's budget (default: the config's own).
@@ -77,7 +77,8 @@ class Engine:
         renders at twice the size and boxes it down with the firefly clamp;
         `walkers` fixes the number of concurrent orbits (default: sized to
         the budget); `exact` accumulates u64 counts and fixed-point colour
-        sums (long renders, order-independent results).
+        sums (long renders, order-independent results); `accumulate`
+        ("direct" or "tiled") picks how the exact sums are gathered.
         """
         text = _text(config)
         request = {"fn": "render", "config": text, "width": width, "height": height,
@@ -93,5 +94,7 @@ class Engine:
             request["walkers"] = int(walkers)
         if exact:
             request["exact"] = True
+        if accumulate:
+            request["accumulate"] = accumulate
         out, info = self._call(request)
         return Image(self, out, info, text)

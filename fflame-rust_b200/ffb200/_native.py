@@ -47,7 +47,7 @@ class Job(ctypes.Structure):
         ("supersample", ctypes.c_uint32), ("rng", ctypes.c_int32), ("math", ctypes.c_int32),
         ("transparent", ctypes.c_int32), ("threads", ctypes.c_int32), ("seed", ctypes.c_uint64),
         ("walker0", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("count_bits", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("accumulate", ctypes.c_uint32),
     ]
 
 
@@ -112,8 +112,12 @@ def _text(config):
 SCHEDULE = {"auto": 0, "plain": 1, "sorted": 2}
 
 
+ACCUMULATE = {"auto": 0, "direct": 1, "tiled": 2}
+
+
 def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0, walkers=0, supersample=1,
-             rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0, schedule="auto", count_bits=32):
+             rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0, schedule="auto", count_bits=32,
+             accumulate="auto"):
     j = Job()
     j.width, j.height, j.iterations = width, height, int(iterations or 0)
     j.iterations_per_thread, j.burn_in, j.walkers = iterations_per_thread, burn_in, walkers
@@ -123,6 +127,7 @@ def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0
     j.transparent, j.threads, j.seed, j.walker0 = int(transparent), threads, int(seed), walker0
     j.schedule = SCHEDULE[schedule] if isinstance(schedule, str) else schedule
     j.count_bits = count_bits
+    j.accumulate = ACCUMULATE[accumulate] if isinstance(accumulate, str) else accumulate
     return j
 
 

@@ -86,7 +86,10 @@ typedef struct {
                                           integer accumulation -- u64 count and u64 colour sums in 24-bit
                                           fixed point (32 B a pixel), independent of the atomics' order
                                           (the exact count of accumulate.wgsl:185-199) */
-    uint32_t reserved;
+    uint32_t accumulate;               /* exact mode: 0 auto (tile-sorted above a 512 MB histogram, else
+                                          direct), 1 direct (a splat's atomics on the histogram), 2
+                                          tile-sorted (samples emitted as records, sorted by 64x64 tile,
+                                          summed in shared memory; the same bits as direct) */
 } ffb_job;
 
 /* RenderOutput (src/renderer/render.rs:207-218). */
