@@ -16,9 +16,10 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "ffb200", "libffb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["ffb_tail.cu", "ffb_diff_tail.cu", "ffb_tiles.cu", "ffb_runtime.cpp", "ffb_flame.cpp", "ffb_codegen.cpp"]
+SOURCES = ["ffb_tail.cu", "ffb_diff_tail.cu", "ffb_tiles.cu", "ffb_runtime.cpp", "ffb_flame.cpp", "ffb_codegen.cpp",
+           "ffb_png.cpp"]
 HEADERS = ["ffb_json.hpp", "ffb_flame.hpp", "ffb_codegen.hpp", "ffb_tail.cuh", "ffb_device.cuh", "ffb_kernels.cuh",
-           "ffb_diff_jac.cuh", "ffb_diff.cuh"]
+           "ffb_diff_jac.cuh", "ffb_diff.cuh", "ffb_png.hpp"]
 
 
 def embed():
@@ -55,7 +56,7 @@ def build(force=False, verbose=False):
            "-gencode", "arch=compute_100a,code=sm_100a",
            "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",
            "-I", os.path.join(HERE, "..", "include"),
-           "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lnvrtc"]
+           "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lnvrtc", "-lz"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

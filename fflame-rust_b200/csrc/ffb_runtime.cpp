@@ -30,6 +30,7 @@
 #include "ffb_codegen.hpp"
 #include "ffb_flame.hpp"
 #include "ffb_json.hpp"
+#include "ffb_png.hpp"
 #include "ffb_tail.cuh"
 
 #define FFB_API extern "C" __attribute__((visibility("default")))
@@ -602,7 +603,33 @@ uint32_t u32_arg(const Json& r, const char* k) {
     return (uint32_t)v->num;
 }
 
-void fae_dispatch(const Json& r, std::vector<uint8_t>& out, std::string& info) {
+// A frame as the PNG the reference's CLI writes (wasm/python/src/render.rs:97-103,
+// src/png_metadata.rs:61-183): the config, the render's numbers and the
+// tone map's settings in tEXt chunks.
+std::vector<uint8_t> encode_png_bytes(const std::string& config, const uint8_t* rgba, size_t len, uint32_t w, uint32_t h,
+                                      uint64_t iterations, double ms, uint32_t ipt) {
+    if (!rgba || len != (size_t)w * h * 4)
+        fail(FFB_ERR_INVALID, std::to_string(len) + " bytes are not " + std::to_string(w) + "x" + std::to_string(h) + " RGBA");
+    if (w == 0 || h == 0) fail(FFB_ERR_INVALID, "width and height must be nonzero");
+    Flame f;
+    PngInfo in;
+    try {
+        JsonPtr j = json_parse(config);
+        f = parse_config(*j);
+        in.speed_factor = (float)j->number_or("speed_factor", 0.5);
+    } catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
+    in.software = ffb_version();
+    in.build_date = __DATE__ " " __TIME__;
+    for (int k = 0; k < 3; ++k) in.background[k] = f.tm.background[k];
+    in.exposure = f.tm.exposure;
+    in.gamma = f.tm.gamma;
+    in.tone_curve = f.tm.curve.size() > 2;
+    in.variations = f.local.size();
+    try { return png_encode(rgba, w, h, png_metadata(config, w, h, iterations, ms, ipt, in)); }
+    catch (const std::exception& e) { fail(FFB_ERR_INVALID, e.what()); }
+}
+
+void fae_dispatch(const Json& r, const uint8_t* data, size_t data_len, std::vector<uint8_t>& out, std::string& info) {
     const Json* fn = r.get("fn");
     if (!fn || fn->kind != Json::String) fail(FFB_ERR_INVALID, "`fn` is missing");
     const std::string& f = fn->str;
@@ -647,8 +674,15 @@ void fae_dispatch(const Json& r, std::vector<uint8_t>& out, std::string& info) {
         w.begin().num("width", job.width).num("height", job.height).num("iterations", (double)o.total_iterations)
             .num("ms", o.render_time_ms).num("iterations_per_thread", job.iterations_per_thread).end();
         info = w.s();
+    } else if (f == "encode_png") {                                     // wasm/python/src/lib.rs:227-232
+        const Json* c = r.get("config");
+        if (!c || c->kind != Json::String) fail(FFB_ERR_INVALID, "`config` (a string) is missing");
+        out = encode_png_bytes(c->str, data, data_len, u32_arg(r, "width"), u32_arg(r, "height"),
+                               (uint64_t)r.number_or("iterations", 0.0), r.number_or("ms", 0.0),
+                               (uint32_t)r.number_or("iterations_per_thread", 0.0));
+        info = "null";
     } else {
-        fail(FFB_ERR_INVALID, "`" + f + "` is not supported by this build (render, info, variations)");
+        fail(FFB_ERR_INVALID, "`" + f + "` is not supported by this build (render, encode_png, info, variations)");
     }
 }
 
@@ -658,6 +692,18 @@ void fae_dispatch(const Json& r, std::vector<uint8_t>& out, std::string& info) {
 // ================================================================ ABI ====
 FFB_API const char* ffb_last_error(void) { return g_err.c_str(); }
 FFB_API const char* ffb_version(void) { return "ffb200 0.1.0 (sm_100a)"; }
+
+FFB_API int ffb_encode_png(const char* config, size_t config_len, const uint8_t* rgba, uint32_t width, uint32_t height,
+                           uint64_t iterations, double ms, uint32_t iterations_per_thread, const uint8_t** out, size_t* out_len) {
+    static thread_local std::vector<uint8_t> png;
+    return guard([&] {
+        if (!config || !out || !out_len) fail(FFB_ERR_INVALID, "NULL argument");
+        png = encode_png_bytes(std::string(config, config_len), rgba, (size_t)width * height * 4, width, height, iterations, ms,
+                               iterations_per_thread);
+        *out = png.data();
+        *out_len = png.size();
+    });
+}
 
 FFB_API int ffb_renderer_create(int device, ffb_renderer** out) {
     return guard([&] {
@@ -1669,7 +1715,6 @@ FFB_API const uint8_t* fae_info_ptr(void) { return g_info.data(); }
 FFB_API size_t fae_info_len(void) { return g_info.size(); }
 
 FFB_API int32_t fae_call(const uint8_t* req, size_t req_len, const uint8_t* data, size_t data_len) {
-    (void)data; (void)data_len;
     std::vector<uint8_t> out;
     std::string info;
     int st = guard([&] {
@@ -1678,7 +1723,7 @@ FFB_API int32_t fae_call(const uint8_t* req, size_t req_len, const uint8_t* data
         try { j = json_parse(text); }
         catch (const std::exception& e) { fail(FFB_ERR_INVALID, std::string("request is not JSON: ") + e.what()); }
         std::lock_guard<std::mutex> lk(g_fae_mu);
-        fae_dispatch(*j, out, info);
+        fae_dispatch(*j, data, data_len, out, info);
     });
     if (st == FFB_OK) {
         g_output = std::move(out);

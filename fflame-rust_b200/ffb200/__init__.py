@@ -47,6 +47,20 @@ class Image:
         import numpy as np
         return np.frombuffer(self.rgba, np.uint8).reshape(self.height, self.width, 4)
 
+    def png(self):
+        """The PNG the reference's CLI writes for this frame, its config and
+        numbers in the metadata (python/pyfae/__init__.py:88-97)."""
+        out, _ = self.engine._module.call({
+            "fn": "encode_png", "config": self.config if isinstance(self.config, str) else self.config.decode(),
+            "width": self.width, "height": self.height, "iterations": self.info.get("iterations", 0),
+            "ms": self.info.get("ms", 0.0), "iterations_per_thread": self.info.get("iterations_per_thread", 1024),
+        }, self.rgba)
+        return out
+
+    def save(self, path):
+        with open(path, "wb") as f:
+            f.write(self.png())
+
 
 class Engine:
     """The engine (pyfae.Engine, python/pyfae/__init__.py:159-221)."""

@@ -28,7 +28,7 @@ EXPORTS = [
     "ffb_hist_unpack", "ffb_finish_device", "ffb_histogram_u64", "ffb_batch_create", "ffb_batch_run",
     "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
     "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
-    "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize",
+    "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize", "ffb_encode_png",
 ]
 
 
@@ -361,3 +361,17 @@ def density_estimate_static(d_hist, width, height, max_radius, min_radius=0.0, c
     _check(lib().ffb_density_estimate_static(ctypes.c_void_p(d_hist), ctypes.c_uint32(width), ctypes.c_uint32(height),
                                              ctypes.c_float(max_radius), ctypes.c_float(min_radius), ctypes.c_float(curve),
                                              ctypes.c_void_p(d_out), ctypes.c_void_p(stream or 0)))
+
+
+def encode_png(config, rgba, width, height, iterations=0, ms=0.0, iterations_per_thread=1024):
+    """A frame (RGBA8 bytes or array) as the PNG the reference's CLI writes,
+    the config and the render's numbers in its tEXt chunks (no GPU needed)."""
+    cfg = _text(config)
+    data = bytes(rgba) if not isinstance(rgba, np.ndarray) else np.ascontiguousarray(rgba, np.uint8).tobytes()
+    if len(data) != width * height * 4:
+        raise EngineError(f"{len(data)} bytes are not {width}x{height} RGBA")
+    out, n = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+    _check(lib().ffb_encode_png(cfg, ctypes.c_size_t(len(cfg)), data, ctypes.c_uint32(width), ctypes.c_uint32(height),
+                                ctypes.c_uint64(int(iterations)), ctypes.c_double(ms), ctypes.c_uint32(iterations_per_thread),
+                                ctypes.byref(out), ctypes.byref(n)))
+    return ctypes.string_at(out, n.value)

@@ -46,7 +46,9 @@ size_t fae_output_len(void);
 const uint8_t* fae_info_ptr(void);
 size_t fae_info_len(void);
 /* wasm/python/src/lib.rs:84-101: one call; 0, or 1 with the error's text
- * as the output.  Calls: "info", "variations", "render". */
+ * as the output.  Calls: "info", "variations", "render", "encode_png"
+ * ({config, width, height, iterations, ms, iterations_per_thread} with the
+ * RGBA8 frame as `data`: the PNG as the output, lib.rs:227-232). */
 int32_t fae_call(const uint8_t* req, size_t req_len, const uint8_t* data, size_t data_len);
 
 /* ---------------------------------------------------------- typed API --- */
@@ -110,6 +112,17 @@ typedef struct ffb_renderer ffb_renderer;   /* FlameRenderer: a device, a stream
 const char* ffb_last_error(void);
 /* Build version and the device it would use. */
 const char* ffb_version(void);
+
+/* A frame (width*height*4 RGBA8 bytes) as the PNG the reference's CLI
+ * writes: the config (.fae JSON) and the render's numbers in tEXt chunks
+ * under src/png_metadata.rs:144-183's keys (Software, Resolution,
+ * Iterations, RenderTime, IterationsPerThread, SpeedFactor, ConfigChecksum
+ * "sha256:<hex>", Config, BackgroundColor, Exposure, Gamma, ToneCurve, ...).
+ * `rgba` must hold width*height*4 bytes.  *out points at a buffer of the
+ * library's, valid until the calling thread's next call.  Host memory
+ * only; needs no GPU. */
+int ffb_encode_png(const char* config, size_t config_len, const uint8_t* rgba, uint32_t width, uint32_t height,
+                   uint64_t iterations, double ms, uint32_t iterations_per_thread, const uint8_t** out, size_t* out_len);
 
 int ffb_renderer_create(int device, ffb_renderer** out);
 void ffb_renderer_destroy(ffb_renderer* r);
