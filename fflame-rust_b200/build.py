@@ -17,9 +17,9 @@ OUT = os.path.join(HERE, "ffb200", "libffb200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 SOURCES = ["ffb_tail.cu", "ffb_diff_tail.cu", "ffb_tiles.cu", "ffb_runtime.cpp", "ffb_flame.cpp", "ffb_codegen.cpp",
-           "ffb_png.cpp"]
+           "ffb_png.cpp", "ffb_flame_xml.cpp"]
 HEADERS = ["ffb_json.hpp", "ffb_flame.hpp", "ffb_codegen.hpp", "ffb_tail.cuh", "ffb_device.cuh", "ffb_kernels.cuh",
-           "ffb_diff_jac.cuh", "ffb_diff.cuh", "ffb_png.hpp"]
+           "ffb_diff_jac.cuh", "ffb_diff.cuh", "ffb_png.hpp", "ffb_flame_xml.hpp"]
 
 
 def embed():

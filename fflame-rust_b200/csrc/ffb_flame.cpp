@@ -147,6 +147,14 @@ Flame parse_config(const Json& cfg) {
     for (auto& t : ts->arr) F.xf.push_back(parse_transform(*t));
     if (const Json* lt = fl->get("linked_transforms"); lt && lt->kind == Json::Array && !lt->arr.empty())
         fail("linked transforms are not supported by this build");
+    // Xaos (utilities.wgsl:110-137): a chaos matrix of all ones is the plain pick.
+    if (const Json* xa = fl->get("xaos"); xa && xa->kind == Json::Array)
+        for (auto& row : xa->arr)
+            if (row->kind == Json::Array)
+                for (auto& v : row->arr)
+                    if (v->kind == Json::Number && v->num != 1.0) fail("xaos (a chaos matrix) is not supported by this build");
+    if (const Json* so = fl->get("solo_transform"); so && so->kind == Json::Number)
+        fail("a solo transform is not supported by this build");
     if (const Json* ft = fl->get("final_transforms"); ft && ft->kind == Json::Array)
         for (auto& t : ft->arr) F.fin.push_back(parse_transform(*t));
     // A legacy singular final joins the pool attached to every normal

@@ -31,6 +31,7 @@
 #include "ffb_flame.hpp"
 #include "ffb_json.hpp"
 #include "ffb_png.hpp"
+#include "ffb_flame_xml.hpp"
 #include "ffb_tail.cuh"
 
 #define FFB_API extern "C" __attribute__((visibility("default")))
@@ -674,6 +675,15 @@ void fae_dispatch(const Json& r, const uint8_t* data, size_t data_len, std::vect
         w.begin().num("width", job.width).num("height", job.height).num("iterations", (double)o.total_iterations)
             .num("ms", o.render_time_ms).num("iterations_per_thread", job.iterations_per_thread).end();
         info = w.s();
+    } else if (f == "flame_import") {                                   // wasm/python/src/lib.rs:214-218
+        const Json* x = r.get("xml");
+        if (!x || x->kind != Json::String) fail(FFB_ERR_INVALID, "`xml` (a string) is missing");
+        std::vector<std::string> cfgs;
+        try { cfgs = flame_xml_import(x->str); }
+        catch (const std::exception& e) { fail(FFB_ERR_CONFIG, e.what()); }
+        std::string a = "[";
+        for (size_t i = 0; i < cfgs.size(); ++i) a += (i ? "," : "") + JsonWriter::quote(cfgs[i]);
+        info = "{\"result\":" + a + "]}";
     } else if (f == "encode_png") {                                     // wasm/python/src/lib.rs:227-232
         const Json* c = r.get("config");
         if (!c || c->kind != Json::String) fail(FFB_ERR_INVALID, "`config` (a string) is missing");
@@ -682,7 +692,7 @@ void fae_dispatch(const Json& r, const uint8_t* data, size_t data_len, std::vect
                                (uint32_t)r.number_or("iterations_per_thread", 0.0));
         info = "null";
     } else {
-        fail(FFB_ERR_INVALID, "`" + f + "` is not supported by this build (render, encode_png, info, variations)");
+        fail(FFB_ERR_INVALID, "`" + f + "` is not supported by this build (render, encode_png, flame_import, info, variations)");
     }
 }
 
@@ -692,6 +702,21 @@ void fae_dispatch(const Json& r, const uint8_t* data, size_t data_len, std::vect
 // ================================================================ ABI ====
 FFB_API const char* ffb_last_error(void) { return g_err.c_str(); }
 FFB_API const char* ffb_version(void) { return "ffb200 0.1.0 (sm_100a)"; }
+
+FFB_API int ffb_flame_import(const char* xml, size_t xml_len, const char** out, size_t* out_len) {
+    static thread_local std::string json;
+    return guard([&] {
+        if (!xml || !out || !out_len) fail(FFB_ERR_INVALID, "NULL argument");
+        std::vector<std::string> cfgs;
+        try { cfgs = flame_xml_import(std::string(xml, xml_len)); }
+        catch (const std::exception& e) { fail(FFB_ERR_CONFIG, e.what()); }
+        json = "[";
+        for (size_t i = 0; i < cfgs.size(); ++i) json += (i ? "," : "") + cfgs[i];
+        json += "]";
+        *out = json.c_str();
+        *out_len = json.size();
+    });
+}
 
 FFB_API int ffb_encode_png(const char* config, size_t config_len, const uint8_t* rgba, uint32_t width, uint32_t height,
                            uint64_t iterations, double ms, uint32_t iterations_per_thread, const uint8_t** out, size_t* out_len) {

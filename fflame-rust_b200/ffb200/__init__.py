@@ -77,6 +77,15 @@ class Engine:
     def info(self):
         return self._data({"fn": "info"})
 
+    def flame_import(self, xml):
+        """`.flame` XML -> config JSON strings, one a flame (wasm/python/src/lib.rs:214-218)."""
+        if isinstance(xml, (bytes, bytearray)):
+            xml = bytes(xml).decode("utf-8")
+        elif not (isinstance(xml, str) and xml.lstrip().startswith("<")):
+            with open(xml, encoding="utf-8") as f:                 # a path
+                xml = f.read()
+        return self._data({"fn": "flame_import", "xml": xml})
+
     def variations(self):
         """{name: [parameter names]} in registration order."""
         return {v["name"]: v["params"] for v in self._data({"fn": "variations"})}

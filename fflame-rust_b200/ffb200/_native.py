@@ -29,6 +29,7 @@ EXPORTS = [
     "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
     "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
     "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize", "ffb_encode_png",
+    "ffb_flame_import",
 ]
 
 
@@ -375,3 +376,12 @@ def encode_png(config, rgba, width, height, iterations=0, ms=0.0, iterations_per
                                 ctypes.c_uint64(int(iterations)), ctypes.c_double(ms), ctypes.c_uint32(iterations_per_thread),
                                 ctypes.byref(out), ctypes.byref(n)))
     return ctypes.string_at(out, n.value)
+
+
+def flame_import(xml):
+    """Apophysis / JWildfire `.flame` XML (text or bytes) -> a list of config
+    dicts, one a flame (2-D; a 3-D camera is refused with the reason)."""
+    data = xml.encode() if isinstance(xml, str) else bytes(xml)
+    out, n = ctypes.c_char_p(), ctypes.c_size_t()
+    _check(lib().ffb_flame_import(data, ctypes.c_size_t(len(data)), ctypes.byref(out), ctypes.byref(n)))
+    return json.loads(ctypes.string_at(out, n.value).decode())

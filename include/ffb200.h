@@ -46,7 +46,8 @@ size_t fae_output_len(void);
 const uint8_t* fae_info_ptr(void);
 size_t fae_info_len(void);
 /* wasm/python/src/lib.rs:84-101: one call; 0, or 1 with the error's text
- * as the output.  Calls: "info", "variations", "render", "encode_png"
+ * as the output.  Calls: "info", "variations", "render", "flame_import"
+ * ({xml}: the configs, lib.rs:214-218), "encode_png"
  * ({config, width, height, iterations, ms, iterations_per_thread} with the
  * RGBA8 frame as `data`: the PNG as the output, lib.rs:227-232). */
 int32_t fae_call(const uint8_t* req, size_t req_len, const uint8_t* data, size_t data_len);
@@ -112,6 +113,13 @@ typedef struct ffb_renderer ffb_renderer;   /* FlameRenderer: a device, a stream
 const char* ffb_last_error(void);
 /* Build version and the device it would use. */
 const char* ffb_version(void);
+
+/* Apophysis / JWildfire `.flame` XML -> `.fae` configs (src/flame_xml.rs:
+ * 41-425): *out is a JSON array of config objects, one a <flame> /
+ * <jwf-flame> element, in a buffer of the library's valid until the calling
+ * thread's next call.  The configs are 2-D (this build's path); a flame
+ * with a 3-D camera is refused with the reason.  Needs no GPU. */
+int ffb_flame_import(const char* xml, size_t xml_len, const char** out, size_t* out_len);
 
 /* A frame (width*height*4 RGBA8 bytes) as the PNG the reference's CLI
  * writes: the config (.fae JSON) and the render's numbers in tEXt chunks
