@@ -4,7 +4,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <sstream>
+#include <stdexcept>
 
 #include "ffb_device_src.inc"
 
@@ -13,6 +15,7 @@ namespace ffb {
 namespace {
 
 constexpr int kSymBlock = 6 + 64;            // post-symmetry table block (floats)
+constexpr int kMaxDrawSlots = 64;            // draws an iteration (pick, opacity, variations)
 
 // Normal-phase variations: those a normal transform uses at a weight other
 // than 0, in local order.  The reference emits every active variation and
@@ -35,25 +38,87 @@ std::vector<const VarDef*> final_vars(const Flame& f, const XForm& x) {
     return out;
 }
 
-std::string call(const VarDef* v, const std::string& prm0, const std::string& prm1, int slot) {
+// Where one call of a variation finds its inputs, as source expressions:
+// its packed parameter row (`prm(q)`), its own weight and its transform's
+// affine (`xf(0..5)` = a..f), and the first of its draw slots.
+struct Site {
+    std::function<std::string(int)> prm;
+    std::string w;
+    std::function<std::string(int)> xf;
+    int slot = -1;
+};
+
+// Normal transform k's site (k a source expression).
+Site normal_site(const Plan& p, int j, const std::string& k) {
+    Site c;
+    const int off = p.vp_off[j];
+    c.prm = [off, k](int q) { return "sm[T_VP + " + std::to_string(off + q) + " * FFB_MAXX + " + k + "]"; };
+    c.w = "sm[T_VW + " + std::to_string(j) + " * FFB_MAXX + " + k + "]";
+    c.xf = [k](int f) { return "sm[T_XF + " + std::to_string(f) + " * FFB_MAXX + " + k + "]"; };
+    c.slot = p.normal_slot[j];
+    return c;
+}
+
+// Final c's site: its record q (affine at q[0..5], weights at q[13..]).
+Site final_site(const Plan::Fin& fi, int j) {
+    Site c;
+    const int nv = (int)fi.vars.size(), off = 13 + nv + fi.prm_off[j];
+    c.prm = [off](int q) { return "q[" + std::to_string(off + q) + "]"; };
+    c.w = "q[" + std::to_string(13 + j) + "]";
+    c.xf = [](int f) { return "q[" + std::to_string(f) + "]"; };
+    c.slot = fi.slot[j];
+    return c;
+}
+
+// `v_name(px, py[, rng, slot][, params...][, w][, a..f], ox, oy)`.
+std::string call(const VarDef* v, const Site& c, const char* px = "x", const char* py = "y") {
     std::ostringstream o;
-    o << v->fn << "(x, y";
-    if (v->needs_rng) o << ", rng.draw(" << slot << ")";
-    if (v->nparams >= 1) o << ", " << prm0;
-    if (v->nparams >= 2) o << ", " << prm1;
+    o << v->fn << "(" << px << ", " << py;
+    if (v->draws) o << ", rng, " << c.slot;
+    for (int q = 0; q < v->slots(); ++q) o << ", " << c.prm(q);
+    if (v->flags & VF_W) o << ", " << c.w;
+    if (v->flags & VF_XF) for (int f = 0; f < 6; ++f) o << ", " << c.xf(f);
     o << ", ox, oy)";
     return o.str();
 }
 
-// The Jacobian of a variation body (ffb_diff.cuh): "v_name" -> "dj_name".
-std::string jcall(const VarDef* v, const std::string& prm0, const std::string& prm1, int slot) {
+// The Jacobian of a variation body (ffb_diff_jac.cuh): "v_name" -> "dj_name".
+// Only variations flagged VF_JAC have one; they take at most one draw.
+std::string jcall(const VarDef* v, const Site& c) {
     std::ostringstream o;
     o << "dj_" << (v->fn + 2) << "(x, y";
-    if (v->needs_rng) o << ", rng.draw(" << slot << ")";
-    if (v->nparams >= 1) o << ", " << prm0;
-    if (v->nparams >= 2) o << ", " << prm1;
+    if (v->draws) o << ", rng.draw(" << c.slot << ")";
+    for (int q = 0; q < v->slots(); ++q) o << ", " << c.prm(q);
     o << ")";
     return o.str();
+}
+
+// The three phases of apply_variations (shader_builder_v2.rs:2589-2800):
+// Pre variations replace the input point in turn (`temp = V(temp)`), the
+// others sum `w * V(temp)` from zero, Post variations replace the sum
+// (`result = V(result)`); each gated on its weight, in local order within
+// its phase.  `site(j)` locates variation j of `vars`; `gate` false drops
+// the weight test (the per-transform form lists only the variations the
+// transform uses).
+void emit_phases(std::ostringstream& s, const std::vector<const VarDef*>& vars,
+                 const std::function<Site(int)>& site, const char* ind, bool gate) {
+    s << ind << "float tx = x, ty = y, rx = 0.0f, ry = 0.0f, ox, oy;\n";
+    auto open = [&](const Site& c) {
+        s << ind << "{ const float w = " << c.w << "; " << (gate ? "if (w != 0.0f) { " : "{ ");
+    };
+    for (int pass = 0; pass < 3; ++pass) {
+        for (size_t j = 0; j < vars.size(); ++j) {
+            const VarDef* v = vars[j];
+            const int ph = (v->flags & VF_PRE) ? 0 : (v->flags & VF_POST) ? 2 : 1;
+            if (ph != pass) continue;
+            const Site c = site((int)j);
+            open(c);
+            if (ph == 0) s << call(v, c, "tx", "ty") << "; tx = ox; ty = oy;";
+            else if (ph == 1) s << call(v, c, "tx", "ty") << "; rx = rx + w * ox; ry = ry + w * oy;";
+            else s << call(v, c, "rx", "ry") << "; rx = ox; ry = oy;";
+            s << " } }   // " << v->name << "\n";
+        }
+    }
 }
 
 // The differentiable render's generated functions and kernels.
@@ -69,14 +134,10 @@ void emit_diff(std::ostringstream& s, const Plan& p) {
     s << "    J = make_float4(0.f, 0.f, 0.f, 0.f);\n    float ox, oy;\n";
     for (int j = 0; j < NVN; ++j) {
         const VarDef* v = p.normal[j];
-        std::ostringstream w, a0, a1;
-        w << "sm[T_VW + " << j << " * FFB_MAXX + k]";
-        a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + k]";
-        a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + k]";
-        s << "    { " << call(v, a0.str(), a1.str(), p.normal_slot[j]) << "; const float g = ax * ox + ay * oy; if (isfinite(g)) gw["
-          << j << " * P] += g;\n      const float w = " << w.str() << "; if (w != 0.0f) { const float4 jj = "
-          << jcall(v, a0.str(), a1.str(), p.normal_slot[j])
-          << "; J.x += w * jj.x; J.y += w * jj.y; J.z += w * jj.z; J.w += w * jj.w; } }   // " << v->name << "\n";
+        const Site c = normal_site(p, j, "k");
+        s << "    { " << call(v, c) << "; const float g = ax * ox + ay * oy; if (isfinite(g)) gw["
+          << j << " * P] += g;\n      const float w = " << c.w << "; if (w != 0.0f) { const float4 jj = "
+          << jcall(v, c) << "; J.x += w * jj.x; J.y += w * jj.y; J.z += w * jj.z; J.w += w * jj.w; } }   // " << v->name << "\n";
     }
     s << "    if (!(isfinite(J.x) && isfinite(J.y) && isfinite(J.z) && isfinite(J.w))) J = make_float4(0.f, 0.f, 0.f, 0.f);\n}\n";
     // One normal variation's value and Jacobian (the probe).
@@ -84,14 +145,17 @@ void emit_diff(std::ostringstream& s, const Plan& p) {
          "float& ox, float& oy, float4& J) {\n    switch (j) {\n";
     for (int j = 0; j < NVN; ++j) {
         const VarDef* v = p.normal[j];
-        std::ostringstream a0, a1;
-        a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + k]";
-        a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + k]";
-        s << "    case " << j << ": " << call(v, a0.str(), a1.str(), p.normal_slot[j]) << "; J = "
-          << jcall(v, a0.str(), a1.str(), p.normal_slot[j]) << "; break;\n";
+        const Site c = normal_site(p, j, "k");
+        s << "    case " << j << ": " << call(v, c) << "; J = " << jcall(v, c) << "; break;\n";
     }
     s << "    default: ox = 0.f; oy = 0.f; J = make_float4(0.f, 0.f, 0.f, 0.f); break;\n    }\n}\n";
     s << kDiffSrc << "\n";
+}
+
+std::string jac_names() {
+    std::string o;
+    for (const VarDef* v : registry_all()) if (v->flags & VF_JAC) o += (o.empty() ? "" : ", ") + std::string(v->name);
+    return o;
 }
 
 }  // namespace
@@ -109,24 +173,56 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     p.threads = threads;
     p.maxx = std::max<int>(maxx, (int)f.xf.size());
     p.normal = normal_vars(f);
-    int slot = 2;                                   // 0: transform pick, 1: opacity
-    for (const VarDef* v : p.normal) p.normal_slot.push_back(v->needs_rng ? slot++ : -1);
+    // Draw slots: 0 the transform pick, 1 the opacity test, then each
+    // NeedsRng variation's draws (consecutive, in its body's order): the
+    // normal phase's in local order, then each final's.
+    int slot = 2, vp = 0;
+    for (const VarDef* v : p.normal) {
+        p.normal_slot.push_back(v->draws ? slot : -1);
+        slot += v->draws;
+        p.vp_off.push_back(vp);
+        vp += v->slots();
+    }
+    p.vp_slots = vp;
     for (int c : f.fin_chain) {
         Plan::Fin fi;
         fi.vars = final_vars(f, f.fin[c]);
-        for (const VarDef* v : fi.vars) fi.slot.push_back(v->needs_rng ? slot++ : -1);
+        int fo = 0;
+        for (const VarDef* v : fi.vars) {
+            fi.slot.push_back(v->draws ? slot : -1);
+            slot += v->draws;
+            fi.prm_off.push_back(fo);
+            fo += v->slots();
+        }
+        fi.prm_slots = fo;
         p.fin.push_back(fi);
     }
     p.n_slots = slot;
+    // Philox words live in registers (4 a block): a bound keeps them there.
+    if (p.n_slots > kMaxDrawSlots)
+        throw std::runtime_error("the flame's variations take " + std::to_string(p.n_slots - 2) +
+                                 " random draws an iteration, over the " + std::to_string(kMaxDrawSlots - 2) + " this build carries");
+    if (diff_window > 0) {
+        // The adjoint differentiates the weighted sum through each
+        // variation's Jacobian; a variation without one (or outside the
+        // normal phase) cannot be differentiated here.
+        auto need = [](const VarDef* v) {
+            if (!(v->flags & VF_JAC))
+                throw std::runtime_error("variation `" + std::string(v->name) +
+                                         "` has no Jacobian in this build; the differentiable render supports " + jac_names());
+        };
+        for (const VarDef* v : p.normal) need(v);
+        for (auto& fi : p.fin) for (const VarDef* v : fi.vars) need(v);
+    }
     for (auto& x : f.xf) p.has_post |= x.post;
     const int M = p.maxx, NVN = (int)p.normal.size();
     p.t_cum = 1;
     p.t_xf = p.t_cum + M;
     p.t_vw = p.t_xf + 16 * M;
     p.t_vp = p.t_vw + NVN * M;
-    p.t_fin = p.t_vp + 2 * NVN * M;
+    p.t_fin = p.t_vp + p.vp_slots * M;
     int off = p.t_fin;
-    for (auto& fi : p.fin) { fi.off = off; off += 13 + 3 * (int)fi.vars.size(); }
+    for (auto& fi : p.fin) { fi.off = off; off += 13 + (int)fi.vars.size() + fi.prm_slots; }
     p.sym_kind = f.sym.kind;
     p.t_sym = off;
     if (p.sym_kind != 0) off += kSymBlock;
@@ -148,38 +244,24 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     // The normal phase (shader_builder_v2.rs:2714-2795): `result += w * V(p)`
     // from zero, in local order, each gated on its weight.
     s << "template <class R> __device__ __forceinline__ void ffb_normal(const float* __restrict__ sm, int k, float& x, float& y, R& rng) {\n";
-    s << "    float rx = 0.0f, ry = 0.0f, ox, oy;\n";
-    for (int j = 0; j < NVN; ++j) {
-        const VarDef* v = p.normal[j];
-        std::ostringstream w, a0, a1;
-        w << "sm[T_VW + " << j << " * FFB_MAXX + k]";
-        a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + k]";
-        a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + k]";
-        s << "    { const float w = " << w.str() << "; if (w != 0.0f) { " << call(v, a0.str(), a1.str(), p.normal_slot[j])
-          << "; rx = rx + w * ox; ry = ry + w * oy; } }   // " << v->name << "\n";
-    }
+    emit_phases(s, p.normal, [&](int j) { return normal_site(p, j, "k"); }, "    ", true);
     s << "    x = rx; y = ry;\n}\n";
     // Per-transform form for the sorted schedule, where k is (mostly)
     // warp-uniform: each case evaluates only its transform's variations, in
     // the same local order, straight-line (their chains overlap).
     s << "template <class R> __device__ __forceinline__ void ffb_normal_k(const float* __restrict__ sm, int k, float& x, float& y, R& rng) {\n";
     if (per_xform) {
-        s << "    float rx = 0.0f, ry = 0.0f, ox, oy;\n    switch (k) {\n";
+        s << "    switch (k) {\n";
         for (size_t k = 0; k < f.xf.size(); ++k) {
             s << "    case " << k << ": {\n";
-            for (int j = 0; j < NVN; ++j) {
-                const VarDef* v = p.normal[j];
-                if (f.xf[k].var_weight(v) == 0.0f) continue;
-                std::ostringstream w, a0, a1;
-                w << "sm[T_VW + " << j << " * FFB_MAXX + " << k << "]";
-                a0 << "sm[T_VP + " << (2 * j) << " * FFB_MAXX + " << k << "]";
-                a1 << "sm[T_VP + " << (2 * j + 1) << " * FFB_MAXX + " << k << "]";
-                s << "        { const float w = " << w.str() << "; " << call(v, a0.str(), a1.str(), p.normal_slot[j])
-                  << "; rx = rx + w * ox; ry = ry + w * oy; }   // " << v->name << "\n";
-            }
-            s << "        break; }\n";
+            std::vector<const VarDef*> used;
+            std::vector<int> idx;
+            for (int j = 0; j < NVN; ++j)
+                if (f.xf[k].var_weight(p.normal[j]) != 0.0f) { used.push_back(p.normal[j]); idx.push_back(j); }
+            emit_phases(s, used, [&](int u) { return normal_site(p, idx[u], std::to_string(k)); }, "        ", false);
+            s << "        x = rx; y = ry;\n        return; }\n";
         }
-        s << "    default: ffb_normal(sm, k, x, y, rng); return;\n    }\n    x = rx; y = ry;\n";
+        s << "    default: ffb_normal(sm, k, x, y, rng); return;\n    }\n";
     } else {
         s << "    ffb_normal(sm, k, x, y, rng);\n";
     }
@@ -187,20 +269,12 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     // One final of the chain (main_template.wgsl:679-704): affine,
     // variations, post-affine; `aff` false evaluates the variations alone.
     s << "template <class R> __device__ __forceinline__ void ffb_final_one(const float* __restrict__ sm, int c, float& x, float& y, R& rng, bool aff) {\n";
-    s << "    float rx = 0.0f, ry = 0.0f, ox, oy;\n    switch (c) {\n";
+    s << "    switch (c) {\n";
     for (size_t c = 0; c < p.fin.size(); ++c) {
         const Plan::Fin& fi = p.fin[c];
         s << "    case " << c << ": {\n        const float* q = sm + " << fi.off << ";\n";
         s << "        if (aff) { float ax = q[0] * x + q[1] * y + q[4]; float ay = q[2] * x + q[3] * y + q[5]; x = ax; y = ay; }\n";
-        const int nv = (int)fi.vars.size();
-        for (int j = 0; j < nv; ++j) {
-            std::ostringstream w, a0, a1;
-            w << "q[" << 13 + j << "]";
-            a0 << "q[" << 13 + nv + 2 * j << "]";
-            a1 << "q[" << 13 + nv + 2 * j + 1 << "]";
-            s << "        { const float w = " << w.str() << "; if (w != 0.0f) { " << call(fi.vars[j], a0.str(), a1.str(), fi.slot[j])
-              << "; rx = rx + w * ox; ry = ry + w * oy; } }   // " << fi.vars[j]->name << "\n";
-        }
+        emit_phases(s, fi.vars, [&](int j) { return final_site(fi, j); }, "        ", true);
         s << "        if (aff && q[12] > 0.5f) { float px = q[6] * rx + q[7] * ry + q[10]; float py = q[8] * rx + q[9] * ry + q[11]; rx = px; ry = py; }\n";
         s << "        x = rx; y = ry;\n        break; }\n";
     }
@@ -241,7 +315,9 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
         for (size_t j = 0; j < p.normal.size(); ++j) {
             const VarDef* v = p.normal[j];
             t[p.t_vw + j * M + k] = x.var_weight(v);
-            for (int q = 0; q < v->nparams; ++q) t[p.t_vp + (2 * j + q) * M + k] = x.param(v, q);
+            float row[kMaxVarSlots];
+            x.slot_values(v, row);
+            for (int q = 0; q < v->slots(); ++q) t[p.t_vp + (size_t)(p.vp_off[j] + q) * M + k] = row[q];
         }
     }
     if (p.sym_kind != 0) {
@@ -269,7 +345,9 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
         const int nv = (int)fi.vars.size();
         for (int j = 0; j < nv; ++j) {
             t[fi.off + 13 + j] = x.var_weight(fi.vars[j]);
-            for (int q = 0; q < fi.vars[j]->nparams; ++q) t[fi.off + 13 + nv + 2 * j + q] = x.param(fi.vars[j], q);
+            float row[kMaxVarSlots];
+            x.slot_values(fi.vars[j], row);
+            for (int q = 0; q < fi.vars[j]->slots(); ++q) t[fi.off + 13 + nv + fi.prm_off[j] + q] = row[q];
         }
     }
     return t;

@@ -25,8 +25,16 @@ enum MathMode { MATH_PRECISE = 0, MATH_SFU = 1 };
 struct Plan {
     int maxx = 0;                          // normal transforms (table capacity)
     std::vector<const VarDef*> normal;     // normal-phase variations, local order
-    std::vector<int> normal_slot;          // draw slot per normal variation (-1: none)
-    struct Fin { std::vector<const VarDef*> vars; std::vector<int> slot; int off = 0; };
+    std::vector<int> normal_slot;          // first draw slot per normal variation (-1: none)
+    std::vector<int> vp_off;               // each normal variation's first row of T_VP
+    int vp_slots = 0;                      // rows of T_VP (packed parameter slots)
+    struct Fin {
+        std::vector<const VarDef*> vars;
+        std::vector<int> slot;             // first draw slot (-1: none)
+        std::vector<int> prm_off;          // parameter offset after the weights
+        int prm_slots = 0;
+        int off = 0;
+    };
     std::vector<Fin> fin;                  // one per final in the chain
     bool has_post = false;
     int n_slots = 2;

@@ -343,7 +343,7 @@ extern "C" __global__ void ffb_dprobe(const float* __restrict__ table, int k, in
     __syncthreads();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    ArrayRng rng{words + (size_t)p * 16};
+    ArrayRng rng{words + (size_t)p * FFB_APPLY_WORDS};
     for (int j = 0; j < FFB_NVN; ++j) {
         float vx, vy;
         float4 J;

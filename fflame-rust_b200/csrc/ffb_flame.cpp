@@ -10,24 +10,95 @@
 
 namespace ffb {
 
+// The host restatements of the variations' `wgsl_init` (f32, the same
+// operations): user parameters -> derived values.
+namespace {
+void derive_julian(const float* u, float* o) {                 // advanced.rs:467-473
+    o[0] = u[1] / std::max(std::fabs(u[0]), 1e-30f) / 2.0f;
+}
+void derive_wedge(const float* u, float* o) {                  // extended.rs:273-281
+    const float angle_rad = u[0] * 3.14159265358979f / 180.0f;
+    o[0] = angle_rad;
+    o[1] = 1.0f - angle_rad * u[2] * 0.15915494309189534f;
+}
+void derive_radial_blur(const float* u, float* o) {            // extended.rs:867-874
+    const float half = u[0] * 3.14159265358979f / 360.0f;
+    o[0] = std::sin(half);
+    o[1] = std::cos(half);
+}
+void derive_perspective(const float* u, float* o) {            // simple_classics.rs:315-322
+    const float ang = u[0] * 1.5707963267948966f;
+    o[0] = std::sin(ang);
+    o[1] = u[1] * std::cos(ang);
+}
+}  // namespace
+
 // The variations this build carries, in the reference's registry order
-// (ALL_VARIATIONS, src/variations/defs/mod.rs:446).  Bodies live in
-// ffb_device.cuh; parameters and their defaults from the defs
-// (src/variations/defs/basic.rs, advanced.rs).
+// (ALL_VARIATIONS, src/variations/defs/mod.rs:446; `id` is the position
+// there).  Bodies live in ffb_device.cuh; parameters, their defaults, the
+// draws each body takes and the derived values from the defs
+// (src/variations/defs/*.rs, cited at each body).
+#define NP {nullptr}
+#define ND {0}
 static const VarDef kRegistry[] = {
-    {"linear", 0, false, 0, {nullptr, nullptr}, {0, 0}, "v_linear"},
-    {"sinusoidal", 1, false, 0, {nullptr, nullptr}, {0, 0}, "v_sinusoidal"},
-    {"spherical", 2, false, 0, {nullptr, nullptr}, {0, 0}, "v_spherical"},
-    {"swirl", 3, false, 0, {nullptr, nullptr}, {0, 0}, "v_swirl"},
-    {"horseshoe", 4, false, 0, {nullptr, nullptr}, {0, 0}, "v_horseshoe"},
-    {"polar", 5, false, 0, {nullptr, nullptr}, {0, 0}, "v_polar"},
-    {"disc", 8, false, 0, {nullptr, nullptr}, {0, 0}, "v_disc"},
-    {"ex", 12, false, 0, {nullptr, nullptr}, {0, 0}, "v_ex"},
-    {"julia", 13, true, 0, {nullptr, nullptr}, {0, 0}, "v_julia"},
-    {"bubble", 27, false, 0, {nullptr, nullptr}, {0, 0}, "v_bubble"},
-    {"cylinder", 28, false, 0, {nullptr, nullptr}, {0, 0}, "v_cylinder"},
-    {"curl", 47, false, 2, {"c1", "c2"}, {1.0f, 0.0f}, "v_curl"},   // advanced.rs:1666-1678
+    {"linear", 0, 0, 0, NP, ND, "v_linear", VF_JAC, 0, nullptr},
+    {"sinusoidal", 1, 0, 0, NP, ND, "v_sinusoidal", VF_JAC, 0, nullptr},
+    {"spherical", 2, 0, 0, NP, ND, "v_spherical", VF_JAC, 0, nullptr},
+    {"swirl", 3, 0, 0, NP, ND, "v_swirl", VF_JAC, 0, nullptr},
+    {"horseshoe", 4, 0, 0, NP, ND, "v_horseshoe", VF_JAC, 0, nullptr},
+    {"polar", 5, 0, 0, NP, ND, "v_polar", VF_JAC, 0, nullptr},
+    {"handkerchief", 6, 0, 0, NP, ND, "v_handkerchief", 0, 0, nullptr},
+    {"heart", 7, 0, 0, NP, ND, "v_heart", 0, 0, nullptr},
+    {"disc", 8, 0, 0, NP, ND, "v_disc", VF_JAC, 0, nullptr},
+    {"spiral", 9, 0, 0, NP, ND, "v_spiral", 0, 0, nullptr},
+    {"hyperbolic", 10, 0, 0, NP, ND, "v_hyperbolic", 0, 0, nullptr},
+    {"diamond", 11, 0, 0, NP, ND, "v_diamond", 0, 0, nullptr},
+    {"ex", 12, 0, 0, NP, ND, "v_ex", VF_JAC, 0, nullptr},
+    {"julia", 13, 1, 0, NP, ND, "v_julia", VF_JAC, 0, nullptr},
+    {"bent", 14, 0, 0, NP, ND, "v_bent", 0, 0, nullptr},
+    {"waves", 15, 0, 0, NP, ND, "v_waves", VF_XF, 0, nullptr},
+    {"flatten", 17, 0, 0, NP, ND, "v_flatten", VF_POST, 0, nullptr},
+    {"julian", 24, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_julian", 0, 1, derive_julian},
+    {"blob", 25, 0, 3, {"high", "low", "waves"}, {1.0f, 1.0f, 6.0f}, "v_blob", 0, 0, nullptr},
+    {"eyefish", 26, 0, 0, NP, ND, "v_eyefish", 0, 0, nullptr},
+    {"bubble", 27, 0, 0, NP, ND, "v_bubble", VF_JAC, 0, nullptr},
+    {"cylinder", 28, 0, 0, NP, ND, "v_cylinder", VF_JAC, 0, nullptr},
+    {"noise", 29, 2, 0, NP, ND, "v_noise", 0, 0, nullptr},
+    {"blur", 30, 2, 0, NP, ND, "v_blur", 0, 0, nullptr},
+    {"gaussian_blur", 31, 5, 0, NP, ND, "v_gaussian_blur", 0, 0, nullptr},
+    {"polar2", 32, 0, 0, NP, ND, "v_polar2", 0, 0, nullptr},
+    {"cross", 33, 0, 0, NP, ND, "v_cross", 0, 0, nullptr},
+    {"rings2", 44, 0, 1, {"val"}, {1.0f}, "v_rings2", 0, 0, nullptr},
+    {"fan2", 45, 0, 2, {"x", "y"}, {1.0f, 0.0f}, "v_fan2", 0, 0, nullptr},
+    {"pdj", 46, 0, 4, {"a", "b", "c", "d"}, {0.0f, 0.0f, 0.0f, 0.0f}, "v_pdj", 0, 0, nullptr},
+    {"curl", 47, 0, 2, {"c1", "c2"}, {1.0f, 0.0f}, "v_curl", VF_JAC, 0, nullptr},
+    {"rectangles", 48, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_rectangles", 0, 0, nullptr},
+    {"splits", 49, 0, 6, {"x", "y", "lshear", "rshear", "ushear", "dshear"}, {0.4f, 0.4f, 0.0f, 0.0f, 0.0f, 0.0f},
+     "v_splits", 0, 0, nullptr},
+    {"ngon", 50, 0, 4, {"sides", "power", "circle", "corners"}, {5.0f, 3.0f, 1.0f, 2.0f}, "v_ngon", 0, 0, nullptr},
+    {"pre_blur", 54, 7, 0, NP, ND, "v_pre_blur", VF_PRE | VF_W, 0, nullptr},
+    {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
+    {"juliascope", 69, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_juliascope", 0, 0, nullptr},
+    {"radial_blur", 73, 4, 1, {"angle"}, {0.0f}, "v_radial_blur", VF_W, 2, derive_radial_blur},
+    {"tangent", 141, 0, 0, NP, ND, "v_tangent", 0, 0, nullptr},
+    {"secant2", 143, 0, 0, NP, ND, "v_secant2", 0, 0, nullptr},
+    {"cosine", 144, 0, 0, NP, ND, "v_cosine", 0, 0, nullptr},
+    {"pie", 150, 3, 3, {"slices", "rotation", "thickness"}, {6.0f, 0.0f, 0.5f}, "v_pie", 0, 0, nullptr},
+    {"butterfly", 152, 0, 0, NP, ND, "v_butterfly", 0, 0, nullptr},
+    {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
+    {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
+    {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
+    {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
+    {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
+    {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
+    {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
+    {"exponential", 341, 0, 0, NP, ND, "v_exponential", 0, 0, nullptr},
+    {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
+    {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
+    {"linear3D", 533, 0, 0, NP, ND, "v_linear3D", 0, 0, nullptr},
 };
+#undef NP
+#undef ND
 
 const VarDef* registry_find(const std::string& name) {
     for (const auto& v : kRegistry) if (name == v.name) return &v;
@@ -47,6 +118,11 @@ float XForm::param(const VarDef* v, int j) const {
     std::string key = std::string(v->name) + "." + v->pname[j];
     for (auto& p : params) if (p.first == key) return p.second;
     return v->pdef[j];
+}
+
+void XForm::slot_values(const VarDef* v, float* out) const {
+    for (int j = 0; j < v->nparams; ++j) out[j] = param(v, j);
+    if (v->nderived > 0) v->derive(out, out + v->nparams);
 }
 
 float XForm::var_weight(const VarDef* v) const {

@@ -19,14 +19,33 @@
 
 namespace ffb {
 
+// A variation's packed parameter row: its user parameters, then the values
+// its `wgsl_init` derives from them (VariationDef::slot_count,
+// src/variations/definition.rs:452-454).
+constexpr int kMaxVarSlots = 6;
+
+enum VarFlags {
+    VF_XF = 1,        // Feature::NeedsTransform reading the affine: the body takes its transform's a..f
+    VF_W = 2,         // the body reads its own weight (transforms[id].variations[idx])
+    VF_PRE = 4,       // VariationPhase::Pre: temp = V(temp), before the weighted sum
+    VF_POST = 8,      // VariationPhase::Post: result = V(result), after it
+    VF_JAC = 16,      // has a Jacobian (dj_*) for the differentiable render
+};
+
 struct VarDef {
     const char* name;
     int id;            // position in the reference's ALL_VARIATIONS
-    bool needs_rng;    // Feature::NeedsRng
-    int nparams;
-    const char* pname[2];
-    float pdef[2];
+    int draws;         // Feature::NeedsRng: draws the body takes, in its order
+    int nparams;       // user parameters
+    const char* pname[kMaxVarSlots];
+    float pdef[kMaxVarSlots];
     const char* fn;    // device function name
+    int flags;         // VarFlags
+    int nderived;      // init_param_count
+    // The variation's `wgsl_init` restated on the host in f32: user -> derived.
+    void (*derive)(const float* user, float* out);
+    int slots() const { return nparams + nderived; }
+    bool needs_rng() const { return draws > 0; }
 };
 
 const VarDef* registry_find(const std::string& name);
@@ -43,6 +62,8 @@ struct XForm {
     std::vector<std::pair<std::string, float>> params;
     std::vector<int> final_att;   // indices into the finals pool
     float param(const VarDef* v, int j) const;
+    // The packed row: user parameters, then the derived values.
+    void slot_values(const VarDef* v, float* out) const;
     float var_weight(const VarDef* v) const;
 };
 

@@ -274,7 +274,13 @@ XformOut parse_xform(const XNode& x, bool is_final) {
                     if (!pv) continue;
                     const std::string pn = k.substr(u + 1);
                     for (int q = 0; q < pv->nparams; ++q)
-                        if (pn == pv->pname[q]) { pending.push_back({std::string(pv->name) + "." + pn, val}); is_param = true; }
+                        if (pn == pv->pname[q]) {
+                            // The .flame's units (flame_xml.rs:957-974): radial_blur's
+                            // angle is in half turns, the config's in degrees.
+                            const float v = (std::string(pv->name) == "radial_blur" && pn == "angle") ? val * 180.0f : val;
+                            pending.push_back({std::string(pv->name) + "." + pn, v});
+                            is_param = true;
+                        }
                     if (is_param) break;
                 }
                 if (is_param) continue;

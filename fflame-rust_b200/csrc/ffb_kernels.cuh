@@ -464,14 +464,14 @@ extern "C" __global__ void ffb_probe(const float* __restrict__ table, int n_xf, 
 }
 
 // Single-step parity: transform xi (affine, variations, post) at n points
-// with given draw words (16 a point).  xi >= n_xf selects final xi - n_xf.
+// with given draw words (FFB_APPLY_WORDS a point).  xi >= n_xf selects final xi - n_xf.
 extern "C" __global__ void ffb_apply_points(const float* __restrict__ table, int n_xf, int xi, int n,
                                             const float* __restrict__ xs, const float* __restrict__ ys,
                                             const float* __restrict__ words, int with_affine,
                                             float* __restrict__ xo, float* __restrict__ yo) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    ArrayRng rng{words + (size_t)i * 16};
+    ArrayRng rng{words + (size_t)i * FFB_APPLY_WORDS};
     float x = xs[i], y = ys[i];
     if (xi < n_xf) {
         const float* q = table + T_XF + xi;

@@ -41,6 +41,9 @@ namespace {
 
 thread_local std::string g_err;
 
+// Draw words a point of the single-step entries (FFB_APPLY_WORDS on the device).
+constexpr size_t kApplyWords = 64;
+
 struct Fail {
     int code;
     std::string msg;
@@ -963,11 +966,11 @@ FFB_API int ffb_apply_points(ffb_renderer* r, const char* config, size_t len, in
         void* d_tab = r->table.ensure(tab.size() * 4);
         ck(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, r->stream), "upload");
         const size_t nn = n;
-        float* d_in = (float*)r->tmp_in.ensure(nn * 4 * 2 + nn * 16 * 4);
+        float* d_in = (float*)r->tmp_in.ensure(nn * 4 * 2 + nn * kApplyWords * 4);
         float* d_x = d_in, *d_y = d_in + nn, *d_w = d_in + 2 * nn;
         ck(cudaMemcpyAsync(d_x, xs, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
         ck(cudaMemcpyAsync(d_y, ys, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
-        ck(cudaMemcpyAsync(d_w, words, nn * 64, cudaMemcpyHostToDevice, r->stream), "upload");
+        ck(cudaMemcpyAsync(d_w, words, nn * kApplyWords * 4, cudaMemcpyHostToDevice, r->stream), "upload");
         float* d_out = (float*)r->f_out.ensure(nn * 8);
         float* d_xo = d_out, *d_yo = d_out + nn;
         int nx = (int)f.xf.size(), xi = xform, ni = (int)n, wa = with_affine;
@@ -1695,11 +1698,11 @@ FFB_API int ffb_diff_jacobians(ffb_diff* d, int32_t xform, uint32_t n, const flo
         d->r->begin();
         ffb_renderer* r = d->r;
         const size_t nn = n;
-        float* d_in = (float*)r->tmp_in.ensure(nn * 4 * 2 + nn * 64);
+        float* d_in = (float*)r->tmp_in.ensure(nn * 4 * 2 + nn * kApplyWords * 4);
         float* d_x = d_in, *d_y = d_in + nn, *d_w = d_in + 2 * nn;
         ck(cudaMemcpyAsync(d_x, xs, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
         ck(cudaMemcpyAsync(d_y, ys, nn * 4, cudaMemcpyHostToDevice, r->stream), "upload");
-        ck(cudaMemcpyAsync(d_w, words, nn * 64, cudaMemcpyHostToDevice, r->stream), "upload");
+        ck(cudaMemcpyAsync(d_w, words, nn * kApplyWords * 4, cudaMemcpyHostToDevice, r->stream), "upload");
         const size_t ob = nn * d->nvn * 6 * 4;
         float* d_out = (float*)r->f_out.ensure(std::max<size_t>(ob, 4));
         const void* tp = d->base.p;

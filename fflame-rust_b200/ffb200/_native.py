@@ -67,6 +67,9 @@ class Output(ctypes.Structure):
 _lib = None
 
 
+APPLY_WORDS = 64          # draw words a point of apply_points / diff jacobians
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -238,7 +241,7 @@ class Renderer:
         ys = np.ascontiguousarray(ys, np.float32)
         words = np.ascontiguousarray(words, np.float32)
         n = len(xs)
-        assert words.size == n * 16
+        assert words.size == n * APPLY_WORDS, "draw words: APPLY_WORDS a point"
         xo, yo = np.zeros(n, np.float32), np.zeros(n, np.float32)
         _check(lib().ffb_apply_points(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.c_int32(xform), ctypes.c_uint32(n),
                                       _p(xs, ctypes.c_float), _p(ys, ctypes.c_float), _p(words, ctypes.c_float),

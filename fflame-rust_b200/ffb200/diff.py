@@ -116,6 +116,7 @@ class DiffRenderer:
         xs = np.ascontiguousarray(xs, np.float32)
         ys = np.ascontiguousarray(ys, np.float32)
         words = np.ascontiguousarray(words, np.float32)
+        assert words.size == len(xs) * 64, "draw words: 64 a point"
         out = np.zeros((len(xs), len(self.variations), 6), np.float32)
         fp = ctypes.POINTER(ctypes.c_float)
         _check(lib().ffb_diff_jacobians(self._h, ctypes.c_int32(xform), ctypes.c_uint32(len(xs)), xs.ctypes.data_as(fp),

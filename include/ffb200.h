@@ -196,7 +196,8 @@ int ffb_density_estimate_static(const void* d_hist, uint32_t w, uint32_t h, floa
 int ffb_probe(ffb_renderer* r, const char* config, size_t config_len, const float* pts, uint32_t npts, int32_t math,
               float* out, uint32_t out_pairs);
 
-/* One transform step at n points with explicit draw words (16 a point):
+/* One transform step at n points with explicit draw words (64 a point: the
+ * iteration's slots, 0 the pick, 1 the opacity, then each variation's):
  * affine, variations, post (with_affine) or the variations alone.  The
  * single-step parity entry; `xform` >= normals selects a final. */
 int ffb_apply_points(ffb_renderer* r, const char* config, size_t config_len, int32_t xform, uint32_t n,

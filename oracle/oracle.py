@@ -23,12 +23,60 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 # Registry ids: positions in ALL_VARIATIONS (src/variations/defs/mod.rs:446).
 REGISTRY = {
     "linear": 0, "sinusoidal": 1, "spherical": 2, "swirl": 3, "horseshoe": 4,
-    "polar": 5, "disc": 8, "ex": 12, "julia": 13, "bubble": 27, "cylinder": 28,
-    "curl": 47,
+    "polar": 5, "handkerchief": 6, "heart": 7, "disc": 8, "spiral": 9, "hyperbolic": 10,
+    "diamond": 11, "ex": 12, "julia": 13, "bent": 14, "waves": 15, "flatten": 17,
+    "julian": 24, "blob": 25, "eyefish": 26, "bubble": 27, "cylinder": 28, "noise": 29,
+    "blur": 30, "gaussian_blur": 31, "polar2": 32, "cross": 33, "rings2": 44, "fan2": 45,
+    "pdj": 46, "curl": 47, "rectangles": 48, "splits": 49, "ngon": 50, "pre_blur": 54,
+    "wedge": 66, "juliascope": 69, "radial_blur": 73, "tangent": 141, "secant2": 143,
+    "cosine": 144, "pie": 150, "butterfly": 152, "popcorn": 181, "fan": 190, "fisheye": 191,
+    "split": 248, "stripes": 250, "bent2": 281, "power": 325, "exponential": 341,
+    "perspective": 345, "rings": 379, "linear3D": 533,
 }
-PARAMS = {"curl": [("c1", 1.0), ("c2", 0.0)]}   # advanced.rs:1666-1678 defaults
+# User parameters and their defaults (the ParamDef lists of
+# src/variations/defs/*.rs); derived values come from the C oracle's
+# restatement of each `wgsl_init` (of_var_row).
+PARAMS = {
+    "curl": [("c1", 1.0), ("c2", 0.0)],
+    "julian": [("power", 2.0), ("dist", 1.0)],
+    "blob": [("high", 1.0), ("low", 1.0), ("waves", 6.0)],
+    "rings2": [("val", 1.0)],
+    "fan2": [("x", 1.0), ("y", 0.0)],
+    "pdj": [("a", 0.0), ("b", 0.0), ("c", 0.0), ("d", 0.0)],
+    "rectangles": [("x", 1.0), ("y", 1.0)],
+    "splits": [("x", 0.4), ("y", 0.4), ("lshear", 0.0), ("rshear", 0.0), ("ushear", 0.0), ("dshear", 0.0)],
+    "ngon": [("sides", 5.0), ("power", 3.0), ("circle", 1.0), ("corners", 2.0)],
+    "wedge": [("angle", 90.0), ("hole", 0.0), ("count", 2.0), ("swirl", 0.0)],
+    "juliascope": [("power", 2.0), ("dist", 1.0)],
+    "radial_blur": [("angle", 0.0)],
+    "pie": [("slices", 6.0), ("rotation", 0.0), ("thickness", 0.5)],
+    "split": [("xsize", 0.4), ("ysize", 0.6)],
+    "stripes": [("space", 0.2), ("warp", 0.6)],
+    "bent2": [("x", 1.0), ("y", 1.0)],
+    "perspective": [("angle", 0.62), ("dist", 2.2)],
+}
+SLOTS = 6          # packed parameter row a variation (user + derived)
+WORDS = 64         # draw words an iteration
 
 XF_STRIDE = 17
+
+
+def var_meta(name):
+    """(draws, user parameters, derived values, phase 0 pre / 1 normal / 2 post)."""
+    out = (ctypes.c_int * 4)()
+    lib().of_var_meta(ctypes.c_int(REGISTRY[name]), out)
+    return tuple(out)
+
+
+def var_row(name, user=None):
+    """The packed parameter row: user parameters (defaults where not given), then the derived values."""
+    if user is None:
+        user = [d for _, d in PARAMS.get(name, [])]
+    u = np.zeros(SLOTS, np.float32)
+    u[:len(user)] = user
+    row = np.zeros(SLOTS, np.float32)
+    lib().of_var_row(ctypes.c_int(REGISTRY[name]), _fp(u), _fp(row))
+    return row
 
 
 def build():
@@ -175,7 +223,7 @@ class Flame:
         self.var_id = np.array([REGISTRY[n] for n in self.names], np.int32)
         self.xf = np.zeros(len(allx) * XF_STRIDE, np.float32)
         self.var_w = np.zeros(len(allx) * max(nv, 1), np.float32)
-        self.var_p = np.zeros(len(allx) * max(nv, 1) * 2, np.float32)
+        self.var_p = np.zeros(len(allx) * max(nv, 1) * SLOTS, np.float32)
         for i, t in enumerate(allx):
             post = bool(t.get("post_affine_enabled", False))      # transforms.rs:1542; buffers.rs:467
             rec = [t["a"], t["b"], t["c"], t["d"], t["e"], t["f"],
@@ -186,8 +234,8 @@ class Flame:
             self.xf[i * XF_STRIDE:(i + 1) * XF_STRIDE] = rec
             for v, n in enumerate(self.names):
                 self.var_w[i * nv + v] = t["variations"].get(n, 0.0)
-                for j, (pn, dflt) in enumerate(PARAMS.get(n, [])):
-                    self.var_p[(i * nv + v) * 2 + j] = t.get("variation_params", {}).get(f"{n}.{pn}", dflt)
+                user = [t.get("variation_params", {}).get(f"{n}.{pn}", dflt) for pn, dflt in PARAMS.get(n, [])]
+                self.var_p[(i * nv + v) * SLOTS:(i * nv + v + 1) * SLOTS] = var_row(n, user)
         self.palette = palette_table(cfg)
         rot = float(cfg.get("rotation", 0.0))
         s = OFlame()
@@ -237,7 +285,8 @@ class Flame:
         xs = np.ascontiguousarray(xs, np.float32)
         ys = np.ascontiguousarray(ys, np.float32)
         n = len(xs)
-        d = np.zeros(n * 16, np.float32) if draws is None else np.ascontiguousarray(draws, np.float32)
+        d = np.zeros(n * WORDS, np.float32) if draws is None else np.ascontiguousarray(draws, np.float32)
+        assert d.size == n * WORDS, "draws: WORDS words a point"
         xo, yo = np.zeros(n, np.float32), np.zeros(n, np.float32)
         sx, sy = np.zeros(n, np.float64), np.zeros(n, np.float64)
         P = ctypes.POINTER(ctypes.c_double)
@@ -260,43 +309,72 @@ class Flame:
 
 # ------------------------------------------------------------ variations --
 
-def variation(name, xs, ys, draws=None, params=None, f64=False, ftz=True):
+def _draws8(draws, n):
+    """Draws as 8 words a point: [n] (one draw) or [n, k] (k <= 8)."""
+    if draws is None:
+        return None
+    d = np.asarray(draws, np.float32)
+    if d.ndim == 1:
+        d = d[:, None]
+    out = np.zeros((n, 8), np.float32)
+    out[:, :d.shape[1]] = d
+    return out
+
+
+def variation(name, xs, ys, draws=None, params=None, f64=False, ftz=True, w=1.0, xf=None):
+    """One variation at n points.  `params` its user parameters (defaults
+    if None), `draws` [n] or [n, k] its draws in order, `w` its weight and
+    `xf` an affine (a..f) for the bodies that read them."""
     xs = np.ascontiguousarray(xs, np.float32)
     ys = np.ascontiguousarray(ys, np.float32)
     n = len(xs)
-    prm = np.array(params if params is not None else [d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
-    d = None if draws is None else np.ascontiguousarray(draws, np.float32)
+    row = var_row(name, params)
+    d = _draws8(draws, n)
+    x6 = None if xf is None else np.asarray(xf, np.float32)
     xo, yo = np.zeros(n, np.float32), np.zeros(n, np.float32)
-    lib().of_variation(ctypes.c_int(REGISTRY[name]), _fp(prm), ctypes.c_int(n), _fp(xs), _fp(ys),
-                       _fp(d) if d is not None else None, _fp(xo), _fp(yo), ctypes.c_int(1 if f64 else 0),
-                       ctypes.c_int(1 if ftz else 0))
+    lib().of_variation(ctypes.c_int(REGISTRY[name]), _fp(row), ctypes.c_int(n), _fp(xs), _fp(ys),
+                       _fp(d) if d is not None else None, ctypes.c_float(w), _fp(x6) if x6 is not None else None,
+                       _fp(xo), _fp(yo), ctypes.c_int(1 if f64 else 0), ctypes.c_int(1 if ftz else 0))
     return xo, yo
 
 
-def variation_scale(name, xs, ys, draws=None, params=None):
-    """Per-component magnitude of the terms of one variation (f64)."""
+def variation_scale(name, xs, ys, draws=None, params=None, w=1.0, xf=None):
+    """Per-component tolerance scale of one variation (f64): the magnitude
+    of its terms, or its numeric conditioning (variations beyond the first
+    twelve)."""
     xs = np.ascontiguousarray(xs, np.float32)
     ys = np.ascontiguousarray(ys, np.float32)
     n = len(xs)
-    prm = np.array(params if params is not None else [d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
-    d = None if draws is None else np.ascontiguousarray(draws, np.float32)
+    row = var_row(name, params)
+    d = _draws8(draws, n)
+    x6 = None if xf is None else np.asarray(xf, np.float32)
     sx, sy = np.zeros(n, np.float64), np.zeros(n, np.float64)
     P = ctypes.POINTER(ctypes.c_double)
-    lib().of_variation_scale(ctypes.c_int(REGISTRY[name]), _fp(prm), ctypes.c_int(n), _fp(xs), _fp(ys),
-                             _fp(d) if d is not None else None, sx.ctypes.data_as(P), sy.ctypes.data_as(P))
+    lib().of_variation_scale(ctypes.c_int(REGISTRY[name]), _fp(row), ctypes.c_int(n), _fp(xs), _fp(ys),
+                             _fp(d) if d is not None else None, ctypes.c_float(w), _fp(x6) if x6 is not None else None,
+                             sx.ctypes.data_as(P), sy.ctypes.data_as(P))
     return sx, sy
 
 
-def probe(name, xform_slot=None, fold_first=None):
-    """(classes, digest, raw outputs) as src/probe/ reports them."""
+def probe(name, xform_slot=None, fold_first=None, report_stream=False):
+    """(classes, digest, raw outputs) as src/probe/ reports them.  With
+    `report_stream`, the draws come from the stream of the build that wrote
+    the reference's committed report (one PCG increment for every thread)."""
     vid = REGISTRY[name]
     slot = vid if xform_slot is None else xform_slot
     fold = (slot == 0) if fold_first is None else fold_first
-    prm = np.array([d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
+    prm = var_row(name)
     cls = ctypes.create_string_buffer(64)
     out = np.zeros(54, np.float32)
-    dig = lib().of_probe(ctypes.c_int(vid), _fp(prm), ctypes.c_int(slot), ctypes.c_int(1 if fold else 0), cls, _fp(out))
+    dig = lib().of_probe(ctypes.c_int(vid), _fp(prm), ctypes.c_int(slot), ctypes.c_int(1 if fold else 0), cls, _fp(out),
+                         ctypes.c_int(1 if report_stream else 0))
     return cls.value.decode(), dig, out
+
+
+def probe_draws(slot, k, seed=0x9E3779B9):
+    """The first k draws of rng_init(slot, seed) as rng_nextf returns them (the current stream)."""
+    st = rng_init(slot, seed)
+    return [f32((rng_next(st) >> 8) / 16777216.0) for _ in range(k)]
 
 
 def probe_draw(slot, seed=0x9E3779B9):
@@ -513,7 +591,7 @@ def variation_jacobian(name, xs, ys, draws=None, params=None):
     """(vx, vy, J00, J01, J10, J11) [n, 6] by central differences in double."""
     xs = np.ascontiguousarray(xs, np.float32)
     ys = np.ascontiguousarray(ys, np.float32)
-    prm = np.array(params if params is not None else [d for _, d in PARAMS.get(name, [])] + [0.0, 0.0], np.float32)
+    prm = var_row(name, params)
     d = None if draws is None else np.ascontiguousarray(draws, np.float32)
     out = np.zeros(len(xs) * 6, np.float64)
     lib().of_variation_jacobian(ctypes.c_int(REGISTRY[name]), _fp(prm), ctypes.c_int(len(xs)), _fp(xs), _fp(ys),

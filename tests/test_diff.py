@@ -104,7 +104,7 @@ def test_variation_jacobians_against_central_differences(diff, renderer, oracle)
     ys = rng.uniform(0.25, 1.5, n) * rng.choice([-1, 1], n)
     xs = np.where(np.abs(1 + xs) < 0.3, xs + 0.6, xs).astype(np.float32)    # away from curl's pole at x = -1
     ys = ys.astype(np.float32)
-    words = rng.uniform(0, 1, (n, 16)).astype(np.float32)
+    words = rng.uniform(0, 1, (n, 64)).astype(np.float32)
     out = dr.jacobians(0, xs, ys, words)
     slots = {"julia": 2}
     for j, name in enumerate(dr.variations):

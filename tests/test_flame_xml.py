@@ -174,6 +174,13 @@ def test_alias_is_stored_canonically_and_summed():
     assert t["variations"] == {"cylinder": 0.75} and t["variation_order"] == ["cylinder"]
 
 
+def test_radial_blur_angle_is_converted_from_half_turns():
+    # flame_xml.rs:957-974: the .flame stores radial_blur's angle in half
+    # turns (1 = pure spin); the config holds degrees.
+    t = one(flame('<xform weight="1" radial_blur="0.5" radial_blur_angle="0.5" coefs="1 0 0 1 0 0" />'))["flame"]["transforms"][0]
+    assert t["variation_params"] == {"radial_blur.angle": 90.0}
+
+
 def test_zero_weight_variation_is_dropped():
     # flame_xml.rs:697-716: a variation is stored only with a non-zero weight.
     t = one(flame('<xform weight="1" linear="1" swirl="0" coefs="1 0 0 1 0 0" />'))["flame"]["transforms"][0]
@@ -288,8 +295,9 @@ def test_imported_configs_specialize_or_say_why():
                    '<finalxform color="0" linear="1" coefs="1 0 0 1 0 0" post="0.9 0 0 0.9 0 0"/>'))
     n, src = _native.specialize(json.dumps(ok))
     assert n > 0 and src
-    bad = one(flame('<xform weight="1" julian="1" julian_power="2" coefs="1 0 0 1 0 0" />'))
-    with pytest.raises(EngineError, match="julian"):
+    bad = one(flame('<xform weight="1" escher="1" escher_beta="0.3" coefs="1 0 0 1 0 0" />'))
+    assert bad["flame"]["transforms"][0]["variation_params"] == {"escher.beta": f32(0.3)}
+    with pytest.raises(EngineError, match="escher"):
         _native.specialize(json.dumps(bad))
     chaos = one(flame('<xform weight="1" linear="1" coefs="1 0 0 1 0 0" chaos="1 0" />'
                       '<xform weight="1" swirl="1" coefs="1 0 0 1 0 0" />'))

@@ -106,11 +106,11 @@ def test_probe_sfu_math_reproduces_reference_classes(renderer, oracle, pts):
     with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "variation_probe_2d.txt")) as f:
         for line in f:
             if not line.startswith("#") and line.strip():
-                n, c, d = line.split()
-                GOLDEN[n] = (c, int(d, 16))
+                n, c, d, slot = line.split()
+                GOLDEN[n] = (c, int(d, 16), int(slot))
     mism = {}
     for name in TWELVE:
-        slot = oracle.REGISTRY[name]
+        slot = GOLDEN[name][2]
         # Place the variation at its probe-batch transform so julia's draw matches.
         cfg = {"flame": {"transforms": [one_xform(name)["flame"]["transforms"][0]] * (slot + 1)}}
         out = renderer.probe(cfg, pts, slot + 1, math="sfu")[slot].reshape(-1)
@@ -149,7 +149,7 @@ def test_apply_points_matches_oracle(renderer, oracle):
     n = 4096
     xs = rng.uniform(-2.5, 2.5, n).astype(np.float32)
     ys = rng.uniform(-2.5, 2.5, n).astype(np.float32)
-    words = (rng.integers(0, 1 << 24, (n, 16)) / float(1 << 24)).astype(np.float32)
+    words = (rng.integers(0, 1 << 24, (n, 64)) / float(1 << 24)).astype(np.float32)
     for xi in range(4):
         for aff in (True, False):
             gx, gy = renderer.apply_points(cfg, xi, xs, ys, words, with_affine=aff)
