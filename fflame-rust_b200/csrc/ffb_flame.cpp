@@ -325,8 +325,8 @@ Flame parse_config(const Json& cfg) {
         fail("palette squeeze / log redistribution are not supported by this build");
     if (const Json* cm = cfg.get("color_mode"); cm && cm->kind == Json::String && cm->str != "Palette" && cm->str != "palette")
         fail("colour mode `" + cm->str + "` is not supported by this build (palette only)");
-    if (num_field(cfg, "filter_radius", false, 0.0f) != 0.0f)
-        fail("the histogram filter (filter_radius) is not supported by this build");
+    F.filter.radius = num_field(cfg, "filter_radius", false, 0.0f);
+    F.filter.blur_edges = num_field(cfg, "filter_blur_edges", false, 0.0f);
     // Tone map (defaults.rs:18-52; fractal_config.rs field defaults).
     ToneMap& tm = F.tm;
     static const char* const kModes[] = {"linear", "Linear", "logarithmic", "Logarithmic", "density", "DensityVisualization"};

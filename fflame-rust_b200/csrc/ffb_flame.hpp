@@ -99,11 +99,21 @@ struct PostSym {
     int copies() const { return kind == 0 ? 1 : kind == 3 ? order : 2; }
 };
 
+// The spatial filter (Apophysis `filter`; fractal_config.rs:381-395,
+// compute_kernel.rs:1663-1725): a bilateral Gaussian on each batch's
+// histogram before it is accumulated; off at radius 0.
+struct SpatialFilter {
+    float radius = 0.0f;       // Gaussian sigma in pixels
+    float blur_edges = 0.0f;   // 0 strict edge preservation .. 1 near-uniform
+    bool on() const { return radius > 0.0f; }
+};
+
 struct Flame {
     std::vector<XForm> xf;              // normal transforms
     std::vector<XForm> fin;             // final transforms pool
     std::vector<int> fin_chain;         // the final chain every normal runs
     std::vector<const VarDef*> local;   // local variation order
+    SpatialFilter filter;
     float zoom = 1.0f;
     double pan_x = 0.0, pan_y = 0.0;
     float rotation = 0.0f;

@@ -138,6 +138,7 @@ struct ffb_renderer {
     std::list<Module> cache;     // most recent first
     DevBuf hist, walkers, table, palette, counters, jobs, rgba, de_out, de_tab, lut, f_out, tmp_in;
     DevBuf tile_rec, tile_tmp, tile_sorted, tile_meta;      // tile-sorted accumulation scratch
+    DevBuf filt_batch, filt_tmp;                            // spatial filter: a batch's histogram, the row pass
     uint64_t h2d = 0, d2h = 0;      // bytes copied by the current call
     uint32_t launches = 0;          // kernels launched by the current call
     std::set<ffb_batch*> batches;   // live objects borrowing this renderer's modules
@@ -156,7 +157,7 @@ struct ffb_renderer {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& m : cache) if (m.lib) cudaLibraryUnload(m.lib);
         for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in,
-                          &tile_rec, &tile_tmp, &tile_sorted, &tile_meta}) b->release();
+                          &tile_rec, &tile_tmp, &tile_sorted, &tile_meta, &filt_batch, &filt_tmp}) b->release();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -385,8 +386,18 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     const size_t npx = (size_t)P.wi * P.hi;
     // Exact mode: four u64 a pixel (ulonglong4); otherwise float4.
     const size_t px_bytes = P.plan.exact ? 32 : 16;
+    const bool filt = P.flame.filter.on();
+    if (filt && (ext_hist || P.plan.exact))
+        fail(FFB_ERR_INVALID, "the spatial filter (filter_radius) works on this library's own u32 histogram: "
+                              "not with count_bits 64 or a caller's device histogram");
     float4* hist = ext_hist ? ext_hist : (float4*)r->hist.ensure(npx * px_bytes);
     ck(cudaMemsetAsync(hist, 0, npx * px_bytes, s), "clear histogram");
+    // Spatial filter (compute_kernel.rs:1663-1725): each batch splats into
+    // its own histogram, which is filtered and added into `hist` (counts as
+    // float).  A batch is `ipt` iterations of every walker, the reference's
+    // dispatch.
+    float4* batch = filt ? (float4*)r->filt_batch.ensure(npx * 16) : nullptr;
+    float4* ftmp = filt ? (float4*)r->filt_tmp.ensure(npx * 16) : nullptr;
     void* d_table = r->table.ensure(P.table.size() * 4);
     ck(cudaMemcpyAsync(d_table, P.table.data(), P.table.size() * 4, cudaMemcpyHostToDevice, s), "upload table");
     r->h2d += P.table.size() * 4;
@@ -419,10 +430,11 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         if (chunk < P.ipt) fail(FFB_ERR_INVALID, "the pcg stream's dispatch does not fit a launch");
         chunk = chunk / P.ipt * P.ipt;
     }
+    if (filt) chunk = P.ipt;
     const uint32_t blocks = (P.walkers + threads - 1) / threads;
     const double rot = P.flame.rotation;
     Launch L{};
-    L.table = d_table; L.palette = d_pal; L.hist = hist; L.walkers = d_walk; L.counters = d_cnt;
+    L.table = d_table; L.palette = d_pal; L.hist = filt ? batch : hist; L.walkers = d_walk; L.counters = d_cnt;
     L.n_walkers = P.walkers; L.walker0 = walker0; L.block0 = 0; L.n_xf = (uint32_t)P.flame.xf.size();
     L.seed_lo = (uint32_t)P.seed; L.seed_hi = (uint32_t)(P.seed >> 32); L.burn_in = P.burn_in; L.ipt = P.ipt;
     L.pal_n = pal_n; L.width = (int32_t)P.wi; L.height = (int32_t)P.hi;
@@ -465,8 +477,20 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         Launch* jp = d_jobs + i;
         int nj = 1;
         void* args[] = {&jp, &nj};
+        if (filt) ck(cudaMemsetAsync(batch, 0, npx * 16, s), "clear batch histogram");
         ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch ffb_chaos");
         r->launches += 1;
+        if (filt) {
+            // The batch's plotted samples, as the reference counts them (compute_kernel.rs:1413-1421):
+            // its walkers' iterations past the burn-in.
+            const uint64_t a = std::max<uint64_t>(ls[i].it0, P.burn_in), b = ls[i].it0 + ls[i].n_iters;
+            const double samples = (double)P.walkers * (double)(b > a ? b - a : 0);
+            // sigma_d = mean density x 100^(2 blur_edges - 1), here in counts (the reference's
+            // densities are counts x 100; its floor of 1 is 0.01 count).
+            const double sd = samples / (double)npx * std::pow(100.0, 2.0 * (double)P.flame.filter.blur_edges - 1.0);
+            ck(launch_hist_filter(batch, ftmp, hist, (int)P.wi, (int)P.hi, P.flame.filter.radius, (float)sd, s), "spatial filter");
+            r->launches += 2;
+        }
         if (P.plan.emit) {
             unsigned* count = (unsigned*)r->tile_meta.p;
             unsigned* fill = count + tg.n_tiles;
@@ -500,7 +524,7 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
 // Density estimation of output rows [y_lo, y_lo + h_out) of a w x h
 // histogram into r->de_out (count as float; row y_lo first).
 float4* run_de(ffb_renderer* r, const float4* hist, uint32_t w, uint32_t h, double r_max, double r_min, double curve, cudaStream_t s,
-               uint32_t y_lo = 0, uint32_t h_out = 0, const ulonglong4* exact = nullptr) {
+               uint32_t y_lo = 0, uint32_t h_out = 0, const ulonglong4* exact = nullptr, bool count_f = false) {
     if (h_out == 0) h_out = h - y_lo;
     int n = 0, radius = 0;
     std::vector<float> tab = de_table(r_max, r_min, curve, n, radius);
@@ -508,7 +532,8 @@ float4* run_de(ffb_renderer* r, const float4* hist, uint32_t w, uint32_t h, doub
     ck(cudaMemcpyAsync(d_tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice, s), "upload DE table");
     r->h2d += tab.size() * 4;
     float4* out = (float4*)r->de_out.ensure((size_t)w * h_out * sizeof(float4));
-    ck(launch_density_estimate(hist, exact, (int)w, (int)h, d_tab, n, radius, (int)y_lo, (int)h_out, out, s), "density estimation");
+    ck(launch_density_estimate(hist, exact, (int)w, (int)h, d_tab, n, radius, (int)y_lo, (int)h_out, out, s, count_f ? 1 : 0),
+       "density estimation");
     r->launches += 1;
     return out;
 }
@@ -529,12 +554,12 @@ void finish_device(ffb_renderer* r, const Prepared& P, const float4* hist, uint6
     const uint32_t ss = P.ss;
     const uint32_t y_lo = row0 * ss, h_band = rows * ss;
     const float4* src = P.plan.exact ? nullptr : hist + (size_t)y_lo * P.wi;
-    bool count_f = false;
+    bool count_f = P.flame.filter.on();              // a filtered histogram holds float counts
     const ulonglong4* ex = P.plan.exact ? (const ulonglong4*)hist : nullptr;
     if (ex) src = nullptr;
     if (P.flame.de.max_radius > 0.0f) {
         src = run_de(r, ex ? nullptr : hist, P.wi, P.hi, (double)P.flame.de.max_radius * ss, (double)P.flame.de.min_radius * ss,
-                     (double)P.flame.de.curve, s, y_lo, h_band, ex);
+                     (double)P.flame.de.curve, s, y_lo, h_band, ex, count_f);
         count_f = true;
     }
     const double sd = std::max((double)samples / ((double)P.wi * (double)P.hi), 1e-6);   // compute_kernel.rs:1796-1840
@@ -789,6 +814,7 @@ FFB_API int ffb_histogram(ffb_renderer* r, const char* config, size_t len, const
         std::lock_guard<std::mutex> lk(r->mu);
         r->begin();
         Prepared P = prepare(config, len, job);
+        if (P.flame.filter.on()) fail(FFB_ERR_INVALID, "a filtered histogram holds fractional counts: use ffb_histogram_f32");
         r->reset_counts();
         uint64_t inframe = 0;
         ck(cudaEventRecord(r->ev0, r->stream), "event");
@@ -812,6 +838,65 @@ FFB_API int ffb_histogram(ffb_renderer* r, const char* config, size_t len, const
             r->fill_counts(out);
             out->d2h_bytes += npx * 16;
         }
+    });
+}
+
+FFB_API int ffb_histogram_f32(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, float* counts, float* rgb,
+                              ffb_output* out) {
+    return guard([&] {
+        if (!r || !job) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Prepared P = prepare(config, len, job);
+        if (P.count_bits != 32) fail(FFB_ERR_INVALID, "ffb_histogram_f32 reads the u32 / filtered histogram (count_bits 32)");
+        r->reset_counts();
+        uint64_t inframe = 0;
+        ck(cudaEventRecord(r->ev0, r->stream), "event");
+        run_chaos(r, P, r->stream, job->walker0, &inframe);
+        ck(cudaEventRecord(r->ev1, r->stream), "event");
+        const size_t npx = (size_t)P.wi * P.hi;
+        std::vector<float> h(npx * 4);
+        ck(cudaMemcpyAsync(h.data(), r->hist.p, npx * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "histogram");
+        const bool f = P.flame.filter.on();
+        for (size_t i = 0; i < npx; ++i) {
+            if (counts) { uint32_t c; std::memcpy(&c, &h[i * 4 + 3], 4); counts[i] = f ? h[i * 4 + 3] : (float)c; }
+            if (rgb) { rgb[i * 3] = h[i * 4]; rgb[i * 3 + 1] = h[i * 4 + 1]; rgb[i * 3 + 2] = h[i * 4 + 2]; }
+        }
+        if (out) {
+            *out = ffb_output{};
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, r->ev0, r->ev1);
+            out->width = P.wi; out->height = P.hi;
+            out->total_iterations = (uint64_t)P.walkers * P.per_walker;
+            out->inframe_samples = inframe;
+            out->render_time_ms = ms;
+            r->fill_counts(out);
+        }
+    });
+}
+
+FFB_API int ffb_hist_filter(ffb_renderer* r, const uint32_t* counts, const float* rgb, uint32_t w, uint32_t h, float sigma,
+                            float sigma_d, float* out) {
+    return guard([&] {
+        if (!r || !counts || !rgb || !out) fail(FFB_ERR_INVALID, "NULL argument");
+        if (w == 0 || h == 0 || w > kMaxDim || h > kMaxDim) fail(FFB_ERR_INVALID, "bad histogram size");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        const size_t npx = (size_t)w * h;
+        std::vector<float> in(npx * 4);
+        for (size_t i = 0; i < npx; ++i) {
+            in[i * 4] = rgb[i * 3]; in[i * 4 + 1] = rgb[i * 3 + 1]; in[i * 4 + 2] = rgb[i * 3 + 2];
+            std::memcpy(&in[i * 4 + 3], &counts[i], 4);
+        }
+        float4* batch = (float4*)r->filt_batch.ensure(npx * 16);
+        float4* tmp = (float4*)r->filt_tmp.ensure(npx * 16);
+        float4* acc = (float4*)r->f_out.ensure(npx * 16);
+        ck(cudaMemcpyAsync(batch, in.data(), npx * 16, cudaMemcpyHostToDevice, r->stream), "upload");
+        ck(cudaMemsetAsync(acc, 0, npx * 16, r->stream), "clear");
+        ck(launch_hist_filter(batch, tmp, acc, (int)w, (int)h, sigma, sigma_d, r->stream), "spatial filter");
+        ck(cudaMemcpyAsync(out, acc, npx * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
+        ck(cudaStreamSynchronize(r->stream), "spatial filter");
     });
 }
 
@@ -1278,6 +1363,8 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
             j.seed = items[i].seed;
             if (j.iterations == 0) fail(FFB_ERR_INVALID, "every batch item needs its sample budget");
             B->flames[i].P = prepare(items[i].config, items[i].config_len, &j);
+            if (B->flames[i].P.flame.filter.on())
+                fail(FFB_ERR_INVALID, "item " + std::to_string(i) + ": the spatial filter (filter_radius) is not batched; render it alone");
             check_de(B->flames[i].P.flame, B->flames[i].P.ss);
             B->flames[i].budget = j.iterations;
             maxx = std::max<int>(maxx, (int)B->flames[i].P.flame.xf.size());
@@ -1514,6 +1601,7 @@ FFB_API int ffb_diff_create(ffb_renderer* r, const char* config, size_t len, con
         std::unique_ptr<ffb_diff> d(new ffb_diff);
         d->exact = exact;
         d->P = prepare(config, len, &j);
+        if (d->P.flame.filter.on()) fail(FFB_ERR_INVALID, "the differentiable render has no spatial filter (filter_radius)");
         const Flame& f = d->P.flame;
         if (d->P.ss != 1) fail(FFB_ERR_INVALID, "the differentiable render has no supersampling");
         if (!f.fin_chain.empty()) fail(FFB_ERR_CONFIG, "the differentiable render takes no final transforms");

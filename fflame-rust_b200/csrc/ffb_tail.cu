@@ -264,7 +264,8 @@ __global__ void __launch_bounds__(256) k_tonemap_batch(const TonemapJob* __restr
 constexpr int DE_TX = 32, DE_TY = 16;
 __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, const ulonglong4* __restrict__ exact,
                                                            int w, int h, const float4* __restrict__ tab,
-                                                           int tab_n, int R, int y_lo, int h_out, float4* __restrict__ out) {
+                                                           int tab_n, int R, int y_lo, int h_out, float4* __restrict__ out,
+                                                           int count_f) {
     extern __shared__ float4 de_smem[];
     const int tw = DE_TX + 2 * R, th = DE_TY + 2 * R, n = tw * th;
     float4* val = de_smem;                                                // (rgb, count) / normaliser
@@ -289,11 +290,13 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
                 hv = make_float4((float)((double)q.x * f), (float)((double)q.y * f), (float)((double)q.z * f), 0.f);
             } else {
                 hv = hist[si];
-                c = (unsigned long long)__float_as_uint(hv.w);
+                // A filtered histogram holds fractional counts: the table
+                // entry of the count rounded up, the count itself as weight.
+                c = count_f ? (unsigned long long)ceilf(fmaxf(hv.w, 0.0f)) : (unsigned long long)__float_as_uint(hv.w);
             }
             if (c > 0ull) {
                 const float4 e = tab[c < (unsigned long long)(tab_n - 1) ? c : (unsigned long long)(tab_n - 1)];
-                const float cf = (float)c;
+                const float cf = count_f ? hv.w : (float)c;
                 v = make_float4(hv.x * e.z, hv.y * e.z, hv.z * e.z, cf * e.z);
                 pr = make_float2(e.x, 4.5f * e.y);
                 my_reach = max(my_reach, (int)e.w);
@@ -379,14 +382,72 @@ cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long t
 }
 
 cudaError_t launch_density_estimate(const float4* hist, const ulonglong4* exact, int w, int h,
-                                    const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s) {
+                                    const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s,
+                                    int count_f) {
     const size_t smem = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius) * (sizeof(float4) + sizeof(float2));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     dim3 grid((w + DE_TX - 1) / DE_TX, (h_out + DE_TY - 1) / DE_TY);
-    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, exact, w, h, table, table_n, radius, y_lo, h_out, out);
+    k_density<<<grid, DE_TX * DE_TY, smem, s>>>(hist, exact, w, h, table, table_n, radius, y_lo, h_out, out, count_f);
+    return cudaGetLastError();
+}
+
+// The spatial filter (shaders/histogram_blur.wgsl:38-119): one separable
+// pass of a bilateral Gaussian, spatial sigma `sigma` pixels (taps within
+// min(ceil(3 sigma), 8), clamped to the edge), density sigma `sigma_d`
+// (weight exp(-(d_tap - d_centre)^2 / 2 sigma_d^2)); the centre density of
+// both passes is the batch's unfiltered one (`orig`).  dir 0 filters rows,
+// 1 columns.  `src_u32`/`orig_u32`: .w holds u32 count bits, else a float.
+// `accumulate`: add the result into `dst` (count as float) instead of
+// storing it.  Counts and colours stay FP32 (the reference truncates its
+// x100 fixed-point values to u32 after each pass).
+__global__ void __launch_bounds__(256) k_hist_filter(const float4* __restrict__ src, int src_u32, const float4* __restrict__ orig,
+                                                     int orig_u32, int w, int h, int dir, float sigma, float sigma_d,
+                                                     float4* __restrict__ dst, int accumulate) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const float sg = fmaxf(sigma, 0.0001f);
+    const int kh = min((int)ceilf(3.0f * sg), 8);
+    const float inv_2s2 = 1.0f / (2.0f * sg * sg);
+    const size_t c = (size_t)y * w + x;
+    const float4 oc = orig[c];
+    const float dc = orig_u32 ? (float)__float_as_uint(oc.w) : oc.w;
+    const float sd = fmaxf(sigma_d, 0.01f);
+    const float inv_2sd2 = 1.0f / (2.0f * sd * sd);
+    float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+    float wt = 0.0f;
+    for (int k = -kh; k <= kh; ++k) {
+        const int nx = dir == 0 ? min(max(x + k, 0), w - 1) : x;
+        const int ny = dir == 0 ? y : min(max(y + k, 0), h - 1);
+        const float4 t = src[(size_t)ny * w + nx];
+        const float td = src_u32 ? (float)__float_as_uint(t.w) : t.w;
+        const float fk = (float)k;
+        const float ws = expf(-fk * fk * inv_2s2);
+        const float dd = td - dc;
+        const float wd = expf(-dd * dd * inv_2sd2);
+        const float wk = ws * wd;
+        sum.x += t.x * wk; sum.y += t.y * wk; sum.z += t.z * wk; sum.w += td * wk;
+        wt += wk;
+    }
+    const float inv = 1.0f / fmaxf(wt, 1e-6f);
+    const float4 r = make_float4(sum.x * inv, sum.y * inv, sum.z * inv, sum.w * inv);
+    if (accumulate) {
+        float4 a = dst[c];
+        a.x += r.x; a.y += r.y; a.z += r.z; a.w += r.w;
+        dst[c] = a;
+    } else {
+        dst[c] = r;
+    }
+}
+
+cudaError_t launch_hist_filter(const float4* batch, float4* tmp, float4* acc, int w, int h, float sigma, float sigma_d,
+                               cudaStream_t s) {
+    const dim3 grid((w + 255) / 256, h);
+    k_hist_filter<<<grid, 256, 0, s>>>(batch, 1, batch, 1, w, h, 0, sigma, sigma_d, tmp, 0);
+    k_hist_filter<<<grid, 256, 0, s>>>(tmp, 0, batch, 1, w, h, 1, sigma, sigma_d, acc, 1);
     return cudaGetLastError();
 }
 
@@ -509,7 +570,7 @@ cudaError_t density_estimate_static(const float4* hist, int w, int h, double r_m
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    return launch_density_estimate(hist, nullptr, w, h, tab, n, (int)std::floor(r_max), 0, h, out, s);
+    return launch_density_estimate(hist, nullptr, w, h, tab, n, (int)std::floor(r_max), 0, h, out, s, 0);
 }
 
 }  // namespace ffb

@@ -55,7 +55,14 @@ cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long t
 // reading sources from the whole w x h histogram (`exact`, when given,
 // instead of `hist`).
 cudaError_t launch_density_estimate(const float4* hist, const ulonglong4* exact, int w, int h,
-                                    const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s);
+                                    const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s,
+                                    int count_f = 0);
+
+// The spatial filter of one batch (histogram_blur.wgsl): `batch` (u32
+// counts) filtered along rows into `tmp`, then along columns and added into
+// `acc` (float counts).  sigma in pixels, sigma_d in counts.
+cudaError_t launch_hist_filter(const float4* batch, float4* tmp, float4* acc, int w, int h, float sigma, float sigma_d,
+                               cudaStream_t s);
 
 // Density estimation of all w x h rows with the weight table in a file-scope
 // device array of kDeStaticEntries entries instead of allocated memory (the

@@ -29,7 +29,7 @@ EXPORTS = [
     "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
     "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
     "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize", "ffb_encode_png",
-    "ffb_flame_import",
+    "ffb_flame_import", "ffb_histogram_f32", "ffb_hist_filter",
 ]
 
 
@@ -188,6 +188,28 @@ class Renderer:
         _check(lib().ffb_histogram(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), _p(cnt, ctypes.c_uint32),
                                    _p(rgb, ctypes.c_float), ctypes.byref(o)))
         return cnt, rgb, o
+
+    def histogram_f32(self, config, width, height, **job):
+        """config -> (counts [h, w] f32, rgb sums [h, w, 3], Output): also a filtered histogram."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        ss = j.supersample or 1
+        cnt = np.zeros((height * ss, width * ss), np.float32)
+        rgb = np.zeros((height * ss, width * ss, 3), np.float32)
+        o = Output()
+        _check(lib().ffb_histogram_f32(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), _p(cnt, ctypes.c_float),
+                                       _p(rgb, ctypes.c_float), ctypes.byref(o)))
+        return cnt, rgb, o
+
+    def hist_filter(self, counts, rgb, sigma, sigma_d):
+        """The spatial filter of one batch histogram (counts u32 [h, w], rgb [h, w, 3]) -> [h, w, 4] (r, g, b, count)."""
+        counts = np.ascontiguousarray(counts, np.uint32)
+        rgb = np.ascontiguousarray(rgb, np.float32)
+        h, w = counts.shape
+        out = np.zeros((h, w, 4), np.float32)
+        _check(lib().ffb_hist_filter(self._h, _p(counts, ctypes.c_uint32), _p(rgb, ctypes.c_float), ctypes.c_uint32(w),
+                                     ctypes.c_uint32(h), ctypes.c_float(sigma), ctypes.c_float(sigma_d), _p(out, ctypes.c_float)))
+        return out
 
     def histogram_u64(self, config, width, height, **job):
         """The chaos game with exact u64 counts: (counts u64 [H, W], rgb f32 [H, W, 3], Output)."""

@@ -154,6 +154,19 @@ int ffb_render_device(ffb_renderer* r, const char* config, size_t config_len, co
 int ffb_histogram(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
                   uint32_t* counts, float* rgb, ffb_output* out);
 
+/* The same with counts as f32: the only form of a histogram the spatial
+ * filter (filter_radius > 0: a bilateral Gaussian on each batch's
+ * histogram, compute_kernel.rs:1663-1725) made fractional; ffb_histogram
+ * refuses those. */
+int ffb_histogram_f32(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,
+                      float* counts, float* rgb, ffb_output* out);
+
+/* The spatial filter alone on a host histogram (u32 counts, rgb sums) of
+ * one batch: out is w*h*4 floats (r, g, b, count) after the row and column
+ * passes; sigma in pixels, sigma_d in counts.  The filter's parity entry. */
+int ffb_hist_filter(ffb_renderer* r, const uint32_t* counts, const float* rgb, uint32_t w, uint32_t h, float sigma,
+                    float sigma_d, float* out);
+
 /* The same in exact mode (job->count_bits taken as 64): counts is w*h u64
  * hits, rgb the colour sums (f32 of the exact fixed-point sums). */
 int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job,

@@ -94,6 +94,7 @@ def lib():
             build()
         L = ctypes.CDLL(LIB_PATH)
         L.of_probe.restype = ctypes.c_uint64
+        L.of_render_filtered.restype = ctypes.c_uint64
         L.of_probe_digest.restype = ctypes.c_uint64
         L.of_render.restype = ctypes.c_uint64
         L.of_pcg_hash.restype = ctypes.c_uint32
@@ -279,6 +280,19 @@ class Flame:
             return plotted, inframe.value, None, None
         return plotted, inframe.value, cnt.reshape(self.height, self.width), rgb.reshape(self.height, self.width, 3)
 
+    def render_filtered(self, walkers, iters, sigma, blur_edges=0.0, *, seed=12345, seed_hi=0, rng="philox", burn_in=20,
+                        ipt=1024, threads=1, walker0=0):
+        """The chaos game in batches of `ipt` iterations, each batch's
+        histogram spatially filtered and summed: (plotted, inframe, [h, w, 4] r, g, b, count)."""
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        inframe = ctypes.c_int64(0)
+        plotted = lib().of_render_filtered(
+            self.ptr, ctypes.c_int(0 if rng == "pcg" else 1), ctypes.c_uint32(seed & 0xFFFFFFFF),
+            ctypes.c_uint32(seed_hi & 0xFFFFFFFF), ctypes.c_uint32(burn_in), ctypes.c_uint32(ipt),
+            ctypes.c_uint32(walker0), ctypes.c_uint32(walkers), ctypes.c_uint64(iters), ctypes.c_int(threads),
+            ctypes.c_float(sigma), ctypes.c_float(blur_edges), _fp(out), ctypes.byref(inframe))
+        return plotted, inframe.value, out
+
     def apply_xform(self, xi, xs, ys, draws=None, with_affine=True, scales=False):
         """One step of transform xi; with `scales`, also the magnitude of the
         terms each output component sums (f64), for cancellation-aware tolerances."""
@@ -369,6 +383,15 @@ def probe(name, xform_slot=None, fold_first=None, report_stream=False):
     dig = lib().of_probe(ctypes.c_int(vid), _fp(prm), ctypes.c_int(slot), ctypes.c_int(1 if fold else 0), cls, _fp(out),
                          ctypes.c_int(1 if report_stream else 0))
     return cls.value.decode(), dig, out
+
+
+def hist_filter(rgbc, sigma, sigma_d):
+    """The spatial filter of one batch ([h, w, 4] r, g, b, count) -> [h, w, 4]."""
+    rgbc = np.ascontiguousarray(rgbc, np.float32)
+    h, w, _ = rgbc.shape
+    out = np.zeros_like(rgbc)
+    lib().of_hist_filter(_fp(rgbc), ctypes.c_int(w), ctypes.c_int(h), ctypes.c_float(sigma), ctypes.c_float(sigma_d), _fp(out))
+    return out
 
 
 def probe_draws(slot, k, seed=0x9E3779B9):

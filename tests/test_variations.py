@@ -246,6 +246,31 @@ def test_apply_points_every_variation(renderer, oracle):
             assert len(bad) <= n // 1000, (xi, aff, len(bad), [(xs[i], ys[i], gx[i], rx[i], gy[i], ry[i], sx[i], sy[i]) for i in bad[:4]])
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(EXACT))
+def test_exactly_rounded_bodies_are_bit_identical(renderer, oracle, name):
+    """One step of a transform holding only `name` (weight 1, non-default
+    parameters) at 65,536 points across magnitudes: the same bits."""
+    rng = np.random.default_rng(REG_SEED + oracle.REGISTRY[name])
+    n = 65536
+    mag = 10.0 ** rng.uniform(-6, 6, n)
+    xs = (rng.choice([-1, 1], n) * mag * rng.random(n)).astype(np.float32)
+    ys = (rng.choice([-1, 1], n) * 10.0 ** rng.uniform(-6, 6, n) * rng.random(n)).astype(np.float32)
+    params = {f"{name}.{p}": float(np.float32(d * 0.7 + 0.11)) for p, d in oracle.PARAMS.get(name, [])}
+    t = {"a": 1, "b": 0, "c": 0, "d": 1, "e": 0, "f": 0, "weight": 1.0, "color": 0.5, "variations": {name: 1.0},
+         "variation_params": params}
+    cfg = {"flame": {"transforms": [t]}}
+    words = np.zeros((n, 64), np.float32)
+    gx, gy = renderer.apply_points(cfg, 0, xs, ys, words, with_affine=False)
+    rx, ry = oracle.Flame(cfg, 8, 8).apply_xform(0, xs, ys, words, with_affine=False)
+    ok = bit_equal(gx, rx) & bit_equal(gy, ry)
+    bad = np.where(~ok)[0]
+    assert len(bad) == 0, (name, len(bad), [(xs[i], ys[i], gx[i], rx[i], gy[i], ry[i]) for i in bad[:4]])
+
+
+REG_SEED = 900
+
+
 def exact_flame():
     """A flame of correctly rounded bodies only."""
     def t(a, b, c, d, e, f, w, col, v, **kw):
