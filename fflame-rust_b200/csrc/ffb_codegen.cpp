@@ -213,6 +213,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
         };
         for (const VarDef* v : p.normal) need(v);
         for (auto& fi : p.fin) for (const VarDef* v : fi.vars) need(v);
+        if (!f.xaos.empty()) throw std::runtime_error("the differentiable render has no xaos");
     }
     for (auto& x : f.xf) p.has_post |= x.post;
     const int M = p.maxx, NVN = (int)p.normal.size();
@@ -226,6 +227,9 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     p.sym_kind = f.sym.kind;
     p.t_sym = off;
     if (p.sym_kind != 0) off += kSymBlock;
+    p.xaos = !f.xaos.empty();
+    p.t_xaos = off;
+    if (p.xaos) off += M * (M + 1);
     p.table_size = off;
 
     std::ostringstream s;
@@ -237,6 +241,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     if (exact) s << "#define FFB_EXACT 1\n";
     if (emit) s << "#define FFB_EMIT 1\n";
     s << "#define FFB_SYM_KIND " << p.sym_kind << "\n#define T_SYM " << p.t_sym << "\n";
+    if (p.xaos) s << "#define FFB_XAOS 1\n#define T_XAOS " << p.t_xaos << "\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
     s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw
       << "\n#define T_VP " << p.t_vp << "\n";
@@ -335,6 +340,20 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
             const float th = ((float)k * 6.28318530717958647692f) / (float)std::max(y.order, 1);
             q[6 + 2 * k] = std::cos(th);
             q[7 + 2 * k] = std::sin(th);
+        }
+    }
+    if (p.xaos) {
+        // Each previous transform's row: total, then the running sums of
+        // weight_i x xaos[prev][i] in f32, left to right (utilities.wgsl:110-137).
+        const size_t n = f.xf.size();
+        for (int r = 0; r < M; ++r) {
+            float* row = t.data() + p.t_xaos + (size_t)r * (M + 1);
+            float cum = 0.0f;
+            for (int i = 0; i < M; ++i) {
+                if ((size_t)i < n && (size_t)r < n) { cum += f.xf[i].weight * f.xaos[(size_t)r * n + i]; row[1 + i] = cum; }
+                else row[1 + i] = INFINITY;
+            }
+            row[0] = (size_t)r < n ? cum : 0.0f;
         }
     }
     for (size_t c = 0; c < p.fin.size(); ++c) {

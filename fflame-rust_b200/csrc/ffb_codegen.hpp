@@ -41,6 +41,8 @@ struct Plan {
     int table_size = 0;
     int t_cum = 0, t_xf = 0, t_vw = 0, t_vp = 0, t_fin = 0;
     int sym_kind = 0, t_sym = 0;           // post-symmetry (compile-time kind; its table block at t_sym)
+    bool xaos = false;                     // xaos pick: M rows of (total, running sums) at t_xaos
+    int t_xaos = 0;
     int rng_mode = RNG_PHILOX;
     int math_mode = MATH_PRECISE;
     int threads = 128;

@@ -211,6 +211,52 @@ int mode_code(const std::string& s, const char* const* names, int n, const char*
 
 }  // namespace
 
+// Whether the xaos walk, not the first pick, decides which closed group of
+// the chain an orbit ends in (xaos.rs:66-123, restated): transitions go
+// where weight x xaos > 0 (a row with none goes to transform 0); a closed
+// group is a set the chain never leaves; a start is any transform of
+// positive weight.
+static bool xaos_walk_splits_orbits(const Flame& F) {
+    const size_t n = F.xf.size();
+    if (F.xaos.empty() || n == 0) return false;
+    std::vector<std::vector<size_t>> next(n);
+    for (size_t i = 0; i < n; ++i) {
+        for (size_t j = 0; j < n; ++j)
+            if (std::max(F.xf[j].weight, 0.0f) * F.xaos[i * n + j] > 0.0f) next[i].push_back(j);
+        if (next[i].empty()) next[i].push_back(0);
+    }
+    std::vector<std::vector<char>> reach(n, std::vector<char>(n, 0));
+    for (size_t s = 0; s < n; ++s) {
+        std::vector<size_t> stack{s};
+        reach[s][s] = 1;
+        while (!stack.empty()) {
+            const size_t i = stack.back();
+            stack.pop_back();
+            for (size_t j : next[i]) if (!reach[s][j]) { reach[s][j] = 1; stack.push_back(j); }
+        }
+    }
+    std::vector<char> first(n), live(n, 0);
+    for (size_t i = 0; i < n; ++i) first[i] = F.xf[i].weight > 0.0f;
+    for (size_t i = 0; i < n; ++i)
+        if (first[i]) for (size_t j = 0; j < n; ++j) live[j] |= reach[i][j];
+    std::vector<size_t> closed;
+    for (size_t i = 0; i < n; ++i) {
+        if (!live[i]) continue;
+        bool cl = true, lowest = true;
+        for (size_t j = 0; j < n; ++j) cl &= !reach[i][j] || reach[j][i];
+        for (size_t j = 0; j < i; ++j) lowest &= !(reach[i][j] && reach[j][i]);
+        if (cl && lowest) closed.push_back(i);
+    }
+    if (closed.size() < 2) return false;
+    for (size_t i = 0; i < n; ++i) {
+        if (!first[i]) continue;
+        int k = 0;
+        for (size_t c : closed) k += reach[i][c] ? 1 : 0;
+        if (k > 1) return true;
+    }
+    return false;
+}
+
 Flame parse_config(const Json& cfg) {
     if (cfg.kind != Json::Object) fail("the config is not a JSON object");
     const Json* fl = cfg.get("flame");
@@ -223,12 +269,30 @@ Flame parse_config(const Json& cfg) {
     for (auto& t : ts->arr) F.xf.push_back(parse_transform(*t));
     if (const Json* lt = fl->get("linked_transforms"); lt && lt->kind == Json::Array && !lt->arr.empty())
         fail("linked transforms are not supported by this build");
-    // Xaos (utilities.wgsl:110-137): a chaos matrix of all ones is the plain pick.
-    if (const Json* xa = fl->get("xaos"); xa && xa->kind == Json::Array)
-        for (auto& row : xa->arr)
-            if (row->kind == Json::Array)
-                for (auto& v : row->arr)
-                    if (v->kind == Json::Number && v->num != 1.0) fail("xaos (a chaos matrix) is not supported by this build");
+    // Xaos (utilities.wgsl:106-137): read when some weight differs from 1
+    // (xaos.rs:29-40); entries beyond the matrix are 1 (get_xaos, xaos.rs:128-135).
+    if (const Json* xa = fl->get("xaos"); xa && xa->kind == Json::Array) {
+        const size_t n = F.xf.size();
+        std::vector<float> m(n * n, 1.0f);
+        bool any = false;
+        for (size_t i = 0; i < xa->arr.size(); ++i) {
+            const Json* row = xa->arr[i].get();
+            if (row->kind != Json::Array) fail("xaos rows must be arrays");
+            for (size_t j = 0; j < row->arr.size(); ++j) {
+                if (row->arr[j]->kind != Json::Number) fail("xaos weights must be numbers");
+                const float v = (float)row->arr[j]->num;
+                any |= std::fabs(v - 1.0f) > 1e-6f;
+                if (i < n && j < n) m[i * n + j] = v;
+            }
+        }
+        if (any) {
+            if (n > 64) fail("xaos over more than 64 transforms is not supported by this build");
+            F.xaos = m;
+            if (xaos_walk_splits_orbits(F))
+                fail("this xaos chain's walk splits orbits between closed groups, which needs the reference's orbit "
+                     "refresh (compute_kernel.rs:45-60); not supported by this build");
+        }
+    }
     if (const Json* so = fl->get("solo_transform"); so && so->kind == Json::Number)
         fail("a solo transform is not supported by this build");
     if (const Json* ft = fl->get("final_transforms"); ft && ft->kind == Json::Array)

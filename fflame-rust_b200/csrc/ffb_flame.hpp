@@ -114,6 +114,9 @@ struct Flame {
     std::vector<int> fin_chain;         // the final chain every normal runs
     std::vector<const VarDef*> local;   // local variation order
     SpatialFilter filter;
+    // Xaos (utilities.wgsl:106-137): row-major n_xf x n_xf transition
+    // weights, empty when every weight is 1 (Flame::has_xaos, xaos.rs:29-40).
+    std::vector<float> xaos;
     float zoom = 1.0f;
     double pan_x = 0.0, pan_y = 0.0;
     float rotation = 0.0f;

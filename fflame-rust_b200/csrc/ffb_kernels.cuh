@@ -31,6 +31,38 @@ __device__ __forceinline__ int ffb_select(const float* __restrict__ sm, int n_xf
     return k;
 }
 
+#ifdef FFB_XAOS
+// Xaos (utilities.wgsl:106-137): the pick from the previous transform's
+// row, whose running sums of weight_i x xaos[prev][i] (f32, left to right)
+// and total the table holds at T_XAOS + prev * (FFB_MAXX + 1).
+__device__ __forceinline__ int ffb_select_xaos(const float* __restrict__ sm, int n_xf, float u, int prev) {
+    const float* row = sm + T_XAOS + prev * (FFB_MAXX + 1);
+    const float t = u * row[0];
+    int k = n_xf - 1;
+    bool found = false;
+#pragma unroll
+    for (int i = 0; i < FFB_MAXX; ++i) {
+        bool hit = (i < n_xf) && !found && (t <= row[1 + i]);
+        k = hit ? i : k;
+        found = found || hit;
+    }
+    return k;
+}
+// A starting walker's previous transform (main_template.wgsl:163-179): an
+// unconditioned pick at a Kronecker point of its index, so every range of
+// walkers starts in each closed group of the chain in proportion.
+__device__ __forceinline__ int ffb_xaos_first(const float* __restrict__ sm, int n_xf, u32 gw, u32 seed) {
+    const u32 ou = gw * 2654435769u + seed;
+    return ffb_select(sm, n_xf, (float)(ou >> 8u) * (1.0f / 16777216.0f));
+}
+#define FFB_PICK(u, prev) ffb_select_xaos(sm, n_xf, (u), (prev))
+// The stored walker state packs the previous transform above the burn-in left.
+#define FFB_PACK_FUSE(fuse, prev) ((fuse) | ((u32)(prev) << 24))
+#else
+#define FFB_PICK(u, prev) ffb_select(sm, n_xf, (u))
+#define FFB_PACK_FUSE(fuse, prev) (fuse)
+#endif
+
 __device__ __forceinline__ int ffb_palette_index(float ci, u32 n) {
     // Nearest sampling, clamp-to-edge (gpu/buffers.rs:1867-1876).
     float t = floorf(ci * (float)n);
@@ -153,11 +185,17 @@ __device__ __forceinline__ const ffb_launch& ffb_stage(const ffb_launch* __restr
     return J;
 }
 
-// A walker's start (main_template.wgsl:25-55) or its stored state.
-__device__ __forceinline__ void ffb_start(const ffb_launch& J, u32 w, u32 gw, float& x, float& y, float& ci, u32& fuse) {
+// A walker's start (main_template.wgsl:25-55) or its stored state; `prev`
+// the previous transform of an xaos walk.
+__device__ __forceinline__ void ffb_start(const float* __restrict__ sm, const ffb_launch& J, u32 w, u32 gw, float& x, float& y,
+                                          float& ci, u32& fuse, int& prev) {
+    prev = 0;
     if (J.it0 == 0) {
         ci = 0.0f;
         fuse = J.burn_in;
+#ifdef FFB_XAOS
+        prev = ffb_xaos_first(sm, (int)J.n_xf, gw, J.seed_lo);
+#endif
 #if FFB_RNG_MODE == 1
         uint4 o = philox4(J.seed_lo, J.seed_hi, gw, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
         x = u24(o.x) * 2.0f - 1.0f;
@@ -168,6 +206,10 @@ __device__ __forceinline__ void ffb_start(const ffb_launch& J, u32 w, u32 gw, fl
     } else {
         float4 s = J.walkers[w];
         x = s.x; y = s.y; ci = s.z; fuse = __float_as_uint(s.w);
+#ifdef FFB_XAOS
+        prev = (int)(fuse >> 24);
+        fuse &= 0xFFFFFFu;
+#endif
     }
 }
 
@@ -300,7 +342,8 @@ __device__ __forceinline__ void ffb_chaos_walker(const float* __restrict__ sm, c
     const int n_xf = (int)J.n_xf;
     float x, y, ci;
     u32 fuse;
-    ffb_start(J, w, gw, x, y, ci, fuse);
+    int prev;
+    ffb_start(sm, J, w, gw, x, y, ci, fuse, prev);
     const float scale = (float)min(J.width, J.height) * 0.25f;
     const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
     u32 inframe = 0;
@@ -316,11 +359,13 @@ __device__ __forceinline__ void ffb_chaos_walker(const float* __restrict__ sm, c
         PhiloxRng rng;
         rng.fill(J.seed_lo, J.seed_hi, gw, it);
 #endif
-        const int k = ffb_select(sm, n_xf, rng.draw(0));                     // main_template.wgsl:198-223
+        const int k = FFB_PICK(rng.draw(0), prev);                            // main_template.wgsl:198-223
+        prev = k;
         const bool plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];       // main_template.wgsl:249
         ffb_step<false>(sm, pal, J, k, plot, rng, gw, it, x, y, ci, fuse, cx, cy, scale, inframe);
     }
-    J.walkers[w] = make_float4(x, y, ci, __uint_as_float(fuse));
+    (void)prev;
+    J.walkers[w] = make_float4(x, y, ci, __uint_as_float(FFB_PACK_FUSE(fuse, prev)));
     ffb_count_inframe(J, inframe);
 }
 
@@ -368,7 +413,8 @@ ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
     u32 wid = J.walker0 + w0;
     float x = 0.f, y = 0.f, ci = 0.f;
     u32 fuse = 0;
-    if (active) ffb_start(J, w0, wid, x, y, ci, fuse);
+    int prev = 0;                                // the held walker's previous transform (xaos)
+    if (active) ffb_start(sm, J, w0, wid, x, y, ci, fuse, prev);
     const int n_xf = (int)J.n_xf;
     const float scale = (float)min(J.width, J.height) * 0.25f;
     const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
@@ -388,13 +434,13 @@ ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
         if (active) {
 #if FFB_RNG_MODE == 0
             ffb_pcg_dispatch(J, rng, wid, it, x, y);
-            k = ffb_select(sm, n_xf, rng.draw(0));
+            k = FFB_PICK(rng.draw(0), prev);
             plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];
             r0 = rng.state; r1 = rng.inc;
 #else
             PhiloxRng rng;
             rng.fill(J.seed_lo, J.seed_hi, wid, it);
-            k = ffb_select(sm, n_xf, rng.draw(0));
+            k = FFB_PICK(rng.draw(0), prev);
             plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];
             r0 = __float_as_uint(rng.w[2]); r1 = __float_as_uint(rng.w[3]);
 #endif
@@ -422,6 +468,7 @@ ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
         const u32 kp = s_kp[tid];
         k = (int)(kp & 0x7FFFFFFFu);
         plot = (kp >> 31) != 0u;
+        prev = k;                                // the gathered walker's transform, its next pick's row
         wid = s_wid[tid];
         active = k < FFB_MAXX;
         if (active) {
@@ -437,7 +484,8 @@ ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
 #endif
         }
     }
-    if (active) J.walkers[wid - J.walker0] = make_float4(x, y, ci, __uint_as_float(fuse));
+    (void)prev;
+    if (active) J.walkers[wid - J.walker0] = make_float4(x, y, ci, __uint_as_float(FFB_PACK_FUSE(fuse, prev)));
     ffb_count_inframe(J, inframe);
 #ifdef FFB_EMIT
     ffb_emit_finish(J, ffb_copies(sm));

@@ -278,6 +278,8 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     P.threads = job->threads ? job->threads : 128;
     if (P.threads % 32 || P.threads > 1024) fail(FFB_ERR_INVALID, "threads must be a multiple of 32, at most 1024");
     P.burn_in = job->burn_in ? job->burn_in : 20;
+    // An xaos walker's stored state holds its previous transform above the burn-in left.
+    if (!P.flame.xaos.empty() && P.burn_in >= (1u << 24)) fail(FFB_ERR_INVALID, "burn_in must be below 2^24 with xaos");
     P.ipt = job->iterations_per_thread ? job->iterations_per_thread : 1024;
     P.target = job->iterations ? job->iterations : P.flame.max_iterations * (uint64_t)P.ss * P.ss;
     uint64_t w = job->walkers;
@@ -1363,6 +1365,8 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
             j.seed = items[i].seed;
             if (j.iterations == 0) fail(FFB_ERR_INVALID, "every batch item needs its sample budget");
             B->flames[i].P = prepare(items[i].config, items[i].config_len, &j);
+            if (!B->flames[i].P.flame.xaos.empty())
+                fail(FFB_ERR_INVALID, "item " + std::to_string(i) + ": xaos flames are not batched; render it alone");
             if (B->flames[i].P.flame.filter.on())
                 fail(FFB_ERR_INVALID, "item " + std::to_string(i) + ": the spatial filter (filter_radius) is not batched; render it alone");
             check_de(B->flames[i].P.flame, B->flames[i].P.ss);

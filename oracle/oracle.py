@@ -122,6 +122,7 @@ class OFlame(ctypes.Structure):
         ("sym_kind", ctypes.c_int), ("sym_order", ctypes.c_int),
         ("sym_cx", ctypes.c_float), ("sym_cy", ctypes.c_float), ("sym_distance", ctypes.c_float),
         ("sym_rotation", ctypes.c_float),
+        ("xaos", ctypes.POINTER(ctypes.c_float)),
     ]
 
 
@@ -248,6 +249,18 @@ class Flame:
         s.cos_r, s.sin_r = math.cos(rot), math.sin(rot)
         s.width, s.height = width, height
         s.palette, s.pal_n = _fp(self.palette), len(self.palette) // 3
+        # Xaos (xaos.rs:29-40, 128-135): read when some weight differs from 1; missing entries are 1.
+        self.xaos = None
+        if flame.get("xaos"):
+            n = len(normals)
+            m = np.ones((n, n), np.float32)
+            for i, row in enumerate(flame["xaos"]):
+                for j, v in enumerate(row):
+                    if i < n and j < n:
+                        m[i, j] = v
+            if any(abs(f32(v) - 1.0) > 1e-6 for row in flame["xaos"] for v in row):
+                self.xaos = np.ascontiguousarray(m.ravel())
+                s.xaos = _fp(self.xaos)
         ps = flame.get("post_symmetry")
         if ps:
             s.sym_kind = {"none": 0, "xaxis": 1, "yaxis": 2, "point": 3}[ps.get("ty", "none")]
