@@ -270,7 +270,8 @@ def run_ours(args, rank, world, local_rank):
         "ms_per_frame": ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "kernel": "ffb_chaos", "kernel_ms": c_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "kernel": "chaos game: ffb_chaos_sorted, with ffb_plot beside it on a second stream (deferred plotting)",
+                     "kernel_ms": c_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
                      "peak_kind": peak_kind},
         "l2_atomic": {"achieved_splats_per_s": splat_rate, "peak_splats_per_s": splat_peak,
                       "frac": splat_rate / splat_peak, "peak_from": "ffb_atomic_bench kind 0, same histogram size"},

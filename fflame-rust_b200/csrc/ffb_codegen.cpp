@@ -161,10 +161,11 @@ std::string jac_names() {
 }  // namespace
 
 Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int threads, bool per_xform, bool exact,
-               int diff_window, int diff_ckpt, bool emit) {
+               int diff_window, int diff_ckpt, bool emit, bool defer) {
     Plan p;
     p.exact = exact;
     p.emit = emit;
+    p.defer = defer && !emit && diff_window == 0;
     p.diff_window = diff_window;
     p.diff_ckpt = diff_ckpt;
     p.rng_mode = rng_mode;
@@ -240,6 +241,9 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     if (math_mode == MATH_SFU) s << "#define FFB_SFU 1\n";
     if (exact) s << "#define FFB_EXACT 1\n";
     if (emit) s << "#define FFB_EMIT 1\n";
+    int nfd = 0;
+    for (auto& fi : p.fin) for (const VarDef* v : fi.vars) nfd += v->draws;
+    if (p.defer) s << "#define FFB_DEFER 1\n#define FFB_NFD " << nfd << "\n";
     s << "#define FFB_SYM_KIND " << p.sym_kind << "\n#define T_SYM " << p.t_sym << "\n";
     if (p.xaos) s << "#define FFB_XAOS 1\n#define T_XAOS " << p.t_xaos << "\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
@@ -287,6 +291,17 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     s << "template <class R> __device__ __forceinline__ void ffb_finals(const float* __restrict__ sm, float& x, float& y, R& rng) {\n";
     for (size_t c = 0; c < p.fin.size(); ++c) s << "    ffb_final_one(sm, " << c << ", x, y, rng, true);\n";
     s << "}\n";
+    if (p.defer) {
+        // The final chain's draws in the order it takes them (slot order),
+        // for the deferred plot: one plane of `stride` a draw.
+        s << "template <class R> __device__ __forceinline__ void ffb_capture_final_draws(R& rng, float* out, unsigned long long stride) {\n";
+        int m = 0;
+        for (auto& fi : p.fin)
+            for (size_t j = 0; j < fi.vars.size(); ++j)
+                for (int d = 0; d < fi.vars[j]->draws; ++d, ++m)
+                    s << "    { const float v = rng.draw(" << fi.slot[j] + d << "); out[" << m << "ull * stride] = v; }\n";
+        s << "    (void)rng; (void)out; (void)stride;\n}\n";
+    }
     s << kKernelsSrc << "\n";
     if (diff_window > 0) emit_diff(s, p);
     p.source = s.str();
@@ -295,7 +310,8 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
 
 bool plan_fits(const Plan& p, const Flame& f) {
     if ((int)f.xf.size() > p.maxx) return false;
-    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform, p.exact, p.diff_window, p.diff_ckpt, p.emit);
+    Plan q = make_plan(f, p.rng_mode, p.math_mode, p.maxx, p.threads, p.per_xform, p.exact, p.diff_window, p.diff_ckpt, p.emit,
+                       p.defer);
     return q.source == p.source;
 }
 

@@ -53,6 +53,7 @@ struct Plan {
     bool per_xform = false;
     bool exact = false;                    // u64 fixed-point histogram (ulonglong4 a pixel)
     bool emit = false;                     // tile-sorted accumulation: samples become records (ffb_emit)
+    bool defer = false;                    // deferred plotting: the chaos kernel stores samples, ffb_plot plots them
     // Differentiable render (ffb_diff.cuh): window = iterations each sample
     // is differentiated through, ckpt = checkpoint interval; 0 = off.
     int diff_window = 0, diff_ckpt = 0;
@@ -61,7 +62,7 @@ struct Plan {
 
 // Structure of `f` (rng/math modes as given; maxx >= f.xf.size()).
 Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx = 0, int threads = 128, bool per_xform = false,
-               bool exact = false, int diff_window = 0, int diff_ckpt = 0, bool emit = false);
+               bool exact = false, int diff_window = 0, int diff_ckpt = 0, bool emit = false, bool defer = false);
 // The table of `f` for a plan made from a flame of the same structure.
 std::vector<float> make_table(const Plan& p, const Flame& f);
 // Whether `f` fits plan `p` (same structure, n_xf <= maxx).

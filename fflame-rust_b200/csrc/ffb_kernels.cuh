@@ -15,6 +15,8 @@ struct ffb_launch {
     u32 n_iters, pal_n;
     int width, height;
     float zoom, pan_x, pan_y, cos_r, sin_r;
+    float4* rec;               // deferred plotting: n_iters x n_walkers samples (x, y, ci, flags)
+    float* rec_draws;          // and their final chain's draws, FFB_NFD planes of the same length
 };
 
 __device__ __forceinline__ int ffb_select(const float* __restrict__ sm, int n_xf, float u) {
@@ -261,40 +263,12 @@ __device__ __forceinline__ void ffb_sym_copy(const float* __restrict__ sm, int k
 }
 #endif
 
-// The rest of an iteration once transform k is picked and the opacity draw
-// made: affine, variations, post, bad-value respawn, colour, fuse, finals,
-// palette, world_to_pixel and the splat (main_template.wgsl:366-1320).
-template <bool PER_XFORM, class R>
-__device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
-                                         int k, bool plot, R& rng, u32 gw, u64 it, float& x, float& y, float& ci, u32& fuse,
-                                         float cx, float cy, float scale, u32& inframe) {
-    const float* q = sm + T_XF + k;
-    float ax = q[F_A * FFB_MAXX] * x + q[F_B * FFB_MAXX] * y + q[F_E * FFB_MAXX];
-    float ay = q[F_C * FFB_MAXX] * x + q[F_D * FFB_MAXX] * y + q[F_F * FFB_MAXX];
-    if (PER_XFORM) ffb_normal_k(sm, k, ax, ay, rng);                        // main_template.wgsl:366-376
-    else ffb_normal(sm, k, ax, ay, rng);
-#if FFB_HAS_POST
-    if (q[F_POST * FFB_MAXX] > 0.5f) {                                      // main_template.wgsl:380-384
-        float px = q[F_PA * FFB_MAXX] * ax + q[F_PB * FFB_MAXX] * ay + q[F_PE * FFB_MAXX];
-        float py = q[F_PC * FFB_MAXX] * ax + q[F_PD * FFB_MAXX] * ay + q[F_PF * FFB_MAXX];
-        ax = px; ay = py;
-    }
-#endif
-    if (!(fabsf(ax) <= 1e32f) || !(fabsf(ay) <= 1e32f)) {                  // main_template.wgsl:449-479
-#if FFB_RNG_MODE == 1
-        uint4 o = philox4(J.seed_lo, J.seed_hi, gw, (u32)it, 0xFFFFFFFFu, (u32)(it >> 32));
-        x = u24(o.x) * 2.0f - 1.0f;
-        y = u24(o.y) * 2.0f - 1.0f;
-#else
-        x = rng.draw(0) * 2.0f - 1.0f;
-        y = rng.draw(0) * 2.0f - 1.0f;
-#endif
-        fuse = J.burn_in;
-        return;
-    }
-    x = ax; y = ay;
-    ci = ci * q[F_C1 * FFB_MAXX] + q[F_C2 * FFB_MAXX];                       // main_template.wgsl:496-508
-    if (fuse > 0u) { fuse -= 1u; return; }                                 // main_template.wgsl:510-514
+// The plot of a kept sample: the final chain, the palette, the symmetry
+// copies, world_to_pixel and the splat (main_template.wgsl:663-1320).
+template <class R>
+__device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
+                                                float x, float y, float ci, bool plot, R& rng, float cx, float cy, float scale,
+                                                u32& inframe) {
     float fx = x, fy = y;
     ffb_finals(sm, fx, fy, rng);                                            // main_template.wgsl:663-717
     const int pal_idx = ffb_palette_index(ci, J.pal_n);
@@ -326,6 +300,74 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
         }
 #endif
     }
+}
+
+#ifdef FFB_DEFER
+// Deferred plotting: the chaos kernel stores each iteration's sample (its
+// point after the transform, colour index, plot flag) and the draws its
+// final chain takes, in the order it takes them; ffb_plot applies the rest.
+// A record a walker and iteration: (x, y, ci, flags) with flags bit 1 a
+// kept sample, bit 0 its opacity draw passed; 0 for burn-in and respawns.
+__device__ __forceinline__ u64 ffb_rec_index(const ffb_launch& J, u32 gw, u64 it) {
+    return (it - J.it0) * (u64)J.n_walkers + (u64)(gw - J.walker0);
+}
+#define FFB_DEFER_SKIP(J, gw, it) ((J).rec[ffb_rec_index((J), (gw), (it))] = make_float4(0.f, 0.f, 0.f, 0.f))
+template <class R>
+__device__ __forceinline__ void ffb_defer_store(const ffb_launch& J, u32 gw, u64 it, float x, float y, float ci, bool plot, R& rng) {
+    const u64 ri = ffb_rec_index(J, gw, it);
+    J.rec[ri] = make_float4(x, y, ci, __uint_as_float(2u | (plot ? 1u : 0u)));
+    ffb_capture_final_draws(rng, J.rec_draws + ri, (u64)J.n_iters * J.n_walkers);
+}
+// The stored draws handed back in order.
+struct SeqRng {
+    const float* d;
+    int i;
+    __device__ __forceinline__ float draw(int) { return d[i++]; }
+};
+#else
+#define FFB_DEFER_SKIP(J, gw, it) ((void)0)
+#endif
+
+// The rest of an iteration once transform k is picked and the opacity draw
+// made: affine, variations, post, bad-value respawn, colour, fuse, finals,
+// palette, world_to_pixel and the splat (main_template.wgsl:366-1320).
+template <bool PER_XFORM, class R>
+__device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
+                                         int k, bool plot, R& rng, u32 gw, u64 it, float& x, float& y, float& ci, u32& fuse,
+                                         float cx, float cy, float scale, u32& inframe) {
+    const float* q = sm + T_XF + k;
+    float ax = q[F_A * FFB_MAXX] * x + q[F_B * FFB_MAXX] * y + q[F_E * FFB_MAXX];
+    float ay = q[F_C * FFB_MAXX] * x + q[F_D * FFB_MAXX] * y + q[F_F * FFB_MAXX];
+    if (PER_XFORM) ffb_normal_k(sm, k, ax, ay, rng);                        // main_template.wgsl:366-376
+    else ffb_normal(sm, k, ax, ay, rng);
+#if FFB_HAS_POST
+    if (q[F_POST * FFB_MAXX] > 0.5f) {                                      // main_template.wgsl:380-384
+        float px = q[F_PA * FFB_MAXX] * ax + q[F_PB * FFB_MAXX] * ay + q[F_PE * FFB_MAXX];
+        float py = q[F_PC * FFB_MAXX] * ax + q[F_PD * FFB_MAXX] * ay + q[F_PF * FFB_MAXX];
+        ax = px; ay = py;
+    }
+#endif
+    if (!(fabsf(ax) <= 1e32f) || !(fabsf(ay) <= 1e32f)) {                  // main_template.wgsl:449-479
+#if FFB_RNG_MODE == 1
+        uint4 o = philox4(J.seed_lo, J.seed_hi, gw, (u32)it, 0xFFFFFFFFu, (u32)(it >> 32));
+        x = u24(o.x) * 2.0f - 1.0f;
+        y = u24(o.y) * 2.0f - 1.0f;
+#else
+        x = rng.draw(0) * 2.0f - 1.0f;
+        y = rng.draw(0) * 2.0f - 1.0f;
+#endif
+        fuse = J.burn_in;
+        FFB_DEFER_SKIP(J, gw, it);
+        return;
+    }
+    x = ax; y = ay;
+    ci = ci * q[F_C1 * FFB_MAXX] + q[F_C2 * FFB_MAXX];                       // main_template.wgsl:496-508
+    if (fuse > 0u) { fuse -= 1u; FFB_DEFER_SKIP(J, gw, it); return; }     // main_template.wgsl:510-514
+#ifdef FFB_DEFER
+    ffb_defer_store(J, gw, it, x, y, ci, plot, rng);
+#else
+    ffb_plot_sample(sm, pal, J, x, y, ci, plot, rng, cx, cy, scale, inframe);
+#endif
 }
 
 __device__ __forceinline__ void ffb_count_inframe(const ffb_launch& J, u32 inframe) {
@@ -539,3 +581,30 @@ extern "C" __global__ void ffb_apply_points(const float* __restrict__ table, int
     }
     xo[i] = x; yo[i] = y;
 }
+
+#ifdef FFB_DEFER
+// The plot of one launch's stored samples (the tail ffb_chaos defers): a
+// thread a record, grid-striding; samples are independent, so this kernel
+// has the parallelism the walkers' chains lack.
+extern "C" __global__ void __launch_bounds__(384) ffb_plot(const ffb_launch* __restrict__ jobs, int n_jobs) {
+    extern __shared__ float4 ffb_smem4[];
+    float* sm = reinterpret_cast<float*>(ffb_smem4);
+    float4* pal;
+    const ffb_launch& J = ffb_stage(jobs, n_jobs, sm, pal);
+    const float scale = (float)min(J.width, J.height) * 0.25f;
+    const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
+    const u64 n = (u64)J.n_iters * J.n_walkers;
+    u32 inframe = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const float4 r = J.rec[i];
+        const u32 fl = __float_as_uint(r.w);
+        if (!(fl & 2u)) continue;
+        float fd[FFB_NFD > 0 ? FFB_NFD : 1];
+#pragma unroll
+        for (int m = 0; m < FFB_NFD; ++m) fd[m] = J.rec_draws[(u64)m * n + i];
+        SeqRng rng{fd, 0};
+        ffb_plot_sample(sm, pal, J, r.x, r.y, r.z, (fl & 1u) != 0u, rng, cx, cy, scale, inframe);
+    }
+    ffb_count_inframe(J, inframe);
+}
+#endif

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <list>
 #include <map>
 #include <memory>
@@ -89,8 +90,10 @@ struct Launch {
     uint32_t n_iters, pal_n;
     int32_t width, height;
     float zoom, pan_x, pan_y, cos_r, sin_r;
+    void* rec;          // deferred plotting: the launch's samples
+    void* rec_draws;    // and their final chain's draws
 };
-static_assert(sizeof(Launch) == 120, "launch record layout");
+static_assert(sizeof(Launch) == 136, "launch record layout");
 
 struct DevBuf {
     void* p = nullptr;
@@ -110,6 +113,8 @@ struct Module {
     std::string key;
     cudaLibrary_t lib = nullptr;
     cudaKernel_t chaos = nullptr, chaos_sorted = nullptr, probe = nullptr, apply = nullptr;
+    cudaKernel_t plot = nullptr;   // deferred-plot modules only
+    int smem_attr_plot = 0;
     // Differentiable-render modules (ffb_diff.cuh) only.
     cudaKernel_t dforward = nullptr, dadjoint = nullptr, dtheta = nullptr, dprobe = nullptr;
     int smem_attr = 0, smem_attr_sorted = 0, smem_attr_dadj = 0;
@@ -139,6 +144,20 @@ struct ffb_renderer {
     DevBuf hist, walkers, table, palette, counters, jobs, rgba, de_out, de_tab, lut, f_out, tmp_in;
     DevBuf tile_rec, tile_tmp, tile_sorted, tile_meta;      // tile-sorted accumulation scratch
     DevBuf filt_batch, filt_tmp;                            // spatial filter: a batch's histogram, the row pass
+    // Deferred plotting: the plot kernel's stream, double-buffered sample
+    // records, events ordering the two streams.
+    cudaStream_t plot_stream = nullptr;
+    cudaEvent_t ev_main[2] = {nullptr, nullptr}, ev_plot[2] = {nullptr, nullptr}, ev_start = nullptr;
+    DevBuf rec[2], rec_draws[2];
+    void ensure_plot_stream() {
+        if (plot_stream) return;
+        ck(cudaStreamCreateWithFlags(&plot_stream, cudaStreamNonBlocking), "plot stream");
+        for (int i = 0; i < 2; ++i) {
+            ck(cudaEventCreateWithFlags(&ev_main[i], cudaEventDisableTiming), "event");
+            ck(cudaEventCreateWithFlags(&ev_plot[i], cudaEventDisableTiming), "event");
+        }
+        ck(cudaEventCreateWithFlags(&ev_start, cudaEventDisableTiming), "event");
+    }
     uint64_t h2d = 0, d2h = 0;      // bytes copied by the current call
     uint32_t launches = 0;          // kernels launched by the current call
     std::set<ffb_batch*> batches;   // live objects borrowing this renderer's modules
@@ -157,7 +176,14 @@ struct ffb_renderer {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& m : cache) if (m.lib) cudaLibraryUnload(m.lib);
         for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in,
-                          &tile_rec, &tile_tmp, &tile_sorted, &tile_meta, &filt_batch, &filt_tmp}) b->release();
+                          &tile_rec, &tile_tmp, &tile_sorted, &tile_meta, &filt_batch, &filt_tmp, &rec[0], &rec[1],
+                          &rec_draws[0], &rec_draws[1]}) b->release();
+        if (plot_stream) {
+            cudaStreamSynchronize(plot_stream);
+            for (int i = 0; i < 2; ++i) { cudaEventDestroy(ev_main[i]); cudaEventDestroy(ev_plot[i]); }
+            cudaEventDestroy(ev_start);
+            cudaStreamDestroy(plot_stream);
+        }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -190,6 +216,8 @@ struct ffb_renderer {
         ck(cudaLibraryGetKernel(&m.chaos_sorted, m.lib, "ffb_chaos_sorted"), "cudaLibraryGetKernel(ffb_chaos_sorted)");
         ck(cudaLibraryGetKernel(&m.probe, m.lib, "ffb_probe"), "cudaLibraryGetKernel(ffb_probe)");
         ck(cudaLibraryGetKernel(&m.apply, m.lib, "ffb_apply_points"), "cudaLibraryGetKernel(ffb_apply_points)");
+        if (src.find("#define FFB_DEFER 1") != std::string::npos)
+            ck(cudaLibraryGetKernel(&m.plot, m.lib, "ffb_plot"), "cudaLibraryGetKernel(ffb_plot)");
         if (src.find("ffb_diff_forward") != std::string::npos) {
             ck(cudaLibraryGetKernel(&m.dforward, m.lib, "ffb_diff_forward"), "cudaLibraryGetKernel(ffb_diff_forward)");
             ck(cudaLibraryGetKernel(&m.dadjoint, m.lib, "ffb_diff_adjoint"), "cudaLibraryGetKernel(ffb_diff_adjoint)");
@@ -239,6 +267,8 @@ struct Prepared {
     uint32_t schedule = 0;
     uint32_t count_bits = 32;
     uint32_t accumulate = 0;    // exact mode: 0 auto, 1 direct, 2 tile-sorted
+    bool threads_set = false;   // the job chose the block size (the sorted schedule's sorting group too)
+    uint32_t plot = 0;          // 0 auto, 1 inline, 2 deferred (the plot in its own kernel)
 };
 
 // Whether a render accumulates by tiles: exact mode, tile-sorted
@@ -276,6 +306,7 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     P.math = job->math;
     if (P.math != MATH_PRECISE && P.math != MATH_SFU) fail(FFB_ERR_INVALID, "math must be 0 (precise) or 1 (sfu)");
     P.threads = job->threads ? job->threads : 128;
+    P.threads_set = job->threads != 0;
     if (P.threads % 32 || P.threads > 1024) fail(FFB_ERR_INVALID, "threads must be a multiple of 32, at most 1024");
     P.burn_in = job->burn_in ? job->burn_in : 20;
     // An xaos walker's stored state holds its previous transform above the burn-in left.
@@ -299,7 +330,16 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     if (P.count_bits != 32 && P.count_bits != 64) fail(FFB_ERR_INVALID, "count_bits must be 32 or 64");
     P.accumulate = job->accumulate;
     if (P.accumulate > 2) fail(FFB_ERR_INVALID, "accumulate must be 0 (auto), 1 (direct) or 2 (tile-sorted)");
-    P.plan = make_plan(P.flame, P.rng, P.math, 0, 128, false, P.count_bits == 64, 0, 0, tiled_accumulation(P));
+    P.plot = job->plot;
+    if (P.plot > 2) fail(FFB_ERR_INVALID, "plot must be 0 (auto), 1 (inline) or 2 (deferred)");
+    const bool tiled = tiled_accumulation(P);
+    // Deferred plotting needs the counter-based stream (a launch of any
+    // length resumes it) and plots straight into the histogram.
+    // Auto: deferred for the sorted schedule over enough walkers to fill
+    // the machine (measured on the 1080p ss2 frame: 51 ms against 66).
+    const bool can_defer = P.rng == RNG_PHILOX && !tiled && !P.flame.filter.on() && P.walkers <= (1u << 23);
+    const bool defer = can_defer && (P.plot == 2 || (P.plot == 0 && P.schedule != 1 && P.walkers >= 16384));
+    P.plan = make_plan(P.flame, P.rng, P.math, 0, P.threads_set ? P.threads : 128, false, P.count_bits == 64, 0, 0, tiled, defer);
     P.table = make_table(P.plan, P.flame);
     P.palette = palette_table(P.flame);
     return P;
@@ -417,6 +457,7 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     if (sorted) {
         uint32_t per_sm = (P.walkers + (uint32_t)r->n_sm - 1) / (uint32_t)r->n_sm;
         threads = std::min<uint32_t>(1024, std::max<uint32_t>(64, (per_sm + 31) / 32 * 32));
+        if (P.threads_set) threads = std::min<uint32_t>(1024, std::max<uint32_t>(32, (P.threads + 31) / 32 * 32));
     }
     int smem = ((P.plan.table_size + 3) / 4) * 16 + (int)pal_n * 16;
     if (sorted) smem += (int)threads * 8 * 4 + 2 * (P.plan.maxx + 1) * 4;
@@ -433,6 +474,17 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         chunk = chunk / P.ipt * P.ipt;
     }
     if (filt) chunk = P.ipt;
+    // Deferred plotting: launches of kDeferIters iterations, each followed
+    // by the plot of its samples on the plot stream, which overlaps the
+    // next launch (two record buffers).  The plot kernel runs one block a
+    // multiprocessor, so the sorted chaos kernel's one block still fits
+    // beside it (with more plot blocks the two stopped overlapping: 77.7 ms
+    // a frame instead of 51; 256 iterations measured best of 64-512).
+    const bool defer = P.plan.defer;
+    constexpr uint64_t kDeferIters = 256;
+    constexpr unsigned kPlotThreads = 384;
+    // At most 2^27 records (2 GiB) a buffer.
+    if (defer) chunk = std::max<uint64_t>(16, std::min<uint64_t>(kDeferIters, (1ull << 27) / P.walkers));
     const uint32_t blocks = (P.walkers + threads - 1) / threads;
     const double rot = P.flame.rotation;
     Launch L{};
@@ -467,21 +519,54 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     }
     const size_t n_chunks = (size_t)((total_iters + chunk - 1) / chunk);
     Launch* d_jobs = (Launch*)r->jobs.ensure(sizeof(Launch) * std::max<size_t>(1, n_chunks));
+    int nfd = 0;
+    if (defer) {
+        for (auto& fi : P.plan.fin) for (const VarDef* v : fi.vars) nfd += v->draws;
+        const size_t nrec = (size_t)chunk * P.walkers;
+        r->ensure_plot_stream();
+        for (int b = 0; b < 2; ++b) {
+            r->rec[b].ensure(nrec * 16);
+            r->rec_draws[b].ensure(std::max<size_t>(4, nrec * 4 * (size_t)nfd));
+        }
+    }
     std::vector<Launch> ls;
     for (uint64_t it0 = 0; it0 < total_iters; it0 += chunk) {
         L.it0 = it0;
         L.n_iters = (uint32_t)std::min<uint64_t>(chunk, total_iters - it0);
+        if (defer) { L.rec = r->rec[ls.size() % 2].p; L.rec_draws = r->rec_draws[ls.size() % 2].p; }
         ls.push_back(L);
     }
     ck(cudaMemcpyAsync(d_jobs, ls.data(), ls.size() * sizeof(Launch), cudaMemcpyHostToDevice, s), "upload launches");
     r->h2d += ls.size() * sizeof(Launch);
+    const int smem_plot = ((P.plan.table_size + 3) / 4) * 16 + (int)pal_n * 16;
+    if (defer) {
+        if (smem_plot > 48 * 1024 && m.smem_attr_plot < smem_plot) {
+            ck(cudaFuncSetAttribute((const void*)m.plot, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_plot), "smem attribute");
+            m.smem_attr_plot = smem_plot;
+        }
+        ck(cudaEventRecord(r->ev_start, s), "event");                          // the clears and uploads before
+        ck(cudaStreamWaitEvent(r->plot_stream, r->ev_start, 0), "plot stream waits");
+    }
     for (size_t i = 0; i < ls.size(); ++i) {
         Launch* jp = d_jobs + i;
         int nj = 1;
         void* args[] = {&jp, &nj};
         if (filt) ck(cudaMemsetAsync(batch, 0, npx * 16, s), "clear batch histogram");
+        if (defer && i >= 2) ck(cudaStreamWaitEvent(s, r->ev_plot[i % 2], 0), "record buffer free");
         ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch ffb_chaos");
         r->launches += 1;
+        if (defer) {
+            ck(cudaEventRecord(r->ev_main[i % 2], s), "event");
+            ck(cudaStreamWaitEvent(r->plot_stream, r->ev_main[i % 2], 0), "plot waits for its samples");
+            ck(cudaLaunchKernel((const void*)m.plot, dim3((unsigned)r->n_sm), dim3(kPlotThreads), args, (size_t)smem_plot,
+                                r->plot_stream), "launch ffb_plot");
+            ck(cudaEventRecord(r->ev_plot[i % 2], r->plot_stream), "event");
+            r->launches += 1;
+            if (i + 1 == ls.size()) {
+                ck(cudaStreamWaitEvent(s, r->ev_plot[i % 2], 0), "render waits for the last plot");
+                if (i >= 1) ck(cudaStreamWaitEvent(s, r->ev_plot[(i + 1) % 2], 0), "render waits for the plots");
+            }
+        }
         if (filt) {
             // The batch's plotted samples, as the reference counts them (compute_kernel.rs:1413-1421):
             // its walkers' iterations past the burn-in.
@@ -1119,6 +1204,20 @@ FFB_API int ffb_finish_device(ffb_renderer* r, const char* config, size_t len, c
         check_de(P.flame, P.ss);
         finish_device(r, P, (const float4*)d_hist, total_samples, row0, rows, job->transparent, d_rgba,
                       stream ? (cudaStream_t)stream : r->stream);
+    });
+}
+
+FFB_API int ffb_specialize_job(const char* config, size_t len, const ffb_job* job, size_t* cubin_bytes, char* source,
+                               size_t source_len) {
+    return guard([&] {
+        Prepared P = prepare(config, len, job, false);
+        std::vector<char> cubin = ffb_renderer::nvrtc_cubin(P.plan.source);
+        if (cubin_bytes) *cubin_bytes = cubin.size();
+        if (source && source_len) {
+            size_t n = std::min(source_len - 1, P.plan.source.size());
+            std::memcpy(source, P.plan.source.data(), n);
+            source[n] = 0;
+        }
     });
 }
 

@@ -29,7 +29,7 @@ EXPORTS = [
     "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
     "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
     "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize", "ffb_encode_png",
-    "ffb_flame_import", "ffb_histogram_f32", "ffb_hist_filter",
+    "ffb_flame_import", "ffb_histogram_f32", "ffb_hist_filter", "ffb_specialize_job",
 ]
 
 
@@ -48,7 +48,7 @@ class Job(ctypes.Structure):
         ("supersample", ctypes.c_uint32), ("rng", ctypes.c_int32), ("math", ctypes.c_int32),
         ("transparent", ctypes.c_int32), ("threads", ctypes.c_int32), ("seed", ctypes.c_uint64),
         ("walker0", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("count_bits", ctypes.c_uint32),
-        ("accumulate", ctypes.c_uint32),
+        ("accumulate", ctypes.c_uint32), ("plot", ctypes.c_uint32),
     ]
 
 
@@ -117,11 +117,12 @@ SCHEDULE = {"auto": 0, "plain": 1, "sorted": 2}
 
 
 ACCUMULATE = {"auto": 0, "direct": 1, "tiled": 2}
+PLOT = {"auto": 0, "inline": 1, "deferred": 2}
 
 
 def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0, walkers=0, supersample=1,
              rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0, schedule="auto", count_bits=32,
-             accumulate="auto"):
+             accumulate="auto", plot="auto"):
     j = Job()
     j.width, j.height, j.iterations = width, height, int(iterations or 0)
     j.iterations_per_thread, j.burn_in, j.walkers = iterations_per_thread, burn_in, walkers
@@ -132,6 +133,7 @@ def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0
     j.schedule = SCHEDULE[schedule] if isinstance(schedule, str) else schedule
     j.count_bits = count_bits
     j.accumulate = ACCUMULATE[accumulate] if isinstance(accumulate, str) else accumulate
+    j.plot = PLOT[plot] if isinstance(plot, str) else plot
     return j
 
 
@@ -376,6 +378,17 @@ def specialize(config, rng="philox", math="precise"):
     buf = ctypes.create_string_buffer(1 << 20)
     _check(lib().ffb_specialize(cfg, ctypes.c_size_t(len(cfg)), ctypes.c_int32(RNG[rng]), ctypes.c_int32(MATH[math]),
                                 ctypes.byref(n), buf, ctypes.c_size_t(len(buf))))
+    return n.value, buf.value.decode()
+
+
+def specialize_job(config, **job):
+    """NVRTC-compile the module a render of `job` would use (no device needed): (cubin bytes, source)."""
+    cfg = _text(config)
+    j = make_job(**job)
+    n = ctypes.c_size_t()
+    buf = ctypes.create_string_buffer(1 << 21)
+    _check(lib().ffb_specialize_job(cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), ctypes.byref(n), buf,
+                                    ctypes.c_size_t(len(buf))))
     return n.value, buf.value.decode()
 
 

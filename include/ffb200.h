@@ -81,7 +81,9 @@ typedef struct {
     int32_t rng;                       /* FFB_RNG_* (default FFB_RNG_PHILOX) ; -1 = default */
     int32_t math;                      /* FFB_MATH_* */
     int32_t transparent;               /* 0 opaque, 1 straight alpha, 2 premultiplied */
-    int32_t threads;                   /* threads a block (0: 128) */
+    int32_t threads;                   /* threads a block (0: 128; the sorted schedule: one block a
+                                          multiprocessor holding its share of the walkers) -- under the
+                                          sorted schedule also the group the walkers are sorted within */
     uint64_t seed;                     /* 0: the config's (12345 under deterministic_rng) */
     uint32_t walker0;                  /* first walker id of this shard (multi-GPU sharding) */
     uint32_t schedule;                 /* 0 auto, 1 one walker a thread, 2 transform-sorted (same orbits) */
@@ -93,6 +95,11 @@ typedef struct {
                                           direct), 1 direct (a splat's atomics on the histogram), 2
                                           tile-sorted (samples emitted as records, sorted by 64x64 tile,
                                           summed in shared memory; the same bits as direct) */
+    uint32_t plot;                     /* 0 auto, 1 inline (each walker plots its own samples), 2 deferred:
+                                          the chaos kernel stores its samples and a plot kernel (the final
+                                          chain, palette, symmetry copies, splat) runs beside the next
+                                          launch on a second stream; the same histogram (Philox stream, no
+                                          spatial filter, direct accumulation; otherwise inline) */
 } ffb_job;
 
 /* RenderOutput (src/renderer/render.rs:207-218). */
@@ -305,6 +312,10 @@ void ffb_batch_destroy(ffb_batch* b);
  * bytes of the generated source.  Needs no GPU. */
 int ffb_specialize(const char* config, size_t config_len, int32_t rng, int32_t math, size_t* cubin_bytes,
                    char* source, size_t source_len);
+/* The module a render of `job` would compile (its rng, math, count_bits,
+ * accumulation and plot modes; width and height may be 0): as ffb_specialize. */
+int ffb_specialize_job(const char* config, size_t config_len, const ffb_job* job, size_t* cubin_bytes, char* source,
+                       size_t source_len);
 
 /* The splat-throughput microbenchmark: `samples` random splats of `kind`
  * (0: the 4-atomic splat, 1: one u32 atomic, 2: one f32x4 reduction) into
