@@ -283,10 +283,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
         const Plan::Fin& fi = p.fin[c];
         s << "    case " << c << ": {\n        const float* q = sm + " << fi.off << ";\n";
         s << "        if (aff) { float ax = q[0] * x + q[1] * y + q[4]; float ay = q[2] * x + q[3] * y + q[5]; x = ax; y = ay; }\n";
-        // A final's variations are those of nonzero weight (final_vars), so
-        // their weight tests are always true: leaving them out makes the chain
-        // straight-line code (the deferred plot interleaves two records' chains).
-        emit_phases(s, fi.vars, [&](int j) { return final_site(fi, j); }, "        ", false);
+        emit_phases(s, fi.vars, [&](int j) { return final_site(fi, j); }, "        ", true);
         s << "        if (aff && q[12] > 0.5f) { float px = q[6] * rx + q[7] * ry + q[10]; float py = q[8] * rx + q[9] * ry + q[11]; rx = px; ry = py; }\n";
         s << "        x = rx; y = ry;\n        break; }\n";
     }

@@ -263,11 +263,14 @@ __device__ __forceinline__ void ffb_sym_copy(const float* __restrict__ sm, int k
 }
 #endif
 
-// The plot of a kept sample after its final chain: the palette, the
-// symmetry copies, world_to_pixel and the splat (main_template.wgsl:747-1320).
-__device__ __forceinline__ void ffb_plot_tail(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
-                                              float fx, float fy, float ci, bool plot, float cx, float cy, float scale,
-                                              u32& inframe) {
+// The plot of a kept sample: the final chain, the palette, the symmetry
+// copies, world_to_pixel and the splat (main_template.wgsl:663-1320).
+template <class R>
+__device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
+                                                float x, float y, float ci, bool plot, R& rng, float cx, float cy, float scale,
+                                                u32& inframe) {
+    float fx = x, fy = y;
+    ffb_finals(sm, fx, fy, rng);                                            // main_template.wgsl:663-717
     const int pal_idx = ffb_palette_index(ci, J.pal_n);
     const float4 c = pal[pal_idx];                                          // main_template.wgsl:766-772
 #if FFB_SYM_KIND != 0
@@ -297,16 +300,6 @@ __device__ __forceinline__ void ffb_plot_tail(const float* __restrict__ sm, cons
         }
 #endif
     }
-}
-
-// The plot of a kept sample: its final chain (main_template.wgsl:663-717), then the tail.
-template <class R>
-__device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
-                                                float x, float y, float ci, bool plot, R& rng, float cx, float cy, float scale,
-                                                u32& inframe) {
-    float fx = x, fy = y;
-    ffb_finals(sm, fx, fy, rng);
-    ffb_plot_tail(sm, pal, J, fx, fy, ci, plot, cx, cy, scale, inframe);
 }
 
 #ifdef FFB_DEFER
@@ -601,29 +594,16 @@ extern "C" __global__ void __launch_bounds__(384) ffb_plot(const ffb_launch* __r
     const float scale = (float)min(J.width, J.height) * 0.25f;
     const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
     const u64 n = (u64)J.n_iters * J.n_walkers;
-    const u64 stride = (u64)gridDim.x * blockDim.x;
     u32 inframe = 0;
-    // Two records a pass: both final chains first (independent straight-line
-    // code the compiler interleaves), then their tails.
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
-        const u64 i1 = i + stride;
-        const bool has1 = i1 < n;
-        const float4 r0 = J.rec[i];
-        const float4 r1 = has1 ? J.rec[i1] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const u32 f0 = __float_as_uint(r0.w), f1 = __float_as_uint(r1.w);
-        if (!((f0 | f1) & 2u)) continue;
-        float d0[FFB_NFD > 0 ? FFB_NFD : 1], d1[FFB_NFD > 0 ? FFB_NFD : 1];
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const float4 r = J.rec[i];
+        const u32 fl = __float_as_uint(r.w);
+        if (!(fl & 2u)) continue;
+        float fd[FFB_NFD > 0 ? FFB_NFD : 1];
 #pragma unroll
-        for (int m = 0; m < FFB_NFD; ++m) {
-            d0[m] = J.rec_draws[(u64)m * n + i];
-            d1[m] = has1 ? J.rec_draws[(u64)m * n + i1] : 0.0f;
-        }
-        SeqRng g0{d0, 0}, g1{d1, 0};
-        float x0 = r0.x, y0 = r0.y, x1 = r1.x, y1 = r1.y;
-        ffb_finals(sm, x0, y0, g0);
-        ffb_finals(sm, x1, y1, g1);
-        if (f0 & 2u) ffb_plot_tail(sm, pal, J, x0, y0, r0.z, (f0 & 1u) != 0u, cx, cy, scale, inframe);
-        if (f1 & 2u) ffb_plot_tail(sm, pal, J, x1, y1, r1.z, (f1 & 1u) != 0u, cx, cy, scale, inframe);
+        for (int m = 0; m < FFB_NFD; ++m) fd[m] = J.rec_draws[(u64)m * n + i];
+        SeqRng rng{fd, 0};
+        ffb_plot_sample(sm, pal, J, r.x, r.y, r.z, (fl & 1u) != 0u, rng, cx, cy, scale, inframe);
     }
     ffb_count_inframe(J, inframe);
 }
