@@ -46,7 +46,75 @@ struct Site {
     std::string w;
     std::function<std::string(int)> xf;
     int slot = -1;
+    std::string st;     // stateful variations: the walker's first state slot of this call (float*)
+    std::string inst;   // subflames: the instance number keying the subflame's own stream (u32)
 };
+
+// The walker's state slots (compute_state_layout, transforms.rs:226-300):
+// transform by transform in the reference's xform-id order -- normals, the
+// final pool, then each subflame's normals and finals -- the stateful
+// variations it uses, in local order.  A subflame variation inside a
+// subflame never runs (the inner dispatcher leaves it out) and takes none.
+// `init` marks the entries whose `wgsl_state_init` runs each dispatch (the
+// reference's layout holds weights above 1e-6 in magnitude).
+struct StEntry {
+    int kind;               // 0 normal, 1 final (pool index), 2 subflame s, transform t (normals then finals)
+    int s, t;
+    const VarDef* v;
+    int base;
+    bool init;
+};
+
+std::vector<StEntry> state_layout(const Flame& f, int& total) {
+    std::vector<StEntry> out;
+    int cur = 0;
+    auto lid = [&](const VarDef* v) { return (int)(std::find(f.local.begin(), f.local.end(), v) - f.local.begin()); };
+    auto emit = [&](int kind, int sidx, int t, const XForm& x) {
+        std::vector<std::pair<const VarDef*, float>> vs;
+        for (auto& pv : x.vars)
+            if (pv.second != 0.0f && pv.first->state > 0 && !(kind == 2 && (pv.first->flags & VF_SUB))) vs.push_back(pv);
+        std::sort(vs.begin(), vs.end(), [&](const auto& a, const auto& b) { return lid(a.first) < lid(b.first); });
+        for (auto& pv : vs) {
+            out.push_back({kind, sidx, t, pv.first, cur, pv.first->init_draws > 0 && std::fabs(pv.second) > 1e-6f});
+            cur += pv.first->state;
+        }
+    };
+    for (size_t k = 0; k < f.xf.size(); ++k) emit(0, 0, (int)k, f.xf[k]);
+    for (size_t c = 0; c < f.fin.size(); ++c) emit(1, 0, (int)c, f.fin[c]);
+    for (size_t si = 0; si < f.sub.size(); ++si) {
+        const SubFlame& S = f.sub[si];
+        for (size_t t = 0; t < S.xf.size() + S.fin.size(); ++t)
+            emit(2, (int)si, (int)t, t < S.xf.size() ? S.xf[t] : S.fin[t - S.xf.size()]);
+    }
+    total = cur;
+    return out;
+}
+
+int state_base(const std::vector<StEntry>& L, int kind, int sidx, int t, const VarDef* v) {
+    for (auto& e : L) if (e.kind == kind && e.s == sidx && e.t == t && e.v == v) return e.base;
+    return -1;
+}
+
+// A subflame's inner transforms (normals then finals) and, per transform,
+// the variations its dispatcher runs: weight other than 0, no subflame
+// variation (shader_builder_v2.rs:2391-2420), local order.
+std::vector<const VarDef*> inner_vars(const Flame& f, const XForm& x) {
+    std::vector<const VarDef*> out;
+    for (const VarDef* v : f.local)
+        if (!(v->flags & VF_SUB) && x.var_weight(v) != 0.0f) out.push_back(v);
+    return out;
+}
+const XForm& inner_xf(const SubFlame& S, size_t t) { return t < S.xf.size() ? S.xf[t] : S.fin[t - S.xf.size()]; }
+
+// Inner transform record: affine a..f, post a..f, post flag, colour
+// C1, C2, opacity, direct colour, then per variation its weight, its
+// packed parameters and (stateful) its state base.
+constexpr int kSubRec = 17;
+int inner_rec_size(const std::vector<const VarDef*>& vs) {
+    int n = kSubRec;
+    for (const VarDef* v : vs) n += 1 + v->slots() + (v->state > 0 ? 1 : 0);
+    return n;
+}
 
 // Normal transform k's site (k a source expression).
 Site normal_site(const Plan& p, int j, const std::string& k) {
@@ -56,10 +124,16 @@ Site normal_site(const Plan& p, int j, const std::string& k) {
     c.w = "sm[T_VW + " + std::to_string(j) + " * FFB_MAXX + " + k + "]";
     c.xf = [k](int f) { return "sm[T_XF + " + std::to_string(f) + " * FFB_MAXX + " + k + "]"; };
     c.slot = p.normal_slot[j];
+    if (p.st_row[j] >= 0) {
+        const std::string b = "sm[T_ST + " + std::to_string(p.st_row[j]) + " * FFB_MAXX + " + k + "]";
+        c.st = "ffb_st(ctx, " + b + ")";
+        c.inst = "ffb_u32(" + b + ")";
+    }
     return c;
 }
 
-// Final c's site: its record q (affine at q[0..5], weights at q[13..]).
+// Final c's site: its record q (affine at q[0..5], weights at q[13..],
+// then the parameter rows, then each variation's state base).
 Site final_site(const Plan::Fin& fi, int j) {
     Site c;
     const int nv = (int)fi.vars.size(), off = 13 + nv + fi.prm_off[j];
@@ -67,7 +141,97 @@ Site final_site(const Plan::Fin& fi, int j) {
     c.w = "q[" + std::to_string(13 + j) + "]";
     c.xf = [](int f) { return "q[" + std::to_string(f) + "]"; };
     c.slot = fi.slot[j];
+    const std::string b = "q[" + std::to_string(13 + nv + fi.prm_slots + j) + "]";
+    c.st = "ffb_st(ctx, " + b + ")";
+    c.inst = "ffb_u32(" + b + ")";
     return c;
+}
+
+// Inner variation j of a subflame transform whose record is q.
+Site inner_site(const std::vector<const VarDef*>& vs, int j) {
+    int off = kSubRec;
+    for (int i = 0; i < j; ++i) off += 1 + vs[i]->slots() + (vs[i]->state > 0 ? 1 : 0);
+    Site c;
+    c.w = "q[" + std::to_string(off) + "]";
+    c.prm = [off](int q) { return "q[" + std::to_string(off + 1 + q) + "]"; };
+    c.xf = [](int f) { return "q[" + std::to_string(f) + "]"; };
+    c.slot = 0;                                   // the subflame's draws are sequential
+    if (vs[j]->state > 0) c.st = "ffb_st(ctx, q[" + std::to_string(off + 1 + vs[j]->slots()) + "])";
+    return c;
+}
+
+void emit_phases(std::ostringstream& s, const std::vector<const VarDef*>& vars, const std::function<Site(int)>& site,
+                 const char* ind, bool gate, const char* vc = "ctx.vc");
+
+// One subflame (subflame.wgsl:254-412, 2-D arm): from the walker's state
+// (point, colour, last output; a zero point or a non-finite one walks the
+// 42-step prefuse from a random start), step the inner chaos game until a
+// visible transform (opacity 1, or its roll passes; at most 1000 steps past
+// the prefuse), map the point through the finals to q, place q by scale,
+// rotation and offset, and keep the walk and q in the state.  State slots:
+// x, y, colour, q.x, q.y, q.colour.  Inner transform t's record at
+// sm[rec[t]]; the block at sm[blk]: total weight (at least 1e-6), whether
+// any transform can be visible, the running sums of the weights.
+void emit_subflame(std::ostringstream& s, const Flame& f, int si, int blk, const std::vector<int>& rec) {
+    const SubFlame& S = f.sub[si];
+    const int N = (int)S.xf.size();
+    s << "template <class S> __device__ void ffb_sub_" << si << "(const float* __restrict__ sm, FfbCtx& ctx, S& rng, float scale, "
+         "float cs, float sn, float offx, float offy, float* st, float& qx, float& qy, float& qw) {\n";
+    if (N == 0) {
+        s << "    (void)sm; (void)ctx; (void)rng; (void)scale; (void)cs; (void)sn; (void)offx; (void)offy; (void)st;\n"
+             "    qx = 0.0f; qy = 0.0f; qw = 0.0f;\n}\n";
+        return;
+    }
+    s << "    const u32 sd = ctx.stride;\n"
+         "    float px = st[0], py = st[sd], color = st[2 * sd];\n"
+         "    const bool pre = (px == 0.0f && py == 0.0f) || !(fabsf(px) <= 1e32f) || !(fabsf(py) <= 1e32f) || !(fabsf(color) <= 1e32f);\n"
+         "    if (pre) { px = rng.draw(0) - 0.5f; py = rng.draw(0) - 0.5f; color = rng.draw(0); }\n"
+         "    const float* B = sm + " << blk << ";\n"
+         "    const u32 pre_steps = pre ? 42u : 0u;\n"
+         "    const u32 steps = pre_steps + (B[1] > 0.5f ? 1000u : 0u);\n"
+         "    bool visible = false;\n"
+         "    for (u32 it = 0; it < steps; ++it) {\n"
+         "        const float r = rng.draw(0) * B[0];\n"
+         "        int pk = " << N - 1 << ";\n"
+         "        for (int i = 0; i < " << N << "; ++i) if (r < B[2 + i]) { pk = i; break; }\n"
+         "        float op = 1.0f;\n"
+         "        switch (pk) {\n";
+    auto body = [&](size_t t, const char* pin_x, const char* pin_y, const char* cin, const char* pout_x, const char* pout_y,
+                    const char* cout, const char* ind) {
+        const std::vector<const VarDef*> vs = inner_vars(f, inner_xf(S, t));
+        s << ind << "const float* q = sm + " << rec[t] << ";\n"
+          << ind << "const float cb = " << cin << " * q[13] + q[14];\n"
+          << ind << "float vc = cb;\n"
+          << ind << "float x = q[0] * " << pin_x << " + q[1] * " << pin_y << " + q[4];\n"
+          << ind << "float y = q[2] * " << pin_x << " + q[3] * " << pin_y << " + q[5];\n"
+          << ind << "{\n";
+        const std::string ind2 = std::string(ind) + "    ";
+        emit_phases(s, vs, [&](int j) { return inner_site(vs, j); }, ind2.c_str(), true, "vc");
+        s << ind2 << "x = rx; y = ry;\n" << ind << "}\n"
+          << ind << "if (q[12] > 0.5f) { const float ux = q[6] * x + q[7] * y + q[10]; const float uy = q[8] * x + q[9] * y + q[11]; x = ux; y = uy; }\n"
+          << ind << pout_x << " = x; " << pout_y << " = y; " << cout << " = cb + q[16] * (vc - cb);\n";
+    };
+    for (int t = 0; t < N; ++t) {
+        s << "        case " << t << ": {\n";
+        body((size_t)t, "px", "py", "color", "px", "py", "color", "            ");
+        s << "            op = q[15];\n            break; }\n";
+    }
+    s << "        default: break;\n        }\n"
+         "        if (it >= pre_steps && (op >= 1.0f || rng.draw(0) < op)) { visible = true; break; }\n"
+         "    }\n"
+         "    st[0] = px; st[sd] = py; st[2 * sd] = color;\n"
+         "    if (!visible) { qx = st[3 * sd]; qy = st[4 * sd]; qw = st[5 * sd]; return; }\n"
+         "    float fx = px, fy = py, fc = color;\n";
+    for (size_t t = (size_t)N; t < S.xf.size() + S.fin.size(); ++t) {
+        s << "    {\n";
+        body(t, "fx", "fy", "fc", "fx", "fy", "fc", "        ");
+        s << "    }\n";
+    }
+    s << "    const float x = scale * fx, y = scale * fy;\n"
+         "    qx = x * cs - y * sn + offx;\n"
+         "    qy = x * sn + y * cs + offy;\n"
+         "    qw = fc;\n"
+         "    st[3 * sd] = qx; st[4 * sd] = qy; st[5 * sd] = qw;\n}\n";
 }
 
 // `v_name(px, py[, rng, slot][, params...][, w][, a..f], ox, oy)`.
@@ -78,7 +242,25 @@ std::string call(const VarDef* v, const Site& c, const char* px = "x", const cha
     for (int q = 0; q < v->slots(); ++q) o << ", " << c.prm(q);
     if (v->flags & VF_W) o << ", " << c.w;
     if (v->flags & VF_XF) for (int f = 0; f < 6; ++f) o << ", " << c.xf(f);
+    if (v->state > 0) o << ", " << c.st << ", ctx.stride";
     o << ", ox, oy)";
+    return o.str();
+}
+
+// subflame_wf / pre_subflame_wf (subflame.rs:122-143, 195-204): step the
+// subflame (subflame_iterate, placed by scale, angle and offsets), take its
+// colour when color_mode is not -1, and return q / weight (the normal
+// phase multiplies the weight back) or, in the pre phase, q itself.
+// Parameter row: subflame_id, scale, angle, offset_x, offset_y, offset_z,
+// colorscale_z, color_mode, cos(angle), sin(angle).
+std::string call_sub(const VarDef* v, const Site& c, const char* vc) {
+    std::ostringstream o;
+    o << "auto&& sq = ffb_sub_stream(rng, ctx, " << c.inst << "); float qx, qy, qw; "
+      << "ffb_subflame(sm, ctx, sq, ffb_u32(" << c.prm(0) << "), " << c.prm(1) << ", " << c.prm(8) << ", " << c.prm(9) << ", "
+      << c.prm(3) << ", " << c.prm(4) << ", " << c.st << ", qx, qy, qw); "
+      << "if (ffb_i32(" << c.prm(7) << ") != -1) " << vc << " = qw; ";
+    if (v->flags & VF_PRE) o << "ox = qx; oy = qy;";
+    else o << "ox = qx / w; oy = qy / w;";
     return o.str();
 }
 
@@ -100,8 +282,9 @@ std::string jcall(const VarDef* v, const Site& c) {
 // its phase.  `site(j)` locates variation j of `vars`; `gate` false drops
 // the weight test (the per-transform form lists only the variations the
 // transform uses).
+// `vc` names the colour register a WritesColor variation writes.
 void emit_phases(std::ostringstream& s, const std::vector<const VarDef*>& vars,
-                 const std::function<Site(int)>& site, const char* ind, bool gate) {
+                 const std::function<Site(int)>& site, const char* ind, bool gate, const char* vc) {
     s << ind << "float tx = x, ty = y, rx = 0.0f, ry = 0.0f, ox, oy;\n";
     auto open = [&](const Site& c) {
         s << ind << "{ const float w = " << c.w << "; " << (gate ? "if (w != 0.0f) { " : "{ ");
@@ -113,9 +296,10 @@ void emit_phases(std::ostringstream& s, const std::vector<const VarDef*>& vars,
             if (ph != pass) continue;
             const Site c = site((int)j);
             open(c);
-            if (ph == 0) s << call(v, c, "tx", "ty") << "; tx = ox; ty = oy;";
-            else if (ph == 1) s << call(v, c, "tx", "ty") << "; rx = rx + w * ox; ry = ry + w * oy;";
-            else s << call(v, c, "rx", "ry") << "; rx = ox; ry = oy;";
+            const std::string body = (v->flags & VF_SUB) ? call_sub(v, c, vc) : call(v, c, ph == 2 ? "rx" : "tx", ph == 2 ? "ry" : "ty") + ";";
+            if (ph == 0) s << body << " tx = ox; ty = oy;";
+            else if (ph == 1) s << body << " rx = rx + w * ox; ry = ry + w * oy;";
+            else s << body << " rx = ox; ry = oy;";
             s << " } }   // " << v->name << "\n";
         }
     }
@@ -199,6 +383,33 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
         p.fin.push_back(fi);
     }
     p.n_slots = slot;
+    int n_state = 0;
+    const std::vector<StEntry> layout = state_layout(f, n_state);
+    p.n_state = n_state;
+    for (auto& e : layout) p.n_init += e.init ? 1 : 0;
+    p.st_row.assign(p.normal.size(), -1);
+    int st_rows = 0;
+    for (size_t j = 0; j < p.normal.size(); ++j) {
+        if (p.normal[j]->state > 0) p.st_row[j] = st_rows++;
+        p.dc |= (p.normal[j]->flags & VF_DC) != 0;
+    }
+    // The deferred plot runs the finals out of walker order, with the draws
+    // captured at their static slots: finals that carry state or step a
+    // subflame stay inline.
+    for (auto& fi : p.fin)
+        for (const VarDef* v : fi.vars)
+            if (v->state > 0 || (v->flags & VF_SUB)) p.defer = false;
+    // A subflame call's own stream holds 2^18 words an instance.
+    for (const SubFlame& S : f.sub) {
+        int most = 0, fin = 0;
+        for (size_t t = 0; t < S.xf.size() + S.fin.size(); ++t) {
+            int d = 0;
+            for (const VarDef* v : inner_vars(f, inner_xf(S, t))) d += v->draws;
+            if (t < S.xf.size()) most = std::max(most, d); else fin += d;
+        }
+        if (3 + 1042 * (2 + most) + fin >= (1 << 18))
+            throw std::runtime_error("a subflame's transforms take too many random draws a step for this build");
+    }
     // Philox words live in registers (4 a block): a bound keeps them there.
     if (p.n_slots > kMaxDrawSlots)
         throw std::runtime_error("the flame's variations take " + std::to_string(p.n_slots - 2) +
@@ -218,19 +429,34 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     }
     for (auto& x : f.xf) p.has_post |= x.post;
     const int M = p.maxx, NVN = (int)p.normal.size();
+    constexpr int kXfFields = 17;                 // F_NFIELDS of ffb_device.cuh
     p.t_cum = 1;
     p.t_xf = p.t_cum + M;
-    p.t_vw = p.t_xf + 16 * M;
+    p.t_vw = p.t_xf + kXfFields * M;
     p.t_vp = p.t_vw + NVN * M;
     p.t_fin = p.t_vp + p.vp_slots * M;
     int off = p.t_fin;
-    for (auto& fi : p.fin) { fi.off = off; off += 13 + (int)fi.vars.size() + fi.prm_slots; }
+    for (auto& fi : p.fin) { fi.off = off; off += 13 + 2 * (int)fi.vars.size() + fi.prm_slots; }
     p.sym_kind = f.sym.kind;
     p.t_sym = off;
     if (p.sym_kind != 0) off += kSymBlock;
     p.xaos = !f.xaos.empty();
     p.t_xaos = off;
     if (p.xaos) off += M * (M + 1);
+    p.t_st = off;
+    off += st_rows * M;
+    p.t_init = off;
+    off += p.n_init;
+    for (const SubFlame& S : f.sub) {
+        p.sub_blk.push_back(off);
+        off += 2 + (int)S.xf.size();
+        std::vector<int> rec;
+        for (size_t t = 0; t < S.xf.size() + S.fin.size(); ++t) {
+            rec.push_back(off);
+            off += inner_rec_size(inner_vars(f, inner_xf(S, t)));
+        }
+        p.sub_rec.push_back(rec);
+    }
     p.table_size = off;
 
     std::ostringstream s;
@@ -246,19 +472,34 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     if (p.defer) s << "#define FFB_DEFER 1\n#define FFB_NFD " << nfd << "\n";
     s << "#define FFB_SYM_KIND " << p.sym_kind << "\n#define T_SYM " << p.t_sym << "\n";
     if (p.xaos) s << "#define FFB_XAOS 1\n#define T_XAOS " << p.t_xaos << "\n";
+    s << "#define FFB_NSTATE " << p.n_state << "\n#define FFB_NINIT " << p.n_init << "\n#define T_ST " << p.t_st
+      << "\n#define T_INIT " << p.t_init << "\n";
+    if (p.dc) s << "#define FFB_DC 1\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
     s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw
       << "\n#define T_VP " << p.t_vp << "\n";
     s << kDeviceSrc << "\n";
+    // Subflames, and the step of subflame `id` (an id with no subflame
+    // behind it returns 0 and keeps no state, as an empty subflame does).
+    for (size_t si = 0; si < f.sub.size(); ++si) emit_subflame(s, f, (int)si, p.sub_blk[si], p.sub_rec[si]);
+    s << "template <class S> __device__ __forceinline__ void ffb_subflame(const float* __restrict__ sm, FfbCtx& ctx, S& rng, u32 id, "
+         "float scale, float cs, float sn, float offx, float offy, float* st, float& qx, float& qy, float& qw) {\n    switch (id) {\n";
+    for (size_t si = 0; si < f.sub.size(); ++si)
+        s << "    case " << si << ": ffb_sub_" << si << "(sm, ctx, rng, scale, cs, sn, offx, offy, st, qx, qy, qw); return;\n";
+    s << "    default: (void)sm; (void)ctx; (void)rng; (void)scale; (void)cs; (void)sn; (void)offx; (void)offy; (void)st;\n"
+         "        qx = 0.0f; qy = 0.0f; qw = 0.0f; return;\n    }\n}\n";
     // The normal phase (shader_builder_v2.rs:2714-2795): `result += w * V(p)`
     // from zero, in local order, each gated on its weight.
-    s << "template <class R> __device__ __forceinline__ void ffb_normal(const float* __restrict__ sm, int k, float& x, float& y, R& rng) {\n";
+    s << "template <class R> __device__ __forceinline__ void ffb_normal(const float* __restrict__ sm, int k, float& x, float& y, R& rng, FfbCtx& ctx) {\n";
     emit_phases(s, p.normal, [&](int j) { return normal_site(p, j, "k"); }, "    ", true);
-    s << "    x = rx; y = ry;\n}\n";
+    s << "    x = rx; y = ry; (void)ctx;\n}\n";
+    // Without a walker (the differentiable render, which has no stateful variations).
+    s << "template <class R> __device__ __forceinline__ void ffb_normal(const float* __restrict__ sm, int k, float& x, float& y, R& rng) {\n"
+         "    FfbCtx ctx{nullptr, 0u, 0.0f, 0u, 0u, 0u, 0ull};\n    ffb_normal(sm, k, x, y, rng, ctx);\n}\n";
     // Per-transform form for the sorted schedule, where k is (mostly)
     // warp-uniform: each case evaluates only its transform's variations, in
     // the same local order, straight-line (their chains overlap).
-    s << "template <class R> __device__ __forceinline__ void ffb_normal_k(const float* __restrict__ sm, int k, float& x, float& y, R& rng) {\n";
+    s << "template <class R> __device__ __forceinline__ void ffb_normal_k(const float* __restrict__ sm, int k, float& x, float& y, R& rng, FfbCtx& ctx) {\n";
     if (per_xform) {
         s << "    switch (k) {\n";
         for (size_t k = 0; k < f.xf.size(); ++k) {
@@ -270,27 +511,28 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
             emit_phases(s, used, [&](int u) { return normal_site(p, idx[u], std::to_string(k)); }, "        ", false);
             s << "        x = rx; y = ry;\n        return; }\n";
         }
-        s << "    default: ffb_normal(sm, k, x, y, rng); return;\n    }\n";
+        s << "    default: ffb_normal(sm, k, x, y, rng, ctx); return;\n    }\n";
     } else {
-        s << "    ffb_normal(sm, k, x, y, rng);\n";
+        s << "    ffb_normal(sm, k, x, y, rng, ctx);\n";
     }
     s << "}\n";
     // One final of the chain (main_template.wgsl:679-704): affine,
     // variations, post-affine; `aff` false evaluates the variations alone.
-    s << "template <class R> __device__ __forceinline__ void ffb_final_one(const float* __restrict__ sm, int c, float& x, float& y, R& rng, bool aff) {\n";
+    s << "template <class R> __device__ __forceinline__ void ffb_final_one(const float* __restrict__ sm, int c, float& x, float& y, R& rng, FfbCtx& ctx, bool aff) {\n";
+    s << "    float vcd = 0.0f;   // a final's colour writes are dropped (main_template.wgsl:299-300)\n    (void)vcd; (void)ctx;\n";
     s << "    switch (c) {\n";
     for (size_t c = 0; c < p.fin.size(); ++c) {
         const Plan::Fin& fi = p.fin[c];
         s << "    case " << c << ": {\n        const float* q = sm + " << fi.off << ";\n";
         s << "        if (aff) { float ax = q[0] * x + q[1] * y + q[4]; float ay = q[2] * x + q[3] * y + q[5]; x = ax; y = ay; }\n";
-        emit_phases(s, fi.vars, [&](int j) { return final_site(fi, j); }, "        ", true);
+        emit_phases(s, fi.vars, [&](int j) { return final_site(fi, j); }, "        ", true, "vcd");
         s << "        if (aff && q[12] > 0.5f) { float px = q[6] * rx + q[7] * ry + q[10]; float py = q[8] * rx + q[9] * ry + q[11]; rx = px; ry = py; }\n";
         s << "        x = rx; y = ry;\n        break; }\n";
     }
     s << "    default: break;\n    }\n}\n";
-    s << "template <class R> __device__ __forceinline__ void ffb_finals(const float* __restrict__ sm, float& x, float& y, R& rng) {\n";
-    for (size_t c = 0; c < p.fin.size(); ++c) s << "    ffb_final_one(sm, " << c << ", x, y, rng, true);\n";
-    s << "}\n";
+    s << "template <class R> __device__ __forceinline__ void ffb_finals(const float* __restrict__ sm, float& x, float& y, R& rng, FfbCtx& ctx) {\n";
+    for (size_t c = 0; c < p.fin.size(); ++c) s << "    ffb_final_one(sm, " << c << ", x, y, rng, ctx, true);\n";
+    s << "    (void)ctx;\n}\n";
     if (p.defer) {
         // The final chain's draws in the order it takes them (slot order),
         // for the deferred plot: one plane of `stride` a draw.
@@ -327,12 +569,12 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
     for (size_t k = f.xf.size(); k < (size_t)M; ++k) t[p.t_cum + k] = INFINITY;
     for (size_t k = 0; k < f.xf.size(); ++k) {
         const XForm& x = f.xf[k];
-        const float rec[16] = {x.a, x.b, x.c, x.d, x.e, x.f, x.pa, x.pb, x.pc, x.pd, x.pe, x.pf,
+        const float rec[17] = {x.a, x.b, x.c, x.d, x.e, x.f, x.pa, x.pb, x.pc, x.pd, x.pe, x.pf,
                                x.post ? 1.0f : 0.0f,
                                (1.0f + x.speed) / 2.0f,                 // main_template.wgsl:499-500
                                x.color * (1.0f - x.speed) / 2.0f,
-                               x.opacity};
-        for (int fld = 0; fld < 16; ++fld) t[p.t_xf + fld * M + k] = rec[fld];
+                               x.opacity, x.direct_color};
+        for (int fld = 0; fld < 17; ++fld) t[p.t_xf + fld * M + k] = rec[fld];
         for (size_t j = 0; j < p.normal.size(); ++j) {
             const VarDef* v = p.normal[j];
             t[p.t_vw + j * M + k] = x.var_weight(v);
@@ -372,6 +614,8 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
             row[0] = (size_t)r < n ? cum : 0.0f;
         }
     }
+    int n_state = 0;
+    const std::vector<StEntry> layout = state_layout(f, n_state);
     for (size_t c = 0; c < p.fin.size(); ++c) {
         const Plan::Fin& fi = p.fin[c];
         const XForm& x = f.fin[f.fin_chain[c]];
@@ -383,6 +627,46 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
             float row[kMaxVarSlots];
             x.slot_values(fi.vars[j], row);
             for (int q = 0; q < fi.vars[j]->slots(); ++q) t[fi.off + 13 + nv + fi.prm_off[j] + q] = row[q];
+            t[fi.off + 13 + nv + fi.prm_slots + j] = (float)state_base(layout, 1, 0, f.fin_chain[c], fi.vars[j]);
+        }
+    }
+    // Each stateful normal variation's first state slot per transform.
+    for (size_t j = 0; j < p.normal.size(); ++j) {
+        if (p.st_row[j] < 0) continue;
+        for (int k = 0; k < M; ++k)
+            t[p.t_st + (size_t)p.st_row[j] * M + k] =
+                (size_t)k < f.xf.size() ? (float)state_base(layout, 0, 0, k, p.normal[j]) : -1.0f;
+    }
+    // The state-init list, in layout order (shader_builder_v2.rs:1272-1306).
+    int ni = 0;
+    for (auto& e : layout) if (e.init && ni < p.n_init) t[p.t_init + ni++] = (float)e.base;
+    // Subflames: total weight (at least 1e-6), whether a transform can be
+    // visible, running sums in f32 (subflame.wgsl:333-361); then the inner
+    // transforms' records.
+    for (size_t si = 0; si < f.sub.size() && si < p.sub_blk.size(); ++si) {
+        const SubFlame& S = f.sub[si];
+        float* B = t.data() + p.sub_blk[si];
+        float tot = 0.0f;
+        bool vis = false;
+        for (auto& x : S.xf) { tot += x.weight; vis = vis || (x.weight > 0.0f && x.opacity > 0.0f); }
+        B[0] = std::max(tot, 1e-6f);
+        B[1] = vis ? 1.0f : 0.0f;
+        float cum = 0.0f;
+        for (size_t i = 0; i < S.xf.size(); ++i) { cum += S.xf[i].weight; B[2 + i] = cum; }
+        for (size_t tt = 0; tt < S.xf.size() + S.fin.size(); ++tt) {
+            const XForm& x = inner_xf(S, tt);
+            float* q = t.data() + p.sub_rec[si][tt];
+            const float rec[kSubRec] = {x.a, x.b, x.c, x.d, x.e, x.f, x.pa, x.pb, x.pc, x.pd, x.pe, x.pf, x.post ? 1.0f : 0.0f,
+                                        (1.0f + x.speed) * 0.5f, x.color * (1.0f - x.speed) * 0.5f, x.opacity, x.direct_color};
+            for (int fld = 0; fld < kSubRec; ++fld) q[fld] = rec[fld];
+            int o = kSubRec;
+            for (const VarDef* v : inner_vars(f, x)) {
+                q[o++] = x.var_weight(v);
+                float row[kMaxVarSlots];
+                x.slot_values(v, row);
+                for (int r = 0; r < v->slots(); ++r) q[o++] = row[r];
+                if (v->state > 0) q[o++] = (float)state_base(layout, 2, (int)si, (int)tt, v);
+            }
         }
     }
     return t;

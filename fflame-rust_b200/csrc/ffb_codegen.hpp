@@ -43,6 +43,16 @@ struct Plan {
     int sym_kind = 0, t_sym = 0;           // post-symmetry (compile-time kind; its table block at t_sym)
     bool xaos = false;                     // xaos pick: M rows of (total, running sums) at t_xaos
     int t_xaos = 0;
+    // Per-walker state of stateful variations and subflames (slots per
+    // walker; rows of T_ST: each stateful normal variation's first slot per
+    // transform), the state-init list (T_INIT), and whether the normal phase
+    // has a variation that writes the colour register (the DC colour flow).
+    int n_state = 0, n_init = 0;
+    std::vector<int> st_row;               // per normal variation: its row of T_ST (-1: stateless)
+    int t_st = 0, t_init = 0;
+    bool dc = false;
+    std::vector<int> sub_blk;              // per subflame: its block (total, any visible, running sums)
+    std::vector<std::vector<int>> sub_rec; // per subflame: each inner transform's record
     int rng_mode = RNG_PHILOX;
     int math_mode = MATH_PRECISE;
     int threads = 128;

@@ -31,6 +31,96 @@ void derive_perspective(const float* u, float* o) {            // simple_classic
     o[0] = std::sin(ang);
     o[1] = u[1] * std::cos(ang);
 }
+
+// f32 complex arithmetic in the operation order of shaders/core/complex.wgsl:20-69.
+struct Cx { float x, y; };
+Cx cadd(Cx a, Cx b) { return {a.x + b.x, a.y + b.y}; }
+Cx csub(Cx a, Cx b) { return {a.x - b.x, a.y - b.y}; }
+Cx cmul(Cx a, Cx b) { return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+Cx cmulr(Cx a, float s) { return {a.x * s, a.y * s}; }
+Cx cdiv(Cx a, Cx b) {
+    const float d = b.x * b.x + b.y * b.y;
+    const float sd = d < 1e-30f ? 1e-30f : d;
+    const Cx n = cmul(a, Cx{b.x, -b.y});
+    return {n.x / sd, n.y / sd};
+}
+Cx csq(Cx a) { return {a.x * a.x - a.y * a.y, 2.0f * a.x * a.y}; }
+Cx csqrt(Cx a) {
+    const float mag = std::sqrt(a.x * a.x + a.y * a.y);
+    const float re = std::sqrt(std::fmax(0.5f * (mag + a.x), 0.0f));
+    const float im = std::sqrt(std::fmax(0.5f * (mag - a.x), 0.0f));
+    return {re, a.y >= 0.0f ? im : -im};
+}
+
+// klein_group's generator pair from its recipe (klein_group_misc.rs:82-225):
+// mat_a then mat_b, each four complex entries as (re, im).
+void derive_klein_group(const float* u, float* o) {
+    const Cx zero{0, 0}, re1{1, 0}, re2{2, 0}, re4{4, 0}, im1{0, 1}, im2{0, 2}, im4{0, 4};
+    const int recipe = (int)u[4];
+    Cx a[4] = {re1, zero, zero, re1}, b[4] = {re1, zero, zero, re1};
+    auto maskit_a = [&](Cx mu) {
+        a[0] = cmul(cmulr(mu, -1.0f), im1);
+        a[1] = cmulr(im1, -1.0f);
+        a[2] = cmulr(im1, -1.0f);
+        a[3] = zero;
+    };
+    // The trace-AB root both trace recipes share: (-bb - sqrt(bb^2 - 4 cc)) / 2.
+    auto tr_ab = [&](Cx trA, Cx trB, Cx& tab, Cx& safe) {
+        const Cx bb = cmulr(cmul(trA, trB), -1.0f);
+        const Cx cc = cadd(csq(trA), csq(trB));
+        const Cx disc = csqrt(csub(csq(bb), cmulr(cc, 4.0f)));
+        tab = cmulr(csub(cmulr(bb, -1.0f), disc), 0.5f);
+        safe = {std::fabs(tab.x) + std::fabs(tab.y) < 1e-15f ? 1e-15f : tab.x, tab.y};
+    };
+    if (recipe == 3) {                                   // Riley
+        a[2] = {u[0], u[1]};
+        b[1] = re2;
+    } else if (recipe == 4) {                            // Riley, b1 given
+        a[2] = {u[0], u[1]};
+        b[1] = {u[2], u[3]};
+    } else if (recipe == 1) {                            // Maskit mu
+        maskit_a({u[0], u[1]});
+        b[1] = re2;
+    } else if (recipe == 5) {                            // Maskit mu, b1 given
+        maskit_a({u[0], u[1]});
+        b[1] = {u[2], u[3]};
+    } else if (recipe == 6) {                            // Maskit-Leys: b1 = 2 cos(pi / n) + i b_im
+        maskit_a({u[0], u[1]});
+        const float safe_br = std::fabs(u[2]) < 1e-30f ? 1e-30f : u[2];
+        b[1] = {2.0f * std::cos(3.14159265358979f / safe_br), u[3]};
+    } else if (recipe == 2) {                            // Jorgensen
+        const Cx trA{u[0], u[1]}, trB{u[2], u[3]};
+        Cx tab, s;
+        tr_ab(trA, trB, tab, s);
+        a[0] = csub(trA, cdiv(trB, s)); a[1] = cdiv(trA, csq(s)); a[2] = trA; a[3] = cdiv(trB, s);
+        b[0] = csub(trB, cdiv(trA, s)); b[1] = cmulr(cdiv(trB, csq(s)), -1.0f); b[2] = cmulr(trB, -1.0f); b[3] = cdiv(trA, s);
+    } else {                                             // Grandma's parabolic commutator (0 and any other)
+        const Cx trA{u[0], u[1]}, trB{u[2], u[3]};
+        Cx tab, s;
+        tr_ab(trA, trB, tab, s);
+        const Cx z0 = cdiv(cmul(csub(tab, re2), trB), cadd(csub(cmul(trB, s), cmulr(trA, 2.0f)), cmul(s, im2)));
+        a[0] = cmulr(trA, 0.5f);
+        a[1] = cdiv(cadd(csub(cmul(trA, s), cmulr(trB, 2.0f)), im4), cmul(cadd(cmulr(s, 2.0f), re4), z0));
+        a[2] = cdiv(cmul(csub(csub(cmul(trA, s), cmulr(trB, 2.0f)), im4), z0), csub(cmulr(s, 2.0f), re4));
+        a[3] = cmulr(trA, 0.5f);
+        b[0] = cmulr(csub(trB, im2), 0.5f);
+        b[1] = cmulr(trB, 0.5f);
+        b[2] = cmulr(trB, 0.5f);
+        b[3] = cmulr(cadd(trB, im2), 0.5f);
+    }
+    for (int i = 0; i < 4; ++i) {
+        o[2 * i] = a[i].x; o[2 * i + 1] = a[i].y;
+        o[8 + 2 * i] = b[i].x; o[8 + 2 * i + 1] = b[i].y;
+    }
+}
+
+// subflame_wf's placement rotation (subflame.wgsl:399-408): cos and sin of
+// angle x 0.017453292519943295 in f32, taken once here instead of per call.
+void derive_subflame(const float* u, float* o) {
+    const float ang = u[2] * 0.017453292519943295f;
+    o[0] = std::cos(ang);
+    o[1] = std::sin(ang);
+}
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -95,6 +185,12 @@ static const VarDef kRegistry[] = {
     {"exponential", 341, 0, 0, NP, ND, "v_exponential", 0, 0, nullptr},
     {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
+    {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},
+     "v_klein_group", VF_W, 16, derive_klein_group, 1, 1},
+    {"subflame_wf", 502, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},
+     {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f}, "v_subflame_wf", VF_W | VF_DC | VF_SUB, 2, derive_subflame, 6, 0},
+    {"pre_subflame_wf", 503, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},
+     {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f}, "v_pre_subflame_wf", VF_PRE | VF_DC | VF_SUB, 2, derive_subflame, 6, 0},
     {"linear3D", 533, 0, 0, NP, ND, "v_linear3D", 0, 0, nullptr},
 };
 #undef NP
@@ -160,6 +256,7 @@ XForm parse_transform(const Json& t) {
     } else x.color = 0.5f;
     x.speed = num_field(t, "color_speed", false, 0.0f);       // transforms.rs:1538
     x.opacity = num_field(t, "opacity", false, 1.0f);
+    x.direct_color = num_field(t, "direct_color", false, 0.0f);      // transforms.rs:1533-1540
     x.post = t.bool_or("post_affine_enabled", false);        // transforms.rs:1542
     x.pa = num_field(t, "post_a", false, 1); x.pb = num_field(t, "post_b", false, 0);
     x.pc = num_field(t, "post_c", false, 0); x.pd = num_field(t, "post_d", false, 1);
@@ -332,13 +429,37 @@ Flame parse_config(const Json& cfg) {
         const float rads_per_deg = 3.14159265358979323846f / 180.0f;      // f32::to_radians
         F.sym.rotation = deg * rads_per_deg;
     }
-    // Local variation order (transforms.rs:2297-2319): normals then finals.
+    // Subflames (fractal_config.rs:178-190; gpu/buffers.rs:36-56, 230-253):
+    // each an inner flame's normals and finals (a legacy singular final
+    // joins its finals); their own xaos and subflames are not read.
+    if (const Json* sfs = fl->get("subflames"); sfs && sfs->kind == Json::Array) {
+        if (sfs->arr.size() > 8) fail("more than 8 subflames (MAX_SUBFLAMES)");
+        size_t total = 0;
+        for (auto& sj : sfs->arr) {
+            if (sj->kind != Json::Object) fail("a subflame is not an object");
+            SubFlame S;
+            if (const Json* st = sj->get("transforms"); st && st->kind == Json::Array)
+                for (auto& t : st->arr) S.xf.push_back(parse_transform(*t));
+            if (const Json* ft = sj->get("final_transforms"); ft && ft->kind == Json::Array)
+                for (auto& t : ft->arr) S.fin.push_back(parse_transform(*t));
+            if (const Json* lf = sj->get("final_transform"); lf && lf->kind == Json::Object) S.fin.push_back(parse_transform(*lf));
+            total += S.xf.size() + S.fin.size();
+            F.sub.push_back(std::move(S));
+        }
+        if (total > 256) fail("TooLarge: the subflames have " + std::to_string(total) + " transforms; the renderer holds 256");
+    }
+    // Local variation order (transforms.rs:2297-2319): normals then finals,
+    // then each subflame's.
     auto absorb = [&](const XForm& x) {
         for (auto& p : x.vars)
             if (std::find(F.local.begin(), F.local.end(), p.first) == F.local.end()) F.local.push_back(p.first);
     };
     for (auto& x : F.xf) absorb(x);
     for (auto& x : F.fin) absorb(x);
+    for (auto& S : F.sub) {
+        for (auto& x : S.xf) absorb(x);
+        for (auto& x : S.fin) absorb(x);
+    }
     // View.
     F.zoom = num_field(cfg, "zoom", false, 1.0f);
     if (const Json* v = cfg.get("pan_x"); v && v->kind == Json::Number) F.pan_x = v->num;

@@ -21,8 +21,8 @@ namespace ffb {
 
 // A variation's packed parameter row: its user parameters, then the values
 // its `wgsl_init` derives from them (VariationDef::slot_count,
-// src/variations/definition.rs:452-454).
-constexpr int kMaxVarSlots = 6;
+// src/variations/definition.rs:452-454).  klein_group's 6 + 16 is the widest.
+constexpr int kMaxVarSlots = 24;
 
 enum VarFlags {
     VF_XF = 1,        // Feature::NeedsTransform reading the affine: the body takes its transform's a..f
@@ -30,6 +30,8 @@ enum VarFlags {
     VF_PRE = 4,       // VariationPhase::Pre: temp = V(temp), before the weighted sum
     VF_POST = 8,      // VariationPhase::Post: result = V(result), after it
     VF_JAC = 16,      // has a Jacobian (dj_*) for the differentiable render
+    VF_DC = 32,       // Feature::WritesColor: may write the iteration's colour register (vc)
+    VF_SUB = 64,      // steps a subflame (subflame_wf, pre_subflame_wf): generated, not a plain body
 };
 
 struct VarDef {
@@ -44,6 +46,11 @@ struct VarDef {
     int nderived;      // init_param_count
     // The variation's `wgsl_init` restated on the host in f32: user -> derived.
     void (*derive)(const float* user, float* out);
+    // Per-walker state a call carries to the next (state_count,
+    // definition.rs; the 2-D slots this build keeps), and the draws its
+    // `wgsl_state_init` takes at every dispatch start (klein_group's one).
+    int state = 0;
+    int init_draws = 0;
     int slots() const { return nparams + nderived; }
     bool needs_rng() const { return draws > 0; }
 };
@@ -56,6 +63,10 @@ struct XForm {
     float pa = 1, pb = 0, pc = 0, pd = 1, pe = 0, pf = 0;
     bool post = false;
     float weight = 1, color = 0.5f, speed = 0, opacity = 1;
+    // Step 3 of the colour flow when a variation writes the colour register
+    // (main_template.wgsl:294-306, 486-490); a `.fflame` without the field
+    // reads 0 (transforms.rs:1533-1540).
+    float direct_color = 0;
     // (variation, weight) in the transform's dispatch order.
     std::vector<std::pair<const VarDef*, float>> vars;
     // "name.param" -> value
@@ -108,11 +119,19 @@ struct SpatialFilter {
     bool on() const { return radius > 0.0f; }
 };
 
+// A subflame (FractalConfig.subflames, gpu/buffers.rs:160-200): an inner
+// flame that subflame_wf steps one visible iteration at a time, its normals
+// picked by weight (no xaos) and its finals applied to the output.
+struct SubFlame {
+    std::vector<XForm> xf, fin;
+};
+
 struct Flame {
     std::vector<XForm> xf;              // normal transforms
     std::vector<XForm> fin;             // final transforms pool
     std::vector<int> fin_chain;         // the final chain every normal runs
-    std::vector<const VarDef*> local;   // local variation order
+    std::vector<const VarDef*> local;   // local variation order (parent, then subflames)
+    std::vector<SubFlame> sub;          // at most 8 (MAX_SUBFLAMES, buffers.rs:36-44)
     SpatialFilter filter;
     // Xaos (utilities.wgsl:106-137): row-major n_xf x n_xf transition
     // weights, empty when every weight is 1 (Flame::has_xaos, xaos.rs:29-40).

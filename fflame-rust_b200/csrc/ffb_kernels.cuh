@@ -17,7 +17,40 @@ struct ffb_launch {
     float zoom, pan_x, pan_y, cos_r, sin_r;
     float4* rec;               // deferred plotting: n_iters x n_walkers samples (x, y, ci, flags)
     float* rec_draws;          // and their final chain's draws, FFB_NFD planes of the same length
+    float* state;              // FFB_NSTATE planes of n_walkers: the walkers' variation state (slot-major)
 };
+
+// The walker context of walker gw at iteration it.
+__device__ __forceinline__ FfbCtx ffb_ctx(const ffb_launch& J, u32 gw, u64 it) {
+    FfbCtx c;
+    c.st = J.state + (gw - J.walker0);
+    c.stride = J.n_walkers;
+    c.vc = 0.0f;
+    c.k0 = J.seed_lo; c.k1 = J.seed_hi; c.gw = gw; c.it = it;
+    return c;
+}
+
+#if FFB_NSTATE > 0
+// A starting walker's variation state: zero (var<private> thread_state,
+// main_template.wgsl:117-122), then each `wgsl_state_init` that draws --
+// klein_group's previous generator, floor(r * 4) (klein_group_misc.rs:227-231).
+// With the reference's stream the draw is taken at every dispatch start
+// (ffb_pcg_dispatch); with the counter-based stream it is Philox counter
+// (walker, 0xFFFFFFFE, entry / 4, 0xFFFFFFFF), once.
+__device__ __forceinline__ void ffb_state_fresh(const float* __restrict__ sm, const ffb_launch& J, u32 gw) {
+    float* st = J.state + (gw - J.walker0);
+    for (int s = 0; s < FFB_NSTATE; ++s) st[(size_t)s * J.n_walkers] = 0.0f;
+#if FFB_RNG_MODE == 1
+    for (int i = 0; i < FFB_NINIT; ++i) {
+        const uint4 o = philox4(J.seed_lo, J.seed_hi, gw, 0xFFFFFFFEu, (u32)(i >> 2), 0xFFFFFFFFu);
+        const u32 wd = (i & 3) == 0 ? o.x : (i & 3) == 1 ? o.y : (i & 3) == 2 ? o.z : o.w;
+        st[(size_t)ffb_u32(sm[T_INIT + i]) * J.n_walkers] = floorf(u24(wd) * 4.0f);
+    }
+#else
+    (void)sm;
+#endif
+}
+#endif
 
 __device__ __forceinline__ int ffb_select(const float* __restrict__ sm, int n_xf, float u) {
     // utilities.wgsl:35-54: first i with u*total <= cumsum_i (f32, left to right).
@@ -195,6 +228,9 @@ __device__ __forceinline__ void ffb_start(const float* __restrict__ sm, const ff
     if (J.it0 == 0) {
         ci = 0.0f;
         fuse = J.burn_in;
+#if FFB_NSTATE > 0
+        ffb_state_fresh(sm, J, gw);
+#endif
 #ifdef FFB_XAOS
         prev = ffb_xaos_first(sm, (int)J.n_xf, gw, J.seed_lo);
 #endif
@@ -225,6 +261,14 @@ __device__ __forceinline__ void ffb_pcg_dispatch(const ffb_launch& J, PcgRng& rn
         rng.init(gw, J.seed_lo + d * 2654435761u);
         float s0 = rng.draw(0), s1 = rng.draw(0);
         if (it == 0) { x = s0 * 2.0f - 1.0f; y = s1 * 2.0f - 1.0f; }
+#if FFB_NINIT > 0
+        // The state-init block (main_template.wgsl:117-122) draws every
+        // dispatch; a resumed orbit then restores its state over it.
+        for (int i = 0; i < FFB_NINIT; ++i) {
+            const float r = rng.draw(0);
+            if (it == 0) J.state[(size_t)ffb_u32(J.table[T_INIT + i]) * J.n_walkers + (gw - J.walker0)] = floorf(r * 4.0f);
+        }
+#endif
     }
 }
 #endif
@@ -267,10 +311,10 @@ __device__ __forceinline__ void ffb_sym_copy(const float* __restrict__ sm, int k
 // copies, world_to_pixel and the splat (main_template.wgsl:663-1320).
 template <class R>
 __device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
-                                                float x, float y, float ci, bool plot, R& rng, float cx, float cy, float scale,
-                                                u32& inframe) {
+                                                float x, float y, float ci, bool plot, R& rng, FfbCtx& ctx, float cx, float cy,
+                                                float scale, u32& inframe) {
     float fx = x, fy = y;
-    ffb_finals(sm, fx, fy, rng);                                            // main_template.wgsl:663-717
+    ffb_finals(sm, fx, fy, rng, ctx);                                       // main_template.wgsl:663-717
     const int pal_idx = ffb_palette_index(ci, J.pal_n);
     const float4 c = pal[pal_idx];                                          // main_template.wgsl:766-772
 #if FFB_SYM_KIND != 0
@@ -336,10 +380,17 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
                                          int k, bool plot, R& rng, u32 gw, u64 it, float& x, float& y, float& ci, u32& fuse,
                                          float cx, float cy, float scale, u32& inframe) {
     const float* q = sm + T_XF + k;
+    FfbCtx ctx = ffb_ctx(J, gw, it);
+#ifdef FFB_DC
+    // Step 1 of the colour flow with a colour-writing variation
+    // (main_template.wgsl:294-306): c_base, the register vc starting there.
+    const float cb = ci * q[F_C1 * FFB_MAXX] + q[F_C2 * FFB_MAXX];
+    ctx.vc = cb;
+#endif
     float ax = q[F_A * FFB_MAXX] * x + q[F_B * FFB_MAXX] * y + q[F_E * FFB_MAXX];
     float ay = q[F_C * FFB_MAXX] * x + q[F_D * FFB_MAXX] * y + q[F_F * FFB_MAXX];
-    if (PER_XFORM) ffb_normal_k(sm, k, ax, ay, rng);                        // main_template.wgsl:366-376
-    else ffb_normal(sm, k, ax, ay, rng);
+    if (PER_XFORM) ffb_normal_k(sm, k, ax, ay, rng, ctx);                   // main_template.wgsl:366-376
+    else ffb_normal(sm, k, ax, ay, rng, ctx);
 #if FFB_HAS_POST
     if (q[F_POST * FFB_MAXX] > 0.5f) {                                      // main_template.wgsl:380-384
         float px = q[F_PA * FFB_MAXX] * ax + q[F_PB * FFB_MAXX] * ay + q[F_PE * FFB_MAXX];
@@ -361,12 +412,16 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
         return;
     }
     x = ax; y = ay;
+#ifdef FFB_DC
+    ci = cb + q[F_DC * FFB_MAXX] * (ctx.vc - cb);                          // main_template.wgsl:486-490
+#else
     ci = ci * q[F_C1 * FFB_MAXX] + q[F_C2 * FFB_MAXX];                       // main_template.wgsl:496-508
+#endif
     if (fuse > 0u) { fuse -= 1u; FFB_DEFER_SKIP(J, gw, it); return; }     // main_template.wgsl:510-514
 #ifdef FFB_DEFER
     ffb_defer_store(J, gw, it, x, y, ci, plot, rng);
 #else
-    ffb_plot_sample(sm, pal, J, x, y, ci, plot, rng, cx, cy, scale, inframe);
+    ffb_plot_sample(sm, pal, J, x, y, ci, plot, rng, ctx, cx, cy, scale, inframe);
 #endif
 }
 
@@ -548,8 +603,12 @@ extern "C" __global__ void ffb_probe(const float* __restrict__ table, int n_xf, 
     if (fabsf(y) < 1.17549435e-38f) y = copysignf(0.0f, y);
     PcgRng rng;
     rng.init((u32)slot, 0x9E3779B9u);
-    if (xi < n_xf) ffb_normal(table, xi, x, y, rng);
-    else ffb_final_one(table, xi - n_xf, x, y, rng, false);
+    // State as a probe thread starts it (zero) and vc = 0.5 (main_template.wgsl:1510-1512).
+    float st[FFB_NSTATE > 0 ? FFB_NSTATE : 1];
+    for (int s = 0; s < (FFB_NSTATE > 0 ? FFB_NSTATE : 1); ++s) st[s] = 0.0f;
+    FfbCtx ctx{st, 1u, 0.5f, 0u, 0u, (u32)slot, 0ull};
+    if (xi < n_xf) ffb_normal(table, xi, x, y, rng, ctx);
+    else ffb_final_one(table, xi - n_xf, x, y, rng, ctx, false);
     out[slot] = make_float2(x, y);
 }
 
@@ -562,6 +621,9 @@ extern "C" __global__ void ffb_apply_points(const float* __restrict__ table, int
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     ArrayRng rng{words + (size_t)i * FFB_APPLY_WORDS};
+    float st[FFB_NSTATE > 0 ? FFB_NSTATE : 1];
+    for (int s = 0; s < (FFB_NSTATE > 0 ? FFB_NSTATE : 1); ++s) st[s] = 0.0f;
+    FfbCtx ctx{st, 1u, 0.5f, 0u, 0u, (u32)i, 0ull};
     float x = xs[i], y = ys[i];
     if (xi < n_xf) {
         const float* q = table + T_XF + xi;
@@ -570,14 +632,14 @@ extern "C" __global__ void ffb_apply_points(const float* __restrict__ table, int
             float ay = q[F_C * FFB_MAXX] * x + q[F_D * FFB_MAXX] * y + q[F_F * FFB_MAXX];
             x = ax; y = ay;
         }
-        ffb_normal(table, xi, x, y, rng);
+        ffb_normal(table, xi, x, y, rng, ctx);
         if (with_affine && q[F_POST * FFB_MAXX] > 0.5f) {
             float px = q[F_PA * FFB_MAXX] * x + q[F_PB * FFB_MAXX] * y + q[F_PE * FFB_MAXX];
             float py = q[F_PC * FFB_MAXX] * x + q[F_PD * FFB_MAXX] * y + q[F_PF * FFB_MAXX];
             x = px; y = py;
         }
     } else {
-        ffb_final_one(table, xi - n_xf, x, y, rng, with_affine != 0);
+        ffb_final_one(table, xi - n_xf, x, y, rng, ctx, with_affine != 0);
     }
     xo[i] = x; yo[i] = y;
 }
@@ -603,7 +665,8 @@ extern "C" __global__ void __launch_bounds__(384) ffb_plot(const ffb_launch* __r
 #pragma unroll
         for (int m = 0; m < FFB_NFD; ++m) fd[m] = J.rec_draws[(u64)m * n + i];
         SeqRng rng{fd, 0};
-        ffb_plot_sample(sm, pal, J, r.x, r.y, r.z, (fl & 1u) != 0u, rng, cx, cy, scale, inframe);
+        FfbCtx ctx{nullptr, 0u, 0.0f, 0u, 0u, 0u, 0ull};                // deferred finals carry no state
+        ffb_plot_sample(sm, pal, J, r.x, r.y, r.z, (fl & 1u) != 0u, rng, ctx, cx, cy, scale, inframe);
     }
     ffb_count_inframe(J, inframe);
 }

@@ -92,8 +92,9 @@ struct Launch {
     float zoom, pan_x, pan_y, cos_r, sin_r;
     void* rec;          // deferred plotting: the launch's samples
     void* rec_draws;    // and their final chain's draws
+    void* state;        // the walkers' variation state (slot-major planes of n_walkers)
 };
-static_assert(sizeof(Launch) == 136, "launch record layout");
+static_assert(sizeof(Launch) == 144, "launch record layout");
 
 struct DevBuf {
     void* p = nullptr;
@@ -144,6 +145,7 @@ struct ffb_renderer {
     DevBuf hist, walkers, table, palette, counters, jobs, rgba, de_out, de_tab, lut, f_out, tmp_in;
     DevBuf tile_rec, tile_tmp, tile_sorted, tile_meta;      // tile-sorted accumulation scratch
     DevBuf filt_batch, filt_tmp;                            // spatial filter: a batch's histogram, the row pass
+    DevBuf vstate;                                          // stateful variations / subflames: per-walker state
     // Deferred plotting: the plot kernel's stream, double-buffered sample
     // records, events ordering the two streams.
     cudaStream_t plot_stream = nullptr;
@@ -176,7 +178,7 @@ struct ffb_renderer {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& m : cache) if (m.lib) cudaLibraryUnload(m.lib);
         for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in,
-                          &tile_rec, &tile_tmp, &tile_sorted, &tile_meta, &filt_batch, &filt_tmp, &rec[0], &rec[1],
+                          &tile_rec, &tile_tmp, &tile_sorted, &tile_meta, &filt_batch, &filt_tmp, &vstate, &rec[0], &rec[1],
                           &rec_draws[0], &rec_draws[1]}) b->release();
         if (plot_stream) {
             cudaStreamSynchronize(plot_stream);
@@ -490,6 +492,9 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     Launch L{};
     L.table = d_table; L.palette = d_pal; L.hist = filt ? batch : hist; L.walkers = d_walk; L.counters = d_cnt;
     L.n_walkers = P.walkers; L.walker0 = walker0; L.block0 = 0; L.n_xf = (uint32_t)P.flame.xf.size();
+    // Stateful variations and subflames: their slots of every walker (set
+    // by the first launch, carried between launches like the walkers).
+    L.state = P.plan.n_state > 0 ? r->vstate.ensure((size_t)P.walkers * (size_t)P.plan.n_state * 4) : nullptr;
     L.seed_lo = (uint32_t)P.seed; L.seed_hi = (uint32_t)(P.seed >> 32); L.burn_in = P.burn_in; L.ipt = P.ipt;
     L.pal_n = pal_n; L.width = (int32_t)P.wi; L.height = (int32_t)P.hi;
     L.zoom = P.flame.zoom; L.pan_x = (float)P.flame.pan_x; L.pan_y = (float)P.flame.pan_y;
@@ -1466,6 +1471,9 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
             B->flames[i].P = prepare(items[i].config, items[i].config_len, &j);
             if (!B->flames[i].P.flame.xaos.empty())
                 fail(FFB_ERR_INVALID, "item " + std::to_string(i) + ": xaos flames are not batched; render it alone");
+            if (B->flames[i].P.plan.n_state > 0)
+                fail(FFB_ERR_INVALID, "item " + std::to_string(i) + ": flames with stateful variations or subflames are not "
+                                      "batched; render it alone");
             if (B->flames[i].P.flame.filter.on())
                 fail(FFB_ERR_INVALID, "item " + std::to_string(i) + ": the spatial filter (filter_radius) is not batched; render it alone");
             check_de(B->flames[i].P.flame, B->flames[i].P.ss);

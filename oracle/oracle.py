@@ -31,7 +31,8 @@ REGISTRY = {
     "wedge": 66, "juliascope": 69, "radial_blur": 73, "tangent": 141, "secant2": 143,
     "cosine": 144, "pie": 150, "butterfly": 152, "popcorn": 181, "fan": 190, "fisheye": 191,
     "split": 248, "stripes": 250, "bent2": 281, "power": 325, "exponential": 341,
-    "perspective": 345, "rings": 379, "linear3D": 533,
+    "perspective": 345, "rings": 379, "klein_group": 501, "subflame_wf": 502, "pre_subflame_wf": 503,
+    "linear3D": 533,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -54,11 +55,15 @@ PARAMS = {
     "stripes": [("space", 0.2), ("warp", 0.6)],
     "bent2": [("x", 1.0), ("y", 1.0)],
     "perspective": [("angle", 0.62), ("dist", 2.2)],
+    "klein_group": [("a_re", 2.0), ("a_im", 0.0), ("b_re", 2.0), ("b_im", 0.0), ("recipe", 0.0), ("avoid_reversal", 1.0)],
+    "subflame_wf": [("subflame_id", 0.0), ("scale", 1.0), ("angle", 0.0), ("offset_x", 0.0), ("offset_y", 0.0),
+                    ("offset_z", 0.0), ("colorscale_z", 0.0), ("color_mode", -1.0)],
 }
-SLOTS = 6          # packed parameter row a variation (user + derived)
+PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
+SLOTS = 24         # packed parameter row a variation (user + derived)
 WORDS = 64         # draw words an iteration
 
-XF_STRIDE = 17
+XF_STRIDE = 18
 
 
 def var_meta(name):
@@ -123,6 +128,9 @@ class OFlame(ctypes.Structure):
         ("sym_cx", ctypes.c_float), ("sym_cy", ctypes.c_float), ("sym_distance", ctypes.c_float),
         ("sym_rotation", ctypes.c_float),
         ("xaos", ctypes.POINTER(ctypes.c_float)),
+        ("n_sub", ctypes.c_int),
+        ("sub_nxf", ctypes.POINTER(ctypes.c_int)),
+        ("sub_nfin", ctypes.POINTER(ctypes.c_int)),
     ]
 
 
@@ -174,10 +182,18 @@ def finals_of(flame):
     return fins
 
 
+def subflame_transforms(flame):
+    """Each subflame's (normals, finals) (gpu/buffers.rs:230-253)."""
+    return [(list(sf.get("transforms", [])), finals_of(sf)) for sf in flame.get("subflames", [])]
+
+
 def local_order(flame):
-    """transforms.rs:2297-2319: normals then finals, first appearance wins."""
+    """transforms.rs:2297-2319: normals then finals, then each subflame's; first appearance wins."""
     out = []
-    for t in list(flame["transforms"]) + finals_of(flame):
+    allx = list(flame["transforms"]) + finals_of(flame)
+    for nx, fx in subflame_transforms(flame):
+        allx += nx + fx
+    for t in allx:
         for n in ordered_variation_names(t):
             if n not in out:
                 out.append(n)
@@ -220,7 +236,10 @@ class Flame:
         self.names = local_order(flame)
         normals = flame["transforms"]
         fins = finals_of(flame)
+        subs = subflame_transforms(flame)
         allx = list(normals) + fins
+        for nx, fx in subs:
+            allx += nx + fx
         nv = len(self.names)
         self.var_id = np.array([REGISTRY[n] for n in self.names], np.int32)
         self.xf = np.zeros(len(allx) * XF_STRIDE, np.float32)
@@ -232,7 +251,7 @@ class Flame:
                    t.get("post_a", 1.0), t.get("post_b", 0.0), t.get("post_c", 0.0),
                    t.get("post_d", 1.0), t.get("post_e", 0.0), t.get("post_f", 0.0),
                    1.0 if post else 0.0, t.get("weight", 1.0), t.get("color", 0.5),
-                   t.get("color_speed", 0.0), t.get("opacity", 1.0)]
+                   t.get("color_speed", 0.0), t.get("opacity", 1.0), t.get("direct_color", 0.0)]
             self.xf[i * XF_STRIDE:(i + 1) * XF_STRIDE] = rec
             for v, n in enumerate(self.names):
                 self.var_w[i * nv + v] = t["variations"].get(n, 0.0)
@@ -249,6 +268,11 @@ class Flame:
         s.cos_r, s.sin_r = math.cos(rot), math.sin(rot)
         s.width, s.height = width, height
         s.palette, s.pal_n = _fp(self.palette), len(self.palette) // 3
+        self.sub_nxf = np.array([len(nx) for nx, _ in subs] or [0], np.int32)
+        self.sub_nfin = np.array([len(fx) for _, fx in subs] or [0], np.int32)
+        s.n_sub = len(subs)
+        s.sub_nxf = self.sub_nxf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        s.sub_nfin = self.sub_nfin.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         # Xaos (xaos.rs:29-40, 128-135): read when some weight differs from 1; missing entries are 1.
         self.xaos = None
         if flame.get("xaos"):

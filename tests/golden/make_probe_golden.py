@@ -12,8 +12,8 @@ the glyphs.  It follows src/probe/batch.rs:94-139: every shipped variation
 in registration order (ALL_VARIATIONS, src/variations/defs/mod.rs:446),
 first-fit into batches of at most 99 variations and 1600 packed parameter
 slots (user parameters + init_param_count, definition.rs:452-454).  A
-definition whose parameter list is not a literal list counts 0 slots here;
-the first such sits after every variation this build carries.
+parameter list given as another definition's (`X.parameters`) counts as
+that one's.
 
 Run where the reference tree is mounted; the output,
 tests/golden/variation_probe_2d.txt, is committed.
@@ -40,16 +40,21 @@ def probe_slots(ref):
     mod = open(os.path.join(defs, "mod.rs"), encoding="utf-8").read()
     i = mod.index("pub static ALL_VARIATIONS")
     order = re.findall(r"&(\w+),", mod[i:mod.index("];", i)])
-    info = {}
+    info, nparams, alias = {}, {}, {}
     for p in glob.glob(os.path.join(defs, "*.rs")):
         src = open(p, encoding="utf-8").read()
         for m in re.finditer(r"pub static (\w+): VariationDef = VariationDef \{(.*?)\n\};", src, re.S):
             body = m.group(2)
             name = re.search(r'name: "([^"]+)"', body).group(1)
             plist = re.search(r"parameters: &\[(.*?)\n    \],", body, re.S)
-            n = len(re.findall(r"ParamDef::new\(|param!\(", plist.group(1))) if plist else 0
+            nparams[m.group(1)] = len(re.findall(r"ParamDef::new\(|param!\(", plist.group(1))) if plist else 0
+            other = re.search(r"parameters: (\w+)\.parameters,", body)
+            if other:
+                alias[m.group(1)] = other.group(1)
             ic = re.search(r"init_param_count: (\d+)", body)
-            info[m.group(1)] = (name, n + (int(ic.group(1)) if ic else 0))
+            info[m.group(1)] = (name, int(ic.group(1)) if ic else 0)
+    for st, (name, ic) in list(info.items()):
+        info[st] = (name, nparams[alias.get(st, st)] + ic)
     slot, count, used = {}, 0, 0
     for st in order:
         name, s = info[st]

@@ -77,7 +77,8 @@ FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "pola
 # Bit for bit with the report (classes and the digest of the quantised values).
 EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bubble", "curl", "handkerchief", "spiral",
                        "hyperbolic", "bent", "eyefish", "noise", "blur", "cross", "rings2", "pdj", "rectangles", "splits",
-                       "pre_blur", "secant2", "pie", "butterfly", "fan", "fisheye", "stripes", "bent2", "rings", "linear3D"])
+                       "pre_blur", "secant2", "pie", "butterfly", "fan", "fisheye", "stripes", "bent2", "rings", "linear3D",
+                       "klein_group", "subflame_wf", "pre_subflame_wf"])
 
 
 def golden():
