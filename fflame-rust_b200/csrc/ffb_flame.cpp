@@ -518,7 +518,6 @@ Flame parse_config(const Json& cfg) {
     static const char* const kHigh[] = {"clip", "Clip", "max_norm", "MaxNorm", "reinhard", "Reinhard", "filmic", "Filmic", "agx", "AgX", "agx_punchy", "AgXPunchy"};
     if (const Json* m = cfg.get("tonemap_mode"); m && m->kind == Json::String) tm.mode = mode_code(m->str, kModes, 3, "tone map mode");
     if (const Json* m = cfg.get("highlight_mode"); m && m->kind == Json::String) tm.highlight = mode_code(m->str, kHigh, 6, "highlight mode");
-    if (tm.highlight >= 4) fail("the AgX highlight modes are not supported by this build");
     tm.exposure = num_field(cfg, "exposure", false, 1.0f);
     tm.gamma = num_field(cfg, "gamma", false, 4.0f);
     tm.gamma_threshold = num_field(cfg, "gamma_threshold", false, 5.0f);

@@ -61,6 +61,33 @@ __device__ __forceinline__ double smooth(double e0, double e1, double x) {
     return t * t * (3.0 - 2.0 * t);
 }
 
+// AgX (Troy Sobotka's view transform, Benjamin Wrensch's minimal fit;
+// tonemap.wgsl:444-477): into AgX's inset gamut, log2 encoded over
+// [-12.47393, 4.026069] stops, the fit's sixth-order sigmoid, for the Punchy
+// look a power of 1.35 and saturation 1.4 about Rec.709 luma, then the outset
+// gamut, clamped, decoded by a power of 2.2.
+__device__ D3 agx(D3 c, bool punchy) {
+    D3 v{0.842479062253094 * c.x + 0.0784335999999992 * c.y + 0.0792237451477643 * c.z,
+         0.0423282422610123 * c.x + 0.878468636469772 * c.y + 0.0791661274605434 * c.z,
+         0.0423756549057051 * c.x + 0.0784336 * c.y + 0.879142973793104 * c.z};
+    const double lo = -12.47393, hi = 4.026069;
+    auto enc = [&](double x) {
+        const double t = (clampd(log2(fmax(x, 1.0e-10)), lo, hi) - lo) / (hi - lo);
+        const double t2 = t * t, t4 = t2 * t2;
+        return 15.5 * t4 * t2 - 40.14 * t4 * t + 31.96 * t4 - 6.868 * t2 * t + 0.4298 * t2 + 0.1191 * t - 0.00232;
+    };
+    v = {enc(v.x), enc(v.y), enc(v.z)};
+    if (punchy) {
+        v = {pow(fmax(v.x, 0.0), 1.35), pow(fmax(v.y, 0.0), 1.35), pow(fmax(v.z, 0.0), 1.35)};
+        const double l = 0.2126 * v.x + 0.7152 * v.y + 0.0722 * v.z;
+        v = {l + 1.4 * (v.x - l), l + 1.4 * (v.y - l), l + 1.4 * (v.z - l)};
+    }
+    const D3 o{1.19687900512017 * v.x - 0.0980208811401368 * v.y - 0.0990297440797205 * v.z,
+               -0.0528968517574562 * v.x + 1.15190312990417 * v.y - 0.0989611768448433 * v.z,
+               -0.0529716355144438 * v.x - 0.0980434501171241 * v.y + 1.15107367264116 * v.z};
+    return {pow(clampd(o.x, 0.0, 1.0), 2.2), pow(clampd(o.y, 0.0, 1.0), 2.2), pow(clampd(o.z, 0.0, 1.0), 2.2)};
+}
+
 // One pixel of the tone map: cnt = hits, sum = colour sums.  Returns the
 // RGBA before quantisation.  Computed in FP64: the pass is bound by HBM
 // (16 bytes in, 4 out a pixel), so the double arithmetic is free, and the
@@ -117,6 +144,8 @@ __device__ D3 tonemap_rgb(const TonemapArgs& A, const float* lut, double cnt, D3
     } else if (A.highlight == 3) {
         auto aces = [](double x) { return clampd((x * (2.51 * x + 0.03)) / (x * (2.43 * x + 0.59) + 0.14), 0.0, 1.0); };
         color = {aces(color.x), aces(color.y), aces(color.z)};
+    } else if (A.highlight == 4 || A.highlight == 5) {
+        color = agx(color, A.highlight == 5);
     } else {
         color = {fmin(color.x, 1.0), fmin(color.y, 1.0), fmin(color.z, 1.0)};
     }

@@ -492,7 +492,8 @@ def tonemap_params_for(cfg, w, h, sd, transparent=0):
     f = lambda key, d: float(np.float32(cfg.get(key, d)))
     tm = TonemapParams()
     modes = {"linear": 0, "Linear": 0, "logarithmic": 1, "Logarithmic": 1, "density": 2, "DensityVisualization": 2}
-    highs = {"clip": 0, "max_norm": 1, "reinhard": 2, "filmic": 3}
+    highs = {"clip": 0, "Clip": 0, "max_norm": 1, "MaxNorm": 1, "reinhard": 2, "Reinhard": 2, "filmic": 3, "Filmic": 3,
+             "agx": 4, "AgX": 4, "agx_punchy": 5, "AgXPunchy": 5}
     tm.mode = modes[cfg.get("tonemap_mode", "logarithmic")]
     tm.highlight_mode = highs[cfg.get("highlight_mode", "clip")]
     tm.exposure = f("exposure", 1.0)
@@ -538,6 +539,15 @@ def tonemap(params, cnt, rgb):
                      rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.c_int(n),
                      of.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ou.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
     return of.reshape(n, 4), ou.reshape(n, 4)
+
+
+def agx_display(rgb, punchy=False):
+    """AgX as the tone map's highlight modes 4 / 5 apply it, display-referred."""
+    a = np.ascontiguousarray(rgb, np.float64)
+    out = np.zeros(3, np.float64)
+    P = ctypes.POINTER(ctypes.c_double)
+    lib().of_agx_display(a.ctypes.data_as(P), ctypes.c_int(1 if punchy else 0), out.ctypes.data_as(P))
+    return out
 
 
 def downsample_firefly(rgba, ow, oh):

@@ -244,6 +244,8 @@ TONEMAP_VARIANTS = [
     {"highlight_mode": "filmic", "background_color": [0.2, 0.1, 0.05]},
     {"tonemap_mode": "linear", "gamma": 2.0},
     {"tonemap_mode": "density", "exposure": 0.5},
+    {"highlight_mode": "agx", "exposure": 2.0},
+    {"highlight_mode": "agx_punchy", "saturation": 1.2},
 ]
 
 

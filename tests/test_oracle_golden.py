@@ -229,6 +229,30 @@ def test_point_render_lights_one_pixel(oracle):
             assert cnt[32, 0] == inframe == plotted
 
 
+def test_agx_shape_of_the_reference(oracle):
+    """The AgX highlight modes' curve against the reference's own checks of
+    it (scene/tonemap.rs:370-397): rising, greys grey, black black, scene
+    middle grey 0.18 to 0.35-0.55 display, white from 16, a bright colour's
+    channels kept in order; the Punchy look darker below the middle, more
+    saturated, greys still grey."""
+    grey = lambda x, p=False: oracle.agx_display([x, x, x], p)
+    last = -1.0
+    for i in range(200):
+        x = 1.0e-4 * 1.08 ** i
+        g = grey(x)
+        assert abs(g[0] - g[1]) < 2e-3 and abs(g[1] - g[2]) < 2e-3, (x, g)
+        assert g[0] >= last - 1e-6, x
+        last = g[0]
+    assert grey(0.0)[0] < 0.01
+    assert 0.35 <= grey(0.18)[0] <= 0.55
+    assert grey(16.0)[0] > 0.97
+    o = oracle.agx_display([8.0, 4.0, 0.5])
+    assert o[0] > o[1] > o[2]
+    assert grey(0.05, True)[0] < grey(0.05)[0] and abs(grey(0.05, True)[0] - grey(0.05, True)[2]) < 2e-3
+    o, p = oracle.agx_display([1.0, 0.3, 0.1]), oracle.agx_display([1.0, 0.3, 0.1], True)
+    assert p[0] - p[2] > o[0] - o[2]
+
+
 def test_firefly_downsample_known_answers(oracle):
     """supersample.rs:132-167: a uniform quad passes; a lone bright sample
     over a dark quad is clamped to 4x the median luminance plus 64."""
