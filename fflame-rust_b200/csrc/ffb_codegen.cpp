@@ -58,7 +58,7 @@ struct Site {
 // `init` marks the entries whose `wgsl_state_init` runs each dispatch (the
 // reference's layout holds weights above 1e-6 in magnitude).
 struct StEntry {
-    int kind;               // 0 normal, 1 final (pool index), 2 subflame s, transform t (normals then finals)
+    int kind;               // 0 normal, 3 linked, 1 final (pool indices), 2 subflame s, transform t (normals then finals)
     int s, t;
     const VarDef* v;
     int base;
@@ -80,6 +80,7 @@ std::vector<StEntry> state_layout(const Flame& f, int& total) {
         }
     };
     for (size_t k = 0; k < f.xf.size(); ++k) emit(0, 0, (int)k, f.xf[k]);
+    for (size_t c = 0; c < f.lnk.size(); ++c) emit(3, 0, (int)c, f.lnk[c]);
     for (size_t c = 0; c < f.fin.size(); ++c) emit(1, 0, (int)c, f.fin[c]);
     for (size_t si = 0; si < f.sub.size(); ++si) {
         const SubFlame& S = f.sub[si];
@@ -360,7 +361,8 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     p.normal = normal_vars(f);
     // Draw slots: 0 the transform pick, 1 the opacity test, then each
     // NeedsRng variation's draws (consecutive, in its body's order): the
-    // normal phase's in local order, then each final's.
+    // normal phase's in local order, then each attached linked transform's,
+    // then each attached final's.
     int slot = 2, vp = 0;
     for (const VarDef* v : p.normal) {
         p.normal_slot.push_back(v->draws ? slot : -1);
@@ -369,9 +371,9 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
         vp += v->slots();
     }
     p.vp_slots = vp;
-    for (int c : f.fin_chain) {
+    auto chain_entry = [&](const XForm& x) {
         Plan::Fin fi;
-        fi.vars = final_vars(f, f.fin[c]);
+        fi.vars = final_vars(f, x);
         int fo = 0;
         for (const VarDef* v : fi.vars) {
             fi.slot.push_back(v->draws ? slot : -1);
@@ -380,9 +382,34 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
             fo += v->slots();
         }
         fi.prm_slots = fo;
-        p.fin.push_back(fi);
-    }
+        return fi;
+    };
+    for (int c : f.lnk_used) { p.lnk.push_back(chain_entry(f.lnk[c])); p.lnk_pool.push_back(c); }
+    p.fin_slot0 = slot;
+    for (int c : f.fin_used) { p.fin.push_back(chain_entry(f.fin[c])); p.fin_pool.push_back(c); }
     p.n_slots = slot;
+    auto index_of = [](const std::vector<int>& pool, int c) { return (int)(std::find(pool.begin(), pool.end(), c) - pool.begin()); };
+    p.fin_uniform = f.fin_uniform;
+    if (p.fin_uniform) for (int c : f.fin_chain) p.fin_chain.push_back(index_of(p.fin_pool, c));
+    for (auto& x : f.xf) {
+        p.lcap = std::max(p.lcap, (int)x.linked_att.size());
+        if (!p.fin_uniform) p.fcap = std::max(p.fcap, (int)x.final_att.size());
+        // With the counter-based stream a transform's draws have fixed
+        // slots: one chain running a drawing transform twice would draw the
+        // same words twice.
+        if (rng_mode == RNG_PHILOX) {
+            auto repeats = [&](const std::vector<int>& att, const std::vector<XForm>& pool) {
+                for (size_t i = 0; i < att.size(); ++i)
+                    for (size_t j = i + 1; j < att.size(); ++j)
+                        if (att[i] == att[j])
+                            for (const VarDef* v : final_vars(f, pool[(size_t)att[i]]))
+                                if (v->draws) return true;
+                return false;
+            };
+            if (repeats(x.linked_att, f.lnk) || repeats(x.final_att, f.fin))
+                throw std::runtime_error("a chain attaching the same randomised transform twice needs the pcg stream in this build");
+        }
+    }
     int n_state = 0;
     const std::vector<StEntry> layout = state_layout(f, n_state);
     p.n_state = n_state;
@@ -437,6 +464,9 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     p.t_fin = p.t_vp + p.vp_slots * M;
     int off = p.t_fin;
     for (auto& fi : p.fin) { fi.off = off; off += 13 + 2 * (int)fi.vars.size() + fi.prm_slots; }
+    for (auto& li : p.lnk) { li.off = off; off += 13 + 2 * (int)li.vars.size() + li.prm_slots; }
+    p.t_att = off;
+    if (p.lcap > 0 || p.fcap > 0) off += M * (2 + p.lcap + p.fcap);
     p.sym_kind = f.sym.kind;
     p.t_sym = off;
     if (p.sym_kind != 0) off += kSymBlock;
@@ -462,6 +492,9 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     std::ostringstream s;
     s << "// generated by ffb_codegen for one flame structure\n";
     s << "#define FFB_MAXX " << M << "\n#define FFB_NVN " << NVN << "\n#define FFB_NFIN " << p.fin.size() << "\n";
+    s << "#define FFB_NLNK " << p.lnk.size() << "\n#define FFB_LCAP " << p.lcap << "\n#define FFB_FCAP " << p.fcap
+      << "\n#define FFB_ATT_STRIDE " << (2 + p.lcap + p.fcap) << "\n#define T_ATT " << p.t_att << "\n#define FFB_FIN_SLOT0 "
+      << p.fin_slot0 << "\n";
     s << "#define FFB_HAS_POST " << (p.has_post ? 1 : 0) << "\n#define FFB_NSLOTS " << p.n_slots << "\n";
     s << "#define FFB_RNG_MODE " << rng_mode << "\n#define FFB_THREADS " << threads << "\n";
     if (math_mode == MATH_SFU) s << "#define FFB_SFU 1\n";
@@ -518,24 +551,45 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     s << "}\n";
     // One final of the chain (main_template.wgsl:679-704): affine,
     // variations, post-affine; `aff` false evaluates the variations alone.
-    s << "template <class R> __device__ __forceinline__ void ffb_final_one(const float* __restrict__ sm, int c, float& x, float& y, R& rng, FfbCtx& ctx, bool aff) {\n";
-    s << "    float vcd = 0.0f;   // a final's colour writes are dropped (main_template.wgsl:299-300)\n    (void)vcd; (void)ctx;\n";
-    s << "    switch (c) {\n";
-    for (size_t c = 0; c < p.fin.size(); ++c) {
-        const Plan::Fin& fi = p.fin[c];
-        s << "    case " << c << ": {\n        const float* q = sm + " << fi.off << ";\n";
-        s << "        if (aff) { float ax = q[0] * x + q[1] * y + q[4]; float ay = q[2] * x + q[3] * y + q[5]; x = ax; y = ay; }\n";
-        emit_phases(s, fi.vars, [&](int j) { return final_site(fi, j); }, "        ", true, "vcd");
-        s << "        if (aff && q[12] > 0.5f) { float px = q[6] * rx + q[7] * ry + q[10]; float py = q[8] * rx + q[9] * ry + q[11]; rx = px; ry = py; }\n";
-        s << "        x = rx; y = ry;\n        break; }\n";
+    // A final's colour writes are dropped (main_template.wgsl:299-300); a
+    // linked transform's reach the register (main_template.wgsl:320-326).
+    auto emit_chain_one = [&](const char* name, const std::vector<Plan::Fin>& list, const char* vc) {
+        s << "template <class R> __device__ __forceinline__ void " << name
+          << "(const float* __restrict__ sm, int c, float& x, float& y, R& rng, FfbCtx& ctx, bool aff) {\n";
+        s << "    float vcd = 0.0f;\n    (void)vcd; (void)ctx;\n";
+        s << "    switch (c) {\n";
+        for (size_t c = 0; c < list.size(); ++c) {
+            const Plan::Fin& fi = list[c];
+            s << "    case " << c << ": {\n        const float* q = sm + " << fi.off << ";\n";
+            s << "        if (aff) { float ax = q[0] * x + q[1] * y + q[4]; float ay = q[2] * x + q[3] * y + q[5]; x = ax; y = ay; }\n";
+            emit_phases(s, fi.vars, [&](int j) { return final_site(fi, j); }, "        ", true, vc);
+            s << "        if (aff && q[12] > 0.5f) { float px = q[6] * rx + q[7] * ry + q[10]; float py = q[8] * rx + q[9] * ry + q[11]; rx = px; ry = py; }\n";
+            s << "        x = rx; y = ry;\n        break; }\n";
+        }
+        s << "    default: break;\n    }\n}\n";
+    };
+    emit_chain_one("ffb_final_one", p.fin, "vcd");
+    emit_chain_one("ffb_linked_one", p.lnk, "ctx.vc");
+    // Normal transform k's linked chain, each output feeding the next
+    // (main_template.wgsl:320-360), from the attachment table.
+    s << "template <class R> __device__ __forceinline__ void ffb_linked(const float* __restrict__ sm, int k, float& x, float& y, R& rng, FfbCtx& ctx) {\n";
+    if (!p.lnk.empty())
+        s << "    const float* a = sm + T_ATT + k * FFB_ATT_STRIDE;\n    const int n = (int)a[0];\n"
+             "    for (int i = 0; i < n; ++i) ffb_linked_one(sm, (int)a[1 + i], x, y, rng, ctx, true);\n";
+    s << "    (void)sm; (void)k; (void)x; (void)y; (void)rng; (void)ctx;\n}\n";
+    // The final chain of normal transform k (main_template.wgsl:663-717):
+    // one chain for every transform, or each its own from the table.
+    s << "template <class R> __device__ __forceinline__ void ffb_finals(const float* __restrict__ sm, int k, float& x, float& y, R& rng, FfbCtx& ctx) {\n";
+    if (p.fin_uniform) {
+        for (int c : p.fin_chain) s << "    ffb_final_one(sm, " << c << ", x, y, rng, ctx, true);\n";
+    } else {
+        s << "    const float* a = sm + T_ATT + k * FFB_ATT_STRIDE + 1 + FFB_LCAP;\n    const int n = (int)a[0];\n"
+             "    for (int i = 0; i < n; ++i) ffb_final_one(sm, (int)a[1 + i], x, y, rng, ctx, true);\n";
     }
-    s << "    default: break;\n    }\n}\n";
-    s << "template <class R> __device__ __forceinline__ void ffb_finals(const float* __restrict__ sm, float& x, float& y, R& rng, FfbCtx& ctx) {\n";
-    for (size_t c = 0; c < p.fin.size(); ++c) s << "    ffb_final_one(sm, " << c << ", x, y, rng, ctx, true);\n";
-    s << "    (void)ctx;\n}\n";
+    s << "    (void)sm; (void)k; (void)x; (void)y; (void)rng; (void)ctx;\n}\n";
     if (p.defer) {
-        // The final chain's draws in the order it takes them (slot order),
-        // for the deferred plot: one plane of `stride` a draw.
+        // The finals' draws by slot (FFB_FIN_SLOT0 onwards), for the
+        // deferred plot: one plane of `stride` a draw.
         s << "template <class R> __device__ __forceinline__ void ffb_capture_final_draws(R& rng, float* out, unsigned long long stride) {\n";
         int m = 0;
         for (auto& fi : p.fin)
@@ -616,9 +670,9 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
     }
     int n_state = 0;
     const std::vector<StEntry> layout = state_layout(f, n_state);
-    for (size_t c = 0; c < p.fin.size(); ++c) {
-        const Plan::Fin& fi = p.fin[c];
-        const XForm& x = f.fin[f.fin_chain[c]];
+    // Final and linked records: affine, post-affine, post flag, then the
+    // weights, the parameter rows, the state bases.
+    auto chain_rec = [&](const Plan::Fin& fi, const XForm& x, int kind, int pool) {
         const float rec[13] = {x.a, x.b, x.c, x.d, x.e, x.f, x.pa, x.pb, x.pc, x.pd, x.pe, x.pf, x.post ? 1.0f : 0.0f};
         for (int q = 0; q < 13; ++q) t[fi.off + q] = rec[q];
         const int nv = (int)fi.vars.size();
@@ -627,7 +681,25 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
             float row[kMaxVarSlots];
             x.slot_values(fi.vars[j], row);
             for (int q = 0; q < fi.vars[j]->slots(); ++q) t[fi.off + 13 + nv + fi.prm_off[j] + q] = row[q];
-            t[fi.off + 13 + nv + fi.prm_slots + j] = (float)state_base(layout, 1, 0, f.fin_chain[c], fi.vars[j]);
+            t[fi.off + 13 + nv + fi.prm_slots + j] = (float)state_base(layout, kind, 0, pool, fi.vars[j]);
+        }
+    };
+    for (size_t c = 0; c < p.fin.size(); ++c) chain_rec(p.fin[c], f.fin[p.fin_pool[c]], 1, p.fin_pool[c]);
+    for (size_t c = 0; c < p.lnk.size(); ++c) chain_rec(p.lnk[c], f.lnk[p.lnk_pool[c]], 3, p.lnk_pool[c]);
+    // Attachments (gpu/buffers.rs:621-660) as indices into the plan's
+    // linked and final lists: per normal, the linked count and entries,
+    // then (chains differing) the final count and entries.
+    if (p.lcap > 0 || p.fcap > 0) {
+        const int stride = 2 + p.lcap + p.fcap;
+        auto at = [](const std::vector<int>& pool, int c) { return (float)(std::find(pool.begin(), pool.end(), c) - pool.begin()); };
+        for (size_t k = 0; k < f.xf.size(); ++k) {
+            float* a = t.data() + p.t_att + k * stride;
+            const XForm& x = f.xf[k];
+            a[0] = (float)std::min<size_t>(x.linked_att.size(), (size_t)p.lcap);
+            for (size_t i = 0; i < x.linked_att.size() && (int)i < p.lcap; ++i) a[1 + i] = at(p.lnk_pool, x.linked_att[i]);
+            float* b = a + 1 + p.lcap;
+            b[0] = (float)std::min<size_t>(x.final_att.size(), (size_t)p.fcap);
+            for (size_t i = 0; i < x.final_att.size() && (int)i < p.fcap; ++i) b[1 + i] = at(p.fin_pool, x.final_att[i]);
         }
     }
     // Each stateful normal variation's first state slot per transform.

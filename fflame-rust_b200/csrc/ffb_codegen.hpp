@@ -35,7 +35,14 @@ struct Plan {
         int prm_slots = 0;
         int off = 0;
     };
-    std::vector<Fin> fin;                  // one per final in the chain
+    std::vector<Fin> fin;                  // one per attached final (pool order)
+    std::vector<Fin> lnk;                  // one per attached linked transform (pool order)
+    std::vector<int> fin_pool, lnk_pool;   // each entry's pool index
+    bool fin_uniform = true;               // every normal runs the same final chain ...
+    std::vector<int> fin_chain;            // ... this one (indices into fin)
+    int lcap = 0, fcap = 0;                // longest linked chain; longest final chain when they differ
+    int t_att = 0;                         // per normal: linked count, lcap entries, final count, fcap entries
+    int fin_slot0 = 2;                     // the finals' first draw slot
     bool has_post = false;
     int n_slots = 2;
     int table_size = 0;

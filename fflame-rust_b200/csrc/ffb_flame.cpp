@@ -292,8 +292,8 @@ XForm parse_transform(const Json& t) {
         for (auto& kv : vp->obj) if (kv.second->kind == Json::Number) x.params.emplace_back(kv.first, (float)kv.second->num);
     if (const Json* fa = t.get("final_attachments"); fa && fa->kind == Json::Array)
         for (auto& e : fa->arr) if (e->kind == Json::Number) x.final_att.push_back((int)e->num);
-    if (const Json* la = t.get("linked_attachments"); la && la->kind == Json::Array && !la->arr.empty())
-        fail("linked transforms are not supported by this build");
+    if (const Json* la = t.get("linked_attachments"); la && la->kind == Json::Array)
+        for (auto& e : la->arr) if (e->kind == Json::Number) x.linked_att.push_back((int)e->num);
     return x;
 }
 
@@ -364,8 +364,8 @@ Flame parse_config(const Json& cfg) {
     const Json* ts = fl->get("transforms");
     if (!ts || ts->kind != Json::Array) fail("missing field `transforms`");
     for (auto& t : ts->arr) F.xf.push_back(parse_transform(*t));
-    if (const Json* lt = fl->get("linked_transforms"); lt && lt->kind == Json::Array && !lt->arr.empty())
-        fail("linked transforms are not supported by this build");
+    if (const Json* lt = fl->get("linked_transforms"); lt && lt->kind == Json::Array)
+        for (auto& t : lt->arr) F.lnk.push_back(parse_transform(*t));
     // Xaos (utilities.wgsl:106-137): read when some weight differs from 1
     // (xaos.rs:29-40); entries beyond the matrix are 1 (get_xaos, xaos.rs:128-135).
     if (const Json* xa = fl->get("xaos"); xa && xa->kind == Json::Array) {
@@ -405,14 +405,32 @@ Flame parse_config(const Json& cfg) {
     if (F.xf.empty()) fail("the flame has no transforms");
     if (F.xf.size() > 128)
         fail("TooLarge: the flame has " + std::to_string(F.xf.size()) + " transforms; the renderer holds 128");
-    for (auto& x : F.xf)
-        for (int a : x.final_att)
-            if (a < 0 || a >= (int)F.fin.size()) fail("a final attachment points past the final pool");
+    // Attachment lists (GpuAttachmentList::from_transform, gpu/buffers.rs:621-660):
+    // indices past their pool dropped, at most kMaxAttach kept.
+    auto clean = [](std::vector<int>& att, size_t pool) {
+        std::vector<int> out;
+        for (int a : att) {
+            if ((int)out.size() >= kMaxAttach) break;
+            if (a >= 0 && (size_t)a < pool) out.push_back(a);
+        }
+        att = out;
+    };
+    for (auto& x : F.xf) { clean(x.final_att, F.fin.size()); clean(x.linked_att, F.lnk.size()); }
+    // Attachments only a normal transform carries.
+    for (auto& x : F.lnk) { x.final_att.clear(); x.linked_att.clear(); }
+    for (auto& x : F.fin) { x.final_att.clear(); x.linked_att.clear(); }
     F.fin_chain = F.xf[0].final_att;
-    for (auto& x : F.xf)
-        if (x.final_att != F.fin_chain)
-            fail("transforms with different final attachments are not supported by this build");
-    if (F.fin_chain.size() > 8) fail("more than 8 chained final transforms are not supported");
+    for (auto& x : F.xf) F.fin_uniform = F.fin_uniform && x.final_att == F.fin_chain;
+    if (!F.fin_uniform) F.fin_chain.clear();
+    std::vector<char> fu(F.fin.size(), 0), lu(F.lnk.size(), 0);
+    for (auto& x : F.xf) {
+        for (int a : x.final_att) fu[(size_t)a] = 1;
+        for (int a : x.linked_att) lu[(size_t)a] = 1;
+    }
+    for (size_t i = 0; i < fu.size(); ++i) if (fu[i]) F.fin_used.push_back((int)i);
+    for (size_t i = 0; i < lu.size(); ++i) if (lu[i]) F.lnk_used.push_back((int)i);
+    if (F.fin_used.size() > 16) fail("more than 16 attached final transforms are not supported by this build");
+    if (F.lnk_used.size() > 16) fail("more than 16 attached linked transforms are not supported by this build");
     // Post-symmetry (transforms.rs:2149-2167; serde: `ty` lowercase, the
     // other fields required when the object is present).
     if (const Json* ps = fl->get("post_symmetry"); ps && ps->kind == Json::Object) {
@@ -448,13 +466,14 @@ Flame parse_config(const Json& cfg) {
         }
         if (total > 256) fail("TooLarge: the subflames have " + std::to_string(total) + " transforms; the renderer holds 256");
     }
-    // Local variation order (transforms.rs:2297-2319): normals then finals,
-    // then each subflame's.
+    // Local variation order (transforms.rs:2297-2319): normals, linked,
+    // finals, then each subflame's.
     auto absorb = [&](const XForm& x) {
         for (auto& p : x.vars)
             if (std::find(F.local.begin(), F.local.end(), p.first) == F.local.end()) F.local.push_back(p.first);
     };
     for (auto& x : F.xf) absorb(x);
+    for (auto& x : F.lnk) absorb(x);
     for (auto& x : F.fin) absorb(x);
     for (auto& S : F.sub) {
         for (auto& x : S.xf) absorb(x);

@@ -72,6 +72,7 @@ struct XForm {
     // "name.param" -> value
     std::vector<std::pair<std::string, float>> params;
     std::vector<int> final_att;   // indices into the finals pool
+    std::vector<int> linked_att;  // indices into the linked pool
     float param(const VarDef* v, int j) const;
     // The packed row: user parameters, then the derived values.
     void slot_values(const VarDef* v, float* out) const;
@@ -126,10 +127,21 @@ struct SubFlame {
     std::vector<XForm> xf, fin;
 };
 
+// Attachments (transforms.rs:470-480; gpu/buffers.rs:600-680): each normal
+// transform's linked chain -- transforms applied after it in the same
+// iteration, their output the walker's next point -- and its final chain,
+// applied at plot time only.  Indices past their pool are dropped and a
+// chain holds at most kMaxAttach (the reference logs and does the same).
+constexpr int kMaxAttach = 32;
+
 struct Flame {
     std::vector<XForm> xf;              // normal transforms
+    std::vector<XForm> lnk;             // linked transforms pool
     std::vector<XForm> fin;             // final transforms pool
-    std::vector<int> fin_chain;         // the final chain every normal runs
+    std::vector<int> fin_chain;         // the final chain every normal runs, when they share one
+    bool fin_uniform = true;            // every normal has the same final chain
+    std::vector<int> fin_used;          // finals some normal attaches, pool order
+    std::vector<int> lnk_used;          // linked transforms some normal attaches, pool order
     std::vector<const VarDef*> local;   // local variation order (parent, then subflames)
     std::vector<SubFlame> sub;          // at most 8 (MAX_SUBFLAMES, buffers.rs:36-44)
     SpatialFilter filter;

@@ -307,14 +307,14 @@ __device__ __forceinline__ void ffb_sym_copy(const float* __restrict__ sm, int k
 }
 #endif
 
-// The plot of a kept sample: the final chain, the palette, the symmetry
-// copies, world_to_pixel and the splat (main_template.wgsl:663-1320).
+// The plot of a kept sample of transform k: its final chain, the palette,
+// the symmetry copies, world_to_pixel and the splat (main_template.wgsl:663-1320).
 template <class R>
 __device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
-                                                float x, float y, float ci, bool plot, R& rng, FfbCtx& ctx, float cx, float cy,
-                                                float scale, u32& inframe) {
+                                                int k, float x, float y, float ci, bool plot, R& rng, FfbCtx& ctx, float cx,
+                                                float cy, float scale, u32& inframe) {
     float fx = x, fy = y;
-    ffb_finals(sm, fx, fy, rng, ctx);                                       // main_template.wgsl:663-717
+    ffb_finals(sm, k, fx, fy, rng, ctx);                                    // main_template.wgsl:663-717
     const int pal_idx = ffb_palette_index(ci, J.pal_n);
     const float4 c = pal[pal_idx];                                          // main_template.wgsl:766-772
 #if FFB_SYM_KIND != 0
@@ -348,25 +348,26 @@ __device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, co
 
 #ifdef FFB_DEFER
 // Deferred plotting: the chaos kernel stores each iteration's sample (its
-// point after the transform, colour index, plot flag) and the draws its
-// final chain takes, in the order it takes them; ffb_plot applies the rest.
-// A record a walker and iteration: (x, y, ci, flags) with flags bit 1 a
-// kept sample, bit 0 its opacity draw passed; 0 for burn-in and respawns.
+// point after the transform, colour index, plot flag, transform) and the
+// draws of the finals' slots; ffb_plot applies the rest.  A record a
+// walker and iteration: (x, y, ci, flags) with flags bit 1 a kept sample,
+// bit 0 its opacity draw passed, bits 8-15 the transform picked; 0 for
+// burn-in and respawns.
 __device__ __forceinline__ u64 ffb_rec_index(const ffb_launch& J, u32 gw, u64 it) {
     return (it - J.it0) * (u64)J.n_walkers + (u64)(gw - J.walker0);
 }
 #define FFB_DEFER_SKIP(J, gw, it) ((J).rec[ffb_rec_index((J), (gw), (it))] = make_float4(0.f, 0.f, 0.f, 0.f))
 template <class R>
-__device__ __forceinline__ void ffb_defer_store(const ffb_launch& J, u32 gw, u64 it, float x, float y, float ci, bool plot, R& rng) {
+__device__ __forceinline__ void ffb_defer_store(const ffb_launch& J, u32 gw, u64 it, int k, float x, float y, float ci, bool plot,
+                                                R& rng) {
     const u64 ri = ffb_rec_index(J, gw, it);
-    J.rec[ri] = make_float4(x, y, ci, __uint_as_float(2u | (plot ? 1u : 0u)));
+    J.rec[ri] = make_float4(x, y, ci, __uint_as_float(2u | (plot ? 1u : 0u) | ((u32)k << 8)));
     ffb_capture_final_draws(rng, J.rec_draws + ri, (u64)J.n_iters * J.n_walkers);
 }
-// The stored draws handed back in order.
-struct SeqRng {
+// The stored draws handed back by slot.
+struct SlotRng {
     const float* d;
-    int i;
-    __device__ __forceinline__ float draw(int) { return d[i++]; }
+    __device__ __forceinline__ float draw(int slot) { return d[slot - FFB_FIN_SLOT0]; }
 };
 #else
 #define FFB_DEFER_SKIP(J, gw, it) ((void)0)
@@ -398,6 +399,9 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
         ax = px; ay = py;
     }
 #endif
+#if FFB_NLNK > 0
+    ffb_linked(sm, k, ax, ay, rng, ctx);                                    // main_template.wgsl:320-360
+#endif
     if (!(fabsf(ax) <= 1e32f) || !(fabsf(ay) <= 1e32f)) {                  // main_template.wgsl:449-479
 #if FFB_RNG_MODE == 1
         uint4 o = philox4(J.seed_lo, J.seed_hi, gw, (u32)it, 0xFFFFFFFFu, (u32)(it >> 32));
@@ -419,9 +423,9 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
 #endif
     if (fuse > 0u) { fuse -= 1u; FFB_DEFER_SKIP(J, gw, it); return; }     // main_template.wgsl:510-514
 #ifdef FFB_DEFER
-    ffb_defer_store(J, gw, it, x, y, ci, plot, rng);
+    ffb_defer_store(J, gw, it, k, x, y, ci, plot, rng);
 #else
-    ffb_plot_sample(sm, pal, J, x, y, ci, plot, rng, ctx, cx, cy, scale, inframe);
+    ffb_plot_sample(sm, pal, J, k, x, y, ci, plot, rng, ctx, cx, cy, scale, inframe);
 #endif
 }
 
@@ -664,9 +668,9 @@ extern "C" __global__ void __launch_bounds__(384) ffb_plot(const ffb_launch* __r
         float fd[FFB_NFD > 0 ? FFB_NFD : 1];
 #pragma unroll
         for (int m = 0; m < FFB_NFD; ++m) fd[m] = J.rec_draws[(u64)m * n + i];
-        SeqRng rng{fd, 0};
+        SlotRng rng{fd};
         FfbCtx ctx{nullptr, 0u, 0.0f, 0u, 0u, 0u, 0ull};                // deferred finals carry no state
-        ffb_plot_sample(sm, pal, J, r.x, r.y, r.z, (fl & 1u) != 0u, rng, ctx, cx, cy, scale, inframe);
+        ffb_plot_sample(sm, pal, J, (int)((fl >> 8) & 0xFFu), r.x, r.y, r.z, (fl & 1u) != 0u, rng, ctx, cx, cy, scale, inframe);
     }
     ffb_count_inframe(J, inframe);
 }

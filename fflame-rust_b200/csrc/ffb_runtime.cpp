@@ -1108,7 +1108,7 @@ FFB_API int ffb_probe(ffb_renderer* r, const char* config, size_t len, const flo
         catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
         Plan p = make_plan(f, RNG_PCG, math, 0, 128);
         std::vector<float> tab = make_table(p, f);
-        const int n_all = (int)(f.xf.size() + f.fin_chain.size());
+        const int n_all = (int)(f.xf.size() + f.fin_used.size());
         if (out_pairs < (uint32_t)n_all * npts) fail(FFB_ERR_INVALID, "output too small");
         Module& m = r->module_for(p.source);
         void* d_tab = r->table.ensure(tab.size() * 4);
@@ -1135,7 +1135,7 @@ FFB_API int ffb_apply_points(ffb_renderer* r, const char* config, size_t len, in
         Flame f;
         try { f = parse_config_text(std::string(config, len)); }
         catch (const std::exception& e) { fail(FFB_ERR_CONFIG, std::string("config did not parse: ") + e.what()); }
-        const int n_all = (int)(f.xf.size() + f.fin_chain.size());
+        const int n_all = (int)(f.xf.size() + f.fin_used.size());
         if (xform < 0 || xform >= n_all) fail(FFB_ERR_INVALID, "no such transform");
         Plan p = make_plan(f, RNG_PHILOX, math, 0, 128);
         std::vector<float> tab = make_table(p, f);
@@ -1715,7 +1715,8 @@ FFB_API int ffb_diff_create(ffb_renderer* r, const char* config, size_t len, con
         if (d->P.flame.filter.on()) fail(FFB_ERR_INVALID, "the differentiable render has no spatial filter (filter_radius)");
         const Flame& f = d->P.flame;
         if (d->P.ss != 1) fail(FFB_ERR_INVALID, "the differentiable render has no supersampling");
-        if (!f.fin_chain.empty()) fail(FFB_ERR_CONFIG, "the differentiable render takes no final transforms");
+        if (!f.fin_used.empty() || !f.lnk_used.empty())
+            fail(FFB_ERR_CONFIG, "the differentiable render takes no final or linked transforms");
         if (f.de.max_radius > 0.0f) fail(FFB_ERR_CONFIG, "the differentiable render takes no density estimation");
         if (f.sym.kind != 0) fail(FFB_ERR_CONFIG, "the differentiable render takes no post-symmetry");
         if (job->transparent) fail(FFB_ERR_INVALID, "the differentiable render is opaque");

@@ -131,7 +131,28 @@ class OFlame(ctypes.Structure):
         ("n_sub", ctypes.c_int),
         ("sub_nxf", ctypes.POINTER(ctypes.c_int)),
         ("sub_nfin", ctypes.POINTER(ctypes.c_int)),
+        ("n_lnk", ctypes.c_int),
+        ("att", ctypes.POINTER(ctypes.c_int)),
     ]
+
+
+ATTACH = 32        # a chain's length at most (MAX_ATTACHMENTS_PER_TRANSFORM)
+
+
+def attachments(flame):
+    """Each normal's (linked, final) chains as pool indices
+    (gpu/buffers.rs:621-660): a legacy singular final attached to every
+    normal, indices past their pool dropped, at most ATTACH kept."""
+    nl, fins = len(flame.get("linked_transforms", [])), finals_of(flame)
+    legacy = len(flame.get("final_transforms", [])) if flame.get("final_transform") else None
+    out = []
+    for t in flame["transforms"]:
+        fa = [int(a) for a in t.get("final_attachments", [])]
+        if legacy is not None and legacy not in fa:
+            fa.append(legacy)
+        la = [int(a) for a in t.get("linked_attachments", [])]
+        out.append(([a for a in la if 0 <= a < nl][:ATTACH], [a for a in fa if 0 <= a < len(fins)][:ATTACH]))
+    return out
 
 
 class TonemapParams(ctypes.Structure):
@@ -188,9 +209,9 @@ def subflame_transforms(flame):
 
 
 def local_order(flame):
-    """transforms.rs:2297-2319: normals then finals, then each subflame's; first appearance wins."""
+    """transforms.rs:2297-2319: normals, linked, finals, then each subflame's; first appearance wins."""
     out = []
-    allx = list(flame["transforms"]) + finals_of(flame)
+    allx = list(flame["transforms"]) + list(flame.get("linked_transforms", [])) + finals_of(flame)
     for nx, fx in subflame_transforms(flame):
         allx += nx + fx
     for t in allx:
@@ -235,9 +256,10 @@ class Flame:
         flame = cfg["flame"]
         self.names = local_order(flame)
         normals = flame["transforms"]
+        links = list(flame.get("linked_transforms", []))
         fins = finals_of(flame)
         subs = subflame_transforms(flame)
-        allx = list(normals) + fins
+        allx = list(normals) + links + fins
         for nx, fx in subs:
             allx += nx + fx
         nv = len(self.names)
@@ -273,6 +295,13 @@ class Flame:
         s.n_sub = len(subs)
         s.sub_nxf = self.sub_nxf.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         s.sub_nfin = self.sub_nfin.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        att = np.zeros((max(len(normals), 1), 2 + 2 * ATTACH), np.int32)
+        for k, (la, fa) in enumerate(attachments(flame)):
+            att[k, 0], att[k, 1:1 + len(la)] = len(la), la
+            att[k, 1 + ATTACH], att[k, 2 + ATTACH:2 + ATTACH + len(fa)] = len(fa), fa
+        self.att = np.ascontiguousarray(att.ravel())
+        s.n_lnk = len(links)
+        s.att = self.att.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         # Xaos (xaos.rs:29-40, 128-135): read when some weight differs from 1; missing entries are 1.
         self.xaos = None
         if flame.get("xaos"):
