@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
+#include <limits>
 #include <random>
 
 namespace ffb {
@@ -525,8 +527,13 @@ Flame parse_config(const Json& cfg) {
     if (F.palette_size < 2 || F.palette_size > 4096) fail("palette_size must be 2..4096");
     F.palette_rotation = num_field(cfg, "palette_rotation", false, 0.0f);
     F.palette_reverse = cfg.bool_or("palette_reverse", false);
-    if (num_field(cfg, "palette_squeeze", false, 1.0f) != 1.0f || num_field(cfg, "palette_log_strength", false, 0.0f) != 0.0f)
-        fail("palette squeeze / log redistribution are not supported by this build");
+    F.palette_squeeze = num_field(cfg, "palette_squeeze", false, 1.0f);              // fractal_config.rs:436-456
+    F.palette_squeeze_falloff = num_field(cfg, "palette_squeeze_falloff", false, 0.5f);
+    F.palette_log_strength = num_field(cfg, "palette_log_strength", false, 0.0f);
+    if (const Json* m = cfg.get("palette_squeeze_mode"); m && m->kind == Json::String) {
+        static const char* const kSqueeze[] = {"linear", "Linear", "geometric", "Geometric"};
+        F.palette_squeeze_mode = mode_code(m->str, kSqueeze, 2, "palette squeeze mode");
+    }
     if (const Json* cm = cfg.get("color_mode"); cm && cm->kind == Json::String && cm->str != "Palette" && cm->str != "palette")
         fail("colour mode `" + cm->str + "` is not supported by this build (palette only)");
     F.filter.radius = num_field(cfg, "filter_radius", false, 0.0f);
@@ -633,6 +640,51 @@ std::vector<float> palette_table(const Flame& f) {
             }
         }
         for (int k = 0; k < 3; ++k) base[(size_t)i * 3 + k] = c[k];
+    }
+    // Squeeze, then redistribution (palette.rs:703-766): entry i reads the
+    // previous table at floor(src_t * size) (saturating, at most size - 1)
+    // for src_t the stage's map of t = i / size.
+    auto remap = [&](std::vector<float>& tab, const std::function<float(float)>& map) {
+        std::vector<float> out((size_t)size * 3);
+        for (int i = 0; i < size; ++i) {
+            const float src_t = map((float)i / (float)size);
+            const float fi = src_t * (float)size;
+            const size_t src = std::min<size_t>(!(fi > 0.0f) ? 0 : fi >= 1.8e19f ? SIZE_MAX : (size_t)fi, (size_t)size - 1);
+            for (int k = 0; k < 3; ++k) out[(size_t)i * 3 + k] = tab[src * 3 + k];
+        }
+        tab = out;
+    };
+    if (f.palette_squeeze_mode == 0 && f.palette_squeeze != 1.0f) {
+        const float factor = f.palette_squeeze;
+        remap(base, [factor](float t) { const float x = t * factor; return x - std::trunc(x); });
+    } else if (f.palette_squeeze_mode == 1) {
+        const float r = f.palette_squeeze_falloff;
+        remap(base, [r](float t) {                        // geometric_squeeze_lookup, palette.rs:607-640
+            if (r >= 0.999f) return t;
+            if (r <= 0.001f) return std::min(std::max(t / std::max(r, 1e-6f), 0.0f), 1.0f);
+            if (t <= 0.0f) return 0.0f;
+            float start = 0.0f, rn = 1.0f;
+            for (int n = 0; n < 64; ++n) {
+                const float width = rn * (1.0f - r);
+                const float end = start + width;
+                if (t < end) return width <= 0.0f ? 0.0f : std::min(std::max((t - start) / width, 0.0f), 1.0f);
+                start = end;
+                rn *= r;
+                if (rn < 1e-10f) return 1.0f;
+            }
+            return 1.0f;
+        });
+    }
+    if (std::fabs(f.palette_log_strength) >= std::numeric_limits<float>::epsilon()) {
+        const float s = f.palette_log_strength;
+        remap(base, [s](float t) {                        // log_redistribute_lookup, palette.rs:653-671
+            if (s > 0.0f) {
+                const float d = std::expm1(s);
+                return d == 0.0f ? t : std::min(std::max(std::expm1(s * t) / d, 0.0f), 1.0f);
+            }
+            const float d = std::expm1(-s);
+            return d == 0.0f ? t : std::min(std::max(1.0f - std::expm1(-s * (1.0f - t)) / d, 0.0f), 1.0f);
+        });
     }
     std::vector<float> rot = base;
     if (f.palette_rotation != 0.f) {                      // palette.rs:768-783

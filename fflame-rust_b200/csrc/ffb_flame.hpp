@@ -157,6 +157,11 @@ struct Flame {
     int palette_size = 256;
     float palette_rotation = 0.0f;
     bool palette_reverse = false;
+    // The lookup pipeline's squeeze and redistribution (palette.rs:485-800):
+    // mode 0 linear (repeat count `palette_squeeze`), 1 geometric (octave
+    // ratio `palette_squeeze_falloff`); then exponential redistribution.
+    int palette_squeeze_mode = 0;
+    float palette_squeeze = 1.0f, palette_squeeze_falloff = 0.5f, palette_log_strength = 0.0f;
     ToneMap tm;
     DensityEstimation de;
     uint64_t max_iterations = 1000000000ull;

@@ -243,9 +243,12 @@ def palette_table(cfg):
         pos = np.array([s["position"] for s in pal["stops"]], np.float32)
         col = np.array([c for s in pal["stops"] for c in s["color"]], np.float32)
     out = np.zeros(size * 3, np.float32)
+    mode = {"linear": 0, "Linear": 0, "geometric": 1, "Geometric": 1}[cfg.get("palette_squeeze_mode", "linear")]
     lib().of_palette_table(ctypes.c_int(len(pos)), _fp(pos), _fp(col), ctypes.c_int(size),
                            ctypes.c_float(cfg.get("palette_rotation", 0.0)),
-                           ctypes.c_int(1 if cfg.get("palette_reverse") else 0), _fp(out))
+                           ctypes.c_int(1 if cfg.get("palette_reverse") else 0), _fp(out), ctypes.c_int(mode),
+                           ctypes.c_float(cfg.get("palette_squeeze", 1.0)), ctypes.c_float(cfg.get("palette_squeeze_falloff", 0.5)),
+                           ctypes.c_float(cfg.get("palette_log_strength", 0.0)))
     return out
 
 
