@@ -414,6 +414,14 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     const std::vector<StEntry> layout = state_layout(f, n_state);
     p.n_state = n_state;
     for (auto& e : layout) p.n_init += e.init ? 1 : 0;
+    // Speed colour: three more slots a walker; its colour travels with the
+    // walker, so the plot stays inline and the splat unaggregated.
+    p.speed = f.color_mode == 1;
+    if (p.speed) {
+        p.speed_slot = p.n_state;
+        p.n_state += 3;
+        p.defer = false;
+    }
     p.st_row.assign(p.normal.size(), -1);
     int st_rows = 0;
     for (size_t j = 0; j < p.normal.size(); ++j) {
@@ -473,6 +481,8 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     p.xaos = !f.xaos.empty();
     p.t_xaos = off;
     if (p.xaos) off += M * (M + 1);
+    p.t_speed = off;
+    if (p.speed) off += 1;
     p.t_st = off;
     off += st_rows * M;
     p.t_init = off;
@@ -508,6 +518,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     s << "#define FFB_NSTATE " << p.n_state << "\n#define FFB_NINIT " << p.n_init << "\n#define T_ST " << p.t_st
       << "\n#define T_INIT " << p.t_init << "\n";
     if (p.dc) s << "#define FFB_DC 1\n";
+    if (p.speed) s << "#define FFB_SPEED 1\n#define FFB_SPEED_SLOT " << p.speed_slot << "\n#define T_SPEED " << p.t_speed << "\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
     s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw
       << "\n#define T_VP " << p.t_vp << "\n";
@@ -702,6 +713,7 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
             for (size_t i = 0; i < x.final_att.size() && (int)i < p.fcap; ++i) b[1 + i] = at(p.fin_pool, x.final_att[i]);
         }
     }
+    if (p.speed) t[p.t_speed] = f.speed_factor;
     // Each stateful normal variation's first state slot per transform.
     for (size_t j = 0; j < p.normal.size(); ++j) {
         if (p.st_row[j] < 0) continue;

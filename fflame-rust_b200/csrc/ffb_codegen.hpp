@@ -58,6 +58,10 @@ struct Plan {
     std::vector<int> st_row;               // per normal variation: its row of T_ST (-1: stateless)
     int t_st = 0, t_init = 0;
     bool dc = false;
+    // Speed colour mode: the walker's RGB in state slots speed_slot..+2,
+    // the mix factor in the table at t_speed.
+    bool speed = false;
+    int speed_slot = 0, t_speed = 0;
     std::vector<int> sub_blk;              // per subflame: its block (total, any visible, running sums)
     std::vector<std::vector<int>> sub_rec; // per subflame: each inner transform's record
     int rng_mode = RNG_PHILOX;

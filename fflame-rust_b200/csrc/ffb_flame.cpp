@@ -534,8 +534,12 @@ Flame parse_config(const Json& cfg) {
         static const char* const kSqueeze[] = {"linear", "Linear", "geometric", "Geometric"};
         F.palette_squeeze_mode = mode_code(m->str, kSqueeze, 2, "palette squeeze mode");
     }
-    if (const Json* cm = cfg.get("color_mode"); cm && cm->kind == Json::String && cm->str != "Palette" && cm->str != "palette")
-        fail("colour mode `" + cm->str + "` is not supported by this build (palette only)");
+    if (const Json* cm = cfg.get("color_mode"); cm && cm->kind == Json::String) {
+        if (cm->str == "speed" || cm->str == "Speed") F.color_mode = 1;
+        else if (cm->str != "Palette" && cm->str != "palette")
+            fail("colour mode `" + cm->str + "` is not supported by this build (palette and speed)");
+    }
+    F.speed_factor = num_field(cfg, "speed_factor", false, 0.5f);      // fractal_config.rs:400-401, 866
     F.filter.radius = num_field(cfg, "filter_radius", false, 0.0f);
     F.filter.blur_edges = num_field(cfg, "filter_blur_edges", false, 0.0f);
     // Tone map (defaults.rs:18-52; fractal_config.rs field defaults).

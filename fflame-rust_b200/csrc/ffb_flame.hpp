@@ -162,6 +162,12 @@ struct Flame {
     // ratio `palette_squeeze_falloff`); then exponential redistribution.
     int palette_squeeze_mode = 0;
     float palette_squeeze = 1.0f, palette_squeeze_falloff = 0.5f, palette_log_strength = 0.0f;
+    // Colour mode (palette.rs:8-18): 0 palette, 1 speed -- each walker
+    // carries an RGB colour mixed toward the palette's entry at its step's
+    // speed, clamp(ln(10 speed + 1) / 3, 0, 1), by `speed_factor`
+    // (main_template.wgsl:483-508; utilities.wgsl:148-156).
+    int color_mode = 0;
+    float speed_factor = 0.5f;
     ToneMap tm;
     DensityEstimation de;
     uint64_t max_iterations = 1000000000ull;

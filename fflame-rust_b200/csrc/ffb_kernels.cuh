@@ -40,6 +40,9 @@ __device__ __forceinline__ FfbCtx ffb_ctx(const ffb_launch& J, u32 gw, u64 it) {
 __device__ __forceinline__ void ffb_state_fresh(const float* __restrict__ sm, const ffb_launch& J, u32 gw) {
     float* st = J.state + (gw - J.walker0);
     for (int s = 0; s < FFB_NSTATE; ++s) st[(size_t)s * J.n_walkers] = 0.0f;
+#ifdef FFB_SPEED
+    for (int s = 0; s < 3; ++s) st[(size_t)(FFB_SPEED_SLOT + s) * J.n_walkers] = 1.0f;   // main_template.wgsl:43
+#endif
 #if FFB_RNG_MODE == 1
     for (int i = 0; i < FFB_NINIT; ++i) {
         const uint4 o = philox4(J.seed_lo, J.seed_hi, gw, 0xFFFFFFFEu, (u32)(i >> 2), 0xFFFFFFFFu);
@@ -315,8 +318,17 @@ __device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, co
                                                 float cy, float scale, u32& inframe) {
     float fx = x, fy = y;
     ffb_finals(sm, k, fx, fy, rng, ctx);                                    // main_template.wgsl:663-717
+#ifdef FFB_SPEED
+    // Speed mode plots the walker's own colour (main_template.wgsl:770-772);
+    // a key of its lane keeps the warp's splats apart.
+    const float* wc = ctx.st + (size_t)FFB_SPEED_SLOT * ctx.stride;
+    const float4 c = make_float4(wc[0], wc[ctx.stride], wc[2 * (size_t)ctx.stride], 1.0f);
+    const int pal_idx = 0x8000 | (int)(threadIdx.x & 31u);
+    (void)ci;
+#else
     const int pal_idx = ffb_palette_index(ci, J.pal_n);
     const float4 c = pal[pal_idx];                                          // main_template.wgsl:766-772
+#endif
 #if FFB_SYM_KIND != 0
     const int ncopy = (int)sm[T_SYM];                                       // main_template.wgsl:747-755, 858-870
     for (int sk = 0; sk < ncopy; ++sk) {
@@ -415,6 +427,22 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
         FFB_DEFER_SKIP(J, gw, it);
         return;
     }
+#ifdef FFB_SPEED
+    {   // Speed colour (main_template.wgsl:483, 491-493; utilities.wgsl:148-156):
+        // the step's length, log-scaled into the palette, mixed into the
+        // walker's colour by speed_factor.
+        const float dx = ax - x, dy = ay - y;
+        const float sp = sqrtf(dx * dx + dy * dy);
+        const float ns = fminf(fmaxf(FLOG(sp * 10.0f + 1.0f) / 3.0f, 0.0f), 1.0f);
+        const float4 sc = pal[ffb_palette_index(ns, J.pal_n)];
+        const float t = sm[T_SPEED];
+        float* wc = ctx.st + (size_t)FFB_SPEED_SLOT * ctx.stride;
+        const size_t sd = ctx.stride;
+        wc[0] = wc[0] * (1.0f - t) + sc.x * t;
+        wc[sd] = wc[sd] * (1.0f - t) + sc.y * t;
+        wc[2 * sd] = wc[2 * sd] * (1.0f - t) + sc.z * t;
+    }
+#endif
     x = ax; y = ay;
 #ifdef FFB_DC
     ci = cb + q[F_DC * FFB_MAXX] * (ctx.vc - cb);                          // main_template.wgsl:486-490

@@ -281,6 +281,7 @@ struct Prepared {
 // 1024 entries.
 bool tiled_accumulation(const Prepared& P) {
     if (P.count_bits != 64 || P.accumulate == 1) return false;
+    if (P.flame.color_mode != 0) return false;      // records hold a palette index, not a walker's colour
     if (P.accumulate == 0 && (double)P.wi * (double)P.hi * 32.0 <= 512e6) return false;
     const int tx = (int)((P.wi + 63) / 64), ty = (int)((P.hi + 63) / 64);
     return tx * ty <= kMaxTiles && tx <= kMaxCols && ty <= kMaxBands && P.flame.palette_size <= 1024;
@@ -332,6 +333,8 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     if (P.count_bits != 32 && P.count_bits != 64) fail(FFB_ERR_INVALID, "count_bits must be 32 or 64");
     P.accumulate = job->accumulate;
     if (P.accumulate > 2) fail(FFB_ERR_INVALID, "accumulate must be 0 (auto), 1 (direct) or 2 (tile-sorted)");
+    if (P.accumulate == 2 && P.flame.color_mode != 0)
+        fail(FFB_ERR_INVALID, "tile-sorted accumulation records palette indices: not with the speed colour mode");
     P.plot = job->plot;
     if (P.plot > 2) fail(FFB_ERR_INVALID, "plot must be 0 (auto), 1 (inline) or 2 (deferred)");
     const bool tiled = tiled_accumulation(P);

@@ -133,6 +133,8 @@ class OFlame(ctypes.Structure):
         ("sub_nfin", ctypes.POINTER(ctypes.c_int)),
         ("n_lnk", ctypes.c_int),
         ("att", ctypes.POINTER(ctypes.c_int)),
+        ("color_mode", ctypes.c_int),
+        ("speed_factor", ctypes.c_float),
     ]
 
 
@@ -304,6 +306,8 @@ class Flame:
             att[k, 1 + ATTACH], att[k, 2 + ATTACH:2 + ATTACH + len(fa)] = len(fa), fa
         self.att = np.ascontiguousarray(att.ravel())
         s.n_lnk = len(links)
+        s.color_mode = {"palette": 0, "Palette": 0, "speed": 1, "Speed": 1}[cfg.get("color_mode", "palette")]
+        s.speed_factor = cfg.get("speed_factor", 0.5)
         s.att = self.att.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         # Xaos (xaos.rs:29-40, 128-135): read when some weight differs from 1; missing entries are 1.
         self.xaos = None

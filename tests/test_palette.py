@@ -120,7 +120,58 @@ def test_squeeze_mode_names():
         _native.specialize(json.dumps(cfg))
 
 
+def test_speed_colour_known_answer(oracle):
+    """Speed colour mode (main_template.wgsl:483-506, utilities.wgsl:148-156):
+    two constant transforms that xaos makes alternate, so every step moves
+    |2P| = 1; with speed_factor 1 each sample carries the palette's entry
+    at clamp(ln(10 + 1) / 3, 0, 1)."""
+    t = [{"a": 0, "b": 0, "c": 0, "d": 0, "e": 0.3 * s, "f": 0.4 * s, "weight": 1.0, "color": 0.0,
+          "variations": {"linear": 1.0}} for s in (1.0, -1.0)]
+    cfg = {"flame": {"transforms": t, "xaos": [[0, 1], [1, 0]]}, "deterministic_rng": True, "palette": RAMP,
+           "color_mode": "speed", "speed_factor": 1.0}
+    fl = oracle.Flame(cfg, 64, 48)
+    _, inframe, cnt, rgb = fl.render(256, 100, threads=4)
+    lit = np.argwhere(cnt > 0)
+    assert len(lit) == 2
+    speed = F(np.sqrt(F(F(0.6) * F(0.6)) + F(F(0.8) * F(0.8))))
+    entry = table(oracle)[int(np.floor(F(np.log(F(speed * F(10)) + F(1)) / F(3)) * F(256)))]
+    for y, x in lit:
+        np.testing.assert_allclose(rgb[y, x] / cnt[y, x], entry, rtol=1e-6)
+
+
+def test_speed_mode_names():
+    cfg = {"flame": {"transforms": [{"a": 1, "b": 0, "c": 0, "d": 1, "e": 0, "f": 0, "weight": 1, "color": 0,
+                                     "variations": {"linear": 1.0}}]}, "color_mode": "Speed"}
+    _, src = _native.specialize(json.dumps(cfg))
+    assert "#define FFB_SPEED 1" in src
+    cfg["color_mode"] = "PathMap"
+    with pytest.raises(EngineError, match="colour mode"):
+        _native.specialize(json.dumps(cfg))
+
+
 # --------------------------------------------------------------------- GPU --
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rng_mode", ["philox", "pcg"])
+def test_speed_colour_render(renderer, oracle, rng_mode):
+    """A linear flame in speed colour mode: the same counts as the oracle,
+    bit for bit, and the same colour sums but where a log's last bit moved
+    a step's speed across a palette entry (rare; the colour then differs by
+    one entry, mixed in by speed_factor)."""
+    t = [{"a": 0.5, "b": 0, "c": 0, "d": 0.5, "e": e, "f": f, "weight": w, "color": 0.0,
+          "variations": {"linear": 1.0}} for e, f, w in ((0.0, 0.5, 1.0), (-0.5, -0.5, 0.7), (0.5, -0.5, 1.3))]
+    cfg = {"flame": {"transforms": t}, "deterministic_rng": True, "palette": RAMP, "color_mode": "speed",
+           "speed_factor": 0.3}
+    W, H, walkers, per = 96, 64, 2048, 300
+    cnt, rgb, out = renderer.histogram_u64(cfg, W, H, iterations=walkers * per, walkers=walkers, count_bits=64,
+                                           rng=rng_mode, iterations_per_thread=256)
+    fl = oracle.Flame(cfg, W, H)
+    _, inframe, rc, rrgb = fl.render(walkers, per + 20, rng=rng_mode, ipt=256, threads=8)
+    assert np.array_equal(cnt.astype(np.int64), rc.astype(np.int64)) and inframe == out.inframe_samples
+    lit = cnt > 0
+    close = np.isclose(rgb[lit], rrgb[lit], rtol=1e-4, atol=1e-4).all(axis=1)
+    assert close.mean() > 0.99, close.mean()
+
 
 @pytest.mark.gpu
 def test_render_colours_go_through_the_pipeline(renderer, oracle):
