@@ -515,6 +515,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     if (p.defer) s << "#define FFB_DEFER 1\n#define FFB_NFD " << nfd << "\n";
     s << "#define FFB_SYM_KIND " << p.sym_kind << "\n#define T_SYM " << p.t_sym << "\n";
     if (p.xaos) s << "#define FFB_XAOS 1\n#define T_XAOS " << p.t_xaos << "\n";
+    if (f.orbit_refresh) s << "#define FFB_REFRESH " << f.orbit_refresh << "\n";
     s << "#define FFB_NSTATE " << p.n_state << "\n#define FFB_NINIT " << p.n_init << "\n#define T_ST " << p.t_st
       << "\n#define T_INIT " << p.t_init << "\n";
     if (p.dc) s << "#define FFB_DC 1\n";

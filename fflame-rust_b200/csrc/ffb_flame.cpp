@@ -387,9 +387,7 @@ Flame parse_config(const Json& cfg) {
         if (any) {
             if (n > 64) fail("xaos over more than 64 transforms is not supported by this build");
             F.xaos = m;
-            if (xaos_walk_splits_orbits(F))
-                fail("this xaos chain's walk splits orbits between closed groups, which needs the reference's orbit "
-                     "refresh (compute_kernel.rs:45-60); not supported by this build");
+            if (xaos_walk_splits_orbits(F)) F.orbit_refresh = 4;           // ORBIT_REFRESH_PERIOD
         }
     }
     if (const Json* so = fl->get("solo_transform"); so && so->kind == Json::Number)

@@ -148,6 +148,10 @@ struct Flame {
     // Xaos (utilities.wgsl:106-137): row-major n_xf x n_xf transition
     // weights, empty when every weight is 1 (Flame::has_xaos, xaos.rs:29-40).
     std::vector<float> xaos;
+    // Orbit refresh (compute_kernel.rs:45-60; main_template.wgsl:125-145):
+    // where the xaos walk decides which closed group an orbit ends in, every
+    // dispatch restarts the walkers w with (w + the dispatch's seed) % 4 == 0.
+    uint32_t orbit_refresh = 0;
     float zoom = 1.0f;
     double pan_x = 0.0, pan_y = 0.0;
     float rotation = 0.0f;

@@ -36,8 +36,9 @@ __device__ __forceinline__ FfbCtx ffb_ctx(const ffb_launch& J, u32 gw, u64 it) {
 // klein_group's previous generator, floor(r * 4) (klein_group_misc.rs:227-231).
 // With the reference's stream the draw is taken at every dispatch start
 // (ffb_pcg_dispatch); with the counter-based stream it is Philox counter
-// (walker, 0xFFFFFFFE, entry / 4, 0xFFFFFFFF), once.
-__device__ __forceinline__ void ffb_state_fresh(const float* __restrict__ sm, const ffb_launch& J, u32 gw) {
+// (walker, 0xFFFFFFFE, entry / 4 + 256 d, 0xFFFFFFFF) for a walker (re)started
+// at dispatch d.
+__device__ __forceinline__ void ffb_state_fresh(const float* __restrict__ sm, const ffb_launch& J, u32 gw, u32 d = 0u) {
     float* st = J.state + (gw - J.walker0);
     for (int s = 0; s < FFB_NSTATE; ++s) st[(size_t)s * J.n_walkers] = 0.0f;
 #ifdef FFB_SPEED
@@ -45,12 +46,12 @@ __device__ __forceinline__ void ffb_state_fresh(const float* __restrict__ sm, co
 #endif
 #if FFB_RNG_MODE == 1
     for (int i = 0; i < FFB_NINIT; ++i) {
-        const uint4 o = philox4(J.seed_lo, J.seed_hi, gw, 0xFFFFFFFEu, (u32)(i >> 2), 0xFFFFFFFFu);
+        const uint4 o = philox4(J.seed_lo, J.seed_hi, gw, 0xFFFFFFFEu, (u32)(i >> 2) | (d << 8), 0xFFFFFFFFu);
         const u32 wd = (i & 3) == 0 ? o.x : (i & 3) == 1 ? o.y : (i & 3) == 2 ? o.z : o.w;
         st[(size_t)ffb_u32(sm[T_INIT + i]) * J.n_walkers] = floorf(u24(wd) * 4.0f);
     }
 #else
-    (void)sm;
+    (void)sm; (void)d;
 #endif
 }
 #endif
@@ -258,21 +259,68 @@ __device__ __forceinline__ void ffb_start(const float* __restrict__ sm, const ff
 // A dispatch boundary of the reference's stream: re-seeded per dispatch, the
 // two start draws consumed before the orbit resumes (main_template.wgsl:25-55,
 // 125-181; compute_kernel.rs:3541-3553).
-__device__ __forceinline__ void ffb_pcg_dispatch(const ffb_launch& J, PcgRng& rng, u32 gw, u64 it, float& x, float& y) {
+__device__ __forceinline__ void ffb_pcg_dispatch(const float* __restrict__ sm, const ffb_launch& J, PcgRng& rng, u32 gw, u64 it,
+                                                 float& x, float& y, float& ci, u32& fuse, int& prev) {
     if (it == J.it0 || (J.ipt != 0 && it % J.ipt == 0)) {
         u32 d = J.ipt ? (u32)(it / J.ipt) : 0u;
-        rng.init(gw, J.seed_lo + d * 2654435761u);
+        const u32 seed_d = J.seed_lo + d * 2654435761u;
+        rng.init(gw, seed_d);
         float s0 = rng.draw(0), s1 = rng.draw(0);
-        if (it == 0) { x = s0 * 2.0f - 1.0f; y = s1 * 2.0f - 1.0f; }
+        bool fresh = it == 0;
+#ifdef FFB_REFRESH
+        // Orbit refresh (main_template.wgsl:125-145, compute_kernel.rs:45-60):
+        // this dispatch starts the walkers w with (w + seed) % period == 0
+        // again -- point from the start draws, colour 0, burn-in, the
+        // stratified first pick, fresh state.
+        if (!fresh && J.ipt != 0 && it % J.ipt == 0 && (gw + seed_d) % (u32)FFB_REFRESH == 0u) {
+            fresh = true;
+            ci = 0.0f;
+            fuse = J.burn_in;
+#ifdef FFB_XAOS
+            prev = ffb_xaos_first(sm, (int)J.n_xf, gw, seed_d);
+#endif
+#if FFB_NSTATE > 0
+            ffb_state_fresh(sm, J, gw, d);
+#endif
+        }
+#endif
+        if (fresh) { x = s0 * 2.0f - 1.0f; y = s1 * 2.0f - 1.0f; }
 #if FFB_NINIT > 0
         // The state-init block (main_template.wgsl:117-122) draws every
         // dispatch; a resumed orbit then restores its state over it.
         for (int i = 0; i < FFB_NINIT; ++i) {
             const float r = rng.draw(0);
-            if (it == 0) J.state[(size_t)ffb_u32(J.table[T_INIT + i]) * J.n_walkers + (gw - J.walker0)] = floorf(r * 4.0f);
+            if (fresh) J.state[(size_t)ffb_u32(J.table[T_INIT + i]) * J.n_walkers + (gw - J.walker0)] = floorf(r * 4.0f);
         }
 #endif
     }
+    (void)sm; (void)ci; (void)fuse; (void)prev;
+}
+#endif
+
+#if defined(FFB_REFRESH) && FFB_RNG_MODE == 1
+// Orbit refresh with the counter-based stream: at each dispatch boundary
+// (every ipt iterations) the walkers w with (w + seed_d) % period == 0 start
+// again, seed_d = seed + d * 2654435761 as the reference's dispatch seeds;
+// the point from Philox counter (walker, 0xFFFFFFFF, d, 0xFFFFFFFD).
+__device__ __forceinline__ void ffb_refresh(const float* __restrict__ sm, const ffb_launch& J, u32 gw, u64 it, float& x, float& y,
+                                            float& ci, u32& fuse, int& prev) {
+    if (it == 0 || J.ipt == 0 || it % J.ipt != 0) return;
+    const u32 d = (u32)(it / J.ipt);
+    const u32 seed_d = J.seed_lo + d * 2654435761u;
+    if ((gw + seed_d) % (u32)FFB_REFRESH != 0u) return;
+    const uint4 o = philox4(J.seed_lo, J.seed_hi, gw, 0xFFFFFFFFu, d, 0xFFFFFFFDu);
+    x = u24(o.x) * 2.0f - 1.0f;
+    y = u24(o.y) * 2.0f - 1.0f;
+    ci = 0.0f;
+    fuse = J.burn_in;
+#ifdef FFB_XAOS
+    prev = ffb_xaos_first(sm, (int)J.n_xf, gw, seed_d);
+#endif
+#if FFB_NSTATE > 0
+    ffb_state_fresh(sm, J, gw, d);
+#endif
+    (void)prev;
 }
 #endif
 
@@ -483,8 +531,11 @@ __device__ __forceinline__ void ffb_chaos_walker(const float* __restrict__ sm, c
     const u64 it1 = J.it0 + J.n_iters;
     for (u64 it = J.it0; it < it1; ++it) {
 #if FFB_RNG_MODE == 0
-        ffb_pcg_dispatch(J, rng, gw, it, x, y);
+        ffb_pcg_dispatch(sm, J, rng, gw, it, x, y, ci, fuse, prev);
 #else
+#ifdef FFB_REFRESH
+        ffb_refresh(sm, J, gw, it, x, y, ci, fuse, prev);
+#endif
         PhiloxRng rng;
         rng.fill(J.seed_lo, J.seed_hi, gw, it);
 #endif
@@ -562,11 +613,14 @@ ffb_chaos_sorted(const ffb_launch* __restrict__ jobs, int n_jobs) {
         u32 r0 = 0, r1 = 0;
         if (active) {
 #if FFB_RNG_MODE == 0
-            ffb_pcg_dispatch(J, rng, wid, it, x, y);
+            ffb_pcg_dispatch(sm, J, rng, wid, it, x, y, ci, fuse, prev);
             k = FFB_PICK(rng.draw(0), prev);
             plot = rng.draw(1) < sm[T_XF + F_OPAC * FFB_MAXX + k];
             r0 = rng.state; r1 = rng.inc;
 #else
+#ifdef FFB_REFRESH
+            ffb_refresh(sm, J, wid, it, x, y, ci, fuse, prev);
+#endif
             PhiloxRng rng;
             rng.fill(J.seed_lo, J.seed_hi, wid, it);
             k = FFB_PICK(rng.draw(0), prev);

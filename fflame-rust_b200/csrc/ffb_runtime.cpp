@@ -314,6 +314,8 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     P.burn_in = job->burn_in ? job->burn_in : 20;
     // An xaos walker's stored state holds its previous transform above the burn-in left.
     if (!P.flame.xaos.empty() && P.burn_in >= (1u << 24)) fail(FFB_ERR_INVALID, "burn_in must be below 2^24 with xaos");
+    if (P.flame.orbit_refresh && P.flame.filter.on())
+        fail(FFB_ERR_INVALID, "the spatial filter with an xaos chain that needs orbit refresh is not supported by this build");
     P.ipt = job->iterations_per_thread ? job->iterations_per_thread : 1024;
     P.target = job->iterations ? job->iterations : P.flame.max_iterations * (uint64_t)P.ss * P.ss;
     uint64_t w = job->walkers;
@@ -424,6 +426,30 @@ std::vector<float> de_table(double r_max, double r_min, double curve, int& n_out
 
 void check_de(const Flame& f, uint32_t ss) {
     if (f.de.max_radius * ss > 36.0f) fail(FFB_ERR_INVALID, "density estimation radius too large (at most 36 histogram pixels)");
+}
+
+// The render's plotted samples -- each walker's iterations past its burn-in
+// (OrbitFuses::dispatch, compute_kernel.rs:85-101).  With orbit refresh a
+// walker restarted at dispatch d (every ipt iterations, (w + seed_d) %
+// period == 0, seed_d = seed + d * 2654435761) burns in again.
+uint64_t plotted_samples(const Prepared& P, uint32_t walker0) {
+    const uint32_t period = P.flame.orbit_refresh;
+    if (!period || P.ipt == 0) return (uint64_t)P.walkers * P.per_walker;
+    const uint64_t total = P.per_walker + P.burn_in, ipt = P.ipt;
+    uint64_t plotted = 0;
+    for (uint32_t w = 0; w < P.walkers; ++w) {
+        const uint32_t gw = walker0 + w;
+        uint64_t left = P.burn_in;
+        for (uint64_t it0 = 0; it0 < total; it0 += ipt) {
+            const uint64_t n = std::min(ipt, total - it0);
+            const uint32_t seed_d = (uint32_t)P.seed + (uint32_t)(it0 / ipt) * 2654435761u;
+            if (it0 > 0 && (gw + seed_d) % period == 0u) left = P.burn_in;
+            const uint64_t burnt = std::min(left, n);
+            plotted += n - burnt;
+            left -= burnt;
+        }
+    }
+    return plotted;
 }
 
 // Chaos game of a prepared flame into r->hist (wi*hi float4, cleared here).
@@ -675,7 +701,7 @@ void render_device(ffb_renderer* r, const char* config, size_t len, const ffb_jo
     static thread_local uint64_t inframe_slot;
     if (sync) h_inframe = &inframe_slot;
     run_chaos(r, P, s, job->walker0, h_inframe);
-    const uint64_t plotted = (uint64_t)P.walkers * P.per_walker;
+    const uint64_t plotted = plotted_samples(P, job->walker0);
     finish_device(r, P, (const float4*)r->hist.p, plotted, 0, job->height, job->transparent, d_rgba, s);
     ck(cudaEventRecord(r->ev1, s), "event");
     if (out) {
@@ -927,7 +953,7 @@ FFB_API int ffb_histogram(ffb_renderer* r, const char* config, size_t len, const
             float ms = 0.f;
             cudaEventElapsedTime(&ms, r->ev0, r->ev1);
             out->width = P.wi; out->height = P.hi;
-            out->total_iterations = (uint64_t)P.walkers * P.per_walker;
+            out->total_iterations = plotted_samples(P, job->walker0);
             out->inframe_samples = inframe;
             out->render_time_ms = ms;
             r->fill_counts(out);
@@ -963,7 +989,7 @@ FFB_API int ffb_histogram_f32(ffb_renderer* r, const char* config, size_t len, c
             float ms = 0.f;
             cudaEventElapsedTime(&ms, r->ev0, r->ev1);
             out->width = P.wi; out->height = P.hi;
-            out->total_iterations = (uint64_t)P.walkers * P.per_walker;
+            out->total_iterations = plotted_samples(P, job->walker0);
             out->inframe_samples = inframe;
             out->render_time_ms = ms;
             r->fill_counts(out);
@@ -1022,7 +1048,7 @@ FFB_API int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t len, c
             float ms = 0.f;
             cudaEventElapsedTime(&ms, r->ev0, r->ev1);
             out->width = P.wi; out->height = P.hi;
-            out->total_iterations = (uint64_t)P.walkers * P.per_walker;
+            out->total_iterations = plotted_samples(P, job->walker0);
             out->inframe_samples = inframe;
             out->render_time_ms = ms;
             r->fill_counts(out);
@@ -1177,7 +1203,7 @@ FFB_API int ffb_chaos_device(ffb_renderer* r, const char* config, size_t len, co
         if (out) {
             *out = ffb_output{};
             out->width = P.wi; out->height = P.hi;
-            out->total_iterations = (uint64_t)P.walkers * P.per_walker;
+            out->total_iterations = plotted_samples(P, job->walker0);
             r->fill_counts(out);
         }
     });

@@ -76,8 +76,14 @@ def render(backend, config, width, height, iterations, walkers, supersample=1, g
     base = dict(job, width=width, height=height, supersample=supersample)
     shard_job = dict(base, walkers=nw, walker0=w0 + base.get("walker0", 0), iterations=nw * per_walker)
     hist = backend.empty(npx * 4, torch.float32)
-    backend.chaos(cfg, shard_job, hist)
-    samples = walkers * per_walker
+    # Each rank's plotted samples (its walkers past their burn-in, restarted
+    # walkers of an orbit-refreshed flame burning in again), summed.
+    samples = int(backend.chaos(cfg, shard_job, hist))
+    if world > 1:
+        total = backend.empty(1, torch.int64)
+        total.fill_(samples)
+        dist.all_reduce(total, op=dist.ReduceOp.SUM, group=group)
+        samples = int(total.item())
     if world > 1:
         counts = backend.empty(npx, torch.int32)
         rgb = backend.empty(npx * 3, torch.float32)

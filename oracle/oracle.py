@@ -135,7 +135,37 @@ class OFlame(ctypes.Structure):
         ("att", ctypes.POINTER(ctypes.c_int)),
         ("color_mode", ctypes.c_int),
         ("speed_factor", ctypes.c_float),
+        ("orbit_refresh", ctypes.c_int),
     ]
+
+
+def walk_splits_orbits(weights, xaos):
+    """xaos.rs:66-123: whether the xaos walk (not the first pick) decides
+    which closed group of the chain an orbit ends in.  Transitions go where
+    weight x xaos > 0 (a row with none goes to transform 0); a closed group
+    is a set the chain never leaves; a start is a transform of positive weight."""
+    n = len(weights)
+    nxt = []
+    for i in range(n):
+        row = [j for j in range(n) if max(weights[j], 0.0) * xaos[i][j] > 0.0] or [0]
+        nxt.append(row)
+    reach = []
+    for s0 in range(n):
+        seen, stack = {s0}, [s0]
+        while stack:
+            i = stack.pop()
+            for j in nxt[i]:
+                if j not in seen:
+                    seen.add(j)
+                    stack.append(j)
+        reach.append(seen)
+    starts = [i for i in range(n) if weights[i] > 0.0]
+    live = set().union(*(reach[i] for i in starts)) if starts else set()
+    closed = [i for i in sorted(live)
+              if all(i in reach[j] for j in reach[i]) and not any(j < i and i in reach[j] and j in reach[i] for j in range(n))]
+    if len(closed) < 2:
+        return False
+    return any(sum(1 for c in closed if c in reach[i]) > 1 for i in starts)
 
 
 ATTACH = 32        # a chain's length at most (MAX_ATTACHMENTS_PER_TRANSFORM)
@@ -321,6 +351,8 @@ class Flame:
             if any(abs(f32(v) - 1.0) > 1e-6 for row in flame["xaos"] for v in row):
                 self.xaos = np.ascontiguousarray(m.ravel())
                 s.xaos = _fp(self.xaos)
+                if walk_splits_orbits([f32(t.get("weight", 1.0)) for t in normals], m.tolist()):
+                    s.orbit_refresh = 4                                    # ORBIT_REFRESH_PERIOD
         ps = flame.get("post_symmetry")
         if ps:
             s.sym_kind = {"none": 0, "xaxis": 1, "yaxis": 2, "point": 3}[ps.get("ty", "none")]

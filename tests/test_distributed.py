@@ -32,11 +32,12 @@ class OracleBackend:
         W, H = job["width"] * ss, job["height"] * ss
         fl = self.O.Flame(c, W, H)
         per = job["iterations"] // job["walkers"]
-        _, _, cnt, rgb = fl.render(job["walkers"], per + 20, seed=job.get("seed", 12345), walker0=job["walker0"], threads=2)
+        plotted, _, cnt, rgb = fl.render(job["walkers"], per + 20, seed=job.get("seed", 12345), walker0=job["walker0"],
+                                         threads=2)
         h = hist.view(-1, 4)
         h[:, :3] = torch.from_numpy(rgb.reshape(-1, 3).astype(np.float32))
         h[:, 3] = torch.from_numpy(cnt.reshape(-1).view(np.float32))
-        return job["walkers"] * per
+        return plotted
 
     def pack(self, hist, counts, rgb):
         h = hist.view(-1, 4)

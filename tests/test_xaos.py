@@ -3,11 +3,15 @@ scene/xaos.rs): the next transform is picked with weight_i x
 xaos[prev][i], a starting walker's previous transform is the unconditioned
 pick at a Kronecker point of its index (walker * 2654435769 + seed), and a
 chain whose walk (not the first pick) splits orbits between closed groups
-needs the reference's orbit refresh, which this build refuses.
+gets the reference's orbit refresh: every dispatch restarts the walkers w
+with (w + the dispatch's seed) % 4 == 0 (compute_kernel.rs:45-101).
 
-CPU: parsing, the refusal, the oracle's walk on chains with known answers.
+CPU: parsing, the refresh decision, the oracle's walk on chains with known
+answers (with refresh, each closed group's share of the samples tends to
+its weight's share).
 GPU: bit-identical count planes against the oracle for a linear flame with
-xaos (both RNG modes, both schedules).
+xaos (both RNG modes, both schedules), with refresh across launches, and
+the plotted-sample count the refresh leaves.
 """
 
 import json
@@ -46,16 +50,45 @@ def test_xaos_specializes_and_all_ones_is_plain():
     assert "#define FFB_XAOS" not in src
 
 
-def test_a_walk_that_splits_orbits_is_refused():
+def test_a_walk_that_splits_orbits_is_refreshed(oracle):
     # Transform 0 leads to 1 and 2, each of which only returns to itself:
     # where an orbit ends is decided by the walk, not the first pick.
     cfg = synthetic.sierpinski()
     cfg["flame"]["xaos"] = [[0, 1, 1], [0, 1, 0], [0, 0, 1]]
-    with pytest.raises(EngineError, match="orbit refresh"):
-        _native.specialize(json.dumps(cfg))
-    # Closed groups picked by the first transform alone are fine (the stratified start).
+    _, src = _native.specialize(json.dumps(cfg))
+    assert "#define FFB_REFRESH 4" in src
+    assert oracle.walk_splits_orbits([1.0, 1.0, 1.0], cfg["flame"]["xaos"])
+    # Closed groups picked by the first transform alone need none (the stratified start).
     cfg["flame"]["xaos"] = [[1, 0, 0], [0, 1, 0], [0, 0, 1]]
-    assert _native.specialize(json.dumps(cfg))[0] > 0
+    _, src = _native.specialize(json.dumps(cfg))
+    assert "#define FFB_REFRESH" not in src
+    assert not oracle.walk_splits_orbits([1.0, 1.0, 1.0], cfg["flame"]["xaos"])
+
+
+def split_chain():
+    """A start transform that leads to one of two absorbing constant
+    transforms, weights 1 : 3."""
+    cfg = two_points([[0, 1, 1], [0, 1, 0], [0, 0, 1]], w=(1.0, 3.0))
+    cfg["flame"]["transforms"].insert(0, {"a": 0.5, "b": 0, "c": 0, "d": 0.5, "e": 0, "f": 0, "weight": 2.0,
+                                          "color": 0.5, "variations": {"linear": 1.0}})
+    return cfg
+
+
+@pytest.mark.parametrize("rng", ["philox", "pcg"])
+def test_refresh_shares_the_groups_by_weight(oracle, rng):
+    """Without refresh an orbit stays in the group its walk first entered;
+    with it a quarter restart each dispatch, and over many dispatches the
+    two absorbing pixels split the samples as their weights (1 : 3) to
+    within sampling noise."""
+    cfg = split_chain()
+    fl = oracle.Flame(cfg, 64, 32)
+    walkers, ipt, per = 4000, 32, 32 * 60
+    plotted, inframe, cnt, _ = fl.render(walkers, per + 20, rng=rng, ipt=ipt, threads=4)
+    lit = sorted(int(v) for v in cnt[cnt > 0])
+    assert len(lit) == 2
+    share = lit[0] / (lit[0] + lit[1])
+    assert abs(share - 0.25) < 0.02, share
+    assert plotted < walkers * per                       # restarted walkers burn in again
 
 
 def test_identity_xaos_keeps_each_walker_in_its_first_transform(oracle):
@@ -109,6 +142,23 @@ def test_histogram_bit_exact_with_xaos(renderer, oracle, rng_mode, schedule):
     plotted, inframe, rc, _ = fl.render(walkers, per + 20, rng=rng_mode, ipt=256, threads=8)
     assert out.total_iterations == plotted
     assert int(cnt.sum()) == inframe
+    assert np.array_equal(cnt, rc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rng_mode", ["philox", "pcg"])
+@pytest.mark.parametrize("schedule", ["plain", "sorted"])
+def test_refresh_bit_exact(renderer, oracle, rng_mode, schedule):
+    """Orbit refresh: the same restarts, orbits and plotted-sample count as
+    the oracle, over launches of many dispatches."""
+    cfg = split_chain()
+    W, H, walkers, per, ipt = 64, 32, 2048, 70_000, 1024
+    cnt, _, out = renderer.histogram(cfg, W, H, iterations=walkers * per, walkers=walkers, rng=rng_mode,
+                                     iterations_per_thread=ipt, schedule=schedule)
+    fl = oracle.Flame(cfg, W, H)
+    plotted, inframe, rc, _ = fl.render(walkers, per + 20, rng=rng_mode, ipt=ipt, threads=8)
+    assert out.total_iterations == plotted < walkers * per
+    assert int(cnt.sum()) == out.inframe_samples == inframe
     assert np.array_equal(cnt, rc)
 
 
