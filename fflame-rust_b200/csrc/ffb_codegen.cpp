@@ -639,7 +639,7 @@ std::vector<float> make_table(const Plan& p, const Flame& f) {
                                x.post ? 1.0f : 0.0f,
                                (1.0f + x.speed) / 2.0f,                 // main_template.wgsl:499-500
                                x.color * (1.0f - x.speed) / 2.0f,
-                               x.opacity, x.direct_color};
+                               f.solo >= 0 && (int)k != f.solo ? 0.0f : x.opacity, x.direct_color};   // gpu/buffers.rs:531-535
         for (int fld = 0; fld < 17; ++fld) t[p.t_xf + fld * M + k] = rec[fld];
         for (size_t j = 0; j < p.normal.size(); ++j) {
             const VarDef* v = p.normal[j];

@@ -390,8 +390,10 @@ Flame parse_config(const Json& cfg) {
             if (xaos_walk_splits_orbits(F)) F.orbit_refresh = 4;           // ORBIT_REFRESH_PERIOD
         }
     }
-    if (const Json* so = fl->get("solo_transform"); so && so->kind == Json::Number)
-        fail("a solo transform is not supported by this build");
+    if (const Json* so = fl->get("solo_transform"); so && so->kind == Json::Number) {
+        if (!(so->num >= 0.0) || so->num != std::floor(so->num)) fail("`solo_transform` is not a usize");
+        F.solo = so->num < 1e9 ? (int)so->num : 1000000000;
+    }
     if (const Json* ft = fl->get("final_transforms"); ft && ft->kind == Json::Array)
         for (auto& t : ft->arr) F.fin.push_back(parse_transform(*t));
     // A legacy singular final joins the pool attached to every normal

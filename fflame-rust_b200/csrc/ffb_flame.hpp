@@ -144,6 +144,10 @@ struct Flame {
     std::vector<int> lnk_used;          // linked transforms some normal attaches, pool order
     std::vector<const VarDef*> local;   // local variation order (parent, then subflames)
     std::vector<SubFlame> sub;          // at most 8 (MAX_SUBFLAMES, buffers.rs:36-44)
+    // The solo transform (Apophysis soloxform; gpu/buffers.rs:523-536):
+    // every other normal transform still moves the walk but plots nothing
+    // (opacity 0); -1 none.
+    int solo = -1;
     SpatialFilter filter;
     // Xaos (utilities.wgsl:106-137): row-major n_xf x n_xf transition
     // weights, empty when every weight is 1 (Flame::has_xaos, xaos.rs:29-40).

@@ -302,13 +302,16 @@ class Flame:
         self.xf = np.zeros(len(allx) * XF_STRIDE, np.float32)
         self.var_w = np.zeros(len(allx) * max(nv, 1), np.float32)
         self.var_p = np.zeros(len(allx) * max(nv, 1) * SLOTS, np.float32)
+        solo = flame.get("solo_transform")
         for i, t in enumerate(allx):
             post = bool(t.get("post_affine_enabled", False))      # transforms.rs:1542; buffers.rs:467
+            # The solo transform (buffers.rs:523-536): the other normals plot nothing.
+            opacity = 0.0 if solo is not None and i < len(normals) and i != solo else t.get("opacity", 1.0)
             rec = [t["a"], t["b"], t["c"], t["d"], t["e"], t["f"],
                    t.get("post_a", 1.0), t.get("post_b", 0.0), t.get("post_c", 0.0),
                    t.get("post_d", 1.0), t.get("post_e", 0.0), t.get("post_f", 0.0),
                    1.0 if post else 0.0, t.get("weight", 1.0), t.get("color", 0.5),
-                   t.get("color_speed", 0.0), t.get("opacity", 1.0), t.get("direct_color", 0.0)]
+                   t.get("color_speed", 0.0), opacity, t.get("direct_color", 0.0)]
             self.xf[i * XF_STRIDE:(i + 1) * XF_STRIDE] = rec
             for v, n in enumerate(self.names):
                 self.var_w[i * nv + v] = t["variations"].get(n, 0.0)

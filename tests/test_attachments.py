@@ -1,6 +1,7 @@
 """Linked transforms and per-transform final chains (the attachments of
 transforms.rs:470-480, gpu/buffers.rs:600-680; main_template.wgsl:320-360
-and 663-717).
+and 663-717), and the solo transform (gpu/buffers.rs:523-536: every other
+normal transform keeps moving the walk but plots nothing).
 
 After the chaos game picks normal transform k, its linked chain runs in the
 same iteration -- affine, variations, post-affine each, every output the
@@ -128,7 +129,28 @@ def test_each_normal_plots_through_its_own_finals(oracle, rng):
     assert a + b == inframe and abs(a - b) < 0.05 * inframe
 
 
+def test_solo_transform_plots_alone(oracle):
+    cfg = {"flame": {"transforms": [xf(a=0, b=0, c=0, d=0, e=0.5, f=0.5), xf(a=0, b=0, c=0, d=0, e=-0.5, f=-0.5)],
+                     "solo_transform": 1}, "deterministic_rng": True}
+    assert _native.specialize(json.dumps(cfg))[0] > 0
+    fl, inframe, cnt = one_pixel(oracle, cfg)
+    lit = np.argwhere(cnt > 0)
+    assert len(lit) == 1 and tuple(lit[0][::-1]) == fl.world_to_pixel(-0.5, -0.5)
+    cfg["flame"]["solo_transform"] = -1
+    with pytest.raises(EngineError, match="solo_transform"):
+        _native.specialize(json.dumps(cfg))
+
+
 # --------------------------------------------------------------------- GPU --
+
+@pytest.mark.gpu
+def test_solo_transform_bit_exact(renderer, oracle):
+    cfg = chained()
+    cfg["flame"]["solo_transform"] = 1
+    cnt, rc = gpu_vs_oracle(renderer, oracle, cfg, 96, 64, 2048, 300)
+    assert np.array_equal(cnt, rc)
+
+
 
 def gpu_vs_oracle(renderer, oracle, cfg, W, H, walkers, per, **job):
     rng = job.get("rng", "philox")
