@@ -151,6 +151,11 @@ struct ffb_renderer {
     cudaStream_t plot_stream = nullptr;
     cudaEvent_t ev_main[2] = {nullptr, nullptr}, ev_plot[2] = {nullptr, nullptr}, ev_start = nullptr;
     DevBuf rec[2], rec_draws[2];
+    cudaEvent_t ev_flight[2] = {nullptr, nullptr};          // RenderProgress: launches in flight
+    void ensure_flight_events() {
+        for (auto& e : ev_flight)
+            if (!e) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    }
     void ensure_plot_stream() {
         if (plot_stream) return;
         ck(cudaStreamCreateWithFlags(&plot_stream, cudaStreamNonBlocking), "plot stream");
@@ -186,6 +191,7 @@ struct ffb_renderer {
             cudaEventDestroy(ev_start);
             cudaStreamDestroy(plot_stream);
         }
+        for (auto e : ev_flight) if (e) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -271,6 +277,9 @@ struct Prepared {
     uint32_t accumulate = 0;    // exact mode: 0 auto, 1 direct, 2 tile-sorted
     bool threads_set = false;   // the job chose the block size (the sorted schedule's sorting group too)
     uint32_t plot = 0;          // 0 auto, 1 inline, 2 deferred (the plot in its own kernel)
+    void (*progress)(void*, uint64_t, uint64_t) = nullptr;   // RenderProgress (render.rs:293-301)
+    int (*cancelled)(void*) = nullptr;
+    void* progress_user = nullptr;
 };
 
 // Whether a render accumulates by tiles: exact mode, tile-sorted
@@ -339,6 +348,9 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
         fail(FFB_ERR_INVALID, "tile-sorted accumulation records palette indices: not with the speed colour mode");
     P.plot = job->plot;
     if (P.plot > 2) fail(FFB_ERR_INVALID, "plot must be 0 (auto), 1 (inline) or 2 (deferred)");
+    P.progress = job->progress;
+    P.cancelled = job->cancelled;
+    P.progress_user = job->progress_user;
     const bool tiled = tiled_accumulation(P);
     // Deferred plotting needs the counter-based stream (a launch of any
     // length resumes it) and plots straight into the histogram.
@@ -581,14 +593,34 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         ck(cudaEventRecord(r->ev_start, s), "event");                          // the clears and uploads before
         ck(cudaStreamWaitEvent(r->plot_stream, r->ev_start, 0), "plot stream waits");
     }
+    // RenderProgress: a cancel is looked at before each launch, progress
+    // reported after it; with either, at most two launches are in flight
+    // (each waits for the one two before it).
+    const bool watched = P.progress || P.cancelled;
+    if (watched) r->ensure_flight_events();
+    const uint64_t plotted_total = (uint64_t)P.walkers * P.per_walker;
     for (size_t i = 0; i < ls.size(); ++i) {
         Launch* jp = d_jobs + i;
         int nj = 1;
         void* args[] = {&jp, &nj};
+        if (watched && i >= 2) ck(cudaEventSynchronize(r->ev_flight[i % 2]), "launch in flight");
+        if (P.cancelled && P.cancelled(P.progress_user)) {
+            ck(cudaStreamSynchronize(s), "cancel");
+            if (defer) ck(cudaStreamSynchronize(r->plot_stream), "cancel");
+            fail(FFB_ERR_CANCELLED, "render cancelled");
+        }
         if (filt) ck(cudaMemsetAsync(batch, 0, npx * 16, s), "clear batch histogram");
         if (defer && i >= 2) ck(cudaStreamWaitEvent(s, r->ev_plot[i % 2], 0), "record buffer free");
         ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch ffb_chaos");
         r->launches += 1;
+        if (watched) {
+            ck(cudaEventRecord(r->ev_flight[i % 2], s), "event");
+            if (P.progress) {
+                const uint64_t end = ls[i].it0 + ls[i].n_iters;
+                const uint64_t done = end > P.burn_in ? std::min<uint64_t>((uint64_t)P.walkers * (end - P.burn_in), plotted_total) : 0;
+                P.progress(P.progress_user, done, plotted_total);
+            }
+        }
         if (defer) {
             ck(cudaEventRecord(r->ev_main[i % 2], s), "event");
             ck(cudaStreamWaitEvent(r->plot_stream, r->ev_main[i % 2], 0), "plot waits for its samples");
@@ -851,6 +883,10 @@ void fae_dispatch(const Json& r, const uint8_t* data, size_t data_len, std::vect
 // ================================================================ ABI ====
 FFB_API const char* ffb_last_error(void) { return g_err.c_str(); }
 FFB_API const char* ffb_version(void) { return "ffb200 0.1.0 (sm_100a)"; }
+FFB_API void ffb_struct_sizes(size_t* job_bytes, size_t* output_bytes) {
+    if (job_bytes) *job_bytes = sizeof(ffb_job);
+    if (output_bytes) *output_bytes = sizeof(ffb_output);
+}
 
 FFB_API int ffb_flame_import(const char* xml, size_t xml_len, const char** out, size_t* out_len) {
     static thread_local std::string json;

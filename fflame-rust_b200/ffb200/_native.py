@@ -29,7 +29,7 @@ EXPORTS = [
     "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
     "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
     "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize", "ffb_encode_png",
-    "ffb_flame_import", "ffb_histogram_f32", "ffb_hist_filter", "ffb_specialize_job",
+    "ffb_flame_import", "ffb_histogram_f32", "ffb_hist_filter", "ffb_specialize_job", "ffb_struct_sizes",
 ]
 
 
@@ -41,6 +41,10 @@ class EngineError(ValueError):
         self.status = status
 
 
+PROGRESS_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64)
+CANCEL_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+
+
 class Job(ctypes.Structure):
     _fields_ = [
         ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("iterations", ctypes.c_uint64),
@@ -49,6 +53,7 @@ class Job(ctypes.Structure):
         ("transparent", ctypes.c_int32), ("threads", ctypes.c_int32), ("seed", ctypes.c_uint64),
         ("walker0", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("count_bits", ctypes.c_uint32),
         ("accumulate", ctypes.c_uint32), ("plot", ctypes.c_uint32),
+        ("progress", PROGRESS_FN), ("cancelled", CANCEL_FN), ("progress_user", ctypes.c_void_p),
     ]
 
 
@@ -122,7 +127,10 @@ PLOT = {"auto": 0, "inline": 1, "deferred": 2}
 
 def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0, walkers=0, supersample=1,
              rng="philox", math="precise", transparent=0, threads=0, seed=0, walker0=0, schedule="auto", count_bits=32,
-             accumulate="auto", plot="auto"):
+             accumulate="auto", plot="auto", progress=None, cancel=None):
+    """The C job; `progress(current, total)` is called after each launch of
+    the chaos game and `cancel()` returning true before one stops the render
+    (RenderProgress, render.rs:293-301)."""
     j = Job()
     j.width, j.height, j.iterations = width, height, int(iterations or 0)
     j.iterations_per_thread, j.burn_in, j.walkers = iterations_per_thread, burn_in, walkers
@@ -134,6 +142,12 @@ def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0
     j.count_bits = count_bits
     j.accumulate = ACCUMULATE[accumulate] if isinstance(accumulate, str) else accumulate
     j.plot = PLOT[plot] if isinstance(plot, str) else plot
+    if progress is not None:
+        j._progress_cb = PROGRESS_FN(lambda _u, cur, tot: progress(int(cur), int(tot)))
+        j.progress = j._progress_cb
+    if cancel is not None:
+        j._cancel_cb = CANCEL_FN(lambda _u: 1 if cancel() else 0)
+        j.cancelled = j._cancel_cb
     return j
 
 

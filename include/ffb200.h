@@ -100,6 +100,16 @@ typedef struct {
                                           chain, palette, symmetry copies, splat) runs beside the next
                                           launch on a second stream; the same histogram (Philox stream, no
                                           spatial filter, direct accumulation; otherwise inline) */
+    /* RenderProgress (src/renderer/render.rs:293-301, 624-693): `progress`
+       is called after each launch of the chaos game with the plotted
+       samples submitted so far and the render's total; `cancelled`
+       returning nonzero before a launch stops the render (status
+       FFB_ERR_CANCELLED, the histogram partial).  NULL: none.  With either
+       set at most two launches are in flight, so a cancel takes effect
+       within one launch of the chaos game. */
+    void (*progress)(void* user, uint64_t current, uint64_t total);
+    int (*cancelled)(void* user);
+    void* progress_user;
 } ffb_job;
 
 /* RenderOutput (src/renderer/render.rs:207-218). */
@@ -118,6 +128,9 @@ typedef struct ffb_renderer ffb_renderer;   /* FlameRenderer: a device, a stream
 
 /* The calling thread's last error message ("" when none). */
 const char* ffb_last_error(void);
+
+/* sizeof(ffb_job) and sizeof(ffb_output), for bindings to check their layouts. */
+void ffb_struct_sizes(size_t* job_bytes, size_t* output_bytes);
 /* Build version and the device it would use. */
 const char* ffb_version(void);
 

@@ -107,3 +107,36 @@ def test_fae_call_without_a_gpu_answers_data_calls(native):
         m.call({"fn": "flame_import", "xml": "<flame/>"})
     with pytest.raises(native.EngineError):
         m.call({"no": "fn"})
+
+
+def test_struct_layouts_match_the_header(native):
+    """The ctypes mirrors of ffb_job and ffb_output have the C layouts."""
+    import ctypes
+    jb, ob = ctypes.c_size_t(), ctypes.c_size_t()
+    native.lib().ffb_struct_sizes(ctypes.byref(jb), ctypes.byref(ob))
+    assert jb.value == ctypes.sizeof(native.Job) and ob.value == ctypes.sizeof(native.Output)
+
+
+@pytest.mark.gpu
+def test_progress_reports_and_cancel_stops(renderer, native):
+    """RenderProgress (render.rs:293-301, 624-693): progress after each
+    launch, rising to the render's total; a cancel before a launch ends the
+    render with the Cancelled status."""
+    cfg = synthetic.plain_flame(2)
+    seen = []
+    job = dict(iterations=1024 * 300_000, walkers=1024)             # five launches of 65,536 iterations
+    renderer.histogram(cfg, 128, 128, progress=lambda c, t: seen.append((c, t)), **job)
+    assert len(seen) == 5
+    assert all(b[0] > a[0] for a, b in zip(seen, seen[1:]))
+    assert seen[-1][0] == seen[-1][1] == 1024 * 300_000
+    calls = []
+
+    def cancel():
+        calls.append(1)
+        return len(calls) > 2
+    with pytest.raises(native.EngineError) as e:
+        renderer.histogram(cfg, 128, 128, cancel=cancel, **job)
+    assert e.value.status == native.ERR_CANCELLED and len(calls) == 3
+    # The renderer is usable after a cancel.
+    cnt, _, out = renderer.histogram(cfg, 128, 128, **job)
+    assert out.total_iterations == 1024 * 300_000
