@@ -34,6 +34,23 @@ void derive_perspective(const float* u, float* o) {            // simple_classic
     o[1] = u[1] * std::cos(ang);
 }
 
+void derive_log(const float* u, float* o) {                    // advanced.rs (init_log)
+    o[0] = 0.5f / std::log(std::max(u[0], 1.000001f));
+}
+void derive_escher(const float* u, float* o) {                 // advanced.rs (init_escher)
+    const float beta = u[0] * 3.14159265358979f / 180.0f;
+    o[0] = 0.5f * (1.0f + std::cos(beta));
+    o[1] = 0.5f * std::sin(beta);
+}
+void derive_modulus(const float* u, float* o) {                // singleton_misc.rs (init_modulus)
+    o[0] = 2.0f * u[0];
+    o[1] = 2.0f * u[1];
+}
+void derive_curve(const float* u, float* o) {                  // erf_misc.rs (init_curve)
+    o[0] = std::max(u[2] * u[2], 1e-20f);
+    o[1] = std::max(u[3] * u[3], 1e-20f);
+}
+
 // f32 complex arithmetic in the operation order of shaders/core/complex.wgsl:20-69.
 struct Cx { float x, y; };
 Cx cadd(Cx a, Cx b) { return {a.x + b.x, a.y + b.y}; }
@@ -160,6 +177,15 @@ static const VarDef kRegistry[] = {
     {"gaussian_blur", 31, 5, 0, NP, ND, "v_gaussian_blur", 0, 0, nullptr},
     {"polar2", 32, 0, 0, NP, ND, "v_polar2", 0, 0, nullptr},
     {"cross", 33, 0, 0, NP, ND, "v_cross", 0, 0, nullptr},
+    {"loonie", 34, 0, 0, NP, ND, "v_loonie", 0, 0, nullptr},
+    {"scry", 35, 0, 0, NP, ND, "v_scry", 0, 0, nullptr},
+    {"foci", 37, 0, 0, NP, ND, "v_foci", 0, 0, nullptr},
+    {"elliptic", 38, 0, 0, NP, ND, "v_elliptic", 0, 0, nullptr},
+    {"waves2", 39, 0, 6, {"freqx", "scalex", "freqy", "scaley", "freqz", "scalez"}, {2.0f, 1.0f, 2.0f, 1.0f, 0.0f, 0.0f}, "v_waves2", 0, 0, nullptr},
+    {"log", 40, 0, 1, {"base"}, {2.718281828f}, "v_log", 0, 1, derive_log},
+    {"escher", 41, 0, 1, {"beta"}, {0.0f}, "v_escher", 0, 2, derive_escher},
+    {"bipolar", 42, 0, 1, {"shift"}, {0.0f}, "v_bipolar", 0, 0, nullptr},
+    {"lazysusan", 43, 0, 5, {"spin", "space", "twist", "x", "y"}, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_lazysusan", 0, 0, nullptr},
     {"rings2", 44, 0, 1, {"val"}, {1.0f}, "v_rings2", 0, 0, nullptr},
     {"fan2", 45, 0, 2, {"x", "y"}, {1.0f, 0.0f}, "v_fan2", 0, 0, nullptr},
     {"pdj", 46, 0, 4, {"a", "b", "c", "d"}, {0.0f, 0.0f, 0.0f, 0.0f}, "v_pdj", 0, 0, nullptr},
@@ -168,22 +194,45 @@ static const VarDef kRegistry[] = {
     {"splits", 49, 0, 6, {"x", "y", "lshear", "rshear", "ushear", "dshear"}, {0.4f, 0.4f, 0.0f, 0.0f, 0.0f, 0.0f},
      "v_splits", 0, 0, nullptr},
     {"ngon", 50, 0, 4, {"sides", "power", "circle", "corners"}, {5.0f, 3.0f, 1.0f, 2.0f}, "v_ngon", 0, 0, nullptr},
+    {"auger", 51, 0, 4, {"freq", "weight", "scale", "sym"}, {1.0f, 0.5f, 0.5f, 0.0f}, "v_auger", 0, 0, nullptr},
     {"pre_blur", 54, 7, 0, NP, ND, "v_pre_blur", VF_PRE | VF_W, 0, nullptr},
     {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
     {"juliascope", 69, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_juliascope", 0, 0, nullptr},
     {"radial_blur", 73, 4, 1, {"angle"}, {0.0f}, "v_radial_blur", VF_W, 2, derive_radial_blur},
+    {"separation", 77, 0, 4, {"x", "y", "xinside", "yinside"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_separation", 0, 0, nullptr},
+    {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
+    {"sin", 93, 0, 0, NP, ND, "v_sin", 0, 0, nullptr},
+    {"cos", 94, 0, 0, NP, ND, "v_cos", 0, 0, nullptr},
+    {"tan", 95, 0, 0, NP, ND, "v_tan", 0, 0, nullptr},
+    {"sec", 96, 0, 0, NP, ND, "v_sec", 0, 0, nullptr},
+    {"csc", 97, 0, 0, NP, ND, "v_csc", 0, 0, nullptr},
+    {"cot", 98, 0, 0, NP, ND, "v_cot", 0, 0, nullptr},
+    {"sinh", 99, 0, 0, NP, ND, "v_sinh", 0, 0, nullptr},
+    {"cosh", 100, 0, 0, NP, ND, "v_cosh", 0, 0, nullptr},
+    {"tanh", 101, 0, 0, NP, ND, "v_tanh", 0, 0, nullptr},
+    {"coth", 102, 0, 0, NP, ND, "v_coth", 0, 0, nullptr},
+    {"sech", 103, 0, 0, NP, ND, "v_sech", 0, 0, nullptr},
+    {"csch", 104, 0, 0, NP, ND, "v_csch", 0, 0, nullptr},
+    {"exp", 136, 0, 0, NP, ND, "v_exp", 0, 0, nullptr},
     {"tangent", 141, 0, 0, NP, ND, "v_tangent", 0, 0, nullptr},
     {"secant2", 143, 0, 0, NP, ND, "v_secant2", 0, 0, nullptr},
     {"cosine", 144, 0, 0, NP, ND, "v_cosine", 0, 0, nullptr},
     {"pie", 150, 3, 3, {"slices", "rotation", "thickness"}, {6.0f, 0.0f, 0.5f}, "v_pie", 0, 0, nullptr},
     {"butterfly", 152, 0, 0, NP, ND, "v_butterfly", 0, 0, nullptr},
+    {"cell", 161, 0, 1, {"size"}, {0.6f}, "v_cell", 0, 0, nullptr},
+    {"popcorn2", 170, 0, 3, {"x", "y", "c"}, {1.0f, 0.5f, 1.5f}, "v_popcorn2", 0, 0, nullptr},
     {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
+    {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
+    {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
+    {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
+    {"edisc", 337, 0, 0, NP, ND, "v_edisc", VF_W, 0, nullptr},
+    {"curve", 338, 0, 4, {"xamp", "yamp", "xlength", "ylength"}, {0.25f, 0.5f, 1.0f, 1.0f}, "v_curve", 0, 2, derive_curve},
     {"exponential", 341, 0, 0, NP, ND, "v_exponential", 0, 0, nullptr},
     {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},

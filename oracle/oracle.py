@@ -33,6 +33,10 @@ REGISTRY = {
     "split": 248, "stripes": 250, "bent2": 281, "power": 325, "exponential": 341,
     "perspective": 345, "rings": 379, "klein_group": 501, "subflame_wf": 502, "pre_subflame_wf": 503,
     "linear3D": 533,
+    "loonie": 34, "scry": 35, "foci": 37, "elliptic": 38, "waves2": 39, "log": 40, "escher": 41, "bipolar": 42,
+    "lazysusan": 43, "auger": 51, "separation": 77, "mobius": 78, "sin": 93, "cos": 94, "tan": 95, "sec": 96,
+    "csc": 97, "cot": 98, "sinh": 99, "cosh": 100, "tanh": 101, "coth": 102, "sech": 103, "csch": 104, "exp": 136,
+    "cell": 161, "popcorn2": 170, "modulus": 273, "whorl": 302, "flux": 307, "edisc": 337, "curve": 338,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -59,6 +63,23 @@ PARAMS = {
     "subflame_wf": [("subflame_id", 0.0), ("scale", 1.0), ("angle", 0.0), ("offset_x", 0.0), ("offset_y", 0.0),
                     ("offset_z", 0.0), ("colorscale_z", 0.0), ("color_mode", -1.0)],
 }
+PARAMS.update({
+    "waves2": [("freqx", 2.0), ("scalex", 1.0), ("freqy", 2.0), ("scaley", 1.0), ("freqz", 0.0), ("scalez", 0.0)],
+    "log": [("base", 2.718281828)],
+    "escher": [("beta", 0.0)],
+    "bipolar": [("shift", 0.0)],
+    "lazysusan": [("spin", 0.0), ("space", 0.0), ("twist", 0.0), ("x", 0.0), ("y", 0.0)],
+    "auger": [("freq", 1.0), ("weight", 0.5), ("scale", 0.5), ("sym", 0.0)],
+    "separation": [("x", 1.0), ("y", 1.0), ("xinside", 0.0), ("yinside", 0.0)],
+    "mobius": [("re_a", 0.1), ("im_a", 0.2), ("re_b", 0.2), ("im_b", -0.12), ("re_c", -0.15), ("im_c", -0.15),
+               ("re_d", 0.21), ("im_d", 0.1)],
+    "cell": [("size", 0.6)],
+    "popcorn2": [("x", 1.0), ("y", 0.5), ("c", 1.5)],
+    "modulus": [("x", 0.2), ("y", 0.5)],
+    "whorl": [("inside", 0.1), ("outside", 0.2)],
+    "flux": [("spread", 0.3)],
+    "curve": [("xamp", 0.25), ("yamp", 0.5), ("xlength", 1.0), ("ylength", 1.0)],
+})
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)
 WORDS = 64         # draw words an iteration

@@ -1,5 +1,6 @@
-"""The variation registry beyond the benchmark configs' twelve: 54
-variations of the reference's ALL_VARIATIONS (src/variations/defs/*.rs),
+"""The variation registry beyond the benchmark configs' twelve: the
+variations of the reference's ALL_VARIATIONS this build carries
+(src/variations/defs/*.rs),
 their parameters and init-derived values, several draws a body, bodies
 that read their transform's affine or their own weight, and the Pre/Post
 phases (pre_blur, flatten).
@@ -43,7 +44,8 @@ PROBE_AFFINE = (1.0, 0.25, 0.1, -0.3, 0.9, -0.2)       # src/probe/flame.rs:4-12
 # Bodies without transcendental arithmetic: +, -, *, /, sqrt, floor are
 # correctly rounded on both sides, so the results are the same bits.
 EXACT = {"linear", "spherical", "horseshoe", "bubble", "curl", "hyperbolic", "bent", "eyefish", "cross", "rings2",
-         "rectangles", "splits", "butterfly", "fisheye", "stripes", "bent2", "linear3D", "flatten"}
+         "rectangles", "splits", "butterfly", "fisheye", "stripes", "bent2", "linear3D", "flatten", "loonie", "scry",
+         "separation", "mobius", "cell", "modulus"}
 
 
 @pytest.fixture(scope="module")
