@@ -51,6 +51,35 @@ void derive_curve(const float* u, float* o) {                  // erf_misc.rs (i
     o[1] = std::max(u[3] * u[3], 1e-20f);
 }
 
+void derive_disc2(const float* u, float* o) {                  // heavy_init.rs (init_disc2)
+    const float two_pi = 6.28318530717959f;
+    const float twist = u[1];
+    float sinadd = std::sin(twist), cosadd = std::cos(twist) - 1.0f;
+    if (twist > two_pi) { const float k = 1.0f + twist - two_pi; cosadd *= k; sinadd *= k; }
+    if (twist < -two_pi) { const float k = 1.0f + twist + two_pi; cosadd *= k; sinadd *= k; }
+    o[0] = u[0] * 3.14159265358979f;
+    o[1] = cosadd;
+    o[2] = sinadd;
+}
+void derive_cpow(const float* u, float* o) {                   // advanced.rs (init_cpow)
+    const float sp = u[2] == 0.0f ? 1e-30f : u[2];
+    o[0] = 6.28318530717959f / sp;
+    o[1] = u[0] / sp;
+    o[2] = u[1] / sp;
+}
+void derive_oscilloscope(const float* u, float* o) {           // misc_extras2.rs (init_oscilloscope)
+    o[0] = 6.28318530717959f * u[1];
+}
+void derive_wedge_julia(const float* u, float* o) {            // wedge_extended.rs (init_wedge_julia)
+    const float sp = u[0] == 0.0f ? 1e-30f : u[0];
+    o[0] = 1.0f - u[3] * u[2] * 0.15915494309189535f;
+    o[1] = std::fabs(u[0]);
+    o[2] = u[1] / sp * 0.5f;
+}
+void derive_wedge_sph(const float* u, float* o) {              // wedge_extended.rs (init_wedge_sph)
+    o[0] = 1.0f - u[0] * u[2] * 0.15915494309189535f;
+}
+
 // f32 complex arithmetic in the operation order of shaders/core/complex.wgsl:20-69.
 struct Cx { float x, y; };
 Cx cadd(Cx a, Cx b) { return {a.x + b.x, a.y + b.y}; }
@@ -201,6 +230,7 @@ static const VarDef kRegistry[] = {
     {"radial_blur", 73, 4, 1, {"angle"}, {0.0f}, "v_radial_blur", VF_W, 2, derive_radial_blur},
     {"separation", 77, 0, 4, {"x", "y", "xinside", "yinside"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_separation", 0, 0, nullptr},
     {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
+    {"cpow", 85, 1, 3, {"r", "i", "power"}, {1.0f, 0.1f, 1.5f}, "v_cpow", 0, 3, derive_cpow},
     {"sin", 93, 0, 0, NP, ND, "v_sin", 0, 0, nullptr},
     {"cos", 94, 0, 0, NP, ND, "v_cos", 0, 0, nullptr},
     {"tan", 95, 0, 0, NP, ND, "v_tan", 0, 0, nullptr},
@@ -217,19 +247,33 @@ static const VarDef kRegistry[] = {
     {"tangent", 141, 0, 0, NP, ND, "v_tangent", 0, 0, nullptr},
     {"secant2", 143, 0, 0, NP, ND, "v_secant2", 0, 0, nullptr},
     {"cosine", 144, 0, 0, NP, ND, "v_cosine", 0, 0, nullptr},
+    {"parabola", 149, 2, 2, {"width", "height"}, {1.0f, 0.5f}, "v_parabola", 0, 0, nullptr},
     {"pie", 150, 3, 3, {"slices", "rotation", "thickness"}, {6.0f, 0.0f, 0.5f}, "v_pie", 0, 0, nullptr},
     {"butterfly", 152, 0, 0, NP, ND, "v_butterfly", 0, 0, nullptr},
     {"cell", 161, 0, 1, {"size"}, {0.6f}, "v_cell", 0, 0, nullptr},
+    {"flower", 163, 1, 2, {"holes", "petals"}, {0.4f, 7.0f}, "v_flower", 0, 0, nullptr},
+    {"square", 166, 2, 0, NP, ND, "v_square", 0, 0, nullptr},
     {"popcorn2", 170, 0, 3, {"x", "y", "c"}, {1.0f, 0.5f, 1.5f}, "v_popcorn2", 0, 0, nullptr},
+    {"disc2", 178, 0, 2, {"rot", "twist"}, {2.0f, 0.5f}, "v_disc2", 0, 3, derive_disc2},
     {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
+    {"wedge_julia", 210, 1, 4, {"power", "dist", "count", "angle"}, {7.0f, 0.2f, 2.0f, 0.3f}, "v_wedge_julia", 0, 3, derive_wedge_julia},
+    {"wedge_sph", 211, 0, 4, {"angle", "hole", "count", "swirl"}, {0.2f, 0.2f, 2.0f, 0.3f}, "v_wedge_sph", 0, 1, derive_wedge_sph},
+    {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
+    {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
+    {"oscilloscope", 284, 0, 4, {"separation", "frequency", "amplitude", "damping"}, {1.0f, 3.14159265f, 1.0f, 0.0f}, "v_oscilloscope", 0, 1, derive_oscilloscope},
     {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
+    {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
+    {"arch", 312, 1, 0, NP, ND, "v_arch", VF_W, 0, nullptr},
+    {"blade", 314, 1, 0, NP, ND, "v_blade", VF_W, 0, nullptr},
+    {"twintrian", 319, 1, 0, NP, ND, "v_twintrian", VF_W, 0, nullptr},
+    {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
     {"edisc", 337, 0, 0, NP, ND, "v_edisc", VF_W, 0, nullptr},
     {"curve", 338, 0, 4, {"xamp", "yamp", "xlength", "ylength"}, {0.25f, 0.5f, 1.0f, 1.0f}, "v_curve", 0, 2, derive_curve},

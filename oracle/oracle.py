@@ -37,6 +37,9 @@ REGISTRY = {
     "lazysusan": 43, "auger": 51, "separation": 77, "mobius": 78, "sin": 93, "cos": 94, "tan": 95, "sec": 96,
     "csc": 97, "cot": 98, "sinh": 99, "cosh": 100, "tanh": 101, "coth": 102, "sech": 103, "csch": 104, "exp": 136,
     "cell": 161, "popcorn2": 170, "modulus": 273, "whorl": 302, "flux": 307, "edisc": 337, "curve": 338,
+    "cpow": 85, "parabola": 149, "flower": 163, "square": 166, "disc2": 178, "wedge_julia": 210, "wedge_sph": 211,
+    "super_shape": 212, "boarders": 229, "oscilloscope": 284, "rays": 308, "arch": 312, "blade": 314,
+    "twintrian": 319, "conic": 324,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -79,6 +82,15 @@ PARAMS.update({
     "whorl": [("inside", 0.1), ("outside", 0.2)],
     "flux": [("spread", 0.3)],
     "curve": [("xamp", 0.25), ("yamp", 0.5), ("xlength", 1.0), ("ylength", 1.0)],
+    "parabola": [("width", 1.0), ("height", 0.5)],
+    "flower": [("holes", 0.4), ("petals", 7.0)],
+    "super_shape": [("rnd", 3.0), ("m", 1.0), ("n1", 1.0), ("n2", 1.0), ("n3", 1.0), ("holes", 0.0)],
+    "conic": [("eccentricity", 1.0), ("holes", 0.0)],
+    "disc2": [("rot", 2.0), ("twist", 0.5)],
+    "cpow": [("r", 1.0), ("i", 0.1), ("power", 1.5)],
+    "oscilloscope": [("separation", 1.0), ("frequency", 3.14159265), ("amplitude", 1.0), ("damping", 0.0)],
+    "wedge_julia": [("power", 7.0), ("dist", 0.2), ("count", 2.0), ("angle", 0.3)],
+    "wedge_sph": [("angle", 0.2), ("hole", 0.2), ("count", 2.0), ("swirl", 0.3)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -97,6 +97,10 @@ WIDER = {
     "modulus": dict.fromkeys(["past_threshold", "lopsided"], "huge"),
     "whorl": {"lopsided": "inf*0"},
     "flux": dict.fromkeys(["+0+0", "+0-0", "-0+0", "-0-0", "-x", "tiny", "normal_min", "subnormal"], "zero"),
+    "rays": dict.fromkeys(["tiny", "normal_min"], "zero"),
+    "flower": dict.fromkeys(["+x", "-x", "unit", "y_neg0x"], "zero"),
+    "disc2": {"lopsided": "huge"},
+    "wedge_julia": {"-y": "zero"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -105,7 +109,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "hyperbolic", "bent", "eyefish", "noise", "blur", "cross", "rings2", "pdj", "rectangles", "splits",
                        "pre_blur", "secant2", "pie", "butterfly", "fan", "fisheye", "stripes", "bent2", "rings", "linear3D",
                        "klein_group", "subflame_wf", "pre_subflame_wf", "loonie", "scry", "elliptic", "bipolar", "lazysusan",
-                       "separation", "cell", "edisc", "curve"])
+                       "separation", "cell", "edisc", "curve", "square", "blade", "twintrian", "arch", "parabola",
+                       "super_shape", "conic", "cpow", "boarders", "oscilloscope"])
 
 
 def golden():
