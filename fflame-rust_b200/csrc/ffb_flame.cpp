@@ -226,8 +226,12 @@ static const VarDef kRegistry[] = {
     {"auger", 51, 0, 4, {"freq", "weight", "scale", "sym"}, {1.0f, 0.5f, 0.5f, 0.0f}, "v_auger", 0, 0, nullptr},
     {"pre_blur", 54, 7, 0, NP, ND, "v_pre_blur", VF_PRE | VF_W, 0, nullptr},
     {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
+    {"epispiral", 67, 1, 3, {"n", "thickness", "holes"}, {6.0f, 0.0f, 1.0f}, "v_epispiral", 0, 0, nullptr},
     {"juliascope", 69, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_juliascope", 0, 0, nullptr},
     {"radial_blur", 73, 4, 1, {"angle"}, {0.0f}, "v_radial_blur", VF_W, 2, derive_radial_blur},
+    {"blur_circle", 74, 2, 0, NP, ND, "v_blur_circle", 0, 0, nullptr},
+    {"blur_zoom", 75, 1, 3, {"length", "x", "y"}, {0.0f, 0.0f, 0.0f}, "v_blur_zoom", 0, 0, nullptr},
+    {"blur_pixelize", 76, 2, 2, {"size", "scale"}, {0.1f, 1.0f}, "v_blur_pixelize", 0, 0, nullptr},
     {"separation", 77, 0, 4, {"x", "y", "xinside", "yinside"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_separation", 0, 0, nullptr},
     {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
     {"cpow", 85, 1, 3, {"r", "i", "power"}, {1.0f, 0.1f, 1.5f}, "v_cpow", 0, 3, derive_cpow},
@@ -244,12 +248,16 @@ static const VarDef kRegistry[] = {
     {"sech", 103, 0, 0, NP, ND, "v_sech", 0, 0, nullptr},
     {"csch", 104, 0, 0, NP, ND, "v_csch", 0, 0, nullptr},
     {"exp", 136, 0, 0, NP, ND, "v_exp", 0, 0, nullptr},
+    {"tancos", 140, 0, 0, NP, ND, "v_tancos", 0, 0, nullptr},
     {"tangent", 141, 0, 0, NP, ND, "v_tangent", 0, 0, nullptr},
     {"secant2", 143, 0, 0, NP, ND, "v_secant2", 0, 0, nullptr},
     {"cosine", 144, 0, 0, NP, ND, "v_cosine", 0, 0, nullptr},
+    {"petal", 145, 0, 0, NP, ND, "v_petal", 0, 0, nullptr},
+    {"cardioid", 146, 0, 1, {"a"}, {1.0f}, "v_cardioid", 0, 0, nullptr},
     {"parabola", 149, 2, 2, {"width", "height"}, {1.0f, 0.5f}, "v_parabola", 0, 0, nullptr},
     {"pie", 150, 3, 3, {"slices", "rotation", "thickness"}, {6.0f, 0.0f, 0.5f}, "v_pie", 0, 0, nullptr},
     {"butterfly", 152, 0, 0, NP, ND, "v_butterfly", 0, 0, nullptr},
+    {"spiralwing", 158, 0, 0, NP, ND, "v_spiralwing", 0, 0, nullptr},
     {"cell", 161, 0, 1, {"size"}, {0.6f}, "v_cell", 0, 0, nullptr},
     {"flower", 163, 1, 2, {"holes", "petals"}, {0.4f, 7.0f}, "v_flower", 0, 0, nullptr},
     {"square", 166, 2, 0, NP, ND, "v_square", 0, 0, nullptr},
@@ -258,10 +266,15 @@ static const VarDef kRegistry[] = {
     {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
+    {"panorama1", 194, 0, 0, NP, ND, "v_panorama1", 0, 0, nullptr},
+    {"panorama2", 195, 0, 0, NP, ND, "v_panorama2", 0, 0, nullptr},
+    {"circleblur", 198, 2, 0, NP, ND, "v_circleblur", 0, 0, nullptr},
     {"wedge_julia", 210, 1, 4, {"power", "dist", "count", "angle"}, {7.0f, 0.2f, 2.0f, 0.3f}, "v_wedge_julia", 0, 3, derive_wedge_julia},
     {"wedge_sph", 211, 0, 4, {"angle", "hole", "count", "swirl"}, {0.2f, 0.2f, 2.0f, 0.3f}, "v_wedge_sph", 0, 1, derive_wedge_sph},
     {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
+    {"henon", 213, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_henon", 0, 0, nullptr},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
+    {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},

@@ -40,6 +40,9 @@ REGISTRY = {
     "cpow": 85, "parabola": 149, "flower": 163, "square": 166, "disc2": 178, "wedge_julia": 210, "wedge_sph": 211,
     "super_shape": 212, "boarders": 229, "oscilloscope": 284, "rays": 308, "arch": 312, "blade": 314,
     "twintrian": 319, "conic": 324,
+    "epispiral": 67, "blur_circle": 74, "blur_zoom": 75, "blur_pixelize": 76, "tancos": 140, "petal": 145,
+    "cardioid": 146, "spiralwing": 158, "panorama1": 194, "panorama2": 195, "circleblur": 198, "henon": 213,
+    "cylinder2": 241,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -91,6 +94,11 @@ PARAMS.update({
     "oscilloscope": [("separation", 1.0), ("frequency", 3.14159265), ("amplitude", 1.0), ("damping", 0.0)],
     "wedge_julia": [("power", 7.0), ("dist", 0.2), ("count", 2.0), ("angle", 0.3)],
     "wedge_sph": [("angle", 0.2), ("hole", 0.2), ("count", 2.0), ("swirl", 0.3)],
+    "epispiral": [("n", 6.0), ("thickness", 0.0), ("holes", 1.0)],
+    "blur_zoom": [("length", 0.0), ("x", 0.0), ("y", 0.0)],
+    "blur_pixelize": [("size", 0.1), ("scale", 1.0)],
+    "cardioid": [("a", 1.0)],
+    "henon": [("a", 0.5), ("b", 1.0), ("c", 1.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

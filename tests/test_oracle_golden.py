@@ -101,6 +101,9 @@ WIDER = {
     "flower": dict.fromkeys(["+x", "-x", "unit", "y_neg0x"], "zero"),
     "disc2": {"lopsided": "huge"},
     "wedge_julia": {"-y": "zero"},
+    "epispiral": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
+    "cardioid": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
+    "petal": {"pi_e": "zero", **dict.fromkeys(HUGE_ARGS, "huge")},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -110,7 +113,9 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "pre_blur", "secant2", "pie", "butterfly", "fan", "fisheye", "stripes", "bent2", "rings", "linear3D",
                        "klein_group", "subflame_wf", "pre_subflame_wf", "loonie", "scry", "elliptic", "bipolar", "lazysusan",
                        "separation", "cell", "edisc", "curve", "square", "blade", "twintrian", "arch", "parabola",
-                       "super_shape", "conic", "cpow", "boarders", "oscilloscope"])
+                       "super_shape", "conic", "cpow", "boarders", "oscilloscope", "blur_circle", "blur_zoom",
+                       "blur_pixelize", "tancos", "spiralwing", "panorama1", "panorama2", "circleblur", "henon",
+                       "cylinder2"])
 
 
 def golden():

@@ -45,7 +45,8 @@ PROBE_AFFINE = (1.0, 0.25, 0.1, -0.3, 0.9, -0.2)       # src/probe/flame.rs:4-12
 # correctly rounded on both sides, so the results are the same bits.
 EXACT = {"linear", "spherical", "horseshoe", "bubble", "curl", "hyperbolic", "bent", "eyefish", "cross", "rings2",
          "rectangles", "splits", "butterfly", "fisheye", "stripes", "bent2", "linear3D", "flatten", "loonie", "scry",
-         "separation", "mobius", "cell", "modulus", "square", "boarders"}
+         "separation", "mobius", "cell", "modulus", "square", "boarders",
+         "blur_zoom", "blur_pixelize", "henon", "cylinder2"}
 
 
 @pytest.fixture(scope="module")
@@ -267,7 +268,7 @@ def test_exactly_rounded_bodies_are_bit_identical(renderer, oracle, name):
     t = {"a": 1, "b": 0, "c": 0, "d": 1, "e": 0, "f": 0, "weight": 1.0, "color": 0.5, "variations": {name: 1.0},
          "variation_params": params}
     cfg = {"flame": {"transforms": [t]}}
-    words = (rng.integers(0, 1 << 24, (n, 64)) / float(1 << 24)).astype(np.float32)   # the draws of square, boarders
+    words = (rng.integers(0, 1 << 24, (n, 64)) / float(1 << 24)).astype(np.float32)   # the draws of square, boarders, the blurs
     gx, gy = renderer.apply_points(cfg, 0, xs, ys, words, with_affine=False)
     rx, ry = oracle.Flame(cfg, 8, 8).apply_xform(0, xs, ys, words, with_affine=False)
     ok = bit_equal(gx, rx) & bit_equal(gy, ry)
