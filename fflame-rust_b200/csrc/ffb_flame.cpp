@@ -269,12 +269,14 @@ static const VarDef kRegistry[] = {
     {"panorama1", 194, 0, 0, NP, ND, "v_panorama1", 0, 0, nullptr},
     {"panorama2", 195, 0, 0, NP, ND, "v_panorama2", 0, 0, nullptr},
     {"circleblur", 198, 2, 0, NP, ND, "v_circleblur", 0, 0, nullptr},
+    {"flipcircle", 200, 0, 0, NP, ND, "v_flipcircle", VF_W, 0, nullptr},
     {"wedge_julia", 210, 1, 4, {"power", "dist", "count", "angle"}, {7.0f, 0.2f, 2.0f, 0.3f}, "v_wedge_julia", 0, 3, derive_wedge_julia},
     {"wedge_sph", 211, 0, 4, {"angle", "hole", "count", "swirl"}, {0.2f, 0.2f, 2.0f, 0.3f}, "v_wedge_sph", 0, 1, derive_wedge_sph},
     {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
     {"henon", 213, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_henon", 0, 0, nullptr},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
+    {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
@@ -284,15 +286,25 @@ static const VarDef kRegistry[] = {
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
     {"arch", 312, 1, 0, NP, ND, "v_arch", VF_W, 0, nullptr},
+    {"bi_linear", 313, 0, 0, NP, ND, "v_bi_linear", 0, 0, nullptr},
     {"blade", 314, 1, 0, NP, ND, "v_blade", VF_W, 0, nullptr},
+    {"twoface", 318, 0, 0, NP, ND, "v_twoface", VF_W, 0, nullptr},
     {"twintrian", 319, 1, 0, NP, ND, "v_twintrian", VF_W, 0, nullptr},
+    {"unpolar", 320, 0, 0, NP, ND, "v_unpolar", VF_W, 0, nullptr},
+    {"idisc", 323, 0, 0, NP, ND, "v_idisc", VF_W, 0, nullptr},
     {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
     {"edisc", 337, 0, 0, NP, ND, "v_edisc", VF_W, 0, nullptr},
     {"curve", 338, 0, 4, {"xamp", "yamp", "xlength", "ylength"}, {0.25f, 0.5f, 1.0f, 1.0f}, "v_curve", 0, 2, derive_curve},
+    {"exp2", 340, 0, 0, NP, ND, "v_exp2", 0, 0, nullptr},
     {"exponential", 341, 0, 0, NP, ND, "v_exponential", 0, 0, nullptr},
+    {"flipy", 342, 0, 0, NP, ND, "v_flipy", 0, 0, nullptr},
+    {"invpolar", 344, 0, 0, NP, ND, "v_invpolar", 0, 0, nullptr},
     {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
+    {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
+    {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
+    {"rippled", 380, 0, 0, NP, ND, "v_rippled", 0, 0, nullptr},
     {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},
      "v_klein_group", VF_W, 16, derive_klein_group, 1, 1},
     {"subflame_wf", 502, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},

@@ -43,6 +43,8 @@ REGISTRY = {
     "epispiral": 67, "blur_circle": 74, "blur_zoom": 75, "blur_pixelize": 76, "tancos": 140, "petal": 145,
     "cardioid": 146, "spiralwing": 158, "panorama1": 194, "panorama2": 195, "circleblur": 198, "henon": 213,
     "cylinder2": 241,
+    "flipcircle": 200, "lozi": 243, "bi_linear": 313, "twoface": 318, "unpolar": 320, "idisc": 323, "exp2": 340,
+    "flipy": 342, "invpolar": 344, "swirl3": 374, "wdisc": 375, "rippled": 380,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -99,6 +101,8 @@ PARAMS.update({
     "blur_pixelize": [("size", 0.1), ("scale", 1.0)],
     "cardioid": [("a", 1.0)],
     "henon": [("a", 0.5), ("b", 1.0), ("c", 1.0)],
+    "lozi": [("a", 0.5), ("b", 1.0), ("c", 1.0)],
+    "swirl3": [("shift", 0.5)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -104,6 +104,14 @@ WIDER = {
     "epispiral": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
     "cardioid": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
     "petal": {"pi_e": "zero", **dict.fromkeys(HUGE_ARGS, "huge")},
+    "unpolar": {"pi_e": "zero", "tiny": "zero", "lopsided": "huge"},
+    "idisc": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "half_unit", "tiny", "normal_min", "neg0y_x"], "zero"),
+    "exp2": {**dict.fromkeys(["+y", "-y", "q1", "q2", "q3", "q4", "tiny", "normal_min", "neg0y_x"], "zero"), "big": "huge",
+             **dict.fromkeys(HUGE_ARGS, "huge")},
+    "invpolar": {**dict.fromkeys(["+x", "-x", "q1", "q2", "mid", "unit", "tiny", "normal_min", "y_neg0x"], "zero"),
+                 "big": "huge", **dict.fromkeys(HUGE_ARGS, "huge")},
+    "swirl3": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
+    "wdisc": dict.fromkeys(["-0-0", "-x", "+y", "-y", "half_unit", "tiny", "neg0y_x"], "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -115,7 +123,7 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "separation", "cell", "edisc", "curve", "square", "blade", "twintrian", "arch", "parabola",
                        "super_shape", "conic", "cpow", "boarders", "oscilloscope", "blur_circle", "blur_zoom",
                        "blur_pixelize", "tancos", "spiralwing", "panorama1", "panorama2", "circleblur", "henon",
-                       "cylinder2"])
+                       "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy", "rippled"])
 
 
 def golden():
