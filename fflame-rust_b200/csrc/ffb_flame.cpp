@@ -247,6 +247,11 @@ static const VarDef kRegistry[] = {
     {"coth", 102, 0, 0, NP, ND, "v_coth", 0, 0, nullptr},
     {"sech", 103, 0, 0, NP, ND, "v_sech", 0, 0, nullptr},
     {"csch", 104, 0, 0, NP, ND, "v_csch", 0, 0, nullptr},
+    {"sin2_bs", 123, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sin2_bs", 0, 0, nullptr},
+    {"cos2_bs", 124, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cos2_bs", 0, 0, nullptr},
+    {"sinh2_bs", 129, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sinh2_bs", 0, 0, nullptr},
+    {"cosh2_bs", 130, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cosh2_bs", 0, 0, nullptr},
+    {"exp2_bs", 135, 0, 3, {"x1", "y1", "y2"}, {1.0f, 1.0f, 1.0f}, "v_exp2_bs", 0, 0, nullptr},
     {"exp", 136, 0, 0, NP, ND, "v_exp", 0, 0, nullptr},
     {"tancos", 140, 0, 0, NP, ND, "v_tancos", 0, 0, nullptr},
     {"tangent", 141, 0, 0, NP, ND, "v_tangent", 0, 0, nullptr},
@@ -277,11 +282,13 @@ static const VarDef kRegistry[] = {
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
+    {"pulse", 244, 0, 4, {"freqx", "freqy", "scalex", "scaley"}, {2.0f, 2.0f, 1.0f, 1.0f}, "v_pulse", 0, 0, nullptr},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
     {"oscilloscope", 284, 0, 4, {"separation", "frequency", "amplitude", "damping"}, {1.0f, 3.14159265f, 1.0f, 0.0f}, "v_oscilloscope", 0, 1, derive_oscilloscope},
+    {"linearT", 287, 0, 2, {"powX", "powY"}, {1.2f, 1.2f}, "v_linearT", 0, 0, nullptr},
     {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
@@ -301,6 +308,7 @@ static const VarDef kRegistry[] = {
     {"flipy", 342, 0, 0, NP, ND, "v_flipy", 0, 0, nullptr},
     {"invpolar", 344, 0, 0, NP, ND, "v_invpolar", 0, 0, nullptr},
     {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
+    {"layered_spiral", 363, 0, 1, {"radius"}, {1.0f}, "v_layered_spiral", 0, 0, nullptr},
     {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
     {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},

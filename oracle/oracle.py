@@ -45,6 +45,8 @@ REGISTRY = {
     "cylinder2": 241,
     "flipcircle": 200, "lozi": 243, "bi_linear": 313, "twoface": 318, "unpolar": 320, "idisc": 323, "exp2": 340,
     "flipy": 342, "invpolar": 344, "swirl3": 374, "wdisc": 375, "rippled": 380,
+    "sin2_bs": 123, "cos2_bs": 124, "sinh2_bs": 129, "cosh2_bs": 130, "exp2_bs": 135, "pulse": 244, "linearT": 287,
+    "layered_spiral": 363,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -103,6 +105,11 @@ PARAMS.update({
     "henon": [("a", 0.5), ("b", 1.0), ("c", 1.0)],
     "lozi": [("a", 0.5), ("b", 1.0), ("c", 1.0)],
     "swirl3": [("shift", 0.5)],
+    **{n: [("x1", 1.0), ("x2", 1.0), ("y1", 1.0), ("y2", 1.0)] for n in ("sin2_bs", "cos2_bs", "sinh2_bs", "cosh2_bs")},
+    "exp2_bs": [("x1", 1.0), ("y1", 1.0), ("y2", 1.0)],
+    "pulse": [("freqx", 2.0), ("freqy", 2.0), ("scalex", 1.0), ("scaley", 1.0)],
+    "linearT": [("powX", 1.2), ("powY", 1.2)],
+    "layered_spiral": [("radius", 1.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -112,6 +112,12 @@ WIDER = {
                  "big": "huge", **dict.fromkeys(HUGE_ARGS, "huge")},
     "swirl3": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
     "wdisc": dict.fromkeys(["-0-0", "-x", "+y", "-y", "half_unit", "tiny", "neg0y_x"], "zero"),
+    "sin2_bs": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "cos2_bs": {"pi_e": "zero", **dict.fromkeys(HUGE_ARGS, "huge")},
+    "sinh2_bs": {**dict.fromkeys(["tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "cosh2_bs": dict.fromkeys(HUGE_ARGS, "huge"),
+    "exp2_bs": {**dict.fromkeys(["tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "layered_spiral": {"tiny": "zero"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
