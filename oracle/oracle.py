@@ -47,6 +47,7 @@ REGISTRY = {
     "flipy": 342, "invpolar": 344, "swirl3": 374, "wdisc": 375, "rippled": 380,
     "sin2_bs": 123, "cos2_bs": 124, "sinh2_bs": 129, "cosh2_bs": 130, "exp2_bs": 135, "pulse": 244, "linearT": 287,
     "layered_spiral": 363,
+    "circlesplit": 199, "loonie3": 217, "mcarpet": 282, "d_spherical": 334, "clifford_js": 435,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -110,6 +111,10 @@ PARAMS.update({
     "pulse": [("freqx", 2.0), ("freqy", 2.0), ("scalex", 1.0), ("scaley", 1.0)],
     "linearT": [("powX", 1.2), ("powY", 1.2)],
     "layered_spiral": [("radius", 1.0)],
+    "circlesplit": [("radius", 1.0), ("split", 0.5)],
+    "mcarpet": [("x", 1.0), ("y", 1.0), ("twist", 0.0), ("tilt", 0.0)],
+    "d_spherical": [("d_spher_weight", 0.5)],
+    "clifford_js": [("a", -1.4), ("b", 1.6), ("c", 1.0), ("d", 0.7)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

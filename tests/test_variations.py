@@ -46,7 +46,8 @@ PROBE_AFFINE = (1.0, 0.25, 0.1, -0.3, 0.9, -0.2)       # src/probe/flame.rs:4-12
 EXACT = {"linear", "spherical", "horseshoe", "bubble", "curl", "hyperbolic", "bent", "eyefish", "cross", "rings2",
          "rectangles", "splits", "butterfly", "fisheye", "stripes", "bent2", "linear3D", "flatten", "loonie", "scry",
          "separation", "mobius", "cell", "modulus", "square", "boarders",
-         "blur_zoom", "blur_pixelize", "henon", "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy"}
+         "blur_zoom", "blur_pixelize", "henon", "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy",
+         "loonie3", "d_spherical"}
 
 
 @pytest.fixture(scope="module")
