@@ -127,27 +127,87 @@ def profile_traffic(name):
 
 
 # ------------------------------------------------------------ CPU baseline --
-def cpu_baseline(wl, budget_s=12.0, threads=None):
-    """The oracle port on the host cores, on a bounded sample of the same
-    workload (same flame, same internal resolution, same RNG); samples/s."""
+def host_info():
+    """The host threads this process may use and the CPU model."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    model = None
+    try:
+        for line in open("/proc/cpuinfo", encoding="utf-8"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return cores, model
+
+
+def cpu_threads(wl):
+    """All host threads, fewer if their private histograms (28 B a pixel
+    each) would not fit in a quarter of the free memory."""
+    cores, _ = host_info()
+    W, H = wl["width"] * wl["supersample"], wl["height"] * wl["supersample"]
+    per_thread = 28.0 * W * H
+    try:
+        import psutil
+        free = psutil.virtual_memory().available
+        cores = max(1, min(cores, int(free / 4 / per_thread)))
+    except Exception:
+        pass
+    return max(1, min(cores, 128))
+
+
+def cpu_rate(wl, steps, warmup, min_samples=1e7, min_s=2.0):
+    """The oracle port of the render path on the host cores: a frame of the
+    workload's flame at its internal size, built over steps.  Each step
+    renders a fresh range of walkers (its own burn-in) into per-thread
+    histograms made once before the first step; only the steps are timed,
+    each at least `min_samples` samples and about `min_s` seconds (sized from
+    the warm-up steps' rate).  Returns samples/s over the timed steps."""
     from oracle import oracle as O
     O.build()
-    threads = threads or min(os.cpu_count() or 1, 64)
+    threads = cpu_threads(wl)
     W, H = wl["width"] * wl["supersample"], wl["height"] * wl["supersample"]
     fl = O.Flame(wl["cfg"], W, H)
-    walkers = threads * 64
-    iters = 64
     t0 = time.perf_counter()
-    fl.render(walkers, iters + 20, threads=threads)
-    dt = time.perf_counter() - t0
-    rate = walkers * iters / max(dt, 1e-6)
-    per = max(64, int(rate * budget_s / walkers))
+    ctx = fl.cpu_render(threads)
+    setup_s = time.perf_counter() - t0
+    walkers = threads * 256
+    per = max(64, int(min_samples) // walkers + 1)
+    w0 = 0
+    rate = None
+    for _ in range(max(1, warmup)):
+        t0 = time.perf_counter()
+        plotted = ctx.run(w0, walkers, per + 20, seed=0x5EED)
+        rate = plotted / max(time.perf_counter() - t0, 1e-9)
+        w0 += walkers
+    per = max(per, int(rate * min_s / walkers) + 1)
+    times, samples = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        plotted = ctx.run(w0, walkers, per + 20, seed=0x5EED)
+        times.append(time.perf_counter() - t0)
+        samples.append(plotted)
+        w0 += walkers
     t0 = time.perf_counter()
-    plotted, _, _, _ = fl.render(walkers, per + 20, threads=threads)
-    dt = time.perf_counter() - t0
-    return {"value": plotted / dt, "unit": "samples/s", "cores": threads, "kind": "port",
-            "sample": f"{plotted:.3g} samples of the same flame at {W}x{H} ({walkers} walkers x {per} after burn-in 20), "
-                      f"{dt:.1f} s, f32, private histograms per thread"}
+    inframe, _, _ = ctx.merge()
+    merge_s = time.perf_counter() - t0
+    ctx.close()
+    _, model = host_info()
+    return {
+        "value": sum(samples) / sum(times), "unit": "samples/s", "cores": threads, "cpu_model": model,
+        "per_core": sum(samples) / sum(times) / threads, "ms_per_step": 1e3 * sum(times) / len(times),
+        "samples_per_step": sum(samples) / len(samples), "steps": steps,
+        "setup_s": setup_s, "merge_s": merge_s, "inframe": int(inframe),
+        "sample": f"{steps} steps of {walkers} walkers x {per} iterations after burn-in 20 "
+                  f"({sum(samples) / len(samples):.3g} samples a step) of the same flame at {W}x{H}, f32, "
+                  f"{threads} threads with a private histogram each (made once, merged after the steps, neither timed)",
+    }
+
+
+def cpu_baseline(wl):
+    r = cpu_rate(wl, steps=3, warmup=1)
+    r["kind"] = "port"
+    return r
 
 
 # ------------------------------------------------------------------ ours --
@@ -262,11 +322,8 @@ def run_ours(args, rank, world, local_rank):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded flame generator; no dataset)",
-        "config": {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
-                   "samples_per_step": samples_per_step, "walkers": wl["walkers"], "rng": "philox",
-                   "schedule": args.schedule, "math": args.math, "accumulate": args.accumulate,
-                   "l2": f"histogram {W * ss * H * ss * (32 if exact else 16) / 1e6:.1f} MB > 126 MB L2, cleared every step",
-                   "parallelism": f"walker shards x{world}" + (" + NCCL histogram all-reduce + row bands" if world > 1 else "")},
+        "config": config_for(args, wl, world),
+        "samples_per_step": samples_per_step * world,
         "ms_per_frame": ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
@@ -284,65 +341,159 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl)
+    if world == 1 and not args.no_extra and args.workload == "full_1080p_ss2":
+        line["parity"] = leg(parity_leg, r, wl)
+        line["batched"] = leg(run_batched, args, local_rank, steps=3, serial_steps=2)
+        line["diff"] = leg(run_diff, args, local_rank, steps=10, cpu=False)
+        line["stress_4k"] = leg(stress_leg, r, args)
+    r.close()
     return line
 
 
-def run_batched(args, local_rank):
+def leg(fn, *a, **k):
+    """An extra measurement of the default line; its failure is reported in
+    the line, not raised."""
+    try:
+        return fn(*a, **k)
+    except Exception as e:          # noqa: BLE001
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
+def parity_leg(r, wl, size=(480, 270)):
+    """The benchmarked path against the oracle at the benchmark's samples a
+    pixel, at a reduced size (outside the timed region): normalised
+    log-density L1 / p99, block z-scores and the tone-mapped image, each
+    beside two oracle renders' own difference (oracle/parity.py)."""
+    from oracle import parity
+    ss = wl["supersample"]
+    spp = wl["iterations"] / float(wl["width"] * ss * wl["height"] * ss)
+    samples = int(spp * size[0] * size[1] * ss * ss)
+    t0 = time.perf_counter()
+    m = parity.render_parity(r, wl["cfg"], size[0], size[1], ss, samples, wl["walkers"])
+    m["within_noise"] = parity.within_noise(m)
+    m["flame"] = f"synthetic.full_flame({FULL_SEED}) (the benchmark's flame), density estimation radius 9"
+    m["seconds"] = time.perf_counter() - t0
+    return m
+
+
+def stress_leg(r, args, steps=2):
+    """The 4K stress frame (7680x4320 internal, exact u64 counts, 1e10
+    samples, DE 12) through the same device path, timed with CUDA events."""
+    import torch
+    wl = workload("stress_4k")
+    cfg = json.dumps(wl["cfg"])
+    W, H, ss = wl["width"], wl["height"], wl["supersample"]
+    job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, seed=0x5EED,
+               count_bits=64, accumulate=args.accumulate)
+    d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+    out = r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=side.cuda_stream, sync=True, **job)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(side)
+    for _ in range(steps):
+        r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=side.cuda_stream, sync=False, **job)
+    ev1.record(side)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    del d_rgba
+    torch.cuda.empty_cache()
+    return {"ms_per_frame": ms, "samples_per_s": out.total_iterations / (ms * 1e-3), "samples": out.total_iterations,
+            "steps": steps, "desc": wl["desc"]}
+
+
+def config_for(args, wl, world):
+    """The workload's description, the same for both arms."""
+    W, H, ss = wl["width"], wl["height"], wl["supersample"]
+    exact = wl.get("count_bits", 32) == 64
+    return {"workload": args.workload, "desc": wl["desc"], "width": W, "height": H, "supersample": ss,
+            "samples": wl["iterations"], "walkers": wl["walkers"], "rng": "philox",
+            "schedule": args.schedule, "math": args.math, "accumulate": args.accumulate,
+            "l2": f"histogram {W * ss * H * ss * (32 if exact else 16) / 1e6:.1f} MB > 126 MB L2, cleared every step",
+            "parallelism": f"walker shards x{world}" + (" + NCCL histogram reduce-scatter + row bands" if world > 1 else "")}
+
+
+def run_batched(args, local_rank, steps=None, serial_steps=None):
     """256 synthetic flames (transform counts 2-12, 128^2-1024^2, 50-2000
     samples a pixel): one batched, graph-captured render against the same
-    flames rendered one after another.  flames/s, device-timed."""
+    flames rendered one after another.  flames/s, device-timed; then the
+    same comparison within each resolution class (the class's flames as a
+    batch of their own, with the whole batch's tuned launch shape)."""
     import torch
     from ffb200 import Batch, _native, synthetic
     torch.cuda.set_device(local_rank)
+    steps = steps or args.steps
+    serial_steps = serial_steps or max(1, args.steps // 2)
     r = _native.Renderer(local_rank)
     items = synthetic.batch_flames(n=256, seed=3)
+    texts = [json.dumps(it[0]) for it in items]
+    side = torch.cuda.Stream()
+    outs = [torch.empty(w * h * 4, dtype=torch.uint8, device="cuda") for _, w, h, _, _ in items]
+
+    def time_batch(b):
+        for _ in range(max(1, min(args.warmup, 2))):
+            b.run()
+        return statistics.median(b.run() for _ in range(steps))
+
+    def time_serial(idx):
+        def serial():
+            for i in idx:
+                _, w, h, samples, seed = items[i]
+                r.render_device(texts[i], w, h, outs[i].data_ptr(), stream=side.cuda_stream, sync=False,
+                                iterations=samples, seed=seed)
+        serial()
+        side.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _ in range(serial_steps):
+            ev0.record(side)
+            serial()
+            ev1.record(side)
+            ev1.synchronize()
+            ms.append(ev0.elapsed_time(ev1))
+        return statistics.median(ms)
+
     t0 = time.perf_counter()
     b = Batch(r, items, tune=True)
     setup_s = time.perf_counter() - t0
     info = b.info()
-    for _ in range(args.warmup):
-        b.run()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    ms_b = [b.run() for _ in range(args.steps)]
+    batched_ms = time_batch(b)
     clk = clocks.stop()
-    batched_ms = statistics.median(ms_b)
-    # Serial: each flame its own render (same budgets), back to back on one stream.
-    side = torch.cuda.Stream()
-    outs = [torch.empty(w * h * 4, dtype=torch.uint8, device="cuda") for _, w, h, _, _ in items]
-    def serial():
-        for (cfg, w, h, samples, seed), o in zip(items, outs):
-            r.render_device(json.dumps(cfg), w, h, o.data_ptr(), stream=side.cuda_stream, sync=False,
-                            iterations=samples, seed=seed)
-    serial()
-    side.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ms_s = []
-    for _ in range(max(1, args.steps // 2)):
-        ev0.record(side)
-        serial()
-        ev1.record(side)
-        ev1.synchronize()
-        ms_s.append(ev0.elapsed_time(ev1))
-    serial_ms = statistics.median(ms_s)
     b.close()
+    serial_ms = time_serial(range(len(items)))
+    classes = {}
+    for size in sorted({w for _, w, _, _, _ in items}):
+        idx = [i for i, it in enumerate(items) if it[1] == size]
+        bc = Batch(r, [items[i] for i in idx], tune=False, threads=info["threads"],
+                   iterations_per_thread=info["iterations_per_walker"])
+        bms = time_batch(bc)
+        samples = bc.info()["samples"]
+        bc.close()
+        sms = time_serial(idx)
+        classes[f"{size}x{size}"] = {"flames": len(idx), "samples": samples, "batched_ms": bms, "serial_ms": sms,
+                                     "batched_flames_per_s": len(idx) / (bms * 1e-3),
+                                     "serial_flames_per_s": len(idx) / (sms * 1e-3), "ratio": sms / bms}
     n = len(items)
+    r.close()
     return {
         "metric": "flames/s (batched 256)", "value": n / (batched_ms * 1e-3), "unit": "flames/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_ms, "higher_is_better": True,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": batched_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flame generator)",
         "config": {"workload": "batched_256", "flames": n, "samples": info["samples"],
                    "desc": "256 flames, 2-12 transforms {linear,sinusoidal,spherical}, 128^2-1024^2, 50-2000 spp",
                    "tuned": {"threads": info["threads"], "iterations_per_walker": info["iterations_per_walker"]},
                    "groups": info["groups"], "setup_s": setup_s},
+        "flames_per_s": n / (batched_ms * 1e-3), "serial_flames_per_s": n / (serial_ms * 1e-3),
         "samples_per_s": info["samples"] / (batched_ms * 1e-3),
         "serial": {"value": n / (serial_ms * 1e-3), "unit": "flames/s", "ms": serial_ms},
-        "batched_over_serial": serial_ms / batched_ms,
+        "batched_over_serial": serial_ms / batched_ms, "ratio": serial_ms / batched_ms,
+        "per_size_class": classes,
         "clocks": clk,
     }
 
 
-def run_diff(args, local_rank):
+def run_diff(args, local_rank, steps=None, cpu=True):
     """The differentiable configuration: 4 transforms at 512^2, bilinear
     splat, 2e8 samples, loss = L2 between the image and the image at
     theta + N(0, 0.05).  One step = forward (theta -> image), the loss's
@@ -354,6 +505,7 @@ def run_diff(args, local_rank):
     torch.cuda.set_device(local_rank)
     side = torch.cuda.Stream()
     torch.cuda.set_stream(side)
+    steps = steps or args.steps
     cfg = synthetic.diff_flame(4)
     W, samples, walkers = 512, 200_000_000, 65536
     r = _native.Renderer(local_rank)
@@ -379,16 +531,16 @@ def run_diff(args, local_rank):
     time.sleep(0.3)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     ev[0].record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         fwd()
     ev[1].record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
     ev[2].record()
     ev[2].synchronize()
     clk = clocks.stop()
-    fwd_ms = ev[0].elapsed_time(ev[1]) / args.steps
-    step_ms = ev[1].elapsed_time(ev[2]) / args.steps
+    fwd_ms = ev[0].elapsed_time(ev[1]) / steps
+    step_ms = ev[1].elapsed_time(ev[2]) / steps
     plotted, inframe = dr.samples()
     # The adjoint kernel alone, and the forward kernel's splat against the
     # vector-reduction ceiling at the same histogram size.
@@ -409,7 +561,7 @@ def run_diff(args, local_rank):
     host_th = th.cpu().pin_memory()
     host_g = torch.empty(th.numel(), dtype=torch.float32).pin_memory()
     e2e = []
-    for i in range(args.warmup + args.steps):
+    for i in range(args.warmup + steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         t = host_th.to("cuda", non_blocking=True).requires_grad_()
@@ -422,7 +574,7 @@ def run_diff(args, local_rank):
             e2e.append(time.perf_counter() - t0)
     e2e_ms = statistics.mean(e2e) * 1e3
     e2e_fwd = []
-    for i in range(args.warmup + args.steps):
+    for i in range(args.warmup + steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         t = host_th.to("cuda", non_blocking=True)
@@ -431,12 +583,12 @@ def run_diff(args, local_rank):
             e2e_fwd.append(time.perf_counter() - t0)
     e2e_fwd_ms = statistics.mean(e2e_fwd) * 1e3
     cpu = None
-    if not args.no_cpu:
+    if cpu and not args.no_cpu:
         cpu = cpu_baseline_diff(cfg, W)
     dr.close()
     return {
         "metric": "fwd+bwd time / fwd time", "value": step_ms / fwd_ms, "unit": "x", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flame generator)",
         "config": {"workload": "diff_512", "desc": "4 xforms {linear,sinusoidal,spherical} (contractive), 512x512 ss1, "
                    "2e8 samples, 65536 walkers, bilinear splat, L2 loss vs image at theta+N(0,0.05); "
@@ -453,7 +605,7 @@ def run_diff(args, local_rank):
                 "h2d_bytes_per_step": th.numel() * 4, "d2h_bytes_per_step": th.numel() * 4 + 8,
                 "path": "ffb200.diff.DiffRenderer.render (torch.autograd.Function): theta from pinned host memory, "
                         "loss and dL/dtheta back to the host"},
-        "gpu_launches": 5 * args.steps + 3 * args.steps,
+        "gpu_launches": 5 * steps + 3 * steps,
         "clocks": clk,
         "cpu_baseline": cpu,
     }
@@ -506,31 +658,20 @@ def run_reference(args, rank, world):
             "note": "the reference has no gradients; this is the oracle's FP64 restatement of this build's definition",
         }
     wl = workload(args.workload)
-    from oracle import oracle as O
-    O.build()
-    threads = os.cpu_count() or 1
-    W, H = wl["width"] * wl["supersample"], wl["height"] * wl["supersample"]
-    fl = O.Flame(wl["cfg"], W, H)
-    walkers = threads * 32
-    per = 128
-    rates = []
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        plotted, _, _, _ = fl.render(walkers, per + 20, threads=threads, walker0=i * walkers)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            rates.append(plotted / dt)
-    v = statistics.mean(rates)
-    ms_frame = wl["iterations"] / v * 1e3
-    sample = f"{walkers * per} samples a step ({walkers} walkers x {per}) of the same flame at {W}x{H}"
+    c = cpu_rate(wl, steps=args.steps, warmup=args.warmup)
+    v = c["value"]
     return {
         "impl": "reference", "metric": "samples/s", "value": v, "unit": "samples/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_frame, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flame generator)",
-        "config": {"workload": args.workload, "desc": wl["desc"]},
-        "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port", "sample": sample},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": c["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded flame generator; no dataset)",
+        "config": config_for(args, wl, world),
+        "samples_per_step": c["samples_per_step"],
+        "ms_per_frame_extrapolated": wl["iterations"] / v * 1e3,
+        "cpu_baseline": dict(c, kind="port"),
         "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference has no CPU render path; this is the oracle's restatement of it (oracle/)",
+        "note": "the reference has no CPU render path (its variations exist only as WGSL); this is the oracle's "
+                "restatement of it (oracle/), each step a timed bounded sample of the frame; ms_per_step is that "
+                "sample's measured time, ms_per_frame_extrapolated the whole frame at the measured rate",
     }
 
 
@@ -543,6 +684,8 @@ def main():
     ap.add_argument("--workload", default="full_1080p_ss2",
                     choices=["full_1080p_ss2", "plain_256", "batched_256", "stress_4k", "diff_512"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the default line's extra legs (parity, batched, diff, 4K stress)")
     ap.add_argument("--math", default="precise", choices=["precise", "sfu"],
                     help="precise: IEEE-accurate sin/cos (the parity-tested path); sfu: the hardware's, as the reference GPU")
     ap.add_argument("--schedule", default="auto", choices=["auto", "plain", "sorted"],

@@ -710,7 +710,9 @@ Flame parse_config(const Json& cfg) {
         F.de.max_radius = (float)de->number_or("radius", 0.0);
         F.de.min_radius = (float)de->number_or("minimum", 0.0);
         F.de.curve = (float)de->number_or("curve", 0.4);
-        if (F.de.max_radius < 0 || F.de.max_radius > 32) fail("density_estimation.radius must be 0..32");
+        if (!(F.de.max_radius >= 0 && F.de.max_radius <= 32)) fail("density_estimation.radius must be 0..32");
+        if (!(F.de.min_radius >= 0 && F.de.min_radius <= 32)) fail("density_estimation.minimum must be 0..32");
+        if (!(F.de.curve >= 0 && F.de.curve <= 16)) fail("density_estimation.curve must be 0..16");
     }
     if (const Json* mi = cfg.get("max_iterations"); mi && mi->kind == Json::Number) F.max_iterations = (uint64_t)mi->num;
     F.deterministic_rng = cfg.bool_or("deterministic_rng", false);

@@ -1121,11 +1121,18 @@ FFB_API int ffb_tonemap(ffb_renderer* r, const char* config, size_t len, const f
     });
 }
 
+// Density-estimation parameters a caller passes: written so that NaN fails
+// every comparison and is refused with the out-of-range values.
+static bool de_params_ok(float max_radius, float min_radius, float curve) {
+    return max_radius > 0.f && max_radius <= 36.f && min_radius >= 0.f && std::isfinite(min_radius) && curve >= 0.f &&
+           std::isfinite(curve);
+}
+
 FFB_API int ffb_density_estimate(ffb_renderer* r, const uint32_t* counts, const float* rgb, uint32_t w, uint32_t h,
                                  float max_radius, float min_radius, float curve, float* out_counts, float* out_rgb) {
     return guard([&] {
         if (!r || !counts || !rgb || !out_counts || !out_rgb) fail(FFB_ERR_INVALID, "NULL argument");
-        if (max_radius <= 0.f || max_radius > 36.f || min_radius < 0.f || curve < 0.f) fail(FFB_ERR_INVALID, "bad DE parameters");
+        if (!de_params_ok(max_radius, min_radius, curve)) fail(FFB_ERR_INVALID, "bad DE parameters: max_radius in (0, 36], min_radius >= 0, curve >= 0, all finite");
         std::lock_guard<std::mutex> lk(r->mu);
         r->begin();
         const size_t npx = (size_t)w * h;
@@ -1152,7 +1159,7 @@ FFB_API int ffb_density_estimate_static(const void* d_hist, uint32_t w, uint32_t
     return guard([&] {
         if (!d_hist || !d_out) fail(FFB_ERR_INVALID, "NULL argument");
         if (w == 0 || h == 0 || w > 65536 || h > 65536) fail(FFB_ERR_INVALID, "histogram size must be 1..65536 on each side");
-        if (max_radius <= 0.f || max_radius > 36.f || min_radius < 0.f || curve < 0.f) fail(FFB_ERR_INVALID, "bad DE parameters");
+        if (!de_params_ok(max_radius, min_radius, curve)) fail(FFB_ERR_INVALID, "bad DE parameters: max_radius in (0, 36], min_radius >= 0, curve >= 0, all finite");
         if (de_static_entries(max_radius, min_radius, curve) < 0)
             fail(FFB_ERR_TOO_LARGE, "density estimation table needs more than " + std::to_string(kDeStaticEntries) +
                                         " entries, the static scratch's size: raise min_radius or curve");

@@ -511,7 +511,10 @@ cudaError_t launch_atomic_bench(uint32_t* buf, uint32_t n_pixels, uint64_t n_sam
 // * Set-up: the first call on a device, with that device current, looks up
 //   the array's device address (cudaGetSymbolAddress) and keeps it for later
 //   calls on that device. That first call should come before any stream
-//   capture.
+//   capture. The kept address belongs to the device's context at set-up: if
+//   that context is destroyed and another made (cudaDeviceReset, or a primary
+//   context released and retained again), the next call sees the new
+//   context's id and looks the address up again.
 // * Every call on a device shares the one array. Calls whose work overlaps on
 //   the GPU race on it: two streams, or a call queued while another's DE
 //   kernel has not yet run. Order them on one stream or with events.
@@ -536,7 +539,32 @@ __global__ void k_de_store(const __grid_constant__ DeChunk c, int n, float4* __r
 }
 
 std::mutex g_de_static_mu;
-float4* g_de_static_ptr[kMaxDevices] = {};
+struct DeStaticSlot {
+    unsigned long long ctx_id = 0;   // the context the address belongs to (0: none yet)
+    float4* ptr = nullptr;
+};
+DeStaticSlot g_de_static[kMaxDevices];
+
+// The unique id of the calling thread's current context (0 when none is
+// current), through the driver's entry points so this library needs no link
+// to libcuda.  Ids are never reused within a process, unlike context handles.
+unsigned long long current_context_id() {
+    typedef int (*GetCurrent)(void**);
+    typedef int (*GetId)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, nullptr) == cudaSuccess) get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, nullptr) == cudaSuccess) get_id = (GetId)f;
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 cudaError_t de_static_scratch(float4** out) {
     int dev = -1;
@@ -544,13 +572,16 @@ cudaError_t de_static_scratch(float4** out) {
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(g_de_static_mu);
-    if (!g_de_static_ptr[dev]) {
+    DeStaticSlot& slot = g_de_static[dev];
+    unsigned long long id = current_context_id();
+    if (!slot.ptr || id == 0 || id != slot.ctx_id) {
         float4* ptr = nullptr;
-        e = cudaGetSymbolAddress((void**)&ptr, g_de_scratch);
+        e = cudaGetSymbolAddress((void**)&ptr, g_de_scratch);   // makes the device's primary context current if none is
         if (e != cudaSuccess) return e;
-        g_de_static_ptr[dev] = ptr;
+        slot.ptr = ptr;
+        slot.ctx_id = id ? id : current_context_id();
     }
-    *out = g_de_static_ptr[dev];
+    *out = slot.ptr;
     return cudaSuccess;
 }
 

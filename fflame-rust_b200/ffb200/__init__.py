@@ -102,6 +102,16 @@ class Engine:
         the budget); `exact` accumulates u64 counts and fixed-point colour
         sums (long renders, order-independent results); `accumulate`
         ("direct" or "tiled") picks how the exact sums are gathered.
+
+        `sticky` and `sequence` are accepted for pyfae's signature and change
+        nothing here.  The reference's `sticky` compiles a superset shader
+        to save recompiles across flames, at the cost of the specialised
+        shader's exact picture (wasm/python/src/render.rs:50-52, 155); this
+        library always renders the specialised picture, and flames sharing a
+        structure already share one compiled module.  `sequence` continues a
+        simulation engine's state from the previous sequence frame
+        (render.rs:185-199); a fractal flame carries no engine state between
+        frames, so a sequence frame is the same render as a still.
         """
         text = _text(config)
         request = {"fn": "render", "config": text, "width": width, "height": height,

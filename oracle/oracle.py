@@ -159,6 +159,14 @@ def lib():
         L.of_render_filtered.restype = ctypes.c_uint64
         L.of_probe_digest.restype = ctypes.c_uint64
         L.of_render.restype = ctypes.c_uint64
+        L.of_ctx_new.restype = ctypes.c_void_p
+        L.of_ctx_new.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.of_ctx_free.argtypes = [ctypes.c_void_p]
+        L.of_ctx_run.restype = ctypes.c_uint64
+        L.of_ctx_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
+        L.of_ctx_merge.restype = ctypes.c_int64
+        L.of_ctx_merge.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_double)]
         L.of_pcg_hash.restype = ctypes.c_uint32
         L.of_rng_next.restype = ctypes.c_uint32
         L.of_f16_round.restype = ctypes.c_float
@@ -444,6 +452,10 @@ class Flame:
         if not hist:
             return plotted, inframe.value, None, None
         return plotted, inframe.value, cnt.reshape(self.height, self.width), rgb.reshape(self.height, self.width, 3)
+
+    def cpu_render(self, threads):
+        """A persistent host render of this flame (CpuRender)."""
+        return CpuRender(self, threads)
 
     def render_filtered(self, walkers, iters, sigma, blur_edges=0.0, *, seed=12345, seed_hi=0, rng="philox", burn_in=20,
                         ipt=1024, threads=1, walker0=0):
@@ -795,3 +807,41 @@ def variation_jacobian(name, xs, ys, draws=None, params=None):
     lib().of_variation_jacobian(ctypes.c_int(REGISTRY[name]), _fp(prm), ctypes.c_int(len(xs)), _fp(xs), _fp(ys),
                                 _fp(d) if d is not None else None, out.ctypes.data_as(_DP))
     return out.reshape(-1, 6)
+
+
+class CpuRender:
+    """One frame rendered on the host cores over several calls: a private
+    histogram a thread, allocated and zeroed when this is made; `run` adds
+    a batch of walkers' samples (the chaos game and its splats, nothing
+    else); `merge` sums the threads' histograms.  The benchmark's CPU legs
+    time `run` alone."""
+
+    def __init__(self, flame, threads):
+        self.flame = flame                       # keeps the flat arrays alive
+        self.threads = int(threads)
+        self.ptr = lib().of_ctx_new(flame.ptr, self.threads)
+
+    def run(self, walker0, walkers, iters, *, seed=12345, seed_hi=0, rng="philox", burn_in=20, ipt=1024):
+        """Plotted samples of walkers [walker0, walker0 + walkers), `iters` iterations each."""
+        return lib().of_ctx_run(self.ptr, 0 if rng == "pcg" else 1, seed & 0xFFFFFFFF, seed_hi & 0xFFFFFFFF, burn_in, ipt,
+                                walker0, walkers, iters)
+
+    def merge(self):
+        """(in-frame splats, counts[h, w] u32, rgb sums[h, w, 3] f64) of every run so far."""
+        n = self.flame.width * self.flame.height
+        cnt = np.zeros(n, np.uint32)
+        rgb = np.zeros(n * 3, np.float64)
+        inf = lib().of_ctx_merge(self.ptr, cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                 rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return inf, cnt.reshape(self.flame.height, self.flame.width), rgb.reshape(self.flame.height, self.flame.width, 3)
+
+    def close(self):
+        if self.ptr:
+            lib().of_ctx_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
