@@ -222,7 +222,7 @@ def run_ours(args, rank, world, local_rank):
     r = _native.Renderer(local_rank)
     job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, walker0=rank * wl["walkers"],
                seed=0x5EED + 0, schedule=args.schedule, math=args.math, count_bits=wl.get("count_bits", 32),
-               accumulate=args.accumulate)
+               accumulate=args.accumulate, plot=args.plot)
     d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
     # The library's kernels and the timing events share one (non-default) stream.
     side = torch.cuda.Stream()
@@ -692,6 +692,9 @@ def main():
                     help="walker scheduling of the chaos kernel (same orbits either way)")
     ap.add_argument("--accumulate", default="auto", choices=["auto", "direct", "tiled"],
                     help="exact mode: direct atomics on the histogram or tile-sorted accumulation")
+    ap.add_argument("--plot", default="auto", choices=["auto", "inline", "deferred", "fused"],
+                    help="where the samples are plotted: by each walker, by a second kernel, or by plot warps "
+                         "in the walkers' own block (the same histogram)")
     ap.add_argument("--profile", type=float, default=0.0,
                     help="profiling run for ncu: only the chaos kernel of the workload, at this many samples")
     args = ap.parse_args()

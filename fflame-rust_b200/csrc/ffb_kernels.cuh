@@ -18,6 +18,7 @@ struct ffb_launch {
     float4* rec;               // deferred plotting: n_iters x n_walkers samples (x, y, ci, flags)
     float* rec_draws;          // and their final chain's draws, FFB_NFD planes of the same length
     float* state;              // FFB_NSTATE planes of n_walkers: the walkers' variation state (slot-major)
+    u32 ring_prod, ring_depth; // fused plotting: producer threads a block, iteration slots of the ring
 };
 
 // The walker context of walker gw at iteration it.
@@ -409,20 +410,26 @@ __device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, co
 #ifdef FFB_DEFER
 // Deferred plotting: the chaos kernel stores each iteration's sample (its
 // point after the transform, colour index, plot flag, transform) and the
-// draws of the finals' slots; ffb_plot applies the rest.  A record a
-// walker and iteration: (x, y, ci, flags) with flags bit 1 a kept sample,
-// bit 0 its opacity draw passed, bits 8-15 the transform picked; 0 for
-// burn-in and respawns.
-__device__ __forceinline__ u64 ffb_rec_index(const ffb_launch& J, u32 gw, u64 it) {
-    return (it - J.it0) * (u64)J.n_walkers + (u64)(gw - J.walker0);
+// draws of the finals' slots; ffb_plot (or the plotting warps of
+// ffb_chaos_fused) applies the rest.  A record a walker and iteration:
+// (x, y, ci, flags) with flags bit 1 a kept sample, bit 0 its opacity draw
+// passed, bits 8-15 the transform picked; 0 for burn-in and respawns.  The
+// final chain's draws go to planes `stride` apart.
+struct FfbRec {
+    float4* rec;
+    float* draws;
+    u64 stride;
+};
+// The record of walker gw at iteration it in the launch's global buffers.
+__device__ __forceinline__ FfbRec ffb_rec_at(const ffb_launch& J, u32 gw, u64 it) {
+    const u64 ri = (it - J.it0) * (u64)J.n_walkers + (u64)(gw - J.walker0);
+    return FfbRec{J.rec + ri, J.rec_draws + ri, (u64)J.n_iters * J.n_walkers};
 }
-#define FFB_DEFER_SKIP(J, gw, it) ((J).rec[ffb_rec_index((J), (gw), (it))] = make_float4(0.f, 0.f, 0.f, 0.f))
+#define FFB_DEFER_SKIP(R) (*(R).rec = make_float4(0.f, 0.f, 0.f, 0.f))
 template <class R>
-__device__ __forceinline__ void ffb_defer_store(const ffb_launch& J, u32 gw, u64 it, int k, float x, float y, float ci, bool plot,
-                                                R& rng) {
-    const u64 ri = ffb_rec_index(J, gw, it);
-    J.rec[ri] = make_float4(x, y, ci, __uint_as_float(2u | (plot ? 1u : 0u) | ((u32)k << 8)));
-    ffb_capture_final_draws(rng, J.rec_draws + ri, (u64)J.n_iters * J.n_walkers);
+__device__ __forceinline__ void ffb_defer_store(const FfbRec& rs, int k, float x, float y, float ci, bool plot, R& rng) {
+    *rs.rec = make_float4(x, y, ci, __uint_as_float(2u | (plot ? 1u : 0u) | ((u32)k << 8)));
+    ffb_capture_final_draws(rng, rs.draws, rs.stride);
 }
 // The stored draws handed back by slot.
 struct SlotRng {
@@ -430,7 +437,8 @@ struct SlotRng {
     __device__ __forceinline__ float draw(int slot) { return d[slot - FFB_FIN_SLOT0]; }
 };
 #else
-#define FFB_DEFER_SKIP(J, gw, it) ((void)0)
+struct FfbRec {};
+#define FFB_DEFER_SKIP(R) ((void)0)
 #endif
 
 // The rest of an iteration once transform k is picked and the opacity draw
@@ -439,8 +447,13 @@ struct SlotRng {
 template <bool PER_XFORM, class R>
 __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
                                          int k, bool plot, R& rng, u32 gw, u64 it, float& x, float& y, float& ci, u32& fuse,
-                                         float cx, float cy, float scale, u32& inframe) {
+                                         float cx, float cy, float scale, u32& inframe, const FfbRec* slot = nullptr) {
     const float* q = sm + T_XF + k;
+#ifdef FFB_DEFER
+    const FfbRec rs = slot ? *slot : ffb_rec_at(J, gw, it);
+#else
+    (void)slot;
+#endif
     FfbCtx ctx = ffb_ctx(J, gw, it);
 #ifdef FFB_DC
     // Step 1 of the colour flow with a colour-writing variation
@@ -472,7 +485,7 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
         y = rng.draw(0) * 2.0f - 1.0f;
 #endif
         fuse = J.burn_in;
-        FFB_DEFER_SKIP(J, gw, it);
+        FFB_DEFER_SKIP(rs);
         return;
     }
 #ifdef FFB_SPEED
@@ -497,9 +510,9 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
 #else
     ci = ci * q[F_C1 * FFB_MAXX] + q[F_C2 * FFB_MAXX];                       // main_template.wgsl:496-508
 #endif
-    if (fuse > 0u) { fuse -= 1u; FFB_DEFER_SKIP(J, gw, it); return; }     // main_template.wgsl:510-514
+    if (fuse > 0u) { fuse -= 1u; FFB_DEFER_SKIP(rs); return; }            // main_template.wgsl:510-514
 #ifdef FFB_DEFER
-    ffb_defer_store(J, gw, it, k, x, y, ci, plot, rng);
+    ffb_defer_store(rs, k, x, y, ci, plot, rng);
 #else
     ffb_plot_sample(sm, pal, J, k, x, y, ci, plot, rng, ctx, cx, cy, scale, inframe);
 #endif
@@ -755,5 +768,303 @@ extern "C" __global__ void __launch_bounds__(384) ffb_plot(const ffb_launch* __r
         ffb_plot_sample(sm, pal, J, (int)((fl >> 8) & 0xFFu), r.x, r.y, r.z, (fl & 1u) != 0u, rng, ctx, cx, cy, scale, inframe);
     }
     ffb_count_inframe(J, inframe);
+}
+#endif
+
+#if defined(FFB_DEFER) && FFB_RNG_MODE == 1 && !defined(FFB_REFRESH)
+// ---------------------------------------------------------------------------
+// Fused plotting: the walkers and the plot of their samples in one block.
+//
+// The first J.ring_prod threads of a block are producer warps: they carry the
+// block's walkers through the transform-sorted schedule of ffb_chaos_sorted
+// and, instead of plotting, write each iteration's samples (the deferred
+// records) into a ring of J.ring_depth iteration slots in shared memory.  The
+// other warps of the block are consumer warps: they take the slots in order
+// and apply the plot tail -- the final chain, the palette, the symmetry
+// copies, world_to_pixel and the warp-aggregated splat.  A sample never goes
+// to HBM on its way from the walker to the histogram, and the plot's long
+// independent work fills the issue slots the walkers' dependent chains and
+// their sorting barrier leave empty.
+//
+// Hand-over: full[d] (one arrival a producer warp) completes when slot d
+// holds an iteration's records, empty[d] (one arrival a consumer warp) when
+// it has been plotted; a slot's u-th use waits on phase parity u & 1.  Every
+// wait is bounded: past FFB_WAIT_LIMIT polls the kernel sets bit 63 of the
+// in-frame counter (the host reports the render failed) and goes on, so no
+// miscounted hand-over can hang the GPU.
+//
+// One barrier an iteration among the producers: the counter-based stream
+// gives every walker's pick ahead of time (it depends only on the walker's
+// id, the iteration and, with xaos, the previous pick), so the picks of
+// iteration j + 2 are counted while iteration j runs, and iteration j + 1's
+// sort needs only its scatter and gather around a single barrier.  Counters
+// are kept in three rotating sets, slot ranks and walker state in two.
+// Orbits are those of ffb_chaos and ffb_chaos_sorted, bit for bit.
+
+#define FFB_WAIT_LIMIT (1u << 21)
+#define FFB_WAIT_HINT_NS 2000
+
+__device__ __forceinline__ u32 ffb_smem_addr(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void ffb_mbar_init(u64* b, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(ffb_smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void ffb_mbar_arrive(u64* b) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(ffb_smem_addr(b)) : "memory");
+}
+// One poll: the thread may sleep up to FFB_WAIT_HINT_NS in it, and wakes when
+// the phase completes.
+__device__ __forceinline__ bool ffb_mbar_test(u64* b, u32 parity) {
+    u32 ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(ffb_smem_addr(b)), "r"(parity), "n"(FFB_WAIT_HINT_NS)
+                 : "memory");
+    return ok != 0u;
+}
+// Wait for phase `parity` of b: at most FFB_WAIT_LIMIT polls (a few seconds).
+// A wait that gives up marks the block aborted (`abort`, shared memory) and
+// the render failed (bit 63 of the in-frame counter); an aborted block waits
+// no more, so it runs to its end at once whatever went wrong.
+__device__ __forceinline__ void ffb_mbar_wait(u64* b, u32 parity, volatile u32* abort, const ffb_launch& J) {
+    if (*abort) return;
+    for (u32 n = 0; n < FFB_WAIT_LIMIT; ++n)
+        if (ffb_mbar_test(b, parity)) return;
+    *abort = 1u;
+    atomicOr(J.counters, 1ull << 63);
+}
+// The producers' barrier (named barrier 1, producer threads only).
+__device__ __forceinline__ void ffb_prod_sync(u32 n_threads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(n_threads) : "memory");
+}
+
+// A walker's pick at iteration it: the transform, its opacity draw, and the
+// two variation words of Philox block 0 (slots 2, 3).
+struct FfbPick {
+    int k;
+    bool plot;
+    float w2, w3;
+};
+__device__ __forceinline__ FfbPick ffb_pick_at(const float* __restrict__ sm, const ffb_launch& J, int n_xf, u32 wid, u64 it,
+                                               int prev) {
+    const uint4 o = philox4(J.seed_lo, J.seed_hi, wid, (u32)it, 0u, (u32)(it >> 32));
+    FfbPick p;
+    p.k = FFB_PICK(u24(o.x), prev);                                              // main_template.wgsl:198-223
+    p.plot = u24(o.y) < sm[T_XF + F_OPAC * FFB_MAXX + p.k];                      // main_template.wgsl:249
+    p.w2 = u24(o.z);
+    p.w3 = u24(o.w);
+    (void)prev;
+    return p;
+}
+__device__ __forceinline__ u32 ffb_pack_pick(int k, bool plot) { return (u32)k | (plot ? 0x8000u : 0u); }
+
+// Count transform k into cnt (warp-aggregated; every lane of the warp takes part).
+__device__ __forceinline__ void ffb_count_pick(u32* cnt, int k) {
+    const unsigned grp = __match_any_sync(0xffffffffu, k);
+    if ((int)(threadIdx.x & 31u) == __ffs(grp) - 1) atomicAdd(&cnt[k], (u32)__popc(grp));
+}
+// The sorted slot of a walker with transform k: walkers of lower transforms
+// (complete counts) + its rank among those of k (a running count).
+__device__ __forceinline__ u32 ffb_sort_slot(const u32* cnt, u32* rnk, int k) {
+    const int lane = (int)(threadIdx.x & 31u);
+    const unsigned grp = __match_any_sync(0xffffffffu, k);
+    const int leader = __ffs(grp) - 1;
+    u32 base = 0;
+    if (lane == leader) base = atomicAdd(&rnk[k], (u32)__popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    u32 off = 0;
+#pragma unroll 4
+    for (int i = 0; i < k; ++i) off += cnt[i];
+    return off + base + (u32)__popc(grp & ((1u << lane) - 1u));
+}
+
+// Shared memory of the fused kernel after the table and palette.
+struct FfbFused {
+    u64* full;          // ring_depth mbarriers
+    u64* empty;         // ring_depth mbarriers
+    u32* abort;         // set when a wait gave up
+    u32* cnt;           // 3 sets of FFB_MAXX + 1 transform counts
+    u32* rnk;           // 2 sets of FFB_MAXX + 1 running ranks
+    u32* st;            // 2 sets of 10 planes of ring_prod words: the regrouped walkers
+    float4* ring;       // ring_depth x ring_prod records
+    float* ring_draws;  // FFB_NFD planes of ring_depth x ring_prod final-chain draws
+};
+#define FFB_FUSED_PLANES 10
+enum { FS_X, FS_Y, FS_CI, FS_FUSE, FS_WID, FS_KP, FS_A2, FS_A3, FS_B2, FS_B3 };
+
+__device__ __forceinline__ void ffb_fused_put(const FfbFused& S, int set, u32 P, u32 slot, float x, float y, float ci, u32 fuse,
+                                              u32 wid, u32 kp, float a2, float a3, float b2, float b3) {
+    u32* b = S.st + (size_t)set * FFB_FUSED_PLANES * P + slot;
+    b[FS_X * P] = __float_as_uint(x); b[FS_Y * P] = __float_as_uint(y); b[FS_CI * P] = __float_as_uint(ci);
+    b[FS_FUSE * P] = fuse; b[FS_WID * P] = wid; b[FS_KP * P] = kp;
+    b[FS_A2 * P] = __float_as_uint(a2); b[FS_A3 * P] = __float_as_uint(a3);
+    b[FS_B2 * P] = __float_as_uint(b2); b[FS_B3 * P] = __float_as_uint(b3);
+}
+__device__ __forceinline__ void ffb_fused_get(const FfbFused& S, int set, u32 P, u32 slot, float& x, float& y, float& ci, u32& fuse,
+                                              u32& wid, u32& kp, float& a2, float& a3, float& b2, float& b3) {
+    const u32* b = S.st + (size_t)set * FFB_FUSED_PLANES * P + slot;
+    x = __uint_as_float(b[FS_X * P]); y = __uint_as_float(b[FS_Y * P]); ci = __uint_as_float(b[FS_CI * P]);
+    fuse = b[FS_FUSE * P]; wid = b[FS_WID * P]; kp = b[FS_KP * P];
+    a2 = __uint_as_float(b[FS_A2 * P]); a3 = __uint_as_float(b[FS_A3 * P]);
+    b2 = __uint_as_float(b[FS_B2 * P]); b3 = __uint_as_float(b[FS_B3 * P]);
+}
+
+// Producer warps: the block's walkers, sorted by transform every iteration.
+// Thread state after each gather: the walker's point, colour index, fuse and
+// id, its picks for this iteration (k, plot; words a2, a3) and the next
+// (kn, plotn; words b2, b3).
+__device__ __forceinline__ void ffb_fused_producer(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
+                                                   const FfbFused& S) {
+    const u32 P = J.ring_prod, D = J.ring_depth;
+    const int tid = (int)threadIdx.x, lane = tid & 31;
+    const int NC = FFB_MAXX + 1;
+    const int n_xf = (int)J.n_xf;
+    const u32 n = J.n_iters;
+    const u32 w0 = (blockIdx.x - J.block0) * P + (u32)tid;
+    bool active = w0 < J.n_walkers;
+    u32 wid = J.walker0 + w0;
+    float x = 0.f, y = 0.f, ci = 0.f;
+    u32 fuse = 0;
+    int prev = 0;
+    if (active) ffb_start(sm, J, w0, wid, x, y, ci, fuse, prev);
+    const float scale = (float)min(J.width, J.height) * 0.25f;
+    const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
+    // The first two iterations' picks, counted into sets 0 and 1.
+    FfbPick p0{FFB_MAXX, false, 0.f, 0.f}, p1{FFB_MAXX, false, 0.f, 0.f};
+    if (active) {
+        p0 = ffb_pick_at(sm, J, n_xf, wid, J.it0, prev);
+        if (n > 1) p1 = ffb_pick_at(sm, J, n_xf, wid, J.it0 + 1, p0.k);
+    }
+    ffb_count_pick(S.cnt, p0.k);
+    if (n > 1) ffb_count_pick(S.cnt + NC, p1.k);
+    ffb_prod_sync(P);
+    {
+        const u32 slot = ffb_sort_slot(S.cnt, S.rnk, p0.k);
+        ffb_fused_put(S, 0, P, slot, x, y, ci, fuse, wid, ffb_pack_pick(p0.k, p0.plot) | (ffb_pack_pick(p1.k, p1.plot) << 16),
+                      p0.w2, p0.w3, p1.w2, p1.w3);
+    }
+    ffb_prod_sync(P);
+    u32 kp;
+    float a2, a3, b2, b3;
+    ffb_fused_get(S, 0, P, (u32)tid, x, y, ci, fuse, wid, kp, a2, a3, b2, b3);
+    u32 inframe = 0;
+    for (u32 j = 0; j < n; ++j) {
+        const u64 it = J.it0 + j;
+        const u32 d = j % D;
+        const int k = (int)(kp & 0x7FFFu);
+        const bool plot = (kp & 0x8000u) != 0u;
+        active = k < FFB_MAXX;
+        // This iteration's records go to ring slot d once the consumers are done with its last use.
+        if (j >= D) ffb_mbar_wait(&S.empty[d], ((j / D) - 1u) & 1u, S.abort, J);
+        const FfbRec rs{S.ring + (size_t)d * P + tid, S.ring_draws + (size_t)d * P + tid, (u64)D * P};
+        if (active) {
+            PhiloxRng rng;
+            rng.w[0] = 0.f;
+            rng.w[1] = 0.f;
+            rng.w[2] = a2;
+            rng.w[3] = a3;
+            rng.fill_from(1, J.seed_lo, J.seed_hi, wid, it);
+            ffb_step<true>(sm, pal, J, k, plot, rng, wid, it, x, y, ci, fuse, cx, cy, scale, inframe, &rs);
+        } else {
+            FFB_DEFER_SKIP(rs);
+        }
+        __syncwarp();
+        if (lane == 0) ffb_mbar_arrive(&S.full[d]);
+        if (j + 1 == n) {
+            prev = k;
+            break;
+        }
+        // The pick two iterations ahead, counted now (set (j + 2) % 3).
+        const int kn = (int)((kp >> 16) & 0x7FFFu);
+        const bool pn = (kp >> 31) != 0u;
+        FfbPick p2{FFB_MAXX, false, 0.f, 0.f};
+        if (active && j + 2 < n) p2 = ffb_pick_at(sm, J, n_xf, wid, it + 2, kn);
+        if (j + 2 < n) ffb_count_pick(S.cnt + ((j + 2) % 3) * NC, p2.k);
+        // Counters whose last reader ran before the previous barrier: zero them for their next use.
+        for (int i = tid; i < NC; i += (int)P) {
+            S.cnt[(j % 3) * NC + i] = 0u;
+            S.rnk[(j % 2) * NC + i] = 0u;
+        }
+        // Regroup by next iteration's transform.
+        const u32 slot = ffb_sort_slot(S.cnt + ((j + 1) % 3) * NC, S.rnk + ((j + 1) % 2) * NC, kn);
+        ffb_fused_put(S, (int)((j + 1) % 2), P, slot, x, y, ci, fuse, wid,
+                      ffb_pack_pick(kn, pn) | (ffb_pack_pick(p2.k, p2.plot) << 16), b2, b3, p2.w2, p2.w3);
+        ffb_prod_sync(P);
+        ffb_fused_get(S, (int)((j + 1) % 2), P, (u32)tid, x, y, ci, fuse, wid, kp, a2, a3, b2, b3);
+    }
+    (void)inframe;
+    if (active) J.walkers[wid - J.walker0] = make_float4(x, y, ci, __uint_as_float(FFB_PACK_FUSE(fuse, prev)));
+}
+
+// Consumer warps: plot each ring slot's records, slot after slot.
+__device__ __forceinline__ void ffb_fused_consumer(const float* __restrict__ sm, const float4* __restrict__ pal, const ffb_launch& J,
+                                                   const FfbFused& S) {
+    const u32 P = J.ring_prod, D = J.ring_depth;
+    const u32 C = blockDim.x - P;
+    const u32 c = threadIdx.x - P;
+    const int lane = (int)(threadIdx.x & 31u);
+    const float scale = (float)min(J.width, J.height) * 0.25f;
+    const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
+    u32 inframe = 0;
+    for (u32 j = 0; j < J.n_iters; ++j) {
+        const u32 d = j % D;
+        ffb_mbar_wait(&S.full[d], (j / D) & 1u, S.abort, J);
+        const float4* rr = S.ring + (size_t)d * P;
+        for (u32 i = c; i < P; i += C) {
+            const float4 r = rr[i];
+            const u32 fl = __float_as_uint(r.w);
+            if (!(fl & 2u)) continue;
+            float fd[FFB_NFD > 0 ? FFB_NFD : 1];
+#pragma unroll
+            for (int m = 0; m < FFB_NFD; ++m) fd[m] = S.ring_draws[(size_t)m * D * P + (size_t)d * P + i];
+            SlotRng rng{fd};
+            FfbCtx ctx{nullptr, 0u, 0.0f, 0u, 0u, 0u, 0ull};                     // deferred finals carry no state
+            ffb_plot_sample(sm, pal, J, (int)((fl >> 8) & 0xFFu), r.x, r.y, r.z, (fl & 1u) != 0u, rng, ctx, cx, cy, scale,
+                            inframe);
+        }
+        __syncwarp();
+        if (lane == 0) ffb_mbar_arrive(&S.empty[d]);
+    }
+    ffb_count_inframe(J, inframe);
+}
+
+// One block: ring_prod producer threads (a multiple of 32) and the rest
+// consumers (a multiple of 32).  Shared memory after the table and palette:
+// 2 x ring_depth mbarriers, the abort word (8 bytes), 5 x (FFB_MAXX + 1)
+// counters, 2 x 10 x ring_prod
+// walker words, up to 12 bytes of padding, ring_depth x ring_prod records of
+// 16 bytes and FFB_NFD x ring_depth x ring_prod draws.
+extern "C" __global__ void __launch_bounds__(1024, 1) ffb_chaos_fused(const ffb_launch* __restrict__ jobs, int n_jobs) {
+    extern __shared__ float4 ffb_smem4[];
+    float* sm = reinterpret_cast<float*>(ffb_smem4);
+    float4* pal;
+    const ffb_launch& J = ffb_stage(jobs, n_jobs, sm, pal);
+    const u32 P = J.ring_prod, D = J.ring_depth;
+    const int NC = FFB_MAXX + 1;
+    FfbFused S;
+    S.full = reinterpret_cast<u64*>(pal + J.pal_n);
+    S.empty = S.full + D;
+    S.abort = reinterpret_cast<u32*>(S.empty + D);
+    S.cnt = S.abort + 2;
+    S.rnk = S.cnt + 3 * NC;
+    S.st = S.rnk + 2 * NC;
+    // The ring starts at the next 16-byte boundary after the walker planes.
+    S.ring = reinterpret_cast<float4*>((reinterpret_cast<size_t>(S.st + 2 * FFB_FUSED_PLANES * P) + 15) & ~(size_t)15);
+    S.ring_draws = reinterpret_cast<float*>(S.ring + (size_t)D * P);
+    // Launch-shape guard (the host sizes the block; a mismatch would miscount the hand-overs).
+    const bool ok = P >= 32 && P % 32 == 0 && P < blockDim.x && (blockDim.x - P) % 32 == 0 && D >= 2;
+    if (threadIdx.x == 0 && ok) {
+        for (u32 i = 0; i < D; ++i) {
+            ffb_mbar_init(&S.full[i], P / 32);
+            ffb_mbar_init(&S.empty[i], (blockDim.x - P) / 32);
+        }
+    }
+    for (int i = (int)threadIdx.x; i < 5 * NC + 2; i += (int)blockDim.x) S.abort[i] = 0u;
+    __syncthreads();
+    if (!ok) {
+        if (threadIdx.x == 0) atomicOr(J.counters, 1ull << 63);
+        return;
+    }
+    if (threadIdx.x < P) ffb_fused_producer(sm, pal, J, S);
+    else ffb_fused_consumer(sm, pal, J, S);
 }
 #endif

@@ -93,8 +93,9 @@ struct Launch {
     void* rec;          // deferred plotting: the launch's samples
     void* rec_draws;    // and their final chain's draws
     void* state;        // the walkers' variation state (slot-major planes of n_walkers)
+    uint32_t ring_prod, ring_depth;   // fused plotting: producer threads a block, iteration slots of the ring
 };
-static_assert(sizeof(Launch) == 144, "launch record layout");
+static_assert(sizeof(Launch) == 152, "launch record layout");
 
 struct DevBuf {
     void* p = nullptr;
@@ -115,7 +116,8 @@ struct Module {
     cudaLibrary_t lib = nullptr;
     cudaKernel_t chaos = nullptr, chaos_sorted = nullptr, probe = nullptr, apply = nullptr;
     cudaKernel_t plot = nullptr;   // deferred-plot modules only
-    int smem_attr_plot = 0;
+    cudaKernel_t fused = nullptr;  // deferred-plot modules of the counter-based stream without orbit refresh
+    int smem_attr_plot = 0, smem_attr_fused = 0;
     // Differentiable-render modules (ffb_diff.cuh) only.
     cudaKernel_t dforward = nullptr, dadjoint = nullptr, dtheta = nullptr, dprobe = nullptr;
     int smem_attr = 0, smem_attr_sorted = 0, smem_attr_dadj = 0;
@@ -123,6 +125,13 @@ struct Module {
 };
 
 std::string nvrtc_options_key() { return "sm_100a|c++17|ftz|prec-div|prec-sqrt|nofmad"; }
+
+// Whether a module's source compiles ffb_chaos_fused (ffb_kernels.cuh): a
+// deferred-plot module of the counter-based stream without orbit refresh.
+bool fused_capable(const std::string& src) {
+    return src.find("#define FFB_DEFER 1") != std::string::npos && src.find("#define FFB_RNG_MODE 1") != std::string::npos &&
+           src.find("#define FFB_REFRESH") == std::string::npos;
+}
 
 }  // namespace
 }  // namespace ffb
@@ -224,8 +233,10 @@ struct ffb_renderer {
         ck(cudaLibraryGetKernel(&m.chaos_sorted, m.lib, "ffb_chaos_sorted"), "cudaLibraryGetKernel(ffb_chaos_sorted)");
         ck(cudaLibraryGetKernel(&m.probe, m.lib, "ffb_probe"), "cudaLibraryGetKernel(ffb_probe)");
         ck(cudaLibraryGetKernel(&m.apply, m.lib, "ffb_apply_points"), "cudaLibraryGetKernel(ffb_apply_points)");
-        if (src.find("#define FFB_DEFER 1") != std::string::npos)
+        if (src.find("#define FFB_DEFER 1") != std::string::npos) {
             ck(cudaLibraryGetKernel(&m.plot, m.lib, "ffb_plot"), "cudaLibraryGetKernel(ffb_plot)");
+            if (fused_capable(src)) ck(cudaLibraryGetKernel(&m.fused, m.lib, "ffb_chaos_fused"), "cudaLibraryGetKernel(ffb_chaos_fused)");
+        }
         if (src.find("ffb_diff_forward") != std::string::npos) {
             ck(cudaLibraryGetKernel(&m.dforward, m.lib, "ffb_diff_forward"), "cudaLibraryGetKernel(ffb_diff_forward)");
             ck(cudaLibraryGetKernel(&m.dadjoint, m.lib, "ffb_diff_adjoint"), "cudaLibraryGetKernel(ffb_diff_adjoint)");
@@ -347,7 +358,7 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     if (P.accumulate == 2 && P.flame.color_mode != 0)
         fail(FFB_ERR_INVALID, "tile-sorted accumulation records palette indices: not with the speed colour mode");
     P.plot = job->plot;
-    if (P.plot > 2) fail(FFB_ERR_INVALID, "plot must be 0 (auto), 1 (inline) or 2 (deferred)");
+    if (P.plot > 3) fail(FFB_ERR_INVALID, "plot must be 0 (auto), 1 (inline), 2 (deferred) or 3 (fused)");
     P.progress = job->progress;
     P.cancelled = job->cancelled;
     P.progress_user = job->progress_user;
@@ -357,7 +368,7 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     // Auto: deferred for the sorted schedule over enough walkers to fill
     // the machine (measured on the 1080p ss2 frame: 51 ms against 66).
     const bool can_defer = P.rng == RNG_PHILOX && !tiled && !P.flame.filter.on() && P.walkers <= (1u << 23);
-    const bool defer = can_defer && (P.plot == 2 || (P.plot == 0 && P.schedule != 1 && P.walkers >= 16384));
+    const bool defer = can_defer && (P.plot >= 2 || (P.plot == 0 && P.schedule != 1 && P.walkers >= 16384));
     P.plan = make_plan(P.flame, P.rng, P.math, 0, P.threads_set ? P.threads : 128, false, P.count_bits == 64, 0, 0, tiled, defer);
     P.table = make_table(P.plan, P.flame);
     P.palette = palette_table(P.flame);
@@ -464,6 +475,32 @@ uint64_t plotted_samples(const Prepared& P, uint32_t walker0) {
     return plotted;
 }
 
+// The in-frame count a render read back.  Bit 63 is set by a kernel whose
+// bounded wait gave up (ffb_chaos_fused's hand-over): the render is void.
+void check_inframe(uint64_t v) {
+    if (v >> 63) fail(FFB_ERR_CUDA, "the fused plot hand-over timed out on the device; the render is incomplete");
+}
+
+// Fused plotting's block shape: consumer threads (the plot warps) beside the
+// producers, ring slots (iterations in flight between the two), iterations
+// a launch.
+#ifndef FFB_FUSED_CONSUMERS
+#define FFB_FUSED_CONSUMERS 256
+#endif
+#ifndef FFB_FUSED_RING
+#define FFB_FUSED_RING 8
+#endif
+constexpr uint32_t kFusedConsumers = FFB_FUSED_CONSUMERS;
+constexpr uint32_t kFusedRing = FFB_FUSED_RING;
+constexpr uint64_t kFusedIters = 4096;
+
+// Shared memory of ffb_chaos_fused after its table and palette (the layout
+// ffb_kernels.cuh carves): mbarriers, the abort word, counters, two sets of ten walker
+// planes, padding to 16 bytes, the record ring and its draw planes.
+int fused_smem_bytes(uint32_t prod, uint32_t ring, int nc, int nfd) {
+    return (int)(2 * ring * 8 + 8 + 5 * (uint32_t)nc * 4 + 2 * 10 * prod * 4 + 16 + ring * prod * 16 + (uint32_t)nfd * ring * prod * 4);
+}
+
 // Chaos game of a prepared flame into r->hist (wi*hi float4, cleared here).
 void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walker0, uint64_t* inframe_out,
                float4* ext_hist = nullptr) {
@@ -502,10 +539,30 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         threads = std::min<uint32_t>(1024, std::max<uint32_t>(64, (per_sm + 31) / 32 * 32));
         if (P.threads_set) threads = std::min<uint32_t>(1024, std::max<uint32_t>(32, (P.threads + 31) / 32 * 32));
     }
+    // Fused plotting (ffb_job.plot 3): producer warps (the sorted walkers)
+    // and consumer warps (the plot) in one block, the samples handed over in
+    // shared memory.  The deferred-plot module carries the kernel.
+    const bool fused = P.plan.defer && P.plot == 3 && sorted && m.fused != nullptr;
+    uint32_t consumers = 0, ring = 0;
+    if (fused) {
+        consumers = kFusedConsumers;
+        ring = kFusedRing;
+        uint32_t per_sm = (P.walkers + (uint32_t)r->n_sm - 1) / (uint32_t)r->n_sm;
+        threads = std::min<uint32_t>(1024 - consumers, std::max<uint32_t>(64, (per_sm + 31) / 32 * 32));
+        if (P.threads_set) threads = std::min<uint32_t>(1024 - consumers, std::max<uint32_t>(32, (P.threads + 31) / 32 * 32));
+    }
     int smem = ((P.plan.table_size + 3) / 4) * 16 + (int)pal_n * 16;
-    if (sorted) smem += (int)threads * 8 * 4 + 2 * (P.plan.maxx + 1) * 4;
-    const void* kfn = sorted ? (const void*)m.chaos_sorted : (const void*)m.chaos;
-    int& attr = sorted ? m.smem_attr_sorted : m.smem_attr;
+    int nfd_fused = 0;
+    if (fused) {
+        for (auto& fi : P.plan.fin) for (const VarDef* v : fi.vars) nfd_fused += v->draws;
+        // A shallower ring where a deep one would not fit the 227 KB of a block.
+        while (ring > 2 && smem + fused_smem_bytes(threads, ring, P.plan.maxx + 1, nfd_fused) > 227 * 1024) ring /= 2;
+        smem += fused_smem_bytes(threads, ring, P.plan.maxx + 1, nfd_fused);
+    } else if (sorted) {
+        smem += (int)threads * 8 * 4 + 2 * (P.plan.maxx + 1) * 4;
+    }
+    const void* kfn = fused ? (const void*)m.fused : sorted ? (const void*)m.chaos_sorted : (const void*)m.chaos;
+    int& attr = fused ? m.smem_attr_fused : sorted ? m.smem_attr_sorted : m.smem_attr;
     if (smem > 48 * 1024 && attr < smem) {
         ck(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
         attr = smem;
@@ -523,11 +580,12 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     // multiprocessor, so the sorted chaos kernel's one block still fits
     // beside it (with more plot blocks the two stopped overlapping: 77.7 ms
     // a frame instead of 51; 256 iterations measured best of 64-512).
-    const bool defer = P.plan.defer;
+    const bool defer = P.plan.defer && !fused;
     constexpr uint64_t kDeferIters = 256;
     constexpr unsigned kPlotThreads = 384;
     // At most 2^27 records (2 GiB) a buffer.
     if (defer) chunk = std::max<uint64_t>(16, std::min<uint64_t>(kDeferIters, (1ull << 27) / P.walkers));
+    if (fused) chunk = kFusedIters;
     const uint32_t blocks = (P.walkers + threads - 1) / threads;
     const double rot = P.flame.rotation;
     Launch L{};
@@ -540,6 +598,8 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     L.pal_n = pal_n; L.width = (int32_t)P.wi; L.height = (int32_t)P.hi;
     L.zoom = P.flame.zoom; L.pan_x = (float)P.flame.pan_x; L.pan_y = (float)P.flame.pan_y;
     L.cos_r = (float)std::cos(rot); L.sin_r = (float)std::sin(rot);
+    L.ring_prod = fused ? threads : 0;
+    L.ring_depth = fused ? ring : 0;
     // Tile-sorted accumulation: launches sized so one launch's records (one
     // a walker slot, iteration and symmetry copy at most) fit the record
     // buffer, about 2^29 of them; each launch is followed by the
@@ -611,7 +671,7 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         }
         if (filt) ck(cudaMemsetAsync(batch, 0, npx * 16, s), "clear batch histogram");
         if (defer && i >= 2) ck(cudaStreamWaitEvent(s, r->ev_plot[i % 2], 0), "record buffer free");
-        ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch ffb_chaos");
+        ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads + consumers), args, (size_t)smem, s), "launch ffb_chaos");
         r->launches += 1;
         if (watched) {
             ck(cudaEventRecord(r->ev_flight[i % 2], s), "event");
@@ -746,6 +806,7 @@ void render_device(ffb_renderer* r, const char* config, size_t len, const ffb_jo
         ck(cudaStreamSynchronize(s), "render");
         float ms = 0.f;
         ck(cudaEventElapsedTime(&ms, r->ev0, r->ev1), "event time");
+        check_inframe(*h_inframe);
         if (out) { out->render_time_ms = ms; out->inframe_samples = *h_inframe; }
     }
     r->fill_counts(out);
@@ -981,6 +1042,7 @@ FFB_API int ffb_histogram(ffb_renderer* r, const char* config, size_t len, const
         std::vector<float> h(npx * 4);
         ck(cudaMemcpyAsync(h.data(), r->hist.p, npx * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
         ck(cudaStreamSynchronize(r->stream), "histogram");
+        check_inframe(inframe);
         for (size_t i = 0; i < npx; ++i) {
             if (counts) { uint32_t c; std::memcpy(&c, &h[i * 4 + 3], 4); counts[i] = c; }
             if (rgb) { rgb[i * 3] = h[i * 4]; rgb[i * 3 + 1] = h[i * 4 + 1]; rgb[i * 3 + 2] = h[i * 4 + 2]; }
@@ -1015,6 +1077,7 @@ FFB_API int ffb_histogram_f32(ffb_renderer* r, const char* config, size_t len, c
         std::vector<float> h(npx * 4);
         ck(cudaMemcpyAsync(h.data(), r->hist.p, npx * 16, cudaMemcpyDeviceToHost, r->stream), "readback");
         ck(cudaStreamSynchronize(r->stream), "histogram");
+        check_inframe(inframe);
         const bool f = P.flame.filter.on();
         for (size_t i = 0; i < npx; ++i) {
             if (counts) { uint32_t c; std::memcpy(&c, &h[i * 4 + 3], 4); counts[i] = f ? h[i * 4 + 3] : (float)c; }
@@ -1075,6 +1138,7 @@ FFB_API int ffb_histogram_u64(ffb_renderer* r, const char* config, size_t len, c
         std::vector<unsigned long long> h(npx * 4);
         ck(cudaMemcpyAsync(h.data(), r->hist.p, npx * 32, cudaMemcpyDeviceToHost, r->stream), "readback");
         ck(cudaStreamSynchronize(r->stream), "histogram");
+        check_inframe(inframe);
         for (size_t i = 0; i < npx; ++i) {
             counts[i] = h[i * 4 + 3];
             if (rgb) for (int q = 0; q < 3; ++q) rgb[i * 3 + q] = (float)((double)h[i * 4 + q] / 16777216.0);

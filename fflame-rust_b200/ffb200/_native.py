@@ -122,7 +122,7 @@ SCHEDULE = {"auto": 0, "plain": 1, "sorted": 2}
 
 
 ACCUMULATE = {"auto": 0, "direct": 1, "tiled": 2}
-PLOT = {"auto": 0, "inline": 1, "deferred": 2}
+PLOT = {"auto": 0, "inline": 1, "deferred": 2, "fused": 3}
 
 
 def make_job(width=0, height=0, iterations=0, iterations_per_thread=0, burn_in=0, walkers=0, supersample=1,
