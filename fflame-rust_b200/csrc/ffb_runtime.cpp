@@ -583,6 +583,10 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     const bool defer = P.plan.defer && !fused;
     constexpr uint64_t kDeferIters = 256;
     constexpr unsigned kPlotThreads = 384;
+#ifndef FFB_PLOT_BLOCKS
+#define FFB_PLOT_BLOCKS 1
+#endif
+    constexpr unsigned kPlotBlocksPerSm = FFB_PLOT_BLOCKS;
     // At most 2^27 records (2 GiB) a buffer.
     if (defer) chunk = std::max<uint64_t>(16, std::min<uint64_t>(kDeferIters, (1ull << 27) / P.walkers));
     if (fused) chunk = kFusedIters;
@@ -684,7 +688,7 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
         if (defer) {
             ck(cudaEventRecord(r->ev_main[i % 2], s), "event");
             ck(cudaStreamWaitEvent(r->plot_stream, r->ev_main[i % 2], 0), "plot waits for its samples");
-            ck(cudaLaunchKernel((const void*)m.plot, dim3((unsigned)r->n_sm), dim3(kPlotThreads), args, (size_t)smem_plot,
+            ck(cudaLaunchKernel((const void*)m.plot, dim3((unsigned)r->n_sm * kPlotBlocksPerSm), dim3(kPlotThreads), args, (size_t)smem_plot,
                                 r->plot_stream), "launch ffb_plot");
             ck(cudaEventRecord(r->ev_plot[i % 2], r->plot_stream), "event");
             r->launches += 1;
@@ -762,16 +766,21 @@ const float* upload_lut(ffb_renderer* r, const Flame& f, cudaStream_t s) {
 // The tail of a render: density estimation (if configured) and the tone map
 // of output rows [row0, row0 + rows) of a summed histogram holding
 // `samples` plotted samples, into `d_rgba` (that band, row0 first).
+// `hist` holds internal rows [hist_row0, hist_row0 + hist_rows) of the
+// histogram (the whole of it by default): a band's rows and the DE reach
+// around them are enough, since density estimation reads no source farther
+// than its radius.
 void finish_device(ffb_renderer* r, const Prepared& P, const float4* hist, uint64_t samples, uint32_t row0, uint32_t rows,
-                   int transparent, void* d_rgba, cudaStream_t s) {
+                   int transparent, void* d_rgba, cudaStream_t s, uint32_t hist_row0 = 0, uint32_t hist_rows = 0) {
     const uint32_t ss = P.ss;
-    const uint32_t y_lo = row0 * ss, h_band = rows * ss;
+    if (hist_rows == 0) hist_rows = P.hi - hist_row0;
+    const uint32_t y_lo = row0 * ss - hist_row0, h_band = rows * ss;
     const float4* src = P.plan.exact ? nullptr : hist + (size_t)y_lo * P.wi;
     bool count_f = P.flame.filter.on();              // a filtered histogram holds float counts
     const ulonglong4* ex = P.plan.exact ? (const ulonglong4*)hist : nullptr;
     if (ex) src = nullptr;
     if (P.flame.de.max_radius > 0.0f) {
-        src = run_de(r, ex ? nullptr : hist, P.wi, P.hi, (double)P.flame.de.max_radius * ss, (double)P.flame.de.min_radius * ss,
+        src = run_de(r, ex ? nullptr : hist, P.wi, hist_rows, (double)P.flame.de.max_radius * ss, (double)P.flame.de.min_radius * ss,
                      (double)P.flame.de.curve, s, y_lo, h_band, ex, count_f);
         count_f = true;
     }
@@ -1345,6 +1354,29 @@ FFB_API int ffb_finish_device(ffb_renderer* r, const char* config, size_t len, c
         check_de(P.flame, P.ss);
         finish_device(r, P, (const float4*)d_hist, total_samples, row0, rows, job->transparent, d_rgba,
                       stream ? (cudaStream_t)stream : r->stream);
+    });
+}
+
+FFB_API int ffb_finish_band(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, const void* d_hist,
+                            uint32_t hist_row0, uint32_t hist_rows, uint64_t total_samples, uint32_t row0, uint32_t rows,
+                            void* d_rgba, void* stream) {
+    return guard([&] {
+        if (!r || !job || !d_hist || !d_rgba) fail(FFB_ERR_INVALID, "NULL argument");
+        if (rows == 0 || row0 + rows > job->height) fail(FFB_ERR_INVALID, "row band outside the image");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Prepared P = prepare(config, len, job);
+        check_de(P.flame, P.ss);
+        if (P.plan.exact) fail(FFB_ERR_INVALID, "histogram bands hold u32 counts (count_bits 32)");
+        // The window must hold the band and the DE reach around it (clamped to the image).
+        const uint32_t reach = P.flame.de.max_radius > 0.0f ? (uint32_t)std::ceil((double)P.flame.de.max_radius * P.ss) : 0u;
+        const uint32_t y_lo = row0 * P.ss, y_hi = (row0 + rows) * P.ss;
+        const uint32_t need_lo = y_lo > reach ? y_lo - reach : 0u, need_hi = std::min<uint32_t>(P.hi, y_hi + reach);
+        if ((uint64_t)hist_row0 + hist_rows > P.hi || hist_row0 > need_lo || hist_row0 + hist_rows < need_hi)
+            fail(FFB_ERR_INVALID, "the histogram window must hold internal rows [" + std::to_string(need_lo) + ", " +
+                                      std::to_string(need_hi) + "): the band and the density-estimation reach around it");
+        finish_device(r, P, (const float4*)d_hist, total_samples, row0, rows, job->transparent, d_rgba,
+                      stream ? (cudaStream_t)stream : r->stream, hist_row0, hist_rows);
     });
 }
 

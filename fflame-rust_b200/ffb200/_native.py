@@ -25,7 +25,7 @@ EXPORTS = [
     "ffb_last_error", "ffb_version", "ffb_renderer_create", "ffb_renderer_destroy", "ffb_render",
     "ffb_render_device", "ffb_histogram", "ffb_tonemap", "ffb_density_estimate", "ffb_probe",
     "ffb_apply_points", "ffb_specialize", "ffb_atomic_bench", "ffb_chaos_device", "ffb_hist_pack",
-    "ffb_hist_unpack", "ffb_finish_device", "ffb_histogram_u64", "ffb_batch_create", "ffb_batch_run",
+    "ffb_hist_unpack", "ffb_finish_device", "ffb_finish_band", "ffb_histogram_u64", "ffb_batch_create", "ffb_batch_run",
     "ffb_batch_output", "ffb_batch_info", "ffb_batch_destroy", "ffb_density_estimate_static",
     "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
     "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize", "ffb_encode_png",
@@ -310,6 +310,17 @@ class Renderer:
         _check(lib().ffb_finish_device(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), ctypes.c_void_p(d_hist),
                                        ctypes.c_uint64(total_samples), ctypes.c_uint32(row0), ctypes.c_uint32(rows),
                                        ctypes.c_void_p(d_rgba), ctypes.c_void_p(stream or 0)))
+
+    def finish_band(self, config, width, height, d_hist, hist_row0, hist_rows, total_samples, row0, rows, d_rgba,
+                    stream=None, **job):
+        """finish_device from a window of the summed histogram: internal rows
+        [hist_row0, hist_row0 + hist_rows), covering the band and the DE reach."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        _check(lib().ffb_finish_band(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), ctypes.c_void_p(d_hist),
+                                     ctypes.c_uint32(hist_row0), ctypes.c_uint32(hist_rows), ctypes.c_uint64(total_samples),
+                                     ctypes.c_uint32(row0), ctypes.c_uint32(rows), ctypes.c_void_p(d_rgba),
+                                     ctypes.c_void_p(stream or 0)))
 
     def atomic_bench(self, pixels, samples, kind=0):
         ms = ctypes.c_double()

@@ -252,6 +252,16 @@ int ffb_hist_unpack(ffb_renderer* r, const void* d_counts, const void* d_rgb, ui
  * (rows*width*4 bytes).  The DE halo is read from the whole histogram. */
 int ffb_finish_device(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, const void* d_hist,
                       uint64_t total_samples, uint32_t row0, uint32_t rows, void* d_rgba, void* stream);
+/* The same from a window of the summed histogram: d_hist holds internal rows
+ * [hist_row0, hist_row0 + hist_rows) (width*ss float4 a row), which must
+ * cover the band's rows and the density-estimation reach around them
+ * (ceil(radius * ss) rows each side, clamped to the image) -- what a rank
+ * receives from a reduce-scatter of row windows (the exchange step planned
+ * in place of the reference's single-GPU accumulate, accumulate.wgsl:115-230;
+ * the reference renders on one device).  FFB_ERR_INVALID when it does not. */
+int ffb_finish_band(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, const void* d_hist,
+                    uint32_t hist_row0, uint32_t hist_rows, uint64_t total_samples, uint32_t row0, uint32_t rows,
+                    void* d_rgba, void* stream);
 
 /* ---- the differentiable render: an addition beside the reference's render
  * (which has no gradients).  The chaos game with a bilinear splat and a
