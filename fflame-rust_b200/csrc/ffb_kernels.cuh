@@ -871,9 +871,15 @@ __device__ __forceinline__ u32 ffb_sort_slot(const u32* cnt, u32* rnk, int k) {
     u32 base = 0;
     if (lane == leader) base = atomicAdd(&rnk[k], (u32)__popc(grp));
     base = __shfl_sync(0xffffffffu, base, leader);
+    // Walkers of lower transforms: every count loaded at once (independent
+    // shared loads), summed under a predicate -- no loop whose length, and
+    // chain of dependent loads, follows k.
     u32 off = 0;
-#pragma unroll 4
-    for (int i = 0; i < k; ++i) off += cnt[i];
+#pragma unroll
+    for (int i = 0; i < FFB_MAXX; ++i) {
+        const u32 c = cnt[i];
+        off += i < k ? c : 0u;
+    }
     return off + base + (u32)__popc(grp & ((1u << lane) - 1u));
 }
 
@@ -953,6 +959,12 @@ __device__ __forceinline__ void ffb_fused_producer(const float* __restrict__ sm,
         const int k = (int)(kp & 0x7FFFu);
         const bool plot = (kp & 0x8000u) != 0u;
         active = k < FFB_MAXX;
+        // The pick two iterations ahead (independent of this step's point:
+        // its Philox rounds overlap the step's latency), counted after it.
+        const int kn = (int)((kp >> 16) & 0x7FFFu);
+        const bool pn = (kp >> 31) != 0u;
+        FfbPick p2{FFB_MAXX, false, 0.f, 0.f};
+        if (active && j + 2 < n) p2 = ffb_pick_at(sm, J, n_xf, wid, it + 2, kn);
         // This iteration's records go to ring slot d once the consumers are done with its last use.
         if (j >= D) ffb_mbar_wait(&S.empty[d], ((j / D) - 1u) & 1u, S.abort, J);
         const FfbRec rs{S.ring + (size_t)d * P + tid, S.ring_draws + (size_t)d * P + tid, (u64)D * P};
@@ -973,11 +985,7 @@ __device__ __forceinline__ void ffb_fused_producer(const float* __restrict__ sm,
             prev = k;
             break;
         }
-        // The pick two iterations ahead, counted now (set (j + 2) % 3).
-        const int kn = (int)((kp >> 16) & 0x7FFFu);
-        const bool pn = (kp >> 31) != 0u;
-        FfbPick p2{FFB_MAXX, false, 0.f, 0.f};
-        if (active && j + 2 < n) p2 = ffb_pick_at(sm, J, n_xf, wid, it + 2, kn);
+        // Count the pick two ahead (set (j + 2) % 3).
         if (j + 2 < n) ffb_count_pick(S.cnt + ((j + 2) % 3) * NC, p2.k);
         // Counters whose last reader ran before the previous barrier: zero them for their next use.
         for (int i = tid; i < NC; i += (int)P) {

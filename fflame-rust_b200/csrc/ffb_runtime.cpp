@@ -485,7 +485,7 @@ void check_inframe(uint64_t v) {
 // producers, ring slots (iterations in flight between the two), iterations
 // a launch.
 #ifndef FFB_FUSED_CONSUMERS
-#define FFB_FUSED_CONSUMERS 256
+#define FFB_FUSED_CONSUMERS 576
 #endif
 #ifndef FFB_FUSED_RING
 #define FFB_FUSED_RING 8
@@ -576,15 +576,18 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
     if (filt) chunk = P.ipt;
     // Deferred plotting: launches of kDeferIters iterations, each followed
     // by the plot of its samples on the plot stream, which overlaps the
-    // next launch (two record buffers).  The plot kernel runs one block a
-    // multiprocessor, so the sorted chaos kernel's one block still fits
-    // beside it (with more plot blocks the two stopped overlapping: 77.7 ms
-    // a frame instead of 51; 256 iterations measured best of 64-512).
+    // next launch (two record buffers).  The plot kernel runs two blocks of
+    // 384 threads a multiprocessor: with the sorted chaos kernel's block
+    // (448 threads x 48 registers) that is 1216 threads and 51K registers,
+    // so both stay resident (measured 1080p ss2 frames: one plot block
+    // 58.6 ms, two 54.2, three -- which no longer fit beside the chaos
+    // block -- 55.5-57.8, eight 77.7; 256 iterations a launch measured best
+    // of 64-512).
     const bool defer = P.plan.defer && !fused;
     constexpr uint64_t kDeferIters = 256;
     constexpr unsigned kPlotThreads = 384;
 #ifndef FFB_PLOT_BLOCKS
-#define FFB_PLOT_BLOCKS 1
+#define FFB_PLOT_BLOCKS 2
 #endif
     constexpr unsigned kPlotBlocksPerSm = FFB_PLOT_BLOCKS;
     // At most 2^27 records (2 GiB) a buffer.
