@@ -342,6 +342,7 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(wl)
     if world == 1 and not args.no_extra and args.workload == "full_1080p_ss2":
+        line["fused"] = leg(fused_leg, r, wl, args)
         line["parity"] = leg(parity_leg, r, wl)
         line["batched"] = leg(run_batched, args, local_rank, steps=3, serial_steps=2)
         line["diff"] = leg(run_diff, args, local_rank, steps=10, cpu=False)
@@ -357,6 +358,32 @@ def leg(fn, *a, **k):
         return fn(*a, **k)
     except Exception as e:          # noqa: BLE001
         return {"error": f"{type(e).__name__}: {e}"}
+
+
+def fused_leg(r, wl, args, steps=10):
+    """The same frame with fused plotting (plot warps beside the walkers in
+    one block, samples handed over in shared memory): frame time and the
+    chaos stage's DRAM traffic, which is the histogram's alone."""
+    import torch
+    cfg = json.dumps(wl["cfg"])
+    W, H, ss = wl["width"], wl["height"], wl["supersample"]
+    job = dict(iterations=wl["iterations"], walkers=wl["walkers"], supersample=ss, seed=0x5EED, plot="fused")
+    d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+    side = torch.cuda.Stream()
+    out = r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=side.cuda_stream, sync=True, **job)
+    for _ in range(3):
+        r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=side.cuda_stream, sync=False, **job)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(side)
+    for _ in range(steps):
+        r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=side.cuda_stream, sync=False, **job)
+    ev1.record(side)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    _, _, o = r.histogram(cfg, wl["width"], wl["height"], **job)
+    return {"ms_per_frame": ms, "samples_per_s": out.total_iterations / (ms * 1e-3), "chaos_ms": o.render_time_ms,
+            "splats_per_s": o.inframe_samples / (o.render_time_ms * 1e-3), "traffic": profile_traffic(args.workload + "_fused"),
+            "kernel": "ffb_chaos_fused (448 walker threads + 576 plot threads a block, 8-iteration shared-memory ring)"}
 
 
 def parity_leg(r, wl, size=(480, 270)):
@@ -719,7 +746,7 @@ def main():
         wl = workload(args.workload)
         r = _native.Renderer(local_rank)
         job = dict(iterations=int(args.profile), walkers=wl["walkers"], supersample=wl["supersample"], seed=0x5EED,
-                   schedule=args.schedule, count_bits=wl.get("count_bits", 32), accumulate=args.accumulate)
+                   schedule=args.schedule, count_bits=wl.get("count_bits", 32), accumulate=args.accumulate, plot=args.plot)
         hist = r.histogram_u64 if wl.get("count_bits", 32) == 64 else r.histogram
         for _ in range(args.warmup + args.steps):
             _, _, o = hist(json.dumps(wl["cfg"]), wl["width"], wl["height"], **job)
