@@ -207,13 +207,17 @@ __device__ __forceinline__ u32 ffb_copies(const float* __restrict__ sm) {
 }
 
 // The job owning this block (block-uniform binary search) and its tables
-// staged in shared memory.
+// staged in shared memory -- the launch record too: its fields are read in
+// every iteration, and from global memory each read would wait on the L1
+// (the compiler cannot keep them in registers across the kernels' stores).
+__shared__ ffb_launch ffb_s_job;
 __device__ __forceinline__ const ffb_launch& ffb_stage(const ffb_launch* __restrict__ jobs, int n_jobs, float* sm, float4*& pal) {
     int lo = 0, hi = n_jobs - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
         if (jobs[mid].block0 <= blockIdx.x) lo = mid; else hi = mid - 1;
     }
+    if (threadIdx.x == 0) ffb_s_job = jobs[lo];
     const ffb_launch& J = jobs[lo];
     for (int i = threadIdx.x; i < FFB_TABLE_SIZE; i += blockDim.x) sm[i] = J.table[i];
     pal = reinterpret_cast<float4*>(sm) + FFB_TABLE_VEC4;
@@ -222,7 +226,7 @@ __device__ __forceinline__ const ffb_launch& ffb_stage(const ffb_launch* __restr
     if (threadIdx.x == 0) ffb_s_emit = 0u;
 #endif
     __syncthreads();
-    return J;
+    return ffb_s_job;
 }
 
 // A walker's start (main_template.wgsl:25-55) or its stored state; `prev`
@@ -1013,24 +1017,28 @@ __device__ __forceinline__ void ffb_fused_consumer(const float* __restrict__ sm,
     const float scale = (float)min(J.width, J.height) * 0.25f;
     const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
     u32 inframe = 0;
-    for (u32 j = 0; j < J.n_iters; ++j) {
-        const u32 d = j % D;
-        ffb_mbar_wait(&S.full[d], (j / D) & 1u, S.abort, J);
-        const float4* rr = S.ring + (size_t)d * P;
-        for (u32 i = c; i < P; i += C) {
-            const float4 r = rr[i];
+    // With more consumer threads than records a slot, a pass covers two
+    // slots, so every consumer thread has records to plot.
+    const u32 G = C > P ? 2u : 1u;
+    for (u32 j = 0; j < J.n_iters; j += G) {
+        const u32 g = min(G, J.n_iters - j);
+        for (u32 q = 0; q < g; ++q) ffb_mbar_wait(&S.full[(j + q) % D], ((j + q) / D) & 1u, S.abort, J);
+        for (u32 i = c; i < g * P; i += C) {
+            const u32 d = (j + i / P) % D, e = i % P;
+            const float4 r = S.ring[(size_t)d * P + e];
             const u32 fl = __float_as_uint(r.w);
             if (!(fl & 2u)) continue;
             float fd[FFB_NFD > 0 ? FFB_NFD : 1];
 #pragma unroll
-            for (int m = 0; m < FFB_NFD; ++m) fd[m] = S.ring_draws[(size_t)m * D * P + (size_t)d * P + i];
+            for (int m = 0; m < FFB_NFD; ++m) fd[m] = S.ring_draws[(size_t)m * D * P + (size_t)d * P + e];
             SlotRng rng{fd};
             FfbCtx ctx{nullptr, 0u, 0.0f, 0u, 0u, 0u, 0ull};                     // deferred finals carry no state
             ffb_plot_sample(sm, pal, J, (int)((fl >> 8) & 0xFFu), r.x, r.y, r.z, (fl & 1u) != 0u, rng, ctx, cx, cy, scale,
                             inframe);
         }
         __syncwarp();
-        if (lane == 0) ffb_mbar_arrive(&S.empty[d]);
+        if (lane == 0)
+            for (u32 q = 0; q < g; ++q) ffb_mbar_arrive(&S.empty[(j + q) % D]);
     }
     ffb_count_inframe(J, inframe);
 }

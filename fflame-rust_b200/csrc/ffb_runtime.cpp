@@ -111,6 +111,23 @@ struct DevBuf {
     void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
 };
 
+// Page-locked host memory the readback lands in (a copy from the device to
+// pageable memory goes through the driver's staging buffer at a fraction of
+// the link's rate).
+struct HostBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    void* ensure(size_t bytes) {
+        if (bytes <= n && p) return p;
+        if (p) cudaFreeHost(p);
+        p = nullptr; n = 0;
+        ck(cudaMallocHost(&p, std::max<size_t>(bytes, 256)), "cudaMallocHost");
+        n = std::max<size_t>(bytes, 256);
+        return p;
+    }
+    void release() { if (p) cudaFreeHost(p); p = nullptr; n = 0; }
+};
+
 struct Module {
     std::string key;
     cudaLibrary_t lib = nullptr;
@@ -155,6 +172,7 @@ struct ffb_renderer {
     DevBuf tile_rec, tile_tmp, tile_sorted, tile_meta;      // tile-sorted accumulation scratch
     DevBuf filt_batch, filt_tmp;                            // spatial filter: a batch's histogram, the row pass
     DevBuf vstate;                                          // stateful variations / subflames: per-walker state
+    HostBuf readback;                                       // fae_call's RGBA8 on its way to the caller
     // Deferred plotting: the plot kernel's stream, double-buffered sample
     // records, events ordering the two streams.
     cudaStream_t plot_stream = nullptr;
@@ -194,6 +212,7 @@ struct ffb_renderer {
         for (DevBuf* b : {&hist, &walkers, &table, &palette, &counters, &jobs, &rgba, &de_out, &de_tab, &lut, &f_out, &tmp_in,
                           &tile_rec, &tile_tmp, &tile_sorted, &tile_meta, &filt_batch, &filt_tmp, &vstate, &rec[0], &rec[1],
                           &rec_draws[0], &rec_draws[1]}) b->release();
+        readback.release();
         if (plot_stream) {
             cudaStreamSynchronize(plot_stream);
             for (int i = 0; i < 2; ++i) { cudaEventDestroy(ev_main[i]); cudaEventDestroy(ev_plot[i]); }
@@ -917,14 +936,16 @@ void fae_dispatch(const Json& r, const uint8_t* data, size_t data_len, std::vect
         ffb_renderer* R = fae_renderer();
         std::lock_guard<std::mutex> lk(R->mu);
         R->begin();
-        out.resize((size_t)job.width * job.height * 4);
-        void* d = R->rgba.ensure(out.size());
+        const size_t n_out = (size_t)job.width * job.height * 4;
+        void* d = R->rgba.ensure(n_out);
         ffb_output o{};
         R->reset_counts();
         render_device(R, c->str.data(), c->str.size(), &job, d, R->stream, true, &o);
-        ck(cudaMemcpyAsync(out.data(), d, out.size(), cudaMemcpyDeviceToHost, R->stream), "readback");
-        R->d2h += out.size();
+        uint8_t* staged = (uint8_t*)R->readback.ensure(n_out);
+        ck(cudaMemcpyAsync(staged, d, n_out, cudaMemcpyDeviceToHost, R->stream), "readback");
+        R->d2h += n_out;
         ck(cudaStreamSynchronize(R->stream), "readback");
+        out.assign(staged, staged + n_out);
         JsonWriter w;
         w.begin().num("width", job.width).num("height", job.height).num("iterations", (double)o.total_iterations)
             .num("ms", o.render_time_ms).num("iterations_per_thread", job.iterations_per_thread).end();
@@ -1479,6 +1500,7 @@ struct ffb_batch {
     std::vector<BatchGroup> groups;
     DevBuf hist, walk, rgba, tables, palettes, counters, launches, tjobs, luts, de, detab;
     uint32_t threads = 256, iters = 1024;
+    bool plain = false;          // one walker a thread (ffb_chaos) instead of the transform-sorted kernel
     uint64_t total_samples = 0;
     std::vector<BatchDe> de_tabs;
     cudaGraph_t graph = nullptr;
@@ -1552,15 +1574,18 @@ void batch_enqueue(ffb_batch* B, uint32_t threads, uint32_t iters, uint64_t scal
         BatchGroup& G = B->groups[g];
         uint32_t blocks = 0;
         for (uint32_t j : G.members) blocks += B->flames[j].walkers / threads;
-        const int smem = ((G.table_size + 3) / 4) * 16 + G.max_pal * 16 + (int)threads * 8 * 4 + 2 * (G.maxx + 1) * 4;
-        if (smem > 48 * 1024 && G.mod->smem_attr_sorted < smem) {
-            ck(cudaFuncSetAttribute((const void*)G.mod->chaos_sorted, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
-            G.mod->smem_attr_sorted = smem;
+        int smem = ((G.table_size + 3) / 4) * 16 + G.max_pal * 16;
+        if (!B->plain) smem += (int)threads * 8 * 4 + 2 * (G.maxx + 1) * 4;
+        const void* kfn = B->plain ? (const void*)G.mod->chaos : (const void*)G.mod->chaos_sorted;
+        int& attr = B->plain ? G.mod->smem_attr : G.mod->smem_attr_sorted;
+        if (smem > 48 * 1024 && attr < smem) {
+            ck(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attribute");
+            attr = smem;
         }
         Launch* jp = d_l + first[g];
         int nj = (int)G.members.size();
         void* args[] = {&jp, &nj};
-        ck(cudaLaunchKernel((const void*)G.mod->chaos_sorted, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch batch");
+        ck(cudaLaunchKernel(kfn, dim3(blocks), dim3(threads), args, (size_t)smem, s), "launch batch");
         r->launches += 1;
     }
     if (!tonemap) return;
@@ -1692,16 +1717,29 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
         ck(cudaMemcpyAsync(B->tables.ensure(tabs.size() * 4), tabs.data(), tabs.size() * 4, cudaMemcpyHostToDevice, s), "upload tables");
         ck(cudaMemcpyAsync(B->palettes.ensure(pals.size() * 4), pals.data(), pals.size() * 4, cudaMemcpyHostToDevice, s), "upload palettes");
         ck(cudaMemcpyAsync(B->luts.ensure(luts.size() * 4), luts.data(), luts.size() * 4, cudaMemcpyHostToDevice, s), "upload curves");
-        // Autotune: time each (threads, iterations a walker) on 1/64 of
-        // every budget; keep the fastest per sample.
+        // Autotune: time each (schedule, threads, iterations a walker) on
+        // 1/64 of every budget; keep the fastest per sample.  The
+        // transform-sorted kernel regroups walkers so a warp runs one
+        // transform's variations; where every transform carries the same
+        // variations (the sort removes no divergence) one walker a thread
+        // saves the regrouping.  The one-walker kernel's blocks are the
+        // modules' 128 threads (its launch bounds).
         B->threads = common->threads ? (uint32_t)common->threads : 256;
         B->iters = common->iterations_per_thread ? common->iterations_per_thread : 1024;
+        B->plain = common->schedule == 1;
+        if (B->plain) B->threads = 128;
         if (tune) {
             double best = 1e30;
-            const uint32_t cand_t[] = {128, 256, 512};
+            bool best_plain = B->plain;
+            struct Cand { bool plain; uint32_t t; };
+            std::vector<Cand> cands;
+            if (common->schedule != 1) for (uint32_t t : {128u, 256u, 512u}) cands.push_back({false, t});
+            if (common->schedule != 2) cands.push_back({true, 128u});
             const uint32_t cand_i[] = {256, 1024, 4096};
-            for (uint32_t t : cand_t)
+            for (const Cand& c : cands)
                 for (uint32_t it : cand_i) {
+                    const uint32_t t = c.t;
+                    B->plain = c.plain;
                     batch_enqueue(B.get(), t, it, 64, s, false);             // warm (allocations)
                     ck(cudaEventRecord(r->ev0, s), "event");
                     batch_enqueue(B.get(), t, it, 64, s, false);
@@ -1712,8 +1750,9 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
                     uint64_t samples = 0;
                     for (auto& F : B->flames) samples += (uint64_t)F.walkers * F.per_walker;
                     const double per = ms / (double)samples;
-                    if (per < best) { best = per; B->threads = t; B->iters = it; }
+                    if (per < best) { best = per; B->threads = t; B->iters = it; best_plain = c.plain; }
                 }
+            B->plain = best_plain;
         }
         // Size the buffers for the real run, then capture it as a graph.
         batch_enqueue(B.get(), B->threads, B->iters, 1, s, true);

@@ -291,7 +291,8 @@ __global__ void __launch_bounds__(256) k_tonemap_batch(const TonemapJob* __restr
 //
 // Sources split by reach.  A *narrow* source (disc radius <= DE_NARROW:
 // counts above a few, the bulk of a lit frame) is gathered from the dense
-// (2 DE_NARROW + 1)^2 window; a *wide* one (a low count, reaching up to R)
+// window of the widest narrow source's reach (at most (2 DE_NARROW + 1)^2,
+// a few pixels where every count is high); a *wide* one (reaching up to R)
 // goes to a per-block list of its window position, which every output of
 // the block walks.  A tile whose window holds one count-1 source so no
 // longer pays the full (2R+1)^2 loop for every pixel.  When the list is
@@ -311,16 +312,17 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
     float2* par = reinterpret_cast<float2*>(de_smem + n);                 // (accepted d^2, 4.5 / h^2); wide: -(d^2 + 1)
     unsigned short* wide = reinterpret_cast<unsigned short*>(par + n);    // wide sources: x | y << 8 in the window
     const int cap = min(n, DE_WIDE_CAP);
-    __shared__ int reach, n_wide;
-    if (threadIdx.x == 0) { reach = 0; n_wide = 0; }
+    __shared__ int reach, reach_n, n_wide;
+    if (threadIdx.x == 0) { reach = 0; reach_n = 0; n_wide = 0; }
     __syncthreads();
     const int x0 = blockIdx.x * DE_TX - R, y0 = y_lo + blockIdx.y * DE_TY - R;
-    int my_reach = 0;
+    int my_reach = 0, my_reach_n = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int lx = i % tw, ly = i / tw;
         const int sx = x0 + lx, sy = y0 + ly;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         float2 pr = make_float2(-1.0f, 0.0f);                              // empty: never accepted
+        bool is_wide = false;
         if (sx >= 0 && sy >= 0 && sx < w && sy < h) {
             const size_t si = (size_t)sy * w + sx;
             float4 hv;
@@ -343,21 +345,34 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
                 pr = make_float2(e.x, 4.5f * e.y);
                 my_reach = max(my_reach, (int)e.w);
                 if ((int)e.w > DE_NARROW) {
-                    const int k = atomicAdd(&n_wide, 1);
-                    if (k < cap) wide[k] = (unsigned short)(lx | (ly << 8));
+                    is_wide = true;
                     pr.x = -(e.x + 1.0f);
+                } else {
+                    my_reach_n = max(my_reach_n, (int)e.w);
                 }
             }
         }
         val[i] = v;
         par[i] = pr;
+        // Append the warp's wide sources to the list with one atomic.
+        const unsigned live = __activemask();
+        const unsigned m = __ballot_sync(live, is_wide);
+        if (m) {
+            const int lane = (int)(threadIdx.x & 31u), leader = __ffs(live) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&n_wide, __popc(m));
+            base = __shfl_sync(live, base, leader);
+            const int k = base + __popc(m & ((1u << lane) - 1u));
+            if (is_wide && k < cap) wide[k] = (unsigned short)(lx | (ly << 8));
+        }
     }
     atomicMax(&reach, my_reach);
+    atomicMax(&reach_n, my_reach_n);
     __syncthreads();
     const int rb = min(R, reach);
     const int nw = n_wide;
     const int dense = (2 * rb + 1) * (2 * rb + 1);
-    const int rn = min(rb, DE_NARROW);
+    const int rn = min(rb, reach_n);                                     // the narrow sources' own reach
     // Whole-window gather when the list would cost more than the loop it saves.
     const bool plain = nw > cap || nw >= dense - (2 * rn + 1) * (2 * rn + 1);
     const int rl = plain ? rb : rn;

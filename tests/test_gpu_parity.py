@@ -383,13 +383,15 @@ def test_exact_u64_counts_carry_past_2_32(renderer):
     np.testing.assert_allclose(mean, entry, rtol=2e-6)
 
 
-def test_batch_matches_single_renders(renderer):
+@pytest.mark.parametrize("schedule", ["sorted", "plain"])
+def test_batch_matches_single_renders(renderer, schedule):
     """A batch of flames of different transform counts and sizes, one
     launch, graph-replayed: each flame's picture is the single render of the
-    same walkers and budget (the streams are keyed by walker and seed)."""
+    same walkers and budget (the streams are keyed by walker and seed), with
+    either kernel schedule."""
     from ffb200 import Batch
     items = synthetic.batch_flames(n=12, seed=5, spp=(20, 60), sizes=(64, 96, 128))
-    b = Batch(renderer, items, tune=False, threads=128, iterations_per_thread=256)
+    b = Batch(renderer, items, tune=False, threads=128, iterations_per_thread=256, schedule=schedule)
     info = b.info()
     assert info["groups"] == 1 and info["threads"] == 128
     ms = b.run()
@@ -399,7 +401,7 @@ def test_batch_matches_single_renders(renderer):
         img, plotted = b.output(k)
         walkers, per = Batch.walkers_for(samples, 128, 256)
         assert plotted == walkers * per >= samples
-        ref, o = renderer.render(cfg, w, h, iterations=walkers * per, walkers=walkers, seed=seed, schedule="sorted",
+        ref, o = renderer.render(cfg, w, h, iterations=walkers * per, walkers=walkers, seed=seed, schedule=schedule,
                                  threads=128)
         assert o.total_iterations == plotted
         d = np.abs(img.astype(int) - ref.astype(int))
