@@ -1015,9 +1015,10 @@ __device__ __forceinline__ void ffb_fused_consumer(const float* __restrict__ sm,
     const float scale = (float)min(J.width, J.height) * 0.25f;
     const float cx = (float)J.width * 0.5f, cy = (float)J.height * 0.5f;
     u32 inframe = 0;
-    // With more consumer threads than records a slot, a pass covers two
-    // slots, so every consumer thread has records to plot.
-    const u32 G = C > P ? 2u : 1u;
+    // A pass covers one slot (a pass over two slots, giving every thread of
+    // 576 work against 448 records, measured 7 % slower: 61.1 ms a frame
+    // against 57.1).
+    const u32 G = 1u;
     for (u32 j = 0; j < J.n_iters; j += G) {
         const u32 g = min(G, J.n_iters - j);
         for (u32 q = 0; q < g; ++q) ffb_mbar_wait(&S.full[(j + q) % D], ((j + q) / D) & 1u, S.abort, J);

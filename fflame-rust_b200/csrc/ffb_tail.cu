@@ -287,21 +287,10 @@ __global__ void __launch_bounds__(256) k_tonemap_batch(const TonemapJob* __restr
 // stages its 32x16 tile's source window in shared memory once, with every
 // source's table entry resolved (its accepted d^2, 4.5/h^2, and its values
 // premultiplied by the normaliser), so a neighbour outside its disc costs
-// one 8-byte shared load and a compare.
-//
-// Sources split by reach.  A *narrow* source (disc radius <= DE_NARROW:
-// counts above a few, the bulk of a lit frame) is gathered from the dense
-// window of the widest narrow source's reach (at most (2 DE_NARROW + 1)^2,
-// a few pixels where every count is high); a *wide* one (reaching up to R)
-// goes to a per-block list of its window position, which every output of
-// the block walks.  A tile whose window holds one count-1 source so no
-// longer pays the full (2R+1)^2 loop for every pixel.  When the list is
-// longer than the window loop it replaces (or overflows its capacity), the
-// block gathers the whole window as a plain loop instead.  Wide sources are
-// marked in the staged parameters by a negative accepted d^2, -(d^2 + 1).
+// one 8-byte shared load and a compare; and the window shrinks to the
+// largest radius any staged source actually has (dense regions, where
+// every count is high, gather over a few pixels only).
 constexpr int DE_TX = 32, DE_TY = 16;
-constexpr int DE_NARROW = 4;
-constexpr int DE_WIDE_CAP = 2048;
 __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restrict__ hist, const ulonglong4* __restrict__ exact,
                                                            int w, int h, const float4* __restrict__ tab,
                                                            int tab_n, int R, int y_lo, int h_out, float4* __restrict__ out,
@@ -309,20 +298,16 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
     extern __shared__ float4 de_smem[];
     const int tw = DE_TX + 2 * R, th = DE_TY + 2 * R, n = tw * th;
     float4* val = de_smem;                                                // (rgb, count) / normaliser
-    float2* par = reinterpret_cast<float2*>(de_smem + n);                 // (accepted d^2, 4.5 / h^2); wide: -(d^2 + 1)
-    unsigned short* wide = reinterpret_cast<unsigned short*>(par + n);    // wide sources: x | y << 8 in the window
-    const int cap = min(n, DE_WIDE_CAP);
-    __shared__ int reach, reach_n, n_wide;
-    if (threadIdx.x == 0) { reach = 0; reach_n = 0; n_wide = 0; }
+    float2* par = reinterpret_cast<float2*>(de_smem + n);                 // (accepted d^2, 4.5 / h^2)
+    __shared__ int reach;
+    if (threadIdx.x == 0) reach = 0;
     __syncthreads();
     const int x0 = blockIdx.x * DE_TX - R, y0 = y_lo + blockIdx.y * DE_TY - R;
-    int my_reach = 0, my_reach_n = 0;
+    int my_reach = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int lx = i % tw, ly = i / tw;
-        const int sx = x0 + lx, sy = y0 + ly;
+        const int sx = x0 + i % tw, sy = y0 + i / tw;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         float2 pr = make_float2(-1.0f, 0.0f);                              // empty: never accepted
-        bool is_wide = false;
         if (sx >= 0 && sy >= 0 && sx < w && sy < h) {
             const size_t si = (size_t)sy * w + sx;
             float4 hv;
@@ -344,65 +329,26 @@ __global__ void __launch_bounds__(DE_TX * DE_TY) k_density(const float4* __restr
                 v = make_float4(hv.x * e.z, hv.y * e.z, hv.z * e.z, cf * e.z);
                 pr = make_float2(e.x, 4.5f * e.y);
                 my_reach = max(my_reach, (int)e.w);
-                if ((int)e.w > DE_NARROW) {
-                    is_wide = true;
-                    pr.x = -(e.x + 1.0f);
-                } else {
-                    my_reach_n = max(my_reach_n, (int)e.w);
-                }
             }
         }
         val[i] = v;
         par[i] = pr;
-        // Append the warp's wide sources to the list with one atomic.
-        const unsigned live = __activemask();
-        const unsigned m = __ballot_sync(live, is_wide);
-        if (m) {
-            const int lane = (int)(threadIdx.x & 31u), leader = __ffs(live) - 1;
-            int base = 0;
-            if (lane == leader) base = atomicAdd(&n_wide, __popc(m));
-            base = __shfl_sync(live, base, leader);
-            const int k = base + __popc(m & ((1u << lane) - 1u));
-            if (is_wide && k < cap) wide[k] = (unsigned short)(lx | (ly << 8));
-        }
     }
     atomicMax(&reach, my_reach);
-    atomicMax(&reach_n, my_reach_n);
     __syncthreads();
     const int rb = min(R, reach);
-    const int nw = n_wide;
-    const int dense = (2 * rb + 1) * (2 * rb + 1);
-    const int rn = min(rb, reach_n);                                     // the narrow sources' own reach
-    // Whole-window gather when the list would cost more than the loop it saves.
-    const bool plain = nw > cap || nw >= dense - (2 * rn + 1) * (2 * rn + 1);
-    const int rl = plain ? rb : rn;
     const int lx = threadIdx.x % DE_TX, ly = threadIdx.x / DE_TX;
     const int px = blockIdx.x * DE_TX + lx, py = y_lo + blockIdx.y * DE_TY + ly;
     if (px >= w || py >= h || py >= y_lo + h_out) return;
     float ar = 0.f, ag = 0.f, ab = 0.f, ac = 0.f;
-    for (int dy = -rl; dy <= rl; ++dy) {
+    for (int dy = -rb; dy <= rb; ++dy) {
         const int row = (ly + R + dy) * tw + (lx + R);
-        for (int dx = -rl; dx <= rl; ++dx) {
+        for (int dx = -rb; dx <= rb; ++dx) {
             const float2 pp = par[row + dx];
-            const float acc = pp.x >= 0.0f ? pp.x : (plain ? -pp.x - 1.0f : -1.0f);
             const float d2 = (float)(dx * dx + dy * dy);
-            if (d2 > acc) continue;
+            if (d2 > pp.x) continue;
             const float wt = __expf(-pp.y * d2);
             const float4 v = val[row + dx];
-            ar += wt * v.x; ag += wt * v.y; ab += wt * v.z; ac += wt * v.w;
-        }
-    }
-    if (!plain) {
-        for (int e = 0; e < nw; ++e) {
-            const int q = wide[e];
-            const int qx = q & 0xFF, qy = q >> 8;
-            const int dx = qx - (lx + R), dy = qy - (ly + R);
-            const int i = qy * tw + qx;
-            const float2 pp = par[i];
-            const float d2 = (float)(dx * dx + dy * dy);
-            if (d2 > -pp.x - 1.0f) continue;
-            const float wt = __expf(-pp.y * d2);
-            const float4 v = val[i];
             ar += wt * v.x; ag += wt * v.y; ab += wt * v.z; ac += wt * v.w;
         }
     }
@@ -467,8 +413,7 @@ cudaError_t launch_tonemap_batch(const TonemapJob* jobs, int n_jobs, long long t
 cudaError_t launch_density_estimate(const float4* hist, const ulonglong4* exact, int w, int h,
                                     const float4* table, int table_n, int radius, int y_lo, int h_out, float4* out, cudaStream_t s,
                                     int count_f) {
-    const size_t nwin = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius);
-    const size_t smem = nwin * (sizeof(float4) + sizeof(float2)) + std::min<size_t>(nwin, DE_WIDE_CAP) * sizeof(unsigned short);
+    const size_t smem = (size_t)(DE_TX + 2 * radius) * (DE_TY + 2 * radius) * (sizeof(float4) + sizeof(float2));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
