@@ -290,16 +290,20 @@ void emit_phases(std::ostringstream& s, const std::vector<const VarDef*>& vars,
     auto open = [&](const Site& c) {
         s << ind << "{ const float w = " << c.w << "; " << (gate ? "if (w != 0.0f) { " : "{ ");
     };
-    for (int pass = 0; pass < 3; ++pass) {
+    // Passes: Pre, the accumulating normal variations, the Replace ones
+    // (shader_builder_v2.rs:2511-2520, 2700-2709: after the others, each
+    // assigning `result = w * V(p)` over the sum so far), Post.
+    for (int pass = 0; pass < 4; ++pass) {
         for (size_t j = 0; j < vars.size(); ++j) {
             const VarDef* v = vars[j];
-            const int ph = (v->flags & VF_PRE) ? 0 : (v->flags & VF_POST) ? 2 : 1;
+            const int ph = (v->flags & VF_PRE) ? 0 : (v->flags & VF_POST) ? 3 : (v->flags & VF_REPLACE) ? 2 : 1;
             if (ph != pass) continue;
             const Site c = site((int)j);
             open(c);
-            const std::string body = (v->flags & VF_SUB) ? call_sub(v, c, vc) : call(v, c, ph == 2 ? "rx" : "tx", ph == 2 ? "ry" : "ty") + ";";
+            const std::string body = (v->flags & VF_SUB) ? call_sub(v, c, vc) : call(v, c, ph == 3 ? "rx" : "tx", ph == 3 ? "ry" : "ty") + ";";
             if (ph == 0) s << body << " tx = ox; ty = oy;";
             else if (ph == 1) s << body << " rx = rx + w * ox; ry = ry + w * oy;";
+            else if (ph == 2) s << body << " rx = w * ox; ry = w * oy;";
             else s << body << " rx = ox; ry = oy;";
             s << " } }   // " << v->name << "\n";
         }

@@ -225,6 +225,9 @@ static const VarDef kRegistry[] = {
     {"ngon", 50, 0, 4, {"sides", "power", "circle", "corners"}, {5.0f, 3.0f, 1.0f, 2.0f}, "v_ngon", 0, 0, nullptr},
     {"auger", 51, 0, 4, {"freq", "weight", "scale", "sym"}, {1.0f, 0.5f, 0.5f, 0.0f}, "v_auger", 0, 0, nullptr},
     {"pre_blur", 54, 7, 0, NP, ND, "v_pre_blur", VF_PRE | VF_W, 0, nullptr},
+    {"pre_spherical", 57, 0, 0, NP, ND, "v_pre_spherical", VF_PRE, 0, nullptr},
+    {"pre_sinusoidal", 58, 0, 0, NP, ND, "v_pre_sinusoidal", VF_PRE | VF_W, 0, nullptr},
+    {"pre_disc", 59, 0, 0, NP, ND, "v_pre_disc", VF_PRE | VF_W, 0, nullptr},
     {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
     {"epispiral", 67, 1, 3, {"n", "thickness", "holes"}, {6.0f, 0.0f, 1.0f}, "v_epispiral", 0, 0, nullptr},
     {"juliascope", 69, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_juliascope", 0, 0, nullptr},
@@ -235,6 +238,9 @@ static const VarDef kRegistry[] = {
     {"separation", 77, 0, 4, {"x", "y", "xinside", "yinside"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_separation", 0, 0, nullptr},
     {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
     {"cpow", 85, 1, 3, {"r", "i", "power"}, {1.0f, 0.1f, 1.5f}, "v_cpow", 0, 3, derive_cpow},
+    {"acoth", 86, 0, 0, NP, ND, "v_acoth", 0, 0, nullptr},
+    {"arcsinh", 91, 0, 0, NP, ND, "v_arcsinh", 0, 0, nullptr},
+    {"arctanh", 92, 0, 0, NP, ND, "v_arctanh", 0, 0, nullptr},
     {"sin", 93, 0, 0, NP, ND, "v_sin", 0, 0, nullptr},
     {"cos", 94, 0, 0, NP, ND, "v_cos", 0, 0, nullptr},
     {"tan", 95, 0, 0, NP, ND, "v_tan", 0, 0, nullptr},
@@ -249,8 +255,16 @@ static const VarDef kRegistry[] = {
     {"csch", 104, 0, 0, NP, ND, "v_csch", 0, 0, nullptr},
     {"sin2_bs", 123, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sin2_bs", 0, 0, nullptr},
     {"cos2_bs", 124, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cos2_bs", 0, 0, nullptr},
+    {"tan2_bs", 125, 0, 4, {"x1", "x2", "y1", "y2"}, {2.0f, 2.0f, 2.0f, 2.0f}, "v_tan2_bs", 0, 0, nullptr},
+    {"sec2_bs", 126, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sec2_bs", 0, 0, nullptr},
+    {"csc2_bs", 127, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_csc2_bs", 0, 0, nullptr},
+    {"cot2_bs", 128, 0, 4, {"x1", "x2", "y1", "y2"}, {2.0f, 2.0f, 2.0f, 2.0f}, "v_cot2_bs", 0, 0, nullptr},
     {"sinh2_bs", 129, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sinh2_bs", 0, 0, nullptr},
     {"cosh2_bs", 130, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cosh2_bs", 0, 0, nullptr},
+    {"tanh2_bs", 131, 0, 4, {"x1", "x2", "y1", "y2"}, {2.0f, 2.0f, 2.0f, 2.0f}, "v_tanh2_bs", 0, 0, nullptr},
+    {"coth2_bs", 132, 0, 4, {"x1", "x2", "y1", "y2"}, {2.0f, 2.0f, 2.0f, 2.0f}, "v_coth2_bs", 0, 0, nullptr},
+    {"sech2_bs", 133, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sech2_bs", 0, 0, nullptr},
+    {"csch2_bs", 134, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_csch2_bs", 0, 0, nullptr},
     {"exp2_bs", 135, 0, 3, {"x1", "y1", "y2"}, {1.0f, 1.0f, 1.0f}, "v_exp2_bs", 0, 0, nullptr},
     {"exp", 136, 0, 0, NP, ND, "v_exp", 0, 0, nullptr},
     {"tancos", 140, 0, 0, NP, ND, "v_tancos", 0, 0, nullptr},
@@ -262,6 +276,9 @@ static const VarDef kRegistry[] = {
     {"parabola", 149, 2, 2, {"width", "height"}, {1.0f, 0.5f}, "v_parabola", 0, 0, nullptr},
     {"pie", 150, 3, 3, {"slices", "rotation", "thickness"}, {6.0f, 0.0f, 0.5f}, "v_pie", 0, 0, nullptr},
     {"butterfly", 152, 0, 0, NP, ND, "v_butterfly", 0, 0, nullptr},
+    {"ennepers", 154, 0, 0, NP, ND, "v_ennepers", VF_REPLACE, 0, nullptr},
+    {"rays2", 156, 0, 0, NP, ND, "v_rays2", VF_REPLACE, 0, nullptr},
+    {"rays3", 157, 0, 0, NP, ND, "v_rays3", VF_REPLACE, 0, nullptr},
     {"spiralwing", 158, 0, 0, NP, ND, "v_spiralwing", 0, 0, nullptr},
     {"cell", 161, 0, 1, {"size"}, {0.6f}, "v_cell", 0, 0, nullptr},
     {"flower", 163, 1, 2, {"holes", "petals"}, {0.4f, 7.0f}, "v_flower", 0, 0, nullptr},
@@ -286,12 +303,14 @@ static const VarDef kRegistry[] = {
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
     {"pulse", 244, 0, 4, {"freqx", "freqy", "scalex", "scaley"}, {2.0f, 2.0f, 1.0f, 1.0f}, "v_pulse", 0, 0, nullptr},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
+    {"squirrel", 249, 0, 2, {"a", "b"}, {1.0f, 1.0f}, "v_squirrel", VF_REPLACE, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
     {"mcarpet", 282, 0, 4, {"x", "y", "twist", "tilt"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_mcarpet", 0, 0, nullptr},
     {"oscilloscope", 284, 0, 4, {"separation", "frequency", "amplitude", "damping"}, {1.0f, 3.14159265f, 1.0f, 0.0f}, "v_oscilloscope", 0, 1, derive_oscilloscope},
     {"linearT", 287, 0, 2, {"powX", "powY"}, {1.2f, 1.2f}, "v_linearT", 0, 0, nullptr},
+    {"anamorphcyl", 296, 0, 3, {"a", "b", "k"}, {1.0f, 1.3f, 3.0f}, "v_anamorphcyl", VF_REPLACE, 0, nullptr},
     {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
@@ -304,7 +323,9 @@ static const VarDef kRegistry[] = {
     {"idisc", 323, 0, 0, NP, ND, "v_idisc", VF_W, 0, nullptr},
     {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
+    {"roundspher", 326, 0, 0, NP, ND, "v_roundspher", VF_W, 0, nullptr},
     {"d_spherical", 334, 1, 1, {"d_spher_weight"}, {0.5f}, "v_d_spherical", 0, 0, nullptr},
+    {"deltaA", 336, 0, 0, NP, ND, "v_deltaA", VF_W, 0, nullptr},
     {"edisc", 337, 0, 0, NP, ND, "v_edisc", VF_W, 0, nullptr},
     {"curve", 338, 0, 4, {"xamp", "yamp", "xlength", "ylength"}, {0.25f, 0.5f, 1.0f, 1.0f}, "v_curve", 0, 2, derive_curve},
     {"exp2", 340, 0, 0, NP, ND, "v_exp2", 0, 0, nullptr},
@@ -312,12 +333,17 @@ static const VarDef kRegistry[] = {
     {"flipy", 342, 0, 0, NP, ND, "v_flipy", 0, 0, nullptr},
     {"invpolar", 344, 0, 0, NP, ND, "v_invpolar", 0, 0, nullptr},
     {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
+    {"sintrange", 354, 0, 1, {"w"}, {1.0f}, "v_sintrange", VF_REPLACE, 0, nullptr},
+    {"hyperbolicellipse", 362, 0, 1, {"a"}, {1.0f}, "v_hyperbolicellipse", VF_REPLACE, 0, nullptr},
     {"layered_spiral", 363, 0, 1, {"radius"}, {1.0f}, "v_layered_spiral", 0, 0, nullptr},
     {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
     {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
     {"rippled", 380, 0, 0, NP, ND, "v_rippled", 0, 0, nullptr},
+    {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
     {"clifford_js", 435, 0, 4, {"a", "b", "c", "d"}, {-1.4f, 1.6f, 1.0f, 0.7f}, "v_clifford_js", 0, 0, nullptr},
+    {"svensson_js", 436, 0, 4, {"a", "b", "c", "d"}, {1.4f, 1.56f, 1.4f, -6.56f}, "v_svensson_js", VF_REPLACE, 0, nullptr},
+    {"epispiral_wf", 446, 0, 1, {"waves"}, {4.0f}, "v_epispiral_wf", 0, 0, nullptr},
     {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},
      "v_klein_group", VF_W, 16, derive_klein_group, 1, 1},
     {"subflame_wf", 502, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},

@@ -32,6 +32,7 @@ enum VarFlags {
     VF_JAC = 16,      // has a Jacobian (dj_*) for the differentiable render
     VF_DC = 32,       // Feature::WritesColor: may write the iteration's colour register (vc)
     VF_SUB = 64,      // steps a subflame (subflame_wf, pre_subflame_wf): generated, not a plain body
+    VF_REPLACE = 128, // Feature::Replace: its w * V(p) overwrites the normal phase's sum, after the others
 };
 
 struct VarDef {

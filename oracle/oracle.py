@@ -48,6 +48,11 @@ REGISTRY = {
     "sin2_bs": 123, "cos2_bs": 124, "sinh2_bs": 129, "cosh2_bs": 130, "exp2_bs": 135, "pulse": 244, "linearT": 287,
     "layered_spiral": 363,
     "circlesplit": 199, "loonie3": 217, "mcarpet": 282, "d_spherical": 334, "clifford_js": 435,
+    "pre_spherical": 57, "pre_sinusoidal": 58, "pre_disc": 59, "acoth": 86, "arcsinh": 91, "arctanh": 92,
+    "tan2_bs": 125, "sec2_bs": 126, "csc2_bs": 127, "cot2_bs": 128, "tanh2_bs": 131, "coth2_bs": 132, "sech2_bs": 133,
+    "csch2_bs": 134, "ennepers": 154, "rays2": 156, "rays3": 157, "squirrel": 249, "anamorphcyl": 296, "roundspher": 326,
+    "deltaA": 336, "sintrange": 354, "hyperbolicellipse": 362, "post_spherical": 388, "svensson_js": 436,
+    "epispiral_wf": 446,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -115,6 +120,14 @@ PARAMS.update({
     "mcarpet": [("x", 1.0), ("y", 1.0), ("twist", 0.0), ("tilt", 0.0)],
     "d_spherical": [("d_spher_weight", 0.5)],
     "clifford_js": [("a", -1.4), ("b", 1.6), ("c", 1.0), ("d", 0.7)],
+    **{n: [("x1", 2.0), ("x2", 2.0), ("y1", 2.0), ("y2", 2.0)] for n in ("tan2_bs", "cot2_bs", "tanh2_bs", "coth2_bs")},
+    **{n: [("x1", 1.0), ("x2", 1.0), ("y1", 1.0), ("y2", 1.0)] for n in ("sec2_bs", "csc2_bs", "sech2_bs", "csch2_bs")},
+    "epispiral_wf": [("waves", 4.0)],
+    "hyperbolicellipse": [("a", 1.0)],
+    "sintrange": [("w", 1.0)],
+    "squirrel": [("a", 1.0), ("b", 1.0)],
+    "anamorphcyl": [("a", 1.0), ("b", 1.3), ("k", 3.0)],
+    "svensson_js": [("a", 1.4), ("b", 1.56), ("c", 1.4), ("d", -6.56)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)
@@ -124,7 +137,7 @@ XF_STRIDE = 18
 
 
 def var_meta(name):
-    """(draws, user parameters, derived values, phase 0 pre / 1 normal / 2 post)."""
+    """(draws, user parameters, derived values, phase 0 pre / 1 normal / 2 post / 3 normal with Feature::Replace)."""
     out = (ctypes.c_int * 4)()
     lib().of_var_meta(ctypes.c_int(REGISTRY[name]), out)
     return tuple(out)

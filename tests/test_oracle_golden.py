@@ -124,6 +124,29 @@ WIDER = {
     "circlesplit": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
     "mcarpet": dict.fromkeys(HUGE_ARGS, "shared-square"),
     "clifford_js": dict.fromkeys(HUGE_ARGS, "huge"),
+    "anamorphcyl": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "tan2_bs": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), "lopsided": "huge"},
+    "tanh2_bs": dict.fromkeys(["tiny", "normal_min"], "zero"),
+    "cot2_bs": {"pi_e": "zero", **dict.fromkeys(["tiny", "normal_min"], "tiny-quotient"), "lopsided": "huge"},
+    "coth2_bs": dict.fromkeys(["tiny", "normal_min"], "tiny-quotient"),
+    "csc2_bs": {"pi_e": "zero", **dict.fromkeys(["tiny", "normal_min"], "tiny-quotient"), "lopsided": "huge"},
+    "csch2_bs": dict.fromkeys(["tiny", "normal_min"], "tiny-quotient"),
+    "sec2_bs": {"pi_e": "zero", "lopsided": "huge"},
+    "deltaA": dict.fromkeys(["+0+0", "+0-0", "-0+0", "-0-0", "-x", "tiny", "normal_min", "subnormal"], "zero"),
+    "epispiral_wf": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "lopsided", "y_neg0x"], "zero"),
+    "hyperbolicellipse": {**dict.fromkeys(["-0+0", "-0-0", "neg0y_x"], "signed-zero"),
+                          **dict.fromkeys(["tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    # A Pre variation feeds the probe's linear carrier; the reference's
+    # compiler folded that carrier's 0 + 1 * p to p, keeping its -0.
+    "pre_disc": {**dict.fromkeys(["-0+0", "-0-0", "+y", "neg0y_x"], "signed-zero"),
+                 **dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero")},
+    "pre_sinusoidal": {**dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
+                       **dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "pre_spherical": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "large", "near_threshold", "past_threshold",
+                                    "y_neg0x", "neg0y_x"], "signed-zero"),
+    "sintrange": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), "lopsided": "inf*0"},
+    "squirrel": dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"),
+    "svensson_js": {**dict.fromkeys(["tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -136,7 +159,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "super_shape", "conic", "cpow", "boarders", "oscilloscope", "blur_circle", "blur_zoom",
                        "blur_pixelize", "tancos", "spiralwing", "panorama1", "panorama2", "circleblur", "henon",
                        "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy", "rippled", "loonie3",
-                       "d_spherical"])
+                       "d_spherical", "acoth", "arcsinh", "arctanh", "ennepers", "post_spherical", "rays2", "rays3",
+                       "roundspher", "sech2_bs"])
 
 
 def golden():

@@ -142,7 +142,7 @@ def test_too_many_draws_are_refused():
 def probe_cfg(name, copies=1, phase=1):
     t = {"a": PROBE_AFFINE[0], "b": PROBE_AFFINE[1], "c": PROBE_AFFINE[2], "d": PROBE_AFFINE[3], "e": PROBE_AFFINE[4],
          "f": PROBE_AFFINE[5], "weight": 1.0, "color": 0.5, "variations": {name: 1.0}}
-    if phase != 1:                                   # the probe's `linear` carrier (src/probe/batch.rs:26-47)
+    if phase in (0, 2):                              # the probe's `linear` carrier (src/probe/batch.rs:26-47)
         t["variations"] = {"linear": 1.0, name: 1.0}
         t["variation_order"] = ["linear", name]
     return {"flame": {"transforms": [t] * copies}, "deterministic_rng": True}
