@@ -444,7 +444,7 @@ def run_batched(args, local_rank, steps=None, serial_steps=None):
     samples a pixel): one batched, graph-captured render against the same
     flames rendered one after another.  flames/s, device-timed; then the
     same comparison within each resolution class (the class's flames as a
-    batch of their own, with the whole batch's tuned launch shape)."""
+    batch of their own, tuned for themselves)."""
     import torch
     from ffb200 import Batch, _native, synthetic
     torch.cuda.set_device(local_rank)
@@ -492,8 +492,7 @@ def run_batched(args, local_rank, steps=None, serial_steps=None):
     classes = {}
     for size in sorted({w for _, w, _, _, _ in items}):
         idx = [i for i, it in enumerate(items) if it[1] == size]
-        bc = Batch(r, [items[i] for i in idx], tune=False, threads=info["threads"],
-                   iterations_per_thread=info["iterations_per_walker"])
+        bc = Batch(r, [items[i] for i in idx], tune=True)
         bms = time_batch(bc)
         samples = bc.info()["samples"]
         bc.close()

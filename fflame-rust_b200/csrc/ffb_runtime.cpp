@@ -1526,12 +1526,15 @@ void batch_enqueue(ffb_batch* B, uint32_t threads, uint32_t iters, uint64_t scal
     ffb_renderer* r = B->r;
     size_t walk_total = 0;
     for (auto& F : B->flames) {
+        // The walkers of the full budget whatever the scale (a tuning run
+        // keeps the real run's occupancy), each walking its share of the
+        // scaled budget.
         const uint64_t budget = std::max<uint64_t>(1, F.budget / scale);
-        uint64_t w = (budget + iters - 1) / iters;
+        uint64_t w = (F.budget + iters - 1) / iters;
         w = std::max<uint64_t>(w, threads);
         w = (w + threads - 1) / threads * threads;
         F.walkers = (uint32_t)w;
-        F.per_walker = (uint32_t)((budget + w - 1) / w);
+        F.per_walker = (uint32_t)std::max<uint64_t>(1, (budget + w - 1) / w);
         F.walk_off = walk_total;
         walk_total += w;
     }
@@ -1718,7 +1721,8 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
         ck(cudaMemcpyAsync(B->palettes.ensure(pals.size() * 4), pals.data(), pals.size() * 4, cudaMemcpyHostToDevice, s), "upload palettes");
         ck(cudaMemcpyAsync(B->luts.ensure(luts.size() * 4), luts.data(), luts.size() * 4, cudaMemcpyHostToDevice, s), "upload curves");
         // Autotune: time each (schedule, threads, iterations a walker) on
-        // 1/64 of every budget; keep the fastest per sample.  The
+        // 1/64 of every budget with the full run's walkers; keep the one
+        // whose time, scaled to the full run, is least.  The
         // transform-sorted kernel regroups walkers so a warp runs one
         // transform's variations; where every transform carries the same
         // variations (the sort removes no divergence) one walker a thread
@@ -1749,7 +1753,17 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
                     ck(cudaEventElapsedTime(&ms, r->ev0, r->ev1), "event time");
                     uint64_t samples = 0;
                     for (auto& F : B->flames) samples += (uint64_t)F.walkers * F.per_walker;
-                    const double per = ms / (double)samples;
+                    // The full run's time at this trial's cost an iteration
+                    // (burn-in included: its share differs between the
+                    // scaled and the full run).
+                    double tuned = 0, full = 0;
+                    for (auto& F : B->flames) {
+                        const uint64_t per_full = (F.budget + F.walkers - 1) / F.walkers;
+                        tuned += (double)F.walkers * (double)(F.per_walker + F.P.burn_in);
+                        full += (double)F.walkers * (double)(per_full + F.P.burn_in);
+                    }
+                    (void)samples;
+                    const double per = ms * full / tuned;
                     if (per < best) { best = per; B->threads = t; B->iters = it; best_plain = c.plain; }
                 }
             B->plain = best_plain;
