@@ -1721,9 +1721,12 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
         ck(cudaMemcpyAsync(B->palettes.ensure(pals.size() * 4), pals.data(), pals.size() * 4, cudaMemcpyHostToDevice, s), "upload palettes");
         ck(cudaMemcpyAsync(B->luts.ensure(luts.size() * 4), luts.data(), luts.size() * 4, cudaMemcpyHostToDevice, s), "upload curves");
         // Autotune: time each (schedule, threads, iterations a walker) on
-        // 1/64 of every budget with the full run's walkers; keep the one
-        // whose time, scaled to the full run, is least.  The
-        // transform-sorted kernel regroups walkers so a warp runs one
+        // 1/8 of every budget with the full run's walkers; keep the one
+        // whose time, scaled to the full run, is least (at 1/64 a trial's
+        // fixed costs and burn-in skewed the choice: 5.26 s picked against
+        // 3.87 s for the best shape on the 256-flame set).
+        constexpr uint64_t kTuneScale = 8;
+        // The transform-sorted kernel regroups walkers so a warp runs one
         // transform's variations; where every transform carries the same
         // variations (the sort removes no divergence) one walker a thread
         // saves the regrouping.  The one-walker kernel's blocks are the
@@ -1744,15 +1747,13 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
                 for (uint32_t it : cand_i) {
                     const uint32_t t = c.t;
                     B->plain = c.plain;
-                    batch_enqueue(B.get(), t, it, 64, s, false);             // warm (allocations)
+                    batch_enqueue(B.get(), t, it, kTuneScale, s, false);     // warm (allocations)
                     ck(cudaEventRecord(r->ev0, s), "event");
-                    batch_enqueue(B.get(), t, it, 64, s, false);
+                    batch_enqueue(B.get(), t, it, kTuneScale, s, false);
                     ck(cudaEventRecord(r->ev1, s), "event");
                     ck(cudaStreamSynchronize(s), "tune");
                     float ms = 0.f;
                     ck(cudaEventElapsedTime(&ms, r->ev0, r->ev1), "event time");
-                    uint64_t samples = 0;
-                    for (auto& F : B->flames) samples += (uint64_t)F.walkers * F.per_walker;
                     // The full run's time at this trial's cost an iteration
                     // (burn-in included: its share differs between the
                     // scaled and the full run).
@@ -1762,7 +1763,6 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
                         tuned += (double)F.walkers * (double)(F.per_walker + F.P.burn_in);
                         full += (double)F.walkers * (double)(per_full + F.P.burn_in);
                     }
-                    (void)samples;
                     const double per = ms * full / tuned;
                     if (per < best) { best = per; B->threads = t; B->iters = it; best_plain = c.plain; }
                 }

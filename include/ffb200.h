@@ -98,8 +98,11 @@ typedef struct {
     uint32_t plot;                     /* 0 auto, 1 inline (each walker plots its own samples), 2 deferred:
                                           the chaos kernel stores its samples and a plot kernel (the final
                                           chain, palette, symmetry copies, splat) runs beside the next
-                                          launch on a second stream; the same histogram (Philox stream, no
-                                          spatial filter, direct accumulation; otherwise inline) */
+                                          launch on a second stream; 3 fused: plot warps in the walkers'
+                                          own blocks take the samples through shared memory (no sample
+                                          leaves the multiprocessor); the same histogram (Philox stream, no
+                                          spatial filter, direct accumulation; fused also without an xaos
+                                          orbit refresh; otherwise deferred or inline) */
     /* RenderProgress (src/renderer/render.rs:293-301, 624-693): `progress`
        is called after each launch of the chaos game with the plotted
        samples submitted so far and the render's total; `cancelled`
