@@ -237,8 +237,11 @@ static const VarDef kRegistry[] = {
     {"blur_pixelize", 76, 2, 2, {"size", "scale"}, {0.1f, 1.0f}, "v_blur_pixelize", 0, 0, nullptr},
     {"separation", 77, 0, 4, {"x", "y", "xinside", "yinside"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_separation", 0, 0, nullptr},
     {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
+    {"post_curl", 83, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_post_curl", VF_POST, 0, nullptr},
     {"cpow", 85, 1, 3, {"r", "i", "power"}, {1.0f, 0.1f, 1.5f}, "v_cpow", 0, 3, derive_cpow},
     {"acoth", 86, 0, 0, NP, ND, "v_acoth", 0, 0, nullptr},
+    {"arcsech", 89, 0, 0, NP, ND, "v_arcsech", 0, 0, nullptr},
+    {"arcsech2", 90, 0, 0, NP, ND, "v_arcsech2", 0, 0, nullptr},
     {"arcsinh", 91, 0, 0, NP, ND, "v_arcsinh", 0, 0, nullptr},
     {"arctanh", 92, 0, 0, NP, ND, "v_arctanh", 0, 0, nullptr},
     {"sin", 93, 0, 0, NP, ND, "v_sin", 0, 0, nullptr},
@@ -253,6 +256,18 @@ static const VarDef kRegistry[] = {
     {"coth", 102, 0, 0, NP, ND, "v_coth", 0, 0, nullptr},
     {"sech", 103, 0, 0, NP, ND, "v_sech", 0, 0, nullptr},
     {"csch", 104, 0, 0, NP, ND, "v_csch", 0, 0, nullptr},
+    {"sinq", 105, 0, 0, NP, ND, "v_sinq", 0, 0, nullptr},
+    {"cosq", 106, 0, 0, NP, ND, "v_cosq", 0, 0, nullptr},
+    {"tanq", 107, 0, 0, NP, ND, "v_tanq", 0, 0, nullptr},
+    {"cotq", 108, 0, 0, NP, ND, "v_cotq", 0, 0, nullptr},
+    {"secq", 109, 0, 0, NP, ND, "v_secq", 0, 0, nullptr},
+    {"cscq", 110, 0, 0, NP, ND, "v_cscq", 0, 0, nullptr},
+    {"sinhq", 111, 0, 0, NP, ND, "v_sinhq", 0, 0, nullptr},
+    {"coshq", 112, 0, 0, NP, ND, "v_coshq", 0, 0, nullptr},
+    {"tanhq", 113, 0, 0, NP, ND, "v_tanhq", 0, 0, nullptr},
+    {"cothq", 114, 0, 0, NP, ND, "v_cothq", 0, 0, nullptr},
+    {"sechq", 115, 0, 0, NP, ND, "v_sechq", 0, 0, nullptr},
+    {"cschq", 116, 0, 0, NP, ND, "v_cschq", 0, 0, nullptr},
     {"sin2_bs", 123, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sin2_bs", 0, 0, nullptr},
     {"cos2_bs", 124, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cos2_bs", 0, 0, nullptr},
     {"tan2_bs", 125, 0, 4, {"x1", "x2", "y1", "y2"}, {2.0f, 2.0f, 2.0f, 2.0f}, "v_tan2_bs", 0, 0, nullptr},
@@ -298,6 +313,7 @@ static const VarDef kRegistry[] = {
     {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
     {"henon", 213, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_henon", 0, 0, nullptr},
     {"loonie3", 217, 0, 0, NP, ND, "v_loonie3", VF_W, 0, nullptr},
+    {"pre_curl", 221, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_pre_curl", VF_PRE | VF_W, 0, nullptr},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
@@ -305,6 +321,16 @@ static const VarDef kRegistry[] = {
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"squirrel", 249, 0, 2, {"a", "b"}, {1.0f, 1.0f}, "v_squirrel", VF_REPLACE, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
+    {"bCollide", 262, 0, 2, {"num", "a"}, {1.0f, 0.0f}, "v_bCollide", 0, 0, nullptr},
+    {"bMod", 263, 0, 2, {"radius", "distance"}, {1.0f, 0.0f}, "v_bMod", 0, 0, nullptr},
+    {"bSwirl", 264, 0, 2, {"in_p", "out_p"}, {0.0f, 0.0f}, "v_bSwirl", 0, 0, nullptr},
+    {"barycentroid", 265, 0, 4, {"a", "b", "c", "d"}, {1.0f, 0.0f, 0.0f, 1.0f}, "v_barycentroid", 0, 0, nullptr},
+    {"eCollide", 266, 0, 2, {"num", "a"}, {1.0f, 0.0f}, "v_eCollide", 0, 0, nullptr},
+    {"eMod", 267, 0, 2, {"radius", "distance"}, {1.0f, 0.0f}, "v_eMod", 0, 0, nullptr},
+    {"eSwirl", 268, 0, 2, {"in_p", "out_p"}, {1.2f, 0.2f}, "v_eSwirl", 0, 0, nullptr},
+    {"eScale", 269, 0, 2, {"scale", "angle"}, {1.0f, 0.0f}, "v_eScale", 0, 0, nullptr},
+    {"ePush", 270, 0, 3, {"push", "dist", "rotate"}, {0.0f, 1.0f, 0.0f}, "v_ePush", 0, 0, nullptr},
+    {"eRotate", 271, 0, 1, {"rotate"}, {0.0f}, "v_eRotate", 0, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
     {"mcarpet", 282, 0, 4, {"x", "y", "twist", "tilt"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_mcarpet", 0, 0, nullptr},

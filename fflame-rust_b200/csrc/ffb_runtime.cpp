@@ -1721,11 +1721,14 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
         ck(cudaMemcpyAsync(B->palettes.ensure(pals.size() * 4), pals.data(), pals.size() * 4, cudaMemcpyHostToDevice, s), "upload palettes");
         ck(cudaMemcpyAsync(B->luts.ensure(luts.size() * 4), luts.data(), luts.size() * 4, cudaMemcpyHostToDevice, s), "upload curves");
         // Autotune: time each (schedule, threads, iterations a walker) on
-        // 1/8 of every budget with the full run's walkers; keep the one
-        // whose time, scaled to the full run, is least (at 1/64 a trial's
-        // fixed costs and burn-in skewed the choice: 5.26 s picked against
-        // 3.87 s for the best shape on the 256-flame set).
-        constexpr uint64_t kTuneScale = 8;
+        // 1/16 and 1/8 of every budget with the full run's walkers, and
+        // extrapolate linearly in the iterations walked (burn-in included)
+        // to the full run: the intercept is the per-flame work that does
+        // not grow with the budget (histogram clears, density estimation,
+        // tone map).  Scaling one trial's time by the iteration ratio
+        // alone charged that fixed work more to shapes whose trials walk
+        // a larger share of burn-in: it picked 256 threads x 256
+        // iterations (4.59 s) over 128 x 4096 (3.87 s) on a 256-flame set.
         // The transform-sorted kernel regroups walkers so a warp runs one
         // transform's variations; where every transform carries the same
         // variations (the sort removes no divergence) one walker a thread
@@ -1747,23 +1750,27 @@ FFB_API int ffb_batch_create(ffb_renderer* r, const ffb_batch_item* items, uint3
                 for (uint32_t it : cand_i) {
                     const uint32_t t = c.t;
                     B->plain = c.plain;
-                    batch_enqueue(B.get(), t, it, kTuneScale, s, false);     // warm (allocations)
-                    ck(cudaEventRecord(r->ev0, s), "event");
-                    batch_enqueue(B.get(), t, it, kTuneScale, s, false);
-                    ck(cudaEventRecord(r->ev1, s), "event");
-                    ck(cudaStreamSynchronize(s), "tune");
-                    float ms = 0.f;
-                    ck(cudaEventElapsedTime(&ms, r->ev0, r->ev1), "event time");
-                    // The full run's time at this trial's cost an iteration
-                    // (burn-in included: its share differs between the
-                    // scaled and the full run).
-                    double tuned = 0, full = 0;
+                    // (time ms, iterations walked) at 1/16 and 1/8; the
+                    // first call of a shape also sizes its buffers.
+                    double ms[2], walked[2], full = 0;
+                    batch_enqueue(B.get(), t, it, 16, s, false);
+                    for (int k = 0; k < 2; ++k) {
+                        ck(cudaEventRecord(r->ev0, s), "event");
+                        batch_enqueue(B.get(), t, it, k ? 8 : 16, s, false);
+                        ck(cudaEventRecord(r->ev1, s), "event");
+                        ck(cudaStreamSynchronize(s), "tune");
+                        float e = 0.f;
+                        ck(cudaEventElapsedTime(&e, r->ev0, r->ev1), "event time");
+                        ms[k] = e;
+                        walked[k] = 0;
+                        for (auto& F : B->flames) walked[k] += (double)F.walkers * (double)(F.per_walker + F.P.burn_in);
+                    }
                     for (auto& F : B->flames) {
                         const uint64_t per_full = (F.budget + F.walkers - 1) / F.walkers;
-                        tuned += (double)F.walkers * (double)(F.per_walker + F.P.burn_in);
                         full += (double)F.walkers * (double)(per_full + F.P.burn_in);
                     }
-                    const double per = ms * full / tuned;
+                    const double slope = walked[1] > walked[0] ? (ms[1] - ms[0]) / (walked[1] - walked[0]) : 0.0;
+                    const double per = slope > 0.0 ? ms[1] + slope * (full - walked[1]) : ms[1] * full / walked[1];
                     if (per < best) { best = per; B->threads = t; B->iters = it; best_plain = c.plain; }
                 }
             B->plain = best_plain;

@@ -53,6 +53,32 @@ REGISTRY = {
     "csch2_bs": 134, "ennepers": 154, "rays2": 156, "rays3": 157, "squirrel": 249, "anamorphcyl": 296, "roundspher": 326,
     "deltaA": 336, "sintrange": 354, "hyperbolicellipse": 362, "post_spherical": 388, "svensson_js": 436,
     "epispiral_wf": 446,
+    "post_curl": 83,
+    "arcsech": 89,
+    "arcsech2": 90,
+    "sinq": 105,
+    "cosq": 106,
+    "tanq": 107,
+    "cotq": 108,
+    "secq": 109,
+    "cscq": 110,
+    "sinhq": 111,
+    "coshq": 112,
+    "tanhq": 113,
+    "cothq": 114,
+    "sechq": 115,
+    "cschq": 116,
+    "pre_curl": 221,
+    "bCollide": 262,
+    "bMod": 263,
+    "bSwirl": 264,
+    "barycentroid": 265,
+    "eCollide": 266,
+    "eMod": 267,
+    "eSwirl": 268,
+    "eScale": 269,
+    "ePush": 270,
+    "eRotate": 271,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -128,6 +154,18 @@ PARAMS.update({
     "squirrel": [("a", 1.0), ("b", 1.0)],
     "anamorphcyl": [("a", 1.0), ("b", 1.3), ("k", 3.0)],
     "svensson_js": [("a", 1.4), ("b", 1.56), ("c", 1.4), ("d", -6.56)],
+    "post_curl": [("c1", 0.0), ("c2", 0.0)],
+    "pre_curl": [("c1", 0.0), ("c2", 0.0)],
+    "bCollide": [("num", 1.0), ("a", 0.0)],
+    "bMod": [("radius", 1.0), ("distance", 0.0)],
+    "bSwirl": [("in_p", 0.0), ("out_p", 0.0)],
+    "barycentroid": [("a", 1.0), ("b", 0.0), ("c", 0.0), ("d", 1.0)],
+    "eCollide": [("num", 1.0), ("a", 0.0)],
+    "eMod": [("radius", 1.0), ("distance", 0.0)],
+    "eSwirl": [("in_p", 1.2), ("out_p", 0.2)],
+    "eScale": [("scale", 1.0), ("angle", 0.0)],
+    "ePush": [("push", 0.0), ("dist", 1.0), ("rotate", 0.0)],
+    "eRotate": [("rotate", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

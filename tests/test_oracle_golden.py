@@ -59,6 +59,10 @@ SFU_SIN = {
 # these inputs, for `twist * p.x * p.x`, so 0 * inf gave NaN where the
 # source order (twist * p.x) * p.x gives a finite value here.
 HUGE_ARGS = ["large", "near_threshold", "past_threshold", "lopsided"]
+# Where the bipolar series' sigma is f32(pi) (sin(sigma) -4.4e-8 here, 0 on
+# the reference) and the elliptic series' nu is f32(pi)/2 (cos(nu) -4.4e-8).
+BIPOLAR_PI = ["+0+0", "+0-0", "-0+0", "-0-0", "+x", "-x", "unit", "tiny", "normal_min", "subnormal", "y_neg0x"]
+ELLIPTIC_PI2 = ["+0+0", "+0-0", "-0+0", "-0-0", "+y", "-y", "tiny", "normal_min", "subnormal", "neg0y_x"]
 WIDER = {
     "heart": dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero"),
     "diamond": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"),
@@ -147,6 +151,36 @@ WIDER = {
     "sintrange": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), "lopsided": "inf*0"},
     "squirrel": dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"),
     "svensson_js": {**dict.fromkeys(["tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "post_curl": {"-0-0": "signed-zero"},
+    "sinq": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"),
+        **dict.fromkeys(["large", "past_threshold"], "inf*0"),
+        **dict.fromkeys(["near_threshold", "lopsided"], "huge")},
+    "cosq": {"pi_e": "zero", **dict.fromkeys(["large", "past_threshold"], "inf*0"),
+        **dict.fromkeys(["near_threshold", "lopsided"], "huge")},
+    "tanq": {**dict.fromkeys(["pi_e", "normal_min"], "zero"), "tiny": "tiny-quotient"},
+    "cotq": {**dict.fromkeys(["pi_e", "normal_min"], "zero"), "tiny": "tiny-quotient"},
+    "secq": dict.fromkeys(["pi_e", "tiny"], "zero"),
+    "cscq": {**dict.fromkeys(["pi_e", "normal_min"], "zero"), "tiny": "tiny-quotient"},
+    "sinhq": {**dict.fromkeys(["tiny", "normal_min"], "zero"),
+        **dict.fromkeys(["large", "past_threshold", "lopsided"], "inf*0"), "near_threshold": "huge"},
+    "coshq": {**dict.fromkeys(["large", "past_threshold", "lopsided"], "inf*0"), "near_threshold": "huge"},
+    "tanhq": {"tiny": "tiny-quotient", "normal_min": "zero"},
+    "cothq": {"tiny": "tiny-quotient", "normal_min": "zero"},
+    "sechq": {"tiny": "zero"},
+    "cschq": {"tiny": "tiny-quotient", "normal_min": "zero"},
+    "bCollide": dict.fromkeys(BIPOLAR_PI, "zero"),
+    "bMod": dict.fromkeys(BIPOLAR_PI, "zero"),
+    "bSwirl": dict.fromkeys(BIPOLAR_PI, "zero"),
+    "eCollide": {**dict.fromkeys(ELLIPTIC_PI2, "zero"),
+        **dict.fromkeys(HUGE_ARGS, "inf*0")},
+    "eMod": {**dict.fromkeys(ELLIPTIC_PI2, "zero"),
+        **dict.fromkeys(HUGE_ARGS, "inf*0")},
+    "eScale": {**dict.fromkeys(ELLIPTIC_PI2, "zero"),
+        **dict.fromkeys(HUGE_ARGS, "inf*0")},
+    "ePush": {**dict.fromkeys(ELLIPTIC_PI2, "zero"),
+        **dict.fromkeys(HUGE_ARGS, "inf*0")},
+    "eRotate": {**dict.fromkeys(ELLIPTIC_PI2, "zero"),
+        **dict.fromkeys(HUGE_ARGS, "inf*0")},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -160,7 +194,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "blur_pixelize", "tancos", "spiralwing", "panorama1", "panorama2", "circleblur", "henon",
                        "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy", "rippled", "loonie3",
                        "d_spherical", "acoth", "arcsinh", "arctanh", "ennepers", "post_spherical", "rays2", "rays3",
-                       "roundspher", "sech2_bs"])
+                       "roundspher", "sech2_bs",
+                       "arcsech", "arcsech2", "pre_curl", "barycentroid"])
 
 
 def golden():
