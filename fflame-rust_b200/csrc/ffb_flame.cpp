@@ -303,24 +303,36 @@ static const VarDef kRegistry[] = {
     {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
+    {"gridout", 192, 0, 0, NP, ND, "v_gridout", 0, 0, nullptr},
     {"panorama1", 194, 0, 0, NP, ND, "v_panorama1", 0, 0, nullptr},
     {"panorama2", 195, 0, 0, NP, ND, "v_panorama2", 0, 0, nullptr},
     {"circleblur", 198, 2, 0, NP, ND, "v_circleblur", 0, 0, nullptr},
     {"circlesplit", 199, 0, 2, {"radius", "split"}, {1.0f, 0.5f}, "v_circlesplit", 0, 0, nullptr},
     {"flipcircle", 200, 0, 0, NP, ND, "v_flipcircle", VF_W, 0, nullptr},
+    {"bipolar2", 202, 0, 9, {"shift", "a", "b", "c", "d", "e", "f1", "g1", "h"}, {0.0f, 1.0f, 2.0f, 0.5f, 1.0f, 2.0f, 0.25f, 1.0f, 1.0f}, "v_bipolar2", 0, 0, nullptr},
     {"wedge_julia", 210, 1, 4, {"power", "dist", "count", "angle"}, {7.0f, 0.2f, 2.0f, 0.3f}, "v_wedge_julia", 0, 3, derive_wedge_julia},
     {"wedge_sph", 211, 0, 4, {"angle", "hole", "count", "swirl"}, {0.2f, 0.2f, 2.0f, 0.3f}, "v_wedge_sph", 0, 1, derive_wedge_sph},
     {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
     {"henon", 213, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_henon", 0, 0, nullptr},
     {"loonie3", 217, 0, 0, NP, ND, "v_loonie3", VF_W, 0, nullptr},
+    {"sigmoid", 219, 0, 2, {"shiftx", "shifty"}, {1.0f, 1.0f}, "v_sigmoid", VF_W, 0, nullptr},
+    {"blocky", 220, 0, 3, {"x", "y", "mp"}, {1.0f, 1.0f, 4.0f}, "v_blocky", VF_W, 0, nullptr},
     {"pre_curl", 221, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_pre_curl", VF_PRE | VF_W, 0, nullptr},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
+    {"kaleidoscope", 233, 0, 5, {"pull", "rotate", "line_up", "x", "y"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_kaleidoscope", VF_W, 0, nullptr},
+    {"hole2", 235, 0, 6, {"a", "b", "c", "d", "inside", "shape"}, {1.0f, 2.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_hole2", 0, 0, nullptr},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
+    {"eclipse", 242, 0, 1, {"shift"}, {0.0f}, "v_eclipse", VF_W, 0, nullptr},
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
     {"pulse", 244, 0, 4, {"freqx", "freqy", "scalex", "scaley"}, {2.0f, 2.0f, 1.0f, 1.0f}, "v_pulse", 0, 0, nullptr},
+    {"hypershift", 245, 0, 2, {"shift", "stretch"}, {2.0f, 1.0f}, "v_hypershift", VF_W, 0, nullptr},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"squirrel", 249, 0, 2, {"a", "b"}, {1.0f, 1.0f}, "v_squirrel", VF_REPLACE, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
+    {"chunk", 257, 0, 7, {"a", "b", "c", "d", "e", "f", "mode"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f, -1.0f, 0.0f}, "v_chunk", VF_W, 0, nullptr},
+    {"pTransform", 258, 0, 5, {"rotate", "power", "move", "split", "use_log"}, {0.0f, 1.0f, 0.0f, 0.0f, 1.0f}, "v_pTransform", 0, 0, nullptr},
+    {"rational3", 259, 0, 8, {"a", "b", "c", "d", "e", "f", "g", "h"}, {0.5f, 0.0f, 0.0f, 1.0f, 0.0f, 1.0f, 0.0f, 1.0f}, "v_rational3", 0, 0, nullptr},
+    {"ortho", 261, 0, 2, {"in_p", "out_p"}, {0.0f, 0.0f}, "v_ortho", 0, 0, nullptr},
     {"bCollide", 262, 0, 2, {"num", "a"}, {1.0f, 0.0f}, "v_bCollide", 0, 0, nullptr},
     {"bMod", 263, 0, 2, {"radius", "distance"}, {1.0f, 0.0f}, "v_bMod", 0, 0, nullptr},
     {"bSwirl", 264, 0, 2, {"in_p", "out_p"}, {0.0f, 0.0f}, "v_bSwirl", 0, 0, nullptr},
@@ -331,18 +343,33 @@ static const VarDef kRegistry[] = {
     {"eScale", 269, 0, 2, {"scale", "angle"}, {1.0f, 0.0f}, "v_eScale", 0, 0, nullptr},
     {"ePush", 270, 0, 3, {"push", "dist", "rotate"}, {0.0f, 1.0f, 0.0f}, "v_ePush", 0, 0, nullptr},
     {"eRotate", 271, 0, 1, {"rotate"}, {0.0f}, "v_eRotate", 0, 0, nullptr},
+    {"corners", 272, 0, 9, {"xwidth", "ywidth", "multx", "multy", "xpower", "ypower", "xypower", "logmode", "log_base"}, {1.0f, 1.0f, 1.0f, 1.0f, 0.75f, 0.75f, 0.0f, 0.0f, 2.71828f}, "v_corners", VF_W, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
+    {"circlize", 276, 0, 1, {"hole"}, {0.4f}, "v_circlize", VF_W, 0, nullptr},
+    {"circlize2", 277, 0, 1, {"hole"}, {0.0f}, "v_circlize2", 0, 0, nullptr},
+    {"atan", 278, 0, 2, {"mode", "stretch"}, {0.0f, 1.0f}, "v_atan", 0, 0, nullptr},
+    {"collideoscope", 280, 0, 2, {"a", "num"}, {0.2f, 1.0f}, "v_collideoscope", 0, 0, nullptr},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
     {"mcarpet", 282, 0, 4, {"x", "y", "twist", "tilt"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_mcarpet", 0, 0, nullptr},
     {"oscilloscope", 284, 0, 4, {"separation", "frequency", "amplitude", "damping"}, {1.0f, 3.14159265f, 1.0f, 0.0f}, "v_oscilloscope", 0, 1, derive_oscilloscope},
+    {"fibonacci2", 285, 0, 2, {"sc", "sc2"}, {1.0f, 1.0f}, "v_fibonacci2", 0, 0, nullptr},
     {"linearT", 287, 0, 2, {"powX", "powY"}, {1.2f, 1.2f}, "v_linearT", 0, 0, nullptr},
+    {"disc3", 290, 0, 8, {"a", "b", "c", "d", "e", "f", "g", "h"}, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f}, "v_disc3", 0, 0, nullptr},
+    {"projective", 291, 0, 9, {"a", "b", "c", "a1", "b1", "c1", "a2", "b2", "c2"}, {0.0f, 0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_projective", 0, 0, nullptr},
     {"anamorphcyl", 296, 0, 3, {"a", "b", "k"}, {1.0f, 1.3f, 3.0f}, "v_anamorphcyl", VF_REPLACE, 0, nullptr},
+    {"shredlin", 298, 0, 4, {"xdistance", "xwidth", "ydistance", "ywidth"}, {1.0f, 0.5f, 1.0f, 0.5f}, "v_shredlin", VF_REPLACE, 0, nullptr},
+    {"stwin", 301, 0, 4, {"distort", "offset_xy", "offset_x2", "offset_y2"}, {1.0f, 0.0f, 0.0f, 0.0f}, "v_stwin", VF_W, 0, nullptr},
     {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
+    {"devil_warp", 303, 0, 6, {"a", "b", "effect", "warp", "rmin", "rmax"}, {2.0f, 1.0f, 1.0f, 0.5f, -0.24f, 100.0f}, "v_devil_warp", VF_W, 0, nullptr},
+    {"squircular", 306, 0, 0, NP, ND, "v_squircular", VF_W, 0, nullptr},
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
+    {"rays1", 309, 0, 0, NP, ND, "v_rays1", VF_W | VF_REPLACE, 0, nullptr},
+    {"fourth", 311, 0, 5, {"spin", "space", "twist", "x", "y"}, {3.14159265f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_fourth", VF_W, 0, nullptr},
     {"arch", 312, 1, 0, NP, ND, "v_arch", VF_W, 0, nullptr},
     {"bi_linear", 313, 0, 0, NP, ND, "v_bi_linear", 0, 0, nullptr},
     {"blade", 314, 1, 0, NP, ND, "v_blade", VF_W, 0, nullptr},
+    {"squarize", 316, 0, 0, NP, ND, "v_squarize", 0, 0, nullptr},
     {"twoface", 318, 0, 0, NP, ND, "v_twoface", VF_W, 0, nullptr},
     {"twintrian", 319, 1, 0, NP, ND, "v_twintrian", VF_W, 0, nullptr},
     {"unpolar", 320, 0, 0, NP, ND, "v_unpolar", VF_W, 0, nullptr},
@@ -350,6 +377,7 @@ static const VarDef kRegistry[] = {
     {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
     {"roundspher", 326, 0, 0, NP, ND, "v_roundspher", VF_W, 0, nullptr},
+    {"erf", 332, 0, 0, NP, ND, "v_erf", 0, 0, nullptr},
     {"d_spherical", 334, 1, 1, {"d_spher_weight"}, {0.5f}, "v_d_spherical", 0, 0, nullptr},
     {"deltaA", 336, 0, 0, NP, ND, "v_deltaA", VF_W, 0, nullptr},
     {"edisc", 337, 0, 0, NP, ND, "v_edisc", VF_W, 0, nullptr},
@@ -357,11 +385,19 @@ static const VarDef kRegistry[] = {
     {"exp2", 340, 0, 0, NP, ND, "v_exp2", 0, 0, nullptr},
     {"exponential", 341, 0, 0, NP, ND, "v_exponential", 0, 0, nullptr},
     {"flipy", 342, 0, 0, NP, ND, "v_flipy", 0, 0, nullptr},
+    {"funnel", 343, 0, 1, {"effect"}, {8.0f}, "v_funnel", 0, 0, nullptr},
     {"invpolar", 344, 0, 0, NP, ND, "v_invpolar", 0, 0, nullptr},
     {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
+    {"holesq", 347, 0, 0, NP, ND, "v_holesq", VF_W, 0, nullptr},
     {"sintrange", 354, 0, 1, {"w"}, {1.0f}, "v_sintrange", VF_REPLACE, 0, nullptr},
+    {"fdisc", 358, 0, 8, {"ashift", "rshift", "xshift", "yshift", "term1", "term2", "term3", "term4"}, {1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_fdisc", 0, 0, nullptr},
+    {"csc_squared", 361, 0, 7, {"csc_div", "cos_div", "tan_div", "csc_pow", "pi_mult", "csc_add", "scaley"}, {1.0f, 1.0f, 1.0f, 0.5f, 0.5f, 0.25f, 1.0f}, "v_csc_squared", 0, 0, nullptr},
     {"hyperbolicellipse", 362, 0, 1, {"a"}, {1.0f}, "v_hyperbolicellipse", VF_REPLACE, 0, nullptr},
     {"layered_spiral", 363, 0, 1, {"radius"}, {1.0f}, "v_layered_spiral", 0, 0, nullptr},
+    {"atan2_spirals", 364, 0, 14, {"r_mult", "r_add", "xy2_mult", "xy2_add", "x_mult", "x_add", "yx_div", "yx_add", "yy_div", "yy_add", "sin_add", "y_mult", "r_power", "x2y2_pow"}, {1.5f, 1.0f, 1.125f, 0.132f, 2.0f, 0.25f, 1.0f, 0.0f, 1.25f, 0.0f, 0.0f, 1.0f, 0.5f, 1.0f}, "v_atan2_spirals", 0, 0, nullptr},
+    {"gridout2", 365, 0, 4, {"a", "b", "c", "d"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_gridout2", 0, 0, nullptr},
+    {"eMotion", 367, 0, 2, {"move", "rotate"}, {0.0f, 0.0f}, "v_eMotion", 0, 0, nullptr},
+    {"mask", 370, 0, 5, {"xshift", "yshift", "ushift", "xscale", "yscale"}, {0.0f, 0.0f, 1.0f, 1.0f, 1.0f}, "v_mask", 0, 0, nullptr},
     {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
     {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},

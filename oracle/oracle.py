@@ -79,6 +79,42 @@ REGISTRY = {
     "eScale": 269,
     "ePush": 270,
     "eRotate": 271,
+    "gridout": 192,
+    "bipolar2": 202,
+    "sigmoid": 219,
+    "blocky": 220,
+    "kaleidoscope": 233,
+    "hole2": 235,
+    "eclipse": 242,
+    "hypershift": 245,
+    "chunk": 257,
+    "pTransform": 258,
+    "rational3": 259,
+    "ortho": 261,
+    "corners": 272,
+    "circlize": 276,
+    "circlize2": 277,
+    "atan": 278,
+    "collideoscope": 280,
+    "fibonacci2": 285,
+    "disc3": 290,
+    "projective": 291,
+    "shredlin": 298,
+    "stwin": 301,
+    "devil_warp": 303,
+    "squircular": 306,
+    "rays1": 309,
+    "fourth": 311,
+    "squarize": 316,
+    "erf": 332,
+    "funnel": 343,
+    "holesq": 347,
+    "fdisc": 358,
+    "csc_squared": 361,
+    "atan2_spirals": 364,
+    "gridout2": 365,
+    "eMotion": 367,
+    "mask": 370,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -166,6 +202,40 @@ PARAMS.update({
     "eScale": [("scale", 1.0), ("angle", 0.0)],
     "ePush": [("push", 0.0), ("dist", 1.0), ("rotate", 0.0)],
     "eRotate": [("rotate", 0.0)],
+})
+PARAMS.update({
+    "bipolar2": [("shift", 0.0), ("a", 1.0), ("b", 2.0), ("c", 0.5), ("d", 1.0), ("e", 2.0), ("f1", 0.25), ("g1", 1.0), ("h", 1.0)],
+    "sigmoid": [("shiftx", 1.0), ("shifty", 1.0)],
+    "blocky": [("x", 1.0), ("y", 1.0), ("mp", 4.0)],
+    "kaleidoscope": [("pull", 0.0), ("rotate", 1.0), ("line_up", 1.0), ("x", 0.0), ("y", 0.0)],
+    "hole2": [("a", 1.0), ("b", 2.0), ("c", 1.0), ("d", 1.0), ("inside", 0.0), ("shape", 0.0)],
+    "eclipse": [("shift", 0.0)],
+    "hypershift": [("shift", 2.0), ("stretch", 1.0)],
+    "chunk": [("a", 1.0), ("b", 0.0), ("c", 1.0), ("d", 0.0), ("e", 0.0), ("f", -1.0), ("mode", 0.0)],
+    "pTransform": [("rotate", 0.0), ("power", 1.0), ("move", 0.0), ("split", 0.0), ("use_log", 1.0)],
+    "rational3": [("a", 0.5), ("b", 0.0), ("c", 0.0), ("d", 1.0), ("e", 0.0), ("f", 1.0), ("g", 0.0), ("h", 1.0)],
+    "ortho": [("in_p", 0.0), ("out_p", 0.0)],
+    "corners": [("xwidth", 1.0), ("ywidth", 1.0), ("multx", 1.0), ("multy", 1.0), ("xpower", 0.75), ("ypower", 0.75), ("xypower", 0.0), ("logmode", 0.0), ("log_base", 2.71828)],
+    "circlize": [("hole", 0.4)],
+    "circlize2": [("hole", 0.0)],
+    "atan": [("mode", 0.0), ("stretch", 1.0)],
+    "collideoscope": [("a", 0.2), ("num", 1.0)],
+    "fibonacci2": [("sc", 1.0), ("sc2", 1.0)],
+    "disc3": [("a", 1.0), ("b", 1.0), ("c", 1.0), ("d", 1.0), ("e", 1.0), ("f", 1.0), ("g", 1.0), ("h", 1.0)],
+    "projective": [("a", 0.0), ("b", 0.0), ("c", 1.0), ("a1", 1.0), ("b1", 0.0), ("c1", 0.0), ("a2", 0.0), ("b2", 1.0), ("c2", 0.0)],
+})
+PARAMS.update({
+    "shredlin": [("xdistance", 1.0), ("xwidth", 0.5), ("ydistance", 1.0), ("ywidth", 0.5)],
+    "stwin": [("distort", 1.0), ("offset_xy", 0.0), ("offset_x2", 0.0), ("offset_y2", 0.0)],
+    "devil_warp": [("a", 2.0), ("b", 1.0), ("effect", 1.0), ("warp", 0.5), ("rmin", -0.24), ("rmax", 100.0)],
+    "fourth": [("spin", 3.14159265), ("space", 0.0), ("twist", 0.0), ("x", 0.0), ("y", 0.0)],
+    "funnel": [("effect", 8.0)],
+    "fdisc": [("ashift", 1.0), ("rshift", 1.0), ("xshift", 0.0), ("yshift", 0.0), ("term1", 1.0), ("term2", 0.0), ("term3", 0.0), ("term4", 0.0)],
+    "csc_squared": [("csc_div", 1.0), ("cos_div", 1.0), ("tan_div", 1.0), ("csc_pow", 0.5), ("pi_mult", 0.5), ("csc_add", 0.25), ("scaley", 1.0)],
+    "atan2_spirals": [("r_mult", 1.5), ("r_add", 1.0), ("xy2_mult", 1.125), ("xy2_add", 0.132), ("x_mult", 2.0), ("x_add", 0.25), ("yx_div", 1.0), ("yx_add", 0.0), ("yy_div", 1.25), ("yy_add", 0.0), ("sin_add", 0.0), ("y_mult", 1.0), ("r_power", 0.5), ("x2y2_pow", 1.0)],
+    "gridout2": [("a", 1.0), ("b", 1.0), ("c", 1.0), ("d", 1.0)],
+    "eMotion": [("move", 0.0), ("rotate", 0.0)],
+    "mask": [("xshift", 0.0), ("yshift", 0.0), ("ushift", 1.0), ("xscale", 1.0), ("yscale", 1.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -57,7 +57,9 @@ SFU_SIN = {
 # denominator the body replaces by 1e-20 is finite here and 0 there;
 # "shared-square": the reference's compiler reused p.x * p.x, infinite at
 # these inputs, for `twist * p.x * p.x`, so 0 * inf gave NaN where the
-# source order (twist * p.x) * p.x gives a finite value here.
+# source order (twist * p.x) * p.x gives a finite value here;
+# "zero-divisor": the reference's tan at f32(pi) returned exactly 0, which
+# the body replaced by a 1e-30 divisor (infinite there, finite here).
 HUGE_ARGS = ["large", "near_threshold", "past_threshold", "lopsided"]
 # Where the bipolar series' sigma is f32(pi) (sin(sigma) -4.4e-8 here, 0 on
 # the reference) and the elliptic series' nu is f32(pi)/2 (cos(nu) -4.4e-8).
@@ -181,6 +183,24 @@ WIDER = {
         **dict.fromkeys(HUGE_ARGS, "inf*0")},
     "eRotate": {**dict.fromkeys(ELLIPTIC_PI2, "zero"),
         **dict.fromkeys(HUGE_ARGS, "inf*0")},
+    "hole2": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
+    "pTransform": {**dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"),
+        "lopsided": "inf*0"},
+    # ortho: the reference's cos(pi/2) = 0 meets x >= 0 at equality (+y, -y),
+    # and a / (2 theta) rounds to 1 on one side, just below it on the other
+    # (half_unit).
+    "ortho": {"-x": "zero", **dict.fromkeys(["+y", "-y", "neg0y_x", "half_unit"], "branch")},
+    "circlize": dict.fromkeys(["-x", "+y", "-y", "lopsided", "neg0y_x"], "zero"),
+    "circlize2": dict.fromkeys(["-x", "+y", "-y", "lopsided", "neg0y_x"], "zero"),
+    "fibonacci2": {**dict.fromkeys(["+x", "-x", "unit", "tiny", "normal_min", "y_neg0x"], "zero"),
+        **dict.fromkeys(["large", "near_threshold", "past_threshold"], "huge"), "lopsided": "inf*0"},
+    "disc3": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
+    "fdisc": dict.fromkeys("+0+0 +0-0 -0+0 -0-0 +x -x +y -y unit half_unit tiny normal_min subnormal y_neg0x "
+                           "neg0y_x".split(), "zero"),
+    "csc_squared": {"pi_e": "zero-divisor", **dict.fromkeys(HUGE_ARGS, "huge")},
+    "atan2_spirals": {"-x": "zero"},
+    "eMotion": {**dict.fromkeys(ELLIPTIC_PI2, "zero"), **dict.fromkeys(HUGE_ARGS, "inf*0")},
+    "mask": {"pi_e": "zero"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -195,7 +215,9 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy", "rippled", "loonie3",
                        "d_spherical", "acoth", "arcsinh", "arctanh", "ennepers", "post_spherical", "rays2", "rays3",
                        "roundspher", "sech2_bs",
-                       "arcsech", "arcsech2", "pre_curl", "barycentroid"])
+                       "arcsech", "arcsech2", "pre_curl", "barycentroid",
+                       "gridout", "bipolar2", "sigmoid", "blocky", "kaleidoscope", "eclipse", "hypershift", "chunk", "rational3", "corners", "atan", "collideoscope", "projective",
+                       "shredlin", "stwin", "squircular", "rays1", "fourth", "squarize", "erf", "holesq", "gridout2"])
 
 
 def golden():
@@ -246,6 +268,8 @@ def test_wider_registry_probe_matches_the_reference(oracle, name):
                 assert math.isfinite(v) and theirs[c] == "n", (name, label, v)
             elif why == "tiny-quotient":
                 assert math.isfinite(v) and theirs[c] in "0o", (name, label, v)
+            elif why == "zero-divisor":
+                assert math.isfinite(v) and theirs[c] in "iI", (name, label, v)
             else:
                 assert why in ("huge", "branch"), why
     if name in EXACT_DIGEST:
