@@ -228,6 +228,8 @@ static const VarDef kRegistry[] = {
     {"pre_spherical", 57, 0, 0, NP, ND, "v_pre_spherical", VF_PRE, 0, nullptr},
     {"pre_sinusoidal", 58, 0, 0, NP, ND, "v_pre_sinusoidal", VF_PRE | VF_W, 0, nullptr},
     {"pre_disc", 59, 0, 0, NP, ND, "v_pre_disc", VF_PRE | VF_W, 0, nullptr},
+    {"pre_crop", 61, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_pre_crop", VF_PRE, 0, nullptr},
+    {"falloff2", 65, 2, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_falloff2", 0, 0, nullptr},
     {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
     {"epispiral", 67, 1, 3, {"n", "thickness", "holes"}, {6.0f, 0.0f, 1.0f}, "v_epispiral", 0, 0, nullptr},
     {"juliascope", 69, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_juliascope", 0, 0, nullptr},
@@ -237,9 +239,13 @@ static const VarDef kRegistry[] = {
     {"blur_pixelize", 76, 2, 2, {"size", "scale"}, {0.1f, 1.0f}, "v_blur_pixelize", 0, 0, nullptr},
     {"separation", 77, 0, 4, {"x", "y", "xinside", "yinside"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_separation", 0, 0, nullptr},
     {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
+    {"crop", 79, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_crop", VF_REPLACE, 0, nullptr},
+    {"post_crop", 81, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_post_crop", VF_POST, 0, nullptr},
     {"post_curl", 83, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_post_curl", VF_POST, 0, nullptr},
     {"cpow", 85, 1, 3, {"r", "i", "power"}, {1.0f, 0.1f, 1.5f}, "v_cpow", 0, 3, derive_cpow},
     {"acoth", 86, 0, 0, NP, ND, "v_acoth", 0, 0, nullptr},
+    {"acosh", 87, 1, 0, NP, ND, "v_acosh", 0, 0, nullptr},
+    {"acosech", 88, 1, 0, NP, ND, "v_acosech", 0, 0, nullptr},
     {"arcsech", 89, 0, 0, NP, ND, "v_arcsech", 0, 0, nullptr},
     {"arcsech2", 90, 0, 0, NP, ND, "v_arcsech2", 0, 0, nullptr},
     {"arcsinh", 91, 0, 0, NP, ND, "v_arcsinh", 0, 0, nullptr},
@@ -268,6 +274,12 @@ static const VarDef kRegistry[] = {
     {"cothq", 114, 0, 0, NP, ND, "v_cothq", 0, 0, nullptr},
     {"sechq", 115, 0, 0, NP, ND, "v_sechq", 0, 0, nullptr},
     {"cschq", 116, 0, 0, NP, ND, "v_cschq", 0, 0, nullptr},
+    {"sqrt_acoth", 117, 1, 0, NP, ND, "v_sqrt_acoth", 0, 0, nullptr},
+    {"sqrt_acosh", 118, 1, 0, NP, ND, "v_sqrt_acosh", 0, 0, nullptr},
+    {"sqrt_acosech", 119, 1, 0, NP, ND, "v_sqrt_acosech", 0, 0, nullptr},
+    {"sqrt_asech", 120, 1, 0, NP, ND, "v_sqrt_asech", 0, 0, nullptr},
+    {"sqrt_asinh", 121, 1, 0, NP, ND, "v_sqrt_asinh", 0, 0, nullptr},
+    {"sqrt_atanh", 122, 1, 0, NP, ND, "v_sqrt_atanh", 0, 0, nullptr},
     {"sin2_bs", 123, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_sin2_bs", 0, 0, nullptr},
     {"cos2_bs", 124, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cos2_bs", 0, 0, nullptr},
     {"tan2_bs", 125, 0, 4, {"x1", "x2", "y1", "y2"}, {2.0f, 2.0f, 2.0f, 2.0f}, "v_tan2_bs", 0, 0, nullptr},
@@ -282,6 +294,8 @@ static const VarDef kRegistry[] = {
     {"csch2_bs", 134, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_csch2_bs", 0, 0, nullptr},
     {"exp2_bs", 135, 0, 3, {"x1", "y1", "y2"}, {1.0f, 1.0f, 1.0f}, "v_exp2_bs", 0, 0, nullptr},
     {"exp", 136, 0, 0, NP, ND, "v_exp", 0, 0, nullptr},
+    {"log_tile2", 138, 4, 3, {"spreadx", "spready", "spreadz"}, {2.0f, 2.0f, 0.0f}, "v_log_tile2", 0, 0, nullptr},
+    {"tile_log", 139, 2, 1, {"spread"}, {1.0f}, "v_tile_log", 0, 0, nullptr},
     {"tancos", 140, 0, 0, NP, ND, "v_tancos", 0, 0, nullptr},
     {"tangent", 141, 0, 0, NP, ND, "v_tangent", 0, 0, nullptr},
     {"secant2", 143, 0, 0, NP, ND, "v_secant2", 0, 0, nullptr},
@@ -295,6 +309,7 @@ static const VarDef kRegistry[] = {
     {"rays2", 156, 0, 0, NP, ND, "v_rays2", VF_REPLACE, 0, nullptr},
     {"rays3", 157, 0, 0, NP, ND, "v_rays3", VF_REPLACE, 0, nullptr},
     {"spiralwing", 158, 0, 0, NP, ND, "v_spiralwing", 0, 0, nullptr},
+    {"chrysanthemum", 160, 1, 0, NP, ND, "v_chrysanthemum", 0, 0, nullptr},
     {"cell", 161, 0, 1, {"size"}, {0.6f}, "v_cell", 0, 0, nullptr},
     {"flower", 163, 1, 2, {"holes", "petals"}, {0.4f, 7.0f}, "v_flower", 0, 0, nullptr},
     {"square", 166, 2, 0, NP, ND, "v_square", 0, 0, nullptr},

@@ -115,6 +115,21 @@ REGISTRY = {
     "gridout2": 365,
     "eMotion": 367,
     "mask": 370,
+    "pre_crop": 61,
+    "falloff2": 65,
+    "crop": 79,
+    "post_crop": 81,
+    "acosh": 87,
+    "acosech": 88,
+    "sqrt_acoth": 117,
+    "sqrt_acosh": 118,
+    "sqrt_acosech": 119,
+    "sqrt_asech": 120,
+    "sqrt_asinh": 121,
+    "sqrt_atanh": 122,
+    "log_tile2": 138,
+    "tile_log": 139,
+    "chrysanthemum": 160,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -236,6 +251,14 @@ PARAMS.update({
     "gridout2": [("a", 1.0), ("b", 1.0), ("c", 1.0), ("d", 1.0)],
     "eMotion": [("move", 0.0), ("rotate", 0.0)],
     "mask": [("xshift", 0.0), ("yshift", 0.0), ("ushift", 1.0), ("xscale", 1.0), ("yscale", 1.0)],
+})
+PARAMS.update({
+    "pre_crop": [("left", -1.0), ("top", -1.0), ("right", 1.0), ("bottom", 1.0), ("scatter_area", 0.0), ("zero", 0.0)],
+    "falloff2": [("scatter", 1.0), ("mindist", 0.5), ("mul_x", 1.0), ("mul_y", 1.0), ("mul_z", 0.0), ("mul_c", 0.0), ("x0", 0.0), ("y0", 0.0), ("z0", 0.0), ("invert", 0.0), ("type", 0.0)],
+    "crop": [("left", -1.0), ("top", -1.0), ("right", 1.0), ("bottom", 1.0), ("scatter_area", 0.0), ("zero", 0.0)],
+    "post_crop": [("left", -1.0), ("top", -1.0), ("right", 1.0), ("bottom", 1.0), ("scatter_area", 0.0), ("zero", 0.0)],
+    "log_tile2": [("spreadx", 2.0), ("spready", 2.0), ("spreadz", 0.0)],
+    "tile_log": [("spread", 1.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

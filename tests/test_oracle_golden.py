@@ -201,6 +201,8 @@ WIDER = {
     "atan2_spirals": {"-x": "zero"},
     "eMotion": {**dict.fromkeys(ELLIPTIC_PI2, "zero"), **dict.fromkeys(HUGE_ARGS, "inf*0")},
     "mask": {"pi_e": "zero"},
+    "pre_crop": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
+    "post_crop": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -217,7 +219,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "roundspher", "sech2_bs",
                        "arcsech", "arcsech2", "pre_curl", "barycentroid",
                        "gridout", "bipolar2", "sigmoid", "blocky", "kaleidoscope", "eclipse", "hypershift", "chunk", "rational3", "corners", "atan", "collideoscope", "projective",
-                       "shredlin", "stwin", "squircular", "rays1", "fourth", "squarize", "erf", "holesq", "gridout2"])
+                       "shredlin", "stwin", "squircular", "rays1", "fourth", "squarize", "erf", "holesq", "gridout2",
+                       "crop", "acosh", "acosech", "sqrt_acoth", "sqrt_acosh", "sqrt_acosech", "sqrt_asech", "sqrt_asinh", "sqrt_atanh", "log_tile2", "tile_log"])
 
 
 def golden():

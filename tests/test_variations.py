@@ -70,18 +70,23 @@ def test_registry_is_the_oracles(oracle):
 
 
 def test_every_variation_compiles_for_sm100a(oracle):
-    """One flame using every variation of the registry, normal transforms
-    and a final chain holding the Pre and Post ones: NVRTC builds it (no
+    """Flames using every variation of the registry between them (normal
+    transforms, and a final chain holding Pre and Post ones; as many flames
+    as keep each within the iteration's draw slots): NVRTC builds them (no
     device needed).  The subflame variations are a call of the subflame
     step, not a body of their own."""
     allv = sorted(oracle.REGISTRY, key=oracle.REGISTRY.get)
-    xfs = [{"a": 0.5, "b": 0.1, "c": -0.1, "d": 0.5, "e": 0.2, "f": -0.3, "weight": 1.0, "color": i / 10,
-            "variations": {n: 0.3 for n in allv[i:i + 6]}} for i in range(0, len(allv), 6)]
-    fin = {"a": 1, "b": 0, "c": 0, "d": 1, "e": 0, "f": 0, "weight": 1, "color": 0.5,
-           "variations": {"pre_blur": 0.1, "linear": 1.0, "flatten": 1.0, "blur": 0.2}}
-    cfg = {"flame": {"transforms": xfs, "final_transforms": [fin]}}
-    n, src = _native.specialize(json.dumps(cfg))
-    assert n > 0
+    src = ""
+    for g in range(0, len(allv), 60):
+        part = allv[g:g + 60]
+        xfs = [{"a": 0.5, "b": 0.1, "c": -0.1, "d": 0.5, "e": 0.2, "f": -0.3, "weight": 1.0, "color": i / 10,
+                "variations": {n: 0.3 for n in part[i:i + 6]}} for i in range(0, len(part), 6)]
+        fin = {"a": 1, "b": 0, "c": 0, "d": 1, "e": 0, "f": 0, "weight": 1, "color": 0.5,
+               "variations": {"pre_blur": 0.1, "linear": 1.0, "flatten": 1.0, "blur": 0.2}}
+        cfg = {"flame": {"transforms": xfs, "final_transforms": [fin]}}
+        n, part_src = _native.specialize(json.dumps(cfg))
+        assert n > 0
+        src += part_src
     for v in allv:
         if v in ("subflame_wf", "pre_subflame_wf"):
             assert f"ffb_subflame(sm, ctx, sq, " in src and f"}} }}   // {v}\n" in src, v
@@ -206,11 +211,25 @@ def test_sfu_probe_reproduces_the_reference_report(renderer, oracle, probe_pts, 
     assert not bad, f"{name}: {bad}"
 
 
-def wider_flame(oracle):
-    """Transforms using every variation beyond the twelve at random weights,
-    non-default parameters; a final chain with Pre and Post variations."""
-    rng = np.random.default_rng(11)
-    names = wider(oracle)
+def wider_flames(oracle, budget=40):
+    """The variations beyond the twelve split over flames whose draws fit
+    the iteration's slots (a final chain takes 11 more)."""
+    chunks, cur, d = [], [], 0
+    for n in wider(oracle):
+        k = oracle.var_meta(n)[0]
+        if cur and d + k > budget:
+            chunks.append(cur)
+            cur, d = [], 0
+        cur.append(n)
+        d += k
+    chunks.append(cur)
+    return [wider_flame(oracle, c, 11 + j) for j, c in enumerate(chunks)]
+
+
+def wider_flame(oracle, names, seed=11):
+    """Transforms using `names` at random weights, non-default parameters;
+    a final chain with Pre and Post variations."""
+    rng = np.random.default_rng(seed)
     xfs = []
     for i in range(0, len(names), 5):
         group = names[i:i + 5]
@@ -238,21 +257,23 @@ def wider_flame(oracle):
 
 @pytest.mark.gpu
 def test_apply_points_every_variation(renderer, oracle):
-    cfg = wider_flame(oracle)
-    fl = oracle.Flame(cfg, 64, 64)
     n = 4096
     rng = np.random.default_rng(5)
     xs = rng.uniform(-2.5, 2.5, n).astype(np.float32)
     ys = rng.uniform(-2.5, 2.5, n).astype(np.float32)
     words = (rng.integers(0, 1 << 24, (n, 64)) / float(1 << 24)).astype(np.float32)
-    n_all = len(cfg["flame"]["transforms"]) + len(cfg["flame"]["final_transforms"])
-    for xi in range(n_all):
-        for aff in (True, False):
-            gx, gy = renderer.apply_points(cfg, xi, xs, ys, words, with_affine=aff)
-            rx, ry, sx, sy = fl.apply_xform(xi, xs, ys, words, with_affine=aff, scales=True)
-            ok = within(gx, rx, 4 * sx) & within(gy, ry, 4 * sy)
-            bad = np.where(~ok)[0]
-            assert len(bad) <= n // 1000, (xi, aff, len(bad), [(xs[i], ys[i], gx[i], rx[i], gy[i], ry[i], sx[i], sy[i]) for i in bad[:4]])
+    for f, cfg in enumerate(wider_flames(oracle)):
+        fl = oracle.Flame(cfg, 64, 64)
+        n_all = len(cfg["flame"]["transforms"]) + len(cfg["flame"]["final_transforms"])
+        for xi in range(n_all):
+            for aff in (True, False):
+                gx, gy = renderer.apply_points(cfg, xi, xs, ys, words, with_affine=aff)
+                rx, ry, sx, sy = fl.apply_xform(xi, xs, ys, words, with_affine=aff, scales=True)
+                ok = within(gx, rx, 4 * sx) & within(gy, ry, 4 * sy)
+                bad = np.where(~ok)[0]
+                names = list(cfg["flame"]["transforms"][xi]["variations"]) if xi < len(cfg["flame"]["transforms"]) else "final"
+                assert len(bad) <= n // 1000, (f, xi, names, aff, len(bad),
+                                               [(xs[i], ys[i], gx[i], rx[i], gy[i], ry[i], sx[i], sy[i]) for i in bad[:4]])
 
 
 @pytest.mark.gpu
@@ -315,13 +336,13 @@ def test_histogram_bit_exact_for_exactly_rounded_variations(renderer, oracle, rn
 def test_sorted_schedule_with_many_draws(renderer, oracle):
     """20 draw words an iteration (5 blocks of the counter stream): the
     regrouped walkers keep their streams."""
-    cfg = wider_flame(oracle)
     job = dict(iterations=2_000_000, walkers=6000, supersample=1)
-    for rng in ("philox", "pcg"):
-        a, _, oa = renderer.histogram(cfg, 160, 90, schedule="plain", rng=rng, iterations_per_thread=64, **job)
-        b, _, ob = renderer.histogram(cfg, 160, 90, schedule="sorted", rng=rng, iterations_per_thread=64, **job)
-        assert np.array_equal(a, b), rng
-        assert oa.inframe_samples == int(a.sum()) > 0
+    for f, cfg in enumerate(wider_flames(oracle)):
+        for rng in ("philox", "pcg"):
+            a, _, oa = renderer.histogram(cfg, 160, 90, schedule="plain", rng=rng, iterations_per_thread=64, **job)
+            b, _, ob = renderer.histogram(cfg, 160, 90, schedule="sorted", rng=rng, iterations_per_thread=64, **job)
+            assert np.array_equal(a, b), (f, rng)
+            assert oa.inframe_samples == int(a.sum()) > 0, (f, rng)
 
 
 def drawing_flame():
