@@ -321,21 +321,28 @@ static const VarDef kRegistry[] = {
     {"gridout", 192, 0, 0, NP, ND, "v_gridout", 0, 0, nullptr},
     {"panorama1", 194, 0, 0, NP, ND, "v_panorama1", 0, 0, nullptr},
     {"panorama2", 195, 0, 0, NP, ND, "v_panorama2", 0, 0, nullptr},
+    {"mobiusN", 196, 1, 10, {"re_a", "re_b", "re_c", "re_d", "im_a", "im_b", "im_c", "im_d", "power", "dist"}, {1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 1.0f}, "v_mobiusN", 0, 0, nullptr},
     {"circleblur", 198, 2, 0, NP, ND, "v_circleblur", 0, 0, nullptr},
     {"circlesplit", 199, 0, 2, {"radius", "split"}, {1.0f, 0.5f}, "v_circlesplit", 0, 0, nullptr},
     {"flipcircle", 200, 0, 0, NP, ND, "v_flipcircle", VF_W, 0, nullptr},
     {"bipolar2", 202, 0, 9, {"shift", "a", "b", "c", "d", "e", "f1", "g1", "h"}, {0.0f, 1.0f, 2.0f, 0.5f, 1.0f, 2.0f, 0.25f, 1.0f, 1.0f}, "v_bipolar2", 0, 0, nullptr},
+    {"glynnia", 205, 1, 0, NP, ND, "v_glynnia", 0, 0, nullptr},
+    {"glynnia3", 206, 1, 4, {"rscale", "dscale", "rthresh", "ythresh"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_glynnia3", 0, 0, nullptr},
     {"wedge_julia", 210, 1, 4, {"power", "dist", "count", "angle"}, {7.0f, 0.2f, 2.0f, 0.3f}, "v_wedge_julia", 0, 3, derive_wedge_julia},
     {"wedge_sph", 211, 0, 4, {"angle", "hole", "count", "swirl"}, {0.2f, 0.2f, 2.0f, 0.3f}, "v_wedge_sph", 0, 1, derive_wedge_sph},
     {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
     {"henon", 213, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_henon", 0, 0, nullptr},
+    {"apollony", 214, 1, 0, NP, ND, "v_apollony", 0, 0, nullptr},
     {"loonie3", 217, 0, 0, NP, ND, "v_loonie3", VF_W, 0, nullptr},
     {"sigmoid", 219, 0, 2, {"shiftx", "shifty"}, {1.0f, 1.0f}, "v_sigmoid", VF_W, 0, nullptr},
     {"blocky", 220, 0, 3, {"x", "y", "mp"}, {1.0f, 1.0f, 4.0f}, "v_blocky", VF_W, 0, nullptr},
     {"pre_curl", 221, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_pre_curl", VF_PRE | VF_W, 0, nullptr},
+    {"sineblur", 226, 2, 1, {"power"}, {1.0f}, "v_sineblur", 0, 0, nullptr},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"kaleidoscope", 233, 0, 5, {"pull", "rotate", "line_up", "x", "y"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_kaleidoscope", VF_W, 0, nullptr},
     {"hole2", 235, 0, 6, {"a", "b", "c", "d", "inside", "shape"}, {1.0f, 2.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_hole2", 0, 0, nullptr},
+    {"spirograph", 236, 2, 9, {"a", "b", "d", "c1", "c2", "tmin", "tmax", "ymin", "ymax"}, {3.0f, 2.0f, 0.0f, 0.0f, 0.0f, -1.0f, 1.0f, -1.0f, 1.0f}, "v_spirograph", 0, 0, nullptr},
+    {"lissajous", 237, 2, 7, {"tmin", "tmax", "a", "b", "c", "d", "e"}, {-3.14159265f, 3.14159265f, 3.0f, 2.0f, 0.0f, 0.0f, 0.0f}, "v_lissajous", 0, 0, nullptr},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
     {"eclipse", 242, 0, 1, {"shift"}, {0.0f}, "v_eclipse", VF_W, 0, nullptr},
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
@@ -344,9 +351,12 @@ static const VarDef kRegistry[] = {
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"squirrel", 249, 0, 2, {"a", "b"}, {1.0f, 1.0f}, "v_squirrel", VF_REPLACE, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
+    {"sphericalN", 253, 1, 2, {"power", "dist"}, {1.0f, 1.0f}, "v_sphericalN", 0, 0, nullptr},
+    {"tile_hlp", 255, 1, 1, {"width"}, {1.0f}, "v_tile_hlp", VF_W, 0, nullptr},
     {"chunk", 257, 0, 7, {"a", "b", "c", "d", "e", "f", "mode"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f, -1.0f, 0.0f}, "v_chunk", VF_W, 0, nullptr},
     {"pTransform", 258, 0, 5, {"rotate", "power", "move", "split", "use_log"}, {0.0f, 1.0f, 0.0f, 0.0f, 1.0f}, "v_pTransform", 0, 0, nullptr},
     {"rational3", 259, 0, 8, {"a", "b", "c", "d", "e", "f", "g", "h"}, {0.5f, 0.0f, 0.0f, 1.0f, 0.0f, 1.0f, 0.0f, 1.0f}, "v_rational3", 0, 0, nullptr},
+    {"tile_reverse", 260, 1, 3, {"space", "reversal", "vertical"}, {1.0f, 1.0f, 0.0f}, "v_tile_reverse", VF_REPLACE, 0, nullptr},
     {"ortho", 261, 0, 2, {"in_p", "out_p"}, {0.0f, 0.0f}, "v_ortho", 0, 0, nullptr},
     {"bCollide", 262, 0, 2, {"num", "a"}, {1.0f, 0.0f}, "v_bCollide", 0, 0, nullptr},
     {"bMod", 263, 0, 2, {"radius", "distance"}, {1.0f, 0.0f}, "v_bMod", 0, 0, nullptr},
@@ -371,6 +381,7 @@ static const VarDef kRegistry[] = {
     {"linearT", 287, 0, 2, {"powX", "powY"}, {1.2f, 1.2f}, "v_linearT", 0, 0, nullptr},
     {"disc3", 290, 0, 8, {"a", "b", "c", "d", "e", "f", "g", "h"}, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f}, "v_disc3", 0, 0, nullptr},
     {"projective", 291, 0, 9, {"a", "b", "c", "a1", "b1", "c1", "a2", "b2", "c2"}, {0.0f, 0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_projective", 0, 0, nullptr},
+    {"tqmirror", 292, 0, 9, {"a", "b", "c", "d", "e", "f", "g", "h", "type"}, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_tqmirror", VF_W, 0, nullptr},
     {"anamorphcyl", 296, 0, 3, {"a", "b", "k"}, {1.0f, 1.3f, 3.0f}, "v_anamorphcyl", VF_REPLACE, 0, nullptr},
     {"shredlin", 298, 0, 4, {"xdistance", "xwidth", "ydistance", "ywidth"}, {1.0f, 0.5f, 1.0f, 0.5f}, "v_shredlin", VF_REPLACE, 0, nullptr},
     {"stwin", 301, 0, 4, {"distort", "offset_xy", "offset_x2", "offset_y2"}, {1.0f, 0.0f, 0.0f, 0.0f}, "v_stwin", VF_W, 0, nullptr},
@@ -413,11 +424,17 @@ static const VarDef kRegistry[] = {
     {"gridout2", 365, 0, 4, {"a", "b", "c", "d"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_gridout2", 0, 0, nullptr},
     {"eMotion", 367, 0, 2, {"move", "rotate"}, {0.0f, 0.0f}, "v_eMotion", 0, 0, nullptr},
     {"mask", 370, 0, 5, {"xshift", "yshift", "ushift", "xscale", "yscale"}, {0.0f, 0.0f, 1.0f, 1.0f, 1.0f}, "v_mask", 0, 0, nullptr},
+    {"murl2", 372, 0, 2, {"c", "power"}, {0.1f, 3.0f}, "v_murl2", VF_W, 0, nullptr},
     {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
     {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
+    {"invsquircular", 377, 0, 0, NP, ND, "v_invsquircular", VF_W, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
     {"rippled", 380, 0, 0, NP, ND, "v_rippled", 0, 0, nullptr},
+    {"stripfit", 382, 0, 1, {"dx"}, {1.0f}, "v_stripfit", VF_W, 0, nullptr},
+    {"q_ode", 383, 0, 12, {"q_ode01", "q_ode02", "q_ode03", "q_ode04", "q_ode05", "q_ode06", "q_ode07", "q_ode08", "q_ode09", "q_ode10", "q_ode11", "q_ode12"}, {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_q_ode", VF_W, 0, nullptr},
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
+    {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
+    {"heart_wf", 429, 0, 5, {"scale_x", "scale_t", "shift_t", "scale_r_left", "scale_r_right"}, {1.0f, 1.0f, 0.0f, 1.0f, 1.0f}, "v_heart_wf", 0, 0, nullptr},
     {"clifford_js", 435, 0, 4, {"a", "b", "c", "d"}, {-1.4f, 1.6f, 1.0f, 0.7f}, "v_clifford_js", 0, 0, nullptr},
     {"svensson_js", 436, 0, 4, {"a", "b", "c", "d"}, {1.4f, 1.56f, 1.4f, -6.56f}, "v_svensson_js", VF_REPLACE, 0, nullptr},
     {"epispiral_wf", 446, 0, 1, {"waves"}, {4.0f}, "v_epispiral_wf", 0, 0, nullptr},

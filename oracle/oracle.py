@@ -130,6 +130,23 @@ REGISTRY = {
     "log_tile2": 138,
     "tile_log": 139,
     "chrysanthemum": 160,
+    "mobiusN": 196,
+    "glynnia": 205,
+    "glynnia3": 206,
+    "apollony": 214,
+    "tqmirror": 292,
+    "sineblur": 226,
+    "spirograph": 236,
+    "lissajous": 237,
+    "sphericalN": 253,
+    "tile_hlp": 255,
+    "tile_reverse": 260,
+    "murl2": 372,
+    "invsquircular": 377,
+    "stripfit": 382,
+    "q_ode": 383,
+    "waves2_radial": 390,
+    "heart_wf": 429,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -259,6 +276,22 @@ PARAMS.update({
     "post_crop": [("left", -1.0), ("top", -1.0), ("right", 1.0), ("bottom", 1.0), ("scatter_area", 0.0), ("zero", 0.0)],
     "log_tile2": [("spreadx", 2.0), ("spready", 2.0), ("spreadz", 0.0)],
     "tile_log": [("spread", 1.0)],
+})
+PARAMS.update({
+    "mobiusN": [("re_a", 1.0), ("re_b", 0.0), ("re_c", 0.0), ("re_d", 1.0), ("im_a", 0.0), ("im_b", 0.0), ("im_c", 0.0), ("im_d", 0.0), ("power", 1.0), ("dist", 1.0)],
+    "glynnia3": [("rscale", 1.0), ("dscale", 1.0), ("rthresh", 0.0), ("ythresh", 0.0)],
+    "tqmirror": [("a", 1.0), ("b", 1.0), ("c", 1.0), ("d", 1.0), ("e", 1.0), ("f", 1.0), ("g", 1.0), ("h", 1.0), ("type", 0.0)],
+    "sineblur": [("power", 1.0)],
+    "spirograph": [("a", 3.0), ("b", 2.0), ("d", 0.0), ("c1", 0.0), ("c2", 0.0), ("tmin", -1.0), ("tmax", 1.0), ("ymin", -1.0), ("ymax", 1.0)],
+    "lissajous": [("tmin", -3.14159265), ("tmax", 3.14159265), ("a", 3.0), ("b", 2.0), ("c", 0.0), ("d", 0.0), ("e", 0.0)],
+    "sphericalN": [("power", 1.0), ("dist", 1.0)],
+    "tile_hlp": [("width", 1.0)],
+    "tile_reverse": [("space", 1.0), ("reversal", 1.0), ("vertical", 0.0)],
+    "murl2": [("c", 0.1), ("power", 3.0)],
+    "stripfit": [("dx", 1.0)],
+    "q_ode": [("q_ode01", 0.0), ("q_ode02", 1.0), ("q_ode03", 0.0), ("q_ode04", 0.0), ("q_ode05", 0.0), ("q_ode06", 0.0), ("q_ode07", 0.0), ("q_ode08", 1.0), ("q_ode09", 0.0), ("q_ode10", 0.0), ("q_ode11", 0.0), ("q_ode12", 0.0)],
+    "waves2_radial": [("w2r_scalex", 0.1), ("w2r_scaley", 0.1), ("w2r_freqx", 7.0), ("w2r_freqy", 13.0), ("w2r_null", 2.0), ("w2r_distance", 10.0)],
+    "heart_wf": [("scale_x", 1.0), ("scale_t", 1.0), ("shift_t", 0.0), ("scale_r_left", 1.0), ("scale_r_right", 1.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

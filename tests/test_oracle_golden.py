@@ -56,7 +56,8 @@ SFU_SIN = {
 # error bound) where ours return the argument, so a quotient whose zero
 # denominator the body replaces by 1e-20 is finite here and 0 there;
 # "shared-square": the reference's compiler reused p.x * p.x, infinite at
-# these inputs, for `twist * p.x * p.x`, so 0 * inf gave NaN where the
+# these inputs, for `twist * p.x * p.x` (mcarpet; q_ode's `q03 * p.x * p.x`
+# and its like), so 0 * inf gave NaN where the
 # source order (twist * p.x) * p.x gives a finite value here;
 # "zero-divisor": the reference's tan at f32(pi) returned exactly 0, which
 # the body replaced by a 1e-30 divisor (infinite there, finite here).
@@ -203,6 +204,11 @@ WIDER = {
     "mask": {"pi_e": "zero"},
     "pre_crop": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
     "post_crop": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
+    "mobiusN": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
+    "sphericalN": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
+    "murl2": {"-x": "zero"},
+    "q_ode": dict.fromkeys(HUGE_ARGS, "shared-square"),
+    "heart_wf": {"-y": "zero"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -220,7 +226,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "arcsech", "arcsech2", "pre_curl", "barycentroid",
                        "gridout", "bipolar2", "sigmoid", "blocky", "kaleidoscope", "eclipse", "hypershift", "chunk", "rational3", "corners", "atan", "collideoscope", "projective",
                        "shredlin", "stwin", "squircular", "rays1", "fourth", "squarize", "erf", "holesq", "gridout2",
-                       "crop", "acosh", "acosech", "sqrt_acoth", "sqrt_acosh", "sqrt_acosech", "sqrt_asech", "sqrt_asinh", "sqrt_atanh", "log_tile2", "tile_log"])
+                       "crop", "acosh", "acosech", "sqrt_acoth", "sqrt_acosh", "sqrt_acosech", "sqrt_asech", "sqrt_asinh", "sqrt_atanh", "log_tile2", "tile_log",
+                       "glynnia", "glynnia3", "apollony", "tqmirror", "spirograph", "lissajous", "tile_hlp", "tile_reverse", "invsquircular", "stripfit"])
 
 
 def golden():
