@@ -229,6 +229,7 @@ static const VarDef kRegistry[] = {
     {"pre_sinusoidal", 58, 0, 0, NP, ND, "v_pre_sinusoidal", VF_PRE | VF_W, 0, nullptr},
     {"pre_disc", 59, 0, 0, NP, ND, "v_pre_disc", VF_PRE | VF_W, 0, nullptr},
     {"pre_crop", 61, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_pre_crop", VF_PRE, 0, nullptr},
+    {"pre_falloff2", 62, 3, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_pre_falloff2", VF_PRE, 0, nullptr},
     {"falloff2", 65, 2, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_falloff2", 0, 0, nullptr},
     {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
     {"epispiral", 67, 1, 3, {"n", "thickness", "holes"}, {6.0f, 0.0f, 1.0f}, "v_epispiral", 0, 0, nullptr},
@@ -241,6 +242,7 @@ static const VarDef kRegistry[] = {
     {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
     {"crop", 79, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_crop", VF_REPLACE, 0, nullptr},
     {"post_crop", 81, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_post_crop", VF_POST, 0, nullptr},
+    {"post_falloff2", 82, 3, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_post_falloff2", VF_POST, 0, nullptr},
     {"post_curl", 83, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_post_curl", VF_POST, 0, nullptr},
     {"cpow", 85, 1, 3, {"r", "i", "power"}, {1.0f, 0.1f, 1.5f}, "v_cpow", 0, 3, derive_cpow},
     {"acoth", 86, 0, 0, NP, ND, "v_acoth", 0, 0, nullptr},
@@ -399,12 +401,14 @@ static const VarDef kRegistry[] = {
     {"twoface", 318, 0, 0, NP, ND, "v_twoface", VF_W, 0, nullptr},
     {"twintrian", 319, 1, 0, NP, ND, "v_twintrian", VF_W, 0, nullptr},
     {"unpolar", 320, 0, 0, NP, ND, "v_unpolar", VF_W, 0, nullptr},
+    {"inverted_julia", 322, 1, 9, {"power", "y2_mult", "a2x_mult", "a2y_mult", "a2y_add", "cos_mult", "y_mult", "center", "x2y2_add"}, {0.25f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 3.14f, 0.0f}, "v_inverted_julia", 0, 0, nullptr},
     {"idisc", 323, 0, 0, NP, ND, "v_idisc", VF_W, 0, nullptr},
     {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
     {"roundspher", 326, 0, 0, NP, ND, "v_roundspher", VF_W, 0, nullptr},
     {"erf", 332, 0, 0, NP, ND, "v_erf", 0, 0, nullptr},
     {"d_spherical", 334, 1, 1, {"d_spher_weight"}, {0.5f}, "v_d_spherical", 0, 0, nullptr},
+    {"dustpoint", 335, 2, 0, NP, ND, "v_dustpoint", 0, 0, nullptr},
     {"deltaA", 336, 0, 0, NP, ND, "v_deltaA", VF_W, 0, nullptr},
     {"edisc", 337, 0, 0, NP, ND, "v_edisc", VF_W, 0, nullptr},
     {"curve", 338, 0, 4, {"xamp", "yamp", "xlength", "ylength"}, {0.25f, 0.5f, 1.0f, 1.0f}, "v_curve", 0, 2, derive_curve},
@@ -417,6 +421,7 @@ static const VarDef kRegistry[] = {
     {"holesq", 347, 0, 0, NP, ND, "v_holesq", VF_W, 0, nullptr},
     {"sintrange", 354, 0, 1, {"w"}, {1.0f}, "v_sintrange", VF_REPLACE, 0, nullptr},
     {"fdisc", 358, 0, 8, {"ashift", "rshift", "xshift", "yshift", "term1", "term2", "term3", "term4"}, {1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_fdisc", 0, 0, nullptr},
+    {"bTransform", 359, 1, 4, {"rotate", "power", "move", "split"}, {0.0f, 1.0f, 0.0f, 0.0f}, "v_bTransform", 0, 0, nullptr},
     {"csc_squared", 361, 0, 7, {"csc_div", "cos_div", "tan_div", "csc_pow", "pi_mult", "csc_add", "scaley"}, {1.0f, 1.0f, 1.0f, 0.5f, 0.5f, 0.25f, 1.0f}, "v_csc_squared", 0, 0, nullptr},
     {"hyperbolicellipse", 362, 0, 1, {"a"}, {1.0f}, "v_hyperbolicellipse", VF_REPLACE, 0, nullptr},
     {"layered_spiral", 363, 0, 1, {"radius"}, {1.0f}, "v_layered_spiral", 0, 0, nullptr},
@@ -434,10 +439,22 @@ static const VarDef kRegistry[] = {
     {"q_ode", 383, 0, 12, {"q_ode01", "q_ode02", "q_ode03", "q_ode04", "q_ode05", "q_ode06", "q_ode07", "q_ode08", "q_ode09", "q_ode10", "q_ode11", "q_ode12"}, {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_q_ode", VF_W, 0, nullptr},
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
+    {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},
     {"heart_wf", 429, 0, 5, {"scale_x", "scale_t", "shift_t", "scale_r_left", "scale_r_right"}, {1.0f, 1.0f, 0.0f, 1.0f, 1.0f}, "v_heart_wf", 0, 0, nullptr},
     {"clifford_js", 435, 0, 4, {"a", "b", "c", "d"}, {-1.4f, 1.6f, 1.0f, 0.7f}, "v_clifford_js", 0, 0, nullptr},
     {"svensson_js", 436, 0, 4, {"a", "b", "c", "d"}, {1.4f, 1.56f, 1.4f, -6.56f}, "v_svensson_js", VF_REPLACE, 0, nullptr},
+    {"sattractor_js", 437, 2, 1, {"m"}, {10.0f}, "v_sattractor_js", 0, 0, nullptr},
+    {"threepoint_js", 438, 2, 0, NP, ND, "v_threepoint_js", 0, 0, nullptr},
+    {"woggle_js", 440, 1, 1, {"m"}, {2.0f}, "v_woggle_js", 0, 0, nullptr},
+    {"lace_js", 441, 1, 0, NP, ND, "v_lace_js", 0, 0, nullptr},
+    {"wallpaper_js", 442, 1, 3, {"a", "b", "c"}, {1.156f, -0.28f, 21.288f}, "v_wallpaper_js", VF_W, 0, nullptr},
+    {"hadamard_js", 443, 2, 0, NP, ND, "v_hadamard_js", 0, 0, nullptr},
+    {"invtree_js", 444, 2, 0, NP, ND, "v_invtree_js", 0, 0, nullptr},
     {"epispiral_wf", 446, 0, 1, {"waves"}, {4.0f}, "v_epispiral_wf", 0, 0, nullptr},
+    {"cloverleaf_wf", 447, 1, 1, {"filled"}, {1.0f}, "v_cloverleaf_wf", 0, 0, nullptr},
+    {"rose_wf", 448, 1, 3, {"amp", "waves", "filled"}, {0.5f, 4.0f, 0.0f}, "v_rose_wf", 0, 0, nullptr},
+    {"apocarpet_js", 458, 1, 0, NP, ND, "v_apocarpet_js", 0, 0, nullptr},
+    {"siercarpet_js", 473, 1, 1, {"m"}, {3.0f}, "v_siercarpet_js", 0, 0, nullptr},
     {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},
      "v_klein_group", VF_W, 16, derive_klein_group, 1, 1},
     {"subflame_wf", 502, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},

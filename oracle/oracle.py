@@ -147,6 +147,23 @@ REGISTRY = {
     "q_ode": 383,
     "waves2_radial": 390,
     "heart_wf": 429,
+    "pre_falloff2": 62,
+    "post_falloff2": 82,
+    "inverted_julia": 322,
+    "dustpoint": 335,
+    "bTransform": 359,
+    "cannabiscurve_wf": 426,
+    "sattractor_js": 437,
+    "threepoint_js": 438,
+    "woggle_js": 440,
+    "lace_js": 441,
+    "wallpaper_js": 442,
+    "hadamard_js": 443,
+    "invtree_js": 444,
+    "cloverleaf_wf": 447,
+    "rose_wf": 448,
+    "apocarpet_js": 458,
+    "siercarpet_js": 473,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -292,6 +309,19 @@ PARAMS.update({
     "q_ode": [("q_ode01", 0.0), ("q_ode02", 1.0), ("q_ode03", 0.0), ("q_ode04", 0.0), ("q_ode05", 0.0), ("q_ode06", 0.0), ("q_ode07", 0.0), ("q_ode08", 1.0), ("q_ode09", 0.0), ("q_ode10", 0.0), ("q_ode11", 0.0), ("q_ode12", 0.0)],
     "waves2_radial": [("w2r_scalex", 0.1), ("w2r_scaley", 0.1), ("w2r_freqx", 7.0), ("w2r_freqy", 13.0), ("w2r_null", 2.0), ("w2r_distance", 10.0)],
     "heart_wf": [("scale_x", 1.0), ("scale_t", 1.0), ("shift_t", 0.0), ("scale_r_left", 1.0), ("scale_r_right", 1.0)],
+})
+PARAMS.update({
+    "pre_falloff2": [("scatter", 1.0), ("mindist", 0.5), ("mul_x", 1.0), ("mul_y", 1.0), ("mul_z", 0.0), ("mul_c", 0.0), ("x0", 0.0), ("y0", 0.0), ("z0", 0.0), ("invert", 0.0), ("type", 0.0)],
+    "post_falloff2": [("scatter", 1.0), ("mindist", 0.5), ("mul_x", 1.0), ("mul_y", 1.0), ("mul_z", 0.0), ("mul_c", 0.0), ("x0", 0.0), ("y0", 0.0), ("z0", 0.0), ("invert", 0.0), ("type", 0.0)],
+    "inverted_julia": [("power", 0.25), ("y2_mult", 1.0), ("a2x_mult", 1.0), ("a2y_mult", 1.0), ("a2y_add", 0.0), ("cos_mult", 0.0), ("y_mult", 1.0), ("center", 3.14), ("x2y2_add", 0.0)],
+    "bTransform": [("rotate", 0.0), ("power", 1.0), ("move", 0.0), ("split", 0.0)],
+    "cannabiscurve_wf": [("filled", 1.0)],
+    "sattractor_js": [("m", 10.0)],
+    "woggle_js": [("m", 2.0)],
+    "wallpaper_js": [("a", 1.156), ("b", -0.28), ("c", 21.288)],
+    "cloverleaf_wf": [("filled", 1.0)],
+    "rose_wf": [("amp", 0.5), ("waves", 4.0), ("filled", 0.0)],
+    "siercarpet_js": [("m", 3.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -65,6 +65,8 @@ HUGE_ARGS = ["large", "near_threshold", "past_threshold", "lopsided"]
 # Where the bipolar series' sigma is f32(pi) (sin(sigma) -4.4e-8 here, 0 on
 # the reference) and the elliptic series' nu is f32(pi)/2 (cos(nu) -4.4e-8).
 BIPOLAR_PI = ["+0+0", "+0-0", "-0+0", "-0-0", "+x", "-x", "unit", "tiny", "normal_min", "subnormal", "y_neg0x"]
+# The wf curves' angle atan2(x, y) at multiples of f32(pi)/2.
+WF_CURVE = ["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "lopsided", "y_neg0x"]
 ELLIPTIC_PI2 = ["+0+0", "+0-0", "-0+0", "-0-0", "+y", "-y", "tiny", "normal_min", "subnormal", "neg0y_x"]
 WIDER = {
     "heart": dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero"),
@@ -140,7 +142,7 @@ WIDER = {
     "csch2_bs": dict.fromkeys(["tiny", "normal_min"], "tiny-quotient"),
     "sec2_bs": {"pi_e": "zero", "lopsided": "huge"},
     "deltaA": dict.fromkeys(["+0+0", "+0-0", "-0+0", "-0-0", "-x", "tiny", "normal_min", "subnormal"], "zero"),
-    "epispiral_wf": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "lopsided", "y_neg0x"], "zero"),
+    "epispiral_wf": dict.fromkeys(WF_CURVE, "zero"),
     "hyperbolicellipse": {**dict.fromkeys(["-0+0", "-0-0", "neg0y_x"], "signed-zero"),
                           **dict.fromkeys(["tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
     # A Pre variation feeds the probe's linear carrier; the reference's
@@ -209,25 +211,37 @@ WIDER = {
     "murl2": {"-x": "zero"},
     "q_ode": dict.fromkeys(HUGE_ARGS, "shared-square"),
     "heart_wf": {"-y": "zero"},
+    "inverted_julia": dict.fromkeys(["+0+0", "+0-0", "-0+0", "-0-0", "-y", "neg0y_x"], "zero"),
+    "bTransform": dict.fromkeys(BIPOLAR_PI, "zero"),
+    "cannabiscurve_wf": dict.fromkeys("+0+0 +0-0 -0+0 -0-0 +x +y -y unit subnormal lopsided y_neg0x "
+                                      "neg0y_x".split(), "zero"),
+    "sattractor_js": dict.fromkeys(["q4", "neg0y_x"], "zero"),
+    "woggle_js": dict.fromkeys(["+0-0", "-0+0", "subnormal"], "zero"),
+    "lace_js": {"-x": "zero", "lopsided": "inf*0"},
+    "cloverleaf_wf": dict.fromkeys(WF_CURVE, "zero"),
+    "rose_wf": dict.fromkeys(WF_CURVE, "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
 # Bit for bit with the report (classes and the digest of the quantised values).
-EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bubble", "curl", "handkerchief", "spiral",
-                       "hyperbolic", "bent", "eyefish", "noise", "blur", "cross", "rings2", "pdj", "rectangles", "splits",
-                       "pre_blur", "secant2", "pie", "butterfly", "fan", "fisheye", "stripes", "bent2", "rings", "linear3D",
-                       "klein_group", "subflame_wf", "pre_subflame_wf", "loonie", "scry", "elliptic", "bipolar", "lazysusan",
-                       "separation", "cell", "edisc", "curve", "square", "blade", "twintrian", "arch", "parabola",
-                       "super_shape", "conic", "cpow", "boarders", "oscilloscope", "blur_circle", "blur_zoom",
-                       "blur_pixelize", "tancos", "spiralwing", "panorama1", "panorama2", "circleblur", "henon",
-                       "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy", "rippled", "loonie3",
-                       "d_spherical", "acoth", "arcsinh", "arctanh", "ennepers", "post_spherical", "rays2", "rays3",
-                       "roundspher", "sech2_bs",
-                       "arcsech", "arcsech2", "pre_curl", "barycentroid",
-                       "gridout", "bipolar2", "sigmoid", "blocky", "kaleidoscope", "eclipse", "hypershift", "chunk", "rational3", "corners", "atan", "collideoscope", "projective",
-                       "shredlin", "stwin", "squircular", "rays1", "fourth", "squarize", "erf", "holesq", "gridout2",
-                       "crop", "acosh", "acosech", "sqrt_acoth", "sqrt_acosh", "sqrt_acosech", "sqrt_asech", "sqrt_asinh", "sqrt_atanh", "log_tile2", "tile_log",
-                       "glynnia", "glynnia3", "apollony", "tqmirror", "spirograph", "lissajous", "tile_hlp", "tile_reverse", "invsquircular", "stripfit"])
+EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bubble", "curl", "handkerchief",
+                       "spiral", "hyperbolic", "bent", "eyefish", "noise", "blur", "cross", "rings2", "pdj",
+                       "rectangles", "splits", "pre_blur", "secant2", "pie", "butterfly", "fan", "fisheye", "stripes",
+                       "bent2", "rings", "linear3D", "klein_group", "subflame_wf", "pre_subflame_wf", "loonie",
+                       "scry", "elliptic", "bipolar", "lazysusan", "separation", "cell", "edisc", "curve", "square",
+                       "blade", "twintrian", "arch", "parabola", "super_shape", "conic", "cpow", "boarders",
+                       "oscilloscope", "blur_circle", "blur_zoom", "blur_pixelize", "tancos", "spiralwing",
+                       "panorama1", "panorama2", "circleblur", "henon", "cylinder2", "flipcircle", "lozi",
+                       "bi_linear", "twoface", "flipy", "rippled", "loonie3", "d_spherical", "acoth", "arcsinh",
+                       "arctanh", "ennepers", "post_spherical", "rays2", "rays3", "roundspher", "sech2_bs", "arcsech",
+                       "arcsech2", "pre_curl", "barycentroid", "gridout", "bipolar2", "sigmoid", "blocky",
+                       "kaleidoscope", "eclipse", "hypershift", "chunk", "rational3", "corners", "atan",
+                       "collideoscope", "projective", "shredlin", "stwin", "squircular", "rays1", "fourth",
+                       "squarize", "erf", "holesq", "gridout2", "crop", "acosh", "acosech", "sqrt_acoth",
+                       "sqrt_acosh", "sqrt_acosech", "sqrt_asech", "sqrt_asinh", "sqrt_atanh", "log_tile2",
+                       "tile_log", "glynnia", "glynnia3", "apollony", "tqmirror", "spirograph", "lissajous",
+                       "tile_hlp", "tile_reverse", "invsquircular", "stripfit", "dustpoint", "threepoint_js",
+                       "wallpaper_js", "hadamard_js", "invtree_js", "apocarpet_js", "siercarpet_js"])
 
 
 def golden():
