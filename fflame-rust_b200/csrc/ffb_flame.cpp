@@ -169,6 +169,52 @@ void derive_subflame(const float* u, float* o) {
     o[0] = std::cos(ang);
     o[1] = std::sin(ang);
 }
+void derive_shift(const float* u, float* o) {                   // misc_2d.rs (init_shift)
+    const float a = u[2] * 3.14159265358979f / 180.0f;
+    o[0] = std::cos(a); o[1] = std::sin(a);
+}
+void derive_pressure_wave(const float* u, float* o) {           // misc_2d.rs (init_pressure_wave)
+    const float tp = 6.28318530717959f;
+    const float px = u[0] != 0.0f ? u[0] * tp : 1.0f, py = u[1] != 0.0f ? u[1] * tp : 1.0f;
+    o[0] = px; o[1] = py; o[2] = 1.0f / px; o[3] = 1.0f / py;
+}
+void derive_spligon(const float* u, float* o) {                 // misc_2d.rs (init_spligon)
+    const float s = u[0] == 0.0f ? 1e-30f : u[0], th = s / 6.28318530717959f;
+    o[0] = th; o[1] = 1.0f / th; o[2] = 3.14159265358979f * u[1] / (-2.0f * s);
+}
+void derive_circus(const float* u, float* o) { o[0] = 1.0f / std::max(u[0], 1e-6f); }   // singleton_misc.rs (init_circus)
+void derive_murl(const float* u, float* o) {                    // singleton_misc.rs (init_murl)
+    float c = u[0];
+    if (u[1] != 1.0f) { const float m = u[1] - 1.0f; c = c / (std::fabs(m) < 1e-30f ? 1e-30f : m); }
+    o[0] = c; o[1] = u[1] * 0.5f; o[2] = c + 1.0f;
+}
+void derive_target(const float* u, float* o) { o[0] = 0.5f * u[2]; }                    // init_ports.rs (init_target)
+void derive_bwraps(const float* u, float* o) {                  // extended.rs (init_bwraps)
+    if (u[0] == 0.0f) { o[0] = o[1] = o[2] = 0.0f; return; }
+    const float rad = 0.5f * (u[0] / (1.0f + u[1] * u[1])), g2 = (u[2] * u[2]) / (rad + 1e-6f) + 1e-6f;
+    float mb = g2 * rad;
+    mb = mb > 2.0f ? 1.0f : mb * (1.0f / ((mb * mb) / 4.0f + 1.0f));
+    o[0] = g2; o[1] = rad * rad; o[2] = rad / mb;
+}
+void derive_hypertile(const float* u, float* o) {               // hypertile.rs (init_hypertile)
+    const float pi = 3.14159265358979f, pa = 2.0f * pi / u[0], qa = 2.0f * pi / u[1];
+    const float ri = (1.0f - std::cos(pa)) / (std::cos(pa) + std::cos(qa)) + 1.0f;
+    const float r = ri > 0.0f ? 1.0f / std::sqrt(ri) : 1.0f, a = u[2] * pa;
+    o[0] = r * std::cos(a); o[1] = r * std::sin(a);
+}
+void derive_hypertile1(const float* u, float* o) {              // hypertile.rs (init_hypertile1)
+    const float pi = 3.14159265358979f, pa = 2.0f * pi / u[0], qa = 2.0f * pi / u[1];
+    const float r2 = 1.0f - (std::cos(pa) - 1.0f) / (std::cos(pa) + std::cos(qa));
+    o[0] = pa; o[1] = r2 > 0.0f ? 1.0f / std::sqrt(r2) : 1.0f;
+}
+void derive_blur_linear(const float* u, float* o) { o[0] = std::cos(u[1]); o[1] = std::sin(u[1]); }   // circle_blur.rs
+void derive_shredrad(const float* u, float* o) {                // misc_extras4.rs (init_shredrad)
+    o[0] = 6.28318530717959f / (std::fabs(u[0]) < 1e-6f ? 1e-6f : u[0]);
+}
+void derive_xheart(const float* u, float* o) {                  // misc_extras4.rs (init_xheart)
+    const float ang = 0.7853981633974483f + 0.39269908169872414f * u[0];
+    o[0] = 6.0f + 2.0f * u[1]; o[1] = std::cos(ang); o[2] = std::sin(ang);
+}
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -233,6 +279,7 @@ static const VarDef kRegistry[] = {
     {"falloff2", 65, 2, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_falloff2", 0, 0, nullptr},
     {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
     {"epispiral", 67, 1, 3, {"n", "thickness", "holes"}, {6.0f, 0.0f, 1.0f}, "v_epispiral", 0, 0, nullptr},
+    {"bwraps", 68, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_bwraps", 0, 3, derive_bwraps},
     {"juliascope", 69, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_juliascope", 0, 0, nullptr},
     {"radial_blur", 73, 4, 1, {"angle"}, {0.0f}, "v_radial_blur", VF_W, 2, derive_radial_blur},
     {"blur_circle", 74, 2, 0, NP, ND, "v_blur_circle", 0, 0, nullptr},
@@ -317,7 +364,10 @@ static const VarDef kRegistry[] = {
     {"square", 166, 2, 0, NP, ND, "v_square", 0, 0, nullptr},
     {"popcorn2", 170, 0, 3, {"x", "y", "c"}, {1.0f, 0.5f, 1.5f}, "v_popcorn2", 0, 0, nullptr},
     {"disc2", 178, 0, 2, {"rot", "twist"}, {2.0f, 0.5f}, "v_disc2", 0, 3, derive_disc2},
+    {"target", 179, 0, 3, {"even", "odd", "size"}, {0.0f, 0.0f, 1.0f}, "v_target", 0, 1, derive_target},
     {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
+    {"hypertile", 184, 0, 3, {"p", "q", "n"}, {3.0f, 7.0f, 1.0f}, "v_hypertile", 0, 2, derive_hypertile},
+    {"hypertile1", 185, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile1", 0, 2, derive_hypertile1},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
     {"gridout", 192, 0, 0, NP, ND, "v_gridout", 0, 0, nullptr},
@@ -327,6 +377,7 @@ static const VarDef kRegistry[] = {
     {"circleblur", 198, 2, 0, NP, ND, "v_circleblur", 0, 0, nullptr},
     {"circlesplit", 199, 0, 2, {"radius", "split"}, {1.0f, 0.5f}, "v_circlesplit", 0, 0, nullptr},
     {"flipcircle", 200, 0, 0, NP, ND, "v_flipcircle", VF_W, 0, nullptr},
+    {"blur_linear", 201, 1, 2, {"length", "angle"}, {1.0f, 0.5f}, "v_blur_linear", 0, 2, derive_blur_linear},
     {"bipolar2", 202, 0, 9, {"shift", "a", "b", "c", "d", "e", "f1", "g1", "h"}, {0.0f, 1.0f, 2.0f, 0.5f, 1.0f, 2.0f, 0.25f, 1.0f, 1.0f}, "v_bipolar2", 0, 0, nullptr},
     {"glynnia", 205, 1, 0, NP, ND, "v_glynnia", 0, 0, nullptr},
     {"glynnia3", 206, 1, 4, {"rscale", "dscale", "rthresh", "ythresh"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_glynnia3", 0, 0, nullptr},
@@ -353,7 +404,10 @@ static const VarDef kRegistry[] = {
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"squirrel", 249, 0, 2, {"a", "b"}, {1.0f, 1.0f}, "v_squirrel", VF_REPLACE, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
+    {"shift", 251, 0, 3, {"shift_x", "shift_y", "angle"}, {0.0f, 0.0f, 0.0f}, "v_shift", 0, 2, derive_shift},
+    {"pressure_wave", 252, 0, 2, {"x_freq", "y_freq"}, {1.0f, 1.0f}, "v_pressure_wave", 0, 4, derive_pressure_wave},
     {"sphericalN", 253, 1, 2, {"power", "dist"}, {1.0f, 1.0f}, "v_sphericalN", 0, 0, nullptr},
+    {"spligon", 254, 0, 2, {"sides", "i"}, {3.0f, 1.0f}, "v_spligon", 0, 3, derive_spligon},
     {"tile_hlp", 255, 1, 1, {"width"}, {1.0f}, "v_tile_hlp", VF_W, 0, nullptr},
     {"chunk", 257, 0, 7, {"a", "b", "c", "d", "e", "f", "mode"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f, -1.0f, 0.0f}, "v_chunk", VF_W, 0, nullptr},
     {"pTransform", 258, 0, 5, {"rotate", "power", "move", "split", "use_log"}, {0.0f, 1.0f, 0.0f, 0.0f, 1.0f}, "v_pTransform", 0, 0, nullptr},
@@ -372,9 +426,11 @@ static const VarDef kRegistry[] = {
     {"eRotate", 271, 0, 1, {"rotate"}, {0.0f}, "v_eRotate", 0, 0, nullptr},
     {"corners", 272, 0, 9, {"xwidth", "ywidth", "multx", "multy", "xpower", "ypower", "xypower", "logmode", "log_base"}, {1.0f, 1.0f, 1.0f, 1.0f, 0.75f, 0.75f, 0.0f, 0.0f, 2.71828f}, "v_corners", VF_W, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
+    {"circus", 275, 0, 1, {"scale"}, {1.0f}, "v_circus", 0, 1, derive_circus},
     {"circlize", 276, 0, 1, {"hole"}, {0.4f}, "v_circlize", VF_W, 0, nullptr},
     {"circlize2", 277, 0, 1, {"hole"}, {0.0f}, "v_circlize2", 0, 0, nullptr},
     {"atan", 278, 0, 2, {"mode", "stretch"}, {0.0f, 1.0f}, "v_atan", 0, 0, nullptr},
+    {"murl", 279, 0, 2, {"c", "power"}, {0.1f, 1.0f}, "v_murl", 0, 3, derive_murl},
     {"collideoscope", 280, 0, 2, {"a", "num"}, {0.2f, 1.0f}, "v_collideoscope", 0, 0, nullptr},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
     {"mcarpet", 282, 0, 4, {"x", "y", "twist", "tilt"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_mcarpet", 0, 0, nullptr},
@@ -386,6 +442,8 @@ static const VarDef kRegistry[] = {
     {"tqmirror", 292, 0, 9, {"a", "b", "c", "d", "e", "f", "g", "h", "type"}, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_tqmirror", VF_W, 0, nullptr},
     {"anamorphcyl", 296, 0, 3, {"a", "b", "k"}, {1.0f, 1.3f, 3.0f}, "v_anamorphcyl", VF_REPLACE, 0, nullptr},
     {"shredlin", 298, 0, 4, {"xdistance", "xwidth", "ydistance", "ywidth"}, {1.0f, 0.5f, 1.0f, 0.5f}, "v_shredlin", VF_REPLACE, 0, nullptr},
+    {"shredrad", 299, 0, 2, {"n", "width"}, {4.0f, 0.5f}, "v_shredrad", 0, 1, derive_shredrad},
+    {"xheart", 300, 0, 2, {"angle", "ratio"}, {0.0f, 0.0f}, "v_xheart", 0, 3, derive_xheart},
     {"stwin", 301, 0, 4, {"distort", "offset_xy", "offset_x2", "offset_y2"}, {1.0f, 0.0f, 0.0f, 0.0f}, "v_stwin", VF_W, 0, nullptr},
     {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
     {"devil_warp", 303, 0, 6, {"a", "b", "effect", "warp", "rmin", "rmax"}, {2.0f, 1.0f, 1.0f, 0.5f, -0.24f, 100.0f}, "v_devil_warp", VF_W, 0, nullptr},

@@ -164,6 +164,18 @@ REGISTRY = {
     "rose_wf": 448,
     "apocarpet_js": 458,
     "siercarpet_js": 473,
+    "bwraps": 68,
+    "hypertile": 184,
+    "hypertile1": 185,
+    "blur_linear": 201,
+    "target": 179,
+    "shift": 251,
+    "pressure_wave": 252,
+    "spligon": 254,
+    "circus": 275,
+    "murl": 279,
+    "shredrad": 299,
+    "xheart": 300,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -322,6 +334,20 @@ PARAMS.update({
     "cloverleaf_wf": [("filled", 1.0)],
     "rose_wf": [("amp", 0.5), ("waves", 4.0), ("filled", 0.0)],
     "siercarpet_js": [("m", 3.0)],
+})
+PARAMS.update({
+    "bwraps": [("cellsize", 1.0), ("space", 0.0), ("gain", 1.0), ("inner_twist", 0.0), ("outer_twist", 0.0)],
+    "hypertile": [("p", 3.0), ("q", 7.0), ("n", 1.0)],
+    "hypertile1": [("p", 3.0), ("q", 7.0)],
+    "blur_linear": [("length", 1.0), ("angle", 0.5)],
+    "target": [("even", 0.0), ("odd", 0.0), ("size", 1.0)],
+    "shift": [("shift_x", 0.0), ("shift_y", 0.0), ("angle", 0.0)],
+    "pressure_wave": [("x_freq", 1.0), ("y_freq", 1.0)],
+    "spligon": [("sides", 3.0), ("i", 1.0)],
+    "circus": [("scale", 1.0)],
+    "murl": [("c", 0.1), ("power", 1.0)],
+    "shredrad": [("n", 4.0), ("width", 0.5)],
+    "xheart": [("angle", 0.0), ("ratio", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -220,6 +220,13 @@ WIDER = {
     "lace_js": {"-x": "zero", "lopsided": "inf*0"},
     "cloverleaf_wf": dict.fromkeys(WF_CURVE, "zero"),
     "rose_wf": dict.fromkeys(WF_CURVE, "zero"),
+    "bwraps": {"lopsided": "zero"},
+    "target": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
+    "spligon": dict.fromkeys(["+0-0", "-0-0", "-y", "tiny", "subnormal"], "zero"),
+    "circus": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
+    "murl": {"-x": "zero"},
+    "shredrad": {**dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"), "lopsided": "inf*0"},
+    "xheart": {"normal_min": "zero"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -241,7 +248,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "sqrt_acosh", "sqrt_acosech", "sqrt_asech", "sqrt_asinh", "sqrt_atanh", "log_tile2",
                        "tile_log", "glynnia", "glynnia3", "apollony", "tqmirror", "spirograph", "lissajous",
                        "tile_hlp", "tile_reverse", "invsquircular", "stripfit", "dustpoint", "threepoint_js",
-                       "wallpaper_js", "hadamard_js", "invtree_js", "apocarpet_js", "siercarpet_js"])
+                       "wallpaper_js", "hadamard_js", "invtree_js", "apocarpet_js", "siercarpet_js", "hypertile",
+                       "hypertile1", "blur_linear", "shift"])
 
 
 def golden():
