@@ -215,6 +215,39 @@ void derive_xheart(const float* u, float* o) {                  // misc_extras4.
     const float ang = 0.7853981633974483f + 0.39269908169872414f * u[0];
     o[0] = 6.0f + 2.0f * u[1]; o[1] = std::cos(ang); o[2] = std::sin(ang);
 }
+void derive_pre_bwraps(const float* u, float* o) {              // pre_phase.rs (init_pre_bwraps), post_phase.rs
+    derive_bwraps(u, o);
+    o[3] = u[3]; o[4] = u[4];
+}
+void derive_hypertile2(const float* u, float* o) { derive_hypertile1(u, o); }   // hypertile.rs (init_hypertile2)
+void derive_glynnSim1(const float* u, float* o) {               // glynn.rs (init_glynnSim1)
+    const float a = 3.14159265358979f * u[2] / 180.0f;
+    o[0] = u[0] * std::cos(a); o[1] = u[0] * std::sin(a); o[2] = std::fabs(u[4]);
+}
+void derive_glynnSim2(const float* u, float* o) {               // glynn.rs (init_glynnSim2)
+    const float pi180 = (float)(3.14159265358979 / 180.0);      // folded in double, as the shader's constant expression
+    const float p10 = pi180 * u[4], p20 = pi180 * u[5];
+    o[0] = p10; o[1] = u[1] * (2.0f * u[0] + u[1]) / std::max(u[0] + u[1], 1e-30f);
+    o[2] = p20 - p10; o[3] = std::fabs(u[3]); o[4] = u[0] + u[1];
+}
+void derive_glynnSim3(const float* u, float* o) {               // glynn.rs (init_glynnSim3)
+    const float r1 = u[0] + u[1], s1 = r1 == 0.0f ? 1e-30f : r1, r2 = (u[0] * u[0]) / s1;
+    o[0] = r1; o[1] = r2; o[2] = r1 / std::max(r1 + r2, 1e-30f); o[3] = std::fabs(u[3]);
+}
+void derive_target_sp(const float* u, float* o) {               // radial_extras.rs (init_target_sp)
+    const float pi = 3.14159265358979f, rota = pi * u[0];
+    o[0] = 0.5f * u[2]; o[1] = rota; o[2] = -pi + rota;
+}
+void derive_starblur(const float* u, float* o) {                // blur_extras.rs (init_starblur)
+    const float pw = std::max(u[0], 1.0f), a0 = 3.14159265358979f / pw;
+    const float len = std::sqrt(std::max(1.0f + u[1] * u[1] - 2.0f * u[1] * std::cos(a0), 1e-30f));
+    o[0] = std::asin(std::sin(a0) * u[1] / len); o[1] = len;
+}
+void derive_vogel(const float* u, float* o) {                   // parametric_curves.rs (init_vogel)
+    (void)u;
+    const float phi = 1.618033988749895f;
+    o[0] = 6.28318530717959f / (phi * phi);
+}
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -274,6 +307,7 @@ static const VarDef kRegistry[] = {
     {"pre_spherical", 57, 0, 0, NP, ND, "v_pre_spherical", VF_PRE, 0, nullptr},
     {"pre_sinusoidal", 58, 0, 0, NP, ND, "v_pre_sinusoidal", VF_PRE | VF_W, 0, nullptr},
     {"pre_disc", 59, 0, 0, NP, ND, "v_pre_disc", VF_PRE | VF_W, 0, nullptr},
+    {"pre_bwraps", 60, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_pre_bwraps", VF_PRE, 5, derive_pre_bwraps},
     {"pre_crop", 61, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_pre_crop", VF_PRE, 0, nullptr},
     {"pre_falloff2", 62, 3, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_pre_falloff2", VF_PRE, 0, nullptr},
     {"falloff2", 65, 2, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_falloff2", 0, 0, nullptr},
@@ -288,6 +322,7 @@ static const VarDef kRegistry[] = {
     {"separation", 77, 0, 4, {"x", "y", "xinside", "yinside"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_separation", 0, 0, nullptr},
     {"mobius", 78, 0, 8, {"re_a", "im_a", "re_b", "im_b", "re_c", "im_c", "re_d", "im_d"}, {0.1f, 0.2f, 0.2f, -0.12f, -0.15f, -0.15f, 0.21f, 0.1f}, "v_mobius", 0, 0, nullptr},
     {"crop", 79, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_crop", VF_REPLACE, 0, nullptr},
+    {"post_bwraps", 80, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_post_bwraps", VF_POST, 5, derive_pre_bwraps},
     {"post_crop", 81, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_post_crop", VF_POST, 0, nullptr},
     {"post_falloff2", 82, 3, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_post_falloff2", VF_POST, 0, nullptr},
     {"post_curl", 83, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_post_curl", VF_POST, 0, nullptr},
@@ -368,6 +403,7 @@ static const VarDef kRegistry[] = {
     {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
     {"hypertile", 184, 0, 3, {"p", "q", "n"}, {3.0f, 7.0f, 1.0f}, "v_hypertile", 0, 2, derive_hypertile},
     {"hypertile1", 185, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile1", 0, 2, derive_hypertile1},
+    {"hypertile2", 186, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile2", 0, 2, derive_hypertile2},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
     {"gridout", 192, 0, 0, NP, ND, "v_gridout", 0, 0, nullptr},
@@ -381,21 +417,27 @@ static const VarDef kRegistry[] = {
     {"bipolar2", 202, 0, 9, {"shift", "a", "b", "c", "d", "e", "f1", "g1", "h"}, {0.0f, 1.0f, 2.0f, 0.5f, 1.0f, 2.0f, 0.25f, 1.0f, 1.0f}, "v_bipolar2", 0, 0, nullptr},
     {"glynnia", 205, 1, 0, NP, ND, "v_glynnia", 0, 0, nullptr},
     {"glynnia3", 206, 1, 4, {"rscale", "dscale", "rthresh", "ythresh"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_glynnia3", 0, 0, nullptr},
+    {"glynnSim1", 207, 3, 6, {"radius", "radius1", "phi1", "thickness", "pow", "contrast"}, {1.0f, 0.1f, 110.0f, 0.1f, 1.5f, 0.5f}, "v_glynnSim1", 0, 3, derive_glynnSim1},
+    {"glynnSim2", 208, 3, 6, {"radius", "thickness", "contrast", "pow", "phi1", "phi2"}, {1.0f, 0.1f, 0.5f, 1.5f, 110.0f, 150.0f}, "v_glynnSim2", 0, 5, derive_glynnSim2},
+    {"glynnSim3", 209, 3, 4, {"radius", "thickness", "contrast", "pow"}, {1.0f, 0.1f, 0.5f, 1.5f}, "v_glynnSim3", 0, 4, derive_glynnSim3},
     {"wedge_julia", 210, 1, 4, {"power", "dist", "count", "angle"}, {7.0f, 0.2f, 2.0f, 0.3f}, "v_wedge_julia", 0, 3, derive_wedge_julia},
     {"wedge_sph", 211, 0, 4, {"angle", "hole", "count", "swirl"}, {0.2f, 0.2f, 2.0f, 0.3f}, "v_wedge_sph", 0, 1, derive_wedge_sph},
     {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
     {"henon", 213, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_henon", 0, 0, nullptr},
     {"apollony", 214, 1, 0, NP, ND, "v_apollony", 0, 0, nullptr},
+    {"target_sp", 216, 0, 4, {"twist", "n_of_sp", "size", "tightness"}, {0.0f, 1.0f, 1.0f, 0.5f}, "v_target_sp", VF_W, 3, derive_target_sp},
     {"loonie3", 217, 0, 0, NP, ND, "v_loonie3", VF_W, 0, nullptr},
     {"sigmoid", 219, 0, 2, {"shiftx", "shifty"}, {1.0f, 1.0f}, "v_sigmoid", VF_W, 0, nullptr},
     {"blocky", 220, 0, 3, {"x", "y", "mp"}, {1.0f, 1.0f, 4.0f}, "v_blocky", VF_W, 0, nullptr},
     {"pre_curl", 221, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_pre_curl", VF_PRE | VF_W, 0, nullptr},
     {"sineblur", 226, 2, 1, {"power"}, {1.0f}, "v_sineblur", 0, 0, nullptr},
+    {"starblur", 227, 2, 2, {"power", "range"}, {5.0f, 0.40162283f}, "v_starblur", 0, 2, derive_starblur},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"kaleidoscope", 233, 0, 5, {"pull", "rotate", "line_up", "x", "y"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_kaleidoscope", VF_W, 0, nullptr},
     {"hole2", 235, 0, 6, {"a", "b", "c", "d", "inside", "shape"}, {1.0f, 2.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_hole2", 0, 0, nullptr},
     {"spirograph", 236, 2, 9, {"a", "b", "d", "c1", "c2", "tmin", "tmax", "ymin", "ymax"}, {3.0f, 2.0f, 0.0f, 0.0f, 0.0f, -1.0f, 1.0f, -1.0f, 1.0f}, "v_spirograph", 0, 0, nullptr},
     {"lissajous", 237, 2, 7, {"tmin", "tmax", "a", "b", "c", "d", "e"}, {-3.14159265f, 3.14159265f, 3.0f, 2.0f, 0.0f, 0.0f, 0.0f}, "v_lissajous", 0, 0, nullptr},
+    {"vogel", 238, 1, 2, {"n", "scale"}, {20.0f, 1.0f}, "v_vogel", 0, 1, derive_vogel},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
     {"eclipse", 242, 0, 1, {"shift"}, {0.0f}, "v_eclipse", VF_W, 0, nullptr},
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},

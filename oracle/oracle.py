@@ -176,6 +176,15 @@ REGISTRY = {
     "murl": 279,
     "shredrad": 299,
     "xheart": 300,
+    "pre_bwraps": 60,
+    "post_bwraps": 80,
+    "hypertile2": 186,
+    "glynnSim1": 207,
+    "glynnSim2": 208,
+    "glynnSim3": 209,
+    "target_sp": 216,
+    "starblur": 227,
+    "vogel": 238,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -348,6 +357,17 @@ PARAMS.update({
     "murl": [("c", 0.1), ("power", 1.0)],
     "shredrad": [("n", 4.0), ("width", 0.5)],
     "xheart": [("angle", 0.0), ("ratio", 0.0)],
+})
+PARAMS.update({
+    "pre_bwraps": [("cellsize", 1.0), ("space", 0.0), ("gain", 1.0), ("inner_twist", 0.0), ("outer_twist", 0.0)],
+    "post_bwraps": [("cellsize", 1.0), ("space", 0.0), ("gain", 1.0), ("inner_twist", 0.0), ("outer_twist", 0.0)],
+    "hypertile2": [("p", 3.0), ("q", 7.0)],
+    "glynnSim1": [("radius", 1.0), ("radius1", 0.1), ("phi1", 110.0), ("thickness", 0.1), ("pow", 1.5), ("contrast", 0.5)],
+    "glynnSim2": [("radius", 1.0), ("thickness", 0.1), ("contrast", 0.5), ("pow", 1.5), ("phi1", 110.0), ("phi2", 150.0)],
+    "glynnSim3": [("radius", 1.0), ("thickness", 0.1), ("contrast", 0.5), ("pow", 1.5)],
+    "target_sp": [("twist", 0.0), ("n_of_sp", 1.0), ("size", 1.0), ("tightness", 0.5)],
+    "starblur": [("power", 5.0), ("range", 0.40162283)],
+    "vogel": [("n", 20.0), ("scale", 1.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -86,6 +86,10 @@ inline RE acos(const RE& a) {
     const double s = std::sqrt(std::max(1 - a.v * a.v, 0.0));
     return re_round(std::acos(a.v), re_cap(s > 0 ? a.e / s : 1e300, a.e, 2.0), 3.0);
 }
+inline RE asin(const RE& a) {
+    const double s = std::sqrt(std::max(1 - a.v * a.v, 0.0));
+    return re_round(std::asin(a.v), re_cap(s > 0 ? a.e / s : 1e300, a.e, 2.0), 3.0);
+}
 inline RE acosh(const RE& a) {
     const double s = std::sqrt(std::max(a.v * a.v - 1, 0.0));
     return re_round(std::acosh(a.v), re_cap(s > 0 ? a.e / s : 1e300, a.e, 2.0), 3.0);

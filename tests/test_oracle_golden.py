@@ -227,6 +227,9 @@ WIDER = {
     "murl": {"-x": "zero"},
     "shredrad": {**dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"), "lopsided": "inf*0"},
     "xheart": {"normal_min": "zero"},
+    "pre_bwraps": {**dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"), "lopsided": "zero"},
+    "post_bwraps": {**dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"), "lopsided": "zero"},
+    "target_sp": {**dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"), "lopsided": "inf*0"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -249,7 +252,7 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "tile_log", "glynnia", "glynnia3", "apollony", "tqmirror", "spirograph", "lissajous",
                        "tile_hlp", "tile_reverse", "invsquircular", "stripfit", "dustpoint", "threepoint_js",
                        "wallpaper_js", "hadamard_js", "invtree_js", "apocarpet_js", "siercarpet_js", "hypertile",
-                       "hypertile1", "blur_linear", "shift"])
+                       "hypertile1", "blur_linear", "shift", "glynnSim1", "glynnSim2", "starblur"])
 
 
 def golden():
