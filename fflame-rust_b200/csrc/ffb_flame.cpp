@@ -248,6 +248,32 @@ void derive_vogel(const float* u, float* o) {                   // parametric_cu
     const float phi = 1.618033988749895f;
     o[0] = 6.28318530717959f / (phi * phi);
 }
+void derive_cpow3(const float* u, float* o) {                   // heavy_init.rs (init_cpow3)
+    const float sd = u[2] == 0.0f ? 1e-30f : u[2];
+    const float log_d = u[1] < 0.0f ? -std::log(std::max(-u[1], 1e-30f)) : std::log(std::max(u[1], 1e-30f));
+    const float pa = std::atan2(log_d * u[0], 6.28318530717959f), cpa = std::cos(pa);
+    const float c = cpa * u[0] * std::cos(pa) / sd, d = cpa * u[0] * std::sin(pa) / sd;
+    o[0] = 6.28318530717959f / sd; o[1] = c; o[2] = d; o[3] = c * 0.5f; o[4] = d * 0.5f;
+    o[5] = d == 0.0f ? 0.0f : -0.095f * u[3] / d;
+}
+void derive_yin_yang(const float* u, float* o) {                // init_ports.rs (init_yin_yang)
+    const float pi = 3.14159265358979f;
+    o[0] = std::sin(pi * u[1]); o[1] = std::cos(pi * u[1]); o[2] = std::sin(pi * u[2]); o[3] = std::cos(pi * u[2]);
+}
+void derive_oscilloscope2(const float* u, float* o) {           // misc_extras3.rs (init_oscilloscope2)
+    o[0] = 6.28318530717959f * u[1]; o[1] = 6.28318530717959f * u[2];
+}
+void derive_phoenix_julia(const float* u, float* o) {           // misc_extras3.rs (init_phoenix_julia)
+    const float sp = u[0] == 0.0f ? 1e-30f : u[0];
+    o[0] = u[1] / sp; o[1] = 6.28318530717959f / sp; o[2] = u[1] / sp * 0.5f;
+}
+void derive_pow_block(const float* u, float* o) {               // misc_extras3.rs (init_pow_block)
+    float pw = u[1] * u[2] / std::max(std::fabs(u[3]), 1e-30f);
+    if (std::fabs(pw) <= 1e-30f) pw = 1e-30f;
+    o[0] = u[0] * 0.5f / pw; o[1] = 1.0f / std::max(std::fabs(u[1]), 1e-30f);
+}
+void derive_trade(const float* u, float* o) { o[0] = u[0] + u[1]; o[1] = u[2] + u[3]; }   // watchlist_misc.rs (init_trade)
+void derive_checks(const float* u, float* o) { o[0] = 1.0f / (u[2] + 1e-30f); }           // apo_misc.rs (init_checks)
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -398,8 +424,10 @@ static const VarDef kRegistry[] = {
     {"flower", 163, 1, 2, {"holes", "petals"}, {0.4f, 7.0f}, "v_flower", 0, 0, nullptr},
     {"square", 166, 2, 0, NP, ND, "v_square", 0, 0, nullptr},
     {"popcorn2", 170, 0, 3, {"x", "y", "c"}, {1.0f, 0.5f, 1.5f}, "v_popcorn2", 0, 0, nullptr},
+    {"cpow3", 177, 4, 4, {"r", "d", "divisor", "spread"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cpow3", 0, 6, derive_cpow3},
     {"disc2", 178, 0, 2, {"rot", "twist"}, {2.0f, 0.5f}, "v_disc2", 0, 3, derive_disc2},
     {"target", 179, 0, 3, {"even", "odd", "size"}, {0.0f, 0.0f, 1.0f}, "v_target", 0, 1, derive_target},
+    {"yin_yang", 180, 1, 5, {"radius", "ang1", "ang2", "dual_t", "outside"}, {0.5f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_yin_yang", 0, 4, derive_yin_yang},
     {"popcorn", 181, 0, 0, NP, ND, "v_popcorn", VF_XF, 0, nullptr},
     {"hypertile", 184, 0, 3, {"p", "q", "n"}, {3.0f, 7.0f, 1.0f}, "v_hypertile", 0, 2, derive_hypertile},
     {"hypertile1", 185, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile1", 0, 2, derive_hypertile1},
@@ -478,7 +506,10 @@ static const VarDef kRegistry[] = {
     {"mcarpet", 282, 0, 4, {"x", "y", "twist", "tilt"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_mcarpet", 0, 0, nullptr},
     {"oscilloscope", 284, 0, 4, {"separation", "frequency", "amplitude", "damping"}, {1.0f, 3.14159265f, 1.0f, 0.0f}, "v_oscilloscope", 0, 1, derive_oscilloscope},
     {"fibonacci2", 285, 0, 2, {"sc", "sc2"}, {1.0f, 1.0f}, "v_fibonacci2", 0, 0, nullptr},
+    {"oscilloscope2", 286, 0, 6, {"separation", "frequencyx", "frequencyy", "amplitude", "perturbation", "damping"}, {1.0f, 3.14159265f, 3.14159265f, 1.0f, 1.0f, 0.0f}, "v_oscilloscope2", 0, 2, derive_oscilloscope2},
     {"linearT", 287, 0, 2, {"powX", "powY"}, {1.2f, 1.2f}, "v_linearT", 0, 0, nullptr},
+    {"phoenix_julia", 288, 1, 4, {"power", "dist", "x_distort", "y_distort"}, {3.0f, 1.0f, -0.5f, 0.0f}, "v_phoenix_julia", 0, 3, derive_phoenix_julia},
+    {"pow_block", 289, 1, 5, {"numerator", "denominator", "correctn", "correctd", "root"}, {3.0f, 2.0f, 1.0f, 1.0f, 1.0f}, "v_pow_block", 0, 2, derive_pow_block},
     {"disc3", 290, 0, 8, {"a", "b", "c", "d", "e", "f", "g", "h"}, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f}, "v_disc3", 0, 0, nullptr},
     {"projective", 291, 0, 9, {"a", "b", "c", "a1", "b1", "c1", "a2", "b2", "c2"}, {0.0f, 0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_projective", 0, 0, nullptr},
     {"tqmirror", 292, 0, 9, {"a", "b", "c", "d", "e", "f", "g", "h", "type"}, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_tqmirror", VF_W, 0, nullptr},
@@ -489,6 +520,7 @@ static const VarDef kRegistry[] = {
     {"stwin", 301, 0, 4, {"distort", "offset_xy", "offset_x2", "offset_y2"}, {1.0f, 0.0f, 0.0f, 0.0f}, "v_stwin", VF_W, 0, nullptr},
     {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
     {"devil_warp", 303, 0, 6, {"a", "b", "effect", "warp", "rmin", "rmax"}, {2.0f, 1.0f, 1.0f, 0.5f, -0.24f, 100.0f}, "v_devil_warp", VF_W, 0, nullptr},
+    {"trade", 304, 0, 4, {"r1", "d1", "r2", "d2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_trade", 0, 2, derive_trade},
     {"squircular", 306, 0, 0, NP, ND, "v_squircular", VF_W, 0, nullptr},
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
@@ -506,6 +538,7 @@ static const VarDef kRegistry[] = {
     {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
     {"roundspher", 326, 0, 0, NP, ND, "v_roundspher", VF_W, 0, nullptr},
+    {"checks", 330, 2, 4, {"x", "y", "size", "rnd"}, {0.5f, 0.5f, 0.5f, 0.0f}, "v_checks", 0, 1, derive_checks},
     {"erf", 332, 0, 0, NP, ND, "v_erf", 0, 0, nullptr},
     {"d_spherical", 334, 1, 1, {"d_spher_weight"}, {0.5f}, "v_d_spherical", 0, 0, nullptr},
     {"dustpoint", 335, 2, 0, NP, ND, "v_dustpoint", 0, 0, nullptr},

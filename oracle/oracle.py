@@ -185,6 +185,13 @@ REGISTRY = {
     "target_sp": 216,
     "starblur": 227,
     "vogel": 238,
+    "cpow3": 177,
+    "yin_yang": 180,
+    "oscilloscope2": 286,
+    "phoenix_julia": 288,
+    "pow_block": 289,
+    "trade": 304,
+    "checks": 330,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -368,6 +375,15 @@ PARAMS.update({
     "target_sp": [("twist", 0.0), ("n_of_sp", 1.0), ("size", 1.0), ("tightness", 0.5)],
     "starblur": [("power", 5.0), ("range", 0.40162283)],
     "vogel": [("n", 20.0), ("scale", 1.0)],
+})
+PARAMS.update({
+    "cpow3": [("r", 1.0), ("d", 1.0), ("divisor", 1.0), ("spread", 1.0)],
+    "yin_yang": [("radius", 0.5), ("ang1", 0.0), ("ang2", 0.0), ("dual_t", 1.0), ("outside", 0.0)],
+    "oscilloscope2": [("separation", 1.0), ("frequencyx", 3.14159265), ("frequencyy", 3.14159265), ("amplitude", 1.0), ("perturbation", 1.0), ("damping", 0.0)],
+    "phoenix_julia": [("power", 3.0), ("dist", 1.0), ("x_distort", -0.5), ("y_distort", 0.0)],
+    "pow_block": [("numerator", 3.0), ("denominator", 2.0), ("correctn", 1.0), ("correctd", 1.0), ("root", 1.0)],
+    "trade": [("r1", 1.0), ("d1", 1.0), ("r2", 1.0), ("d2", 1.0)],
+    "checks": [("x", 0.5), ("y", 0.5), ("size", 0.5), ("rnd", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)
