@@ -274,6 +274,34 @@ void derive_pow_block(const float* u, float* o) {               // misc_extras3.
 }
 void derive_trade(const float* u, float* o) { o[0] = u[0] + u[1]; o[1] = u[2] + u[3]; }   // watchlist_misc.rs (init_trade)
 void derive_checks(const float* u, float* o) { o[0] = 1.0f / (u[2] + 1e-30f); }           // apo_misc.rs (init_checks)
+void derive_boarders2(const float* u, float* o) {               // boarders.rs (init_boarders2)
+    const float c0 = std::max(std::fabs(u[0]), 1e-6f), cl0 = std::max(std::fabs(u[1]), 1e-6f), cr0 = std::max(std::fabs(u[2]), 1e-6f);
+    o[0] = c0; o[1] = c0 * cl0; o[2] = c0 + c0 * cr0;
+}
+void derive_squish(const float* u, float* o) { o[0] = 1.0f / std::max(u[0], 2.0f); }   // classic_blades_misc.rs (init_squish)
+void derive_eJulia(const float* u, float* o) { o[0] = u[0] < 0.0f ? -1.0f : 1.0f; }     // apo_misc9.rs (init_eJulia)
+void derive_julian2(const float* u, float* o) {                 // apo_misc9.rs (init_julian2)
+    const float sp = std::fabs(u[0]) < 1e-30f ? 1.0f : u[0];
+    o[0] = std::fabs(sp); o[1] = u[1] / (2.0f * sp);
+}
+// WGSL's saturating f32 -> i32 (toward zero, clamped, NaN 0).
+int32_t sat_i32f(float f) {
+    if (std::isnan(f)) return 0;
+    if (f <= -2147483648.0f) return INT32_MIN;
+    if (f >= 2147483648.0f) return INT32_MAX;
+    return (int32_t)f;
+}
+void derive_npolar(const float* u, float* o) {                  // apo_misc7.rs (init_npolar)
+    const int p = sat_i32f(u[0]), n = sat_i32f(u[1]), nz = n == 0 ? 1 : n;
+    const int ap = std::abs(p), odd = ap - (ap / 2) * 2;
+    o[0] = (float)nz; o[1] = (float)odd; o[2] = (float)std::abs(nz); o[3] = 1.0f / (2.0f * (float)nz);
+}
+void derive_waffle(const float* u, float* o) { o[0] = std::cos(u[3]); o[1] = std::sin(u[3]); }   // apo_misc12.rs (init_waffle)
+void derive_ripple(const float* u, float* o) {                  // apo_misc13.rs (init_ripple)
+    const float pi = 3.14159265358979f, tp = 6.28318530717959f;
+    const float al = u[2] * 0.01f, pl = u[5] * tp - pi, s = std::fabs(u[6]) < 1e-30f ? 1e-30f : u[6];
+    o[0] = u[0] * 5.0f; o[1] = pl; o[2] = s; o[3] = u[1] * pl; o[4] = pl * al; o[5] = (pi - pl) * al;
+}
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -461,6 +489,7 @@ static const VarDef kRegistry[] = {
     {"sineblur", 226, 2, 1, {"power"}, {1.0f}, "v_sineblur", 0, 0, nullptr},
     {"starblur", 227, 2, 2, {"power", "range"}, {5.0f, 0.40162283f}, "v_starblur", 0, 2, derive_starblur},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
+    {"boarders2", 230, 1, 3, {"c", "left", "right"}, {0.4f, 0.65f, 0.35f}, "v_boarders2", 0, 3, derive_boarders2},
     {"kaleidoscope", 233, 0, 5, {"pull", "rotate", "line_up", "x", "y"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_kaleidoscope", VF_W, 0, nullptr},
     {"hole2", 235, 0, 6, {"a", "b", "c", "d", "inside", "shape"}, {1.0f, 2.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_hole2", 0, 0, nullptr},
     {"spirograph", 236, 2, 9, {"a", "b", "d", "c1", "c2", "tmin", "tmax", "ymin", "ymax"}, {3.0f, 2.0f, 0.0f, 0.0f, 0.0f, -1.0f, 1.0f, -1.0f, 1.0f}, "v_spirograph", 0, 0, nullptr},
@@ -530,6 +559,7 @@ static const VarDef kRegistry[] = {
     {"bi_linear", 313, 0, 0, NP, ND, "v_bi_linear", 0, 0, nullptr},
     {"blade", 314, 1, 0, NP, ND, "v_blade", VF_W, 0, nullptr},
     {"squarize", 316, 0, 0, NP, ND, "v_squarize", 0, 0, nullptr},
+    {"squish", 317, 1, 1, {"power"}, {2.0f}, "v_squish", 0, 1, derive_squish},
     {"twoface", 318, 0, 0, NP, ND, "v_twoface", VF_W, 0, nullptr},
     {"twintrian", 319, 1, 0, NP, ND, "v_twintrian", VF_W, 0, nullptr},
     {"unpolar", 320, 0, 0, NP, ND, "v_unpolar", VF_W, 0, nullptr},
@@ -555,12 +585,15 @@ static const VarDef kRegistry[] = {
     {"sintrange", 354, 0, 1, {"w"}, {1.0f}, "v_sintrange", VF_REPLACE, 0, nullptr},
     {"fdisc", 358, 0, 8, {"ashift", "rshift", "xshift", "yshift", "term1", "term2", "term3", "term4"}, {1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_fdisc", 0, 0, nullptr},
     {"bTransform", 359, 1, 4, {"rotate", "power", "move", "split"}, {0.0f, 1.0f, 0.0f, 0.0f}, "v_bTransform", 0, 0, nullptr},
+    {"npolar", 360, 1, 2, {"parity", "n"}, {0.0f, 1.0f}, "v_npolar", VF_W, 4, derive_npolar},
     {"csc_squared", 361, 0, 7, {"csc_div", "cos_div", "tan_div", "csc_pow", "pi_mult", "csc_add", "scaley"}, {1.0f, 1.0f, 1.0f, 0.5f, 0.5f, 0.25f, 1.0f}, "v_csc_squared", 0, 0, nullptr},
     {"hyperbolicellipse", 362, 0, 1, {"a"}, {1.0f}, "v_hyperbolicellipse", VF_REPLACE, 0, nullptr},
     {"layered_spiral", 363, 0, 1, {"radius"}, {1.0f}, "v_layered_spiral", 0, 0, nullptr},
     {"atan2_spirals", 364, 0, 14, {"r_mult", "r_add", "xy2_mult", "xy2_add", "x_mult", "x_add", "yx_div", "yx_add", "yy_div", "yy_add", "sin_add", "y_mult", "r_power", "x2y2_pow"}, {1.5f, 1.0f, 1.125f, 0.132f, 2.0f, 0.25f, 1.0f, 0.0f, 1.25f, 0.0f, 0.0f, 1.0f, 0.5f, 1.0f}, "v_atan2_spirals", 0, 0, nullptr},
     {"gridout2", 365, 0, 4, {"a", "b", "c", "d"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_gridout2", 0, 0, nullptr},
+    {"eJulia", 366, 1, 1, {"power"}, {2.0f}, "v_eJulia", 0, 1, derive_eJulia},
     {"eMotion", 367, 0, 2, {"move", "rotate"}, {0.0f, 0.0f}, "v_eMotion", 0, 0, nullptr},
+    {"julian2", 369, 1, 8, {"power", "dist", "a", "b", "c", "d", "e", "f"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_julian2", 0, 2, derive_julian2},
     {"mask", 370, 0, 5, {"xshift", "yshift", "ushift", "xscale", "yscale"}, {0.0f, 0.0f, 1.0f, 1.0f, 1.0f}, "v_mask", 0, 0, nullptr},
     {"murl2", 372, 0, 2, {"c", "power"}, {0.1f, 3.0f}, "v_murl2", VF_W, 0, nullptr},
     {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
@@ -568,8 +601,10 @@ static const VarDef kRegistry[] = {
     {"invsquircular", 377, 0, 0, NP, ND, "v_invsquircular", VF_W, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
     {"rippled", 380, 0, 0, NP, ND, "v_rippled", 0, 0, nullptr},
+    {"waffle", 381, 5, 4, {"slices", "xthickness", "ythickness", "rotation"}, {6.0f, 0.5f, 0.5f, 0.0f}, "v_waffle", 0, 2, derive_waffle},
     {"stripfit", 382, 0, 1, {"dx"}, {1.0f}, "v_stripfit", VF_W, 0, nullptr},
     {"q_ode", 383, 0, 12, {"q_ode01", "q_ode02", "q_ode03", "q_ode04", "q_ode05", "q_ode06", "q_ode07", "q_ode08", "q_ode09", "q_ode10", "q_ode11", "q_ode12"}, {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_q_ode", VF_W, 0, nullptr},
+    {"ripple", 384, 0, 8, {"frequency", "velocity", "amplitude", "centerx", "centery", "phase", "scale", "fixed_dist_calc"}, {2.0f, 1.0f, 0.5f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_ripple", VF_REPLACE, 6, derive_ripple},
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
     {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},

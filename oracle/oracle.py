@@ -192,6 +192,13 @@ REGISTRY = {
     "pow_block": 289,
     "trade": 304,
     "checks": 330,
+    "boarders2": 230,
+    "squish": 317,
+    "npolar": 360,
+    "eJulia": 366,
+    "julian2": 369,
+    "waffle": 381,
+    "ripple": 384,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -384,6 +391,15 @@ PARAMS.update({
     "pow_block": [("numerator", 3.0), ("denominator", 2.0), ("correctn", 1.0), ("correctd", 1.0), ("root", 1.0)],
     "trade": [("r1", 1.0), ("d1", 1.0), ("r2", 1.0), ("d2", 1.0)],
     "checks": [("x", 0.5), ("y", 0.5), ("size", 0.5), ("rnd", 0.0)],
+})
+PARAMS.update({
+    "boarders2": [("c", 0.4), ("left", 0.65), ("right", 0.35)],
+    "squish": [("power", 2.0)],
+    "npolar": [("parity", 0.0), ("n", 1.0)],
+    "eJulia": [("power", 2.0)],
+    "julian2": [("power", 0.0), ("dist", 1.0), ("a", 1.0), ("b", 0.0), ("c", 0.0), ("d", 1.0), ("e", 0.0), ("f", 0.0)],
+    "waffle": [("slices", 6.0), ("xthickness", 0.5), ("ythickness", 0.5), ("rotation", 0.0)],
+    "ripple": [("frequency", 2.0), ("velocity", 1.0), ("amplitude", 0.5), ("centerx", 0.0), ("centery", 0.0), ("phase", 0.0), ("scale", 1.0), ("fixed_dist_calc", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)
