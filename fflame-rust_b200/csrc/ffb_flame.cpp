@@ -630,7 +630,31 @@ static const VarDef kRegistry[] = {
     {"pre_subflame_wf", 503, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},
      {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, -1.0f}, "v_pre_subflame_wf", VF_PRE | VF_DC | VF_SUB, 2, derive_subflame, 6, 0},
     {"linear3D", 533, 0, 0, NP, ND, "v_linear3D", 0, 0, nullptr},
-};
+
+    {"sym_ng1", 544, 1, 2, {"stepx", "stepy"}, {0.5f, 0.5f}, "v_sym_ng1", 0, 0, nullptr},
+    {"sym_ng2", 545, 1, 2, {"stepx", "stepy"}, {2.0f, 2.0f}, "v_sym_ng2", 0, 0, nullptr},
+    {"sym_ng3", 546, 1, 3, {"sepx", "sepy", "step"}, {0.5f, 0.0f, 2.0f}, "v_sym_ng3", 0, 0, nullptr},
+    {"sym_ng4", 547, 1, 4, {"sepx", "sepy", "stepx", "stepy"}, {0.0f, 0.0f, 0.0f, 0.0f}, "v_sym_ng4", 0, 0, nullptr},
+    {"sym_ng5", 548, 1, 3, {"sepx", "sepy", "stepx"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng5", 0, 0, nullptr},
+    {"sym_ng6", 549, 1, 3, {"sepy", "stepx", "stepy"}, {0.1f, 1.0f, 1.0f}, "v_sym_ng6", 0, 0, nullptr},
+    {"sym_ng7", 550, 1, 2, {"sepx", "sepy"}, {0.0f, 0.0f}, "v_sym_ng7", 0, 0, nullptr},
+    {"sym_ng8", 551, 1, 4, {"sepx", "sepy", "skewx", "skewy"}, {0.0f, 0.0f, 0.0f, 0.0f}, "v_sym_ng8", 0, 0, nullptr},
+    {"sym_ng9", 552, 1, 2, {"sepx", "sepy"}, {0.0f, 0.0f}, "v_sym_ng9", 0, 0, nullptr},
+    {"sym_ng10", 553, 1, 3, {"space", "spacex", "spacey"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng10", 0, 0, nullptr},
+    {"sym_ng11", 554, 1, 5, {"space", "spacex", "spacey", "stepx", "stepy"}, {0.0f, 0.0f, 0.0f, 1.5f, 1.5f}, "v_sym_ng11", 0, 0, nullptr},
+    {"sym_ng12", 555, 1, 3, {"space", "spacex", "spacey"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng12", 0, 0, nullptr},
+    {"sym_ng13", 556, 1, 3, {"radius", "stepx", "stepy"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng13", 0, 0, nullptr},
+    {"sym_ng14", 557, 1, 3, {"radius", "stepx", "stepy"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng14", 0, 0, nullptr},
+    {"sym_ng15", 558, 1, 3, {"radius", "stepx", "stepy"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng15", 0, 0, nullptr},
+    {"sym_ng16", 559, 1, 3, {"radius", "stepx", "stepy"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng16", 0, 0, nullptr},
+    {"sym_ng17", 560, 1, 3, {"radius", "stepx", "stepy"}, {0.0f, 0.0f, 0.0f}, "v_sym_ng17", 0, 0, nullptr},
+    {"sym_bg1", 561, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg1", 0, 0, nullptr},
+    {"sym_bg2", 562, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg2", 0, 0, nullptr},
+    {"sym_bg3", 563, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg3", 0, 0, nullptr},
+    {"sym_bg4", 564, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg4", 0, 0, nullptr},
+    {"sym_bg5", 565, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg5", 0, 0, nullptr},
+    {"sym_bg6", 566, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg6", 0, 0, nullptr},
+    {"sym_bg7", 567, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg7", 0, 0, nullptr},};
 #undef NP
 #undef ND
 

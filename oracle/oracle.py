@@ -199,6 +199,30 @@ REGISTRY = {
     "julian2": 369,
     "waffle": 381,
     "ripple": 384,
+    "sym_ng1": 544,
+    "sym_ng2": 545,
+    "sym_ng3": 546,
+    "sym_ng4": 547,
+    "sym_ng5": 548,
+    "sym_ng6": 549,
+    "sym_ng7": 550,
+    "sym_ng8": 551,
+    "sym_ng9": 552,
+    "sym_ng10": 553,
+    "sym_ng11": 554,
+    "sym_ng12": 555,
+    "sym_ng13": 556,
+    "sym_ng14": 557,
+    "sym_ng15": 558,
+    "sym_ng16": 559,
+    "sym_ng17": 560,
+    "sym_bg1": 561,
+    "sym_bg2": 562,
+    "sym_bg3": 563,
+    "sym_bg4": 564,
+    "sym_bg5": 565,
+    "sym_bg6": 566,
+    "sym_bg7": 567,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -400,6 +424,32 @@ PARAMS.update({
     "julian2": [("power", 0.0), ("dist", 1.0), ("a", 1.0), ("b", 0.0), ("c", 0.0), ("d", 1.0), ("e", 0.0), ("f", 0.0)],
     "waffle": [("slices", 6.0), ("xthickness", 0.5), ("ythickness", 0.5), ("rotation", 0.0)],
     "ripple": [("frequency", 2.0), ("velocity", 1.0), ("amplitude", 0.5), ("centerx", 0.0), ("centery", 0.0), ("phase", 0.0), ("scale", 1.0), ("fixed_dist_calc", 0.0)],
+})
+PARAMS.update({
+    "sym_ng1": [("stepx", 0.5), ("stepy", 0.5)],
+    "sym_ng2": [("stepx", 2.0), ("stepy", 2.0)],
+    "sym_ng3": [("sepx", 0.5), ("sepy", 0.0), ("step", 2.0)],
+    "sym_ng4": [("sepx", 0.0), ("sepy", 0.0), ("stepx", 0.0), ("stepy", 0.0)],
+    "sym_ng5": [("sepx", 0.0), ("sepy", 0.0), ("stepx", 0.0)],
+    "sym_ng6": [("sepy", 0.1), ("stepx", 1.0), ("stepy", 1.0)],
+    "sym_ng7": [("sepx", 0.0), ("sepy", 0.0)],
+    "sym_ng8": [("sepx", 0.0), ("sepy", 0.0), ("skewx", 0.0), ("skewy", 0.0)],
+    "sym_ng9": [("sepx", 0.0), ("sepy", 0.0)],
+    "sym_ng10": [("space", 0.0), ("spacex", 0.0), ("spacey", 0.0)],
+    "sym_ng11": [("space", 0.0), ("spacex", 0.0), ("spacey", 0.0), ("stepx", 1.5), ("stepy", 1.5)],
+    "sym_ng12": [("space", 0.0), ("spacex", 0.0), ("spacey", 0.0)],
+    "sym_ng13": [("radius", 0.0), ("stepx", 0.0), ("stepy", 0.0)],
+    "sym_ng14": [("radius", 0.0), ("stepx", 0.0), ("stepy", 0.0)],
+    "sym_ng15": [("radius", 0.0), ("stepx", 0.0), ("stepy", 0.0)],
+    "sym_ng16": [("radius", 0.0), ("stepx", 0.0), ("stepy", 0.0)],
+    "sym_ng17": [("radius", 0.0), ("stepx", 0.0), ("stepy", 0.0)],
+    "sym_bg1": [("stepx", 0.0), ("stepy", 0.0)],
+    "sym_bg2": [("stepx", 0.0), ("stepy", 0.0)],
+    "sym_bg3": [("stepx", 0.0), ("stepy", 0.0)],
+    "sym_bg4": [("stepx", 0.0), ("stepy", 0.0)],
+    "sym_bg5": [("stepx", 0.0), ("stepy", 0.0)],
+    "sym_bg6": [("stepx", 0.0), ("stepy", 0.0)],
+    "sym_bg7": [("stepx", 0.0), ("stepy", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -267,7 +267,10 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "tile_hlp", "tile_reverse", "invsquircular", "stripfit", "dustpoint", "threepoint_js",
                        "wallpaper_js", "hadamard_js", "invtree_js", "apocarpet_js", "siercarpet_js", "hypertile",
                        "hypertile1", "blur_linear", "shift", "glynnSim1", "glynnSim2", "starblur", "yin_yang",
-                       "oscilloscope2", "boarders2", "squish", "julian2", "waffle"])
+                       "oscilloscope2", "boarders2", "squish", "julian2", "waffle", "sym_ng1", "sym_ng2", "sym_ng3",
+                       "sym_ng4", "sym_ng5", "sym_ng6", "sym_ng7", "sym_ng8", "sym_ng9", "sym_ng10", "sym_ng11",
+                       "sym_ng12", "sym_ng13", "sym_ng14", "sym_ng15", "sym_ng16", "sym_ng17", "sym_bg1", "sym_bg2",
+                       "sym_bg3", "sym_bg4", "sym_bg5", "sym_bg6", "sym_bg7"])
 
 
 def golden():
