@@ -235,7 +235,7 @@ void emit_subflame(std::ostringstream& s, const Flame& f, int si, int blk, const
          "    st[3 * sd] = qx; st[4 * sd] = qy; st[5 * sd] = qw;\n}\n";
 }
 
-// `v_name(px, py[, rng, slot][, params...][, w][, a..f], ox, oy)`.
+// `v_name(px, py[, rng, slot][, params...][, w][, a..f][, state, stride][, hide], ox, oy)`.
 std::string call(const VarDef* v, const Site& c, const char* px = "x", const char* py = "y") {
     std::ostringstream o;
     o << v->fn << "(" << px << ", " << py;
@@ -244,6 +244,7 @@ std::string call(const VarDef* v, const Site& c, const char* px = "x", const cha
     if (v->flags & VF_W) o << ", " << c.w;
     if (v->flags & VF_XF) for (int f = 0; f < 6; ++f) o << ", " << c.xf(f);
     if (v->state > 0) o << ", " << c.st << ", ctx.stride";
+    if (v->flags & VF_HIDE) o << ", ctx.hide";
     o << ", ox, oy)";
     return o.str();
 }
@@ -431,7 +432,11 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     for (size_t j = 0; j < p.normal.size(); ++j) {
         if (p.normal[j]->state > 0) p.st_row[j] = st_rows++;
         p.dc |= (p.normal[j]->flags & VF_DC) != 0;
+        p.hide |= (p.normal[j]->flags & VF_HIDE) != 0;
     }
+    for (const auto* list : {&p.lnk, &p.fin})
+        for (auto& fi : *list)
+            for (const VarDef* v : fi.vars) p.hide |= (v->flags & VF_HIDE) != 0;
     // The deferred plot runs the finals out of walker order, with the draws
     // captured at their static slots: finals that carry state or step a
     // subflame stay inline.
@@ -523,6 +528,7 @@ Plan make_plan(const Flame& f, int rng_mode, int math_mode, int maxx, int thread
     s << "#define FFB_NSTATE " << p.n_state << "\n#define FFB_NINIT " << p.n_init << "\n#define T_ST " << p.t_st
       << "\n#define T_INIT " << p.t_init << "\n";
     if (p.dc) s << "#define FFB_DC 1\n";
+    if (p.hide) s << "#define FFB_HIDE 1\n";
     if (p.speed) s << "#define FFB_SPEED 1\n#define FFB_SPEED_SLOT " << p.speed_slot << "\n#define T_SPEED " << p.t_speed << "\n";
     s << "#define FFB_TABLE_SIZE " << p.table_size << "\n#define FFB_TABLE_VEC4 " << (p.table_size + 3) / 4 << "\n";
     s << "#define T_TOTAL 0\n#define T_CUM " << p.t_cum << "\n#define T_XF " << p.t_xf << "\n#define T_VW " << p.t_vw

@@ -58,6 +58,7 @@ struct Plan {
     std::vector<int> st_row;               // per normal variation: its row of T_ST (-1: stateless)
     int t_st = 0, t_init = 0;
     bool dc = false;
+    bool hide = false;                     // a Feature::CanHide variation anywhere in the flame
     // Speed colour mode: the walker's RGB in state slots speed_slot..+2,
     // the mix factor in the table at t_speed.
     bool speed = false;

@@ -302,6 +302,7 @@ void derive_ripple(const float* u, float* o) {                  // apo_misc13.rs
     const float al = u[2] * 0.01f, pl = u[5] * tp - pi, s = std::fabs(u[6]) < 1e-30f ? 1e-30f : u[6];
     o[0] = u[0] * 5.0f; o[1] = pl; o[2] = s; o[3] = u[1] * pl; o[4] = pl * al; o[5] = (pi - pl) * al;
 }
+void derive_circlecrop(const float* u, float* o) { o[0] = std::min(std::max(u[3], -1.0f), 1.0f); }   // circlecrop_*.rs (init)
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -495,6 +496,7 @@ static const VarDef kRegistry[] = {
     {"spirograph", 236, 2, 9, {"a", "b", "d", "c1", "c2", "tmin", "tmax", "ymin", "ymax"}, {3.0f, 2.0f, 0.0f, 0.0f, 0.0f, -1.0f, 1.0f, -1.0f, 1.0f}, "v_spirograph", 0, 0, nullptr},
     {"lissajous", 237, 2, 7, {"tmin", "tmax", "a", "b", "c", "d", "e"}, {-3.14159265f, 3.14159265f, 3.0f, 2.0f, 0.0f, 0.0f, 0.0f}, "v_lissajous", 0, 0, nullptr},
     {"vogel", 238, 1, 2, {"n", "scale"}, {20.0f, 1.0f}, "v_vogel", 0, 1, derive_vogel},
+    {"bsplit", 240, 0, 2, {"x", "y"}, {0.0f, 0.0f}, "v_bsplit", VF_HIDE, 0, nullptr},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
     {"eclipse", 242, 0, 1, {"shift"}, {0.0f}, "v_eclipse", VF_W, 0, nullptr},
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
@@ -607,6 +609,9 @@ static const VarDef kRegistry[] = {
     {"ripple", 384, 0, 8, {"frequency", "velocity", "amplitude", "centerx", "centery", "phase", "scale", "fixed_dist_calc"}, {2.0f, 1.0f, 0.5f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_ripple", VF_REPLACE, 6, derive_ripple},
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
+    {"pre_circlecrop", 410, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_pre_circlecrop", VF_PRE | VF_W | VF_HIDE, 1, derive_circlecrop},
+    {"post_circlecrop", 411, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_post_circlecrop", VF_POST | VF_W | VF_HIDE, 1, derive_circlecrop},
+    {"circlecrop", 412, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_circlecrop", VF_W | VF_HIDE, 1, derive_circlecrop},
     {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},
     {"heart_wf", 429, 0, 5, {"scale_x", "scale_t", "shift_t", "scale_r_left", "scale_r_right"}, {1.0f, 1.0f, 0.0f, 1.0f, 1.0f}, "v_heart_wf", 0, 0, nullptr},
     {"clifford_js", 435, 0, 4, {"a", "b", "c", "d"}, {-1.4f, 1.6f, 1.0f, 0.7f}, "v_clifford_js", 0, 0, nullptr},

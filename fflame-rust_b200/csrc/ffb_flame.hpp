@@ -33,6 +33,7 @@ enum VarFlags {
     VF_DC = 32,       // Feature::WritesColor: may write the iteration's colour register (vc)
     VF_SUB = 64,      // steps a subflame (subflame_wf, pre_subflame_wf): generated, not a plain body
     VF_REPLACE = 128, // Feature::Replace: its w * V(p) overwrites the normal phase's sum, after the others
+    VF_HIDE = 256,    // Feature::CanHide: the body sets (or clears) the iteration's hide flag
 };
 
 struct VarDef {

@@ -369,6 +369,9 @@ __device__ __forceinline__ void ffb_plot_sample(const float* __restrict__ sm, co
                                                 float cy, float scale, u32& inframe) {
     float fx = x, fy = y;
     ffb_finals(sm, k, fx, fy, rng, ctx);                                    // main_template.wgsl:663-717
+#ifdef FFB_HIDE
+    if (ctx.hide) plot = false;                                             // main_template.wgsl:725-731
+#endif
 #ifdef FFB_SPEED
     // Speed mode plots the walker's own colour (main_template.wgsl:770-772);
     // a key of its lane keeps the warp's splats apart.
@@ -476,6 +479,9 @@ __device__ __forceinline__ void ffb_step(const float* __restrict__ sm, const flo
 #endif
 #if FFB_NLNK > 0
     ffb_linked(sm, k, ax, ay, rng, ctx);                                    // main_template.wgsl:320-360
+#endif
+#ifdef FFB_HIDE
+    if (ctx.hide) { FFB_DEFER_SKIP(rs); return; }                          // main_template.wgsl:389-400: the point reverts
 #endif
     if (!(fabsf(ax) <= 1e32f) || !(fabsf(ay) <= 1e32f)) {                  // main_template.wgsl:449-479
 #if FFB_RNG_MODE == 1

@@ -223,6 +223,10 @@ REGISTRY = {
     "sym_bg5": 565,
     "sym_bg6": 566,
     "sym_bg7": 567,
+    "bsplit": 240,
+    "pre_circlecrop": 410,
+    "post_circlecrop": 411,
+    "circlecrop": 412,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -450,6 +454,12 @@ PARAMS.update({
     "sym_bg5": [("stepx", 0.0), ("stepy", 0.0)],
     "sym_bg6": [("stepx", 0.0), ("stepy", 0.0)],
     "sym_bg7": [("stepx", 0.0), ("stepy", 0.0)],
+})
+PARAMS.update({
+    "bsplit": [("x", 0.0), ("y", 0.0)],
+    "pre_circlecrop": [("radius", 1.0), ("x", 0.0), ("y", 0.0), ("scatter_area", 0.0), ("zero", 1.0)],
+    "post_circlecrop": [("radius", 1.0), ("x", 0.0), ("y", 0.0), ("scatter_area", 0.0), ("zero", 1.0)],
+    "circlecrop": [("radius", 1.0), ("x", 0.0), ("y", 0.0), ("scatter_area", 0.0), ("zero", 1.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -295,9 +295,9 @@ def test_imported_configs_specialize_or_say_why():
                    '<finalxform color="0" linear="1" coefs="1 0 0 1 0 0" post="0.9 0 0 0.9 0 0"/>'))
     n, src = _native.specialize(json.dumps(ok))
     assert n > 0 and src
-    bad = one(flame('<xform weight="1" bwraps="1" bwraps_gain="0.3" coefs="1 0 0 1 0 0" />'))
-    assert bad["flame"]["transforms"][0]["variation_params"] == {"bwraps.gain": f32(0.3)}
-    with pytest.raises(EngineError, match="bwraps"):
+    bad = one(flame('<xform weight="1" synth="1" synth_power="0.3" coefs="1 0 0 1 0 0" />'))
+    assert bad["flame"]["transforms"][0]["variation_params"] == {"synth.power": f32(0.3)}
+    with pytest.raises(EngineError, match="synth"):
         _native.specialize(json.dumps(bad))
     chaos = one(flame('<xform weight="1" linear="1" coefs="1 0 0 1 0 0" chaos="1 0" />'
                       '<xform weight="1" swirl="1" coefs="1 0 0 1 0 0" />'))

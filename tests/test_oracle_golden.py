@@ -244,6 +244,7 @@ WIDER = {
     "npolar": dict.fromkeys(["+0+0", "-0+0", "-x", "neg0y_x"], "branch"),
     "eJulia": {"-x": "zero"},
     "ripple": {"lopsided": "reassociated"},
+    "bsplit": {**dict.fromkeys(["tiny", "normal_min"], "tiny-quotient"), **dict.fromkeys(HUGE_ARGS, "huge")},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -270,7 +271,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "oscilloscope2", "boarders2", "squish", "julian2", "waffle", "sym_ng1", "sym_ng2", "sym_ng3",
                        "sym_ng4", "sym_ng5", "sym_ng6", "sym_ng7", "sym_ng8", "sym_ng9", "sym_ng10", "sym_ng11",
                        "sym_ng12", "sym_ng13", "sym_ng14", "sym_ng15", "sym_ng16", "sym_ng17", "sym_bg1", "sym_bg2",
-                       "sym_bg3", "sym_bg4", "sym_bg5", "sym_bg6", "sym_bg7"])
+                       "sym_bg3", "sym_bg4", "sym_bg5", "sym_bg6", "sym_bg7", "pre_circlecrop", "post_circlecrop",
+                       "circlecrop"])
 
 
 def golden():

@@ -332,6 +332,43 @@ def test_histogram_bit_exact_for_exactly_rounded_variations(renderer, oracle, rn
     assert np.array_equal(cnt, rc)
 
 
+def hide_flame():
+    """Feature::CanHide on the exactly rounded flame: a transform of
+    circlecrop at radius 0 (every point escapes: the iteration is dropped
+    and the point reverts) and a final circlecrop of radius 0.8 (samples
+    outside it are not plotted, the rest pass unchanged)."""
+    cfg = exact_flame()
+    xfs = cfg["flame"]["transforms"]
+    xfs.append(dict(a=0.7, b=0.1, c=-0.2, d=0.6, e=0.1, f=0.1, weight=0.9, color=0.3, variations={"circlecrop": 1.0},
+                    variation_params={"circlecrop.radius": 0.0}))
+    fin = dict(a=1.0, b=0.0, c=0.0, d=1.0, e=0.0, f=0.0, weight=1, color=0.5, variations={"circlecrop": 1.0},
+               variation_params={"circlecrop.radius": 0.8})
+    cfg["flame"]["final_transforms"].append(fin)
+    for x in xfs:
+        x["final_attachments"] = [0, 1]
+    return cfg
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rng_mode", ["pcg", "philox"])
+def test_canhide_drops_iterations_and_samples(renderer, oracle, rng_mode):
+    """main_template.wgsl:389-400, 725-731: a hiding normal transform
+    reverts the point and drops the iteration, a hiding final drops the
+    sample; the orbits stay exact, so the count planes match bit for bit."""
+    cfg = hide_flame()
+    W, H = 96, 64
+    job = dict(iterations=2048 * 300, walkers=2048, rng=rng_mode, iterations_per_thread=256)
+    cnt, rgb, out = renderer.histogram(cfg, W, H, **job)
+    fl = oracle.Flame(cfg, W, H)
+    plotted, inframe, rc, rr = fl.render(2048, 300 + 20, rng=rng_mode, ipt=256, threads=8)
+    assert int(cnt.sum()) == out.inframe_samples == inframe > 0
+    assert np.array_equal(cnt, rc)
+    # the hidden transform and the final's rim take samples away
+    cfg_open = exact_flame()
+    cnt_open, _, _ = renderer.histogram(cfg_open, W, H, **job)
+    assert int(cnt.sum()) < int(cnt_open.sum())
+
+
 @pytest.mark.gpu
 def test_sorted_schedule_with_many_draws(renderer, oracle):
     """20 draw words an iteration (5 blocks of the counter stream): the
