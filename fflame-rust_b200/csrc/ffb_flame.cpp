@@ -329,7 +329,14 @@ static const VarDef kRegistry[] = {
     {"julia", 13, 1, 0, NP, ND, "v_julia", VF_JAC, 0, nullptr},
     {"bent", 14, 0, 0, NP, ND, "v_bent", 0, 0, nullptr},
     {"waves", 15, 0, 0, NP, ND, "v_waves", VF_XF, 0, nullptr},
+    {"zcone", 16, 0, 0, NP, ND, "v_zcone", 0, 0, nullptr},
     {"flatten", 17, 0, 0, NP, ND, "v_flatten", VF_POST, 0, nullptr},
+    {"hemisphere", 18, 0, 0, NP, ND, "v_hemisphere", 0, 0, nullptr},
+    {"pre_rotate_x", 19, 0, 0, NP, ND, "v_pre_rotate_x", VF_PRE, 0, nullptr},
+    {"pre_rotate_y", 20, 0, 0, NP, ND, "v_pre_rotate_y", VF_PRE, 0, nullptr},
+    {"post_rotate_x", 21, 0, 0, NP, ND, "v_post_rotate_x", VF_POST, 0, nullptr},
+    {"post_rotate_y", 22, 0, 0, NP, ND, "v_post_rotate_y", VF_POST, 0, nullptr},
+    {"zscale", 23, 0, 0, NP, ND, "v_zscale", 0, 0, nullptr},
     {"julian", 24, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_julian", 0, 1, derive_julian},
     {"blob", 25, 0, 3, {"high", "low", "waves"}, {1.0f, 1.0f, 6.0f}, "v_blob", 0, 0, nullptr},
     {"eyefish", 26, 0, 0, NP, ND, "v_eyefish", 0, 0, nullptr},
@@ -358,18 +365,26 @@ static const VarDef kRegistry[] = {
      "v_splits", 0, 0, nullptr},
     {"ngon", 50, 0, 4, {"sides", "power", "circle", "corners"}, {5.0f, 3.0f, 1.0f, 2.0f}, "v_ngon", 0, 0, nullptr},
     {"auger", 51, 0, 4, {"freq", "weight", "scale", "sym"}, {1.0f, 0.5f, 0.5f, 0.0f}, "v_auger", 0, 0, nullptr},
+    {"zblur", 52, 0, 0, NP, ND, "v_zblur", 0, 0, nullptr},
+    {"blur3D", 53, 6, 0, NP, ND, "v_blur3D", 0, 0, nullptr},
     {"pre_blur", 54, 7, 0, NP, ND, "v_pre_blur", VF_PRE | VF_W, 0, nullptr},
+    {"pre_zscale", 55, 0, 0, NP, ND, "v_pre_zscale", VF_PRE, 0, nullptr},
+    {"pre_ztranslate", 56, 0, 0, NP, ND, "v_pre_ztranslate", VF_PRE, 0, nullptr},
     {"pre_spherical", 57, 0, 0, NP, ND, "v_pre_spherical", VF_PRE, 0, nullptr},
     {"pre_sinusoidal", 58, 0, 0, NP, ND, "v_pre_sinusoidal", VF_PRE | VF_W, 0, nullptr},
     {"pre_disc", 59, 0, 0, NP, ND, "v_pre_disc", VF_PRE | VF_W, 0, nullptr},
     {"pre_bwraps", 60, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_pre_bwraps", VF_PRE, 5, derive_pre_bwraps},
     {"pre_crop", 61, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_pre_crop", VF_PRE, 0, nullptr},
     {"pre_falloff2", 62, 3, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_pre_falloff2", VF_PRE, 0, nullptr},
+    {"ztranslate", 63, 0, 0, NP, ND, "v_ztranslate", 0, 0, nullptr},
+    {"julia3D", 64, 1, 1, {"power"}, {2.0f}, "v_julia3D", 0, 0, nullptr},
     {"falloff2", 65, 2, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_falloff2", 0, 0, nullptr},
     {"wedge", 66, 0, 4, {"angle", "hole", "count", "swirl"}, {90.0f, 0.0f, 2.0f, 0.0f}, "v_wedge", 0, 2, derive_wedge},
     {"epispiral", 67, 1, 3, {"n", "thickness", "holes"}, {6.0f, 0.0f, 1.0f}, "v_epispiral", 0, 0, nullptr},
     {"bwraps", 68, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_bwraps", 0, 3, derive_bwraps},
     {"juliascope", 69, 1, 2, {"power", "dist"}, {2.0f, 1.0f}, "v_juliascope", 0, 0, nullptr},
+    {"julia3Dz", 71, 0, 1, {"power"}, {2.0f}, "v_julia3Dz", 0, 0, nullptr},
+    {"curl3D", 72, 0, 3, {"cx", "cy", "cz"}, {0.0f, 0.0f, 0.0f}, "v_curl3D", 0, 0, nullptr},
     {"radial_blur", 73, 4, 1, {"angle"}, {0.0f}, "v_radial_blur", VF_W, 2, derive_radial_blur},
     {"blur_circle", 74, 2, 0, NP, ND, "v_blur_circle", 0, 0, nullptr},
     {"blur_zoom", 75, 1, 3, {"length", "x", "y"}, {0.0f, 0.0f, 0.0f}, "v_blur_zoom", 0, 0, nullptr},
@@ -381,6 +396,7 @@ static const VarDef kRegistry[] = {
     {"post_crop", 81, 2, 6, {"left", "top", "right", "bottom", "scatter_area", "zero"}, {-1.0f, -1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_post_crop", VF_POST, 0, nullptr},
     {"post_falloff2", 82, 3, 11, {"scatter", "mindist", "mul_x", "mul_y", "mul_z", "mul_c", "x0", "y0", "z0", "invert", "type"}, {1.0f, 0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_post_falloff2", VF_POST, 0, nullptr},
     {"post_curl", 83, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_post_curl", VF_POST, 0, nullptr},
+    {"post_curl3D", 84, 0, 3, {"cx", "cy", "cz"}, {0.0f, 0.0f, 0.0f}, "v_post_curl3D", VF_POST, 0, nullptr},
     {"cpow", 85, 1, 3, {"r", "i", "power"}, {1.0f, 0.1f, 1.5f}, "v_cpow", 0, 3, derive_cpow},
     {"acoth", 86, 0, 0, NP, ND, "v_acoth", 0, 0, nullptr},
     {"acosh", 87, 1, 0, NP, ND, "v_acosh", 0, 0, nullptr},
@@ -437,22 +453,37 @@ static const VarDef kRegistry[] = {
     {"tile_log", 139, 2, 1, {"spread"}, {1.0f}, "v_tile_log", 0, 0, nullptr},
     {"tancos", 140, 0, 0, NP, ND, "v_tancos", 0, 0, nullptr},
     {"tangent", 141, 0, 0, NP, ND, "v_tangent", 0, 0, nullptr},
+    {"tangent3D", 142, 0, 0, NP, ND, "v_tangent3D", 0, 0, nullptr},
     {"secant2", 143, 0, 0, NP, ND, "v_secant2", 0, 0, nullptr},
     {"cosine", 144, 0, 0, NP, ND, "v_cosine", 0, 0, nullptr},
     {"petal", 145, 0, 0, NP, ND, "v_petal", 0, 0, nullptr},
     {"cardioid", 146, 0, 1, {"a"}, {1.0f}, "v_cardioid", 0, 0, nullptr},
+    {"helix", 147, 0, 2, {"frequency", "width"}, {1.0f, 0.5f}, "v_helix", 0, 0, nullptr},
+    {"helicoid", 148, 0, 1, {"frequency"}, {1.0f}, "v_helicoid", 0, 0, nullptr},
     {"parabola", 149, 2, 2, {"width", "height"}, {1.0f, 0.5f}, "v_parabola", 0, 0, nullptr},
     {"pie", 150, 3, 3, {"slices", "rotation", "thickness"}, {6.0f, 0.0f, 0.5f}, "v_pie", 0, 0, nullptr},
+    {"pie3D", 151, 3, 3, {"slices", "rotation", "thickness"}, {7.0f, 0.0f, 0.5f}, "v_pie3D", 0, 0, nullptr},
     {"butterfly", 152, 0, 0, NP, ND, "v_butterfly", 0, 0, nullptr},
+    {"butterfly3D", 153, 0, 0, NP, ND, "v_butterfly3D", 0, 0, nullptr},
     {"ennepers", 154, 0, 0, NP, ND, "v_ennepers", VF_REPLACE, 0, nullptr},
+    {"pyramid", 155, 0, 0, NP, ND, "v_pyramid", 0, 0, nullptr},
     {"rays2", 156, 0, 0, NP, ND, "v_rays2", VF_REPLACE, 0, nullptr},
     {"rays3", 157, 0, 0, NP, ND, "v_rays3", VF_REPLACE, 0, nullptr},
     {"spiralwing", 158, 0, 0, NP, ND, "v_spiralwing", 0, 0, nullptr},
+    {"whitney_umbrella", 159, 0, 0, NP, ND, "v_whitney_umbrella", 0, 0, nullptr},
     {"chrysanthemum", 160, 1, 0, NP, ND, "v_chrysanthemum", 0, 0, nullptr},
     {"cell", 161, 0, 1, {"size"}, {0.6f}, "v_cell", 0, 0, nullptr},
+    {"ennepers2", 162, 0, 3, {"a", "b", "c"}, {1.0f, 0.3333f, 0.075f}, "v_ennepers2", 0, 0, nullptr},
     {"flower", 163, 1, 2, {"holes", "petals"}, {0.4f, 7.0f}, "v_flower", 0, 0, nullptr},
+    {"spherical3D", 164, 0, 0, NP, ND, "v_spherical3D", 0, 0, nullptr},
+    {"sinusoidal3d", 165, 0, 0, NP, ND, "v_sinusoidal3d", 0, 0, nullptr},
     {"square", 166, 2, 0, NP, ND, "v_square", 0, 0, nullptr},
+    {"square3D", 167, 2, 0, NP, ND, "v_square3D", 0, 0, nullptr},
+    {"disc3d", 168, 0, 1, {"pi"}, {3.14159265358979f}, "v_disc3d", 0, 0, nullptr},
+    {"bubble2", 169, 0, 3, {"x", "y", "z"}, {1.0f, 1.0f, 0.0f}, "v_bubble2", 0, 0, nullptr},
     {"popcorn2", 170, 0, 3, {"x", "y", "c"}, {1.0f, 0.5f, 1.5f}, "v_popcorn2", 0, 0, nullptr},
+    {"splits3D", 171, 0, 3, {"x", "y", "z"}, {0.1f, 0.3f, 0.2f}, "v_splits3D", 0, 0, nullptr},
+    {"waves2_3D", 172, 0, 2, {"freq", "scale"}, {2.0f, 1.0f}, "v_waves2_3D", 0, 0, nullptr},
     {"cpow3", 177, 4, 4, {"r", "d", "divisor", "spread"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cpow3", 0, 6, derive_cpow3},
     {"disc2", 178, 0, 2, {"rot", "twist"}, {2.0f, 0.5f}, "v_disc2", 0, 3, derive_disc2},
     {"target", 179, 0, 3, {"even", "odd", "size"}, {0.0f, 0.0f, 1.0f}, "v_target", 0, 1, derive_target},
@@ -472,6 +503,7 @@ static const VarDef kRegistry[] = {
     {"flipcircle", 200, 0, 0, NP, ND, "v_flipcircle", VF_W, 0, nullptr},
     {"blur_linear", 201, 1, 2, {"length", "angle"}, {1.0f, 0.5f}, "v_blur_linear", 0, 2, derive_blur_linear},
     {"bipolar2", 202, 0, 9, {"shift", "a", "b", "c", "d", "e", "f1", "g1", "h"}, {0.0f, 1.0f, 2.0f, 0.5f, 1.0f, 2.0f, 0.25f, 1.0f, 1.0f}, "v_bipolar2", 0, 0, nullptr},
+    {"blob3D", 203, 0, 3, {"low", "high", "waves"}, {0.3f, 1.2f, 6.0f}, "v_blob3D", 0, 0, nullptr},
     {"glynnia", 205, 1, 0, NP, ND, "v_glynnia", 0, 0, nullptr},
     {"glynnia3", 206, 1, 4, {"rscale", "dscale", "rthresh", "ythresh"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_glynnia3", 0, 0, nullptr},
     {"glynnSim1", 207, 3, 6, {"radius", "radius1", "phi1", "thickness", "pow", "contrast"}, {1.0f, 0.1f, 110.0f, 0.1f, 1.5f, 0.5f}, "v_glynnSim1", 0, 3, derive_glynnSim1},

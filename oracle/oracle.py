@@ -227,6 +227,38 @@ REGISTRY = {
     "pre_circlecrop": 410,
     "post_circlecrop": 411,
     "circlecrop": 412,
+    "zcone": 16,
+    "hemisphere": 18,
+    "pre_rotate_x": 19,
+    "pre_rotate_y": 20,
+    "post_rotate_x": 21,
+    "post_rotate_y": 22,
+    "zscale": 23,
+    "zblur": 52,
+    "blur3D": 53,
+    "pre_zscale": 55,
+    "pre_ztranslate": 56,
+    "ztranslate": 63,
+    "julia3D": 64,
+    "julia3Dz": 71,
+    "curl3D": 72,
+    "post_curl3D": 84,
+    "tangent3D": 142,
+    "helix": 147,
+    "helicoid": 148,
+    "pie3D": 151,
+    "butterfly3D": 153,
+    "pyramid": 155,
+    "whitney_umbrella": 159,
+    "ennepers2": 162,
+    "spherical3D": 164,
+    "sinusoidal3d": 165,
+    "square3D": 167,
+    "disc3d": 168,
+    "bubble2": 169,
+    "splits3D": 171,
+    "waves2_3D": 172,
+    "blob3D": 203,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -460,6 +492,21 @@ PARAMS.update({
     "pre_circlecrop": [("radius", 1.0), ("x", 0.0), ("y", 0.0), ("scatter_area", 0.0), ("zero", 1.0)],
     "post_circlecrop": [("radius", 1.0), ("x", 0.0), ("y", 0.0), ("scatter_area", 0.0), ("zero", 1.0)],
     "circlecrop": [("radius", 1.0), ("x", 0.0), ("y", 0.0), ("scatter_area", 0.0), ("zero", 1.0)],
+})
+PARAMS.update({
+    "julia3D": [("power", 2.0)],
+    "julia3Dz": [("power", 2.0)],
+    "curl3D": [("cx", 0.0), ("cy", 0.0), ("cz", 0.0)],
+    "post_curl3D": [("cx", 0.0), ("cy", 0.0), ("cz", 0.0)],
+    "helix": [("frequency", 1.0), ("width", 0.5)],
+    "helicoid": [("frequency", 1.0)],
+    "pie3D": [("slices", 7.0), ("rotation", 0.0), ("thickness", 0.5)],
+    "ennepers2": [("a", 1.0), ("b", 0.3333), ("c", 0.075)],
+    "disc3d": [("pi", 3.14159265358979)],
+    "bubble2": [("x", 1.0), ("y", 1.0), ("z", 0.0)],
+    "splits3D": [("x", 0.1), ("y", 0.3), ("z", 0.2)],
+    "waves2_3D": [("freq", 2.0), ("scale", 1.0)],
+    "blob3D": [("low", 0.3), ("high", 1.2), ("waves", 6.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -68,13 +68,16 @@ HUGE_ARGS = ["large", "near_threshold", "past_threshold", "lopsided"]
 # Where the bipolar series' sigma is f32(pi) (sin(sigma) -4.4e-8 here, 0 on
 # the reference) and the elliptic series' nu is f32(pi)/2 (cos(nu) -4.4e-8).
 BIPOLAR_PI = ["+0+0", "+0-0", "-0+0", "-0-0", "+x", "-x", "unit", "tiny", "normal_min", "subnormal", "y_neg0x"]
+# The inputs whose signed zeros a Pre or Post variation's linear carrier
+# keeps on the reference (its compiler folded 0 + 1 * p into p).
+CARRIER_ZEROS = ["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"]
 # The wf curves' angle atan2(x, y) at multiples of f32(pi)/2.
 WF_CURVE = ["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "lopsided", "y_neg0x"]
 ELLIPTIC_PI2 = ["+0+0", "+0-0", "-0+0", "-0-0", "+y", "-y", "tiny", "normal_min", "subnormal", "neg0y_x"]
 WIDER = {
     "heart": dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero"),
     "diamond": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"),
-    "flatten": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
+    "flatten": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
     "julian": {"-x": "zero", "y_neg0x": "zero", "lopsided": "inf*0"},
     "blob": {**dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero"), "lopsided": "inf*0"},
     "fan2": {**dict.fromkeys(["+x", "+y", "-y", "unit", "y_neg0x", "neg0y_x"], "zero"), "lopsided": "inf*0"},
@@ -152,7 +155,7 @@ WIDER = {
     # compiler folded that carrier's 0 + 1 * p to p, keeping its -0.
     "pre_disc": {**dict.fromkeys(["-0+0", "-0-0", "+y", "neg0y_x"], "signed-zero"),
                  **dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero")},
-    "pre_sinusoidal": {**dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
+    "pre_sinusoidal": {**dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
                        **dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
     "pre_spherical": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "large", "near_threshold", "past_threshold",
                                     "y_neg0x", "neg0y_x"], "signed-zero"),
@@ -207,8 +210,8 @@ WIDER = {
     "atan2_spirals": {"-x": "zero"},
     "eMotion": {**dict.fromkeys(ELLIPTIC_PI2, "zero"), **dict.fromkeys(HUGE_ARGS, "inf*0")},
     "mask": {"pi_e": "zero"},
-    "pre_crop": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
-    "post_crop": dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"),
+    "pre_crop": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "post_crop": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
     "mobiusN": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
     "sphericalN": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
     "murl2": {"-x": "zero"},
@@ -230,8 +233,8 @@ WIDER = {
     "murl": {"-x": "zero"},
     "shredrad": {**dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"), "lopsided": "inf*0"},
     "xheart": {"normal_min": "zero"},
-    "pre_bwraps": {**dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"), "lopsided": "zero"},
-    "post_bwraps": {**dict.fromkeys(["+0-0", "-0+0", "-0-0", "subnormal", "y_neg0x", "neg0y_x"], "signed-zero"), "lopsided": "zero"},
+    "pre_bwraps": {**dict.fromkeys(CARRIER_ZEROS, "signed-zero"), "lopsided": "zero"},
+    "post_bwraps": {**dict.fromkeys(CARRIER_ZEROS, "signed-zero"), "lopsided": "zero"},
     "target_sp": {**dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"), "lopsided": "inf*0"},
     "cpow3": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"),
     "phoenix_julia": dict.fromkeys(["-0+0", "-0-0"], "zero"),
@@ -245,6 +248,20 @@ WIDER = {
     "eJulia": {"-x": "zero"},
     "ripple": {"lopsided": "reassociated"},
     "bsplit": {**dict.fromkeys(["tiny", "normal_min"], "tiny-quotient"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "pre_rotate_x": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "pre_rotate_y": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "post_rotate_x": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "post_rotate_y": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "pre_zscale": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "pre_ztranslate": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "julia3D": dict.fromkeys(["-x", "unit"], "zero"),
+    "post_curl3D": dict.fromkeys(CARRIER_ZEROS, "signed-zero"),
+    "tangent3D": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "sinusoidal3d": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "disc3d": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "tiny",
+                             "normal_min", "subnormal", "y_neg0x"], "zero"),
+    "waves2_3D": {"tiny": "zero"},
+    "blob3D": {**dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero"), "lopsided": "inf*0"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -272,7 +289,9 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "sym_ng4", "sym_ng5", "sym_ng6", "sym_ng7", "sym_ng8", "sym_ng9", "sym_ng10", "sym_ng11",
                        "sym_ng12", "sym_ng13", "sym_ng14", "sym_ng15", "sym_ng16", "sym_ng17", "sym_bg1", "sym_bg2",
                        "sym_bg3", "sym_bg4", "sym_bg5", "sym_bg6", "sym_bg7", "pre_circlecrop", "post_circlecrop",
-                       "circlecrop"])
+                       "circlecrop", "zcone", "hemisphere", "zscale", "zblur", "blur3D", "ztranslate", "julia3Dz",
+                       "curl3D", "helix", "helicoid", "pie3D", "butterfly3D", "pyramid", "whitney_umbrella",
+                       "ennepers2", "spherical3D", "square3D", "bubble2", "splits3D"])
 
 
 def golden():
