@@ -516,6 +516,7 @@ static const VarDef kRegistry[] = {
     {"apollony", 214, 1, 0, NP, ND, "v_apollony", 0, 0, nullptr},
     {"target_sp", 216, 0, 4, {"twist", "n_of_sp", "size", "tightness"}, {0.0f, 1.0f, 1.0f, 0.5f}, "v_target_sp", VF_W, 3, derive_target_sp},
     {"loonie3", 217, 0, 0, NP, ND, "v_loonie3", VF_W, 0, nullptr},
+    {"loonie_3D", 218, 0, 0, NP, ND, "v_loonie_3D", VF_W, 0, nullptr},
     {"sigmoid", 219, 0, 2, {"shiftx", "shifty"}, {1.0f, 1.0f}, "v_sigmoid", VF_W, 0, nullptr},
     {"blocky", 220, 0, 3, {"x", "y", "mp"}, {1.0f, 1.0f, 4.0f}, "v_blocky", VF_W, 0, nullptr},
     {"pre_curl", 221, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_pre_curl", VF_PRE | VF_W, 0, nullptr},
@@ -524,6 +525,7 @@ static const VarDef kRegistry[] = {
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"boarders2", 230, 1, 3, {"c", "left", "right"}, {0.4f, 0.65f, 0.35f}, "v_boarders2", 0, 3, derive_boarders2},
     {"kaleidoscope", 233, 0, 5, {"pull", "rotate", "line_up", "x", "y"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_kaleidoscope", VF_W, 0, nullptr},
+    {"taurus", 234, 0, 4, {"r", "n", "inv", "sor"}, {3.0f, 5.0f, 1.5f, 1.0f}, "v_taurus", 0, 0, nullptr},
     {"hole2", 235, 0, 6, {"a", "b", "c", "d", "inside", "shape"}, {1.0f, 2.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_hole2", 0, 0, nullptr},
     {"spirograph", 236, 2, 9, {"a", "b", "d", "c1", "c2", "tmin", "tmax", "ymin", "ymax"}, {3.0f, 2.0f, 0.0f, 0.0f, 0.0f, -1.0f, 1.0f, -1.0f, 1.0f}, "v_spirograph", 0, 0, nullptr},
     {"lissajous", 237, 2, 7, {"tmin", "tmax", "a", "b", "c", "d", "e"}, {-3.14159265f, 3.14159265f, 3.0f, 2.0f, 0.0f, 0.0f, 0.0f}, "v_lissajous", 0, 0, nullptr},
@@ -567,6 +569,7 @@ static const VarDef kRegistry[] = {
     {"collideoscope", 280, 0, 2, {"a", "num"}, {0.2f, 1.0f}, "v_collideoscope", 0, 0, nullptr},
     {"bent2", 281, 0, 2, {"x", "y"}, {1.0f, 1.0f}, "v_bent2", 0, 0, nullptr},
     {"mcarpet", 282, 0, 4, {"x", "y", "twist", "tilt"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_mcarpet", 0, 0, nullptr},
+    {"linearT3D", 283, 0, 3, {"powX", "powY", "powZ"}, {1.2f, 1.2f, 1.2f}, "v_linearT3D", 0, 0, nullptr},
     {"oscilloscope", 284, 0, 4, {"separation", "frequency", "amplitude", "damping"}, {1.0f, 3.14159265f, 1.0f, 0.0f}, "v_oscilloscope", 0, 1, derive_oscilloscope},
     {"fibonacci2", 285, 0, 2, {"sc", "sc2"}, {1.0f, 1.0f}, "v_fibonacci2", 0, 0, nullptr},
     {"oscilloscope2", 286, 0, 6, {"separation", "frequencyx", "frequencyy", "amplitude", "perturbation", "damping"}, {1.0f, 3.14159265f, 3.14159265f, 1.0f, 1.0f, 0.0f}, "v_oscilloscope2", 0, 2, derive_oscilloscope2},
@@ -577,6 +580,7 @@ static const VarDef kRegistry[] = {
     {"projective", 291, 0, 9, {"a", "b", "c", "a1", "b1", "c1", "a2", "b2", "c2"}, {0.0f, 0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_projective", 0, 0, nullptr},
     {"tqmirror", 292, 0, 9, {"a", "b", "c", "d", "e", "f", "g", "h", "type"}, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_tqmirror", VF_W, 0, nullptr},
     {"anamorphcyl", 296, 0, 3, {"a", "b", "k"}, {1.0f, 1.3f, 3.0f}, "v_anamorphcyl", VF_REPLACE, 0, nullptr},
+    {"svf", 297, 0, 1, {"n"}, {2.0f}, "v_svf", 0, 0, nullptr},
     {"shredlin", 298, 0, 4, {"xdistance", "xwidth", "ydistance", "ywidth"}, {1.0f, 0.5f, 1.0f, 0.5f}, "v_shredlin", VF_REPLACE, 0, nullptr},
     {"shredrad", 299, 0, 2, {"n", "width"}, {4.0f, 0.5f}, "v_shredrad", 0, 1, derive_shredrad},
     {"xheart", 300, 0, 2, {"angle", "ratio"}, {0.0f, 0.0f}, "v_xheart", 0, 3, derive_xheart},
@@ -592,6 +596,7 @@ static const VarDef kRegistry[] = {
     {"arch", 312, 1, 0, NP, ND, "v_arch", VF_W, 0, nullptr},
     {"bi_linear", 313, 0, 0, NP, ND, "v_bi_linear", 0, 0, nullptr},
     {"blade", 314, 1, 0, NP, ND, "v_blade", VF_W, 0, nullptr},
+    {"blade3D", 315, 1, 0, NP, ND, "v_blade3D", VF_W, 0, nullptr},
     {"squarize", 316, 0, 0, NP, ND, "v_squarize", 0, 0, nullptr},
     {"squish", 317, 1, 1, {"power"}, {2.0f}, "v_squish", 0, 1, derive_squish},
     {"twoface", 318, 0, 0, NP, ND, "v_twoface", VF_W, 0, nullptr},
@@ -603,6 +608,7 @@ static const VarDef kRegistry[] = {
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
     {"roundspher", 326, 0, 0, NP, ND, "v_roundspher", VF_W, 0, nullptr},
     {"checks", 330, 2, 4, {"x", "y", "size", "rnd"}, {0.5f, 0.5f, 0.5f, 0.0f}, "v_checks", 0, 1, derive_checks},
+    {"cone", 331, 1, 9, {"radius1", "radius2", "size1", "size2", "ywave", "xwave", "height", "warp", "weight"}, {0.5f, 1.0f, 0.5f, 2.0f, 1.0f, 1.0f, 1.0f, 1.0f, 2.0f}, "v_cone", 0, 0, nullptr},
     {"erf", 332, 0, 0, NP, ND, "v_erf", 0, 0, nullptr},
     {"d_spherical", 334, 1, 1, {"d_spher_weight"}, {0.5f}, "v_d_spherical", 0, 0, nullptr},
     {"dustpoint", 335, 2, 0, NP, ND, "v_dustpoint", 0, 0, nullptr},
@@ -615,8 +621,17 @@ static const VarDef kRegistry[] = {
     {"funnel", 343, 0, 1, {"effect"}, {8.0f}, "v_funnel", 0, 0, nullptr},
     {"invpolar", 344, 0, 0, NP, ND, "v_invpolar", 0, 0, nullptr},
     {"perspective", 345, 0, 2, {"angle", "dist"}, {0.62f, 2.2f}, "v_perspective", 0, 2, derive_perspective},
+    {"line", 346, 1, 2, {"delta", "phi"}, {0.0f, 0.0f}, "v_line", VF_W, 0, nullptr},
     {"holesq", 347, 0, 0, NP, ND, "v_holesq", VF_W, 0, nullptr},
+    {"inflateZ_1", 348, 0, 0, NP, ND, "v_inflateZ_1", 0, 0, nullptr},
+    {"inflateZ_2", 349, 0, 0, NP, ND, "v_inflateZ_2", 0, 0, nullptr},
+    {"inflateZ_3", 350, 0, 0, NP, ND, "v_inflateZ_3", 0, 0, nullptr},
+    {"inflateZ_4", 351, 1, 0, NP, ND, "v_inflateZ_4", 0, 0, nullptr},
+    {"inflateZ_5", 352, 0, 0, NP, ND, "v_inflateZ_5", 0, 0, nullptr},
+    {"inflateZ_6", 353, 0, 0, NP, ND, "v_inflateZ_6", 0, 0, nullptr},
     {"sintrange", 354, 0, 1, {"w"}, {1.0f}, "v_sintrange", VF_REPLACE, 0, nullptr},
+    {"foci_3D", 355, 0, 0, NP, ND, "v_foci_3D", 0, 0, nullptr},
+    {"estiq", 357, 0, 0, NP, ND, "v_estiq", 0, 0, nullptr},
     {"fdisc", 358, 0, 8, {"ashift", "rshift", "xshift", "yshift", "term1", "term2", "term3", "term4"}, {1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_fdisc", 0, 0, nullptr},
     {"bTransform", 359, 1, 4, {"rotate", "power", "move", "split"}, {0.0f, 1.0f, 0.0f, 0.0f}, "v_bTransform", 0, 0, nullptr},
     {"npolar", 360, 1, 2, {"parity", "n"}, {0.0f, 1.0f}, "v_npolar", VF_W, 4, derive_npolar},
@@ -629,9 +644,11 @@ static const VarDef kRegistry[] = {
     {"eMotion", 367, 0, 2, {"move", "rotate"}, {0.0f, 0.0f}, "v_eMotion", 0, 0, nullptr},
     {"julian2", 369, 1, 8, {"power", "dist", "a", "b", "c", "d", "e", "f"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_julian2", 0, 2, derive_julian2},
     {"mask", 370, 0, 5, {"xshift", "yshift", "ushift", "xscale", "yscale"}, {0.0f, 0.0f, 1.0f, 1.0f, 1.0f}, "v_mask", 0, 0, nullptr},
+    {"ovoid3d", 371, 0, 3, {"x", "y", "z"}, {1.0f, 1.0f, 1.0f}, "v_ovoid3d", 0, 0, nullptr},
     {"murl2", 372, 0, 2, {"c", "power"}, {0.1f, 3.0f}, "v_murl2", VF_W, 0, nullptr},
     {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
     {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
+    {"sph3D", 376, 0, 3, {"x", "y", "z"}, {1.0f, 1.0f, 1.0f}, "v_sph3D", 0, 0, nullptr},
     {"invsquircular", 377, 0, 0, NP, ND, "v_invsquircular", VF_W, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
     {"rippled", 380, 0, 0, NP, ND, "v_rippled", 0, 0, nullptr},
@@ -639,13 +656,20 @@ static const VarDef kRegistry[] = {
     {"stripfit", 382, 0, 1, {"dx"}, {1.0f}, "v_stripfit", VF_W, 0, nullptr},
     {"q_ode", 383, 0, 12, {"q_ode01", "q_ode02", "q_ode03", "q_ode04", "q_ode05", "q_ode06", "q_ode07", "q_ode08", "q_ode09", "q_ode10", "q_ode11", "q_ode12"}, {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_q_ode", VF_W, 0, nullptr},
     {"ripple", 384, 0, 8, {"frequency", "velocity", "amplitude", "centerx", "centery", "phase", "scale", "fixed_dist_calc"}, {2.0f, 1.0f, 0.5f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_ripple", VF_REPLACE, 6, derive_ripple},
+    {"pre_spin_z", 386, 0, 0, NP, ND, "v_pre_spin_z", VF_PRE | VF_W, 0, nullptr},
+    {"post_spin_z", 387, 0, 0, NP, ND, "v_post_spin_z", VF_POST | VF_W, 0, nullptr},
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
+    {"pre_disc3d", 389, 0, 1, {"pi"}, {3.141592653589793f}, "v_pre_disc3d", VF_PRE | VF_W, 0, nullptr},
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
+    {"pre_sinusoidal3d", 393, 0, 0, NP, ND, "v_pre_sinusoidal3d", VF_PRE | VF_W, 0, nullptr},
+    {"pre_blur3D", 394, 8, 0, NP, ND, "v_pre_blur3D", VF_PRE | VF_W, 0, nullptr},
     {"pre_circlecrop", 410, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_pre_circlecrop", VF_PRE | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"post_circlecrop", 411, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_post_circlecrop", VF_POST | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"circlecrop", 412, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_circlecrop", VF_W | VF_HIDE, 1, derive_circlecrop},
+    {"extrude", 415, 1, 1, {"root_face"}, {0.5f}, "v_extrude", 0, 0, nullptr},
     {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},
     {"heart_wf", 429, 0, 5, {"scale_x", "scale_t", "shift_t", "scale_r_left", "scale_r_right"}, {1.0f, 1.0f, 0.0f, 1.0f, 1.0f}, "v_heart_wf", 0, 0, nullptr},
+    {"post_ztranslate_wf", 430, 0, 0, NP, ND, "v_post_ztranslate_wf", VF_POST, 0, nullptr},
     {"clifford_js", 435, 0, 4, {"a", "b", "c", "d"}, {-1.4f, 1.6f, 1.0f, 0.7f}, "v_clifford_js", 0, 0, nullptr},
     {"svensson_js", 436, 0, 4, {"a", "b", "c", "d"}, {1.4f, 1.56f, 1.4f, -6.56f}, "v_svensson_js", VF_REPLACE, 0, nullptr},
     {"sattractor_js", 437, 2, 1, {"m"}, {10.0f}, "v_sattractor_js", 0, 0, nullptr},
@@ -658,8 +682,11 @@ static const VarDef kRegistry[] = {
     {"epispiral_wf", 446, 0, 1, {"waves"}, {4.0f}, "v_epispiral_wf", 0, 0, nullptr},
     {"cloverleaf_wf", 447, 1, 1, {"filled"}, {1.0f}, "v_cloverleaf_wf", 0, 0, nullptr},
     {"rose_wf", 448, 1, 3, {"amp", "waves", "filled"}, {0.5f, 4.0f, 0.0f}, "v_rose_wf", 0, 0, nullptr},
+    {"bubble_wf", 449, 0, 0, NP, ND, "v_bubble_wf", 0, 0, nullptr},
+    {"dinis_surface_wf", 455, 0, 2, {"a", "b"}, {0.8f, 0.2f}, "v_dinis_surface_wf", 0, 0, nullptr},
     {"apocarpet_js", 458, 1, 0, NP, ND, "v_apocarpet_js", 0, 0, nullptr},
     {"siercarpet_js", 473, 1, 1, {"m"}, {3.0f}, "v_siercarpet_js", 0, 0, nullptr},
+    {"popcorn2_3D", 474, 0, 4, {"popcorn2_3D_x", "popcorn2_3D_y", "popcorn2_3D_z", "popcorn2_3D_c"}, {0.1f, 0.1f, 0.1f, 3.0f}, "v_popcorn2_3D", 0, 0, nullptr},
     {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},
      "v_klein_group", VF_W, 16, derive_klein_group, 1, 1},
     {"subflame_wf", 502, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},
@@ -691,7 +718,9 @@ static const VarDef kRegistry[] = {
     {"sym_bg4", 564, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg4", 0, 0, nullptr},
     {"sym_bg5", 565, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg5", 0, 0, nullptr},
     {"sym_bg6", 566, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg6", 0, 0, nullptr},
-    {"sym_bg7", 567, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg7", 0, 0, nullptr},};
+    {"sym_bg7", 567, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg7", 0, 0, nullptr},
+    {"solid_sphere", 605, 2, 5, {"radius", "thickness", "cx", "cy", "cz"}, {1.0f, 0.1f, 0.0f, 0.0f, 0.0f}, "v_solid_sphere", 0, 0, nullptr},
+    {"matrix3D", 643, 0, 12, {"xx", "xy", "xz", "yx", "yy", "yz", "zx", "zy", "zz", "tx", "ty", "tz"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_matrix3D", 0, 0, nullptr},};
 #undef NP
 #undef ND
 

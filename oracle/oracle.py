@@ -259,6 +259,35 @@ REGISTRY = {
     "splits3D": 171,
     "waves2_3D": 172,
     "blob3D": 203,
+    "loonie_3D": 218,
+    "taurus": 234,
+    "linearT3D": 283,
+    "svf": 297,
+    "blade3D": 315,
+    "cone": 331,
+    "line": 346,
+    "inflateZ_1": 348,
+    "inflateZ_2": 349,
+    "inflateZ_3": 350,
+    "inflateZ_4": 351,
+    "inflateZ_5": 352,
+    "inflateZ_6": 353,
+    "foci_3D": 355,
+    "estiq": 357,
+    "ovoid3d": 371,
+    "sph3D": 376,
+    "pre_spin_z": 386,
+    "post_spin_z": 387,
+    "pre_disc3d": 389,
+    "pre_sinusoidal3d": 393,
+    "pre_blur3D": 394,
+    "extrude": 415,
+    "post_ztranslate_wf": 430,
+    "bubble_wf": 449,
+    "dinis_surface_wf": 455,
+    "popcorn2_3D": 474,
+    "solid_sphere": 605,
+    "matrix3D": 643,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -507,6 +536,21 @@ PARAMS.update({
     "splits3D": [("x", 0.1), ("y", 0.3), ("z", 0.2)],
     "waves2_3D": [("freq", 2.0), ("scale", 1.0)],
     "blob3D": [("low", 0.3), ("high", 1.2), ("waves", 6.0)],
+})
+PARAMS.update({
+    "taurus": [("r", 3.0), ("n", 5.0), ("inv", 1.5), ("sor", 1.0)],
+    "linearT3D": [("powX", 1.2), ("powY", 1.2), ("powZ", 1.2)],
+    "svf": [("n", 2.0)],
+    "cone": [("radius1", 0.5), ("radius2", 1.0), ("size1", 0.5), ("size2", 2.0), ("ywave", 1.0), ("xwave", 1.0), ("height", 1.0), ("warp", 1.0), ("weight", 2.0)],
+    "line": [("delta", 0.0), ("phi", 0.0)],
+    "ovoid3d": [("x", 1.0), ("y", 1.0), ("z", 1.0)],
+    "sph3D": [("x", 1.0), ("y", 1.0), ("z", 1.0)],
+    "pre_disc3d": [("pi", 3.141592653589793)],
+    "extrude": [("root_face", 0.5)],
+    "dinis_surface_wf": [("a", 0.8), ("b", 0.2)],
+    "popcorn2_3D": [("popcorn2_3D_x", 0.1), ("popcorn2_3D_y", 0.1), ("popcorn2_3D_z", 0.1), ("popcorn2_3D_c", 3.0)],
+    "solid_sphere": [("radius", 1.0), ("thickness", 0.1), ("cx", 0.0), ("cy", 0.0), ("cz", 0.0)],
+    "matrix3D": [("xx", 1.0), ("xy", 0.0), ("xz", 0.0), ("yx", 0.0), ("yy", 1.0), ("yz", 0.0), ("zx", 0.0), ("zy", 0.0), ("zz", 1.0), ("tx", 0.0), ("ty", 0.0), ("tz", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -262,6 +262,21 @@ WIDER = {
                              "normal_min", "subnormal", "y_neg0x"], "zero"),
     "waves2_3D": {"tiny": "zero"},
     "blob3D": {**dict.fromkeys(["+x", "-x", "-y", "unit", "y_neg0x"], "zero"), "lopsided": "inf*0"},
+    "taurus": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "svf": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "cone": dict.fromkeys(["-0+0", "-0-0", "-x", "y_neg0x"], "zero"),
+    "foci_3D": dict.fromkeys(["tiny", "normal_min"], "zero"),
+    "estiq": {**dict.fromkeys(["tiny", "normal_min"], "zero"),
+        **dict.fromkeys(["large", "past_threshold", "lopsided"], "inf*0"), "near_threshold": "huge"},
+    "pre_spin_z": dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "lopsided", "y_neg0x", "neg0y_x"], "zero"),
+    "post_spin_z": {**dict.fromkeys(["+0+0", "+0-0", "-0+0", "-0-0", "subnormal"], "signed-zero"),
+        **dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "lopsided", "y_neg0x", "neg0y_x"], "zero")},
+    "pre_disc3d": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit",
+                                 "tiny", "normal_min", "subnormal", "y_neg0x"], "zero"),
+    "pre_sinusoidal3d": {**dict.fromkeys(["pi_e", "tiny", "normal_min"], "zero"), **dict.fromkeys(HUGE_ARGS, "huge")},
+    "dinis_surface_wf": {**dict.fromkeys(["pi_e", "tiny", "lopsided"], "zero"),
+        **dict.fromkeys(["large", "near_threshold", "past_threshold"], "huge")},
+    "popcorn2_3D": {"lopsided": "huge"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -291,7 +306,9 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "sym_bg3", "sym_bg4", "sym_bg5", "sym_bg6", "sym_bg7", "pre_circlecrop", "post_circlecrop",
                        "circlecrop", "zcone", "hemisphere", "zscale", "zblur", "blur3D", "ztranslate", "julia3Dz",
                        "curl3D", "helix", "helicoid", "pie3D", "butterfly3D", "pyramid", "whitney_umbrella",
-                       "ennepers2", "spherical3D", "square3D", "bubble2", "splits3D"])
+                       "ennepers2", "spherical3D", "square3D", "bubble2", "splits3D", "loonie_3D", "blade3D", "line",
+                       "inflateZ_1", "inflateZ_2", "inflateZ_3", "inflateZ_4", "inflateZ_5", "inflateZ_6", "ovoid3d",
+                       "sph3D", "pre_blur3D", "extrude", "post_ztranslate_wf", "bubble_wf", "solid_sphere", "matrix3D"])
 
 
 def golden():
