@@ -514,6 +514,7 @@ static const VarDef kRegistry[] = {
     {"super_shape", 212, 1, 6, {"rnd", "m", "n1", "n2", "n3", "holes"}, {3.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_super_shape", 0, 0, nullptr},
     {"henon", 213, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_henon", 0, 0, nullptr},
     {"apollony", 214, 1, 0, NP, ND, "v_apollony", 0, 0, nullptr},
+    {"onion", 215, 0, 2, {"centre_x", "centre_y"}, {0.0f, 0.0f}, "v_onion", VF_W, 0, nullptr},
     {"target_sp", 216, 0, 4, {"twist", "n_of_sp", "size", "tightness"}, {0.0f, 1.0f, 1.0f, 0.5f}, "v_target_sp", VF_W, 3, derive_target_sp},
     {"loonie3", 217, 0, 0, NP, ND, "v_loonie3", VF_W, 0, nullptr},
     {"loonie_3D", 218, 0, 0, NP, ND, "v_loonie_3D", VF_W, 0, nullptr},
@@ -544,6 +545,7 @@ static const VarDef kRegistry[] = {
     {"sphericalN", 253, 1, 2, {"power", "dist"}, {1.0f, 1.0f}, "v_sphericalN", 0, 0, nullptr},
     {"spligon", 254, 0, 2, {"sides", "i"}, {3.0f, 1.0f}, "v_spligon", 0, 3, derive_spligon},
     {"tile_hlp", 255, 1, 1, {"width"}, {1.0f}, "v_tile_hlp", VF_W, 0, nullptr},
+    {"ho", 256, 0, 3, {"xpow", "ypow", "zpow"}, {3.0f, 3.0f, 3.0f}, "v_ho", 0, 0, nullptr},
     {"chunk", 257, 0, 7, {"a", "b", "c", "d", "e", "f", "mode"}, {1.0f, 0.0f, 1.0f, 0.0f, 0.0f, -1.0f, 0.0f}, "v_chunk", VF_W, 0, nullptr},
     {"pTransform", 258, 0, 5, {"rotate", "power", "move", "split", "use_log"}, {0.0f, 1.0f, 0.0f, 0.0f, 1.0f}, "v_pTransform", 0, 0, nullptr},
     {"rational3", 259, 0, 8, {"a", "b", "c", "d", "e", "f", "g", "h"}, {0.5f, 0.0f, 0.0f, 1.0f, 0.0f, 1.0f, 0.0f, 1.0f}, "v_rational3", 0, 0, nullptr},
@@ -561,6 +563,7 @@ static const VarDef kRegistry[] = {
     {"eRotate", 271, 0, 1, {"rotate"}, {0.0f}, "v_eRotate", 0, 0, nullptr},
     {"corners", 272, 0, 9, {"xwidth", "ywidth", "multx", "multy", "xpower", "ypower", "xypower", "logmode", "log_base"}, {1.0f, 1.0f, 1.0f, 1.0f, 0.75f, 0.75f, 0.0f, 0.0f, 2.71828f}, "v_corners", VF_W, 0, nullptr},
     {"modulus", 273, 0, 2, {"x", "y"}, {0.2f, 0.5f}, "v_modulus", 0, 2, derive_modulus},
+    {"octagon", 274, 0, 3, {"x", "y", "z"}, {0.0f, 0.0f, 0.0f}, "v_octagon", 0, 0, nullptr},
     {"circus", 275, 0, 1, {"scale"}, {1.0f}, "v_circus", 0, 1, derive_circus},
     {"circlize", 276, 0, 1, {"hole"}, {0.4f}, "v_circlize", VF_W, 0, nullptr},
     {"circlize2", 277, 0, 1, {"hole"}, {0.0f}, "v_circlize2", 0, 0, nullptr},
@@ -602,6 +605,7 @@ static const VarDef kRegistry[] = {
     {"twoface", 318, 0, 0, NP, ND, "v_twoface", VF_W, 0, nullptr},
     {"twintrian", 319, 1, 0, NP, ND, "v_twintrian", VF_W, 0, nullptr},
     {"unpolar", 320, 0, 0, NP, ND, "v_unpolar", VF_W, 0, nullptr},
+    {"xerf", 321, 0, 0, NP, ND, "v_xerf", 0, 0, nullptr},
     {"inverted_julia", 322, 1, 9, {"power", "y2_mult", "a2x_mult", "a2y_mult", "a2y_add", "cos_mult", "y_mult", "center", "x2y2_add"}, {0.25f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 3.14f, 0.0f}, "v_inverted_julia", 0, 0, nullptr},
     {"idisc", 323, 0, 0, NP, ND, "v_idisc", VF_W, 0, nullptr},
     {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
@@ -610,6 +614,7 @@ static const VarDef kRegistry[] = {
     {"checks", 330, 2, 4, {"x", "y", "size", "rnd"}, {0.5f, 0.5f, 0.5f, 0.0f}, "v_checks", 0, 1, derive_checks},
     {"cone", 331, 1, 9, {"radius1", "radius2", "size1", "size2", "ywave", "xwave", "height", "warp", "weight"}, {0.5f, 1.0f, 0.5f, 2.0f, 1.0f, 1.0f, 1.0f, 1.0f, 2.0f}, "v_cone", 0, 0, nullptr},
     {"erf", 332, 0, 0, NP, ND, "v_erf", 0, 0, nullptr},
+    {"erf3D", 333, 0, 0, NP, ND, "v_erf3D", 0, 0, nullptr},
     {"d_spherical", 334, 1, 1, {"d_spher_weight"}, {0.5f}, "v_d_spherical", 0, 0, nullptr},
     {"dustpoint", 335, 2, 0, NP, ND, "v_dustpoint", 0, 0, nullptr},
     {"deltaA", 336, 0, 0, NP, ND, "v_deltaA", VF_W, 0, nullptr},
@@ -642,6 +647,7 @@ static const VarDef kRegistry[] = {
     {"gridout2", 365, 0, 4, {"a", "b", "c", "d"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_gridout2", 0, 0, nullptr},
     {"eJulia", 366, 1, 1, {"power"}, {2.0f}, "v_eJulia", 0, 1, derive_eJulia},
     {"eMotion", 367, 0, 2, {"move", "rotate"}, {0.0f, 0.0f}, "v_eMotion", 0, 0, nullptr},
+    {"flower_db", 368, 0, 7, {"petals", "petal_split", "petal_spread", "stem_thickness", "stem_length", "petal_fold_strength", "petal_fold_radius"}, {6.0f, 0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f}, "v_flower_db", VF_W, 0, nullptr},
     {"julian2", 369, 1, 8, {"power", "dist", "a", "b", "c", "d", "e", "f"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_julian2", 0, 2, derive_julian2},
     {"mask", 370, 0, 5, {"xshift", "yshift", "ushift", "xscale", "yscale"}, {0.0f, 0.0f, 1.0f, 1.0f, 1.0f}, "v_mask", 0, 0, nullptr},
     {"ovoid3d", 371, 0, 3, {"x", "y", "z"}, {1.0f, 1.0f, 1.0f}, "v_ovoid3d", 0, 0, nullptr},
@@ -650,6 +656,7 @@ static const VarDef kRegistry[] = {
     {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
     {"sph3D", 376, 0, 3, {"x", "y", "z"}, {1.0f, 1.0f, 1.0f}, "v_sph3D", 0, 0, nullptr},
     {"invsquircular", 377, 0, 0, NP, ND, "v_invsquircular", VF_W, 0, nullptr},
+    {"sphere_nja", 378, 0, 6, {"circle_a", "circle_b", "shift_x", "shift_y", "shift_z", "stretch"}, {1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_sphere_nja", VF_W, 0, nullptr},
     {"rings", 379, 0, 0, NP, ND, "v_rings", VF_XF | VF_W, 0, nullptr},
     {"rippled", 380, 0, 0, NP, ND, "v_rippled", 0, 0, nullptr},
     {"waffle", 381, 5, 4, {"slices", "xthickness", "ythickness", "rotation"}, {6.0f, 0.5f, 0.5f, 0.0f}, "v_waffle", 0, 2, derive_waffle},
@@ -663,6 +670,7 @@ static const VarDef kRegistry[] = {
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
     {"pre_sinusoidal3d", 393, 0, 0, NP, ND, "v_pre_sinusoidal3d", VF_PRE | VF_W, 0, nullptr},
     {"pre_blur3D", 394, 8, 0, NP, ND, "v_pre_blur3D", VF_PRE | VF_W, 0, nullptr},
+    {"loq", 400, 0, 1, {"base"}, {2.718281828459045f}, "v_loq", 0, 0, nullptr},
     {"pre_circlecrop", 410, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_pre_circlecrop", VF_PRE | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"post_circlecrop", 411, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_post_circlecrop", VF_POST | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"circlecrop", 412, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_circlecrop", VF_W | VF_HIDE, 1, derive_circlecrop},

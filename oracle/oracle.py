@@ -288,6 +288,14 @@ REGISTRY = {
     "popcorn2_3D": 474,
     "solid_sphere": 605,
     "matrix3D": 643,
+    "onion": 215,
+    "ho": 256,
+    "octagon": 274,
+    "xerf": 321,
+    "erf3D": 333,
+    "flower_db": 368,
+    "sphere_nja": 378,
+    "loq": 400,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -551,6 +559,14 @@ PARAMS.update({
     "popcorn2_3D": [("popcorn2_3D_x", 0.1), ("popcorn2_3D_y", 0.1), ("popcorn2_3D_z", 0.1), ("popcorn2_3D_c", 3.0)],
     "solid_sphere": [("radius", 1.0), ("thickness", 0.1), ("cx", 0.0), ("cy", 0.0), ("cz", 0.0)],
     "matrix3D": [("xx", 1.0), ("xy", 0.0), ("xz", 0.0), ("yx", 0.0), ("yy", 1.0), ("yz", 0.0), ("zx", 0.0), ("zy", 0.0), ("zz", 1.0), ("tx", 0.0), ("ty", 0.0), ("tz", 0.0)],
+})
+PARAMS.update({
+    "onion": [("centre_x", 0.0), ("centre_y", 0.0)],
+    "ho": [("xpow", 3.0), ("ypow", 3.0), ("zpow", 3.0)],
+    "octagon": [("x", 0.0), ("y", 0.0), ("z", 0.0)],
+    "flower_db": [("petals", 6.0), ("petal_split", 0.0), ("petal_spread", 1.0), ("stem_thickness", 1.0), ("stem_length", 0.0), ("petal_fold_strength", 0.0), ("petal_fold_radius", 1.0)],
+    "sphere_nja": [("circle_a", 1.0), ("circle_b", 1.0), ("shift_x", 0.0), ("shift_y", 0.0), ("shift_z", 0.0), ("stretch", 1.0)],
+    "loq": [("base", 2.718281828459045)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -277,6 +277,9 @@ WIDER = {
     "dinis_surface_wf": {**dict.fromkeys(["pi_e", "tiny", "lopsided"], "zero"),
         **dict.fromkeys(["large", "near_threshold", "past_threshold"], "huge")},
     "popcorn2_3D": {"lopsided": "huge"},
+    "ho": {**dict.fromkeys(["tiny", "normal_min"], "zero"), "lopsided": "huge"},
+    "flower_db": dict.fromkeys(["-x", "+y", "-y", "q3", "neg0y_x"], "zero"),
+    "sphere_nja": {"tiny": "tiny-quotient"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -308,7 +311,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "curl3D", "helix", "helicoid", "pie3D", "butterfly3D", "pyramid", "whitney_umbrella",
                        "ennepers2", "spherical3D", "square3D", "bubble2", "splits3D", "loonie_3D", "blade3D", "line",
                        "inflateZ_1", "inflateZ_2", "inflateZ_3", "inflateZ_4", "inflateZ_5", "inflateZ_6", "ovoid3d",
-                       "sph3D", "pre_blur3D", "extrude", "post_ztranslate_wf", "bubble_wf", "solid_sphere", "matrix3D"])
+                       "sph3D", "pre_blur3D", "extrude", "post_ztranslate_wf", "bubble_wf", "solid_sphere",
+                       "matrix3D", "onion", "octagon", "xerf", "erf3D"])
 
 
 def golden():
