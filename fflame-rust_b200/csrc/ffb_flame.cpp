@@ -303,6 +303,7 @@ void derive_ripple(const float* u, float* o) {                  // apo_misc13.rs
     o[0] = u[0] * 5.0f; o[1] = pl; o[2] = s; o[3] = u[1] * pl; o[4] = pl * al; o[5] = (pi - pl) * al;
 }
 void derive_circlecrop(const float* u, float* o) { o[0] = std::min(std::max(u[3], -1.0f), 1.0f); }   // circlecrop_*.rs (init)
+void derive_spherical3D_wf(const float* u, float* o) { o[0] = std::fabs(u[1] - 2.0f) < 1e-6f ? 1.0f : 0.0f; }   // apo_misc20.rs
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -670,12 +671,16 @@ static const VarDef kRegistry[] = {
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
     {"pre_sinusoidal3d", 393, 0, 0, NP, ND, "v_pre_sinusoidal3d", VF_PRE | VF_W, 0, nullptr},
     {"pre_blur3D", 394, 8, 0, NP, ND, "v_pre_blur3D", VF_PRE | VF_W, 0, nullptr},
+    {"seashell3D", 397, 2, 4, {"final_radius", "height", "inner_radius", "nSpirals"}, {0.25f, 3.5f, 0.4f, 3.0f}, "v_seashell3D", 0, 0, nullptr},
     {"loq", 400, 0, 1, {"base"}, {2.718281828459045f}, "v_loq", 0, 0, nullptr},
     {"pre_circlecrop", 410, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_pre_circlecrop", VF_PRE | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"post_circlecrop", 411, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_post_circlecrop", VF_POST | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"circlecrop", 412, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_circlecrop", VF_W | VF_HIDE, 1, derive_circlecrop},
+    {"exblur", 413, 6, 5, {"dist", "r", "x_origin", "y_origin", "z_origin"}, {0.5f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_exblur", 0, 0, nullptr},
     {"extrude", 415, 1, 1, {"root_face"}, {0.5f}, "v_extrude", 0, 0, nullptr},
+    {"lazysensen", 421, 0, 3, {"scale_x", "scale_y", "scale_z"}, {1.0f, 1.0f, 0.0f}, "v_lazysensen", 0, 0, nullptr},
     {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},
+    {"spherical3D_wf", 427, 0, 2, {"invert", "exponent"}, {0.0f, 2.0f}, "v_spherical3D_wf", 0, 1, derive_spherical3D_wf},
     {"heart_wf", 429, 0, 5, {"scale_x", "scale_t", "shift_t", "scale_r_left", "scale_r_right"}, {1.0f, 1.0f, 0.0f, 1.0f, 1.0f}, "v_heart_wf", 0, 0, nullptr},
     {"post_ztranslate_wf", 430, 0, 0, NP, ND, "v_post_ztranslate_wf", VF_POST, 0, nullptr},
     {"clifford_js", 435, 0, 4, {"a", "b", "c", "d"}, {-1.4f, 1.6f, 1.0f, 0.7f}, "v_clifford_js", 0, 0, nullptr},
@@ -693,6 +698,7 @@ static const VarDef kRegistry[] = {
     {"bubble_wf", 449, 0, 0, NP, ND, "v_bubble_wf", 0, 0, nullptr},
     {"dinis_surface_wf", 455, 0, 2, {"a", "b"}, {0.8f, 0.2f}, "v_dinis_surface_wf", 0, 0, nullptr},
     {"apocarpet_js", 458, 1, 0, NP, ND, "v_apocarpet_js", 0, 0, nullptr},
+    {"pre_wave3D_wf", 468, 0, 7, {"axis", "wavelen", "phase", "damping", "centre_x", "centre_y", "centre_z"}, {0.0f, 0.5f, 0.0f, 0.01f, 0.0f, 0.0f, 0.0f}, "v_pre_wave3D_wf", VF_PRE | VF_W, 0, nullptr},
     {"siercarpet_js", 473, 1, 1, {"m"}, {3.0f}, "v_siercarpet_js", 0, 0, nullptr},
     {"popcorn2_3D", 474, 0, 4, {"popcorn2_3D_x", "popcorn2_3D_y", "popcorn2_3D_z", "popcorn2_3D_c"}, {0.1f, 0.1f, 0.1f, 3.0f}, "v_popcorn2_3D", 0, 0, nullptr},
     {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},

@@ -296,6 +296,11 @@ REGISTRY = {
     "flower_db": 368,
     "sphere_nja": 378,
     "loq": 400,
+    "seashell3D": 397,
+    "exblur": 413,
+    "lazysensen": 421,
+    "spherical3D_wf": 427,
+    "pre_wave3D_wf": 468,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -567,6 +572,13 @@ PARAMS.update({
     "flower_db": [("petals", 6.0), ("petal_split", 0.0), ("petal_spread", 1.0), ("stem_thickness", 1.0), ("stem_length", 0.0), ("petal_fold_strength", 0.0), ("petal_fold_radius", 1.0)],
     "sphere_nja": [("circle_a", 1.0), ("circle_b", 1.0), ("shift_x", 0.0), ("shift_y", 0.0), ("shift_z", 0.0), ("stretch", 1.0)],
     "loq": [("base", 2.718281828459045)],
+})
+PARAMS.update({
+    "seashell3D": [("final_radius", 0.25), ("height", 3.5), ("inner_radius", 0.4), ("nSpirals", 3.0)],
+    "exblur": [("dist", 0.5), ("r", 0.0), ("x_origin", 0.0), ("y_origin", 0.0), ("z_origin", 0.0)],
+    "lazysensen": [("scale_x", 1.0), ("scale_y", 1.0), ("scale_z", 0.0)],
+    "spherical3D_wf": [("invert", 0.0), ("exponent", 2.0)],
+    "pre_wave3D_wf": [("axis", 0.0), ("wavelen", 0.5), ("phase", 0.0), ("damping", 0.01), ("centre_x", 0.0), ("centre_y", 0.0), ("centre_z", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -280,6 +280,9 @@ WIDER = {
     "ho": {**dict.fromkeys(["tiny", "normal_min"], "zero"), "lopsided": "huge"},
     "flower_db": dict.fromkeys(["-x", "+y", "-y", "q3", "neg0y_x"], "zero"),
     "sphere_nja": {"tiny": "tiny-quotient"},
+    "exblur": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
+    # lazysensen: i32 of an out-of-range floor(c * scale); the reference's conversion gives the other parity.
+    "lazysensen": dict.fromkeys(HUGE_ARGS, "branch"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -312,7 +315,7 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "ennepers2", "spherical3D", "square3D", "bubble2", "splits3D", "loonie_3D", "blade3D", "line",
                        "inflateZ_1", "inflateZ_2", "inflateZ_3", "inflateZ_4", "inflateZ_5", "inflateZ_6", "ovoid3d",
                        "sph3D", "pre_blur3D", "extrude", "post_ztranslate_wf", "bubble_wf", "solid_sphere",
-                       "matrix3D", "onion", "octagon", "xerf", "erf3D"])
+                       "matrix3D", "onion", "octagon", "xerf", "erf3D", "spherical3D_wf", "pre_wave3D_wf"])
 
 
 def golden():
