@@ -304,6 +304,44 @@ void derive_ripple(const float* u, float* o) {                  // apo_misc13.rs
 }
 void derive_circlecrop(const float* u, float* o) { o[0] = std::min(std::max(u[3], -1.0f), 1.0f); }   // circlecrop_*.rs (init)
 void derive_spherical3D_wf(const float* u, float* o) { o[0] = std::fabs(u[1] - 2.0f) < 1e-6f ? 1.0f : 0.0f; }   // apo_misc20.rs
+void derive_hypertile3D(const float* u, float* o) {             // hypertile.rs (init_hypertile3D)
+    const float pi = 3.14159265358979f, pa = 2.0f * pi / u[0], qa = 2.0f * pi / u[1];
+    const float r_alt = -(std::cos(pa) - 1.0f) / (std::cos(pa) + std::cos(qa));
+    const float r = r_alt > 0.0f ? 1.0f / std::sqrt(1.0f + r_alt) : 1.0f, na = u[2] * pa;
+    const float cx = r * std::cos(na), cy = r * std::sin(na), cx2 = cx * cx, cy2 = cy * cy;
+    o[0] = cx; o[1] = cy; o[2] = cx2 + cy2; o[3] = 2.0f * cx; o[4] = 2.0f * cy;
+    o[5] = 1.0f + cx2 - cy2; o[6] = 1.0f + cy2 - cx2; o[7] = 1.0f - cx2 - cy2;
+}
+void derive_hypercrop(const float* u, float* o) {               // maurer_hyper.rs (init_hypercrop)
+    const float n = std::fmax(u[0], 3.0f), a0 = 3.14159265358979f / n, len = 1.0f / std::cos(a0);
+    o[0] = n / 6.28318530717959f; o[1] = a0; o[2] = len; o[3] = u[1] * std::sin(a0) * len;
+}
+void derive_poincare3D(const float* u, float* o) {              // apo_misc14.rs (init_poincare3D)
+    const float h = 1.5707963267948966f, r = u[0], cb = std::cos(u[2] * h);
+    const float cx = -r * std::cos(u[1] * h) * cb, cy = r * std::sin(u[1] * h) * cb, cz = -r * std::sin(u[2] * h);
+    const float cx2 = cx * cx, cy2 = cy * cy, cz2 = cz * cz;
+    o[0] = cx; o[1] = cy; o[2] = cz; o[3] = cx2 + cy2 + cz2; o[4] = 2.0f * cx; o[5] = 2.0f * cy; o[6] = 2.0f * cz;
+    o[7] = cx2 - cy2 - cz2 + 1.0f; o[8] = cy2 - cx2 - cz2 + 1.0f; o[9] = cz2 - cy2 - cx2 + 1.0f;
+}
+void derive_rosoni(const float* u, float* o) {                  // rosoni_misc.rs (init_rosoni)
+    const float phi = 6.28318530717959f / std::fmax(u[0], 1.0f);
+    o[0] = std::sin(phi); o[1] = std::cos(phi);
+}
+void derive_bwraps7(const float* u, float* o) {                 // bwraps7_misc.rs (init_bwraps7)
+    if (std::fabs(u[0]) < 1e-30f) { o[0] = o[1] = o[2] = 0.0f; return; }
+    const float radius = 0.5f * (u[0] / (1.0f + u[1] * u[1])), g2 = u[2] * u[2] + 1e-6f;
+    float mb = g2 * radius;
+    mb = mb > 2.0f ? 1.0f : mb * (1.0f / ((mb * mb) * 0.25f + 1.0f));
+    o[0] = g2; o[1] = radius * radius; o[2] = radius / std::fmax(mb, 1e-30f);
+}
+void derive_curl_sp(const float* u, float* o) {                 // curl_sp_misc.rs (init_curl_sp)
+    const float p = std::fabs(u[0]) < 1e-30f ? 1e-6f : u[0];
+    o[0] = p; o[1] = 2.0f * u[2]; o[2] = 1.0f / p; o[3] = 0.1f * u[5];
+}
+void derive_waves_wf(const float* u, float* o) {                // waves_wf_family.rs (init_waves2_wf, shared)
+    o[0] = std::fabs(u[6]) < 1e-6f ? 1.0f : std::exp(u[6]);
+    o[1] = std::fabs(u[7]) < 1e-6f ? 1.0f : std::exp(u[7]);
+}
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -493,6 +531,7 @@ static const VarDef kRegistry[] = {
     {"hypertile", 184, 0, 3, {"p", "q", "n"}, {3.0f, 7.0f, 1.0f}, "v_hypertile", 0, 2, derive_hypertile},
     {"hypertile1", 185, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile1", 0, 2, derive_hypertile1},
     {"hypertile2", 186, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile2", 0, 2, derive_hypertile2},
+    {"hypertile3D", 187, 0, 3, {"p", "q", "n"}, {3.0f, 7.0f, 0.0f}, "v_hypertile3D", 0, 8, derive_hypertile3D},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
     {"gridout", 192, 0, 0, NP, ND, "v_gridout", 0, 0, nullptr},
@@ -538,6 +577,7 @@ static const VarDef kRegistry[] = {
     {"lozi", 243, 0, 3, {"a", "b", "c"}, {0.5f, 1.0f, 1.0f}, "v_lozi", 0, 0, nullptr},
     {"pulse", 244, 0, 4, {"freqx", "freqy", "scalex", "scaley"}, {2.0f, 2.0f, 1.0f, 1.0f}, "v_pulse", 0, 0, nullptr},
     {"hypershift", 245, 0, 2, {"shift", "stretch"}, {2.0f, 1.0f}, "v_hypershift", VF_W, 0, nullptr},
+    {"hypercrop", 247, 0, 3, {"n", "rad", "zero"}, {4.0f, 1.0f, 0.0f}, "v_hypercrop", 0, 4, derive_hypercrop},
     {"split", 248, 0, 2, {"xsize", "ysize"}, {0.4f, 0.6f}, "v_split", 0, 0, nullptr},
     {"squirrel", 249, 0, 2, {"a", "b"}, {1.0f, 1.0f}, "v_squirrel", VF_REPLACE, 0, nullptr},
     {"stripes", 250, 0, 2, {"space", "warp"}, {0.2f, 0.6f}, "v_stripes", 0, 0, nullptr},
@@ -592,6 +632,7 @@ static const VarDef kRegistry[] = {
     {"whorl", 302, 0, 2, {"inside", "outside"}, {0.1f, 0.2f}, "v_whorl", VF_W, 0, nullptr},
     {"devil_warp", 303, 0, 6, {"a", "b", "effect", "warp", "rmin", "rmax"}, {2.0f, 1.0f, 1.0f, 0.5f, -0.24f, 100.0f}, "v_devil_warp", VF_W, 0, nullptr},
     {"trade", 304, 0, 4, {"r1", "d1", "r2", "d2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_trade", 0, 2, derive_trade},
+    {"voron", 305, 0, 5, {"k", "step", "num", "xseed", "yseed"}, {0.99f, 0.25f, 1.0f, 3.0f, 7.0f}, "v_voron", 0, 0, nullptr},
     {"squircular", 306, 0, 0, NP, ND, "v_squircular", VF_W, 0, nullptr},
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
@@ -653,6 +694,7 @@ static const VarDef kRegistry[] = {
     {"mask", 370, 0, 5, {"xshift", "yshift", "ushift", "xscale", "yscale"}, {0.0f, 0.0f, 1.0f, 1.0f, 1.0f}, "v_mask", 0, 0, nullptr},
     {"ovoid3d", 371, 0, 3, {"x", "y", "z"}, {1.0f, 1.0f, 1.0f}, "v_ovoid3d", 0, 0, nullptr},
     {"murl2", 372, 0, 2, {"c", "power"}, {0.1f, 3.0f}, "v_murl2", VF_W, 0, nullptr},
+    {"minkQM", 373, 0, 6, {"a", "b", "c", "dd", "e", "f"}, {1.0f, 1.0f, 1.0f, 1.0f, 0.5f, 20.0f}, "v_minkQM", 0, 0, nullptr},
     {"swirl3", 374, 0, 1, {"shift"}, {0.5f}, "v_swirl3", 0, 0, nullptr},
     {"wdisc", 375, 0, 0, NP, ND, "v_wdisc", 0, 0, nullptr},
     {"sph3D", 376, 0, 3, {"x", "y", "z"}, {1.0f, 1.0f, 1.0f}, "v_sph3D", 0, 0, nullptr},
@@ -669,16 +711,23 @@ static const VarDef kRegistry[] = {
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
     {"pre_disc3d", 389, 0, 1, {"pi"}, {3.141592653589793f}, "v_pre_disc3d", VF_PRE | VF_W, 0, nullptr},
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
+    {"poincare3D", 392, 0, 3, {"r", "a", "b"}, {0.0f, 0.0f, 0.0f}, "v_poincare3D", 0, 10, derive_poincare3D},
     {"pre_sinusoidal3d", 393, 0, 0, NP, ND, "v_pre_sinusoidal3d", VF_PRE | VF_W, 0, nullptr},
     {"pre_blur3D", 394, 8, 0, NP, ND, "v_pre_blur3D", VF_PRE | VF_W, 0, nullptr},
+    {"rosoni", 396, 0, 7, {"maxiter", "sweetiter", "altshapes", "cutoff", "radius", "dx", "dy"}, {25.0f, 3.0f, 0.0f, 1.0f, 0.4f, 0.6f, 0.0f}, "v_rosoni", 0, 2, derive_rosoni},
     {"seashell3D", 397, 2, 4, {"final_radius", "height", "inner_radius", "nSpirals"}, {0.25f, 3.5f, 0.4f, 3.0f}, "v_seashell3D", 0, 0, nullptr},
+    {"bwraps7", 399, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_bwraps7", 0, 3, derive_bwraps7},
     {"loq", 400, 0, 1, {"base"}, {2.718281828459045f}, "v_loq", 0, 0, nullptr},
+    {"post_heat", 404, 0, 9, {"theta_period", "theta_phase", "theta_amp", "phi_period", "phi_phase", "phi_amp", "r_period", "r_phase", "r_amp"}, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_post_heat", VF_POST | VF_W, 0, nullptr},
+    {"onion2", 406, 0, 8, {"meeting_pt", "circle_a", "circle_b", "shift_x", "shift_y", "shift_z", "top_crop", "stretch"}, {0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_onion2", VF_W, 0, nullptr},
     {"pre_circlecrop", 410, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_pre_circlecrop", VF_PRE | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"post_circlecrop", 411, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_post_circlecrop", VF_POST | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"circlecrop", 412, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_circlecrop", VF_W | VF_HIDE, 1, derive_circlecrop},
     {"exblur", 413, 6, 5, {"dist", "r", "x_origin", "y_origin", "z_origin"}, {0.5f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_exblur", 0, 0, nullptr},
+    {"curl_sp", 414, 0, 6, {"pow", "c1", "c2", "sx", "sy", "dc"}, {1.0f, -0.01f, 0.03f, 0.0f, 0.0f, 0.0f}, "v_curl_sp", VF_W, 4, derive_curl_sp},
     {"extrude", 415, 1, 1, {"root_face"}, {0.5f}, "v_extrude", 0, 0, nullptr},
     {"lazysensen", 421, 0, 3, {"scale_x", "scale_y", "scale_z"}, {1.0f, 1.0f, 0.0f}, "v_lazysensen", 0, 0, nullptr},
+    {"circleLinear", 425, 0, 8, {"Sc", "K", "Dens1", "Dens2", "Reverse", "X", "Y", "Seed"}, {1.0f, 0.5f, 0.5f, 0.5f, 1.0f, 10.0f, 10.0f, 0.0f}, "v_circleLinear", 0, 0, nullptr},
     {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},
     {"spherical3D_wf", 427, 0, 2, {"invert", "exponent"}, {0.0f, 2.0f}, "v_spherical3D_wf", 0, 1, derive_spherical3D_wf},
     {"heart_wf", 429, 0, 5, {"scale_x", "scale_t", "shift_t", "scale_r_left", "scale_r_right"}, {1.0f, 1.0f, 0.0f, 1.0f, 1.0f}, "v_heart_wf", 0, 0, nullptr},
@@ -696,11 +745,16 @@ static const VarDef kRegistry[] = {
     {"cloverleaf_wf", 447, 1, 1, {"filled"}, {1.0f}, "v_cloverleaf_wf", 0, 0, nullptr},
     {"rose_wf", 448, 1, 3, {"amp", "waves", "filled"}, {0.5f, 4.0f, 0.0f}, "v_rose_wf", 0, 0, nullptr},
     {"bubble_wf", 449, 0, 0, NP, ND, "v_bubble_wf", 0, 0, nullptr},
+    {"waves2_wf", 452, 0, 8, {"scalex", "scaley", "freqx", "freqy", "use_cos_x", "use_cos_y", "dampx", "dampy"}, {0.25f, 0.5f, 1.5707963267948966f, 0.7853981633974483f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_waves2_wf", 0, 2, derive_waves_wf},
+    {"waves3_wf", 453, 0, 8, {"scalex", "scaley", "freqx", "freqy", "use_cos_x", "use_cos_y", "dampx", "dampy"}, {0.25f, 0.5f, 1.5707963267948966f, 0.7853981633974483f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_waves3_wf", 0, 2, derive_waves_wf},
+    {"waves4_wf", 454, 0, 8, {"scalex", "scaley", "freqx", "freqy", "use_cos_x", "use_cos_y", "dampx", "dampy"}, {0.25f, 0.5f, 1.5707963267948966f, 0.7853981633974483f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_waves4_wf", 0, 2, derive_waves_wf},
     {"dinis_surface_wf", 455, 0, 2, {"a", "b"}, {0.8f, 0.2f}, "v_dinis_surface_wf", 0, 0, nullptr},
     {"apocarpet_js", 458, 1, 0, NP, ND, "v_apocarpet_js", 0, 0, nullptr},
     {"pre_wave3D_wf", 468, 0, 7, {"axis", "wavelen", "phase", "damping", "centre_x", "centre_y", "centre_z"}, {0.0f, 0.5f, 0.0f, 0.01f, 0.0f, 0.0f, 0.0f}, "v_pre_wave3D_wf", VF_PRE | VF_W, 0, nullptr},
     {"siercarpet_js", 473, 1, 1, {"m"}, {3.0f}, "v_siercarpet_js", 0, 0, nullptr},
     {"popcorn2_3D", 474, 0, 4, {"popcorn2_3D_x", "popcorn2_3D_y", "popcorn2_3D_z", "popcorn2_3D_c"}, {0.1f, 0.1f, 0.1f, 3.0f}, "v_popcorn2_3D", 0, 0, nullptr},
+    {"plusrecip", 476, 0, 2, {"ar", "ai"}, {4.0f, 0.0f}, "v_plusrecip", 0, 0, nullptr},
+    {"gamma", 477, 0, 0, NP, ND, "v_gamma", 0, 0, nullptr},
     {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},
      "v_klein_group", VF_W, 16, derive_klein_group, 1, 1},
     {"subflame_wf", 502, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},

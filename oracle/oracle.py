@@ -301,6 +301,22 @@ REGISTRY = {
     "lazysensen": 421,
     "spherical3D_wf": 427,
     "pre_wave3D_wf": 468,
+    "hypertile3D": 187,
+    "hypercrop": 247,
+    "voron": 305,
+    "minkQM": 373,
+    "poincare3D": 392,
+    "rosoni": 396,
+    "bwraps7": 399,
+    "post_heat": 404,
+    "onion2": 406,
+    "curl_sp": 414,
+    "circleLinear": 425,
+    "waves2_wf": 452,
+    "waves3_wf": 453,
+    "waves4_wf": 454,
+    "plusrecip": 476,
+    "gamma": 477,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -579,6 +595,23 @@ PARAMS.update({
     "lazysensen": [("scale_x", 1.0), ("scale_y", 1.0), ("scale_z", 0.0)],
     "spherical3D_wf": [("invert", 0.0), ("exponent", 2.0)],
     "pre_wave3D_wf": [("axis", 0.0), ("wavelen", 0.5), ("phase", 0.0), ("damping", 0.01), ("centre_x", 0.0), ("centre_y", 0.0), ("centre_z", 0.0)],
+})
+PARAMS.update({
+    "hypertile3D": [("p", 3.0), ("q", 7.0), ("n", 0.0)],
+    "hypercrop": [("n", 4.0), ("rad", 1.0), ("zero", 0.0)],
+    "voron": [("k", 0.99), ("step", 0.25), ("num", 1.0), ("xseed", 3.0), ("yseed", 7.0)],
+    "minkQM": [("a", 1.0), ("b", 1.0), ("c", 1.0), ("dd", 1.0), ("e", 0.5), ("f", 20.0)],
+    "poincare3D": [("r", 0.0), ("a", 0.0), ("b", 0.0)],
+    "rosoni": [("maxiter", 25.0), ("sweetiter", 3.0), ("altshapes", 0.0), ("cutoff", 1.0), ("radius", 0.4), ("dx", 0.6), ("dy", 0.0)],
+    "bwraps7": [("cellsize", 1.0), ("space", 0.0), ("gain", 2.0), ("inner_twist", 0.0), ("outer_twist", 0.0)],
+    "post_heat": [("theta_period", 0.0), ("theta_phase", 0.0), ("theta_amp", 0.0), ("phi_period", 0.0), ("phi_phase", 0.0), ("phi_amp", 0.0), ("r_period", 0.0), ("r_phase", 0.0), ("r_amp", 0.0)],
+    "onion2": [("meeting_pt", 0.5), ("circle_a", 1.0), ("circle_b", 1.0), ("shift_x", 0.0), ("shift_y", 0.0), ("shift_z", 0.0), ("top_crop", 0.0), ("stretch", 1.0)],
+    "curl_sp": [("pow", 1.0), ("c1", -0.01), ("c2", 0.03), ("sx", 0.0), ("sy", 0.0), ("dc", 0.0)],
+    "circleLinear": [("Sc", 1.0), ("K", 0.5), ("Dens1", 0.5), ("Dens2", 0.5), ("Reverse", 1.0), ("X", 10.0), ("Y", 10.0), ("Seed", 0.0)],
+    "waves2_wf": [("scalex", 0.25), ("scaley", 0.5), ("freqx", 1.5707963267948966), ("freqy", 0.7853981633974483), ("use_cos_x", 1.0), ("use_cos_y", 0.0), ("dampx", 0.0), ("dampy", 0.0)],
+    "waves3_wf": [("scalex", 0.25), ("scaley", 0.5), ("freqx", 1.5707963267948966), ("freqy", 0.7853981633974483), ("use_cos_x", 1.0), ("use_cos_y", 0.0), ("dampx", 0.0), ("dampy", 0.0)],
+    "waves4_wf": [("scalex", 0.25), ("scaley", 0.5), ("freqx", 1.5707963267948966), ("freqy", 0.7853981633974483), ("use_cos_x", 1.0), ("use_cos_y", 0.0), ("dampx", 0.0), ("dampy", 0.0)],
+    "plusrecip": [("ar", 4.0), ("ai", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

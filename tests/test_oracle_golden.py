@@ -63,7 +63,15 @@ SFU_SIN = {
 # the body replaced by a 1e-30 divisor (infinite there, finite here);
 # "reassociated": the reference's compiler grouped `x * x * y * y` as
 # (x * x) * (y * y), inf * 0 = NaN, which its max() then replaced, where
-# the source order gives inf and a NaN further on.
+# the source order gives inf and a NaN further on;
+# "fused": the reference's compiler contracted `x * x - y * y` into one
+# fused multiply-add, fma(x, x, -(y * y)) = -inf where x * x and y * y
+# both overflow, where the source order's inf - inf is NaN (plusrecip's
+# square root of z^2 - a then stays finite here and is infinite there);
+# "scaled-zero": the reference's cos(f32(pi) / 2) is exactly 0 where ours
+# is -4.4e-8, and the body multiplies it by a large finite factor
+# (onion2's p / max(|p|, 1e-30) at the 1e-20 input, whose squares flush to
+# zero), finite here and 0 there.
 HUGE_ARGS = ["large", "near_threshold", "past_threshold", "lopsided"]
 # Where the bipolar series' sigma is f32(pi) (sin(sigma) -4.4e-8 here, 0 on
 # the reference) and the elliptic series' nu is f32(pi)/2 (cos(nu) -4.4e-8).
@@ -283,6 +291,15 @@ WIDER = {
     "exblur": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "neg0y_x"], "zero"),
     # lazysensen: i32 of an out-of-range floor(c * scale); the reference's conversion gives the other parity.
     "lazysensen": dict.fromkeys(HUGE_ARGS, "branch"),
+    "hypercrop": dict.fromkeys(["-x", "-y"], "zero"),
+    "post_heat": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
+    "onion2": {"tiny": "scaled-zero", "normal_min": "zero"},
+    "waves2_wf": {**dict.fromkeys(["+y", "-y", "neg0y_x"], "zero"), "lopsided": "huge"},
+    "waves3_wf": dict.fromkeys(["+y", "-y", "neg0y_x"], "zero"),
+    "waves4_wf": dict.fromkeys(["+y", "-y", "neg0y_x"], "zero"),
+    "plusrecip": dict.fromkeys(["large", "near_threshold", "past_threshold"], "fused"),
+    # gamma: log|Gamma(r)| at r = 1 is 0; ours and the reference's logs round it to a few ulp of either sign.
+    "gamma": dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "half_unit", "y_neg0x", "neg0y_x"], "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -315,7 +332,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "ennepers2", "spherical3D", "square3D", "bubble2", "splits3D", "loonie_3D", "blade3D", "line",
                        "inflateZ_1", "inflateZ_2", "inflateZ_3", "inflateZ_4", "inflateZ_5", "inflateZ_6", "ovoid3d",
                        "sph3D", "pre_blur3D", "extrude", "post_ztranslate_wf", "bubble_wf", "solid_sphere",
-                       "matrix3D", "onion", "octagon", "xerf", "erf3D", "spherical3D_wf", "pre_wave3D_wf"])
+                       "matrix3D", "onion", "octagon", "xerf", "erf3D", "spherical3D_wf", "pre_wave3D_wf",
+                       "hypertile3D", "voron", "minkQM", "poincare3D", "rosoni", "bwraps7", "curl_sp", "circleLinear"])
 
 
 def golden():
@@ -368,6 +386,10 @@ def test_wider_registry_probe_matches_the_reference(oracle, name):
                 assert math.isfinite(v) and theirs[c] in "0o", (name, label, v)
             elif why == "zero-divisor":
                 assert math.isfinite(v) and theirs[c] in "iI", (name, label, v)
+            elif why == "fused":
+                assert math.isfinite(v) and theirs[c] in "iI", (name, label, v)
+            elif why == "scaled-zero":
+                assert math.isfinite(v) and theirs[c] in "0o", (name, label, v)
             elif why == "reassociated":
                 assert math.isnan(v) and theirs[c] != "n", (name, label, v)
             else:

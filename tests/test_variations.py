@@ -47,7 +47,8 @@ EXACT = {"linear", "spherical", "horseshoe", "bubble", "curl", "hyperbolic", "be
          "rectangles", "splits", "butterfly", "fisheye", "stripes", "bent2", "linear3D", "flatten", "loonie", "scry",
          "separation", "mobius", "cell", "modulus", "square", "boarders",
          "blur_zoom", "blur_pixelize", "henon", "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy",
-         "loonie3", "d_spherical"}
+         "loonie3", "d_spherical", "hypertile3D", "voron", "minkQM", "poincare3D", "rosoni", "circleLinear",
+         "plusrecip"}
 
 
 @pytest.fixture(scope="module")
