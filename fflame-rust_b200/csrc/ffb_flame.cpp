@@ -342,6 +342,23 @@ void derive_waves_wf(const float* u, float* o) {                // waves_wf_fami
     o[0] = std::fabs(u[6]) < 1e-6f ? 1.0f : std::exp(u[6]);
     o[1] = std::fabs(u[7]) < 1e-6f ? 1.0f : std::exp(u[7]);
 }
+void derive_xheart_blur_wf(const float* u, float* o) {          // apo_misc18.rs (init_xheart_blur_wf)
+    const float pi_4 = 0.7853981633974483f, ang = pi_4 + 0.5f * pi_4 * u[0];
+    o[0] = std::sin(ang); o[1] = std::cos(ang); o[2] = 6.0f + 2.0f * u[1];
+}
+void derive_affine3D(const float* u, float* o) {                // affine3d_misc.rs (init_affine3D)
+    const float d2r = 0.017453292519943295f;
+    const bool shear = std::fabs(u[9]) + std::fabs(u[10]) + std::fabs(u[11]) + std::fabs(u[12]) + std::fabs(u[13]) + std::fabs(u[14]) > 1e-6f;
+    o[0] = std::sin(u[6] * d2r); o[1] = std::cos(u[6] * d2r); o[2] = std::sin(u[7] * d2r); o[3] = std::cos(u[7] * d2r);
+    o[4] = std::sin(u[8] * d2r); o[5] = std::cos(u[8] * d2r); o[6] = shear ? 1.0f : 0.0f;
+}
+// z and w (wz_lost_variations.rs init_z, init_w): `h` the index of hypergon.
+void derive_wz(const float* u, float* o, int h) {
+    o[0] = std::sqrt(1.0f + u[h + 2] * u[h + 2]); o[1] = u[h + 1]; o[2] = -u[h + 7]; o[3] = u[h + 4];
+    o[4] = std::tan(u[h + 5]); o[5] = u[h + 9] * 0.25f; o[6] = -1.0f / (u[h + 10] + 1e-7f);
+}
+void derive_z(const float* u, float* o) { derive_wz(u, o, 0); }
+void derive_w(const float* u, float* o) { derive_wz(u, o, 1); }
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -538,6 +555,7 @@ static const VarDef kRegistry[] = {
     {"panorama1", 194, 0, 0, NP, ND, "v_panorama1", 0, 0, nullptr},
     {"panorama2", 195, 0, 0, NP, ND, "v_panorama2", 0, 0, nullptr},
     {"mobiusN", 196, 1, 10, {"re_a", "re_b", "re_c", "re_d", "im_a", "im_b", "im_c", "im_d", "power", "dist"}, {1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 1.0f}, "v_mobiusN", 0, 0, nullptr},
+    {"mobiq", 197, 0, 16, {"qat", "qax", "qay", "qaz", "qbt", "qbx", "qby", "qbz", "qct", "qcx", "qcy", "qcz", "qdt", "qdx", "qdy", "qdz"}, {1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_mobiq", 0, 0, nullptr},
     {"circleblur", 198, 2, 0, NP, ND, "v_circleblur", 0, 0, nullptr},
     {"circlesplit", 199, 0, 2, {"radius", "split"}, {1.0f, 0.5f}, "v_circlesplit", 0, 0, nullptr},
     {"flipcircle", 200, 0, 0, NP, ND, "v_flipcircle", VF_W, 0, nullptr},
@@ -720,6 +738,9 @@ static const VarDef kRegistry[] = {
     {"loq", 400, 0, 1, {"base"}, {2.718281828459045f}, "v_loq", 0, 0, nullptr},
     {"post_heat", 404, 0, 9, {"theta_period", "theta_phase", "theta_amp", "phi_period", "phi_phase", "phi_amp", "r_period", "r_phase", "r_amp"}, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_post_heat", VF_POST | VF_W, 0, nullptr},
     {"onion2", 406, 0, 8, {"meeting_pt", "circle_a", "circle_b", "shift_x", "shift_y", "shift_z", "top_crop", "stretch"}, {0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_onion2", VF_W, 0, nullptr},
+    {"jac_sn", 407, 0, 1, {"jac_sn_k"}, {0.5f}, "v_jac_sn", 0, 0, nullptr},
+    {"jac_cn", 408, 0, 1, {"jac_cn_k"}, {0.5f}, "v_jac_cn", 0, 0, nullptr},
+    {"jac_dn", 409, 0, 1, {"jac_dn_k"}, {0.5f}, "v_jac_dn", 0, 0, nullptr},
     {"pre_circlecrop", 410, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_pre_circlecrop", VF_PRE | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"post_circlecrop", 411, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_post_circlecrop", VF_POST | VF_W | VF_HIDE, 1, derive_circlecrop},
     {"circlecrop", 412, 1, 5, {"radius", "x", "y", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_circlecrop", VF_W | VF_HIDE, 1, derive_circlecrop},
@@ -727,6 +748,7 @@ static const VarDef kRegistry[] = {
     {"curl_sp", 414, 0, 6, {"pow", "c1", "c2", "sx", "sy", "dc"}, {1.0f, -0.01f, 0.03f, 0.0f, 0.0f, 0.0f}, "v_curl_sp", VF_W, 4, derive_curl_sp},
     {"extrude", 415, 1, 1, {"root_face"}, {0.5f}, "v_extrude", 0, 0, nullptr},
     {"lazysensen", 421, 0, 3, {"scale_x", "scale_y", "scale_z"}, {1.0f, 1.0f, 0.0f}, "v_lazysensen", 0, 0, nullptr},
+    {"xheart_blur_wf", 423, 2, 2, {"angle", "ratio"}, {0.0f, 0.0f}, "v_xheart_blur_wf", 0, 3, derive_xheart_blur_wf},
     {"circleLinear", 425, 0, 8, {"Sc", "K", "Dens1", "Dens2", "Reverse", "X", "Y", "Seed"}, {1.0f, 0.5f, 0.5f, 0.5f, 1.0f, 10.0f, 10.0f, 0.0f}, "v_circleLinear", 0, 0, nullptr},
     {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},
     {"spherical3D_wf", 427, 0, 2, {"invert", "exponent"}, {0.0f, 2.0f}, "v_spherical3D_wf", 0, 1, derive_spherical3D_wf},
@@ -750,11 +772,15 @@ static const VarDef kRegistry[] = {
     {"waves4_wf", 454, 0, 8, {"scalex", "scaley", "freqx", "freqy", "use_cos_x", "use_cos_y", "dampx", "dampy"}, {0.25f, 0.5f, 1.5707963267948966f, 0.7853981633974483f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_waves4_wf", 0, 2, derive_waves_wf},
     {"dinis_surface_wf", 455, 0, 2, {"a", "b"}, {0.8f, 0.2f}, "v_dinis_surface_wf", 0, 0, nullptr},
     {"apocarpet_js", 458, 1, 0, NP, ND, "v_apocarpet_js", 0, 0, nullptr},
+    {"affine3D", 464, 0, 15, {"translateX", "translateY", "translateZ", "scaleX", "scaleY", "scaleZ", "rotateX", "rotateY", "rotateZ", "shearXY", "shearXZ", "shearYX", "shearYZ", "shearZX", "shearZY"}, {0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_affine3D", 0, 7, derive_affine3D},
     {"pre_wave3D_wf", 468, 0, 7, {"axis", "wavelen", "phase", "damping", "centre_x", "centre_y", "centre_z"}, {0.0f, 0.5f, 0.0f, 0.01f, 0.0f, 0.0f, 0.0f}, "v_pre_wave3D_wf", VF_PRE | VF_W, 0, nullptr},
     {"siercarpet_js", 473, 1, 1, {"m"}, {3.0f}, "v_siercarpet_js", 0, 0, nullptr},
     {"popcorn2_3D", 474, 0, 4, {"popcorn2_3D_x", "popcorn2_3D_y", "popcorn2_3D_z", "popcorn2_3D_c"}, {0.1f, 0.1f, 0.1f, 3.0f}, "v_popcorn2_3D", 0, 0, nullptr},
     {"plusrecip", 476, 0, 2, {"ar", "ai"}, {4.0f, 0.0f}, "v_plusrecip", 0, 0, nullptr},
     {"gamma", 477, 0, 0, NP, ND, "v_gamma", 0, 0, nullptr},
+    {"z", 489, 0, 13, {"hypergon", "hypergon_n", "hypergon_r", "star", "star_n", "star_slope", "lituus", "lituus_a", "super_shape", "super_m", "super_n1", "super_n2", "super_n3"}, {0.0f, 4.0f, 1.0f, 0.0f, 5.0f, 2.0f, 0.0f, 1.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_z", 0, 7, derive_z},
+    {"w", 490, 0, 14, {"angle", "hypergon", "hypergon_n", "hypergon_r", "star", "star_n", "star_slope", "lituus", "lituus_a", "super_shape", "super_m", "super_n1", "super_n2", "super_n3"}, {0.0f, 0.0f, 4.0f, 1.0f, 0.0f, 5.0f, 2.0f, 0.0f, 1.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_w", 0, 7, derive_w},
+    {"harmonograph_js", 496, 1, 18, {"seed", "time", "a1", "f1", "p1", "d1", "a2", "f2", "p2", "d2", "a3", "f3", "p3", "d3", "a4", "f4", "p4", "d4"}, {1234.0f, 100.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_harmonograph_js", 0, 0, nullptr},
     {"klein_group", 501, 1, 6, {"a_re", "a_im", "b_re", "b_im", "recipe", "avoid_reversal"}, {2.0f, 0.0f, 2.0f, 0.0f, 0.0f, 1.0f},
      "v_klein_group", VF_W, 16, derive_klein_group, 1, 1},
     {"subflame_wf", 502, 0, 8, {"subflame_id", "scale", "angle", "offset_x", "offset_y", "offset_z", "colorscale_z", "color_mode"},

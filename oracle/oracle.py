@@ -317,6 +317,15 @@ REGISTRY = {
     "waves4_wf": 454,
     "plusrecip": 476,
     "gamma": 477,
+    "mobiq": 197,
+    "jac_sn": 407,
+    "jac_cn": 408,
+    "jac_dn": 409,
+    "xheart_blur_wf": 423,
+    "affine3D": 464,
+    "z": 489,
+    "w": 490,
+    "harmonograph_js": 496,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -612,6 +621,17 @@ PARAMS.update({
     "waves3_wf": [("scalex", 0.25), ("scaley", 0.5), ("freqx", 1.5707963267948966), ("freqy", 0.7853981633974483), ("use_cos_x", 1.0), ("use_cos_y", 0.0), ("dampx", 0.0), ("dampy", 0.0)],
     "waves4_wf": [("scalex", 0.25), ("scaley", 0.5), ("freqx", 1.5707963267948966), ("freqy", 0.7853981633974483), ("use_cos_x", 1.0), ("use_cos_y", 0.0), ("dampx", 0.0), ("dampy", 0.0)],
     "plusrecip": [("ar", 4.0), ("ai", 0.0)],
+})
+PARAMS.update({
+    "mobiq": [("qat", 1.0), ("qax", 0.0), ("qay", 0.0), ("qaz", 0.0), ("qbt", 0.0), ("qbx", 0.0), ("qby", 0.0), ("qbz", 0.0), ("qct", 0.0), ("qcx", 0.0), ("qcy", 0.0), ("qcz", 0.0), ("qdt", 1.0), ("qdx", 0.0), ("qdy", 0.0), ("qdz", 0.0)],
+    "jac_sn": [("jac_sn_k", 0.5)],
+    "jac_cn": [("jac_cn_k", 0.5)],
+    "jac_dn": [("jac_dn_k", 0.5)],
+    "xheart_blur_wf": [("angle", 0.0), ("ratio", 0.0)],
+    "affine3D": [("translateX", 0.0), ("translateY", 0.0), ("translateZ", 0.0), ("scaleX", 1.0), ("scaleY", 1.0), ("scaleZ", 1.0), ("rotateX", 0.0), ("rotateY", 0.0), ("rotateZ", 0.0), ("shearXY", 0.0), ("shearXZ", 0.0), ("shearYX", 0.0), ("shearYZ", 0.0), ("shearZX", 0.0), ("shearZY", 0.0)],
+    "z": [("hypergon", 0.0), ("hypergon_n", 4.0), ("hypergon_r", 1.0), ("star", 0.0), ("star_n", 5.0), ("star_slope", 2.0), ("lituus", 0.0), ("lituus_a", 1.0), ("super_shape", 0.0), ("super_m", 1.0), ("super_n1", 1.0), ("super_n2", 1.0), ("super_n3", 0.0)],
+    "w": [("angle", 0.0), ("hypergon", 0.0), ("hypergon_n", 4.0), ("hypergon_r", 1.0), ("star", 0.0), ("star_n", 5.0), ("star_slope", 2.0), ("lituus", 0.0), ("lituus_a", 1.0), ("super_shape", 0.0), ("super_m", 1.0), ("super_n1", 1.0), ("super_n2", 1.0), ("super_n3", 0.0)],
+    "harmonograph_js": [("seed", 1234.0), ("time", 100.0), ("a1", 0.0), ("f1", 0.0), ("p1", 0.0), ("d1", 0.0), ("a2", 0.0), ("f2", 0.0), ("p2", 0.0), ("d2", 0.0), ("a3", 0.0), ("f3", 0.0), ("p3", 0.0), ("d3", 0.0), ("a4", 0.0), ("f4", 0.0), ("p4", 0.0), ("d4", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)
