@@ -359,6 +359,29 @@ void derive_wz(const float* u, float* o, int h) {
 }
 void derive_z(const float* u, float* o) { derive_wz(u, o, 0); }
 void derive_w(const float* u, float* o) { derive_wz(u, o, 1); }
+void derive_loonie2(const float* u, float* o) {                 // watchlist_misc.rs (init_loonie2), apo_misc13.rs (init_scry2)
+    const float a = 6.28318530717959f / std::fmax(u[0], 1.0f), as = -1.5707963267948966f * u[1], ac = 1.5707963267948966f * u[2];
+    o[0] = std::sin(a); o[1] = std::cos(a); o[2] = std::sin(as); o[3] = std::cos(as); o[4] = std::sin(ac); o[5] = std::cos(ac);
+}
+void derive_elliptic2(const float* u, float* o) { o[0] = u[10] * 0.31830988618379f; }   // erf_misc.rs (init_elliptic2)
+void derive_asteria(const float* u, float* o) {                 // apo_misc7.rs (init_asteria)
+    o[0] = std::sin(3.14159265358979f * u[0]); o[1] = std::cos(3.14159265358979f * u[0]);
+}
+void derive_bwraps2(const float* u, float* o) {                 // bwraps2_phase.rs (init_pre_bwraps2, init_post_bwraps2)
+    if (std::fabs(u[0]) < 1e-30f) { o[0] = o[1] = o[2] = 0.0f; return; }
+    const float radius = 0.5f * (u[0] / (1.0f + u[1] * u[1])), g2 = u[2] * u[2] / u[0] + 1e-6f;
+    float mb = g2 * radius;
+    mb = mb > 2.0f ? 1.0f : mb * (1.0f / ((mb * mb) * 0.25f + 1.0f));
+    o[0] = g2; o[1] = radius * radius; o[2] = radius / std::fmax(mb, 1e-30f);
+}
+void derive_post_rblur(const float* u, float* o) { o[0] = 2.0f * u[0]; }   // post_rblur_misc.rs (init_post_rblur)
+void derive_cpow3_wf(const float* u, float* o) {                // apo_misc22.rs (init_cpow3_wf)
+    const float pi = 3.14159265358979f, two_pi = 6.28318530717959f;
+    const float div = std::fabs(u[2]) < 1e-30f ? 1e-30f : u[2], spr = std::fabs(u[3]) < 1e-30f ? 1e-30f : u[3];
+    const float c = u[0] * std::cos(pi * 0.5f * u[1]) / div, d = u[0] * std::sin(pi * 0.5f * u[1]) / div;
+    o[0] = c; o[1] = d; o[2] = c * 0.5f; o[3] = d * 0.5f; o[4] = two_pi / div; o[5] = 0.5f / spr; o[6] = two_pi * u[3];
+}
+void derive_pre_rect_wf(const float* u, float* o) { o[0] = u[1] - u[0]; o[1] = u[3] - u[2]; }   // dc_misc2.rs (init_pre_rect_wf)
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -655,6 +678,7 @@ static const VarDef kRegistry[] = {
     {"flux", 307, 0, 1, {"spread"}, {0.3f}, "v_flux", VF_W, 0, nullptr},
     {"rays", 308, 1, 0, NP, ND, "v_rays", VF_W, 0, nullptr},
     {"rays1", 309, 0, 0, NP, ND, "v_rays1", VF_W | VF_REPLACE, 0, nullptr},
+    {"loonie2", 310, 0, 3, {"sides", "star", "circle"}, {4.0f, 0.0f, 0.0f}, "v_loonie2", VF_W, 6, derive_loonie2},
     {"fourth", 311, 0, 5, {"spin", "space", "twist", "x", "y"}, {3.14159265f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_fourth", VF_W, 0, nullptr},
     {"arch", 312, 1, 0, NP, ND, "v_arch", VF_W, 0, nullptr},
     {"bi_linear", 313, 0, 0, NP, ND, "v_bi_linear", 0, 0, nullptr},
@@ -680,6 +704,7 @@ static const VarDef kRegistry[] = {
     {"deltaA", 336, 0, 0, NP, ND, "v_deltaA", VF_W, 0, nullptr},
     {"edisc", 337, 0, 0, NP, ND, "v_edisc", VF_W, 0, nullptr},
     {"curve", 338, 0, 4, {"xamp", "yamp", "xlength", "ylength"}, {0.25f, 0.5f, 1.0f, 1.0f}, "v_curve", 0, 2, derive_curve},
+    {"elliptic2", 339, 1, 11, {"a1", "a2", "a3", "b1", "b2", "c", "d", "e", "f", "g", "h"}, {1.0f, 1.0f, 0.0f, 2.0f, 1.0f, 0.5f, 1.0f, 0.5f, 1.0f, 1.0f, 2.0f}, "v_elliptic2", VF_W, 1, derive_elliptic2},
     {"exp2", 340, 0, 0, NP, ND, "v_exp2", 0, 0, nullptr},
     {"exponential", 341, 0, 0, NP, ND, "v_exponential", 0, 0, nullptr},
     {"flipy", 342, 0, 0, NP, ND, "v_flipy", 0, 0, nullptr},
@@ -696,6 +721,7 @@ static const VarDef kRegistry[] = {
     {"inflateZ_6", 353, 0, 0, NP, ND, "v_inflateZ_6", 0, 0, nullptr},
     {"sintrange", 354, 0, 1, {"w"}, {1.0f}, "v_sintrange", VF_REPLACE, 0, nullptr},
     {"foci_3D", 355, 0, 0, NP, ND, "v_foci_3D", 0, 0, nullptr},
+    {"asteria", 356, 1, 1, {"alpha"}, {0.0f}, "v_asteria", VF_W, 2, derive_asteria},
     {"estiq", 357, 0, 0, NP, ND, "v_estiq", 0, 0, nullptr},
     {"fdisc", 358, 0, 8, {"ashift", "rshift", "xshift", "yshift", "term1", "term2", "term3", "term4"}, {1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_fdisc", 0, 0, nullptr},
     {"bTransform", 359, 1, 4, {"rotate", "power", "move", "split"}, {0.0f, 1.0f, 0.0f, 0.0f}, "v_bTransform", 0, 0, nullptr},
@@ -724,6 +750,7 @@ static const VarDef kRegistry[] = {
     {"stripfit", 382, 0, 1, {"dx"}, {1.0f}, "v_stripfit", VF_W, 0, nullptr},
     {"q_ode", 383, 0, 12, {"q_ode01", "q_ode02", "q_ode03", "q_ode04", "q_ode05", "q_ode06", "q_ode07", "q_ode08", "q_ode09", "q_ode10", "q_ode11", "q_ode12"}, {0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_q_ode", VF_W, 0, nullptr},
     {"ripple", 384, 0, 8, {"frequency", "velocity", "amplitude", "centerx", "centery", "phase", "scale", "fixed_dist_calc"}, {2.0f, 1.0f, 0.5f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_ripple", VF_REPLACE, 6, derive_ripple},
+    {"scry2", 385, 0, 3, {"sides", "star", "circle"}, {4.0f, 0.0f, 0.0f}, "v_scry2", VF_W, 6, derive_loonie2},
     {"pre_spin_z", 386, 0, 0, NP, ND, "v_pre_spin_z", VF_PRE | VF_W, 0, nullptr},
     {"post_spin_z", 387, 0, 0, NP, ND, "v_post_spin_z", VF_POST | VF_W, 0, nullptr},
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
@@ -736,7 +763,10 @@ static const VarDef kRegistry[] = {
     {"seashell3D", 397, 2, 4, {"final_radius", "height", "inner_radius", "nSpirals"}, {0.25f, 3.5f, 0.4f, 3.0f}, "v_seashell3D", 0, 0, nullptr},
     {"bwraps7", 399, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_bwraps7", 0, 3, derive_bwraps7},
     {"loq", 400, 0, 1, {"base"}, {2.718281828459045f}, "v_loq", 0, 0, nullptr},
+    {"pre_bwraps2", 402, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_pre_bwraps2", VF_PRE | VF_W, 3, derive_bwraps2},
+    {"post_bwraps2", 403, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_pre_bwraps2", VF_POST | VF_W, 3, derive_bwraps2},
     {"post_heat", 404, 0, 9, {"theta_period", "theta_phase", "theta_amp", "phi_period", "phi_phase", "phi_amp", "r_period", "r_phase", "r_amp"}, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_post_heat", VF_POST | VF_W, 0, nullptr},
+    {"post_rblur", 405, 2, 4, {"strength", "offset", "center_x", "center_y"}, {1.0f, 1.0f, 0.0f, 1.0f}, "v_post_rblur", VF_POST | VF_W, 1, derive_post_rblur},
     {"onion2", 406, 0, 8, {"meeting_pt", "circle_a", "circle_b", "shift_x", "shift_y", "shift_z", "top_crop", "stretch"}, {0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_onion2", VF_W, 0, nullptr},
     {"jac_sn", 407, 0, 1, {"jac_sn_k"}, {0.5f}, "v_jac_sn", 0, 0, nullptr},
     {"jac_cn", 408, 0, 1, {"jac_cn_k"}, {0.5f}, "v_jac_cn", 0, 0, nullptr},
@@ -754,6 +784,7 @@ static const VarDef kRegistry[] = {
     {"spherical3D_wf", 427, 0, 2, {"invert", "exponent"}, {0.0f, 2.0f}, "v_spherical3D_wf", 0, 1, derive_spherical3D_wf},
     {"heart_wf", 429, 0, 5, {"scale_x", "scale_t", "shift_t", "scale_r_left", "scale_r_right"}, {1.0f, 1.0f, 0.0f, 1.0f, 1.0f}, "v_heart_wf", 0, 0, nullptr},
     {"post_ztranslate_wf", 430, 0, 0, NP, ND, "v_post_ztranslate_wf", VF_POST, 0, nullptr},
+    {"cpow3_wf", 434, 3, 7, {"r", "a", "divisor", "spread", "discrete_spread", "spread2", "offset2"}, {1.0f, 0.1f, 1.0f, 1.0f, 1.0f, 0.0f, 1.0f}, "v_cpow3_wf", 0, 7, derive_cpow3_wf},
     {"clifford_js", 435, 0, 4, {"a", "b", "c", "d"}, {-1.4f, 1.6f, 1.0f, 0.7f}, "v_clifford_js", 0, 0, nullptr},
     {"svensson_js", 436, 0, 4, {"a", "b", "c", "d"}, {1.4f, 1.56f, 1.4f, -6.56f}, "v_svensson_js", VF_REPLACE, 0, nullptr},
     {"sattractor_js", 437, 2, 1, {"m"}, {10.0f}, "v_sattractor_js", 0, 0, nullptr},
@@ -772,6 +803,7 @@ static const VarDef kRegistry[] = {
     {"waves4_wf", 454, 0, 8, {"scalex", "scaley", "freqx", "freqy", "use_cos_x", "use_cos_y", "dampx", "dampy"}, {0.25f, 0.5f, 1.5707963267948966f, 0.7853981633974483f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_waves4_wf", 0, 2, derive_waves_wf},
     {"dinis_surface_wf", 455, 0, 2, {"a", "b"}, {0.8f, 0.2f}, "v_dinis_surface_wf", 0, 0, nullptr},
     {"apocarpet_js", 458, 1, 0, NP, ND, "v_apocarpet_js", 0, 0, nullptr},
+    {"pre_rect_wf", 463, 2, 4, {"x0", "x1", "y0", "y1"}, {-0.5f, 0.5f, -0.5f, 0.5f}, "v_pre_rect_wf", VF_PRE | VF_W, 2, derive_pre_rect_wf},
     {"affine3D", 464, 0, 15, {"translateX", "translateY", "translateZ", "scaleX", "scaleY", "scaleZ", "rotateX", "rotateY", "rotateZ", "shearXY", "shearXZ", "shearYX", "shearYZ", "shearZX", "shearZY"}, {0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_affine3D", 0, 7, derive_affine3D},
     {"pre_wave3D_wf", 468, 0, 7, {"axis", "wavelen", "phase", "damping", "centre_x", "centre_y", "centre_z"}, {0.0f, 0.5f, 0.0f, 0.01f, 0.0f, 0.0f, 0.0f}, "v_pre_wave3D_wf", VF_PRE | VF_W, 0, nullptr},
     {"siercarpet_js", 473, 1, 1, {"m"}, {3.0f}, "v_siercarpet_js", 0, 0, nullptr},

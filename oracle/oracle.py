@@ -326,6 +326,15 @@ REGISTRY = {
     "z": 489,
     "w": 490,
     "harmonograph_js": 496,
+    "loonie2": 310,
+    "elliptic2": 339,
+    "asteria": 356,
+    "scry2": 385,
+    "pre_bwraps2": 402,
+    "post_bwraps2": 403,
+    "post_rblur": 405,
+    "cpow3_wf": 434,
+    "pre_rect_wf": 463,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -632,6 +641,17 @@ PARAMS.update({
     "z": [("hypergon", 0.0), ("hypergon_n", 4.0), ("hypergon_r", 1.0), ("star", 0.0), ("star_n", 5.0), ("star_slope", 2.0), ("lituus", 0.0), ("lituus_a", 1.0), ("super_shape", 0.0), ("super_m", 1.0), ("super_n1", 1.0), ("super_n2", 1.0), ("super_n3", 0.0)],
     "w": [("angle", 0.0), ("hypergon", 0.0), ("hypergon_n", 4.0), ("hypergon_r", 1.0), ("star", 0.0), ("star_n", 5.0), ("star_slope", 2.0), ("lituus", 0.0), ("lituus_a", 1.0), ("super_shape", 0.0), ("super_m", 1.0), ("super_n1", 1.0), ("super_n2", 1.0), ("super_n3", 0.0)],
     "harmonograph_js": [("seed", 1234.0), ("time", 100.0), ("a1", 0.0), ("f1", 0.0), ("p1", 0.0), ("d1", 0.0), ("a2", 0.0), ("f2", 0.0), ("p2", 0.0), ("d2", 0.0), ("a3", 0.0), ("f3", 0.0), ("p3", 0.0), ("d3", 0.0), ("a4", 0.0), ("f4", 0.0), ("p4", 0.0), ("d4", 0.0)],
+})
+PARAMS.update({
+    "loonie2": [("sides", 4.0), ("star", 0.0), ("circle", 0.0)],
+    "elliptic2": [("a1", 1.0), ("a2", 1.0), ("a3", 0.0), ("b1", 2.0), ("b2", 1.0), ("c", 0.5), ("d", 1.0), ("e", 0.5), ("f", 1.0), ("g", 1.0), ("h", 2.0)],
+    "asteria": [("alpha", 0.0)],
+    "scry2": [("sides", 4.0), ("star", 0.0), ("circle", 0.0)],
+    "pre_bwraps2": [("cellsize", 1.0), ("space", 0.0), ("gain", 2.0), ("inner_twist", 0.0), ("outer_twist", 0.0)],
+    "post_bwraps2": [("cellsize", 1.0), ("space", 0.0), ("gain", 2.0), ("inner_twist", 0.0), ("outer_twist", 0.0)],
+    "post_rblur": [("strength", 1.0), ("offset", 1.0), ("center_x", 0.0), ("center_y", 1.0)],
+    "cpow3_wf": [("r", 1.0), ("a", 0.1), ("divisor", 1.0), ("spread", 1.0), ("discrete_spread", 1.0), ("spread2", 0.0), ("offset2", 1.0)],
+    "pre_rect_wf": [("x0", -0.5), ("x1", 0.5), ("y0", -0.5), ("y1", 0.5)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

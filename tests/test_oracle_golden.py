@@ -307,6 +307,7 @@ WIDER = {
     "jac_cn": {"tiny": "tiny-branch", **dict.fromkeys(HUGE_ARGS, "huge")},
     "jac_dn": {"tiny": "tiny-branch", **dict.fromkeys(HUGE_ARGS, "huge")},
     "z": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
+    "cpow3_wf": {"half_unit": "zero"},
     "gamma": dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "half_unit", "y_neg0x", "neg0y_x"], "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
@@ -342,7 +343,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "sph3D", "pre_blur3D", "extrude", "post_ztranslate_wf", "bubble_wf", "solid_sphere",
                        "matrix3D", "onion", "octagon", "xerf", "erf3D", "spherical3D_wf", "pre_wave3D_wf",
                        "hypertile3D", "voron", "minkQM", "poincare3D", "rosoni", "bwraps7", "curl_sp", "circleLinear",
-                       "mobiq", "xheart_blur_wf", "affine3D", "w", "harmonograph_js"])
+                       "mobiq", "xheart_blur_wf", "affine3D", "w", "harmonograph_js",
+                       "loonie2", "elliptic2", "asteria", "scry2", "pre_bwraps2", "post_bwraps2", "pre_rect_wf"])
 
 
 def golden():
