@@ -764,7 +764,7 @@ static const VarDef kRegistry[] = {
     {"bwraps7", 399, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_bwraps7", 0, 3, derive_bwraps7},
     {"loq", 400, 0, 1, {"base"}, {2.718281828459045f}, "v_loq", 0, 0, nullptr},
     {"pre_bwraps2", 402, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_pre_bwraps2", VF_PRE | VF_W, 3, derive_bwraps2},
-    {"post_bwraps2", 403, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_pre_bwraps2", VF_POST | VF_W, 3, derive_bwraps2},
+    {"post_bwraps2", 403, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_post_bwraps2", VF_POST | VF_W, 3, derive_bwraps2},
     {"post_heat", 404, 0, 9, {"theta_period", "theta_phase", "theta_amp", "phi_period", "phi_phase", "phi_amp", "r_period", "r_phase", "r_amp"}, {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_post_heat", VF_POST | VF_W, 0, nullptr},
     {"post_rblur", 405, 2, 4, {"strength", "offset", "center_x", "center_y"}, {1.0f, 1.0f, 0.0f, 1.0f}, "v_post_rblur", VF_POST | VF_W, 1, derive_post_rblur},
     {"onion2", 406, 0, 8, {"meeting_pt", "circle_a", "circle_b", "shift_x", "shift_y", "shift_z", "top_crop", "stretch"}, {0.5f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_onion2", VF_W, 0, nullptr},
