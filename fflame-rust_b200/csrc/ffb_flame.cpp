@@ -382,6 +382,22 @@ void derive_cpow3_wf(const float* u, float* o) {                // apo_misc22.rs
     o[0] = c; o[1] = d; o[2] = c * 0.5f; o[3] = d * 0.5f; o[4] = two_pi / div; o[5] = 0.5f / spr; o[6] = two_pi * u[3];
 }
 void derive_pre_rect_wf(const float* u, float* o) { o[0] = u[1] - u[0]; o[1] = u[3] - u[2]; }   // dc_misc2.rs (init_pre_rect_wf)
+void derive_spliptic_bs(const float*, float* o) { o[0] = 0.6366197723675814f; }   // apo_misc14.rs (init_spliptic_bs)
+void derive_pointgrid_wf(const float* u, float* o) {            // pointgrid_misc.rs (init_pointgrid_wf)
+    o[0] = (u[1] - u[0]) / std::fmax(u[2], 1.0f); o[1] = (u[4] - u[3]) / std::fmax(u[5], 1.0f);
+}
+void derive_bubbleT3D(const float* u, float* o) {               // bubblet3d_misc.rs (init_bubbleT3D)
+    const float pi = 3.14159265358979f, two_pi = 6.28318530717959f, as = std::fabs(u[0]);
+    const float ratio = std::fmin(std::fmax(u[1], 0.01f), 1.99f);
+    float s = 0.0f, s1 = 0.0f, s2 = 0.0f;
+    if (as > 0.5f) { s = pi / as; s2 = 2.0f * s; s1 = ratio * s; }
+    float ah = u[2];
+    if (u[4] > 0.5f) ah = std::fmin(std::fabs(ah), 179.9f);
+    const float inv_hole = ah < 0.0f ? 1.0f : 0.0f;
+    float ae = std::fabs(ah);
+    ae = inv_hole > 0.5f ? (ae / 360.0f * two_pi) * 0.5f : pi - (ae / 360.0f * two_pi) * 0.5f;
+    o[0] = pi - ae; o[1] = s; o[2] = s1; o[3] = s2; o[4] = u[0] < 0.0f ? 1.0f : 0.0f; o[5] = inv_hole; o[6] = ae;
+}
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -756,6 +772,7 @@ static const VarDef kRegistry[] = {
     {"post_spherical", 388, 0, 0, NP, ND, "v_post_spherical", VF_POST | VF_W, 0, nullptr},
     {"pre_disc3d", 389, 0, 1, {"pi"}, {3.141592653589793f}, "v_pre_disc3d", VF_PRE | VF_W, 0, nullptr},
     {"waves2_radial", 390, 0, 6, {"w2r_scalex", "w2r_scaley", "w2r_freqx", "w2r_freqy", "w2r_null", "w2r_distance"}, {0.1f, 0.1f, 7.0f, 13.0f, 2.0f, 10.0f}, "v_waves2_radial", 0, 0, nullptr},
+    {"spliptic_bs", 391, 1, 2, {"x", "y"}, {0.05f, 0.05f}, "v_spliptic_bs", VF_W, 1, derive_spliptic_bs},
     {"poincare3D", 392, 0, 3, {"r", "a", "b"}, {0.0f, 0.0f, 0.0f}, "v_poincare3D", 0, 10, derive_poincare3D},
     {"pre_sinusoidal3d", 393, 0, 0, NP, ND, "v_pre_sinusoidal3d", VF_PRE | VF_W, 0, nullptr},
     {"pre_blur3D", 394, 8, 0, NP, ND, "v_pre_blur3D", VF_PRE | VF_W, 0, nullptr},
@@ -802,14 +819,17 @@ static const VarDef kRegistry[] = {
     {"waves3_wf", 453, 0, 8, {"scalex", "scaley", "freqx", "freqy", "use_cos_x", "use_cos_y", "dampx", "dampy"}, {0.25f, 0.5f, 1.5707963267948966f, 0.7853981633974483f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_waves3_wf", 0, 2, derive_waves_wf},
     {"waves4_wf", 454, 0, 8, {"scalex", "scaley", "freqx", "freqy", "use_cos_x", "use_cos_y", "dampx", "dampy"}, {0.25f, 0.5f, 1.5707963267948966f, 0.7853981633974483f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_waves4_wf", 0, 2, derive_waves_wf},
     {"dinis_surface_wf", 455, 0, 2, {"a", "b"}, {0.8f, 0.2f}, "v_dinis_surface_wf", 0, 0, nullptr},
+    {"pointgrid_wf", 456, 2, 8, {"xmin", "xmax", "xcount", "ymin", "ymax", "ycount", "distortion", "seed"}, {-3.0f, 3.0f, 32.0f, -3.0f, 3.0f, 32.0f, 2.3f, 1234.0f}, "v_pointgrid_wf", 0, 2, derive_pointgrid_wf},
     {"apocarpet_js", 458, 1, 0, NP, ND, "v_apocarpet_js", 0, 0, nullptr},
     {"pre_rect_wf", 463, 2, 4, {"x0", "x1", "y0", "y1"}, {-0.5f, 0.5f, -0.5f, 0.5f}, "v_pre_rect_wf", VF_PRE | VF_W, 2, derive_pre_rect_wf},
     {"affine3D", 464, 0, 15, {"translateX", "translateY", "translateZ", "scaleX", "scaleY", "scaleZ", "rotateX", "rotateY", "rotateZ", "shearXY", "shearXZ", "shearYX", "shearYZ", "shearZX", "shearZY"}, {0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_affine3D", 0, 7, derive_affine3D},
+    {"truchet2", 465, 0, 7, {"exponent1", "exponent2", "width1", "width2", "scale", "seed", "inverse"}, {1.0f, 2.0f, 0.5f, 0.5f, 10.0f, 50.0f, 0.0f}, "v_truchet2", 0, 0, nullptr},
     {"pre_wave3D_wf", 468, 0, 7, {"axis", "wavelen", "phase", "damping", "centre_x", "centre_y", "centre_z"}, {0.0f, 0.5f, 0.0f, 0.01f, 0.0f, 0.0f, 0.0f}, "v_pre_wave3D_wf", VF_PRE | VF_W, 0, nullptr},
     {"siercarpet_js", 473, 1, 1, {"m"}, {3.0f}, "v_siercarpet_js", 0, 0, nullptr},
     {"popcorn2_3D", 474, 0, 4, {"popcorn2_3D_x", "popcorn2_3D_y", "popcorn2_3D_z", "popcorn2_3D_c"}, {0.1f, 0.1f, 0.1f, 3.0f}, "v_popcorn2_3D", 0, 0, nullptr},
     {"plusrecip", 476, 0, 2, {"ar", "ai"}, {4.0f, 0.0f}, "v_plusrecip", 0, 0, nullptr},
     {"gamma", 477, 0, 0, NP, ND, "v_gamma", 0, 0, nullptr},
+    {"bubbleT3D", 478, 0, 6, {"number_of_stripes", "ratio_of_stripes", "angle_of_hole", "exponent_z", "symmetry_z", "modus_blur"}, {0.0f, 1.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_bubbleT3D", 0, 7, derive_bubbleT3D},
     {"z", 489, 0, 13, {"hypergon", "hypergon_n", "hypergon_r", "star", "star_n", "star_slope", "lituus", "lituus_a", "super_shape", "super_m", "super_n1", "super_n2", "super_n3"}, {0.0f, 4.0f, 1.0f, 0.0f, 5.0f, 2.0f, 0.0f, 1.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_z", 0, 7, derive_z},
     {"w", 490, 0, 14, {"angle", "hypergon", "hypergon_n", "hypergon_r", "star", "star_n", "star_slope", "lituus", "lituus_a", "super_shape", "super_m", "super_n1", "super_n2", "super_n3"}, {0.0f, 0.0f, 4.0f, 1.0f, 0.0f, 5.0f, 2.0f, 0.0f, 1.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_w", 0, 7, derive_w},
     {"harmonograph_js", 496, 1, 18, {"seed", "time", "a1", "f1", "p1", "d1", "a2", "f2", "p2", "d2", "a3", "f3", "p3", "d3", "a4", "f4", "p4", "d4"}, {1234.0f, 100.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_harmonograph_js", 0, 0, nullptr},
@@ -845,6 +865,7 @@ static const VarDef kRegistry[] = {
     {"sym_bg5", 565, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg5", 0, 0, nullptr},
     {"sym_bg6", 566, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg6", 0, 0, nullptr},
     {"sym_bg7", 567, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg7", 0, 0, nullptr},
+    {"pRose3D", 568, 2, 16, {"l", "k", "c", "z1", "z2", "refSc", "opt", "optSc", "opt3", "transp", "dist", "wagsc", "srvsc", "f", "wigsc", "offset"}, {1.0f, 6.0f, 0.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.5f, 1.0f, 0.0f, 0.0f, 3.0f, 0.0f, 0.0f}, "v_pRose3D", 0, 0, nullptr},
     {"solid_sphere", 605, 2, 5, {"radius", "thickness", "cx", "cy", "cz"}, {1.0f, 0.1f, 0.0f, 0.0f, 0.0f}, "v_solid_sphere", 0, 0, nullptr},
     {"matrix3D", 643, 0, 12, {"xx", "xy", "xz", "yx", "yy", "yz", "zx", "zy", "zz", "tx", "ty", "tz"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_matrix3D", 0, 0, nullptr},};
 #undef NP

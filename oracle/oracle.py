@@ -335,6 +335,11 @@ REGISTRY = {
     "post_rblur": 405,
     "cpow3_wf": 434,
     "pre_rect_wf": 463,
+    "spliptic_bs": 391,
+    "pointgrid_wf": 456,
+    "truchet2": 465,
+    "bubbleT3D": 478,
+    "pRose3D": 568,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -652,6 +657,13 @@ PARAMS.update({
     "post_rblur": [("strength", 1.0), ("offset", 1.0), ("center_x", 0.0), ("center_y", 1.0)],
     "cpow3_wf": [("r", 1.0), ("a", 0.1), ("divisor", 1.0), ("spread", 1.0), ("discrete_spread", 1.0), ("spread2", 0.0), ("offset2", 1.0)],
     "pre_rect_wf": [("x0", -0.5), ("x1", 0.5), ("y0", -0.5), ("y1", 0.5)],
+})
+PARAMS.update({
+    "spliptic_bs": [("x", 0.05), ("y", 0.05)],
+    "pointgrid_wf": [("xmin", -3.0), ("xmax", 3.0), ("xcount", 32.0), ("ymin", -3.0), ("ymax", 3.0), ("ycount", 32.0), ("distortion", 2.3), ("seed", 1234.0)],
+    "truchet2": [("exponent1", 1.0), ("exponent2", 2.0), ("width1", 0.5), ("width2", 0.5), ("scale", 10.0), ("seed", 50.0), ("inverse", 0.0)],
+    "bubbleT3D": [("number_of_stripes", 0.0), ("ratio_of_stripes", 1.0), ("angle_of_hole", 0.0), ("exponent_z", 1.0), ("symmetry_z", 0.0), ("modus_blur", 0.0)],
+    "pRose3D": [("l", 1.0), ("k", 6.0), ("c", 0.0), ("z1", 1.0), ("z2", 1.0), ("refSc", 1.0), ("opt", 1.0), ("optSc", 1.0), ("opt3", 0.0), ("transp", 0.5), ("dist", 1.0), ("wagsc", 0.0), ("srvsc", 0.0), ("f", 3.0), ("wigsc", 0.0), ("offset", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -308,6 +308,9 @@ WIDER = {
     "jac_dn": {"tiny": "tiny-branch", **dict.fromkeys(HUGE_ARGS, "huge")},
     "z": dict.fromkeys(["-x", "+y", "-y", "neg0y_x"], "zero"),
     "cpow3_wf": {"half_unit": "zero"},
+    # pRose3D: cos(6 th) at multiples of pi / 4 and its reflections; the reference's cos rounds to either sign.
+    "pRose3D": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "q1", "q2", "q3", "q4", "half_unit", "tiny", "normal_min",
+                              "large", "near_threshold", "past_threshold", "neg0y_x"], "zero"),
     "gamma": dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "half_unit", "y_neg0x", "neg0y_x"], "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
@@ -344,7 +347,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "matrix3D", "onion", "octagon", "xerf", "erf3D", "spherical3D_wf", "pre_wave3D_wf",
                        "hypertile3D", "voron", "minkQM", "poincare3D", "rosoni", "bwraps7", "curl_sp", "circleLinear",
                        "mobiq", "xheart_blur_wf", "affine3D", "w", "harmonograph_js",
-                       "loonie2", "elliptic2", "asteria", "scry2", "pre_bwraps2", "post_bwraps2", "pre_rect_wf"])
+                       "loonie2", "elliptic2", "asteria", "scry2", "pre_bwraps2", "post_bwraps2", "pre_rect_wf",
+                       "spliptic_bs", "pointgrid_wf", "truchet2", "bubbleT3D"])
 
 
 def golden():
