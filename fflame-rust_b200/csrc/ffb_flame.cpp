@@ -398,6 +398,30 @@ void derive_bubbleT3D(const float* u, float* o) {               // bubblet3d_mis
     ae = inv_hole > 0.5f ? (ae / 360.0f * two_pi) * 0.5f : pi - (ae / 360.0f * two_pi) * 0.5f;
     o[0] = pi - ae; o[1] = s; o[2] = s1; o[3] = s2; o[4] = u[0] < 0.0f ? 1.0f : 0.0f; o[5] = inv_hole; o[6] = ae;
 }
+// hypertile3D1, hypertile3D2 (hypertile.rs init_hypertile3D1, 2): the tile
+// angle 2 pi / p and the tile centre's distance r.
+void ffb_hypertile3_r(const float* u, float& pa, float& r) {
+    const float pi = 3.14159265358979f, qa = 2.0f * pi / u[1];
+    pa = 2.0f * pi / u[0];
+    const float r_alt = -(std::cos(pa) - 1.0f) / (std::cos(pa) + std::cos(qa));
+    r = r_alt > 0.0f ? 1.0f / std::sqrt(1.0f + r_alt) : 1.0f;
+}
+void derive_hypertile3D1(const float* u, float* o) {
+    float pa, r;
+    ffb_hypertile3_r(u, pa, r);
+    o[0] = pa; o[1] = r; o[2] = r * r; o[3] = 1.0f - r * r;
+}
+void derive_hypertile3D2(const float* u, float* o) {
+    float pa, r;
+    ffb_hypertile3_r(u, pa, r);
+    const float cx2 = r * r;
+    o[0] = pa; o[1] = r; o[2] = cx2; o[3] = 2.0f * r; o[4] = 1.0f + cx2; o[5] = 1.0f - cx2; o[6] = 1.0f - cx2;
+}
+void derive_julian3Dx(const float* u, float* o) {               // apo_misc15.rs (init_julian3Dx)
+    const float p = std::fabs(u[0]) < 1e-30f ? 1.0f : u[0];
+    o[0] = std::fabs(p); o[1] = (u[1] / p - 1.0f) * 0.5f;
+}
+void derive_waves2b(const float* u, float* o) { o[0] = u[4] - u[5]; o[1] = u[6] - u[7]; }   // waves2b_misc.rs (init_waves2b)
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -588,6 +612,8 @@ static const VarDef kRegistry[] = {
     {"hypertile1", 185, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile1", 0, 2, derive_hypertile1},
     {"hypertile2", 186, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile2", 0, 2, derive_hypertile2},
     {"hypertile3D", 187, 0, 3, {"p", "q", "n"}, {3.0f, 7.0f, 0.0f}, "v_hypertile3D", 0, 8, derive_hypertile3D},
+    {"hypertile3D1", 188, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile3D1", 0, 4, derive_hypertile3D1},
+    {"hypertile3D2", 189, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypertile3D2", 0, 7, derive_hypertile3D2},
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
     {"gridout", 192, 0, 0, NP, ND, "v_gridout", 0, 0, nullptr},
@@ -776,6 +802,7 @@ static const VarDef kRegistry[] = {
     {"poincare3D", 392, 0, 3, {"r", "a", "b"}, {0.0f, 0.0f, 0.0f}, "v_poincare3D", 0, 10, derive_poincare3D},
     {"pre_sinusoidal3d", 393, 0, 0, NP, ND, "v_pre_sinusoidal3d", VF_PRE | VF_W, 0, nullptr},
     {"pre_blur3D", 394, 8, 0, NP, ND, "v_pre_blur3D", VF_PRE | VF_W, 0, nullptr},
+    {"julian3Dx", 395, 1, 8, {"power", "dist", "a", "b", "c", "d", "e", "f"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_julian3Dx", VF_W, 2, derive_julian3Dx},
     {"rosoni", 396, 0, 7, {"maxiter", "sweetiter", "altshapes", "cutoff", "radius", "dx", "dy"}, {25.0f, 3.0f, 0.0f, 1.0f, 0.4f, 0.6f, 0.0f}, "v_rosoni", 0, 2, derive_rosoni},
     {"seashell3D", 397, 2, 4, {"final_radius", "height", "inner_radius", "nSpirals"}, {0.25f, 3.5f, 0.4f, 3.0f}, "v_seashell3D", 0, 0, nullptr},
     {"bwraps7", 399, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_bwraps7", 0, 3, derive_bwraps7},
@@ -830,6 +857,7 @@ static const VarDef kRegistry[] = {
     {"plusrecip", 476, 0, 2, {"ar", "ai"}, {4.0f, 0.0f}, "v_plusrecip", 0, 0, nullptr},
     {"gamma", 477, 0, 0, NP, ND, "v_gamma", 0, 0, nullptr},
     {"bubbleT3D", 478, 0, 6, {"number_of_stripes", "ratio_of_stripes", "angle_of_hole", "exponent_z", "symmetry_z", "modus_blur"}, {0.0f, 1.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_bubbleT3D", 0, 7, derive_bubbleT3D},
+    {"waves2b", 479, 0, 10, {"freqx", "freqy", "pwx", "pwy", "scalex", "scaleinfx", "scaley", "scaleinfy", "unity", "jacok"}, {2.0f, 2.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.25f}, "v_waves2b", 0, 2, derive_waves2b},
     {"z", 489, 0, 13, {"hypergon", "hypergon_n", "hypergon_r", "star", "star_n", "star_slope", "lituus", "lituus_a", "super_shape", "super_m", "super_n1", "super_n2", "super_n3"}, {0.0f, 4.0f, 1.0f, 0.0f, 5.0f, 2.0f, 0.0f, 1.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_z", 0, 7, derive_z},
     {"w", 490, 0, 14, {"angle", "hypergon", "hypergon_n", "hypergon_r", "star", "star_n", "star_slope", "lituus", "lituus_a", "super_shape", "super_m", "super_n1", "super_n2", "super_n3"}, {0.0f, 0.0f, 4.0f, 1.0f, 0.0f, 5.0f, 2.0f, 0.0f, 1.0f, 0.0f, 1.0f, 1.0f, 1.0f, 0.0f}, "v_w", 0, 7, derive_w},
     {"harmonograph_js", 496, 1, 18, {"seed", "time", "a1", "f1", "p1", "d1", "a2", "f2", "p2", "d2", "a3", "f3", "p3", "d3", "a4", "f4", "p4", "d4"}, {1234.0f, 100.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_harmonograph_js", 0, 0, nullptr},

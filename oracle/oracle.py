@@ -340,6 +340,10 @@ REGISTRY = {
     "truchet2": 465,
     "bubbleT3D": 478,
     "pRose3D": 568,
+    "hypertile3D1": 188,
+    "hypertile3D2": 189,
+    "julian3Dx": 395,
+    "waves2b": 479,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -664,6 +668,12 @@ PARAMS.update({
     "truchet2": [("exponent1", 1.0), ("exponent2", 2.0), ("width1", 0.5), ("width2", 0.5), ("scale", 10.0), ("seed", 50.0), ("inverse", 0.0)],
     "bubbleT3D": [("number_of_stripes", 0.0), ("ratio_of_stripes", 1.0), ("angle_of_hole", 0.0), ("exponent_z", 1.0), ("symmetry_z", 0.0), ("modus_blur", 0.0)],
     "pRose3D": [("l", 1.0), ("k", 6.0), ("c", 0.0), ("z1", 1.0), ("z2", 1.0), ("refSc", 1.0), ("opt", 1.0), ("optSc", 1.0), ("opt3", 0.0), ("transp", 0.5), ("dist", 1.0), ("wagsc", 0.0), ("srvsc", 0.0), ("f", 3.0), ("wigsc", 0.0), ("offset", 0.0)],
+})
+PARAMS.update({
+    "hypertile3D1": [("p", 3.0), ("q", 7.0)],
+    "hypertile3D2": [("p", 3.0), ("q", 7.0)],
+    "julian3Dx": [("power", 0.0), ("dist", 1.0), ("a", 1.0), ("b", 0.0), ("c", 0.0), ("d", 1.0), ("e", 0.0), ("f", 0.0)],
+    "waves2b": [("freqx", 2.0), ("freqy", 2.0), ("pwx", 1.0), ("pwy", 1.0), ("scalex", 1.0), ("scaleinfx", 1.0), ("scaley", 1.0), ("scaleinfy", 1.0), ("unity", 1.0), ("jacok", 0.25)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -311,6 +311,7 @@ WIDER = {
     # pRose3D: cos(6 th) at multiples of pi / 4 and its reflections; the reference's cos rounds to either sign.
     "pRose3D": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "q1", "q2", "q3", "q4", "half_unit", "tiny", "normal_min",
                               "large", "near_threshold", "past_threshold", "neg0y_x"], "zero"),
+    "waves2b": dict.fromkeys(["+0+0", "+0-0", "-0+0", "-0-0", "tiny", "normal_min", "subnormal"], "zero"),
     "gamma": dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "half_unit", "y_neg0x", "neg0y_x"], "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
@@ -348,7 +349,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "hypertile3D", "voron", "minkQM", "poincare3D", "rosoni", "bwraps7", "curl_sp", "circleLinear",
                        "mobiq", "xheart_blur_wf", "affine3D", "w", "harmonograph_js",
                        "loonie2", "elliptic2", "asteria", "scry2", "pre_bwraps2", "post_bwraps2", "pre_rect_wf",
-                       "spliptic_bs", "pointgrid_wf", "truchet2", "bubbleT3D"])
+                       "spliptic_bs", "pointgrid_wf", "truchet2", "bubbleT3D",
+                       "hypertile3D1", "hypertile3D2", "julian3Dx"])
 
 
 def golden():
