@@ -422,6 +422,33 @@ void derive_julian3Dx(const float* u, float* o) {               // apo_misc15.rs
     o[0] = std::fabs(p); o[1] = (u[1] / p - 1.0f) * 0.5f;
 }
 void derive_waves2b(const float* u, float* o) { o[0] = u[4] - u[5]; o[1] = u[6] - u[7]; }   // waves2b_misc.rs (init_waves2b)
+void derive_log_db(const float* u, float* o) {                  // exp_log.rs (init_log_db)
+    o[0] = u[0] <= 1e-20f ? 0.5f : 0.5f / std::log(std::fmax(2.71828182845905f * u[0], 1e-20f));
+    o[1] = u[1] <= 1e-20f ? 3.14159265358979f : 3.14159265358979f * u[1];
+}
+void derive_juliaq(const float* u, float* o) {                  // numbered.rs (init_juliaq)
+    const float power = std::fmax(u[0], 1.0f), ip = u[1] / power;
+    o[0] = ip; o[1] = 6.28318530717959f / power; o[2] = 0.5f * ip;
+}
+void derive_julia3Dq(const float* u, float* o) {                // numbered.rs (init_julia3Dq)
+    const float power = std::fmax(u[0], 1.0f), ip = u[1] / power;
+    o[0] = ip; o[1] = 6.28318530717959f / power; o[2] = 0.5f * ip - 0.5f; o[3] = std::fabs(ip);
+}
+void derive_juliac(const float* u, float* o) { o[0] = 1.0f / (u[0] + 1e-30f); o[1] = u[1] / 100.0f; }   // numbered.rs (init_juliac)
+void derive_cpow2(const float* u, float* o) {                   // heavy_init.rs (init_cpow2)
+    const float sd = u[2] == 0.0f ? 1e-30f : u[2], range = std::fmax(u[3], 1.0f);
+    const float c = u[0] * std::cos(1.5707963267948966f * u[1]) / sd, d = u[0] * std::sin(1.5707963267948966f * u[1]) / sd;
+    o[0] = 6.28318530717959f / sd; o[1] = c; o[2] = d; o[3] = c * 0.5f; o[4] = d * 0.5f; o[5] = 0.5f / range;
+    o[6] = 6.28318530717959f * range;
+}
+void derive_post_juliaq(const float* u, float* o) {             // pre_post_bridges.rs (init_post_juliaq)
+    const float sp = u[0] == 0.0f ? 1e-30f : u[0];
+    o[0] = 0.5f * u[1] / sp; o[1] = u[1] / sp; o[2] = 6.28318530717959f / sp;
+}
+void derive_post_julia3Dq(const float* u, float* o) {           // pre_post_bridges.rs (init_post_julia3Dq)
+    const float sp = u[0] == 0.0f ? 1e-30f : u[0], ip = u[1] / sp;
+    o[0] = ip; o[1] = std::fabs(ip); o[2] = 0.5f * ip - 0.5f; o[3] = 6.28318530717959f / sp;
+}
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -568,6 +595,7 @@ static const VarDef kRegistry[] = {
     {"csch2_bs", 134, 0, 4, {"x1", "x2", "y1", "y2"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_csch2_bs", 0, 0, nullptr},
     {"exp2_bs", 135, 0, 3, {"x1", "y1", "y2"}, {1.0f, 1.0f, 1.0f}, "v_exp2_bs", 0, 0, nullptr},
     {"exp", 136, 0, 0, NP, ND, "v_exp", 0, 0, nullptr},
+    {"log_db", 137, 7, 2, {"base", "fix_period"}, {1.0f, 1.0f}, "v_log_db", 0, 2, derive_log_db},
     {"log_tile2", 138, 4, 3, {"spreadx", "spready", "spreadz"}, {2.0f, 2.0f, 0.0f}, "v_log_tile2", 0, 0, nullptr},
     {"tile_log", 139, 2, 1, {"spread"}, {1.0f}, "v_tile_log", 0, 0, nullptr},
     {"tancos", 140, 0, 0, NP, ND, "v_tancos", 0, 0, nullptr},
@@ -603,6 +631,10 @@ static const VarDef kRegistry[] = {
     {"popcorn2", 170, 0, 3, {"x", "y", "c"}, {1.0f, 0.5f, 1.5f}, "v_popcorn2", 0, 0, nullptr},
     {"splits3D", 171, 0, 3, {"x", "y", "z"}, {0.1f, 0.3f, 0.2f}, "v_splits3D", 0, 0, nullptr},
     {"waves2_3D", 172, 0, 2, {"freq", "scale"}, {2.0f, 1.0f}, "v_waves2_3D", 0, 0, nullptr},
+    {"juliaq", 173, 1, 2, {"power", "divisor"}, {3.0f, 2.0f}, "v_juliaq", 0, 3, derive_juliaq},
+    {"julia3Dq", 174, 1, 2, {"power", "divisor"}, {3.0f, 2.0f}, "v_julia3Dq", 0, 4, derive_julia3Dq},
+    {"juliac", 175, 1, 3, {"re", "im", "dist"}, {3.0f, 0.5f, 1.0f}, "v_juliac", 0, 2, derive_juliac},
+    {"cpow2", 176, 3, 4, {"r", "a", "divisor", "range"}, {1.0f, 0.0f, 1.0f, 1.0f}, "v_cpow2", 0, 7, derive_cpow2},
     {"cpow3", 177, 4, 4, {"r", "d", "divisor", "spread"}, {1.0f, 1.0f, 1.0f, 1.0f}, "v_cpow3", 0, 6, derive_cpow3},
     {"disc2", 178, 0, 2, {"rot", "twist"}, {2.0f, 0.5f}, "v_disc2", 0, 3, derive_disc2},
     {"target", 179, 0, 3, {"even", "odd", "size"}, {0.0f, 0.0f, 1.0f}, "v_target", 0, 1, derive_target},
@@ -644,6 +676,8 @@ static const VarDef kRegistry[] = {
     {"sigmoid", 219, 0, 2, {"shiftx", "shifty"}, {1.0f, 1.0f}, "v_sigmoid", VF_W, 0, nullptr},
     {"blocky", 220, 0, 3, {"x", "y", "mp"}, {1.0f, 1.0f, 4.0f}, "v_blocky", VF_W, 0, nullptr},
     {"pre_curl", 221, 0, 2, {"c1", "c2"}, {0.0f, 0.0f}, "v_pre_curl", VF_PRE | VF_W, 0, nullptr},
+    {"post_juliaq", 222, 1, 2, {"power", "divisor"}, {3.0f, 2.0f}, "v_post_juliaq", VF_POST | VF_W, 3, derive_post_juliaq},
+    {"post_julia3Dq", 223, 1, 2, {"power", "divisor"}, {3.0f, 2.0f}, "v_post_julia3Dq", VF_POST | VF_W, 4, derive_post_julia3Dq},
     {"sineblur", 226, 2, 1, {"power"}, {1.0f}, "v_sineblur", 0, 0, nullptr},
     {"starblur", 227, 2, 2, {"power", "range"}, {5.0f, 0.40162283f}, "v_starblur", 0, 2, derive_starblur},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},

@@ -440,6 +440,7 @@ __device__ __forceinline__ void ffb_defer_store(const FfbRec& rs, int k, float x
 struct SlotRng {
     const float* d;
     __device__ __forceinline__ float draw(int slot) { return d[slot - FFB_FIN_SLOT0]; }
+    __device__ __forceinline__ u32 word(int slot) { return ffb_word_of(draw(slot)); }
 };
 #else
 struct FfbRec {};

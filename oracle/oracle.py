@@ -344,6 +344,13 @@ REGISTRY = {
     "hypertile3D2": 189,
     "julian3Dx": 395,
     "waves2b": 479,
+    "log_db": 137,
+    "juliaq": 173,
+    "julia3Dq": 174,
+    "juliac": 175,
+    "cpow2": 176,
+    "post_juliaq": 222,
+    "post_julia3Dq": 223,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -674,6 +681,15 @@ PARAMS.update({
     "hypertile3D2": [("p", 3.0), ("q", 7.0)],
     "julian3Dx": [("power", 0.0), ("dist", 1.0), ("a", 1.0), ("b", 0.0), ("c", 0.0), ("d", 1.0), ("e", 0.0), ("f", 0.0)],
     "waves2b": [("freqx", 2.0), ("freqy", 2.0), ("pwx", 1.0), ("pwy", 1.0), ("scalex", 1.0), ("scaleinfx", 1.0), ("scaley", 1.0), ("scaleinfy", 1.0), ("unity", 1.0), ("jacok", 0.25)],
+})
+PARAMS.update({
+    "log_db": [("base", 1.0), ("fix_period", 1.0)],
+    "juliaq": [("power", 3.0), ("divisor", 2.0)],
+    "julia3Dq": [("power", 3.0), ("divisor", 2.0)],
+    "juliac": [("re", 3.0), ("im", 0.5), ("dist", 1.0)],
+    "cpow2": [("r", 1.0), ("a", 0.0), ("divisor", 1.0), ("range", 1.0)],
+    "post_juliaq": [("power", 3.0), ("divisor", 2.0)],
+    "post_julia3Dq": [("power", 3.0), ("divisor", 2.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -312,6 +312,12 @@ WIDER = {
     "pRose3D": dict.fromkeys(["-0+0", "-0-0", "-x", "+y", "-y", "q1", "q2", "q3", "q4", "half_unit", "tiny", "normal_min",
                               "large", "near_threshold", "past_threshold", "neg0y_x"], "zero"),
     "waves2b": dict.fromkeys(["+0+0", "+0-0", "-0+0", "-0-0", "tiny", "normal_min", "subnormal"], "zero"),
+    "juliaq": {**dict.fromkeys(["-0+0", "+y", "q4", "tiny", "neg0y_x"], "zero"), "large": "inf*0"},
+    "julia3Dq": dict.fromkeys(["+y", "q1", "q2", "half_unit", "tiny"], "zero"),
+    "juliac": dict.fromkeys(["-x", "-y", "neg0y_x"], "zero"),
+    "cpow2": dict.fromkeys(["+0-0", "-0-0", "+x", "-x", "-y", "unit", "subnormal", "y_neg0x"], "zero"),
+    "post_juliaq": {**dict.fromkeys(["-y", "normal_min"], "zero"), "large": "inf*0"},
+    "post_julia3Dq": {**dict.fromkeys(["q3", "q4"], "zero"), "normal_min": "signed-zero"},
     "gamma": dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "half_unit", "y_neg0x", "neg0y_x"], "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
