@@ -928,6 +928,13 @@ static const VarDef kRegistry[] = {
     {"sym_bg6", 566, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg6", 0, 0, nullptr},
     {"sym_bg7", 567, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg7", 0, 0, nullptr},
     {"pRose3D", 568, 2, 16, {"l", "k", "c", "z1", "z2", "refSc", "opt", "optSc", "opt3", "transp", "dist", "wagsc", "srvsc", "f", "wigsc", "offset"}, {1.0f, 6.0f, 0.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.5f, 1.0f, 0.0f, 0.0f, 3.0f, 0.0f, 0.0f}, "v_pRose3D", 0, 0, nullptr},
+    {"cut_sqcir", 570, 2, 4, {"mode", "zoom", "invert", "power"}, {1.0f, 2.0f, 0.0f, 2.0f}, "v_cut_sqcir", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_yuebing", 571, 2, 5, {"mode", "zoom", "invert", "p1", "p2"}, {1.0f, 0.25f, 0.0f, 2.0f, 25.0f}, "v_cut_yuebing", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_vasarely", 572, 2, 4, {"mode", "zoom", "invert", "size"}, {1.0f, 1.0f, 0.0f, 0.5f}, "v_cut_vasarely", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_sincos", 573, 2, 5, {"seed", "mode", "time", "zoom", "invert"}, {1000.0f, 1.0f, 0.9f, 0.5f, 0.0f}, "v_cut_sincos", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_chains", 574, 2, 5, {"shiftX", "shiftY", "mode", "zoom", "invert"}, {0.0f, 0.0f, 1.0f, 2.5f, 0.0f}, "v_cut_chains", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_hexdots", 575, 2, 4, {"mode", "size", "zoom", "invert"}, {1.0f, 0.5f, 4.0f, 0.0f}, "v_cut_hexdots", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_booleans", 576, 2, 5, {"seed", "mode", "type", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 250.0f, 0.0f}, "v_cut_booleans", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"solid_sphere", 605, 2, 5, {"radius", "thickness", "cx", "cy", "cz"}, {1.0f, 0.1f, 0.0f, 0.0f, 0.0f}, "v_solid_sphere", 0, 0, nullptr},
     {"matrix3D", 643, 0, 12, {"xx", "xy", "xz", "yx", "yy", "yz", "zx", "zy", "zz", "tx", "ty", "tz"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_matrix3D", 0, 0, nullptr},};
 #undef NP

@@ -351,6 +351,13 @@ REGISTRY = {
     "cpow2": 176,
     "post_juliaq": 222,
     "post_julia3Dq": 223,
+    "cut_sqcir": 570,
+    "cut_yuebing": 571,
+    "cut_vasarely": 572,
+    "cut_sincos": 573,
+    "cut_chains": 574,
+    "cut_hexdots": 575,
+    "cut_booleans": 576,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -690,6 +697,15 @@ PARAMS.update({
     "cpow2": [("r", 1.0), ("a", 0.0), ("divisor", 1.0), ("range", 1.0)],
     "post_juliaq": [("power", 3.0), ("divisor", 2.0)],
     "post_julia3Dq": [("power", 3.0), ("divisor", 2.0)],
+})
+PARAMS.update({
+    "cut_sqcir": [("mode", 1.0), ("zoom", 2.0), ("invert", 0.0), ("power", 2.0)],
+    "cut_yuebing": [("mode", 1.0), ("zoom", 0.25), ("invert", 0.0), ("p1", 2.0), ("p2", 25.0)],
+    "cut_vasarely": [("mode", 1.0), ("zoom", 1.0), ("invert", 0.0), ("size", 0.5)],
+    "cut_sincos": [("seed", 1000.0), ("mode", 1.0), ("time", 0.9), ("zoom", 0.5), ("invert", 0.0)],
+    "cut_chains": [("shiftX", 0.0), ("shiftY", 0.0), ("mode", 1.0), ("zoom", 2.5), ("invert", 0.0)],
+    "cut_hexdots": [("mode", 1.0), ("size", 0.5), ("zoom", 4.0), ("invert", 0.0)],
+    "cut_booleans": [("seed", 1000.0), ("mode", 1.0), ("type", 0.0), ("zoom", 250.0), ("invert", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -48,7 +48,7 @@ EXACT = {"linear", "spherical", "horseshoe", "bubble", "curl", "hyperbolic", "be
          "separation", "mobius", "cell", "modulus", "square", "boarders",
          "blur_zoom", "blur_pixelize", "henon", "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy",
          "loonie3", "d_spherical", "hypertile3D", "voron", "minkQM", "poincare3D", "rosoni", "circleLinear",
-         "plusrecip", "mobiq", "pointgrid_wf", "bubbleT3D"}
+         "plusrecip", "mobiq", "pointgrid_wf", "bubbleT3D", "cut_hexdots"}
 
 
 @pytest.fixture(scope="module")
@@ -337,11 +337,16 @@ def hide_flame():
     """Feature::CanHide on the exactly rounded flame: a transform of
     circlecrop at radius 0 (every point escapes: the iteration is dropped
     and the point reverts) and a final circlecrop of radius 0.8 (samples
-    outside it are not plotted, the rest pass unchanged)."""
+    outside it are not plotted, the rest pass unchanged), and a transform
+    whose circlecrop hides every point before a cut_hexdots stencil on the
+    point (mode 0) assigns the flag again: the stencil's verdict stands."""
     cfg = exact_flame()
     xfs = cfg["flame"]["transforms"]
     xfs.append(dict(a=0.7, b=0.1, c=-0.2, d=0.6, e=0.1, f=0.1, weight=0.9, color=0.3, variations={"circlecrop": 1.0},
                     variation_params={"circlecrop.radius": 0.0}))
+    xfs.append(dict(a=0.6, b=-0.2, c=0.2, d=0.7, e=-0.2, f=0.1, weight=0.7, color=0.8,
+                    variations={"circlecrop": 0.5, "cut_hexdots": 0.9},
+                    variation_params={"circlecrop.radius": 0.0, "cut_hexdots.mode": 0.0, "cut_hexdots.zoom": 3.0}))
     fin = dict(a=1.0, b=0.0, c=0.0, d=1.0, e=0.0, f=0.0, weight=1, color=0.5, variations={"circlecrop": 1.0},
                variation_params={"circlecrop.radius": 0.8})
     cfg["flame"]["final_transforms"].append(fin)
