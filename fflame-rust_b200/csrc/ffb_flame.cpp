@@ -449,6 +449,12 @@ void derive_post_julia3Dq(const float* u, float* o) {           // pre_post_brid
     const float sp = u[0] == 0.0f ? 1e-30f : u[0], ip = u[1] / sp;
     o[0] = ip; o[1] = std::fabs(ip); o[2] = 0.5f * ip - 0.5f; o[3] = 6.28318530717959f / sp;
 }
+// cut_fractal's constant c and cut_snowflake's starting depth, functions of
+// the time parameter alone (cut_simple.rs), taken once on the host.
+void derive_cut_fractal(const float* u, float* o) {
+    o[0] = std::cos(u[2] + 1.5f) * 0.15f - 0.25f; o[1] = std::sin(u[2] + 1.8f) * 0.15f - 0.25f;
+}
+void derive_cut_snowflake(const float* u, float* o) { o[0] = std::sin(u[2] * 0.4f) * 0.5f - 0.5f; }
 }  // namespace
 
 // The variations this build carries, in the reference's registry order
@@ -935,6 +941,12 @@ static const VarDef kRegistry[] = {
     {"cut_chains", 574, 2, 5, {"shiftX", "shiftY", "mode", "zoom", "invert"}, {0.0f, 0.0f, 1.0f, 2.5f, 0.0f}, "v_cut_chains", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_hexdots", 575, 2, 4, {"mode", "size", "zoom", "invert"}, {1.0f, 0.5f, 4.0f, 0.0f}, "v_cut_hexdots", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_booleans", 576, 2, 5, {"seed", "mode", "type", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 250.0f, 0.0f}, "v_cut_booleans", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_sqsplits", 577, 2, 5, {"seed", "mode", "time", "zoom", "invert"}, {1000.0f, 1.0f, 0.9f, 2.0f, 0.0f}, "v_cut_sqsplits", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_btree", 578, 2, 6, {"seed", "time", "thickness", "zoom", "mode", "invert"}, {0.0f, 1.0f, 5.0f, 1.0f, 1.0f, 1.0f}, "v_cut_btree", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_fractal", 579, 2, 6, {"seed", "mode", "time", "iters", "zoom", "invert"}, {0.0f, 1.0f, 0.0f, 30.0f, 1.0f, 0.0f}, "v_cut_fractal", VF_REPLACE | VF_HIDE, 2, derive_cut_fractal},
+    {"cut_glypho", 580, 2, 6, {"mode", "zoom", "invert", "f1", "f2", "f3"}, {1.0f, 1.0f, 0.0f, 0.115f, 0.75f, 1.5f}, "v_cut_glypho", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_circdes", 581, 2, 5, {"seed", "mode", "time", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 10.0f, 0.0f}, "v_cut_circdes", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_snowflake", 582, 2, 6, {"seed", "mode", "time", "level", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 10.0f, 10.0f, 0.0f}, "v_cut_snowflake", VF_REPLACE | VF_HIDE, 1, derive_cut_snowflake},
     {"solid_sphere", 605, 2, 5, {"radius", "thickness", "cx", "cy", "cz"}, {1.0f, 0.1f, 0.0f, 0.0f, 0.0f}, "v_solid_sphere", 0, 0, nullptr},
     {"matrix3D", 643, 0, 12, {"xx", "xy", "xz", "yx", "yy", "yz", "zx", "zy", "zz", "tx", "ty", "tz"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_matrix3D", 0, 0, nullptr},};
 #undef NP

@@ -358,6 +358,12 @@ REGISTRY = {
     "cut_chains": 574,
     "cut_hexdots": 575,
     "cut_booleans": 576,
+    "cut_sqsplits": 577,
+    "cut_btree": 578,
+    "cut_fractal": 579,
+    "cut_glypho": 580,
+    "cut_circdes": 581,
+    "cut_snowflake": 582,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -706,6 +712,14 @@ PARAMS.update({
     "cut_chains": [("shiftX", 0.0), ("shiftY", 0.0), ("mode", 1.0), ("zoom", 2.5), ("invert", 0.0)],
     "cut_hexdots": [("mode", 1.0), ("size", 0.5), ("zoom", 4.0), ("invert", 0.0)],
     "cut_booleans": [("seed", 1000.0), ("mode", 1.0), ("type", 0.0), ("zoom", 250.0), ("invert", 0.0)],
+})
+PARAMS.update({
+    "cut_sqsplits": [("seed", 1000.0), ("mode", 1.0), ("time", 0.9), ("zoom", 2.0), ("invert", 0.0)],
+    "cut_btree": [("seed", 0.0), ("time", 1.0), ("thickness", 5.0), ("zoom", 1.0), ("mode", 1.0), ("invert", 1.0)],
+    "cut_fractal": [("seed", 0.0), ("mode", 1.0), ("time", 0.0), ("iters", 30.0), ("zoom", 1.0), ("invert", 0.0)],
+    "cut_glypho": [("mode", 1.0), ("zoom", 1.0), ("invert", 0.0), ("f1", 0.115), ("f2", 0.75), ("f3", 1.5)],
+    "cut_circdes": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("zoom", 10.0), ("invert", 0.0)],
+    "cut_snowflake": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("level", 10.0), ("zoom", 10.0), ("invert", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -72,6 +72,7 @@ inline RE sinh(const RE& a) { return re_fn(std::sinh(a.v), std::cosh(a.v), a); }
 inline RE cosh(const RE& a) { return re_fn(std::cosh(a.v), std::sinh(a.v), a); }
 inline RE tanh(const RE& a) { const double t = std::tanh(a.v); return re_fn(t, 1 - t * t, a); }
 inline RE exp(const RE& a) { const double v = std::exp(a.v); return re_fn(v, v, a); }
+inline RE exp2(const RE& a) { const double v = std::exp2(a.v); return re_fn(v, v * 0.6931471805599453, a); }
 inline RE log(const RE& a) { return re_fn(std::log(a.v), a.v != 0 ? 1 / a.v : 0.0, a); }
 inline RE atan(const RE& a) { return re_fn(std::atan(a.v), 1 / (1 + a.v * a.v), a); }
 inline RE atan2(const RE& y, const RE& x) {

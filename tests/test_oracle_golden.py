@@ -357,7 +357,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "loonie2", "elliptic2", "asteria", "scry2", "pre_bwraps2", "post_bwraps2", "pre_rect_wf",
                        "spliptic_bs", "pointgrid_wf", "truchet2", "bubbleT3D",
                        "hypertile3D1", "hypertile3D2", "julian3Dx",
-                       "cut_sqcir", "cut_yuebing", "cut_sincos", "cut_chains", "cut_hexdots"])
+                       "cut_sqcir", "cut_yuebing", "cut_sincos", "cut_chains", "cut_hexdots",
+                       "cut_sqsplits", "cut_btree", "cut_fractal", "cut_glypho", "cut_circdes", "cut_snowflake"])
 
 
 def golden():

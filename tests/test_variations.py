@@ -48,7 +48,8 @@ EXACT = {"linear", "spherical", "horseshoe", "bubble", "curl", "hyperbolic", "be
          "separation", "mobius", "cell", "modulus", "square", "boarders",
          "blur_zoom", "blur_pixelize", "henon", "cylinder2", "flipcircle", "lozi", "bi_linear", "twoface", "flipy",
          "loonie3", "d_spherical", "hypertile3D", "voron", "minkQM", "poincare3D", "rosoni", "circleLinear",
-         "plusrecip", "mobiq", "pointgrid_wf", "bubbleT3D", "cut_hexdots"}
+         "plusrecip", "mobiq", "pointgrid_wf", "bubbleT3D", "cut_hexdots", "cut_fractal",
+         "cut_snowflake"}
 
 
 @pytest.fixture(scope="module")
