@@ -347,6 +347,7 @@ def run_ours(args, rank, world, local_rank):
         line["batched"] = leg(run_batched, args, local_rank, steps=3, serial_steps=2)
         line["diff"] = leg(run_diff, args, local_rank, steps=10, cpu=False)
         line["stress_4k"] = leg(stress_leg, r, args)
+        line["tiles"] = leg(tiles_leg, r)
     r.close()
     return line
 
@@ -426,6 +427,41 @@ def stress_leg(r, args, steps=2):
     torch.cuda.empty_cache()
     return {"ms_per_frame": ms, "samples_per_s": out.total_iterations / (ms * 1e-3), "samples": out.total_iterations,
             "steps": steps, "desc": wl["desc"]}
+
+
+def tiles_leg(r, steps=2):
+    """Direct splat against tile-sorted accumulation for the u32-count /
+    FP32-colour histogram: the stress flame at 7680x4320 internal (531 MB,
+    4x the L2) and 3e9 samples, then the benchmark frame (133 MB), each
+    timed both ways with CUDA events."""
+    import torch
+    out = {}
+    for name, cfg, W, H, iters, walkers in (
+            ("f32_7680x4320_3e9", synthetic_cfg("stress"), 3840, 2160, 3_000_000_000, 0),
+            ("f32_3840x2160_1e9", synthetic_cfg("full"), 1920, 1080, 1_000_000_000, 65536)):
+        d_rgba = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+        side = torch.cuda.Stream()
+        row = {"histogram_mb": W * 2 * H * 2 * 16 / 1e6}
+        for acc in ("direct", "tiled"):
+            job = dict(iterations=iters, walkers=walkers, supersample=2, seed=0x5EED, accumulate=acc)
+            r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=side.cuda_stream, sync=True, **job)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(side)
+            for _ in range(steps):
+                r.render_device(cfg, W, H, d_rgba.data_ptr(), stream=side.cuda_stream, sync=False, **job)
+            ev1.record(side)
+            ev1.synchronize()
+            row[f"{acc}_ms"] = ev0.elapsed_time(ev1) / steps
+        row["tiled_speedup"] = row["direct_ms"] / row["tiled_ms"]
+        out[name] = row
+        del d_rgba
+        torch.cuda.empty_cache()
+    return out
+
+
+def synthetic_cfg(kind):
+    from ffb200 import synthetic
+    return json.dumps(synthetic.stress_flame(21) if kind == "stress" else synthetic.full_flame(FULL_SEED))
 
 
 def config_for(args, wl, world):

@@ -304,7 +304,7 @@ struct Prepared {
     int rng = RNG_PHILOX, math = MATH_PRECISE;
     uint32_t schedule = 0;
     uint32_t count_bits = 32;
-    uint32_t accumulate = 0;    // exact mode: 0 auto, 1 direct, 2 tile-sorted
+    uint32_t accumulate = 0;    // 0 auto, 1 direct, 2 tile-sorted
     bool threads_set = false;   // the job chose the block size (the sorted schedule's sorting group too)
     uint32_t plot = 0;          // 0 auto, 1 inline, 2 deferred (the plot in its own kernel)
     void (*progress)(void*, uint64_t, uint64_t) = nullptr;   // RenderProgress (render.rs:293-301)
@@ -312,16 +312,19 @@ struct Prepared {
     void* progress_user = nullptr;
 };
 
-// Whether a render accumulates by tiles: exact mode, tile-sorted
-// accumulation asked for -- or auto with an exact histogram above 512 MB
-// (4x the L2, where the direct splat's 64-bit atomics mostly miss it;
-// measured at 7680x4320: 546 ms against 585 for 1e10 samples) -- a tile
-// grid the sort's shared-memory counters hold, and a palette of at most
-// 1024 entries.
+// Whether a render accumulates by tiles: tile-sorted accumulation asked
+// for -- or auto with a histogram above 512 MB (4x the L2, where the direct
+// splat's atomics mostly miss it) -- a tile grid the sort's shared-memory
+// counters hold, and a palette of at most 1024 entries.  Measured at
+// 7680x4320: exact (1.06 GB), 1e10 samples, 546 ms tiled against 585
+// direct; u32 / FP32 (531 MB), 3e9 samples, 213 against 259.  At
+// 3840x2160 (u32 / FP32, 133 MB, 1e9 samples) the direct splat, deferred
+// beside the walkers, wins: 57 ms against 82.
 bool tiled_accumulation(const Prepared& P) {
-    if (P.count_bits != 64 || P.accumulate == 1) return false;
+    if (P.accumulate == 1) return false;
     if (P.flame.color_mode != 0) return false;      // records hold a palette index, not a walker's colour
-    if (P.accumulate == 0 && (double)P.wi * (double)P.hi * 32.0 <= 512e6) return false;
+    const double px_bytes = P.count_bits == 64 ? 32.0 : 16.0;
+    if (P.accumulate == 0 && (P.flame.filter.on() || (double)P.wi * (double)P.hi * px_bytes <= 512e6)) return false;
     const int tx = (int)((P.wi + 63) / 64), ty = (int)((P.hi + 63) / 64);
     return tx * ty <= kMaxTiles && tx <= kMaxCols && ty <= kMaxBands && P.flame.palette_size <= 1024;
 }
@@ -376,6 +379,8 @@ Prepared prepare(const char* config, size_t len, const ffb_job* job, bool need_s
     if (P.accumulate > 2) fail(FFB_ERR_INVALID, "accumulate must be 0 (auto), 1 (direct) or 2 (tile-sorted)");
     if (P.accumulate == 2 && P.flame.color_mode != 0)
         fail(FFB_ERR_INVALID, "tile-sorted accumulation records palette indices: not with the speed colour mode");
+    if (P.accumulate == 2 && P.flame.filter.on())
+        fail(FFB_ERR_INVALID, "tile-sorted accumulation adds into the render's histogram: not with the spatial filter's batches");
     P.plot = job->plot;
     if (P.plot > 3) fail(FFB_ERR_INVALID, "plot must be 0 (auto), 1 (inline), 2 (deferred) or 3 (fused)");
     P.progress = job->progress;
@@ -741,7 +746,8 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
             const uint64_t seg_cap = (uint64_t)threads * ls[i].n_iters * (uint64_t)P.flame.sym.copies();
             ck(launch_tile_pass((const unsigned long long*)r->tile_rec.p, seg_cap, (int)blocks, tg, 1u << 18, count, off, fill,
                                 work_off, work, band_fill, band_part_off, (unsigned long long*)r->tile_tmp.p,
-                                (unsigned*)r->tile_sorted.p, (const float4*)d_pal, (int)pal_n, (ulonglong4*)hist, r->n_sm, s),
+                                (unsigned*)r->tile_sorted.p, (const float4*)d_pal, (int)pal_n, (void*)hist, P.count_bits == 64,
+                                r->n_sm, s),
                "tile-sorted accumulation");
             r->launches += 5;
         }

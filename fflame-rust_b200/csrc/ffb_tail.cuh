@@ -84,8 +84,9 @@ cudaError_t launch_diff_tonemap_vjp(const float4* hist, const float4* dimg, size
                                     const uint64_t* samples, double npx, double area, double white, float4* dh, cudaStream_t s);
 
 // Tile-sorted accumulation (ffb_tiles.cu): one pass over a launch's records
-// (u64: pixel index | palette index << 32) into the exact histogram `hist`
-// (ulonglong4 a pixel), by 64x64-pixel tiles.  The records are n_segs
+// (u64: pixel index | palette index << 32) into the histogram `hist` --
+// the exact one (ulonglong4 a pixel) when `exact`, else the u32-count /
+// FP32-colour one (float4 a pixel) -- by 64x64-pixel tiles.  The records are n_segs
 // segments of seg_cap (one a chaos block), followed by the segments' counts
 // (u32 each).  Scratch: count/fill n_tiles words, off/work_off n_tiles + 1,
 // work 2, band_fill tiles_y, band_part_off kMaxBands + 1, then (16-byte
@@ -96,7 +97,7 @@ constexpr int kMaxTiles = 16384, kMaxBands = 512, kMaxCols = 512;
 cudaError_t launch_tile_pass(const unsigned long long* rec, unsigned long long seg_cap, int n_segs, const TileGeom& g,
                              unsigned slice, unsigned* count, unsigned* off, unsigned* fill, unsigned* work_off, unsigned* work,
                              unsigned* band_fill, unsigned* band_part_off, unsigned long long* tmp, unsigned* sorted,
-                             const float4* pal, int pal_n, ulonglong4* hist, int n_sm, cudaStream_t s);
+                             const float4* pal, int pal_n, void* hist, bool exact, int n_sm, cudaStream_t s);
 
 // The deterministic accumulation's u64 sums (2^-32 units) as float4.
 cudaError_t launch_fixed_to_float(const ulonglong4* fx, size_t n, float4* out, cudaStream_t s);

@@ -21,8 +21,13 @@
 //      the carry taken from the returned old value) and add the tile to the
 //      histogram with plain read-modify-writes (with atomics when a hot tile
 //      is split over several slices).
-// The integer sums make the result the same bits as the direct path.  The
-// reference's counterpart is the sample-emit path for histograms larger
+// The integer sums make the result the same bits as the direct path.
+// The same passes serve the u32-count / FP32-colour histogram (float4 a
+// pixel): k_tile_accumulate_f32 sums a slice in shared memory (u32 count,
+// FP32 colour) and adds it with one 16-byte read-modify-write a pixel, so
+// the count plane is the direct splat's exactly and the colour sums differ
+// from it only by the order of the FP32 additions.  The reference's
+// counterpart is the sample-emit path for histograms larger
 // than one storage binding (main_template.wgsl:1324-1353,
 // shaders/core/accumulate_samples.wgsl, src/export/high_res.rs:2139-2175).
 
@@ -281,6 +286,70 @@ __global__ void __launch_bounds__(512) k_tile_accumulate(const unsigned* __restr
     }
 }
 
+// The u32-count / FP32-colour histogram's slices: the tile's pixels as
+// shared-memory bins (u32 count, FP32 r, g, b: 64 KB), summed with shared
+// atomics, then added to the histogram -- one 16-byte read-modify-write a
+// pixel when the tile is one slice, atomics when a hot tile is split over
+// several (its slices run in any order on any block).
+__global__ void __launch_bounds__(512) k_tile_accumulate_f32(const unsigned* __restrict__ sorted, const unsigned* __restrict__ off,
+                                                             const unsigned* __restrict__ work_off, unsigned* __restrict__ work,
+                                                             unsigned slice, const float4* __restrict__ pal, TileGeom g,
+                                                             float4* __restrict__ hist) {
+    extern __shared__ unsigned s_acc[];
+    unsigned* s_n = s_acc;                                        // [4096] counts
+    float* s_r = reinterpret_cast<float*>(s_n + 4096);            // [4096] each: r, g, b sums
+    float* s_g = s_r + 4096;
+    float* s_b = s_g + 4096;
+    __shared__ unsigned s_item;
+    const unsigned items = work[0];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(&work[1], 1u);
+        for (int i = threadIdx.x; i < 4 * 4096; i += blockDim.x) s_acc[i] = 0u;
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= items) break;
+        int lo = 0, hi = g.n_tiles - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (work_off[mid] <= item) lo = mid; else hi = mid - 1;
+        }
+        const int t = lo;
+        const unsigned slices = work_off[t + 1] - work_off[t];
+        const unsigned k = item - work_off[t];
+        const unsigned i0 = off[t] + k * slice, i1 = min(i0 + slice, off[t + 1]);
+        for (unsigned i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            const unsigned v = sorted[i];
+            const unsigned li = v & 4095u;
+            const float4 c = __ldg(pal + (v >> 12));                // linear palette colour (L1)
+            atomicAdd(&s_n[li], 1u);
+            atomicAdd(&s_r[li], c.x);
+            atomicAdd(&s_g[li], c.y);
+            atomicAdd(&s_b[li], c.z);
+        }
+        __syncthreads();
+        const int tx = t % g.tiles_x, ty = t / g.tiles_x;
+        for (int li = threadIdx.x; li < 4096; li += blockDim.x) {
+            const unsigned n = s_n[li];
+            if (!n) continue;
+            const int x = tx * 64 + (li & 63), y = ty * 64 + (li >> 6);
+            float4* p = hist + (size_t)y * g.w + x;
+            if (slices == 1) {
+                float4 h = *p;
+                h.x += s_r[li]; h.y += s_g[li]; h.z += s_b[li];
+                h.w = __uint_as_float(__float_as_uint(h.w) + n);
+                *p = h;
+            } else {
+                float* q = reinterpret_cast<float*>(p);
+                atomicAdd(q + 0, s_r[li]);
+                atomicAdd(q + 1, s_g[li]);
+                atomicAdd(q + 2, s_b[li]);
+                atomicAdd(reinterpret_cast<unsigned*>(q + 3), n);
+            }
+        }
+    }
+}
+
 // The palette's colours as the exact splat's integers: round(c * 2^24).
 __global__ void k_pal_fixed(const float4* __restrict__ pal, int n, uint4* __restrict__ out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -295,7 +364,7 @@ __global__ void k_pal_fixed(const float4* __restrict__ pal, int n, uint4* __rest
 cudaError_t launch_tile_pass(const unsigned long long* rec, unsigned long long seg_cap, int n_segs, const TileGeom& g,
                              unsigned slice, unsigned* count, unsigned* off, unsigned* fill, unsigned* work_off, unsigned* work,
                              unsigned* band_fill, unsigned* band_part_off, unsigned long long* tmp, unsigned* sorted,
-                             const float4* pal, int pal_n, ulonglong4* hist, int n_sm, cudaStream_t s) {
+                             const float4* pal, int pal_n, void* hist, bool exact, int n_sm, cudaStream_t s) {
     const unsigned* seg_n = reinterpret_cast<const unsigned*>(rec + seg_cap * (unsigned long long)n_segs);
     cudaError_t e;
     if (g.n_tiles > kMaxTiles || g.tiles_y > kMaxBands || g.tiles_x > kMaxCols || pal_n > 1024) return cudaErrorInvalidValue;
@@ -307,7 +376,10 @@ cudaError_t launch_tile_pass(const unsigned long long* rec, unsigned long long s
     if ((e = cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxTiles * 4)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_band_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_tile_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k_tile_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_acc)) != cudaSuccess)
+    const size_t smem_f32 = 4 * 4096 * 4;
+    if (exact && (e = cudaFuncSetAttribute(k_tile_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_acc)) != cudaSuccess)
+        return e;
+    if (!exact && (e = cudaFuncSetAttribute(k_tile_accumulate_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_f32)) != cudaSuccess)
         return e;
     if ((e = cudaMemsetAsync(count, 0, (size_t)g.n_tiles * 4, s)) != cudaSuccess) return e;
     k_tile_count<<<std::min(n_sm * 4, n_segs), 512, smem_c, s>>>(rec, seg_cap, n_segs, seg_n, g, count);
@@ -317,8 +389,13 @@ cudaError_t launch_tile_pass(const unsigned long long* rec, unsigned long long s
     const unsigned long long total_cap = seg_cap * (unsigned long long)n_segs;
     const unsigned items_max = (unsigned)((total_cap + range - 1) / range) + (unsigned)g.tiles_y;
     k_tile_scatter<<<items_max, 512, smem_b, s>>>(tmp, g, range, off, band_part_off, fill, sorted);
-    k_pal_fixed<<<(pal_n + 255) / 256, 256, 0, s>>>(pal, pal_n, pal_fx);
-    k_tile_accumulate<<<n_sm * 2, 512, smem_acc, s>>>(sorted, off, work_off, work, slice, pal_fx, g, hist);
+    if (exact) {
+        k_pal_fixed<<<(pal_n + 255) / 256, 256, 0, s>>>(pal, pal_n, pal_fx);
+        k_tile_accumulate<<<n_sm * 2, 512, smem_acc, s>>>(sorted, off, work_off, work, slice, pal_fx, g,
+                                                          static_cast<ulonglong4*>(hist));
+    } else {
+        k_tile_accumulate_f32<<<n_sm * 3, 512, smem_f32, s>>>(sorted, off, work_off, work, slice, pal, g, static_cast<float4*>(hist));
+    }
     return cudaGetLastError();
 }
 

@@ -101,7 +101,7 @@ class Engine:
         `walkers` fixes the number of concurrent orbits (default: sized to
         the budget); `exact` accumulates u64 counts and fixed-point colour
         sums (long renders, order-independent results); `accumulate`
-        ("direct" or "tiled") picks how the exact sums are gathered.
+        ("direct" or "tiled") picks how the sums are gathered.
 
         `sticky` and `sequence` are accepted for pyfae's signature and change
         nothing here.  The reference's `sticky` compiles a superset shader

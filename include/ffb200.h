@@ -91,10 +91,11 @@ typedef struct {
                                           integer accumulation -- u64 count and u64 colour sums in 24-bit
                                           fixed point (32 B a pixel), independent of the atomics' order
                                           (the exact count of accumulate.wgsl:185-199) */
-    uint32_t accumulate;               /* exact mode: 0 auto (tile-sorted above a 512 MB histogram, else
-                                          direct), 1 direct (a splat's atomics on the histogram), 2
+    uint32_t accumulate;               /* 0 auto (tile-sorted above a 512 MB histogram, else direct),
+                                          1 direct (a splat's atomics on the histogram), 2
                                           tile-sorted (samples emitted as records, sorted by 64x64 tile,
-                                          summed in shared memory; the same bits as direct) */
+                                          summed in shared-memory bins; exact mode: the same bits as direct;
+                                          32-bit mode: the same counts, colour sums in another FP32 order) */
     uint32_t plot;                     /* 0 auto, 1 inline (each walker plots its own samples), 2 deferred:
                                           the chaos kernel stores its samples and a plot kernel (the final
                                           chain, palette, symmetry copies, splat) runs beside the next
