@@ -12,9 +12,10 @@ reference's own boundary (`fae_call` render request -> RGBA8 in host memory).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Under torchrun each rank renders its own 65,536 walkers (weak scaling); the
-ranks' histograms are summed with an NCCL all-reduce (the path's one exchange
-step), each rank tone-maps a band of rows and the bands are gathered; the
-step time is the max over ranks, and rank 0 prints one JSON line.
+ranks' histograms are summed with an NCCL reduce-scatter of row windows (the
+path's one exchange step: a band of rows plus the density estimation's
+reach), each rank finishes its band and the bands are gathered; the step
+time is the max over ranks, and rank 0 prints one JSON line.
 """
 
 import argparse
@@ -230,7 +231,7 @@ def run_ours(args, rank, world, local_rank):
     stream = side.cuda_stream
     if world > 1:
         # Weak scaling: every rank renders its own 65,536 walkers x 1e9
-        # samples; the frame sums all ranks' histograms (NCCL all-reduce),
+        # samples; the frame sums all ranks' histograms (NCCL reduce-scatter of row windows),
         # each rank tone-maps a band of rows, the bands are gathered.
         from ffb200 import distributed as D
         backend = D.CudaBackend(r, torch.device("cuda", local_rank), side)
@@ -299,6 +300,17 @@ def run_ours(args, rank, world, local_rank):
     bench_ms = r.atomic_bench(npx, 400_000_000, 0)
     splat_peak = 400_000_000 / (bench_ms * 1e-3)
     splat_rate = statistics.median(inframe) / (c_ms * 1e-3)
+    # The splat kernel alone: ffb_plot over the same frame's records, each
+    # launch run after its chaos launch instead of beside the next one.
+    plot_alone = None
+    if not exact and args.plot in ("auto", "deferred"):
+        try:
+            p_ms, p_samples, p_in = r.plot_bench(cfg, W, H, **job)
+            plot_alone = {"kernel": "ffb_plot (final chain, palette, world_to_pixel, warp-aggregated 4-atomic splat)",
+                          "ms": p_ms, "records": p_samples, "splats": p_in,
+                          "splats_per_s": p_in / (p_ms * 1e-3), "frac": p_in / (p_ms * 1e-3) / splat_peak}
+        except Exception as e:  # noqa: BLE001
+            plot_alone = {"error": f"{type(e).__name__}: {e}"}
 
     # End to end: the reference's boundary, host buffers, copies inside.
     eng = Engine()
@@ -331,7 +343,8 @@ def run_ours(args, rank, world, local_rank):
                      "kernel_ms": c_ms, "algorithmic_bytes_per_launch": bytes_per_launch,
                      "peak_kind": peak_kind},
         "l2_atomic": {"achieved_splats_per_s": splat_rate, "peak_splats_per_s": splat_peak,
-                      "frac": splat_rate / splat_peak, "peak_from": "ffb_atomic_bench kind 0, same histogram size"},
+                      "frac": splat_rate / splat_peak, "peak_from": "ffb_atomic_bench kind 0, same histogram size",
+                      "plot_kernel_alone": plot_alone},
         "e2e": {"value": samples_per_step / e2e_s, "unit": "samples/s", "ms_per_frame": e2e_s * 1e3,
                 "h2d_bytes_per_step": rr.h2d_bytes, "d2h_bytes_per_step": W * H * 4,
                 "path": "fae_call render request (JSON config in, RGBA8 host bytes out)",

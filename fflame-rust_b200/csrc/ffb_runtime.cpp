@@ -179,6 +179,10 @@ struct ffb_renderer {
     cudaEvent_t ev_main[2] = {nullptr, nullptr}, ev_plot[2] = {nullptr, nullptr}, ev_start = nullptr;
     DevBuf rec[2], rec_draws[2];
     cudaEvent_t ev_flight[2] = {nullptr, nullptr};          // RenderProgress: launches in flight
+    // ffb_plot_bench: when set, each plot launch runs after its chaos launch
+    // on the render's stream and its device time is added here.
+    double* plot_timing = nullptr;
+    cudaEvent_t ev_p[2] = {nullptr, nullptr};
     void ensure_flight_events() {
         for (auto& e : ev_flight)
             if (!e) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
@@ -220,6 +224,7 @@ struct ffb_renderer {
             cudaStreamDestroy(plot_stream);
         }
         for (auto e : ev_flight) if (e) cudaEventDestroy(e);
+        for (auto e : ev_p) if (e) cudaEventDestroy(e);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -712,7 +717,19 @@ void run_chaos(ffb_renderer* r, const Prepared& P, cudaStream_t s, uint32_t walk
                 P.progress(P.progress_user, done, plotted_total);
             }
         }
-        if (defer) {
+        if (defer && r->plot_timing) {
+            // The plot kernel alone: after its chaos launch, on the same
+            // stream, timed by events (a measurement mode, not a render's).
+            ck(cudaEventRecord(r->ev_p[0], s), "event");
+            ck(cudaLaunchKernel((const void*)m.plot, dim3((unsigned)r->n_sm * kPlotBlocksPerSm), dim3(kPlotThreads), args, (size_t)smem_plot,
+                                s), "launch ffb_plot");
+            ck(cudaEventRecord(r->ev_p[1], s), "event");
+            ck(cudaEventSynchronize(r->ev_p[1]), "plot launch");
+            float t = 0.f;
+            ck(cudaEventElapsedTime(&t, r->ev_p[0], r->ev_p[1]), "event time");
+            *r->plot_timing += t;
+            r->launches += 1;
+        } else if (defer) {
             ck(cudaEventRecord(r->ev_main[i % 2], s), "event");
             ck(cudaStreamWaitEvent(r->plot_stream, r->ev_main[i % 2], 0), "plot waits for its samples");
             ck(cudaLaunchKernel((const void*)m.plot, dim3((unsigned)r->n_sm * kPlotBlocksPerSm), dim3(kPlotThreads), args, (size_t)smem_plot,
@@ -1462,6 +1479,41 @@ FFB_API int ffb_atomic_bench(ffb_renderer* r, uint32_t pixels, uint64_t samples,
     });
 }
 
+
+// The splat kernel's own throughput: a deferred-plot render of `job` (the
+// sorted schedule's records, ffb_plot applying the final chain, palette,
+// symmetry copies and the warp-aggregated splat) with each plot launch run
+// alone after its chaos launch; *plot_ms = the plot launches' summed device
+// time, *inframe = the splats they made, *samples = the records plotted.
+FFB_API int ffb_plot_bench(ffb_renderer* r, const char* config, size_t len, const ffb_job* job, double* plot_ms, uint64_t* samples,
+                           uint64_t* inframe) {
+    return guard([&] {
+        if (!r || !job || !plot_ms) fail(FFB_ERR_INVALID, "NULL argument");
+        std::lock_guard<std::mutex> lk(r->mu);
+        r->begin();
+        Prepared P = prepare(config, len, job);
+        if (!P.plan.defer || P.plot == 3)
+            fail(FFB_ERR_INVALID, "ffb_plot_bench times deferred plotting (plot 0 or 2): this job does not defer its plot");
+        for (auto& e : r->ev_p)
+            if (!e) ck(cudaEventCreate(&e), "event");
+        r->reset_counts();
+        double t = 0.0;
+        uint64_t n_in = 0;
+        r->plot_timing = &t;
+        try {
+            run_chaos(r, P, r->stream, job->walker0, &n_in);
+            ck(cudaStreamSynchronize(r->stream), "plot bench");
+        } catch (...) {
+            r->plot_timing = nullptr;
+            throw;
+        }
+        r->plot_timing = nullptr;
+        check_inframe(n_in);
+        *plot_ms = t;
+        if (inframe) *inframe = n_in;
+        if (samples) *samples = plotted_samples(P, job->walker0);
+    });
+}
 
 // =============================================================== batches ===
 // Many flames in one persistent launch a structure group (the batched

@@ -30,6 +30,7 @@ EXPORTS = [
     "ffb_diff_create", "ffb_diff_layout", "ffb_diff_theta", "ffb_diff_forward", "ffb_diff_backward", "ffb_diff_samples",
     "ffb_diff_jacobians", "ffb_diff_destroy", "ffb_diff_specialize", "ffb_encode_png",
     "ffb_flame_import", "ffb_histogram_f32", "ffb_hist_filter", "ffb_specialize_job", "ffb_struct_sizes",
+    "ffb_plot_bench",
 ]
 
 
@@ -326,6 +327,16 @@ class Renderer:
         ms = ctypes.c_double()
         _check(lib().ffb_atomic_bench(self._h, ctypes.c_uint32(pixels), ctypes.c_uint64(samples), ctypes.c_int32(kind), ctypes.byref(ms)))
         return ms.value
+
+    def plot_bench(self, config, width, height, **job):
+        """The plot kernel alone (deferred plotting, each plot launch after
+        its chaos launch on one stream): (plot ms, samples, in-frame splats)."""
+        cfg = _text(config)
+        j = make_job(width, height, **job)
+        ms, n, inf = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().ffb_plot_bench(self._h, cfg, ctypes.c_size_t(len(cfg)), ctypes.byref(j), ctypes.byref(ms), ctypes.byref(n),
+                                    ctypes.byref(inf)))
+        return ms.value, n.value, inf.value
 
 
 class BatchItem(ctypes.Structure):

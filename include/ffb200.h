@@ -348,6 +348,14 @@ int ffb_specialize_job(const char* config, size_t config_len, const ffb_job* job
  * (0: the 4-atomic splat, 1: one u32 atomic, 2: one f32x4 reduction) into
  * a histogram of `pixels`; returns the device milliseconds. */
 int ffb_atomic_bench(ffb_renderer* r, uint32_t pixels, uint64_t samples, int32_t kind, double* ms);
+/* The splat kernel's own throughput (no reference counterpart; a
+ * measurement beside the render boundary): `job` rendered with deferred
+ * plotting (plot 0 or 2; refused otherwise), each plot launch run alone
+ * after its chaos launch on one stream.  *plot_ms: the plot launches'
+ * summed device milliseconds; *samples: the records they plotted (post-
+ * burn-in iterations); *inframe: the splats they made. */
+int ffb_plot_bench(ffb_renderer* r, const char* config, size_t config_len, const ffb_job* job, double* plot_ms,
+                   uint64_t* samples, uint64_t* inframe);
 
 #ifdef __cplusplus
 }

@@ -148,3 +148,20 @@ def test_fused_render_is_the_same_image(renderer):
     a, _ = renderer.render(cfg, 320, 180, plot="deferred", **job)
     b, _ = renderer.render(cfg, 320, 180, plot="fused", **job)
     assert np.abs(a.astype(int) - b.astype(int)).max() <= 1           # FP32 colour sums in another order
+
+
+@pytest.mark.gpu
+def test_plot_bench_plots_the_same_frame(renderer):
+    """ffb_plot_bench (each plot launch alone after its chaos launch) makes
+    the render's splats: the same plotted samples and in-frame count as the
+    deferred histogram, a positive plot time; refused for fused plotting,
+    which has no plot kernel of its own."""
+    cfg = full_with_final_draws()
+    job = dict(iterations=16384 * 600, walkers=16384, plot="deferred")
+    cnt, _, o = renderer.histogram(cfg, 320, 200, **job)
+    ms, samples, inframe = renderer.plot_bench(cfg, 320, 200, **job)
+    assert ms > 0.0
+    assert samples == o.total_iterations
+    assert inframe == o.inframe_samples == int(cnt.sum())
+    with pytest.raises(_native.EngineError, match="deferred plotting"):
+        renderer.plot_bench(cfg, 320, 200, iterations=16384 * 600, walkers=16384, plot="fused")
