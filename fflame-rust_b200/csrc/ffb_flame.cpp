@@ -947,6 +947,13 @@ static const VarDef kRegistry[] = {
     {"cut_glypho", 580, 2, 6, {"mode", "zoom", "invert", "f1", "f2", "f3"}, {1.0f, 1.0f, 0.0f, 0.115f, 0.75f, 1.5f}, "v_cut_glypho", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_circdes", 581, 2, 5, {"seed", "mode", "time", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 10.0f, 0.0f}, "v_cut_circdes", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_snowflake", 582, 2, 6, {"seed", "mode", "time", "level", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 10.0f, 10.0f, 0.0f}, "v_cut_snowflake", VF_REPLACE | VF_HIDE, 1, derive_cut_snowflake},
+    {"cut_jigsaw", 583, 2, 5, {"seed", "time", "mode", "zoom", "invert"}, {1000.0f, 0.0f, 1.0f, 4.0f, 0.0f}, "v_cut_jigsaw", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_rgrid", 584, 2, 4, {"mode", "zoom", "invert", "angle"}, {1.0f, 7.0f, 0.0f, 0.0f}, "v_cut_rgrid", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_x", 585, 2, 4, {"mode", "zoom", "invert", "size"}, {1.0f, 1.0f, 0.0f, 0.1f}, "v_cut_x", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_metaballs", 586, 2, 4, {"mode", "zoom", "invert", "time"}, {1.0f, 7.0f, 0.0f, 0.0f}, "v_cut_metaballs", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_kaleido", 587, 2, 6, {"seed", "mode", "time", "n", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 6.0f, 0.5f, 0.0f}, "v_cut_kaleido", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_spiral", 588, 2, 4, {"time", "mode", "zoom", "invert"}, {0.0f, 1.0f, 2.5f, 0.0f}, "v_cut_spiral", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_swarp", 589, 2, 6, {"seed", "mode", "time", "type", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_cut_swarp", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"solid_sphere", 605, 2, 5, {"radius", "thickness", "cx", "cy", "cz"}, {1.0f, 0.1f, 0.0f, 0.0f, 0.0f}, "v_solid_sphere", 0, 0, nullptr},
     {"matrix3D", 643, 0, 12, {"xx", "xy", "xz", "yx", "yy", "yz", "zx", "zy", "zz", "tx", "ty", "tz"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_matrix3D", 0, 0, nullptr},};
 #undef NP

@@ -364,6 +364,13 @@ REGISTRY = {
     "cut_glypho": 580,
     "cut_circdes": 581,
     "cut_snowflake": 582,
+    "cut_jigsaw": 583,
+    "cut_rgrid": 584,
+    "cut_x": 585,
+    "cut_metaballs": 586,
+    "cut_kaleido": 587,
+    "cut_spiral": 588,
+    "cut_swarp": 589,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -720,6 +727,15 @@ PARAMS.update({
     "cut_glypho": [("mode", 1.0), ("zoom", 1.0), ("invert", 0.0), ("f1", 0.115), ("f2", 0.75), ("f3", 1.5)],
     "cut_circdes": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("zoom", 10.0), ("invert", 0.0)],
     "cut_snowflake": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("level", 10.0), ("zoom", 10.0), ("invert", 0.0)],
+})
+PARAMS.update({
+    "cut_jigsaw": [("seed", 1000.0), ("time", 0.0), ("mode", 1.0), ("zoom", 4.0), ("invert", 0.0)],
+    "cut_rgrid": [("mode", 1.0), ("zoom", 7.0), ("invert", 0.0), ("angle", 0.0)],
+    "cut_x": [("mode", 1.0), ("zoom", 1.0), ("invert", 0.0), ("size", 0.1)],
+    "cut_metaballs": [("mode", 1.0), ("zoom", 7.0), ("invert", 0.0), ("time", 0.0)],
+    "cut_kaleido": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("n", 6.0), ("zoom", 0.5), ("invert", 0.0)],
+    "cut_spiral": [("time", 0.0), ("mode", 1.0), ("zoom", 2.5), ("invert", 0.0)],
+    "cut_swarp": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("type", 0.0), ("zoom", 1.0), ("invert", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

@@ -319,6 +319,12 @@ WIDER = {
     "post_juliaq": {**dict.fromkeys(["-y", "normal_min"], "zero"), "large": "inf*0"},
     "post_julia3Dq": {**dict.fromkeys(["q3", "q4"], "zero"), "normal_min": "signed-zero"},
     "gamma": dict.fromkeys(["+x", "-x", "+y", "-y", "unit", "half_unit", "y_neg0x", "neg0y_x"], "zero"),
+    # cut_jigsaw's piece orientation hashes the cell: fract(1e5 sin(27 ix + 57 iy)) takes the sine's last
+    # bits 1e5-fold, so the hide branch follows the platform's sine ("large": a cell past 1e6).
+    "cut_jigsaw": {"odd": "branch", "large": "huge"},
+    # cut_metaballs' jitter: fract(43758.5453 sin(.)) of the neighbouring cells, the same amplification,
+    # decides m_dist against its 0.06 step.
+    "cut_metaballs": {"+x": "branch"},
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -358,7 +364,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "spliptic_bs", "pointgrid_wf", "truchet2", "bubbleT3D",
                        "hypertile3D1", "hypertile3D2", "julian3Dx",
                        "cut_sqcir", "cut_yuebing", "cut_sincos", "cut_chains", "cut_hexdots",
-                       "cut_sqsplits", "cut_btree", "cut_fractal", "cut_glypho", "cut_circdes", "cut_snowflake"])
+                       "cut_sqsplits", "cut_btree", "cut_fractal", "cut_glypho", "cut_circdes", "cut_snowflake",
+                       "cut_rgrid", "cut_x", "cut_kaleido", "cut_spiral", "cut_swarp"])
 
 
 def golden():

@@ -78,9 +78,17 @@ def test_every_variation_compiles_for_sm100a(oracle):
     device needed).  The subflame variations are a call of the subflame
     step, not a body of their own."""
     allv = sorted(oracle.REGISTRY, key=oracle.REGISTRY.get)
+    parts, cur, d = [], [], 0
+    for n in allv:                                   # at most 60 a flame, and 48 draws (the final takes more)
+        k = oracle.var_meta(n)[0]
+        if cur and (len(cur) == 60 or d + k > 48):
+            parts.append(cur)
+            cur, d = [], 0
+        cur.append(n)
+        d += k
+    parts.append(cur)
     src = ""
-    for g in range(0, len(allv), 60):
-        part = allv[g:g + 60]
+    for part in parts:
         xfs = [{"a": 0.5, "b": 0.1, "c": -0.1, "d": 0.5, "e": 0.2, "f": -0.3, "weight": 1.0, "color": i / 10,
                 "variations": {n: 0.3 for n in part[i:i + 6]}} for i in range(0, len(part), 6)]
         fin = {"a": 1, "b": 0, "c": 0, "d": 1, "e": 0, "f": 0, "weight": 1, "color": 0.5,
