@@ -954,6 +954,13 @@ static const VarDef kRegistry[] = {
     {"cut_kaleido", 587, 2, 6, {"seed", "mode", "time", "n", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 6.0f, 0.5f, 0.0f}, "v_cut_kaleido", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_spiral", 588, 2, 4, {"time", "mode", "zoom", "invert"}, {0.0f, 1.0f, 2.5f, 0.0f}, "v_cut_spiral", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_swarp", 589, 2, 6, {"seed", "mode", "time", "type", "zoom", "invert"}, {1000.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f}, "v_cut_swarp", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_apollonian", 590, 2, 4, {"mode", "levels", "zoom", "invert"}, {1.0f, 4.0f, 2.0f, 0.0f}, "v_cut_apollonian", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_zigzag", 591, 2, 5, {"mode", "xpar", "ypar", "zoom", "invert"}, {1.0f, 1.0f, 2.0f, 2.0f, 0.0f}, "v_cut_zigzag", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_bricks", 592, 2, 5, {"seed", "mode", "size", "zoom", "invert"}, {1000.0f, 1.0f, 0.9f, 3.0f, 0.0f}, "v_cut_bricks", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_web", 593, 2, 5, {"seed", "time", "mode", "thick", "invert"}, {1000.0f, 0.0f, 1.0f, 0.05f, 1.0f}, "v_cut_web", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_tileillusion", 595, 2, 4, {"time", "mode", "zoom", "invert"}, {0.0f, 1.0f, 15.0f, 0.0f}, "v_cut_tileillusion", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_pattern", 596, 2, 5, {"seed", "mode", "time", "zoom", "invert"}, {1000.0f, 1.0f, 0.9f, 0.5f, 0.0f}, "v_cut_pattern", VF_REPLACE | VF_HIDE, 0, nullptr},
+    {"cut_celtic", 597, 2, 3, {"mode", "zoom", "invert"}, {1.0f, 5.0f, 0.0f}, "v_cut_celtic", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"solid_sphere", 605, 2, 5, {"radius", "thickness", "cx", "cy", "cz"}, {1.0f, 0.1f, 0.0f, 0.0f, 0.0f}, "v_solid_sphere", 0, 0, nullptr},
     {"matrix3D", 643, 0, 12, {"xx", "xy", "xz", "yx", "yy", "yz", "zx", "zy", "zz", "tx", "ty", "tz"}, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f}, "v_matrix3D", 0, 0, nullptr},};
 #undef NP

@@ -371,6 +371,13 @@ REGISTRY = {
     "cut_kaleido": 587,
     "cut_spiral": 588,
     "cut_swarp": 589,
+    "cut_apollonian": 590,
+    "cut_zigzag": 591,
+    "cut_bricks": 592,
+    "cut_web": 593,
+    "cut_tileillusion": 595,
+    "cut_pattern": 596,
+    "cut_celtic": 597,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -736,6 +743,13 @@ PARAMS.update({
     "cut_kaleido": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("n", 6.0), ("zoom", 0.5), ("invert", 0.0)],
     "cut_spiral": [("time", 0.0), ("mode", 1.0), ("zoom", 2.5), ("invert", 0.0)],
     "cut_swarp": [("seed", 1000.0), ("mode", 1.0), ("time", 0.0), ("type", 0.0), ("zoom", 1.0), ("invert", 0.0)],
+    "cut_apollonian": [("mode", 1.0), ("levels", 4.0), ("zoom", 2.0), ("invert", 0.0)],
+    "cut_zigzag": [("mode", 1.0), ("xpar", 1.0), ("ypar", 2.0), ("zoom", 2.0), ("invert", 0.0)],
+    "cut_bricks": [("seed", 1000.0), ("mode", 1.0), ("size", 0.9), ("zoom", 3.0), ("invert", 0.0)],
+    "cut_web": [("seed", 1000.0), ("time", 0.0), ("mode", 1.0), ("thick", 0.05), ("invert", 1.0)],
+    "cut_tileillusion": [("time", 0.0), ("mode", 1.0), ("zoom", 15.0), ("invert", 0.0)],
+    "cut_pattern": [("seed", 1000.0), ("mode", 1.0), ("time", 0.9), ("zoom", 0.5), ("invert", 0.0)],
+    "cut_celtic": [("mode", 1.0), ("zoom", 5.0), ("invert", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

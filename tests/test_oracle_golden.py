@@ -365,7 +365,8 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "hypertile3D1", "hypertile3D2", "julian3Dx",
                        "cut_sqcir", "cut_yuebing", "cut_sincos", "cut_chains", "cut_hexdots",
                        "cut_sqsplits", "cut_btree", "cut_fractal", "cut_glypho", "cut_circdes", "cut_snowflake",
-                       "cut_rgrid", "cut_x", "cut_kaleido", "cut_spiral", "cut_swarp"])
+                       "cut_rgrid", "cut_x", "cut_kaleido", "cut_spiral", "cut_swarp",
+                       "cut_apollonian", "cut_bricks", "cut_web", "cut_tileillusion", "cut_pattern", "cut_celtic"])
 
 
 def golden():
