@@ -934,6 +934,7 @@ static const VarDef kRegistry[] = {
     {"sym_bg6", 566, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg6", 0, 0, nullptr},
     {"sym_bg7", 567, 1, 2, {"stepx", "stepy"}, {0.0f, 0.0f}, "v_sym_bg7", 0, 0, nullptr},
     {"pRose3D", 568, 2, 16, {"l", "k", "c", "z1", "z2", "refSc", "opt", "optSc", "opt3", "transp", "dist", "wagsc", "srvsc", "f", "wigsc", "offset"}, {1.0f, 6.0f, 0.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.5f, 1.0f, 0.0f, 0.0f, 3.0f, 0.0f, 0.0f}, "v_pRose3D", 0, 0, nullptr},
+    {"cut_hextruchetflow", 569, 2, 5, {"randomize", "mode", "grid", "zoom", "invert"}, {0.0f, 1.0f, 0.0f, 10.0f, 0.0f}, "v_cut_hextruchetflow", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_sqcir", 570, 2, 4, {"mode", "zoom", "invert", "power"}, {1.0f, 2.0f, 0.0f, 2.0f}, "v_cut_sqcir", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_yuebing", 571, 2, 5, {"mode", "zoom", "invert", "p1", "p2"}, {1.0f, 0.25f, 0.0f, 2.0f, 25.0f}, "v_cut_yuebing", VF_REPLACE | VF_HIDE, 0, nullptr},
     {"cut_vasarely", 572, 2, 4, {"mode", "zoom", "invert", "size"}, {1.0f, 1.0f, 0.0f, 0.5f}, "v_cut_vasarely", VF_REPLACE | VF_HIDE, 0, nullptr},

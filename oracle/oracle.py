@@ -378,6 +378,7 @@ REGISTRY = {
     "cut_tileillusion": 595,
     "cut_pattern": 596,
     "cut_celtic": 597,
+    "cut_hextruchetflow": 569,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -750,6 +751,7 @@ PARAMS.update({
     "cut_tileillusion": [("time", 0.0), ("mode", 1.0), ("zoom", 15.0), ("invert", 0.0)],
     "cut_pattern": [("seed", 1000.0), ("mode", 1.0), ("time", 0.9), ("zoom", 0.5), ("invert", 0.0)],
     "cut_celtic": [("mode", 1.0), ("zoom", 5.0), ("invert", 0.0)],
+    "cut_hextruchetflow": [("randomize", 0.0), ("mode", 1.0), ("grid", 0.0), ("zoom", 10.0), ("invert", 0.0)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

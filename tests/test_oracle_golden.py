@@ -325,6 +325,10 @@ WIDER = {
     # cut_metaballs' jitter: fract(43758.5453 sin(.)) of the neighbouring cells, the same amplification,
     # decides m_dist against its 0.06 step.
     "cut_metaballs": {"+x": "branch"},
+    # cut_hextruchetflow's arc orientation: fract(43758.54 sin(37 hx + 39 hz)) of the hex cell, at sine
+    # arguments of 72-115 here; every one of these five points takes the reference's side once that
+    # orientation is flipped.
+    "cut_hextruchetflow": dict.fromkeys(["+0+0", "+x", "tiny", "large", "near_threshold"], "branch"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
