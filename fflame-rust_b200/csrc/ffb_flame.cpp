@@ -196,6 +196,15 @@ void derive_bwraps(const float* u, float* o) {                  // extended.rs (
     mb = mb > 2.0f ? 1.0f : mb * (1.0f / ((mb * mb) / 4.0f + 1.0f));
     o[0] = g2; o[1] = rad * rad; o[2] = rad / mb;
 }
+void derive_hypershift2(const float* u, float* o) {             // apo_misc16.rs (init_hypershift2)
+    const float pi = 3.14159265358979f, pi_2 = 1.5707963267948966f;
+    const float p = std::fmax(u[0], 2.0f), q = std::fmax(u[1], 2.0f), pq = pi / q, pp = pi / p;
+    const float spq = std::sin(pq), spp = std::sin(pp);
+    const float shift = std::sin(pi_2 - pq - pp) / std::sqrt(std::fmax(1.0f - spq * spq - spp * spp, 1e-30f));
+    const float s_p2pp = std::sin(pi_2 + pp), r_inner = s_p2pp * s_p2pp / (spq * spq) - 1.0f;
+    const float scale2 = 1.0f / std::sqrt(std::fmax(r_inner, 1e-30f)) * (s_p2pp / spq - 1.0f);
+    o[0] = shift; o[1] = scale2; o[2] = 1.0f - shift * shift; o[3] = 1.0f / p;
+}
 void derive_hypertile(const float* u, float* o) {               // hypertile.rs (init_hypertile)
     const float pi = 3.14159265358979f, pa = 2.0f * pi / u[0], qa = 2.0f * pi / u[1];
     const float ri = (1.0f - std::cos(pa)) / (std::cos(pa) + std::cos(qa)) + 1.0f;
@@ -303,6 +312,16 @@ void derive_ripple(const float* u, float* o) {                  // apo_misc13.rs
     o[0] = u[0] * 5.0f; o[1] = pl; o[2] = s; o[3] = u[1] * pl; o[4] = pl * al; o[5] = (pi - pl) * al;
 }
 void derive_circlecrop(const float* u, float* o) { o[0] = std::min(std::max(u[3], -1.0f), 1.0f); }   // circlecrop_*.rs (init)
+void derive_minkowskope(const float* u, float* o) { o[0] = 0.5f * u[1]; o[1] = 0.5f * u[2]; }   // minkowskope_misc.rs (init)
+void derive_glynnlissa(const float* u, float* o) {              // glynnlissa_misc.rs (init)
+    const float pi = 3.14159265358979f, phi = u[3] * pi / 180.0f;
+    o[0] = u[0] * std::cos(phi); o[1] = u[0] * std::sin(phi); o[2] = std::fabs(u[9]);
+}
+void derive_crop3D(const float* u, float* o) {                  // parametric_curves.rs (init_crop3D)
+    o[0] = std::fmin(u[0], u[3]); o[1] = std::fmax(u[0], u[3]); o[2] = std::fmin(u[1], u[4]);
+    o[3] = std::fmax(u[1], u[4]); o[4] = std::fmin(u[2], u[5]); o[5] = std::fmax(u[2], u[5]);
+}
+void derive_spherecrop(const float* u, float* o) { o[0] = std::min(std::max(u[4], -1.0f), 1.0f); }   // apo_misc18.rs (init)
 void derive_spherical3D_wf(const float* u, float* o) { o[0] = std::fabs(u[1] - 2.0f) < 1e-6f ? 1.0f : 0.0f; }   // apo_misc20.rs
 void derive_hypertile3D(const float* u, float* o) {             // hypertile.rs (init_hypertile3D)
     const float pi = 3.14159265358979f, pa = 2.0f * pi / u[0], qa = 2.0f * pi / u[1];
@@ -501,6 +520,7 @@ static const VarDef kRegistry[] = {
     {"cross", 33, 0, 0, NP, ND, "v_cross", 0, 0, nullptr},
     {"loonie", 34, 0, 0, NP, ND, "v_loonie", 0, 0, nullptr},
     {"scry", 35, 0, 0, NP, ND, "v_scry", 0, 0, nullptr},
+    {"scry_3D", 36, 0, 0, NP, ND, "v_scry_3D", VF_W, 0, nullptr},
     {"foci", 37, 0, 0, NP, ND, "v_foci", 0, 0, nullptr},
     {"elliptic", 38, 0, 0, NP, ND, "v_elliptic", 0, 0, nullptr},
     {"waves2", 39, 0, 6, {"freqx", "scalex", "freqy", "scaley", "freqz", "scalez"}, {2.0f, 1.0f, 2.0f, 1.0f, 0.0f, 0.0f}, "v_waves2", 0, 0, nullptr},
@@ -655,6 +675,7 @@ static const VarDef kRegistry[] = {
     {"fan", 190, 0, 0, NP, ND, "v_fan", VF_XF, 0, nullptr},
     {"fisheye", 191, 0, 0, NP, ND, "v_fisheye", 0, 0, nullptr},
     {"gridout", 192, 0, 0, NP, ND, "v_gridout", 0, 0, nullptr},
+    {"circular", 193, 1, 2, {"angle", "seed"}, {90.0f, 0.0f}, "v_circular", 0, 0, nullptr},
     {"panorama1", 194, 0, 0, NP, ND, "v_panorama1", 0, 0, nullptr},
     {"panorama2", 195, 0, 0, NP, ND, "v_panorama2", 0, 0, nullptr},
     {"mobiusN", 196, 1, 10, {"re_a", "re_b", "re_c", "re_d", "im_a", "im_b", "im_c", "im_d", "power", "dist"}, {1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f, 1.0f}, "v_mobiusN", 0, 0, nullptr},
@@ -665,6 +686,7 @@ static const VarDef kRegistry[] = {
     {"blur_linear", 201, 1, 2, {"length", "angle"}, {1.0f, 0.5f}, "v_blur_linear", 0, 2, derive_blur_linear},
     {"bipolar2", 202, 0, 9, {"shift", "a", "b", "c", "d", "e", "f1", "g1", "h"}, {0.0f, 1.0f, 2.0f, 0.5f, 1.0f, 2.0f, 0.25f, 1.0f, 1.0f}, "v_bipolar2", 0, 0, nullptr},
     {"blob3D", 203, 0, 3, {"low", "high", "waves"}, {0.3f, 1.2f, 6.0f}, "v_blob3D", 0, 0, nullptr},
+    {"circular2", 204, 1, 4, {"angle", "seed", "xx", "yy"}, {90.0f, 0.0f, 12.9898f, 78.233f}, "v_circular2", 0, 0, nullptr},
     {"glynnia", 205, 1, 0, NP, ND, "v_glynnia", 0, 0, nullptr},
     {"glynnia3", 206, 1, 4, {"rscale", "dscale", "rthresh", "ythresh"}, {1.0f, 1.0f, 0.0f, 0.0f}, "v_glynnia3", 0, 0, nullptr},
     {"glynnSim1", 207, 3, 6, {"radius", "radius1", "phi1", "thickness", "pow", "contrast"}, {1.0f, 0.1f, 110.0f, 0.1f, 1.5f, 0.5f}, "v_glynnSim1", 0, 3, derive_glynnSim1},
@@ -686,14 +708,18 @@ static const VarDef kRegistry[] = {
     {"post_julia3Dq", 223, 1, 2, {"power", "divisor"}, {3.0f, 2.0f}, "v_post_julia3Dq", VF_POST | VF_W, 4, derive_post_julia3Dq},
     {"sineblur", 226, 2, 1, {"power"}, {1.0f}, "v_sineblur", 0, 0, nullptr},
     {"starblur", 227, 2, 2, {"power", "range"}, {5.0f, 0.40162283f}, "v_starblur", 0, 2, derive_starblur},
+    {"r_circleblur", 228, 2, 5, {"n", "seed", "dist", "min", "max"}, {1.0f, 0.0f, 0.5f, 0.1f, 1.0f}, "v_r_circleblur", 0, 0, nullptr},
     {"boarders", 229, 1, 0, NP, ND, "v_boarders", 0, 0, nullptr},
     {"boarders2", 230, 1, 3, {"c", "left", "right"}, {0.4f, 0.65f, 0.35f}, "v_boarders2", 0, 3, derive_boarders2},
+    {"pre_boarders2", 231, 1, 3, {"c", "left", "right"}, {0.4f, 0.65f, 0.35f}, "v_pre_boarders2", VF_PRE | VF_W, 3, derive_boarders2},
+    {"splitbrdr", 232, 1, 4, {"x", "y", "px", "py"}, {0.25f, 0.25f, 0.0f, 0.0f}, "v_splitbrdr", VF_W, 0, nullptr},
     {"kaleidoscope", 233, 0, 5, {"pull", "rotate", "line_up", "x", "y"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_kaleidoscope", VF_W, 0, nullptr},
     {"taurus", 234, 0, 4, {"r", "n", "inv", "sor"}, {3.0f, 5.0f, 1.5f, 1.0f}, "v_taurus", 0, 0, nullptr},
     {"hole2", 235, 0, 6, {"a", "b", "c", "d", "inside", "shape"}, {1.0f, 2.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_hole2", 0, 0, nullptr},
     {"spirograph", 236, 2, 9, {"a", "b", "d", "c1", "c2", "tmin", "tmax", "ymin", "ymax"}, {3.0f, 2.0f, 0.0f, 0.0f, 0.0f, -1.0f, 1.0f, -1.0f, 1.0f}, "v_spirograph", 0, 0, nullptr},
     {"lissajous", 237, 2, 7, {"tmin", "tmax", "a", "b", "c", "d", "e"}, {-3.14159265f, 3.14159265f, 3.0f, 2.0f, 0.0f, 0.0f, 0.0f}, "v_lissajous", 0, 0, nullptr},
     {"vogel", 238, 1, 2, {"n", "scale"}, {20.0f, 1.0f}, "v_vogel", 0, 1, derive_vogel},
+    {"crop3D", 239, 2, 8, {"left", "top", "floor", "right", "bottom", "ceiling", "scatter_area", "zero"}, {-1.0f, -1.0f, -1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f}, "v_crop3D", VF_REPLACE, 6, derive_crop3D},
     {"bsplit", 240, 0, 2, {"x", "y"}, {0.0f, 0.0f}, "v_bsplit", VF_HIDE, 0, nullptr},
     {"cylinder2", 241, 0, 0, NP, ND, "v_cylinder2", 0, 0, nullptr},
     {"eclipse", 242, 0, 1, {"shift"}, {0.0f}, "v_eclipse", VF_W, 0, nullptr},
@@ -777,6 +803,7 @@ static const VarDef kRegistry[] = {
     {"conic", 324, 1, 2, {"eccentricity", "holes"}, {1.0f, 0.0f}, "v_conic", VF_W, 0, nullptr},
     {"power", 325, 0, 0, NP, ND, "v_power", 0, 0, nullptr},
     {"roundspher", 326, 0, 0, NP, ND, "v_roundspher", VF_W, 0, nullptr},
+    {"roundspher3D", 327, 0, 0, NP, ND, "v_roundspher3D", VF_W, 0, nullptr},
     {"checks", 330, 2, 4, {"x", "y", "size", "rnd"}, {0.5f, 0.5f, 0.5f, 0.0f}, "v_checks", 0, 1, derive_checks},
     {"cone", 331, 1, 9, {"radius1", "radius2", "size1", "size2", "ywave", "xwave", "height", "warp", "weight"}, {0.5f, 1.0f, 0.5f, 2.0f, 1.0f, 1.0f, 1.0f, 1.0f, 2.0f}, "v_cone", 0, 0, nullptr},
     {"erf", 332, 0, 0, NP, ND, "v_erf", 0, 0, nullptr},
@@ -845,6 +872,7 @@ static const VarDef kRegistry[] = {
     {"julian3Dx", 395, 1, 8, {"power", "dist", "a", "b", "c", "d", "e", "f"}, {0.0f, 1.0f, 1.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f}, "v_julian3Dx", VF_W, 2, derive_julian3Dx},
     {"rosoni", 396, 0, 7, {"maxiter", "sweetiter", "altshapes", "cutoff", "radius", "dx", "dy"}, {25.0f, 3.0f, 0.0f, 1.0f, 0.4f, 0.6f, 0.0f}, "v_rosoni", 0, 2, derive_rosoni},
     {"seashell3D", 397, 2, 4, {"final_radius", "height", "inner_radius", "nSpirals"}, {0.25f, 3.5f, 0.4f, 3.0f}, "v_seashell3D", 0, 0, nullptr},
+    {"hypershift2", 398, 1, 2, {"p", "q"}, {3.0f, 7.0f}, "v_hypershift2", VF_REPLACE, 4, derive_hypershift2},
     {"bwraps7", 399, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_bwraps7", 0, 3, derive_bwraps7},
     {"loq", 400, 0, 1, {"base"}, {2.718281828459045f}, "v_loq", 0, 0, nullptr},
     {"pre_bwraps2", 402, 0, 5, {"cellsize", "space", "gain", "inner_twist", "outer_twist"}, {1.0f, 0.0f, 2.0f, 0.0f, 0.0f}, "v_pre_bwraps2", VF_PRE | VF_W, 3, derive_bwraps2},
@@ -861,7 +889,10 @@ static const VarDef kRegistry[] = {
     {"exblur", 413, 6, 5, {"dist", "r", "x_origin", "y_origin", "z_origin"}, {0.5f, 0.0f, 0.0f, 0.0f, 0.0f}, "v_exblur", 0, 0, nullptr},
     {"curl_sp", 414, 0, 6, {"pow", "c1", "c2", "sx", "sy", "dc"}, {1.0f, -0.01f, 0.03f, 0.0f, 0.0f, 0.0f}, "v_curl_sp", VF_W, 4, derive_curl_sp},
     {"extrude", 415, 1, 1, {"root_face"}, {0.5f}, "v_extrude", 0, 0, nullptr},
+    {"minkowskope", 417, 0, 6, {"separation", "frequencyx", "frequencyy", "amplitude", "perturbation", "damping"}, {0.5f, 1.5f, 1.0f, 0.5f, 0.3f, 0.0f}, "v_minkowskope", 0, 2, derive_minkowskope},
+    {"glynnlissa", 418, 4, 11, {"radius", "radius1", "thickness", "phi1", "a", "b", "width", "phase", "scale", "pow", "contrast"}, {1.0f, 0.5f, 1.0f, 0.0f, 3.0f, 2.0f, 0.0f, 0.0f, 0.71f, 1.5f, 0.5f}, "v_glynnlissa", 0, 3, derive_glynnlissa},
     {"lazysensen", 421, 0, 3, {"scale_x", "scale_y", "scale_z"}, {1.0f, 1.0f, 0.0f}, "v_lazysensen", 0, 0, nullptr},
+    {"spherecrop", 422, 1, 6, {"radius", "x", "y", "z", "scatter_area", "zero"}, {1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.0f}, "v_spherecrop", VF_W | VF_HIDE, 1, derive_spherecrop},
     {"xheart_blur_wf", 423, 2, 2, {"angle", "ratio"}, {0.0f, 0.0f}, "v_xheart_blur_wf", 0, 3, derive_xheart_blur_wf},
     {"circleLinear", 425, 0, 8, {"Sc", "K", "Dens1", "Dens2", "Reverse", "X", "Y", "Seed"}, {1.0f, 0.5f, 0.5f, 0.5f, 1.0f, 10.0f, 10.0f, 0.0f}, "v_circleLinear", 0, 0, nullptr},
     {"cannabiscurve_wf", 426, 1, 1, {"filled"}, {1.0f}, "v_cannabiscurve_wf", 0, 0, nullptr},

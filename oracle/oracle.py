@@ -379,6 +379,18 @@ REGISTRY = {
     "cut_pattern": 596,
     "cut_celtic": 597,
     "cut_hextruchetflow": 569,
+    "circular": 193,
+    "circular2": 204,
+    "r_circleblur": 228,
+    "hypershift2": 398,
+    "spherecrop": 422,
+    "scry_3D": 36,
+    "roundspher3D": 327,
+    "crop3D": 239,
+    "pre_boarders2": 231,
+    "splitbrdr": 232,
+    "minkowskope": 417,
+    "glynnlissa": 418,
 }
 # User parameters and their defaults (the ParamDef lists of
 # src/variations/defs/*.rs); derived values come from the C oracle's
@@ -752,6 +764,19 @@ PARAMS.update({
     "cut_pattern": [("seed", 1000.0), ("mode", 1.0), ("time", 0.9), ("zoom", 0.5), ("invert", 0.0)],
     "cut_celtic": [("mode", 1.0), ("zoom", 5.0), ("invert", 0.0)],
     "cut_hextruchetflow": [("randomize", 0.0), ("mode", 1.0), ("grid", 0.0), ("zoom", 10.0), ("invert", 0.0)],
+    "circular": [("angle", 90.0), ("seed", 0.0)],
+    "circular2": [("angle", 90.0), ("seed", 0.0), ("xx", 12.9898), ("yy", 78.233)],
+    "r_circleblur": [("n", 1.0), ("seed", 0.0), ("dist", 0.5), ("min", 0.1), ("max", 1.0)],
+    "hypershift2": [("p", 3.0), ("q", 7.0)],
+    "spherecrop": [("radius", 1.0), ("x", 0.0), ("y", 0.0), ("z", 0.0), ("scatter_area", 0.0), ("zero", 1.0)],
+    "crop3D": [("left", -1.0), ("top", -1.0), ("floor", -1.0), ("right", 1.0), ("bottom", 1.0), ("ceiling", 1.0),
+               ("scatter_area", 0.0), ("zero", 0.0)],
+    "pre_boarders2": [("c", 0.4), ("left", 0.65), ("right", 0.35)],
+    "splitbrdr": [("x", 0.25), ("y", 0.25), ("px", 0.0), ("py", 0.0)],
+    "minkowskope": [("separation", 0.5), ("frequencyx", 1.5), ("frequencyy", 1.0), ("amplitude", 0.5), ("perturbation", 0.3),
+                    ("damping", 0.0)],
+    "glynnlissa": [("radius", 1.0), ("radius1", 0.5), ("thickness", 1.0), ("phi1", 0.0), ("a", 3.0), ("b", 2.0), ("width", 0.0),
+                   ("phase", 0.0), ("scale", 0.71), ("pow", 1.5), ("contrast", 0.5)],
 })
 PARAMS["pre_subflame_wf"] = PARAMS["subflame_wf"]
 SLOTS = 24         # packed parameter row a variation (user + derived)

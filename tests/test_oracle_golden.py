@@ -329,6 +329,16 @@ WIDER = {
     # arguments of 72-115 here; every one of these five points takes the reference's side once that
     # orientation is flipped.
     "cut_hextruchetflow": dict.fromkeys(["+0+0", "+x", "tiny", "large", "near_threshold"], "branch"),
+    # circular, circular2: the turn adds fract(43758.5453 sin(12.9898 x + 78.233 y)); at sine arguments
+    # of tens to hundreds the platform sine's last bits, 43758-fold, set the turn (agreement where the
+    # argument is 0: the zero inputs).
+    "circular": {**dict.fromkeys(["q1", "q3", "odd", "pi_e", "y_neg0x"], "branch"), "near_threshold": "huge"},
+    "circular2": {**dict.fromkeys(["+y", "-y", "q1", "q3", "odd", "big", "pi_e", "unit", "y_neg0x"], "branch"),
+                  "near_threshold": "huge"},
+    # r_circleblur: the cell's jitter, the same hash of the cell.
+    "r_circleblur": {"half_unit": "branch"},
+    # hypershift2: the draw picks the rotation by f32(pi), whose sine the reference returns as 0.
+    "hypershift2": dict.fromkeys(["+0+0", "+0-0", "normal_min", "subnormal", "lopsided", "y_neg0x"], "zero"),
 }
 FIRST_TWELVE = {"linear", "sinusoidal", "spherical", "swirl", "horseshoe", "polar", "disc", "ex", "julia", "bubble",
                 "cylinder", "curl"}
@@ -370,7 +380,9 @@ EXACT_DIGEST = sorted(["linear", "spherical", "swirl", "horseshoe", "polar", "bu
                        "cut_sqcir", "cut_yuebing", "cut_sincos", "cut_chains", "cut_hexdots",
                        "cut_sqsplits", "cut_btree", "cut_fractal", "cut_glypho", "cut_circdes", "cut_snowflake",
                        "cut_rgrid", "cut_x", "cut_kaleido", "cut_spiral", "cut_swarp",
-                       "cut_apollonian", "cut_bricks", "cut_web", "cut_tileillusion", "cut_pattern", "cut_celtic"])
+                       "cut_apollonian", "cut_bricks", "cut_web", "cut_tileillusion", "cut_pattern", "cut_celtic",
+                       "spherecrop", "scry_3D", "roundspher3D", "crop3D", "pre_boarders2", "splitbrdr", "minkowskope",
+                       "glynnlissa"])
 
 
 def golden():

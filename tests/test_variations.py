@@ -387,10 +387,11 @@ def test_canhide_drops_iterations_and_samples(renderer, oracle, rng_mode):
 @pytest.mark.gpu
 def test_sorted_schedule_with_many_draws(renderer, oracle):
     """20 draw words an iteration (5 blocks of the counter stream): the
-    regrouped walkers keep their streams."""
+    regrouped walkers keep their streams.  The flames alternate between
+    the two streams (each flame's four modules compile separately)."""
     job = dict(iterations=2_000_000, walkers=6000, supersample=1)
     for f, cfg in enumerate(wider_flames(oracle)):
-        for rng in ("philox", "pcg"):
+        for rng in (("philox", "pcg")[f % 2],):
             a, _, oa = renderer.histogram(cfg, 160, 90, schedule="plain", rng=rng, iterations_per_thread=64, **job)
             b, _, ob = renderer.histogram(cfg, 160, 90, schedule="sorted", rng=rng, iterations_per_thread=64, **job)
             assert np.array_equal(a, b), (f, rng)
