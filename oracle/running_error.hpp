@@ -8,7 +8,11 @@
 // ulp of its result; each library function adds three ulps of its result
 // (the device's and the host's libm each within two).  Comparisons,
 // floor and the like act on the value: a result on the far side of a
-// branch or a step from its f32 twin is outside what the bound covers.
+// branch or a step from its f32 twin is outside what the bound covers, so
+// each one taken within its operands' bounds (the values closer than the
+// bounds' sum, or an integer step inside [v - e, v + e]) marks the
+// evaluation undecided (re_undecided()): an f32 twin may have taken the
+// other side, and the caller treats the point's result as arbitrary.
 //
 // The variation bodies are templates over their arithmetic type; the
 // std:: overloads below let the same source run over RE, so each body's
@@ -35,6 +39,23 @@ struct RE {
 
 constexpr double kF32Eps = 1.0 / 8388608.0;
 
+// Set by a comparison or an integer step taken within the bounds; the
+// caller clears it before an evaluation and reads it after.
+inline bool& re_undecided() {
+    static thread_local bool flag = false;
+    return flag;
+}
+// (The bounds are in units of the f32 epsilon.)
+inline void re_compare(const RE& a, const RE& b) {
+    const double e = (a.e + b.e) * kF32Eps;
+    if (e > 0 && std::fabs(a.v - b.v) <= e) re_undecided() = true;
+}
+// An integer step (floor, ceil, trunc, rounding) between v - e and v + e.
+template <class F> inline void re_step(const RE& a, F f) {
+    const double e = a.e * kF32Eps;
+    if (e > 0 && f(a.v - e) != f(a.v + e)) re_undecided() = true;
+}
+
 inline RE re_round(double v, double e, double ulps) { return {v, e + ulps * std::fabs(v)}; }
 inline RE operator+(const RE& a, const RE& b) { return re_round(a.v + b.v, a.e + b.e, 0.5); }
 inline RE operator-(const RE& a, const RE& b) { return re_round(a.v - b.v, a.e + b.e, 0.5); }
@@ -51,12 +72,12 @@ inline RE& RE::operator+=(const RE& o) { return *this = *this + o; }
 inline RE& RE::operator-=(const RE& o) { return *this = *this - o; }
 inline RE& RE::operator*=(const RE& o) { return *this = *this * o; }
 inline RE& RE::operator/=(const RE& o) { return *this = *this / o; }
-inline bool operator<(const RE& a, const RE& b) { return a.v < b.v; }
-inline bool operator>(const RE& a, const RE& b) { return a.v > b.v; }
-inline bool operator<=(const RE& a, const RE& b) { return a.v <= b.v; }
-inline bool operator>=(const RE& a, const RE& b) { return a.v >= b.v; }
-inline bool operator==(const RE& a, const RE& b) { return a.v == b.v; }
-inline bool operator!=(const RE& a, const RE& b) { return a.v != b.v; }
+inline bool operator<(const RE& a, const RE& b) { re_compare(a, b); return a.v < b.v; }
+inline bool operator>(const RE& a, const RE& b) { re_compare(a, b); return a.v > b.v; }
+inline bool operator<=(const RE& a, const RE& b) { re_compare(a, b); return a.v <= b.v; }
+inline bool operator>=(const RE& a, const RE& b) { re_compare(a, b); return a.v >= b.v; }
+inline bool operator==(const RE& a, const RE& b) { re_compare(a, b); return a.v == b.v; }
+inline bool operator!=(const RE& a, const RE& b) { re_compare(a, b); return a.v != b.v; }
 
 // f(a) with derivative d at a: the propagated bound plus three ulps.
 inline RE re_fn(double v, double d, const RE& a) { return re_round(v, std::fabs(d) * a.e, 3.0); }
@@ -105,12 +126,14 @@ inline RE fabs(const RE& a) { return {std::fabs(a.v), a.e}; }
 inline RE abs(const RE& a) { return {std::fabs(a.v), a.e}; }
 inline RE fmax(const RE& a, const RE& b) { return a.v >= b.v || std::isnan(b.v) ? a : b; }
 inline RE fmin(const RE& a, const RE& b) { return a.v <= b.v || std::isnan(b.v) ? a : b; }
-inline RE floor(const RE& a) { return {std::floor(a.v), 0.0}; }
-inline RE ceil(const RE& a) { return {std::ceil(a.v), 0.0}; }
-inline RE trunc(const RE& a) { return {std::trunc(a.v), 0.0}; }
-inline RE nearbyint(const RE& a) { return {std::nearbyint(a.v), 0.0}; }
+inline RE floor(const RE& a) { re_step(a, [](double t) { return std::floor(t); }); return {std::floor(a.v), 0.0}; }
+inline RE ceil(const RE& a) { re_step(a, [](double t) { return std::ceil(t); }); return {std::ceil(a.v), 0.0}; }
+inline RE trunc(const RE& a) { re_step(a, [](double t) { return std::trunc(t); }); return {std::trunc(a.v), 0.0}; }
+inline RE nearbyint(const RE& a) { re_step(a, [](double t) { return std::nearbyint(t); }); return {std::nearbyint(a.v), 0.0}; }
 inline RE fmod(const RE& a, const RE& b) {
     const double v = std::fmod(a.v, b.v), n = b.v != 0 ? std::trunc(a.v / b.v) : 0.0;
+    if (b.v != 0 && a.e > 0 && std::trunc((a.v - a.e * kF32Eps) / b.v) != std::trunc((a.v + a.e * kF32Eps) / b.v))
+        re_undecided() = true;
     return re_round(v, a.e + std::fabs(n) * b.e, 0.5);
 }
 inline bool signbit(const RE& a) { return std::signbit(a.v); }
